@@ -1,0 +1,135 @@
+"""Seeded synthetic RI-GW systems.
+
+The reference benchmarks molecules whose density-fitted tensors come from
+PySCF; here those inputs are replaced by seeded synthetic systems with the
+same shapes and value distributions:
+
+* occupied orbital energies ~ U[-1.2, -0.3] Ha, virtual ~ U[0.05, 3.0] Ha,
+  each block sorted ascending;
+* B[P, p, q] = B[P, q, p] ~ N(0, 0.05^2): the upper triangle p <= q is drawn
+  in the order (P, then row-major p <= q) and mirrored;
+* B is rescaled so that the spectral norm of Pi(i*0) equals ``pi_norm``,
+  where Pi(iw) = 4 * sum_ia B_ia e_ia / (w^2 + e_ia^2) B_ia^T with
+  e_ia = eps_i - eps_a (the reference's sign convention,
+  quasix_core/src/selfenergy/correlation_ac.rs:184-211).  Pi is quadratic in B,
+  so the rescaling is exact and eps(0) = 1 - Pi(0) has eigenvalues in
+  [1, 1 + pi_norm].
+
+The tensor layout is the reference's ``lpq[naux, nmo, nmo]``
+(quasix_core/src/qp/evgw.rs:539-543).
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+
+
+@dataclass
+class SyntheticSystem:
+    mo_energy: np.ndarray  # [nmo]
+    lpq: np.ndarray  # [naux, nmo, nmo], symmetric in the last two indices
+    nocc: int
+    seed: int
+
+    @property
+    def nmo(self) -> int:
+        return self.mo_energy.shape[0]
+
+    @property
+    def naux(self) -> int:
+        return self.lpq.shape[0]
+
+    @property
+    def nvir(self) -> int:
+        return self.nmo - self.nocc
+
+    @property
+    def mo_occ(self) -> np.ndarray:
+        occ = np.zeros(self.nmo)
+        occ[: self.nocc] = 2.0
+        return occ
+
+    # Block views in the layouts the reference's Python front ends pass in
+    # (quasix/src/evgw.rs:103-140): iaP[nocc, nvir, naux], miP[nmo, nocc, naux],
+    # abP[nvir, nvir, naux].
+    def iaP(self) -> np.ndarray:
+        o = self.nocc
+        return np.ascontiguousarray(self.lpq[:, :o, o:].transpose(1, 2, 0))
+
+    def miP(self) -> np.ndarray:
+        o = self.nocc
+        return np.ascontiguousarray(self.lpq[:, :, :o].transpose(1, 2, 0))
+
+    def abP(self) -> np.ndarray:
+        o = self.nocc
+        return np.ascontiguousarray(self.lpq[:, o:, o:].transpose(1, 2, 0))
+
+    def mn_full(self) -> np.ndarray:
+        return np.ascontiguousarray(self.lpq.transpose(1, 2, 0))
+
+
+def pi0_spectral_norm(mo_energy: np.ndarray, lpq: np.ndarray, nocc: int) -> float:
+    """||Pi(i*0)||_2 for the occupied-virtual block of ``lpq``."""
+    naux = lpq.shape[0]
+    bov = lpq[:, :nocc, nocc:].reshape(naux, -1)
+    e_ia = (mo_energy[:nocc, None] - mo_energy[None, nocc:]).reshape(-1)
+    pi0 = 4.0 * (bov / e_ia) @ bov.T
+    return float(np.abs(np.linalg.eigvalsh(pi0)).max())
+
+
+def make_system(nocc: int, nvir: int, naux: int, seed: int, pi_norm: float) -> SyntheticSystem:
+    """Build one seeded synthetic system (see module docstring)."""
+    rng = np.random.default_rng(seed)
+    nmo = nocc + nvir
+    e_occ = np.sort(rng.uniform(-1.2, -0.3, nocc))
+    e_vir = np.sort(rng.uniform(0.05, 3.0, nvir))
+    mo_energy = np.concatenate([e_occ, e_vir])
+    iu, ju = np.triu_indices(nmo)
+    upper = rng.normal(0.0, 0.05, size=(naux, iu.shape[0]))
+    lpq = np.empty((naux, nmo, nmo))
+    lpq[:, iu, ju] = upper
+    lpq[:, ju, iu] = upper
+    scale = np.sqrt(pi_norm / pi0_spectral_norm(mo_energy, lpq, nocc))
+    lpq *= scale
+    return SyntheticSystem(mo_energy=mo_energy, lpq=lpq, nocc=nocc, seed=seed)
+
+
+# Workloads, each named by what it is and its sizes.
+def g0w0_cd_small() -> SyntheticSystem:
+    """nocc 5, nvirt 19, naux 84, seed 0, ||Pi(0)|| = 2."""
+    return make_system(5, 19, 84, seed=0, pi_norm=2.0)
+
+
+def evgw_nmo300() -> SyntheticSystem:
+    """nocc 40, nvirt 260, naux 1000, seed 1, ||Pi(0)|| = 4."""
+    return make_system(40, 260, 1000, seed=1, pi_norm=4.0)
+
+
+def batch64_shapes(seed0: int = 100, count: int = 64):
+    """Shapes of the 64-system batch: nmo ~ U[40, 400] drawn from each system's seed,
+    nocc = round(nmo / 6), naux = round(3.5 nmo), ||Pi(0)|| ~ U[1, 6]."""
+    shapes = []
+    for s in range(seed0, seed0 + count):
+        rng = np.random.default_rng(s + 1_000_000)
+        nmo = int(rng.integers(40, 401))
+        pi_norm = float(rng.uniform(1.0, 6.0))
+        nocc = int(round(nmo / 6))
+        naux = int(round(3.5 * nmo))
+        shapes.append((s, nocc, nmo - nocc, naux, pi_norm))
+    return shapes
+
+
+def batch64_system(index: int) -> SyntheticSystem:
+    s, nocc, nvir, naux, pi_norm = batch64_shapes()[index]
+    return make_system(nocc, nvir, naux, seed=s, pi_norm=pi_norm)
+
+
+def grad_nmo200() -> SyntheticSystem:
+    """nocc 30, nvirt 170, naux 700, seed 7 (pi norm as the small G0W0 case: 2)."""
+    return make_system(30, 170, 700, seed=7, pi_norm=2.0)
+
+
+def bse_dim26400_bov() -> SyntheticSystem:
+    """nocc 60, nvirt 440, naux 1800, seed 11, ||Pi(0)|| = 5 (full tensor is 3.6 GB)."""
+    return make_system(60, 440, 1800, seed=11, pi_norm=5.0)
