@@ -1,0 +1,330 @@
+#!/usr/bin/env python
+"""Benchmark: evGW iterations per second on one B200 (replicas on N GPUs).
+
+Workload (one "step" = one evGW iteration over all orbitals):
+  nocc 40, nvirt 260 (nmo 300), naux 1000, seed 1, ||Pi(0)||_2 = 4, 32-point
+  imaginary-frequency GL grid, linearized QP, reference Pade point rule.
+  Inputs are synthetic (seeded), far larger than L2 (lpq is 720 MB), so no
+  explicit L2 flush is needed between steps.
+
+The headline value is the mixed-precision (tcgen05 BF16x3) form; the plain FP64
+GPU path is timed in the same run and the QP-energy error of the mixed form
+against it is reported in meV.  ``--impl reference`` times the reference's
+algorithm on the host cores (the CPU oracle restatement; the Rust reference
+cannot be built here).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "evGW iter/s: mixed-prec vs FP64 GPU at ≤1 meV QP err; TC util %; CPU ref"
+NOCC, NVIR, NAUX, SEED, PINORM, NW = 40, 260, 1000, 1, 4.0, 32
+WORKLOAD = "evgw_nmo300_naux1000_nw32"
+HA_TO_MEV = 27211.386
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--precision", choices=["bf16x3", "fp64"], default=None)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def dist_setup(n):
+    import torch
+    import torch.distributed as dist
+    if int(os.environ.get("WORLD_SIZE", "1")) > 1:
+        from datetime import timedelta
+        local = int(os.environ.get("LOCAL_RANK", "0"))
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+        return dist.get_rank(), dist.get_world_size(), local
+    return 0, 1, 0
+
+
+class Clocks:
+    """nvidia-smi sampler for the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}",
+                 "--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+                 "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_power_cap", "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=self.f, stderr=subprocess.DEVNULL)
+        except FileNotFoundError:
+            self.p = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.p is not None:
+            self.p.terminate()
+            try:
+                self.p.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.p.kill()
+
+    def summary(self):
+        self.f.flush()
+        self.f.seek(0)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.f.read().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx.append(float(parts[1]))
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[3:7]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f), "measured"
+    except Exception:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
+
+
+def fp64_dgemm_peak_tflops():
+    """cuBLAS DGEMM rate on this GPU (the FP64 tensor-pipe denominator)."""
+    import torch
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    for _ in range(2):
+        torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 1e9
+    for _ in range(5):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        torch.matmul(a, b)
+        e.record()
+        torch.cuda.synchronize()
+        best = min(best, s.elapsed_time(e))
+    del a, b
+    return 2.0 * n ** 3 / (best * 1e-3) / 1e12
+
+
+def contraction_flops(nmo, naux, nw):
+    npair = nmo * (nmo + 1) // 2
+    return 2.0 * naux * naux * npair * nw + 2.0 * naux * npair * nw
+
+
+def iteration_flops(nocc, nvir, naux, nw):
+    nmo = nocc + nvir
+    nov = nocc * nvir
+    p0 = 2.0 * nov * naux * naux * nw / 2.0  # lower-triangle tiles of the symmetric product
+    inv = 2.0 * naux ** 3 * nw
+    return p0 + inv + contraction_flops(nmo, naux, nw)
+
+
+def cpu_reference_sample(sysm, budget_s=15.0):
+    """The reference's per-frequency algorithm (oracle restatement, BLAS threads
+    on every host core) on a bounded sample of one evGW iteration: frequencies
+    are processed until the budget is spent, then scaled to all NW."""
+    from oracle import qx_oracle as O
+    e = sysm.mo_energy
+    lpq = sysm.lpq
+    nocc = sysm.nocc
+    freqs, wts, iw = O.sigma_grid(NW)
+    orbs = list(range(sysm.nmo))
+    lov = lpq[:, :nocc, nocc:]
+    t0 = time.perf_counter()
+    done = 0
+    for w in range(NW):
+        pi = O.get_rho_response(freqs[w], e, lov)
+        wc = O.epsilon_inverse_minus_identity(pi)
+        for n in orbs:
+            q = wc.T @ lpq[:, n, :]
+            np.sum(q * lpq[:, :, n], axis=0)
+        done += 1
+        if time.perf_counter() - t0 > budget_s:
+            break
+    el = time.perf_counter() - t0
+    per_iter = el * NW / done
+    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+    return {"value": 1.0 / per_iter, "unit": "evGW iter/s", "cores": cores, "kind": "port",
+            "sample": f"{done} of {NW} frequencies of one evGW iteration (P0, Cholesky inverse, one GEMM per "
+                      f"orbital for all {sysm.nmo} orbitals), {el:.1f} s, scaled by {NW}/{done}"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    from quasix_b200.synth import make_system
+    sysm = make_system(NOCC, NVIR, NAUX, seed=SEED, pi_norm=PINORM)
+    # Warm-up: one frequency.
+    cpu_reference_sample(sysm, budget_s=0.0)
+    vals = []
+    for _ in range(max(1, args.steps)):
+        vals.append(cpu_reference_sample(sysm, budget_s=max(2.0, 20.0 / max(1, args.steps))))
+    v = statistics.median([x["value"] for x in vals])
+    base = vals[0]
+    base["value"] = v
+    line = {"metric": METRIC, "value": v, "unit": "evGW iter/s", "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / v, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "nocc": NOCC, "nvirt": NVIR, "naux": NAUX, "nw": NW, "seed": SEED,
+                       "orbitals": "all", "qp": "linearized"},
+            "cpu_baseline": base,
+            "e2e": {"value": v, "unit": "evGW iter/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    import torch
+
+    import quasix_b200 as q
+    from quasix_b200 import _native as N
+    from quasix_b200.synth import make_system
+
+    rank, world, local = dist_setup(args.gpus)
+    torch.cuda.set_device(local)
+    dev = local
+    sysm = make_system(NOCC, NVIR, NAUX, seed=SEED, pi_norm=PINORM)
+    nmo = sysm.nmo
+    lpq_d = torch.from_numpy(sysm.lpq).to(f"cuda:{dev}")
+    vxc = np.zeros(nmo)
+    ctx = N.context(dev)
+    have_tc = True
+    prec_main = args.precision or "bf16x3"
+
+    def run(prec, iters, lpq):
+        return q.run_evgw_blocks(sysm.mo_energy, lpq, vxc, sysm.nocc, device=dev, nfreq=NW, precision=prec,
+                                 fixed_iterations=iters, max_iterations=iters)
+
+    def timed(prec, iters, lpq):
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+        t0 = time.perf_counter()
+        r = run(prec, iters, lpq)
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+        el = time.perf_counter() - t0
+        return r, el
+
+    # Warm-up (W steps) for each form, then the timed K steps.
+    try:
+        run(prec_main, args.warmup, lpq_d)
+    except N.QxError as e:
+        if prec_main != "bf16x3":
+            raise
+        have_tc = False
+        prec_main = "fp64"
+        if rank == 0:
+            print(f"# mixed-precision form unavailable ({e}); timing FP64 only", file=sys.stderr)
+        run(prec_main, args.warmup, lpq_d)
+    with Clocks(dev) as clk:
+        res_main, t_main = timed(prec_main, args.steps, lpq_d)
+        launches = ctx.launches()
+        stage = ctx.timings()
+    clocks = clk.summary()
+    res_fp64, t_fp64 = (res_main, t_main)
+    if prec_main != "fp64":
+        run("fp64", min(args.warmup, 1), lpq_d)
+        res_fp64, t_fp64 = timed("fp64", args.steps, lpq_d)
+    # max over ranks
+    if world > 1:
+        tt = torch.tensor([t_main, t_fp64], device=f"cuda:{dev}")
+        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+        t_main, t_fp64 = float(tt[0]), float(tt[1])
+    value = world * args.steps / t_main
+    fp64_rate = world * args.steps / t_fp64
+    err_mev = float(np.abs(res_main["qp_energies"] - res_fp64["qp_energies"]).max() * HA_TO_MEV)
+
+    # End to end through the C ABI with host (pinned) inputs: H2D of lpq and the
+    # energies and D2H of the results happen inside the call.
+    lpq_h = torch.from_numpy(sysm.lpq).pin_memory()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    run(prec_main, args.steps, lpq_h.numpy())
+    torch.cuda.synchronize()
+    t_e2e = time.perf_counter() - t0
+    if world > 1:
+        tt = torch.tensor([t_e2e], device=f"cuda:{dev}")
+        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+        t_e2e = float(tt[0])
+    e2e = {"value": world * args.steps / t_e2e, "unit": "evGW iter/s",
+           "h2d_bytes_per_step": int((sysm.lpq.nbytes + 2 * nmo * 8) / args.steps + nmo * 8 * 2),
+           "d2h_bytes_per_step": int(nmo * 8 * 4)}
+
+    peaks, peak_src = measured_peaks()
+    cflops = contraction_flops(nmo, NAUX, NW)
+    ms_contract = stage["contraction"] / args.steps
+    achieved = cflops / (ms_contract * 1e-3) / 1e12
+    if prec_main == "fp64":
+        dpeak = fp64_dgemm_peak_tflops()
+        roof = {"bound": "tensor", "achieved": achieved, "peak": dpeak, "unit": "TFLOP/s", "frac": achieved / dpeak,
+                "traffic": None, "kernel": "k_pair_contract_f64",
+                "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (FP64 has no entry in MEASURED_PEAKS.json)"}
+    else:
+        pk = peaks.get("bf16_tflops_sustained", peaks.get("bf16_tflops"))
+        roof = {"bound": "tensor", "achieved": achieved, "peak": pk, "unit": "TFLOP/s", "frac": achieved / pk,
+                "traffic": None, "kernel": "k_pair_contract_bf16x3",
+                "peak_source": f"bf16_tflops_sustained, {peak_src}",
+                "mma_flops_per_algorithmic_flop": 3}
+
+    line = {"metric": METRIC, "value": value, "unit": "evGW iter/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * t_main / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "bf16x3->f32" if prec_main == "bf16x3" else "f64",
+            "data": "synthetic",
+            "config": {"workload": WORKLOAD, "nocc": NOCC, "nvirt": NVIR, "naux": NAUX, "nw": NW, "seed": SEED,
+                       "orbitals": "all", "qp": "linearized", "precision": prec_main,
+                       "parallelism": f"replicas{world}" if world > 1 else "single",
+                       "l2": "inputs larger than L2 (lpq 720 MB, pair tensor 361 MB); no flush"},
+            "fp64_gpu_iter_per_s": fp64_rate, "speedup_vs_fp64_gpu": value / fp64_rate,
+            "max_qp_err_meV_vs_fp64": err_mev,
+            "stage_ms_per_step": {k: v / args.steps for k, v in stage.items()},
+            "roofline": roof, "clocks": clocks, "e2e": e2e, "gpu_launches": launches}
+    if rank == 0 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_reference_sample(sysm, budget_s=12.0)
+    if rank == 0:
+        print(json.dumps(line))
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

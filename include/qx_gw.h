@@ -1,0 +1,196 @@
+/*
+ * qx_gw.h -- C ABI of the B200-native RI GW/BSE hot path (libqxgpu.so).
+ *
+ * The entry points mirror the QuasiX Rust API (quasix_core) and its PyO3
+ * bindings; each declaration names the reference interface it replaces, by
+ * file:line within the QuasiX project.  Conventions:
+ *
+ *  - Row-major (C order) arrays, FP64 unless stated.  Complex arrays are
+ *    interleaved (re, im) doubles.
+ *  - Every array argument may be a host pointer or a device pointer of the
+ *    context's device; the library checks with cudaPointerGetAttributes and
+ *    copies host data in and results out inside the call.
+ *  - Every call returns a qx_status; on failure qx_last_error(ctx) holds a
+ *    message.  No exceptions cross the ABI and no device code traps.
+ *  - A context owns one CUDA stream and a cached device workspace; calls on
+ *    one context are serialised by the caller (one thread at a time).
+ */
+#ifndef QX_GW_H
+#define QX_GW_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Mirrors QuasixError (quasix_core/src/common/mod.rs:18-70). */
+typedef enum {
+  QX_OK = 0,
+  QX_ERR_INVALID_INPUT = 1,      /* QuasixError::InvalidInput */
+  QX_ERR_DIMENSION_MISMATCH = 2, /* QuasixError::DimensionMismatch */
+  QX_ERR_NUMERICAL = 3,          /* QuasixError::NumericalError (non-finite, singular) */
+  QX_ERR_CONVERGENCE = 4,        /* QuasixError::ConvergenceError */
+  QX_ERR_NOT_IMPLEMENTED = 5,    /* QuasixError::NotImplemented */
+  QX_ERR_CUDA = 6,               /* CUDA runtime / launch failure */
+  QX_ERR_NO_DEVICE = 7           /* no usable sm_100 device */
+} qx_status;
+
+/* Arithmetic form of the dense contractions (P0, Sigma_c pair contraction,
+ * BSE matvecs).  FP64: the plain path.  BF16X3: tcgen05 tensor cores, each
+ * FP64 operand split into bf16 hi + lo, three products hi*hi + hi*lo + lo*hi
+ * accumulated in FP32 in TMEM; factorisations, Pade and QP stay FP64. */
+typedef enum { QX_PREC_FP64 = 0, QX_PREC_BF16X3 = 1 } qx_precision;
+
+typedef struct qx_ctx qx_ctx;
+
+/* ---- context -------------------------------------------------------------- */
+qx_status qx_ctx_create(qx_ctx** ctx, int device);
+qx_status qx_ctx_destroy(qx_ctx* ctx);
+const char* qx_last_error(const qx_ctx* ctx);
+/* Run on a caller stream (cudaStream_t as void*); NULL restores the context's own. */
+qx_status qx_ctx_set_stream(qx_ctx* ctx, void* stream);
+/* Milliseconds of device time of the last call, per stage (P0, inversion,
+ * contraction, sigma assembly, QP), measured with CUDA events. */
+qx_status qx_ctx_last_timings(const qx_ctx* ctx, double* ms_p0, double* ms_inv, double* ms_contract,
+                              double* ms_sigma, double* ms_qp);
+/* Number of kernel launches issued by the last call. */
+int64_t qx_ctx_last_launches(const qx_ctx* ctx);
+/* Library version string. */
+const char* qx_version(void);
+
+/* ---- freq ----------------------------------------------------------------- */
+/* get_scaled_legendre_roots (quasix_core/src/selfenergy/correlation_ac.rs:94-114):
+ * GL rule on [-1,1] mapped by w = x0 (1+t)/(1-t); host-only, no context. */
+qx_status qx_get_scaled_legendre_roots(int nw, double x0, double* freqs, double* wts);
+
+/* ---- gw: polarizability / screening ---------------------------------------- */
+/* get_rho_response for nfreq imaginary frequencies at once
+ * (correlation_ac.rs:184-211; S3-2 compute_polarizability_p0,
+ * quasix_core/src/dielectric/polarizability.rs:169-275).
+ * lpq_ov: [naux][nocc][nvir]; mo_energy: [nocc+nvir]; pi: [nfreq][naux][naux]. */
+qx_status qx_get_rho_response(qx_ctx* ctx, int nfreq, const double* freqs, const double* mo_energy,
+                              const double* lpq_ov, int naux, int nocc, int nvir, int precision,
+                              double* pi);
+
+/* Wc = (I - Pi)^-1 - I for nfreq matrices (correlation_ac.rs:377-401).
+ * pi, wc: [nfreq][naux][naux] (may alias). */
+qx_status qx_screened_interaction(qx_ctx* ctx, int nfreq, int naux, const double* pi, double* wc);
+
+/* ---- selfenergy ------------------------------------------------------------ */
+/* get_sigma_diag (correlation_ac.rs:241-449).  lpq: [naux][nmo][nmo] (symmetric
+ * in the MO pair), orbs: [norbs].  Outputs sigma, omega: complex
+ * [norbs][nw_sigma_max]; *nw_sigma receives the grid length
+ * (1 + #{GL frequencies < iw_cutoff}).  nw_sigma_max must be >= nw + 1. */
+qx_status qx_get_sigma_diag(qx_ctx* ctx, const double* mo_energy, const double* lpq, const int* orbs,
+                            int norbs, int nmo, int nocc, int naux, int nw, double iw_cutoff, double x0,
+                            int precision, double* sigma, double* omega, int nw_sigma_max,
+                            int* nw_sigma);
+
+/* thiele + ac_pade_thiele_diag (correlation_ac.rs:470-509, 587-654).
+ * sigma, omega: complex [norbs][nw_sigma].  npade < 0 selects the reference's
+ * point rule; npade = k selects 2k points (the [k/k] form).
+ * coeff: complex [nfit][norbs], omega_fit: complex [norbs][nfit]; *nfit out. */
+qx_status qx_ac_pade_thiele_diag(qx_ctx* ctx, int norbs, int nw_sigma, const double* sigma,
+                                 const double* omega, int npade, double* coeff, double* omega_fit,
+                                 int nfit_max, int* nfit);
+
+/* pade_thiele (correlation_ac.rs:530-566) at nomega real points for one orbital. */
+qx_status qx_pade_thiele(int nfit, const double* zn, const double* coeff, int nomega,
+                         const double* omega, double* out);
+
+/* Exchange self-energy diagonal (qp/evgw.rs:1167-1193):
+ * sigma_x[p] = -sum_{i,R} lpq[R][p][i]^2. */
+qx_status qx_compute_exchange_diag(qx_ctx* ctx, const double* lpq, int naux, int nmo, int nocc,
+                                   double* sigma_x);
+
+/* ---- qp: evGW driver -------------------------------------------------------- */
+/* EvGWConfig (quasix_core/src/qp/evgw.rs:161-316) with the fields the driver uses. */
+typedef struct {
+  int max_iterations;          /* 12 */
+  double energy_tolerance;     /* 1e-4 */
+  double damping_factor;       /* 0.5 */
+  double z_min, z_max;         /* 0.1, 0.999 */
+  int use_diis;                /* 1 */
+  int diis_space_dim;          /* 6 */
+  int frontier_convergence;    /* 1 */
+  double frontier_window;      /* 1.0 */
+  int nfreq;                   /* 100 */
+  double iw_cutoff;            /* 5.0 */
+  double x0;                   /* 0.5 */
+  int use_solved_qp;           /* 0 = linearized, 1 = Newton */
+  double newton_energy_tolerance; /* 1e-8 */
+  int newton_max_iterations;   /* 50 */
+  int npade;                   /* -1 = reference point rule, k = [k/k] */
+  int precision;               /* qx_precision */
+  int fixed_iterations;        /* >0: run exactly this many iterations (benchmarking) */
+} qx_evgw_config;
+
+void qx_evgw_config_default(qx_evgw_config* cfg);
+
+/* EvGWResult (qp/evgw.rs:329-350).  Caller-allocated arrays of nmo entries;
+ * history_* arrays hold max_iterations entries (may be NULL). */
+typedef struct {
+  double* qp_energies;   /* [nmo] */
+  double* z_factors;     /* [nmo] */
+  double* sigma_x;       /* [nmo] diagonal */
+  double* sigma_c;       /* complex [nmo] */
+  double* history_energies; /* [max_iterations][nmo] or NULL */
+  double* history_max_change; /* [max_iterations] or NULL */
+  double* history_rms_change; /* [max_iterations] or NULL */
+  int n_iterations;
+  int converged;
+} qx_evgw_result;
+
+/* EvGWDriver::run_evgw_blocks (qp/evgw.rs:420-1049) on lpq [naux][nmo][nmo]
+ * (the driver's permuted mn_full, evgw.rs:539-543); vxc: [nmo]. */
+qx_status qx_evgw(qx_ctx* ctx, const double* mo_energy, const double* lpq, const double* vxc, int nmo,
+                  int nocc, int naux, const qx_evgw_config* cfg, qx_evgw_result* res);
+
+/* ---- G0W0 by contour deformation -------------------------------------------- */
+/* Sigma_c(w) = imaginary-axis GL integral + residues at the real shifts
+ * |w - e_m| (imaginary-axis integrand of compute_sigma_c_pyscf_cd,
+ * quasix_core/src/selfenergy/correlation_pyscf_cd.rs:164-259; residues restated
+ * from the full-frequency formulation, no reference implementation), Newton QP
+ * root for each target.  Outputs [ntarget]. */
+qx_status qx_g0w0_cd(qx_ctx* ctx, const double* mo_energy, const double* lpq, const double* vxc, int nmo,
+                     int nocc, int naux, const int* targets, int ntarget, int nw, double x0, double tol,
+                     int max_iter, int precision, double* qp_energies, double* z_factors,
+                     double* sigma_c, double* sigma_x);
+
+/* ---- bse -------------------------------------------------------------------- */
+typedef struct qx_bse qx_bse;
+/* BSETDAKernel::new (quasix_core/src/bse/kernel.rs:259-337; PyO3
+ * quasix/src/bse.rs:139-200).  delta_qp [nov], df_ia [nov][naux],
+ * df_ij [nocc*nocc][naux], df_ab [nvirt*nvirt][naux], w0 [naux][naux].
+ * spin: 0 singlet (alpha_x = 2), 1 triplet (alpha_x = 0). */
+qx_status qx_bse_create(qx_ctx* ctx, qx_bse** bse, int nocc, int nvirt, int naux, const double* delta_qp,
+                        const double* df_ia, const double* df_ij, const double* df_ab, const double* w0,
+                        int spin, int precision);
+qx_status qx_bse_destroy(qx_bse* bse);
+/* apply_tda_hamiltonian_batch (kernel.rs:550-598): x, y [nov][nvec]. */
+qx_status qx_bse_apply(qx_bse* bse, const double* x, double* y, int nvec);
+
+/* DavidsonConfig / DavidsonResult (quasix_core/src/bse/davidson.rs:47-145). */
+typedef struct {
+  int n_roots, max_iter, max_space;
+  double tol_residual, lindep_threshold, level_shift;
+} qx_davidson_config;
+void qx_davidson_config_default(qx_davidson_config* cfg);
+
+/* solve_davidson / davidson_bse (kernel.rs:652-663, davidson.rs:372-508).
+ * eigenvalues [n_roots], eigenvectors [nov][n_roots], converged [n_roots],
+ * residual_norms [n_roots]. */
+qx_status qx_bse_davidson(qx_bse* bse, const qx_davidson_config* cfg, double* eigenvalues,
+                          double* eigenvectors, int* converged, double* residual_norms,
+                          int* iterations);
+
+/* W(w=0) = (I - Pi(0))^-1 for the screened-direct kernel, from lpq_ov [naux][nocc][nvir]. */
+qx_status qx_bse_w0(qx_ctx* ctx, const double* mo_energy, const double* lpq_ov, int naux, int nocc,
+                    int nvir, double* w0);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* QX_GW_H */

@@ -247,8 +247,8 @@ def pade_point_indices(nw_sigma: int, npade: Optional[int] = None) -> List[int]:
 
     ``npade=None`` is the reference rule (correlation_ac.rs:599-622): indices
     1, 7, 13, ... (< min(40, nw)), then every 4th from the last + 4, truncated to
-    an even count.  ``npade=k`` selects 2k consecutive points from index 1 (the
-    [k/k] variant, e.g. k = 15); it needs nw_sigma >= 2k + 1.
+    an even count.  ``npade=k`` selects 2k points spread evenly over indices
+    1 .. nw_sigma-1 (the [k/k] variant, e.g. k = 15); it needs nw_sigma >= 2k + 1.
     """
     if npade is None:
         idx1 = list(range(1, min(40, nw_sigma), 6))
@@ -260,7 +260,10 @@ def pade_point_indices(nw_sigma: int, npade: Optional[int] = None) -> List[int]:
         return allidx[:nfit]
     if 2 * npade + 1 > nw_sigma:
         raise ValueError(f"[{npade}/{npade}] Pade needs {2 * npade + 1} sigma points, have {nw_sigma}")
-    return list(range(1, 2 * npade + 1))
+    m = 2 * npade
+    if m == 1:
+        return [1]
+    return [int(math.floor(1.0 + j * (nw_sigma - 2) / (m - 1) + 0.5)) for j in range(m)]
 
 
 def ac_pade_thiele_diag(sigma: np.ndarray, omega: np.ndarray, npade: Optional[int] = None):
@@ -713,7 +716,7 @@ def build_mn_full(mo_energy, mo_occ, iaP, ijP, abP, naux) -> Tuple[np.ndarray, i
 def evgw(mo_energy, mo_occ, iaP, ijP, abP, chol_v, vxc_dft, max_cycle=12, conv_tol=1e-4,
          damping=0.5, diis=False, diis_space=6, nfreq=48, frontier_convergence=True,
          frontier_window=1.0, qp_solver="linearized", newton_max_iterations=50,
-         newton_energy_tolerance=1e-8, npade=None, **_unused) -> Dict:
+         newton_energy_tolerance=1e-8, npade=None, iw_cutoff=5.0, **_unused) -> Dict:
     """quasix.quasix.evgw, quasix/src/evgw.rs:22-453 (result dict :339-452)."""
     mo_energy = np.asarray(mo_energy, dtype=np.float64)
     naux = np.asarray(chol_v).shape[0]
@@ -729,7 +732,8 @@ def evgw(mo_energy, mo_occ, iaP, ijP, abP, chol_v, vxc_dft, max_cycle=12, conv_t
                      use_diis=diis, diis_space_dim=diis_space, frontier_convergence=frontier_convergence,
                      frontier_window=frontier_window, nfreq=nfreq, use_solved_qp=solved,
                      newton_energy_tolerance=newton_energy_tolerance,
-                     newton_max_iterations=newton_max_iterations, npade=npade)
+                     newton_max_iterations=newton_max_iterations, npade=npade,
+                     iw_cutoff=iw_cutoff)
     lpq = np.ascontiguousarray(mn.transpose(2, 0, 1))
     mi = mn[:, :n_occ, :]
     res = run_evgw_blocks(mo_energy, mi, np.asarray(vxc_dft, dtype=np.float64), lpq, n_occ, cfg)
@@ -781,7 +785,7 @@ def run_evgw(config: Dict) -> Dict:
                 qp_solver=config.get("qp_solver", "linearized"),
                 newton_max_iterations=config.get("newton_max_iterations", 50),
                 newton_energy_tolerance=config.get("newton_energy_tolerance", 1e-8),
-                npade=config.get("npade"))
+                npade=config.get("npade"), iw_cutoff=config.get("iw_cutoff", 5.0))
 
 
 # ---------------------------------------------------------------------------

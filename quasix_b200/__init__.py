@@ -1,0 +1,17 @@
+"""quasix_b200: B200-native RI GW/BSE hot path of QuasiX (sm_100a CUDA behind a C ABI).
+
+Drop-in entry points with the reference's names and argument meaning:
+``run_evgw`` / ``evgw`` (quasix/src/evgw.rs), ``get_sigma_diag`` and friends
+(quasix_core/src/selfenergy/correlation_ac.rs), ``g0w0_cd``, and the BSE-TDA
+``bse.BSETDAKernel`` / ``run_bse_tda`` (quasix/src/bse.rs, quasix/quasix/bse_driver.py).
+"""
+from . import _native
+from .gw import (ac_pade_thiele_diag, compute_epsilon_inverse_minus_identity, compute_exchange_diag,
+                 compute_polarizability_p0, evgw, g0w0_cd, get_rho_response, get_rho_response_batch,
+                 get_scaled_legendre_roots, get_sigma_diag, pade_thiele, run_evgw, run_evgw_blocks)
+
+__all__ = [
+    "ac_pade_thiele_diag", "compute_epsilon_inverse_minus_identity", "compute_exchange_diag",
+    "compute_polarizability_p0", "evgw", "g0w0_cd", "get_rho_response", "get_rho_response_batch",
+    "get_scaled_legendre_roots", "get_sigma_diag", "pade_thiele", "run_evgw", "run_evgw_blocks",
+]

@@ -1,0 +1,471 @@
+// FP64 kernels of the GW chain: chi weights, eps = I + B chi B^T, block-sweep
+// inversion to Wc = eps^-1 - I, pair gathers, exchange diagonal, the Sigma_c
+// pair contraction v = B_p^T Wc B_p, and the Sigma_c(iw) assembly.
+#include "gemm_f64.cuh"
+#include "qx_internal.cuh"
+
+namespace qx {
+
+// ---------------------------------------------------------------------------
+// chi'[w][k] = -4 e_k / (f_w^2 + e_k^2)  (imaginary axis, e_k = e_i - e_a < 0)
+// chi'[w][k] = -4 e_k / (e_k^2 - f_w^2)  (real axis)
+// so that eps = I - Pi = I + B diag(chi') B^T  (correlation_ac.rs:184-211).
+// ---------------------------------------------------------------------------
+__global__ void k_chi(const double* __restrict__ en, int nocc, int nvir, const double* __restrict__ freqs,
+                      int real_axis, double* __restrict__ chi, int ldov) {
+  const int w = blockIdx.y;
+  const int nov = nocc * nvir;
+  const double f = freqs[w];
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < ldov; k += gridDim.x * blockDim.x) {
+    double v = 0.0;
+    if (k < nov) {
+      const int i = k / nvir, a = k % nvir;
+      const double e = en[i] - en[nocc + a];
+      v = real_axis ? (-4.0 * e / (e * e - f * f)) : (-4.0 * e / (f * f + e * e));
+    }
+    chi[(size_t)w * ldov + k] = v;
+  }
+}
+
+void launch_chi(qx_ctx* ctx, const double* energies, int nocc, int nvir, const double* freqs, int nw,
+                int real_axis, double* chi, int ldov) {
+  dim3 grid(ceil_div(ldov, 256), nw);
+  k_chi<<<grid, 256, 0, ctx->stream>>>(energies, nocc, nvir, freqs, real_axis, chi, ldov);
+  check_launch(ctx);
+}
+
+// ---------------------------------------------------------------------------
+// eps[w] = I + B_ov diag(chi'[w]) B_ov^T on lower-triangular tile pairs,
+// mirrored on store.
+// ---------------------------------------------------------------------------
+using EpsTile = F64Tile<64, 64, 2, 2, 3>;
+
+__global__ void __launch_bounds__(EpsTile::THREADS) k_eps_f64(const double* __restrict__ bov, int ldov, int naux,
+                                                              int nov, const double* __restrict__ chi,
+                                                              double* __restrict__ eps, int ldn,
+                                                              size_t eps_stride) {
+  using T = EpsTile;
+  extern __shared__ double smem[];
+  // Lower-triangular tile index -> (tm, tn), tm >= tn.
+  const int t = blockIdx.x;
+  int tm = (int)floor((sqrt(8.0 * t + 1.0) - 1.0) * 0.5);
+  while ((tm + 1) * (tm + 2) / 2 <= t) ++tm;
+  while (tm * (tm + 1) / 2 > t) --tm;
+  const int tn = t - tm * (tm + 1) / 2;
+  const int w = blockIdx.y;
+  const int m0 = tm * T::BM, n0 = tn * T::BN;
+  double acc[T::MI][T::NJ][2];
+#pragma unroll
+  for (int i = 0; i < T::MI; ++i)
+#pragma unroll
+    for (int j = 0; j < T::NJ; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+  f64_mainloop<T>(acc, smem, bov + (size_t)m0 * ldov, ldov, naux - m0, bov + (size_t)n0 * ldov, ldov, naux - n0,
+                  chi + (size_t)w * ldov, nov);
+  double* E = eps + (size_t)w * eps_stride;
+#pragma unroll
+  for (int i = 0; i < T::MI; ++i)
+#pragma unroll
+    for (int j = 0; j < T::NJ; ++j)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int m = m0 + f64_row<T>(i), n = n0 + f64_col<T>(j, e);
+        if (m < naux && n < naux) {
+          const double v = acc[i][j][e] + (m == n ? 1.0 : 0.0);
+          E[(size_t)m * ldn + n] = v;
+          if (tm != tn) E[(size_t)n * ldn + m] = v;
+        }
+      }
+}
+
+void launch_eps_fp64(qx_ctx* ctx, const double* bov, int ldov, int naux, int nov, const double* chi, int nw,
+                     double* eps, int ldn, size_t eps_stride) {
+  using T = EpsTile;
+  const int tiles = ceil_div(naux, T::BM);
+  dim3 grid(tiles * (tiles + 1) / 2, nw);
+  static bool attr = false;
+  if (!attr) {
+    QX_CUDA(cudaFuncSetAttribute(k_eps_f64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::SMEM));
+    attr = true;
+  }
+  k_eps_f64<<<grid, T::THREADS, T::SMEM, ctx->stream>>>(bov, ldov, naux, nov, chi, eps, ldn, eps_stride);
+  check_launch(ctx);
+}
+
+// ---------------------------------------------------------------------------
+// Block sweep inversion.  For an SPD matrix M and index block K, the sweep
+//   D = M_KK^-1;  M_RR -= M_RK D M_KR;  M_RK = M_RK D;  M_KR = D M_KR;  M_KK = -D
+// applied to every block in turn leaves -M^-1 (Gauss-Jordan without
+// pivoting, stable for SPD).  Panel kernel: D and T = M[:,K] D, P = M[:,K].
+// ---------------------------------------------------------------------------
+constexpr int SWEEP_NB = 64;
+constexpr int PANEL_ROWS = 64;
+
+__global__ void __launch_bounds__(256) k_sweep_panel(const double* __restrict__ M, int n, int ldn, size_t stride,
+                                                     int k0, int kb, double* __restrict__ Tp,
+                                                     double* __restrict__ Pp, double* __restrict__ Dp,
+                                                     int ldp, size_t pstride, int* __restrict__ status) {
+  __shared__ double S[SWEEP_NB][SWEEP_NB + 1];
+  __shared__ double rowp[SWEEP_NB], colp[SWEEP_NB];
+  const int w = blockIdx.y;
+  const double* A = M + (size_t)w * stride;
+  for (int idx = threadIdx.x; idx < SWEEP_NB * SWEEP_NB; idx += blockDim.x) {
+    int i = idx / SWEEP_NB, j = idx % SWEEP_NB;
+    S[i][j] = (i < kb && j < kb) ? A[(size_t)(k0 + i) * ldn + k0 + j] : (i == j ? 1.0 : 0.0);
+  }
+  __syncthreads();
+  // Element-wise sweep of the kb x kb block (leaves -inverse).
+  for (int p = 0; p < kb; ++p) {
+    const double d = S[p][p];
+    if (threadIdx.x < SWEEP_NB) {
+      rowp[threadIdx.x] = S[p][threadIdx.x];
+      colp[threadIdx.x] = S[threadIdx.x][p];
+    }
+    __syncthreads();
+    // eps is positive definite on the imaginary axis; when energies reorder it
+    // can turn indefinite, and the sweep then still inverts it with negative
+    // pivots (the reference falls back from Cholesky to LU there,
+    // correlation_ac.rs:383-399).  Only a zero or non-finite pivot is singular.
+    const bool bad = !(fabs(d) > 0.0) || !isfinite(d);
+    if (bad && threadIdx.x == 0 && blockIdx.x == 0) atomicExch(status + w, 1);
+    const double inv = bad ? 0.0 : 1.0 / d;
+    for (int idx = threadIdx.x; idx < kb * kb; idx += blockDim.x) {
+      int i = idx / kb, j = idx % kb;
+      double v;
+      if (i == p && j == p) v = -inv;
+      else if (i == p) v = rowp[j] * inv;
+      else if (j == p) v = colp[i] * inv;
+      else v = S[i][j] - colp[i] * rowp[j] * inv;
+      S[i][j] = v;
+    }
+    __syncthreads();
+  }
+  // D = -S.
+  if (blockIdx.x == 0) {
+    for (int idx = threadIdx.x; idx < kb * kb; idx += blockDim.x) {
+      int i = idx / kb, j = idx % kb;
+      Dp[(size_t)w * SWEEP_NB * SWEEP_NB + i * SWEEP_NB + j] = -S[i][j];
+    }
+  }
+  // Rows of this CTA: P[r][:] = M[r][K], T[r][:] = M[r][K] D.
+  const int r0 = blockIdx.x * PANEL_ROWS;
+  for (int idx = threadIdx.x; idx < PANEL_ROWS * kb; idx += blockDim.x) {
+    int rr = idx / kb, j = idx % kb;
+    int r = r0 + rr;
+    if (r >= n) continue;
+    const double* row = A + (size_t)r * ldn + k0;
+    double t = 0.0;
+    for (int q = 0; q < kb; ++q) t -= row[q] * S[q][j];
+    Tp[(size_t)w * pstride + (size_t)r * ldp + j] = t;
+    Pp[(size_t)w * pstride + (size_t)r * ldp + j] = row[j];
+  }
+}
+
+using SweepTile = F64Tile<64, 64, 2, 2, 3>;
+
+__global__ void __launch_bounds__(SweepTile::THREADS) k_sweep_update(double* __restrict__ M, int n, int ldn,
+                                                                     size_t stride, int k0, int kb,
+                                                                     const double* __restrict__ Tp,
+                                                                     const double* __restrict__ Pp,
+                                                                     const double* __restrict__ Dp, int ldp,
+                                                                     size_t pstride) {
+  using T = SweepTile;
+  extern __shared__ double smem[];
+  const int w = blockIdx.z;
+  const int m0 = blockIdx.y * T::BM, n0 = blockIdx.x * T::BN;
+  const double* Tw = Tp + (size_t)w * pstride;
+  const double* Pw = Pp + (size_t)w * pstride;
+  double acc[T::MI][T::NJ][2];
+#pragma unroll
+  for (int i = 0; i < T::MI; ++i)
+#pragma unroll
+    for (int j = 0; j < T::NJ; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+  f64_mainloop<T>(acc, smem, Tw + (size_t)m0 * ldp, ldp, n - m0, Pw + (size_t)n0 * ldp, ldp, n - n0, nullptr, kb);
+  double* A = M + (size_t)w * stride;
+  const double* D = Dp + (size_t)w * SWEEP_NB * SWEEP_NB;
+#pragma unroll
+  for (int i = 0; i < T::MI; ++i)
+#pragma unroll
+    for (int j = 0; j < T::NJ; ++j)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int r = m0 + f64_row<T>(i), c = n0 + f64_col<T>(j, e);
+        if (r >= n || c >= n) continue;
+        const bool rk = (r >= k0 && r < k0 + kb), ck = (c >= k0 && c < k0 + kb);
+        double v;
+        if (!rk && !ck) v = A[(size_t)r * ldn + c] - acc[i][j][e];
+        else if (!rk && ck) v = Tw[(size_t)r * ldp + (c - k0)];
+        else if (rk && !ck) v = Tw[(size_t)c * ldp + (r - k0)];
+        else v = -D[(r - k0) * SWEEP_NB + (c - k0)];
+        A[(size_t)r * ldn + c] = v;
+      }
+}
+
+// After the last sweep M = -eps^-1; Wc = eps^-1 - I = -M - I.
+__global__ void k_finish_wc(double* __restrict__ M, int n, int ldn, size_t stride) {
+  const int w = blockIdx.y;
+  double* A = M + (size_t)w * stride;
+  for (size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x; idx < (size_t)n * n;
+       idx += (size_t)gridDim.x * blockDim.x) {
+    int r = (int)(idx / n), c = (int)(idx % n);
+    A[(size_t)r * ldn + c] = -A[(size_t)r * ldn + c] - (r == c ? 1.0 : 0.0);
+  }
+}
+
+void launch_invert_wc(qx_ctx* ctx, double* eps, int n, int ldn, size_t stride, int nw) {
+  using T = SweepTile;
+  const int ldp = SWEEP_NB;
+  const size_t pstride = (size_t)n * ldp;
+  DevBuf& pan = ctx->ws[WS_PANEL];
+  const size_t need = (2 * pstride * nw + (size_t)nw * SWEEP_NB * SWEEP_NB) * sizeof(double) + nw * sizeof(int) + 256;
+  pan.reserve(need);
+  double* Tp = pan.as<double>();
+  double* Pp = Tp + pstride * nw;
+  double* Dp = Pp + pstride * nw;
+  int* status = reinterpret_cast<int*>(Dp + (size_t)nw * SWEEP_NB * SWEEP_NB);
+  QX_CUDA(cudaMemsetAsync(status, 0, nw * sizeof(int), ctx->stream));
+  static bool attr = false;
+  if (!attr) {
+    QX_CUDA(cudaFuncSetAttribute(k_sweep_update, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::SMEM));
+    attr = true;
+  }
+  for (int k0 = 0; k0 < n; k0 += SWEEP_NB) {
+    const int kb = min(SWEEP_NB, n - k0);
+    dim3 pg(ceil_div(n, PANEL_ROWS), nw);
+    k_sweep_panel<<<pg, 256, 0, ctx->stream>>>(eps, n, ldn, stride, k0, kb, Tp, Pp, Dp, ldp, pstride, status);
+    check_launch(ctx);
+    dim3 ug(ceil_div(n, T::BN), ceil_div(n, T::BM), nw);
+    k_sweep_update<<<ug, T::THREADS, T::SMEM, ctx->stream>>>(eps, n, ldn, stride, k0, kb, Tp, Pp, Dp, ldp, pstride);
+    check_launch(ctx);
+  }
+  dim3 fg(ceil_div(n * n, 256 * 4), nw);
+  k_finish_wc<<<fg, 256, 0, ctx->stream>>>(eps, n, ldn, stride);
+  check_launch(ctx);
+  std::vector<int> st(nw);
+  QX_CUDA(cudaMemcpyAsync(st.data(), status, nw * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  QX_CUDA(cudaStreamSynchronize(ctx->stream));
+  for (int w = 0; w < nw; ++w)
+    if (st[w]) {
+      // Singular eps: the reference substitutes the identity for eps^-1
+      // (correlation_ac.rs:390-397), i.e. Wc = 0 at this frequency.
+      fprintf(stderr, "WARNING: Matrix inversion failed at freq %d: singular eps, using Wc = 0\n", w);
+      QX_CUDA(cudaMemset2DAsync(eps + (size_t)w * stride, ldn * sizeof(double), 0, n * sizeof(double), n, ctx->stream));
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Gathers.
+// bpt[p][P] = lpq[P][pairs[p].x][pairs[p].y]   (tiled transpose through smem)
+// ---------------------------------------------------------------------------
+__global__ void k_gather_pairs(const double* __restrict__ lpq, int naux, int nmo, const int2* __restrict__ pairs,
+                               int npair, double* __restrict__ bpt, int ldk) {
+  __shared__ double tile[32][33];
+  __shared__ int off[32];
+  const int p0 = blockIdx.x * 32, P0 = blockIdx.y * 32;
+  if (threadIdx.y == 0) {
+    int p = p0 + threadIdx.x;
+    off[threadIdx.x] = (p < npair) ? pairs[p].x * nmo + pairs[p].y : 0;
+  }
+  __syncthreads();
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    int P = P0 + r, p = p0 + threadIdx.x;
+    tile[r][threadIdx.x] = (P < naux && p < npair) ? lpq[(size_t)P * nmo * nmo + off[threadIdx.x]] : 0.0;
+  }
+  __syncthreads();
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    int p = p0 + r, P = P0 + threadIdx.x;
+    if (p < npair && P < ldk) bpt[(size_t)p * ldk + P] = (P < naux) ? tile[threadIdx.x][r] : 0.0;
+  }
+}
+
+void launch_gather_pairs(qx_ctx* ctx, const double* lpq, int naux, int nmo, const int2* pairs, int npair,
+                         double* bpt, int ldk) {
+  dim3 grid(ceil_div(npair, 32), ceil_div(ldk, 32));
+  k_gather_pairs<<<grid, dim3(32, 8), 0, ctx->stream>>>(lpq, naux, nmo, pairs, npair, bpt, ldk);
+  check_launch(ctx);
+}
+
+// bov[P][i*nvir + a] = lpq[P][i][nocc + a]
+__global__ void k_gather_ov(const double* __restrict__ lpq, int naux, int nmo, int nocc, double* __restrict__ bov,
+                            int ldov) {
+  const int P = blockIdx.y;
+  const int nvir = nmo - nocc;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < ldov; k += gridDim.x * blockDim.x) {
+    double v = 0.0;
+    if (k < nocc * nvir) {
+      int i = k / nvir, a = k % nvir;
+      v = lpq[(size_t)P * nmo * nmo + (size_t)i * nmo + nocc + a];
+    }
+    bov[(size_t)P * ldov + k] = v;
+  }
+}
+
+void launch_gather_ov(qx_ctx* ctx, const double* lpq, int naux, int nmo, int nocc, double* bov, int ldov) {
+  dim3 grid(ceil_div(ldov, 256), naux);
+  k_gather_ov<<<grid, 256, 0, ctx->stream>>>(lpq, naux, nmo, nocc, bov, ldov);
+  check_launch(ctx);
+}
+
+// sx[p] = -sum_{R,i} lpq[R][p][i]^2   (qp/evgw.rs:1167-1193)
+__global__ void k_exchange_diag(const double* __restrict__ lpq, int naux, int nmo, int nocc, double* __restrict__ sx) {
+  const int p = blockIdx.x;
+  double s = 0.0;
+  for (int idx = threadIdx.x; idx < naux * nocc; idx += blockDim.x) {
+    int R = idx / nocc, i = idx % nocc;
+    double v = lpq[(size_t)R * nmo * nmo + (size_t)p * nmo + i];
+    s += v * v;
+  }
+  __shared__ double red[256];
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) sx[p] = -red[0];
+}
+
+void launch_exchange_diag(qx_ctx* ctx, const double* lpq, int naux, int nmo, int nocc, double* sx) {
+  k_exchange_diag<<<nmo, 256, 0, ctx->stream>>>(lpq, naux, nmo, nocc, sx);
+  check_launch(ctx);
+}
+
+// ---------------------------------------------------------------------------
+// Pair contraction: v[w][p] = sum_Q Bpt[p][Q] sum_P Wc[w][Q][P] Bpt[p][P].
+// One CTA per (128-pair block, frequency); it walks every Q tile, so the
+// per-pair sums stay in shared memory and are written once (deterministic).
+// ---------------------------------------------------------------------------
+using PairTile = F64Tile<128, 64, 4, 2, 3>;
+
+__global__ void __launch_bounds__(PairTile::THREADS) k_pair_contract_f64(const double* __restrict__ bpt, int ldk,
+                                                                         int npair, int naux,
+                                                                         const double* __restrict__ wc, int ldn,
+                                                                         size_t wc_stride,
+                                                                         double* __restrict__ v, int ldv) {
+  using T = PairTile;
+  extern __shared__ double smem[];
+  __shared__ double part[T::WARPS_N][T::BM];
+  __shared__ double rowacc[T::BM];
+  const int w = blockIdx.y;
+  const int m0 = blockIdx.x * T::BM;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int wn = warp % T::WARPS_N;
+  for (int i = threadIdx.x; i < T::BM; i += T::THREADS) rowacc[i] = 0.0;
+  const double* Wc = wc + (size_t)w * wc_stride;
+  const double* Arow = bpt + (size_t)m0 * ldk;
+  for (int n0 = 0; n0 < naux; n0 += T::BN) {
+    double acc[T::MI][T::NJ][2];
+#pragma unroll
+    for (int i = 0; i < T::MI; ++i)
+#pragma unroll
+      for (int j = 0; j < T::NJ; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+    f64_mainloop<T>(acc, smem, Arow, ldk, npair - m0, Wc + (size_t)n0 * ldn, ldn, naux - n0, nullptr, naux);
+    // Row partials: sum_n acc[m][n] * Bpt[m0+m][n0+n].
+#pragma unroll
+    for (int i = 0; i < T::MI; ++i) {
+      const int m = f64_row<T>(i);
+      double s = 0.0;
+      if (m0 + m < npair) {
+        const double* brow = bpt + (size_t)(m0 + m) * ldk + n0;
+#pragma unroll
+        for (int j = 0; j < T::NJ; ++j) {
+          const int c = f64_col<T>(j, 0);
+          if (n0 + c + 1 < naux) {
+            double2 bb = *reinterpret_cast<const double2*>(brow + c);
+            s += acc[i][j][0] * bb.x + acc[i][j][1] * bb.y;
+          } else if (n0 + c < naux) {
+            s += acc[i][j][0] * brow[c];
+          }
+        }
+      }
+      s += __shfl_xor_sync(0xffffffffu, s, 1);
+      s += __shfl_xor_sync(0xffffffffu, s, 2);
+      if ((lane & 3) == 0) part[wn][m] = s;
+    }
+    __syncthreads();
+    for (int r = threadIdx.x; r < T::BM; r += T::THREADS) {
+      double s = rowacc[r];
+#pragma unroll
+      for (int q = 0; q < T::WARPS_N; ++q) s += part[q][r];
+      rowacc[r] = s;
+    }
+    __syncthreads();
+  }
+  for (int r = threadIdx.x; r < T::BM; r += T::THREADS)
+    if (m0 + r < npair) v[(size_t)w * ldv + m0 + r] = rowacc[r];
+}
+
+void launch_pair_contract_fp64(qx_ctx* ctx, const double* bpt, int ldk, int npair, int naux, const double* wc,
+                               int ldn, size_t wc_stride, int nw, double* v, int ldv) {
+  using T = PairTile;
+  static bool attr = false;
+  if (!attr) {
+    QX_CUDA(cudaFuncSetAttribute(k_pair_contract_f64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::SMEM));
+    attr = true;
+  }
+  dim3 grid(ceil_div(npair, T::BM), nw);
+  k_pair_contract_f64<<<grid, T::THREADS, T::SMEM, ctx->stream>>>(bpt, ldk, npair, naux, wc, ldn, wc_stride, v, ldv);
+  check_launch(ctx);
+}
+
+// ---------------------------------------------------------------------------
+// Sigma_c(iw_k) = -(1/pi) sum_w sum_m v[w][pair(t,m)] wts_w emo/(emo^2 + f_w^2),
+// emo = s i iw_k + ef - e_m, s = -1 for occupied targets, +1 for virtual
+// (correlation_ac.rs:286-314, 404-438).  One CTA per target; each warp takes
+// one k at a time, lanes stride over m, the frequency loop is outermost.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_sigma_assemble(const double* __restrict__ v, int ldv, int nw,
+                                                        const int* __restrict__ pair_index, int nmo,
+                                                        const int* __restrict__ orbs, int nocc,
+                                                        const double* __restrict__ en, double ef,
+                                                        const double* __restrict__ freqs,
+                                                        const double* __restrict__ wts,
+                                                        const double* __restrict__ iw, int nws,
+                                                        double* __restrict__ sigma) {
+  const int t = blockIdx.x;
+  const int n = orbs[t];
+  const double s = (n < nocc) ? -1.0 : 1.0;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+  const int* pidx = pair_index + (size_t)t * nmo;
+  for (int k = warp; k < nws; k += nwarp) {
+    const double b = s * iw[k];
+    double re = 0.0, im = 0.0;
+    for (int w = 0; w < nw; ++w) {
+      const double f2 = freqs[w] * freqs[w];
+      const double wt = wts[w];
+      double sre = 0.0, sim = 0.0;
+      for (int m = lane; m < nmo; m += 32) {
+        const double a = ef - en[m];
+        // emo = a + ib ; den = emo^2 + f^2 = (a^2 - b^2 + f^2) + i 2ab
+        const double dr = a * a - b * b + f2, di = 2.0 * a * b;
+        const double dd = dr * dr + di * di;
+        const double gr = wt * (a * dr + b * di) / dd;
+        const double gi = wt * (b * dr - a * di) / dd;
+        const double vv = v[(size_t)w * ldv + pidx[m]];
+        sre += vv * gr;
+        sim += vv * gi;
+      }
+      re += sre;
+      im += sim;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      re += __shfl_xor_sync(0xffffffffu, re, o);
+      im += __shfl_xor_sync(0xffffffffu, im, o);
+    }
+    if (lane == 0) {
+      sigma[((size_t)t * nws + k) * 2 + 0] = -re / M_PI;
+      sigma[((size_t)t * nws + k) * 2 + 1] = -im / M_PI;
+    }
+  }
+}
+
+void launch_sigma_assemble(qx_ctx* ctx, const double* v, int ldv, int nw, const int* pair_index, int norbs,
+                           int nmo, const int* orbs, int nocc, const double* energies, double ef,
+                           const double* freqs, const double* wts, const double* iw, int nws,
+                           double* sigma) {
+  k_sigma_assemble<<<norbs, 256, 0, ctx->stream>>>(v, ldv, nw, pair_index, nmo, orbs, nocc, energies, ef, freqs, wts,
+                                                   iw, nws, sigma);
+  check_launch(ctx);
+}
+
+}  // namespace qx

@@ -1,0 +1,539 @@
+// tcgen05 (5th-generation tensor core) kernels for the BF16x3 form.
+//
+// Each FP64 operand X is split into bf16 hi = bf16(X) and lo = bf16(X - hi);
+// a product is formed as hi*hi' + hi*lo' + lo*hi' with FP32 accumulation in
+// TMEM (relative error ~2^-17 per product, vs 2^-9 for one bf16 product).
+//
+// One warp-specialised "NT" GEMM serves both contractions of the GW chain:
+//   C[m][n] = sum_k A[m][k] B[w][n][k]     (A, B K-major, bf16 hi/lo pairs)
+//   EPI_ROWDOT : out[w][m] = sum_n C[m][n] X[m][n]          (Sigma_c pair contraction)
+//   EPI_STORE  : out[w][m][n] = C[m][n] + delta_mn (FP64)   (eps = I + B chi B^T)
+// Warp 0 issues TMA loads (128B-swizzled K-major tiles), warp 1 allocates TMEM
+// and issues tcgen05.mma (M=128, N=BN, K=16), warps 2..5 drain the
+// double-buffered TMEM accumulator with tcgen05.ld.  Every wait is bounded:
+// on timeout the CTA records an error code and unwinds.
+#include <cuda.h>
+#include <cuda_bf16.h>
+
+#include "qx_internal.cuh"
+
+namespace qx {
+
+// ---------------------------------------------------------------------------
+// PTX helpers
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count));
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Bounded wait (about one second of SM clock).  Returns false on timeout or
+// when another thread of the CTA has already aborted.
+constexpr long long WAIT_CYCLES = 2000000000LL;
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort_flag,
+                                          int* err, int code) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const long long t0 = clock64();
+  while (true) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if (*abort_flag) return false;
+    if (clock64() - t0 > WAIT_CYCLES) {
+      *abort_flag = 1;
+      atomicCAS(err, 0, code);
+      return false;
+    }
+  }
+}
+
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, uint64_t* bar, int c0, int c1) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];\n" ::"r"(
+          smem_u32(dst)),
+      "l"(map), "r"(smem_u32(bar)), "r"(c0), "r"(c1)
+      : "memory");
+}
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, uint64_t* bar, int c0, int c1,
+                                            int c2) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], "
+      "[%2];\n" ::"r"(smem_u32(dst)),
+      "l"(map), "r"(smem_u32(bar)), "r"(c0), "r"(c1), "r"(c2)
+      : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory"); }
+
+// SM100 shared-memory matrix descriptor: K-major, 128-byte swizzle, rows of
+// 128 bytes, 8-row groups 1024 bytes apart (SBO), version 1.
+__device__ __forceinline__ uint64_t umma_desc_sw128(uint32_t saddr) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr & 0x3FFFF) >> 4);  // start address
+  d |= (uint64_t)1 << 16;                   // leading byte offset (unused for swizzled K-major)
+  d |= (uint64_t)(1024 >> 4) << 32;         // stride byte offset
+  d |= (uint64_t)1 << 46;                   // descriptor version (sm_100)
+  d |= (uint64_t)2 << 61;                   // SWIZZLE_128B
+  return d;
+}
+
+// Instruction descriptor: kind::f16 with bf16 A/B, f32 accumulator, K-major A and B.
+__host__ __device__ constexpr uint32_t umma_idesc_bf16(int M, int N) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                          uint32_t accumulate) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(
+          tmem_d),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
+}
+__device__ __forceinline__ void umma_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(smem_u32(bar))
+               : "memory");
+}
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// ---------------------------------------------------------------------------
+// The GEMM kernel.
+// ---------------------------------------------------------------------------
+enum { EPI_ROWDOT = 0, EPI_STORE = 1 };
+
+constexpr int TC_BM = 128;
+constexpr int TC_BK = 64;  // one 128-byte swizzle row of bf16
+constexpr int TC_STAGES = 2;
+constexpr int TC_THREADS = 192;
+
+template <int BN>
+struct TcSmem {
+  static constexpr int A_BYTES = TC_BM * TC_BK * 2;
+  static constexpr int B_BYTES = BN * TC_BK * 2;
+  static constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;
+  static constexpr int BAR_OFF = TC_STAGES * STAGE_BYTES;
+  static constexpr int TOTAL = BAR_OFF + 256 + 1024;  // barriers + misc + alignment slack
+};
+
+struct TcArgs {
+  int M, N, K;          // rows of A, rows of B (per batch), reduction length
+  int nbatch;           // frequencies
+  int m_blocks;         // ceil(M / 128)
+  int wgroup;           // frequencies grouped per pair block in the CTA order
+  // EPI_ROWDOT
+  const float* X;       // [M][ldx]
+  int ldx;
+  double* out;          // ROWDOT: [nbatch][ldo]; STORE: [nbatch][M][ldo]
+  int ldo;
+  size_t out_stride;
+  int lower_tiles;      // STORE: enumerate lower-triangular (m, n) tile pairs and mirror
+  int* err;
+};
+
+template <int BN, int EPI>
+__global__ void __launch_bounds__(TC_THREADS, 1)
+    k_tc_gemm(const __grid_constant__ CUtensorMap mapAh, const __grid_constant__ CUtensorMap mapAl,
+              const __grid_constant__ CUtensorMap mapBh, const __grid_constant__ CUtensorMap mapBl, TcArgs args) {
+  using L = TcSmem<BN>;
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + L::BAR_OFF);
+  uint64_t* empty = full + TC_STAGES;
+  uint64_t* acc_full = empty + TC_STAGES;   // [2]
+  uint64_t* acc_empty = acc_full + 2;       // [2]
+  uint64_t* drain = acc_empty + 2;          // all issued MMAs complete
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain + 1);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+  // CTA -> (m block, batch, n tile range).
+  int mb, w, nt_begin, nt_end;
+  const int n_tiles = (args.N + BN - 1) / BN;
+  if (EPI == EPI_ROWDOT) {
+    const int g = args.wgroup;
+    const int per_group = args.m_blocks * g;
+    const int b = blockIdx.x;
+    const int grp = b / per_group, r = b % per_group;
+    mb = r / g;
+    w = grp * g + r % g;
+    nt_begin = 0;
+    nt_end = n_tiles;
+  } else {
+    w = blockIdx.y;
+    if (args.lower_tiles) {
+      const int t = blockIdx.x;
+      int tm = (int)floor((sqrt(8.0 * t + 1.0) - 1.0) * 0.5);
+      while ((tm + 1) * (tm + 2) / 2 <= t) ++tm;
+      while (tm * (tm + 1) / 2 > t) --tm;
+      mb = tm;
+      nt_begin = t - tm * (tm + 1) / 2;
+    } else {
+      mb = blockIdx.x / n_tiles;
+      nt_begin = blockIdx.x % n_tiles;
+    }
+    nt_end = nt_begin + 1;
+  }
+  const bool active = (w < args.nbatch);
+  const int m0 = mb * TC_BM;
+  const int k_blocks = (args.K + TC_BK - 1) / TC_BK;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < TC_STAGES; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&acc_full[b], 1);
+      mbar_init(&acc_empty[b], 4);  // one arrival per epilogue warp
+    }
+    mbar_init(drain, 1);
+    *abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(tmem_slot)),
+                 "r"(2 * BN));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem_base = *tmem_slot;
+
+  if (active) {
+    if (warp == 0) {
+      // ---------------- TMA producer ----------------
+      if (lane == 0) {
+        int g = 0;
+        int issued = 0;
+        for (int nt = nt_begin; nt < nt_end; ++nt) {
+          const int n0 = nt * BN;
+          for (int kb = 0; kb < k_blocks; ++kb, ++g) {
+            const int s = g % TC_STAGES;
+            if (g >= TC_STAGES) {
+              if (!mbar_wait(&empty[s], ((g / TC_STAGES) - 1) & 1, abort_flag, args.err, 1)) goto producer_done;
+            }
+            uint8_t* st = smem + s * L::STAGE_BYTES;
+            mbar_expect_tx(&full[s], L::STAGE_BYTES);
+            const int k0 = kb * TC_BK;
+            tma_load_2d(st, &mapAh, &full[s], k0, m0);
+            tma_load_2d(st + L::A_BYTES, &mapAl, &full[s], k0, m0);
+            tma_load_3d(st + 2 * L::A_BYTES, &mapBh, &full[s], k0, n0, w);
+            tma_load_3d(st + 2 * L::A_BYTES + L::B_BYTES, &mapBl, &full[s], k0, n0, w);
+            issued = g + 1;
+          }
+        }
+      producer_done:
+        if (*abort_flag) {
+          // Let the copies still in flight land before the CTA exits.
+          for (int q = (issued > TC_STAGES ? issued - TC_STAGES : 0); q < issued; ++q) {
+            volatile int no_abort = 0;
+            mbar_wait(&full[q % TC_STAGES], (q / TC_STAGES) & 1, &no_abort, args.err, 5);
+          }
+        }
+      }
+    } else if (warp == 1) {
+      // ---------------- MMA issuer ----------------
+      if (lane == 0) {
+        constexpr uint32_t idesc = umma_idesc_bf16(TC_BM, BN);
+        int g = 0, t = 0;
+        for (int nt = nt_begin; nt < nt_end; ++nt, ++t) {
+          const int buf = t & 1;
+          if (t >= 2) {
+            if (!mbar_wait(&acc_empty[buf], ((t / 2) - 1) & 1, abort_flag, args.err, 2)) break;
+          }
+          tc_fence_after();
+          const uint32_t dacc = tmem_base + buf * BN;
+          bool ok = true;
+          for (int kb = 0; kb < k_blocks; ++kb, ++g) {
+            const int s = g % TC_STAGES;
+            if (!mbar_wait(&full[s], (g / TC_STAGES) & 1, abort_flag, args.err, 3)) {
+              ok = false;
+              break;
+            }
+            tc_fence_after();
+            uint8_t* st = smem + s * L::STAGE_BYTES;
+            const uint32_t ah = smem_u32(st), al = ah + L::A_BYTES;
+            const uint32_t bh = ah + 2 * L::A_BYTES, bl = bh + L::B_BYTES;
+#pragma unroll
+            for (int kk = 0; kk < TC_BK / 16; ++kk) {
+              const uint32_t off = kk * 32;
+              const uint32_t acc0 = (kb > 0 || kk > 0) ? 1u : 0u;
+              umma_bf16(dacc, umma_desc_sw128(ah + off), umma_desc_sw128(bh + off), idesc, acc0);
+              umma_bf16(dacc, umma_desc_sw128(ah + off), umma_desc_sw128(bl + off), idesc, 1u);
+              umma_bf16(dacc, umma_desc_sw128(al + off), umma_desc_sw128(bh + off), idesc, 1u);
+            }
+            umma_commit(&empty[s]);
+          }
+          if (!ok) break;
+          umma_commit(&acc_full[buf]);
+        }
+        // Wait until every MMA this thread issued has completed (TMEM and the
+        // stages are released only after that).
+        umma_commit(drain);
+        volatile int no_abort = 0;
+        mbar_wait(drain, 0, &no_abort, args.err, 6);
+      }
+    } else {
+      // ---------------- epilogue (warps 2..5) ----------------
+      const int quarter = warp & 3;  // TMEM lane quarter this warp may access
+      const int row = quarter * 32 + lane;
+      const int m = m0 + row;
+      double rowsum = 0.0;
+      int t = 0;
+      for (int nt = nt_begin; nt < nt_end; ++nt, ++t) {
+        const int buf = t & 1;
+        if (!mbar_wait(&acc_full[buf], (t / 2) & 1, abort_flag, args.err, 4)) break;
+        tc_fence_after();
+        const int n0 = nt * BN;
+        const uint32_t taddr = tmem_base + ((uint32_t)(quarter * 32) << 16) + buf * BN;
+#pragma unroll 1
+        for (int c = 0; c < BN; c += 16) {
+          float v[16];
+          tmem_ld16(taddr + c, v);
+          if (EPI == EPI_ROWDOT) {
+            if (m < args.M) {
+              const float* xr = args.X + (size_t)m * args.ldx + n0 + c;
+              if (n0 + c + 16 <= args.N) {
+#pragma unroll
+                for (int q = 0; q < 16; q += 4) {
+                  const float4 xx = *reinterpret_cast<const float4*>(xr + q);
+                  rowsum += (double)v[q] * xx.x + (double)v[q + 1] * xx.y + (double)v[q + 2] * xx.z +
+                            (double)v[q + 3] * xx.w;
+                }
+              } else {
+                for (int q = 0; q < 16 && n0 + c + q < args.N; ++q) rowsum += (double)v[q] * xr[q];
+              }
+            }
+          } else {
+            if (m < args.M) {
+              double* orow = args.out + (size_t)w * args.out_stride + (size_t)m * args.ldo;
+#pragma unroll
+              for (int q = 0; q < 16; ++q) {
+                const int n = n0 + c + q;
+                // Lower-triangular mode writes the lower triangle and mirrors it,
+                // so the stored matrix is exactly symmetric.
+                if (n < args.N && !(args.lower_tiles && n > m)) {
+                  const double val = (double)v[q] + (m == n ? 1.0 : 0.0);
+                  orow[n] = val;
+                  if (args.lower_tiles && n != m)
+                    args.out[(size_t)w * args.out_stride + (size_t)n * args.ldo + m] = val;
+                }
+              }
+            }
+          }
+        }
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&acc_empty[buf]);
+      }
+      if (EPI == EPI_ROWDOT && m < args.M && t == nt_end - nt_begin)
+        args.out[(size_t)w * args.ldo + m] = rowsum;
+    }
+  }
+  // Teardown: every warp reaches this point (all waits are bounded).
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == 1) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem_base), "r"(2 * BN));
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Host side: tensor maps and launchers.
+// ---------------------------------------------------------------------------
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn encode_fn() {
+  static EncodeTiledFn fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    QX_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q));
+    QX_REQUIRE(p != nullptr && q == cudaDriverEntryPointSuccess, QX_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
+    fn = reinterpret_cast<EncodeTiledFn>(p);
+  }
+  return fn;
+}
+
+// bf16 matrix [batch][rows][ld] (K contiguous, K valid = cols) with box {64, box_rows, 1}.
+static CUtensorMap make_map(const void* base, int cols, int rows, int ld, int batch, int box_rows, int rank) {
+  QX_REQUIRE((reinterpret_cast<uintptr_t>(base) & 15) == 0 && (ld * 2) % 16 == 0, QX_ERR_INVALID_INPUT,
+             "tensor map base/stride not 16-byte aligned");
+  CUtensorMap m;
+  cuuint64_t dims[3] = {(cuuint64_t)cols, (cuuint64_t)rows, (cuuint64_t)batch};
+  cuuint64_t strides[2] = {(cuuint64_t)ld * 2, (cuuint64_t)ld * 2 * rows};
+  cuuint32_t box[3] = {(cuuint32_t)TC_BK, (cuuint32_t)box_rows, 1};
+  cuuint32_t estr[3] = {1, 1, 1};
+  CUresult r = encode_fn()(&m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, rank, const_cast<void*>(base), dims, strides, box,
+                           estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                           CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  QX_REQUIRE(r == CUDA_SUCCESS, QX_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+  return m;
+}
+
+bool tc_supported(qx_ctx* ctx) {
+  cudaDeviceProp p;
+  if (cudaGetDeviceProperties(&p, ctx->device) != cudaSuccess) return false;
+  return p.major == 10;
+}
+
+// Split: hi = bf16(s x), lo = bf16(s x - hi), s = scale[batch][col] (or 1).
+__global__ void k_split_bf16(const double* __restrict__ src, int rows, int cols, int ld_src, size_t src_stride,
+                             __nv_bfloat16* __restrict__ hi, __nv_bfloat16* __restrict__ lo, int ld_dst,
+                             size_t dst_stride, const double* __restrict__ scale, int ld_scale) {
+  const int b = blockIdx.y;
+  const size_t total = (size_t)rows * ld_dst;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+    const int r = (int)(i / ld_dst), c = (int)(i % ld_dst);
+    double x = 0.0;
+    if (c < cols) {
+      x = src[(size_t)b * src_stride + (size_t)r * ld_src + c];
+      if (scale) x *= scale[(size_t)b * ld_scale + c];
+    }
+    const __nv_bfloat16 h = __float2bfloat16_rn((float)x);
+    const double rem = x - (double)__bfloat162float(h);
+    hi[(size_t)b * dst_stride + i] = h;
+    lo[(size_t)b * dst_stride + i] = __float2bfloat16_rn((float)rem);
+  }
+}
+
+static void split(qx_ctx* ctx, const double* src, int rows, int cols, int ld_src, size_t src_stride, void* hi,
+                  void* lo, int ld_dst, size_t dst_stride, int batch, const double* scale, int ld_scale) {
+  const size_t total = (size_t)rows * ld_dst;
+  dim3 grid((unsigned)std::min<size_t>((total + 255) / 256, 4096), batch);
+  k_split_bf16<<<grid, 256, 0, ctx->stream>>>(src, rows, cols, ld_src, src_stride,
+                                              reinterpret_cast<__nv_bfloat16*>(hi),
+                                              reinterpret_cast<__nv_bfloat16*>(lo), ld_dst, dst_stride, scale,
+                                              ld_scale);
+  check_launch(ctx);
+}
+
+void launch_split_bf16(qx_ctx* ctx, const double* src, int rows, int cols, int ld_src, void* hi, void* lo,
+                       int ld_dst, size_t src_stride, size_t dst_stride, int batch) {
+  split(ctx, src, rows, cols, ld_src, src_stride, hi, lo, ld_dst, dst_stride, batch, nullptr, 0);
+}
+
+static int* tc_err_slot(qx_ctx* ctx) {
+  DevBuf& b = ctx->ws[WS_TCERR];
+  b.reserve(256);
+  return b.as<int>();
+}
+
+static void check_tc_err(qx_ctx* ctx, int* d_err) {
+  int e = 0;
+  QX_CUDA(cudaMemcpyAsync(&e, d_err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  QX_CUDA(cudaStreamSynchronize(ctx->stream));
+  QX_REQUIRE(e == 0, QX_ERR_CUDA, "tcgen05 GEMM pipeline wait timed out (code %d)", e);
+}
+
+template <int BN, int EPI>
+static void launch_tc(qx_ctx* ctx, const CUtensorMap& ah, const CUtensorMap& al, const CUtensorMap& bh,
+                      const CUtensorMap& bl, const TcArgs& a, dim3 grid) {
+  using L = TcSmem<BN>;
+  static bool attr = false;
+  if (!attr) {
+    QX_CUDA(cudaFuncSetAttribute(k_tc_gemm<BN, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, L::TOTAL));
+    attr = true;
+  }
+  k_tc_gemm<BN, EPI><<<grid, TC_THREADS, L::TOTAL, ctx->stream>>>(ah, al, bh, bl, a);
+  check_launch(ctx);
+}
+
+// v[w][p] = sum_Q X[p][Q] sum_P (Bh+Bl)[p][P] (Wh+Wl)[w][Q][P]   (three products)
+void launch_pair_contract_bf16x3(qx_ctx* ctx, const void* bpt_hi, const void* bpt_lo, const float* bpt_f32, int ldk,
+                                 int npair, int naux, const void* wc_hi, const void* wc_lo, int ldw,
+                                 size_t wc_stride, int nw, double* v, int ldv) {
+  constexpr int BN = 256;
+  QX_REQUIRE(wc_stride == (size_t)naux * ldw, QX_ERR_INVALID_INPUT, "Wc stride must be naux*ldw");
+  CUtensorMap ah = make_map(bpt_hi, naux, npair, ldk, 1, TC_BM, 2);
+  CUtensorMap al = make_map(bpt_lo, naux, npair, ldk, 1, TC_BM, 2);
+  CUtensorMap bh = make_map(wc_hi, naux, naux, ldw, nw, BN, 3);
+  CUtensorMap bl = make_map(wc_lo, naux, naux, ldw, nw, BN, 3);
+  int* d_err = tc_err_slot(ctx);
+  QX_CUDA(cudaMemsetAsync(d_err, 0, sizeof(int), ctx->stream));
+  TcArgs a{};
+  a.M = npair;
+  a.N = naux;
+  a.K = naux;
+  a.nbatch = nw;
+  a.m_blocks = ceil_div(npair, TC_BM);
+  a.wgroup = std::min(nw, 8);
+  a.X = bpt_f32;
+  a.ldx = ldk;
+  a.out = v;
+  a.ldo = ldv;
+  a.err = d_err;
+  const int groups = ceil_div(nw, a.wgroup);
+  launch_tc<BN, EPI_ROWDOT>(ctx, ah, al, bh, bl, a, dim3(groups * a.m_blocks * a.wgroup));
+  check_tc_err(ctx, d_err);
+}
+
+// eps[w] = I + Bov diag(chi[w]) Bov^T with A = split(Bov), B = split(Bov * chi[w]).
+void launch_eps_bf16x3(qx_ctx* ctx, const double* bov, int ldov, int naux, int nov, const double* chi, int nw,
+                       double* eps, int ldn, size_t eps_stride) {
+  constexpr int BN = 128;
+  const size_t a_elems = (size_t)naux * ldov;
+  DevBuf& buf = ctx->ws[WS_BOV_HI];
+  buf.reserve(a_elems * 2 * 2 * (1 + (size_t)nw));
+  uint8_t* p = buf.as<uint8_t>();
+  void* a_hi = p;
+  void* a_lo = p + a_elems * 2;
+  void* b_hi = p + a_elems * 4;
+  void* b_lo = p + a_elems * 4 + a_elems * 2 * nw;
+  split(ctx, bov, naux, nov, ldov, 0, a_hi, a_lo, ldov, 0, 1, nullptr, 0);
+  split(ctx, bov, naux, nov, ldov, 0, b_hi, b_lo, ldov, a_elems, nw, chi, ldov);
+  CUtensorMap ah = make_map(a_hi, nov, naux, ldov, 1, TC_BM, 2);
+  CUtensorMap al = make_map(a_lo, nov, naux, ldov, 1, TC_BM, 2);
+  CUtensorMap bh = make_map(b_hi, nov, naux, ldov, nw, BN, 3);
+  CUtensorMap bl = make_map(b_lo, nov, naux, ldov, nw, BN, 3);
+  int* d_err = tc_err_slot(ctx);
+  QX_CUDA(cudaMemsetAsync(d_err, 0, sizeof(int), ctx->stream));
+  TcArgs a{};
+  a.M = naux;
+  a.N = naux;
+  a.K = nov;
+  a.nbatch = nw;
+  a.m_blocks = ceil_div(naux, TC_BM);
+  a.out = eps;
+  a.ldo = ldn;
+  a.out_stride = eps_stride;
+  a.lower_tiles = 1;
+  a.err = d_err;
+  const int tiles = ceil_div(naux, TC_BM);  // BM == BN for the symmetric product
+  static_assert(BN == TC_BM, "eps tiles are square");
+  launch_tc<BN, EPI_STORE>(ctx, ah, al, bh, bl, a, dim3(tiles * (tiles + 1) / 2, nw));
+  check_tc_err(ctx, d_err);
+}
+
+}  // namespace qx

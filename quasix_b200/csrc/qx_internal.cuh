@@ -1,0 +1,213 @@
+// Internal declarations shared by the CUDA translation units of libqxgpu.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cmath>
+#include <complex>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/qx_gw.h"
+
+namespace qx {
+
+// Error carried to the C ABI boundary as a qx_status plus message.
+struct Error : public std::runtime_error {
+  qx_status status;
+  Error(qx_status s, const std::string& m) : std::runtime_error(m), status(s) {}
+};
+
+inline std::string fmt(const char* f, ...) {
+  char buf[1024];
+  va_list ap;
+  va_start(ap, f);
+  vsnprintf(buf, sizeof(buf), f, ap);
+  va_end(ap);
+  return std::string(buf);
+}
+
+#define QX_CUDA(call)                                                                    \
+  do {                                                                                   \
+    cudaError_t e_ = (call);                                                             \
+    if (e_ != cudaSuccess)                                                               \
+      throw ::qx::Error(QX_ERR_CUDA, ::qx::fmt("%s failed: %s (%s:%d)", #call,          \
+                                               cudaGetErrorString(e_), __FILE__, __LINE__)); \
+  } while (0)
+
+#define QX_REQUIRE(cond, status, ...)                       \
+  do {                                                      \
+    if (!(cond)) throw ::qx::Error(status, ::qx::fmt(__VA_ARGS__)); \
+  } while (0)
+
+// Device buffer owned by a context; grows, never shrinks, reused across calls.
+struct DevBuf {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+  void reserve(size_t n) {
+    if (n <= bytes) return;
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    bytes = 0;
+    QX_CUDA(cudaMalloc(&ptr, n));
+    bytes = n;
+  }
+  template <class T>
+  T* as() const { return reinterpret_cast<T*>(ptr); }
+  ~DevBuf() {
+    if (ptr) cudaFree(ptr);
+  }
+};
+
+}  // namespace qx
+
+// Stage indices for timing.
+enum { QX_ST_P0 = 0, QX_ST_INV, QX_ST_CONTRACT, QX_ST_SIGMA, QX_ST_QP, QX_ST_COUNT };
+
+struct qx_ctx {
+  int device = 0;
+  int sm_count = 148;
+  cudaStream_t own_stream = nullptr;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  int64_t launches = 0;
+  double stage_ms[QX_ST_COUNT] = {0, 0, 0, 0, 0};
+  cudaEvent_t ev[2 * QX_ST_COUNT] = {};
+  // Named workspace slots.
+  qx::DevBuf ws[32];
+};
+
+namespace qx {
+
+// Workspace slot identifiers.
+enum WsSlot {
+  WS_LPQ = 0,     // lpq copy when the caller passes host memory
+  WS_BPT,         // gathered pair tensor [npair][ldk] FP64
+  WS_BOV,         // B_ov [naux][ldov] FP64
+  WS_CHI,         // chi' [nw][ldov]
+  WS_EPS,         // eps / Wc [nw][naux][ldn]
+  WS_PANEL,       // sweep panels
+  WS_VPAIR,       // v[w][npair]
+  WS_SIGMA,       // sigma [norbs][nws] complex
+  WS_SMALL,       // small per-call arrays (energies, grids, indices)
+  WS_QPOUT,       // QP outputs
+  WS_BPT_HI,      // bf16 split pair tensor
+  WS_BPT_LO,
+  WS_BOV_HI,
+  WS_BOV_LO,
+  WS_WC_HI,
+  WS_WC_LO,
+  WS_BPT_F32,     // FP32 copy of the pair tensor (epilogue operand)
+  WS_HOSTIN,      // generic staging
+  WS_BSE0, WS_BSE1, WS_BSE2, WS_BSE3, WS_BSE4, WS_BSE5, WS_BSE6, WS_BSE7,
+  WS_CD0, WS_CD1, WS_CD2, WS_CD3,
+  WS_TCERR,       // tcgen05 pipeline error word
+  WS_COUNT
+};
+static_assert(WS_COUNT <= 32, "workspace slots");
+
+// Is p a device-accessible pointer of the current device?
+bool is_device_ptr(const void* p);
+
+// Make a device copy of a caller array when it is host memory; returns the
+// device pointer to read.
+const void* device_view(qx_ctx* ctx, int slot, const void* p, size_t bytes);
+
+inline int ceil_div(int a, int b) { return (a + b - 1) / b; }
+inline int round_up(int a, int b) { return ceil_div(a, b) * b; }
+
+inline void check_launch(qx_ctx* ctx) {
+  ctx->launches++;
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) throw Error(QX_ERR_CUDA, fmt("kernel launch failed: %s", cudaGetErrorString(e)));
+}
+
+// Stage timer (CUDA events on the context stream).
+struct StageTimer {
+  qx_ctx* ctx;
+  int st;
+  StageTimer(qx_ctx* c, int s) : ctx(c), st(s) { cudaEventRecord(ctx->ev[2 * s], ctx->stream); }
+  ~StageTimer() { cudaEventRecord(ctx->ev[2 * st + 1], ctx->stream); }
+};
+
+// ---------------------------------------------------------------------------
+// Host-side numerics shared by the drivers.
+// ---------------------------------------------------------------------------
+void scaled_legendre_roots(int nw, double x0, double* freqs, double* wts);
+
+// ---------------------------------------------------------------------------
+// Kernel launchers (defined in the .cu files).
+// ---------------------------------------------------------------------------
+// chi'[w][k] = -4 e_k / (f_w^2 + e_k^2) (imaginary axis) or -4 e_k / (e_k^2 - f_w^2)
+// (real axis), e_k = e_i - e_a over the ov pairs in row-major (i, a) order.
+void launch_chi(qx_ctx* ctx, const double* energies, int nocc, int nvir, const double* freqs, int nw,
+                int real_axis, double* chi, int ldov);
+
+// eps[w] = I + B_ov diag(chi'[w]) B_ov^T for nw frequencies (FP64).
+void launch_eps_fp64(qx_ctx* ctx, const double* bov, int ldov, int naux, int nov, const double* chi, int nw,
+                     double* eps, int ldn, size_t eps_stride);
+
+// In-place inversion of nw SPD matrices by the block sweep operator;
+// output Wc = eps^-1 - I (FP64).
+void launch_invert_wc(qx_ctx* ctx, double* eps, int n, int ldn, size_t stride, int nw);
+
+// v[w][p] = Bpt[p]^T Wc[w] Bpt[p] for all pairs (FP64).
+void launch_pair_contract_fp64(qx_ctx* ctx, const double* bpt, int ldk, int npair, int naux, const double* wc,
+                               int ldn, size_t wc_stride, int nw, double* v, int ldv);
+
+// Gathers.
+void launch_gather_pairs(qx_ctx* ctx, const double* lpq, int naux, int nmo, const int2* pairs, int npair,
+                         double* bpt, int ldk);
+void launch_gather_ov(qx_ctx* ctx, const double* lpq, int naux, int nmo, int nocc, double* bov, int ldov);
+void launch_exchange_diag(qx_ctx* ctx, const double* lpq, int naux, int nmo, int nocc, double* sx);
+
+// Sigma_c(iw_k) assembly: sigma[t][k] (complex) for each target t.
+void launch_sigma_assemble(qx_ctx* ctx, const double* v, int ldv, int nw, const int* pair_index, int norbs,
+                           int nmo, const int* orbs, int nocc, const double* energies, double ef,
+                           const double* freqs, const double* wts, const double* iw, int nws,
+                           double* sigma);
+
+// Pade + QP per orbital (see k_qp.cu for the exact semantics).
+struct QPParams {
+  int norbs;
+  int nws;
+  int nfit;
+  const int* fit_idx;       // [nfit]
+  const double* sigma;      // complex [norbs][nws]
+  const double* iw;         // [nws]
+  const int* orbs;          // [norbs]
+  int nocc;
+  const double* mo_energy;  // reference (HF) energies [nmo]
+  const double* eval_energy;// evaluation energies [nmo] (HF at iteration 0, previous QP after)
+  const double* sigma_x;    // [nmo]
+  const double* vxc;        // [nmo]
+  double ef;
+  double z_min, z_max;
+  int solved;               // 0 linearized, 1 Newton
+  int first_iteration;
+  double newton_tol;
+  int newton_max_iter;
+  double* coeff;            // complex [nfit][norbs]
+  double* qp_out;           // [norbs]
+  double* z_out;            // [norbs]
+  double* sc_out;           // complex [norbs]
+};
+void launch_pade_qp(qx_ctx* ctx, const QPParams& p);
+
+// Mixed-precision (tcgen05) forms.
+void launch_split_bf16(qx_ctx* ctx, const double* src, int rows, int cols, int ld_src, void* hi, void* lo,
+                       int ld_dst, size_t src_stride, size_t dst_stride, int batch);
+void launch_eps_bf16x3(qx_ctx* ctx, const double* bov, int ldov, int naux, int nov, const double* chi, int nw,
+                       double* eps, int ldn, size_t eps_stride);
+void launch_pair_contract_bf16x3(qx_ctx* ctx, const void* bpt_hi, const void* bpt_lo, const float* bpt_f32,
+                                 int ldk, int npair, int naux, const void* wc_hi, const void* wc_lo, int ldw,
+                                 size_t wc_stride, int nw, double* v, int ldv);
+bool tc_supported(qx_ctx* ctx);
+
+
+}  // namespace qx
