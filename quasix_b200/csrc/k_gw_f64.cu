@@ -92,96 +92,93 @@ void launch_eps_fp64(qx_ctx* ctx, const double* bov, int ldov, int naux, int nov
 }
 
 // ---------------------------------------------------------------------------
-// Block sweep inversion.  For an SPD matrix M and index block K, the sweep
+// Block sweep inversion.  For a symmetric M and index block K, the sweep
 //   D = M_KK^-1;  M_RR -= M_RK D M_KR;  M_RK = M_RK D;  M_KR = D M_KR;  M_KK = -D
 // applied to every block in turn leaves -M^-1 (Gauss-Jordan without
-// pivoting, stable for SPD).  Panel kernel: D and T = M[:,K] D, P = M[:,K].
+// pivoting; stable for SPD, and it still inverts an indefinite eps as long as
+// no pivot vanishes).  Per block of SWEEP_NB columns:
+//   k_sweep_diag   : D = inverse of the current diagonal block (one CTA per matrix)
+//   k_sweep_tpanel : T = M[:, K] D                      (DMMA GEMM, K = nb)
+//   k_sweep_update : M[r][c] -= T[r] . M[c][K]  for r, c outside K, lower
+//                    tiles only, mirrored (DMMA GEMM, K = nb)
+//   k_sweep_write  : M[r][K] = M[K][r] = T[r], M[K][K] = -D
 // ---------------------------------------------------------------------------
-constexpr int SWEEP_NB = 64;
-constexpr int PANEL_ROWS = 64;
+constexpr int SWEEP_NB = 128;
 
-__global__ void __launch_bounds__(256) k_sweep_panel(const double* __restrict__ M, int n, int ldn, size_t stride,
-                                                     int k0, int kb, double* __restrict__ Tp,
-                                                     double* __restrict__ Pp, double* __restrict__ Dp,
-                                                     int ldp, size_t pstride, int* __restrict__ status) {
-  __shared__ double S[SWEEP_NB][SWEEP_NB + 1];
+// The kb x kb diagonal block, padded with the identity to 128 x 128, is swept
+// element-wise in shared memory: thread t owns column j = t % 128 and rows
+// i = t / 128 + 4 k (k < 32), so a warp touches 32 consecutive doubles of a row.
+__global__ void __launch_bounds__(512) k_sweep_diag(const double* __restrict__ M, int ldn, size_t stride, int k0,
+                                                    int kb, double* __restrict__ Dp, int* __restrict__ status) {
+  static_assert(SWEEP_NB == 128, "thread mapping assumes 128 columns");
+  extern __shared__ double S[];  // [128][128]
   __shared__ double rowp[SWEEP_NB], colp[SWEEP_NB];
-  const int w = blockIdx.y;
+  const int w = blockIdx.x;
   const double* A = M + (size_t)w * stride;
-  for (int idx = threadIdx.x; idx < SWEEP_NB * SWEEP_NB; idx += blockDim.x) {
-    int i = idx / SWEEP_NB, j = idx % SWEEP_NB;
-    S[i][j] = (i < kb && j < kb) ? A[(size_t)(k0 + i) * ldn + k0 + j] : (i == j ? 1.0 : 0.0);
+  const int j = threadIdx.x & 127, r0 = threadIdx.x >> 7;
+#pragma unroll 4
+  for (int k = 0; k < 32; ++k) {
+    const int i = r0 + 4 * k;
+    S[i * SWEEP_NB + j] = (i < kb && j < kb) ? A[(size_t)(k0 + i) * ldn + k0 + j] : (i == j ? 1.0 : 0.0);
   }
   __syncthreads();
-  // Element-wise sweep of the kb x kb block (leaves -inverse).
+  bool bad_any = false;
   for (int p = 0; p < kb; ++p) {
-    const double d = S[p][p];
     if (threadIdx.x < SWEEP_NB) {
-      rowp[threadIdx.x] = S[p][threadIdx.x];
-      colp[threadIdx.x] = S[threadIdx.x][p];
+      rowp[threadIdx.x] = S[p * SWEEP_NB + threadIdx.x];
+      colp[threadIdx.x] = S[threadIdx.x * SWEEP_NB + p];
     }
     __syncthreads();
+    const double d = rowp[p];
     // eps is positive definite on the imaginary axis; when energies reorder it
     // can turn indefinite, and the sweep then still inverts it with negative
     // pivots (the reference falls back from Cholesky to LU there,
     // correlation_ac.rs:383-399).  Only a zero or non-finite pivot is singular.
     const bool bad = !(fabs(d) > 0.0) || !isfinite(d);
-    if (bad && threadIdx.x == 0 && blockIdx.x == 0) atomicExch(status + w, 1);
+    bad_any |= bad;
     const double inv = bad ? 0.0 : 1.0 / d;
-    for (int idx = threadIdx.x; idx < kb * kb; idx += blockDim.x) {
-      int i = idx / kb, j = idx % kb;
-      double v;
-      if (i == p && j == p) v = -inv;
-      else if (i == p) v = rowp[j] * inv;
-      else if (j == p) v = colp[i] * inv;
-      else v = S[i][j] - colp[i] * rowp[j] * inv;
-      S[i][j] = v;
+    const double rj = rowp[j] * inv;
+#pragma unroll 8
+    for (int k = 0; k < 32; ++k) {
+      const int i = r0 + 4 * k;
+      const double ci = colp[i];
+      double nv;
+      if (i == p) nv = (j == p) ? -inv : rj;
+      else if (j == p) nv = ci * inv;
+      else nv = S[i * SWEEP_NB + j] - ci * rj;
+      S[i * SWEEP_NB + j] = nv;
     }
     __syncthreads();
   }
-  // D = -S.
-  if (blockIdx.x == 0) {
-    for (int idx = threadIdx.x; idx < kb * kb; idx += blockDim.x) {
-      int i = idx / kb, j = idx % kb;
-      Dp[(size_t)w * SWEEP_NB * SWEEP_NB + i * SWEEP_NB + j] = -S[i][j];
-    }
-  }
-  // Rows of this CTA: P[r][:] = M[r][K], T[r][:] = M[r][K] D.
-  const int r0 = blockIdx.x * PANEL_ROWS;
-  for (int idx = threadIdx.x; idx < PANEL_ROWS * kb; idx += blockDim.x) {
-    int rr = idx / kb, j = idx % kb;
-    int r = r0 + rr;
-    if (r >= n) continue;
-    const double* row = A + (size_t)r * ldn + k0;
-    double t = 0.0;
-    for (int q = 0; q < kb; ++q) t -= row[q] * S[q][j];
-    Tp[(size_t)w * pstride + (size_t)r * ldp + j] = t;
-    Pp[(size_t)w * pstride + (size_t)r * ldp + j] = row[j];
+  if (bad_any && threadIdx.x == 0) atomicExch(status + w, 1);
+  // D = -S, zero outside the kb x kb block.
+  double* D = Dp + (size_t)w * SWEEP_NB * SWEEP_NB;
+  for (int k = 0; k < 32; ++k) {
+    const int i = r0 + 4 * k;
+    D[(size_t)i * SWEEP_NB + j] = (i < kb && j < kb) ? -S[i * SWEEP_NB + j] : 0.0;
   }
 }
 
-using SweepTile = F64Tile<64, 64, 2, 2, 3>;
+using PanelTile = F64Tile<64, 64, 2, 2, 3>;
 
-__global__ void __launch_bounds__(SweepTile::THREADS) k_sweep_update(double* __restrict__ M, int n, int ldn,
+// T[w][r][:] = M[w][r][K] D[w]   (D symmetric: its rows serve as the B operand)
+__global__ void __launch_bounds__(PanelTile::THREADS) k_sweep_tpanel(const double* __restrict__ M, int n, int ldn,
                                                                      size_t stride, int k0, int kb,
-                                                                     const double* __restrict__ Tp,
-                                                                     const double* __restrict__ Pp,
-                                                                     const double* __restrict__ Dp, int ldp,
-                                                                     size_t pstride) {
-  using T = SweepTile;
+                                                                     const double* __restrict__ Dp,
+                                                                     double* __restrict__ Tp, size_t pstride) {
+  using T = PanelTile;
   extern __shared__ double smem[];
   const int w = blockIdx.z;
-  const int m0 = blockIdx.y * T::BM, n0 = blockIdx.x * T::BN;
-  const double* Tw = Tp + (size_t)w * pstride;
-  const double* Pw = Pp + (size_t)w * pstride;
+  const int m0 = blockIdx.x * T::BM, n0 = blockIdx.y * T::BN;
   double acc[T::MI][T::NJ][2];
 #pragma unroll
   for (int i = 0; i < T::MI; ++i)
 #pragma unroll
     for (int j = 0; j < T::NJ; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
-  f64_mainloop<T>(acc, smem, Tw + (size_t)m0 * ldp, ldp, n - m0, Pw + (size_t)n0 * ldp, ldp, n - n0, nullptr, kb);
-  double* A = M + (size_t)w * stride;
-  const double* D = Dp + (size_t)w * SWEEP_NB * SWEEP_NB;
+  const double* A = M + (size_t)w * stride + (size_t)m0 * ldn + k0;
+  const double* D = Dp + (size_t)w * SWEEP_NB * SWEEP_NB + (size_t)n0 * SWEEP_NB;
+  f64_mainloop<T>(acc, smem, A, ldn, n - m0, D, SWEEP_NB, kb - n0, nullptr, kb);
+  double* Tw = Tp + (size_t)w * pstride;
 #pragma unroll
   for (int i = 0; i < T::MI; ++i)
 #pragma unroll
@@ -189,67 +186,118 @@ __global__ void __launch_bounds__(SweepTile::THREADS) k_sweep_update(double* __r
 #pragma unroll
       for (int e = 0; e < 2; ++e) {
         const int r = m0 + f64_row<T>(i), c = n0 + f64_col<T>(j, e);
-        if (r >= n || c >= n) continue;
-        const bool rk = (r >= k0 && r < k0 + kb), ck = (c >= k0 && c < k0 + kb);
-        double v;
-        if (!rk && !ck) v = A[(size_t)r * ldn + c] - acc[i][j][e];
-        else if (!rk && ck) v = Tw[(size_t)r * ldp + (c - k0)];
-        else if (rk && !ck) v = Tw[(size_t)c * ldp + (r - k0)];
-        else v = -D[(r - k0) * SWEEP_NB + (c - k0)];
-        A[(size_t)r * ldn + c] = v;
+        if (r < n && c < SWEEP_NB) Tw[(size_t)r * SWEEP_NB + c] = acc[i][j][e];
       }
 }
 
-// After the last sweep M = -eps^-1; Wc = eps^-1 - I = -M - I.
-__global__ void k_finish_wc(double* __restrict__ M, int n, int ldn, size_t stride) {
+using SweepTile = F64Tile<64, 64, 2, 2, 3>;
+
+__global__ void __launch_bounds__(SweepTile::THREADS) k_sweep_update(double* __restrict__ M, int n, int ldn,
+                                                                     size_t stride, int k0, int kb,
+                                                                     const double* __restrict__ Tp,
+                                                                     size_t pstride) {
+  using T = SweepTile;
+  extern __shared__ double smem[];
+  const int t = blockIdx.x;
+  int tm = (int)floor((sqrt(8.0 * t + 1.0) - 1.0) * 0.5);
+  while ((tm + 1) * (tm + 2) / 2 <= t) ++tm;
+  while (tm * (tm + 1) / 2 > t) --tm;
+  const int tn = t - tm * (tm + 1) / 2;
+  const int w = blockIdx.y;
+  const int m0 = tm * T::BM, n0 = tn * T::BN;
+  // Tiles entirely inside the K block rows or columns have nothing to update.
+  if ((m0 >= k0 && m0 + T::BM <= k0 + kb) || (n0 >= k0 && n0 + T::BN <= k0 + kb)) return;
+  double* A = M + (size_t)w * stride;
+  const double* Tw = Tp + (size_t)w * pstride;
+  double acc[T::MI][T::NJ][2];
+#pragma unroll
+  for (int i = 0; i < T::MI; ++i)
+#pragma unroll
+    for (int j = 0; j < T::NJ; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+  f64_mainloop<T>(acc, smem, Tw + (size_t)m0 * SWEEP_NB, SWEEP_NB, n - m0, A + (size_t)n0 * ldn + k0, ldn, n - n0,
+                  nullptr, kb);
+#pragma unroll
+  for (int i = 0; i < T::MI; ++i)
+#pragma unroll
+    for (int j = 0; j < T::NJ; ++j)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int r = m0 + f64_row<T>(i), c = n0 + f64_col<T>(j, e);
+        if (r >= n || c >= n || c > r) continue;
+        if ((r >= k0 && r < k0 + kb) || (c >= k0 && c < k0 + kb)) continue;
+        const double v = A[(size_t)r * ldn + c] - acc[i][j][e];
+        A[(size_t)r * ldn + c] = v;
+        if (c != r) A[(size_t)c * ldn + r] = v;
+      }
+}
+
+__global__ void k_sweep_write(double* __restrict__ M, int n, int ldn, size_t stride, int k0, int kb,
+                              const double* __restrict__ Tp, size_t pstride, const double* __restrict__ Dp) {
   const int w = blockIdx.y;
   double* A = M + (size_t)w * stride;
+  const double* Tw = Tp + (size_t)w * pstride;
+  const double* D = Dp + (size_t)w * SWEEP_NB * SWEEP_NB;
+  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < n * kb; idx += gridDim.x * blockDim.x) {
+    const int r = idx / kb, q = idx % kb;
+    const double v = (r >= k0 && r < k0 + kb) ? -D[(r - k0) * SWEEP_NB + q] : Tw[(size_t)r * SWEEP_NB + q];
+    A[(size_t)r * ldn + k0 + q] = v;
+    A[(size_t)(k0 + q) * ldn + r] = v;
+  }
+}
+
+// After the last sweep M = -eps^-1; Wc = eps^-1 - I = -M - I.  A frequency
+// whose eps was singular gets Wc = 0 (eps^-1 replaced by the identity).
+__global__ void k_finish_wc(double* __restrict__ M, int n, int ldn, size_t stride, const int* __restrict__ status) {
+  const int w = blockIdx.y;
+  double* A = M + (size_t)w * stride;
+  const bool singular = status[w] != 0;
   for (size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x; idx < (size_t)n * n;
        idx += (size_t)gridDim.x * blockDim.x) {
     int r = (int)(idx / n), c = (int)(idx % n);
-    A[(size_t)r * ldn + c] = -A[(size_t)r * ldn + c] - (r == c ? 1.0 : 0.0);
+    A[(size_t)r * ldn + c] = singular ? 0.0 : -A[(size_t)r * ldn + c] - (r == c ? 1.0 : 0.0);
   }
 }
 
 void launch_invert_wc(qx_ctx* ctx, double* eps, int n, int ldn, size_t stride, int nw) {
-  using T = SweepTile;
-  const int ldp = SWEEP_NB;
-  const size_t pstride = (size_t)n * ldp;
+  const size_t pstride = (size_t)n * SWEEP_NB;
   DevBuf& pan = ctx->ws[WS_PANEL];
-  const size_t need = (2 * pstride * nw + (size_t)nw * SWEEP_NB * SWEEP_NB) * sizeof(double) + nw * sizeof(int) + 256;
+  const size_t need = (pstride * nw + (size_t)nw * SWEEP_NB * SWEEP_NB) * sizeof(double) + nw * sizeof(int) + 256;
   pan.reserve(need);
   double* Tp = pan.as<double>();
-  double* Pp = Tp + pstride * nw;
-  double* Dp = Pp + pstride * nw;
+  double* Dp = Tp + pstride * nw;
   int* status = reinterpret_cast<int*>(Dp + (size_t)nw * SWEEP_NB * SWEEP_NB);
   QX_CUDA(cudaMemsetAsync(status, 0, nw * sizeof(int), ctx->stream));
+  const int diag_smem = SWEEP_NB * SWEEP_NB * sizeof(double);
   static bool attr = false;
   if (!attr) {
-    QX_CUDA(cudaFuncSetAttribute(k_sweep_update, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::SMEM));
+    QX_CUDA(cudaFuncSetAttribute(k_sweep_diag, cudaFuncAttributeMaxDynamicSharedMemorySize, diag_smem));
+    QX_CUDA(cudaFuncSetAttribute(k_sweep_tpanel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)PanelTile::SMEM));
+    QX_CUDA(cudaFuncSetAttribute(k_sweep_update, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)SweepTile::SMEM));
     attr = true;
   }
+  const int tiles = ceil_div(n, SweepTile::BM);
   for (int k0 = 0; k0 < n; k0 += SWEEP_NB) {
     const int kb = min(SWEEP_NB, n - k0);
-    dim3 pg(ceil_div(n, PANEL_ROWS), nw);
-    k_sweep_panel<<<pg, 256, 0, ctx->stream>>>(eps, n, ldn, stride, k0, kb, Tp, Pp, Dp, ldp, pstride, status);
+    k_sweep_diag<<<nw, 512, diag_smem, ctx->stream>>>(eps, ldn, stride, k0, kb, Dp, status);
     check_launch(ctx);
-    dim3 ug(ceil_div(n, T::BN), ceil_div(n, T::BM), nw);
-    k_sweep_update<<<ug, T::THREADS, T::SMEM, ctx->stream>>>(eps, n, ldn, stride, k0, kb, Tp, Pp, Dp, ldp, pstride);
+    dim3 tg(ceil_div(n, PanelTile::BM), ceil_div(kb, PanelTile::BN), nw);
+    k_sweep_tpanel<<<tg, PanelTile::THREADS, PanelTile::SMEM, ctx->stream>>>(eps, n, ldn, stride, k0, kb, Dp, Tp,
+                                                                             pstride);
+    check_launch(ctx);
+    dim3 ug(tiles * (tiles + 1) / 2, nw);
+    k_sweep_update<<<ug, SweepTile::THREADS, SweepTile::SMEM, ctx->stream>>>(eps, n, ldn, stride, k0, kb, Tp,
+                                                                             pstride);
+    check_launch(ctx);
+    dim3 wg(ceil_div(n * kb, 256), nw);
+    k_sweep_write<<<wg, 256, 0, ctx->stream>>>(eps, n, ldn, stride, k0, kb, Tp, pstride, Dp);
     check_launch(ctx);
   }
   dim3 fg(ceil_div(n * n, 256 * 4), nw);
-  k_finish_wc<<<fg, 256, 0, ctx->stream>>>(eps, n, ldn, stride);
+  k_finish_wc<<<fg, 256, 0, ctx->stream>>>(eps, n, ldn, stride, status);
   check_launch(ctx);
-  std::vector<int> st(nw);
-  QX_CUDA(cudaMemcpyAsync(st.data(), status, nw * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
-  QX_CUDA(cudaStreamSynchronize(ctx->stream));
-  for (int w = 0; w < nw; ++w)
-    if (st[w]) {
-      // Singular eps: the reference substitutes the identity for eps^-1
-      // (correlation_ac.rs:390-397), i.e. Wc = 0 at this frequency.
-      fprintf(stderr, "WARNING: Matrix inversion failed at freq %d: singular eps, using Wc = 0\n", w);
-      QX_CUDA(cudaMemset2DAsync(eps + (size_t)w * stride, ldn * sizeof(double), 0, n * sizeof(double), n, ctx->stream));
-    }
+  ctx->pending.push_back({status, nw, 1});
 }
 
 // ---------------------------------------------------------------------------

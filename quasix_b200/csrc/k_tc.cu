@@ -444,18 +444,15 @@ void launch_split_bf16(qx_ctx* ctx, const double* src, int rows, int cols, int l
   split(ctx, src, rows, cols, ld_src, src_stride, hi, lo, ld_dst, dst_stride, batch, nullptr, 0);
 }
 
-static int* tc_err_slot(qx_ctx* ctx) {
+// Error words: one per tcgen05 GEMM kind, so both launches of an iteration
+// can be checked after a single synchronisation.
+static int* tc_err_slot(qx_ctx* ctx, int which) {
   DevBuf& b = ctx->ws[WS_TCERR];
   b.reserve(256);
-  return b.as<int>();
+  return b.as<int>() + which;
 }
 
-static void check_tc_err(qx_ctx* ctx, int* d_err) {
-  int e = 0;
-  QX_CUDA(cudaMemcpyAsync(&e, d_err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
-  QX_CUDA(cudaStreamSynchronize(ctx->stream));
-  QX_REQUIRE(e == 0, QX_ERR_CUDA, "tcgen05 GEMM pipeline wait timed out (code %d)", e);
-}
+static void check_tc_err(qx_ctx* ctx, int* d_err) { ctx->pending.push_back({d_err, 1, 0}); }
 
 template <int BN, int EPI>
 static void launch_tc(qx_ctx* ctx, const CUtensorMap& ah, const CUtensorMap& al, const CUtensorMap& bh,
@@ -480,7 +477,7 @@ void launch_pair_contract_bf16x3(qx_ctx* ctx, const void* bpt_hi, const void* bp
   CUtensorMap al = make_map(bpt_lo, naux, npair, ldk, 1, TC_BM, 2);
   CUtensorMap bh = make_map(wc_hi, naux, naux, ldw, nw, BN, 3);
   CUtensorMap bl = make_map(wc_lo, naux, naux, ldw, nw, BN, 3);
-  int* d_err = tc_err_slot(ctx);
+  int* d_err = tc_err_slot(ctx, 0);
   QX_CUDA(cudaMemsetAsync(d_err, 0, sizeof(int), ctx->stream));
   TcArgs a{};
   a.M = npair;
@@ -517,7 +514,7 @@ void launch_eps_bf16x3(qx_ctx* ctx, const double* bov, int ldov, int naux, int n
   CUtensorMap al = make_map(a_lo, nov, naux, ldov, 1, TC_BM, 2);
   CUtensorMap bh = make_map(b_hi, nov, naux, ldov, nw, BN, 3);
   CUtensorMap bl = make_map(b_lo, nov, naux, ldov, nw, BN, 3);
-  int* d_err = tc_err_slot(ctx);
+  int* d_err = tc_err_slot(ctx, 1);
   QX_CUDA(cudaMemsetAsync(d_err, 0, sizeof(int), ctx->stream));
   TcArgs a{};
   a.M = naux;

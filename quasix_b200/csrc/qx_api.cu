@@ -230,10 +230,28 @@ void gw_setup(qx_ctx* ctx, GWSystem& S, const double* d_lpq, int nmo, int nocc, 
   }
 }
 
+void sync_and_check(qx_ctx* ctx) {
+  QX_CUDA(cudaStreamSynchronize(ctx->stream));
+  std::vector<qx_ctx::Pending> pend;
+  pend.swap(ctx->pending);
+  for (const auto& pd : pend) {
+    std::vector<int> h(pd.count);
+    QX_CUDA(cudaMemcpy(h.data(), pd.dev, pd.count * sizeof(int), cudaMemcpyDeviceToHost));
+    for (int i = 0; i < pd.count; ++i) {
+      if (!h[i]) continue;
+      if (pd.kind == 0)
+        throw Error(QX_ERR_CUDA, fmt("tcgen05 GEMM pipeline wait timed out (code %d)", h[i]));
+      // Singular eps: the reference substitutes the identity for eps^-1
+      // (correlation_ac.rs:390-397); the device already set Wc = 0 there.
+      fprintf(stderr, "WARNING: Matrix inversion failed at freq %d: singular eps, using Wc = 0\n", i);
+    }
+  }
+}
+
 void record_stage(qx_ctx* ctx, int st, bool begin) { cudaEventRecord(ctx->ev[2 * st + (begin ? 0 : 1)], ctx->stream); }
 
 void accumulate_stage_times(qx_ctx* ctx) {
-  QX_CUDA(cudaStreamSynchronize(ctx->stream));
+  sync_and_check(ctx);
   for (int s = 0; s < QX_ST_COUNT; ++s) {
     float ms = 0.f;
     if (cudaEventElapsedTime(&ms, ctx->ev[2 * s], ctx->ev[2 * s + 1]) == cudaSuccess) ctx->stage_ms[s] += ms;
@@ -402,6 +420,7 @@ template <class F>
 static qx_status guarded(qx_ctx* ctx, F&& f) {
   try {
     if (ctx) {
+      ctx->pending.clear();
       ctx->launches = 0;
       for (double& v : ctx->stage_ms) v = 0.0;
       QX_CUDA(cudaSetDevice(ctx->device));
@@ -546,7 +565,7 @@ qx_status qx_get_rho_response(qx_ctx* ctx, int nfreq, const double* freqs, const
     // Pi = I - eps.
     std::vector<double> h((size_t)nfreq * stride);
     QX_CUDA(cudaMemcpyAsync(h.data(), eps, h.size() * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-    QX_CUDA(cudaStreamSynchronize(ctx->stream));
+    sync_and_check(ctx);
     std::vector<double> out((size_t)nfreq * naux * naux);
     for (int w = 0; w < nfreq; ++w)
       for (int r = 0; r < naux; ++r)
@@ -573,7 +592,7 @@ qx_status qx_screened_interaction(qx_ctx* ctx, int nfreq, int naux, const double
     QX_CUDA(cudaMemcpyAsync(eps, he.data(), he.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
     launch_invert_wc(ctx, eps, naux, ldn, stride, nfreq);
     QX_CUDA(cudaMemcpyAsync(he.data(), eps, he.size() * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-    QX_CUDA(cudaStreamSynchronize(ctx->stream));
+    sync_and_check(ctx);
     for (int w = 0; w < nfreq; ++w)
       for (int r = 0; r < naux; ++r)
         for (int c = 0; c < naux; ++c) hp[((size_t)w * naux + r) * naux + c] = he[w * stride + (size_t)r * ldn + c];
@@ -702,7 +721,7 @@ qx_status qx_compute_exchange_diag(qx_ctx* ctx, const double* lpq, int naux, int
     double* d = ctx->ws[WS_QPOUT].as<double>();
     launch_exchange_diag(ctx, d_lpq, naux, nmo, nocc, d);
     QX_CUDA(cudaMemcpyAsync(sigma_x, d, nmo * sizeof(double), cudaMemcpyDefault, ctx->stream));
-    QX_CUDA(cudaStreamSynchronize(ctx->stream));
+    sync_and_check(ctx);
   });
 }
 

@@ -80,6 +80,15 @@ struct qx_ctx {
   cudaEvent_t ev[2 * QX_ST_COUNT] = {};
   // Named workspace slots.
   qx::DevBuf ws[32];
+  // Device status words to inspect after the next stream synchronisation:
+  // (pointer, count, kind) with kind 0 = tcgen05 pipeline error code,
+  // kind 1 = per-frequency singular-eps flags.
+  struct Pending {
+    const int* dev;
+    int count;
+    int kind;
+  };
+  std::vector<Pending> pending;
 };
 
 namespace qx {
@@ -126,6 +135,9 @@ inline void check_launch(qx_ctx* ctx) {
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) throw Error(QX_ERR_CUDA, fmt("kernel launch failed: %s", cudaGetErrorString(e)));
 }
+
+// Synchronise the context stream and act on the pending device status words.
+void sync_and_check(qx_ctx* ctx);
 
 // Stage timer (CUDA events on the context stream).
 struct StageTimer {
