@@ -1,0 +1,268 @@
+// Generic FP64 building blocks on the DMMA mainloop: a batched "NT" GEMM with
+// split-K, small combination kernels and a one-CTA parallel Jacobi
+// eigensolver for the Davidson Rayleigh-Ritz step.
+#include "gemm_f64.cuh"
+#include "qx_internal.cuh"
+#include "qx_blas.cuh"
+
+namespace qx {
+
+using GemmTile = F64Tile<64, 64, 2, 2, 3>;
+
+// C[b][m][n] (or the split-K partial) = sum_{k in split} A[b][m][k] B[b][n][k]
+__global__ void __launch_bounds__(GemmTile::THREADS) k_gemm_nt(GemmNT g, double* __restrict__ part) {
+  using T = GemmTile;
+  extern __shared__ double smem[];
+  const int nsplit = g.splitk;
+  const int b = blockIdx.z / nsplit, sk = blockIdx.z % nsplit;
+  const int m0 = blockIdx.y * T::BM, n0 = blockIdx.x * T::BN;
+  const int kchunk = ((g.K + nsplit - 1) / nsplit + T::BK - 1) / T::BK * T::BK;
+  const int kbeg = sk * kchunk;
+  const int klen = max(0, min(g.K - kbeg, kchunk));
+  double acc[T::MI][T::NJ][2];
+#pragma unroll
+  for (int i = 0; i < T::MI; ++i)
+#pragma unroll
+    for (int j = 0; j < T::NJ; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+  if (klen > 0)
+    f64_mainloop<T>(acc, smem, g.A + (size_t)b * g.sA + (size_t)m0 * g.lda + kbeg, g.lda, g.M - m0,
+                    g.B + (size_t)b * g.sB + (size_t)n0 * g.ldb + kbeg, g.ldb, g.N - n0, nullptr, klen);
+#pragma unroll
+  for (int i = 0; i < T::MI; ++i)
+#pragma unroll
+    for (int j = 0; j < T::NJ; ++j)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int m = m0 + f64_row<T>(i), n = n0 + f64_col<T>(j, e);
+        if (m >= g.M || n >= g.N) continue;
+        if (nsplit == 1) {
+          double* c = g.C + (size_t)b * g.sC + (size_t)m * g.ldc + n;
+          *c = g.alpha * acc[i][j][e] + (g.beta != 0.0 ? g.beta * *c : 0.0);
+        } else {
+          part[((size_t)sk * g.batch + b) * g.M * g.N + (size_t)m * g.N + n] = acc[i][j][e];
+        }
+      }
+}
+
+__global__ void k_splitk_reduce(GemmNT g, const double* __restrict__ part) {
+  const size_t mn = (size_t)g.M * g.N;
+  for (size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x; idx < mn * g.batch;
+       idx += (size_t)gridDim.x * blockDim.x) {
+    const int b = (int)(idx / mn);
+    const size_t r = idx % mn;
+    const int m = (int)(r / g.N), n = (int)(r % g.N);
+    double s = 0.0;
+    for (int k = 0; k < g.splitk; ++k) s += part[((size_t)k * g.batch + b) * mn + r];
+    double* c = g.C + (size_t)b * g.sC + (size_t)m * g.ldc + n;
+    *c = g.alpha * s + (g.beta != 0.0 ? g.beta * *c : 0.0);
+  }
+}
+
+void gemm_nt_f64(qx_ctx* ctx, GemmNT g) {
+  using T = GemmTile;
+  QX_REQUIRE(g.lda % 2 == 0 && g.ldb % 2 == 0 && (reinterpret_cast<uintptr_t>(g.A) & 15) == 0 &&
+                 (reinterpret_cast<uintptr_t>(g.B) & 15) == 0 && g.sA % 2 == 0 && g.sB % 2 == 0,
+             QX_ERR_INVALID_INPUT, "gemm_nt_f64: operands must be 16-byte aligned with even leading dimensions");
+  if (g.M <= 0 || g.N <= 0 || g.batch <= 0) return;
+  static bool attr = false;
+  if (!attr) {
+    QX_CUDA(cudaFuncSetAttribute(k_gemm_nt, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::SMEM));
+    attr = true;
+  }
+  if (g.splitk < 1) {
+    // Enough CTAs to fill the GPU about twice.
+    const long tiles = (long)ceil_div(g.M, T::BM) * ceil_div(g.N, T::BN) * g.batch;
+    int s = 1;
+    while (tiles * s < 2L * ctx->sm_count * 3 && g.K / (s * 2) >= 4 * T::BK && s < 64) s *= 2;
+    g.splitk = s;
+  }
+  double* part = nullptr;
+  if (g.splitk > 1) {
+    DevBuf& pb = ctx->ws[WS_HOSTIN];
+    pb.reserve((size_t)g.splitk * g.batch * g.M * g.N * sizeof(double));
+    part = pb.as<double>();
+  }
+  dim3 grid(ceil_div(g.N, T::BN), ceil_div(g.M, T::BM), g.batch * g.splitk);
+  k_gemm_nt<<<grid, T::THREADS, T::SMEM, ctx->stream>>>(g, part);
+  check_launch(ctx);
+  if (g.splitk > 1) {
+    const size_t n = (size_t)g.M * g.N * g.batch;
+    k_splitk_reduce<<<(unsigned)std::min<size_t>((n + 255) / 256, 8192), 256, 0, ctx->stream>>>(g, part);
+    check_launch(ctx);
+  }
+}
+
+// out[r][k] (+)= sum_i coef[i * ldc + r] V[i][k]  for r < nr, k < n.
+__global__ void k_combine(const double* __restrict__ V, int ldv, int nv, const double* __restrict__ coef, int ldc,
+                          int nr, int n, double* __restrict__ out, int ldo, double beta, double alpha) {
+  constexpr int MAXR = 16;
+  const int r0 = blockIdx.y * MAXR;
+  const int nrb = min(MAXR, nr - r0);
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+    double acc[MAXR];
+#pragma unroll
+    for (int r = 0; r < MAXR; ++r) acc[r] = 0.0;
+    for (int i = 0; i < nv; ++i) {
+      const double x = V[(size_t)i * ldv + k];
+#pragma unroll
+      for (int r = 0; r < MAXR; ++r)
+        if (r < nrb) acc[r] += coef[(size_t)i * ldc + r0 + r] * x;
+    }
+#pragma unroll
+    for (int r = 0; r < MAXR; ++r)
+      if (r < nrb) {
+        double* o = out + (size_t)(r0 + r) * ldo + k;
+        *o = alpha * acc[r] + (beta != 0.0 ? beta * *o : 0.0);
+      }
+  }
+}
+
+void combine_rows(qx_ctx* ctx, const double* V, int ldv, int nv, const double* coef, int ldc, int nr, int n,
+                  double* out, int ldo, double alpha, double beta) {
+  if (nr <= 0 || n <= 0) return;
+  dim3 grid(std::min(ceil_div(n, 256), 2 * ctx->sm_count), ceil_div(nr, 16));
+  k_combine<<<grid, 256, 0, ctx->stream>>>(V, ldv, nv, coef, ldc, nr, n, out, ldo, beta, alpha);
+  check_launch(ctx);
+}
+
+// ---------------------------------------------------------------------------
+// Parallel cyclic Jacobi (round-robin pairing) for a symmetric n x n matrix,
+// one CTA.  A is overwritten (diagonal -> eigenvalues), V receives the
+// eigenvectors as columns.  Output sorted ascending into w and Z (columns).
+// Converges when the off-diagonal Frobenius norm falls below tol * ||A||_F.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(1024) k_jacobi(double* __restrict__ A, double* __restrict__ V, int n, int lda,
+                                                 double* __restrict__ w, double* __restrict__ Z, int ldz,
+                                                 int max_sweeps, int* __restrict__ info) {
+  extern __shared__ double sh[];
+  const int m = n + (n & 1);  // even number of players (a dummy when n is odd)
+  double* cs = sh;            // [m/2] cosines
+  double* sn = cs + m / 2;    // [m/2] sines
+  int* pp = reinterpret_cast<int*>(sn + m / 2);  // [m/2]
+  int* qq = pp + m / 2;                          // [m/2]
+  __shared__ double red[32];
+  __shared__ int done;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  // Symmetrize and V = I.
+  for (int idx = tid; idx < n * n; idx += nt) {
+    const int i = idx / n, j = idx % n;
+    if (i < j) {
+      const double s = 0.5 * (A[(size_t)i * lda + j] + A[(size_t)j * lda + i]);
+      A[(size_t)i * lda + j] = s;
+      A[(size_t)j * lda + i] = s;
+    }
+    V[(size_t)i * lda + j] = (i == j) ? 1.0 : 0.0;
+  }
+  __syncthreads();
+  int sweep = 0;
+  for (; sweep < max_sweeps; ++sweep) {
+    // Convergence test: off-diagonal norm vs total norm.
+    double off = 0.0, tot = 0.0;
+    for (int idx = tid; idx < n * n; idx += nt) {
+      const int i = idx / n, j = idx % n;
+      const double a = A[(size_t)i * lda + j];
+      tot += a * a;
+      if (i != j) off += a * a;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      off += __shfl_xor_sync(0xffffffffu, off, o);
+      tot += __shfl_xor_sync(0xffffffffu, tot, o);
+    }
+    if ((tid & 31) == 0) red[tid >> 5] = off;
+    __syncthreads();
+    if (tid == 0) {
+      double s = 0.0;
+      for (int i = 0; i < (nt + 31) / 32; ++i) s += red[i];
+      red[31] = s;
+    }
+    __syncthreads();
+    const double offs = red[31];
+    __syncthreads();
+    if ((tid & 31) == 0) red[tid >> 5] = tot;
+    __syncthreads();
+    if (tid == 0) {
+      double s = 0.0;
+      for (int i = 0; i < (nt + 31) / 32; ++i) s += red[i];
+      done = (offs <= 1e-30 * s) || (sqrt(offs) <= 1e-15 * sqrt(s));
+    }
+    __syncthreads();
+    if (done) break;
+    for (int round = 0; round < m - 1; ++round) {
+      // Round-robin pairing: player 0 fixed, others rotate.
+      for (int k = tid; k < m / 2; k += nt) {
+        int a = (k == 0) ? 0 : 1 + (k - 1 + round) % (m - 1);
+        int b = 1 + (m - 2 - k + round) % (m - 1);
+        const int p = min(a, b), q = max(a, b);
+        pp[k] = p;
+        qq[k] = q;
+        double c = 1.0, s = 0.0;
+        if (q < n) {
+          const double apq = A[(size_t)p * lda + q];
+          if (fabs(apq) > 1e-300) {
+            const double app = A[(size_t)p * lda + p], aqq = A[(size_t)q * lda + q];
+            const double theta = (aqq - app) / (2.0 * apq);
+            const double t = (theta >= 0.0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
+            c = 1.0 / sqrt(t * t + 1.0);
+            s = t * c;
+          }
+        }
+        cs[k] = c;
+        sn[k] = s;
+      }
+      __syncthreads();
+      // A <- A J (columns p, q of every row), V <- V J.
+      for (int idx = tid; idx < (m / 2) * n; idx += nt) {
+        const int k = idx / n, r = idx % n;
+        const int p = pp[k], q = qq[k];
+        if (q >= n) continue;
+        const double c = cs[k], s = sn[k];
+        const double ap = A[(size_t)r * lda + p], aq = A[(size_t)r * lda + q];
+        A[(size_t)r * lda + p] = c * ap - s * aq;
+        A[(size_t)r * lda + q] = s * ap + c * aq;
+        const double vp = V[(size_t)r * lda + p], vq = V[(size_t)r * lda + q];
+        V[(size_t)r * lda + p] = c * vp - s * vq;
+        V[(size_t)r * lda + q] = s * vp + c * vq;
+      }
+      __syncthreads();
+      // A <- J^T A (rows p, q).
+      for (int idx = tid; idx < (m / 2) * n; idx += nt) {
+        const int k = idx / n, col = idx % n;
+        const int p = pp[k], q = qq[k];
+        if (q >= n) continue;
+        const double c = cs[k], s = sn[k];
+        const double ap = A[(size_t)p * lda + col], aq = A[(size_t)q * lda + col];
+        A[(size_t)p * lda + col] = c * ap - s * aq;
+        A[(size_t)q * lda + col] = s * ap + c * aq;
+      }
+      __syncthreads();
+    }
+  }
+  if (tid == 0) info[0] = sweep;
+  __syncthreads();
+  // Sort eigenvalues ascending (selection by rank; ties broken by index).
+  for (int i = tid; i < n; i += nt) {
+    const double di = A[(size_t)i * lda + i];
+    int rank = 0;
+    for (int j = 0; j < n; ++j) {
+      const double dj = A[(size_t)j * lda + j];
+      if (dj < di || (dj == di && j < i)) ++rank;
+    }
+    w[rank] = di;
+    for (int r = 0; r < n; ++r) Z[(size_t)r * ldz + rank] = V[(size_t)r * lda + i];
+  }
+}
+
+void jacobi_eigh(qx_ctx* ctx, double* A, double* V, int n, int lda, double* w, double* Z, int ldz, int* info) {
+  const int m = n + (n & 1);
+  const size_t sh = (size_t)m * sizeof(double) + (size_t)m * sizeof(int) + 64;
+  static bool attr = false;
+  if (!attr) {
+    QX_CUDA(cudaFuncSetAttribute(k_jacobi, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024));
+    attr = true;
+  }
+  QX_REQUIRE(sh <= 64 * 1024, QX_ERR_INVALID_INPUT, "subspace too large for the Jacobi kernel (%d)", n);
+  k_jacobi<<<1, 1024, sh, ctx->stream>>>(A, V, n, lda, w, Z, ldz, 60, info);
+  check_launch(ctx);
+}
+
+}  // namespace qx

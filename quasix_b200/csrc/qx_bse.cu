@@ -1,7 +1,287 @@
-// BSE-TDA and contour-deformation entry points (filled in below the GW chain).
+// BSE-TDA on the GPU: the matrix-free Hamiltonian of BSETDAKernel
+// (quasix_core/src/bse/kernel.rs:501-598) as batched GEMMs, and the block
+// Davidson of davidson_bse (quasix_core/src/bse/davidson.rs:372-508) with the
+// subspace, Rayleigh-Ritz (parallel Jacobi) and re-orthonormalisation on the
+// device; the host only steers (convergence flags, subspace size).
+#include <algorithm>
+#include <numeric>
+
+#include "qx_blas.cuh"
 #include "qx_internal.cuh"
 
+namespace qx {
+
+// out[b][c][r] = in[b][r][c]   (rows x cols per batch)
+__global__ void k_transpose(const double* __restrict__ in, int rows, int cols, int ldi, size_t si,
+                            double* __restrict__ out, int ldo, size_t so) {
+  __shared__ double t[32][33];
+  const int b = blockIdx.z;
+  const int r0 = blockIdx.y * 32, c0 = blockIdx.x * 32;
+  for (int y = threadIdx.y; y < 32; y += blockDim.y) {
+    const int r = r0 + y, c = c0 + threadIdx.x;
+    t[y][threadIdx.x] = (r < rows && c < cols) ? in[(size_t)b * si + (size_t)r * ldi + c] : 0.0;
+  }
+  __syncthreads();
+  for (int y = threadIdx.y; y < 32; y += blockDim.y) {
+    const int c = c0 + y, r = r0 + threadIdx.x;
+    if (c < cols && r < rows) out[(size_t)b * so + (size_t)c * ldo + r] = t[threadIdx.x][y];
+  }
+}
+
+static void transpose(qx_ctx* ctx, const double* in, int rows, int cols, int ldi, size_t si, double* out, int ldo,
+                      size_t so, int batch) {
+  dim3 grid(ceil_div(cols, 32), ceil_div(rows, 32), batch);
+  k_transpose<<<grid, dim3(32, 8), 0, ctx->stream>>>(in, rows, cols, ldi, si, out, ldo, so);
+  check_launch(ctx);
+}
+
+// Xp[(v, j)][b] = X[v][j * nvir + b] (rows padded to ldvp).
+__global__ void k_pack_x(const double* __restrict__ X, int ldx, int nvec, int nocc, int nvir,
+                         double* __restrict__ Xp, int ldvp) {
+  const size_t total = (size_t)nvec * nocc * ldvp;
+  for (size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+       idx += (size_t)gridDim.x * blockDim.x) {
+    const int b = (int)(idx % ldvp);
+    const size_t row = idx / ldvp;
+    const int v = (int)(row / nocc), j = (int)(row % nocc);
+    Xp[idx] = (b < nvir) ? X[(size_t)v * ldx + (size_t)j * nvir + b] : 0.0;
+  }
+}
+
+// Y[v][ia] = delta[ia] X[v][ia] + ax Yx[v][ia] - Yd[i][a * nvec + v]
+__global__ void k_bse_combine(const double* __restrict__ X, const double* __restrict__ delta,
+                              const double* __restrict__ Yx, const double* __restrict__ Yd, int nvec, int nocc,
+                              int nvir, int ldx, double ax, double* __restrict__ Y) {
+  const int nov = nocc * nvir;
+  const size_t total = (size_t)nvec * ldx;
+  for (size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+       idx += (size_t)gridDim.x * blockDim.x) {
+    const int v = (int)(idx / ldx), ia = (int)(idx % ldx);
+    double y = 0.0;
+    if (ia < nov) {
+      const int i = ia / nvir, a = ia % nvir;
+      y = delta[ia] * X[idx] - Yd[(size_t)i * nvir * nvec + (size_t)a * nvec + v];
+      if (ax != 0.0) y += ax * Yx[idx];
+    }
+    Y[idx] = y;
+  }
+}
+
+// R[r] = AX[r] - theta[r] X[r]; nrm2[r] = |R[r]|^2
+__global__ void k_residual(const double* __restrict__ AX, const double* __restrict__ X, const double* __restrict__ theta,
+                           int ld, int n, double* __restrict__ R, double* __restrict__ nrm2) {
+  const int r = blockIdx.y;
+  double s = 0.0;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+    const double v = AX[(size_t)r * ld + k] - theta[r] * X[(size_t)r * ld + k];
+    R[(size_t)r * ld + k] = v;
+    s += v * v;
+  }
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  __shared__ double red[32];
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int i = 0; i < (int)(blockDim.x >> 5); ++i) t += red[i];
+    atomicAdd(nrm2 + r, t);
+  }
+}
+
+// t = r / (delta - theta + shift) with the reference's clamp (davidson.rs:194-225); nrm2 += |t|^2
+__global__ void k_precond(const double* __restrict__ R, const double* __restrict__ delta, double theta, double shift,
+                          int n, double* __restrict__ t, double* __restrict__ nrm2) {
+  double s = 0.0;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+    double den = delta[k] - theta + shift;
+    if (fabs(den) < 1e-8) den = (den >= 0.0) ? 1e-8 : -1e-8;
+    const double v = R[k] / den;
+    t[k] = v;
+    s += v * v;
+  }
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  __shared__ double red[32];
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double tt = 0.0;
+    for (int i = 0; i < (int)(blockDim.x >> 5); ++i) tt += red[i];
+    atomicAdd(nrm2, tt);
+  }
+}
+
+// x[k] *= 1/sqrt(nrm2[0]) when sqrt(nrm2) > thr (thr < 0: always)
+__global__ void k_normalize(double* __restrict__ x, int n, const double* __restrict__ nrm2, double thr) {
+  const double nr = sqrt(nrm2[0]);
+  if (!(nr > thr)) return;
+  const double inv = 1.0 / nr;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) x[k] *= inv;
+}
+
+__global__ void k_norm2(const double* __restrict__ x, int n, double* __restrict__ nrm2) {
+  double s = 0.0;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) s += x[k] * x[k];
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  __shared__ double red[32];
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int i = 0; i < (int)(blockDim.x >> 5); ++i) t += red[i];
+    atomicAdd(nrm2, t);
+  }
+}
+
+}  // namespace qx
+
+using namespace qx;
+
+struct DevArr {
+  double* p = nullptr;
+  size_t n = 0;
+  void alloc(size_t count) {
+    if (count <= n) return;
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+    QX_CUDA(cudaMalloc(&p, count * sizeof(double)));
+    n = count;
+  }
+  ~DevArr() {
+    if (p) cudaFree(p);
+  }
+};
+
+struct qx_bse {
+  qx_ctx* ctx;
+  int nocc, nvir, naux, nov, precision;
+  int ldq, ldvp, ldov;
+  double alpha_x;
+  DevArr delta, dia, diaT, ijw, dabT;
+  DevArr xp, T, Yd, Z, Yx, Xr, Yr;  // matvec scratch
+  DevArr V, AV, X, AX, R, heff, jv, Z2, small;
+  std::vector<double> h_delta;
+};
+
+// y[v] = H x[v] for nvec vectors in row layout [nvec][ldov] (device).
+static void bse_apply_rows(qx_bse* B, const double* X, double* Y, int nvec) {
+  qx_ctx* ctx = B->ctx;
+  const int nocc = B->nocc, nvir = B->nvir, naux = B->naux;
+  // Direct term, step 1: T[a][(v,j)][Q] = sum_b X[v][j,b] dab[a][b][Q].
+  B->xp.alloc((size_t)nvec * nocc * B->ldvp);
+  {
+    const size_t tot = (size_t)nvec * nocc * B->ldvp;
+    k_pack_x<<<(unsigned)std::min<size_t>((tot + 255) / 256, 4096), 256, 0, ctx->stream>>>(X, B->ldov, nvec, nocc, nvir,
+                                                                                          B->xp.p, B->ldvp);
+    check_launch(ctx);
+  }
+  const size_t tslab = (size_t)nvec * nocc * B->ldq;
+  if (B->T.n < tslab * nvir) {
+    B->T.alloc(tslab * nvir);
+    QX_CUDA(cudaMemsetAsync(B->T.p, 0, tslab * nvir * sizeof(double), ctx->stream));  // Q padding stays zero
+  }
+  {
+    GemmNT g{};
+    g.M = nvec * nocc;
+    g.N = naux;
+    g.K = nvir;
+    g.A = B->xp.p;
+    g.lda = B->ldvp;
+    g.sA = 0;
+    g.B = B->dabT.p;
+    g.ldb = B->ldvp;
+    g.sB = (size_t)naux * B->ldvp;
+    g.C = B->T.p;
+    g.ldc = B->ldq;
+    g.sC = tslab;
+    g.batch = nvir;
+    g.alpha = 1.0;
+    g.beta = 0.0;
+    g.splitk = 1;
+    gemm_nt_f64(ctx, g);
+  }
+  // Step 2: Yd[i][(a,v)] = sum_{(j,Q)} ijw[i][(j,Q)] T[a][v][(j,Q)].
+  B->Yd.alloc((size_t)nocc * nvir * nvec);
+  {
+    GemmNT g{};
+    g.M = nocc;
+    g.N = nvir * nvec;
+    g.K = nocc * B->ldq;
+    g.A = B->ijw.p;
+    g.lda = nocc * B->ldq;
+    g.B = B->T.p;
+    g.ldb = nocc * B->ldq;
+    g.C = B->Yd.p;
+    g.ldc = nvir * nvec;
+    g.batch = 1;
+    g.alpha = 1.0;
+    g.beta = 0.0;
+    g.splitk = 0;
+    gemm_nt_f64(ctx, g);
+  }
+  // Exchange: Z[v][Q] = sum_ia X[v][ia] dia[ia][Q]; Yx[v][ia] = sum_Q Z[v][Q] dia[ia][Q].
+  if (B->alpha_x != 0.0) {
+    B->Z.alloc((size_t)nvec * B->ldq);
+    B->Yx.alloc((size_t)nvec * B->ldov);
+    GemmNT g{};
+    g.M = nvec;
+    g.N = naux;
+    g.K = B->nov;
+    g.A = X;
+    g.lda = B->ldov;
+    g.B = B->diaT.p;
+    g.ldb = B->ldov;
+    g.C = B->Z.p;
+    g.ldc = B->ldq;
+    g.batch = 1;
+    g.alpha = 1.0;
+    g.splitk = 0;
+    gemm_nt_f64(ctx, g);
+    GemmNT h{};
+    h.M = nvec;
+    h.N = B->nov;
+    h.K = naux;
+    h.A = B->Z.p;
+    h.lda = B->ldq;
+    h.B = B->dia.p;
+    h.ldb = B->ldq;
+    h.C = B->Yx.p;
+    h.ldc = B->ldov;
+    h.batch = 1;
+    h.alpha = 1.0;
+    h.splitk = 1;
+    gemm_nt_f64(ctx, h);
+  }
+  const size_t tot = (size_t)nvec * B->ldov;
+  k_bse_combine<<<(unsigned)std::min<size_t>((tot + 255) / 256, 4096), 256, 0, ctx->stream>>>(
+      X, B->delta.p, B->alpha_x != 0.0 ? B->Yx.p : nullptr, B->Yd.p, nvec, nocc, nvir, B->ldov, B->alpha_x, Y);
+  check_launch(ctx);
+}
+
+template <class F>
+static qx_status bse_guard(qx_ctx* ctx, F&& f) {
+  try {
+    ctx->pending.clear();
+    ctx->launches = 0;
+    QX_CUDA(cudaSetDevice(ctx->device));
+    f();
+    ctx->err.clear();
+    return QX_OK;
+  } catch (const Error& e) {
+    ctx->err = e.what();
+    return e.status;
+  } catch (const std::exception& e) {
+    ctx->err = e.what();
+    return QX_ERR_INVALID_INPUT;
+  }
+}
+
+static void upload(qx_ctx* ctx, double* dst, const double* src, size_t n) {
+  QX_CUDA(cudaMemcpyAsync(dst, src, n * sizeof(double), cudaMemcpyDefault, ctx->stream));
+}
+
 extern "C" {
+
 void qx_davidson_config_default(qx_davidson_config* c) {
   c->n_roots = 3;
   c->max_iter = 100;
@@ -10,16 +290,408 @@ void qx_davidson_config_default(qx_davidson_config* c) {
   c->lindep_threshold = 1e-12;
   c->level_shift = 0.001;
 }
-qx_status qx_bse_create(qx_ctx*, qx_bse**, int, int, int, const double*, const double*, const double*,
-                        const double*, const double*, int, int) { return QX_ERR_NOT_IMPLEMENTED; }
-qx_status qx_bse_destroy(qx_bse*) { return QX_OK; }
-qx_status qx_bse_apply(qx_bse*, const double*, double*, int) { return QX_ERR_NOT_IMPLEMENTED; }
-qx_status qx_bse_davidson(qx_bse*, const qx_davidson_config*, double*, double*, int*, double*, int*) {
-  return QX_ERR_NOT_IMPLEMENTED;
+
+qx_status qx_bse_create(qx_ctx* ctx, qx_bse** out, int nocc, int nvirt, int naux, const double* delta_qp,
+                        const double* df_ia, const double* df_ij, const double* df_ab, const double* w0, int spin,
+                        int precision) {
+  if (!ctx || !out) return QX_ERR_INVALID_INPUT;
+  *out = nullptr;
+  qx_bse* B = new qx_bse();
+  qx_status st = bse_guard(ctx, [&] {
+    QX_REQUIRE(nocc > 0 && nvirt > 0 && naux > 0, QX_ERR_DIMENSION_MISMATCH, "nocc=%d nvirt=%d naux=%d must be positive",
+               nocc, nvirt, naux);
+    QX_REQUIRE(delta_qp && df_ia && df_ij && df_ab && w0, QX_ERR_INVALID_INPUT, "null BSE input");
+    QX_REQUIRE(spin == 0 || spin == 1, QX_ERR_INVALID_INPUT, "Unknown spin type %d", spin);
+    QX_REQUIRE(precision == QX_PREC_FP64 || precision == QX_PREC_BF16X3, QX_ERR_INVALID_INPUT, "bad precision");
+    B->ctx = ctx;
+    B->nocc = nocc;
+    B->nvir = nvirt;
+    B->naux = naux;
+    B->nov = nocc * nvirt;
+    B->precision = precision;
+    B->ldq = round_up(naux, 8);
+    B->ldvp = round_up(nvirt, 8);
+    B->ldov = round_up(B->nov, 8);
+    B->alpha_x = spin == 0 ? 2.0 : 0.0;  // SpinType::exchange_prefactor (kernel.rs:67-79)
+    const int nov = B->nov;
+    B->h_delta.resize(nov);
+    QX_CUDA(cudaMemcpy(B->h_delta.data(), delta_qp, nov * sizeof(double), cudaMemcpyDefault));
+    for (double d : B->h_delta) QX_REQUIRE(std::isfinite(d), QX_ERR_NUMERICAL, "delta_qp contains NaN or Inf");
+    B->delta.alloc(B->ldov);
+    QX_CUDA(cudaMemsetAsync(B->delta.p, 0, B->ldov * sizeof(double), ctx->stream));
+    upload(ctx, B->delta.p, B->h_delta.data(), nov);
+    // Staging for unpadded inputs.
+    DevArr stage;
+    stage.alloc(std::max({(size_t)nvirt * nvirt * naux, (size_t)nov * naux, (size_t)naux * naux,
+                          (size_t)nocc * nocc * naux}));
+    // df_ia -> dia [nov][ldq] and diaT [naux][ldov].
+    upload(ctx, stage.p, df_ia, (size_t)nov * naux);
+    B->dia.alloc((size_t)nov * B->ldq);
+    QX_CUDA(cudaMemsetAsync(B->dia.p, 0, (size_t)nov * B->ldq * sizeof(double), ctx->stream));
+    QX_CUDA(cudaMemcpy2DAsync(B->dia.p, B->ldq * sizeof(double), stage.p, naux * sizeof(double), naux * sizeof(double),
+                              nov, cudaMemcpyDeviceToDevice, ctx->stream));
+    B->diaT.alloc((size_t)naux * B->ldov);
+    QX_CUDA(cudaMemsetAsync(B->diaT.p, 0, (size_t)naux * B->ldov * sizeof(double), ctx->stream));
+    transpose(ctx, stage.p, nov, naux, naux, 0, B->diaT.p, B->ldov, 0, 1);
+    // w0^T [Q][P] (ldq), df_ij [nocc^2][ldq]; ijw = df_ij w0 (kernel.rs:286-291).
+    DevArr w0T, dij;
+    upload(ctx, stage.p, w0, (size_t)naux * naux);
+    w0T.alloc((size_t)naux * B->ldq);
+    QX_CUDA(cudaMemsetAsync(w0T.p, 0, (size_t)naux * B->ldq * sizeof(double), ctx->stream));
+    transpose(ctx, stage.p, naux, naux, naux, 0, w0T.p, B->ldq, 0, 1);
+    QX_CUDA(cudaStreamSynchronize(ctx->stream));
+    upload(ctx, stage.p, df_ij, (size_t)nocc * nocc * naux);
+    dij.alloc((size_t)nocc * nocc * B->ldq);
+    QX_CUDA(cudaMemsetAsync(dij.p, 0, (size_t)nocc * nocc * B->ldq * sizeof(double), ctx->stream));
+    QX_CUDA(cudaMemcpy2DAsync(dij.p, B->ldq * sizeof(double), stage.p, naux * sizeof(double), naux * sizeof(double),
+                              (size_t)nocc * nocc, cudaMemcpyDeviceToDevice, ctx->stream));
+    B->ijw.alloc((size_t)nocc * nocc * B->ldq);
+    QX_CUDA(cudaMemsetAsync(B->ijw.p, 0, (size_t)nocc * nocc * B->ldq * sizeof(double), ctx->stream));
+    {
+      GemmNT g{};
+      g.M = nocc * nocc;
+      g.N = naux;
+      g.K = naux;
+      g.A = dij.p;
+      g.lda = B->ldq;
+      g.B = w0T.p;
+      g.ldb = B->ldq;
+      g.C = B->ijw.p;
+      g.ldc = B->ldq;
+      g.batch = 1;
+      g.alpha = 1.0;
+      g.splitk = 0;
+      gemm_nt_f64(ctx, g);
+    }
+    // df_ab [a][b][Q] -> dabT [a][Q][b] (ldvp).
+    QX_CUDA(cudaStreamSynchronize(ctx->stream));
+    upload(ctx, stage.p, df_ab, (size_t)nvirt * nvirt * naux);
+    B->dabT.alloc((size_t)nvirt * naux * B->ldvp);
+    QX_CUDA(cudaMemsetAsync(B->dabT.p, 0, (size_t)nvirt * naux * B->ldvp * sizeof(double), ctx->stream));
+    transpose(ctx, stage.p, nvirt, naux, naux, (size_t)nvirt * naux, B->dabT.p, B->ldvp, (size_t)naux * B->ldvp,
+              nvirt);
+    sync_and_check(ctx);
+  });
+  if (st != QX_OK) {
+    delete B;
+    return st;
+  }
+  *out = B;
+  return QX_OK;
 }
-qx_status qx_bse_w0(qx_ctx*, const double*, const double*, int, int, int, double*) { return QX_ERR_NOT_IMPLEMENTED; }
+
+qx_status qx_bse_destroy(qx_bse* B) {
+  if (!B) return QX_OK;
+  cudaSetDevice(B->ctx->device);
+  cudaStreamSynchronize(B->ctx->stream);
+  delete B;
+  return QX_OK;
+}
+
+qx_status qx_bse_apply(qx_bse* B, const double* x, double* y, int nvec) {
+  if (!B) return QX_ERR_INVALID_INPUT;
+  return bse_guard(B->ctx, [&] {
+    QX_REQUIRE(x && y && nvec > 0, QX_ERR_INVALID_INPUT, "invalid arguments to apply");
+    qx_ctx* ctx = B->ctx;
+    const int nov = B->nov;
+    // x, y are [nov][nvec] (apply_tda_hamiltonian_batch layout).
+    std::vector<double> hx((size_t)nov * nvec), hr((size_t)nvec * B->ldov, 0.0);
+    QX_CUDA(cudaMemcpy(hx.data(), x, hx.size() * sizeof(double), cudaMemcpyDefault));
+    for (double v : hx) QX_REQUIRE(std::isfinite(v), QX_ERR_NUMERICAL, "input vector contains NaN or Inf");
+    for (int k = 0; k < nov; ++k)
+      for (int v = 0; v < nvec; ++v) hr[(size_t)v * B->ldov + k] = hx[(size_t)k * nvec + v];
+    B->Xr.alloc(hr.size());
+    B->Yr.alloc(hr.size());
+    QX_CUDA(cudaMemcpyAsync(B->Xr.p, hr.data(), hr.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    bse_apply_rows(B, B->Xr.p, B->Yr.p, nvec);
+    QX_CUDA(cudaMemcpyAsync(hr.data(), B->Yr.p, hr.size() * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    sync_and_check(ctx);
+    for (int k = 0; k < nov; ++k)
+      for (int v = 0; v < nvec; ++v) hx[(size_t)k * nvec + v] = hr[(size_t)v * B->ldov + k];
+    for (double v : hx)
+      QX_REQUIRE(std::isfinite(v), QX_ERR_NUMERICAL, "BSE Hamiltonian application produced non-finite values");
+    QX_CUDA(cudaMemcpy(y, hx.data(), hx.size() * sizeof(double), cudaMemcpyDefault));
+  });
+}
+
+qx_status qx_bse_davidson(qx_bse* B, const qx_davidson_config* cfgp, double* eigenvalues, double* eigenvectors,
+                          int* converged_out, double* residual_norms, int* iterations) {
+  if (!B || !cfgp) return QX_ERR_INVALID_INPUT;
+  return bse_guard(B->ctx, [&] {
+    qx_ctx* ctx = B->ctx;
+    const qx_davidson_config cfg = *cfgp;
+    const int n = B->nov, ld = B->ldov;
+    const int nroots = std::min(cfg.n_roots, n);
+    const int max_space = std::min(cfg.max_space, n);
+    QX_REQUIRE(nroots > 0 && eigenvalues && eigenvectors, QX_ERR_INVALID_INPUT, "invalid Davidson arguments");
+    QX_REQUIRE(max_space <= 1024, QX_ERR_INVALID_INPUT, "max_space %d exceeds 1024", max_space);
+    const int cap = std::max(max_space, nroots) + nroots + 1;
+    B->V.alloc((size_t)cap * ld);
+    B->AV.alloc((size_t)cap * ld);
+    B->X.alloc((size_t)nroots * ld);
+    B->AX.alloc((size_t)nroots * ld);
+    B->R.alloc((size_t)nroots * ld);
+    B->heff.alloc((size_t)cap * cap);
+    B->jv.alloc((size_t)cap * cap);
+    B->Z2.alloc((size_t)cap * cap);
+    B->small.alloc((size_t)4 * cap + 64);
+    double* d_theta = B->small.p;
+    double* d_nrm = d_theta + cap;
+    double* d_c = d_nrm + cap;
+    int* d_info = reinterpret_cast<int*>(d_c + cap);
+    QX_CUDA(cudaMemsetAsync(B->V.p, 0, (size_t)cap * ld * sizeof(double), ctx->stream));
+    auto apply = [&](int first, int count) { bse_apply_rows(B, B->V.p + (size_t)first * ld, B->AV.p + (size_t)first * ld, count); };
+    auto rr = [&](int nv) {
+      // heff = V AV^T, then Jacobi (symmetrises) -> theta, Z2 (columns).
+      GemmNT g{};
+      g.M = nv;
+      g.N = nv;
+      g.K = n;
+      g.A = B->V.p;
+      g.lda = ld;
+      g.B = B->AV.p;
+      g.ldb = ld;
+      g.C = B->heff.p;
+      g.ldc = nv;
+      g.batch = 1;
+      g.alpha = 1.0;
+      g.splitk = 0;
+      gemm_nt_f64(ctx, g);
+      jacobi_eigh(ctx, B->heff.p, B->jv.p, nv, nv, d_theta, B->Z2.p, nv, d_info);
+    };
+    const int nthreads = 256, nblk = std::min(ceil_div(n, nthreads), 2 * ctx->sm_count);
+    // Trivial case (davidson.rs:384-387, 510-540): the full matrix.
+    if (n <= nroots) {
+      std::vector<double> id((size_t)n * ld, 0.0);
+      for (int i = 0; i < n; ++i) id[(size_t)i * ld + i] = 1.0;
+      QX_CUDA(cudaMemcpyAsync(B->V.p, id.data(), id.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+      apply(0, n);
+      rr(n);
+      std::vector<double> th(n), zz((size_t)n * n);
+      QX_CUDA(cudaMemcpyAsync(th.data(), d_theta, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+      QX_CUDA(cudaMemcpyAsync(zz.data(), B->Z2.p, zz.size() * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+      sync_and_check(ctx);
+      std::vector<double> ev((size_t)n * nroots);
+      for (int k = 0; k < n; ++k)
+        for (int r = 0; r < nroots; ++r) ev[(size_t)k * nroots + r] = zz[(size_t)k * n + r];
+      QX_CUDA(cudaMemcpy(eigenvalues, th.data(), nroots * sizeof(double), cudaMemcpyDefault));
+      QX_CUDA(cudaMemcpy(eigenvectors, ev.data(), ev.size() * sizeof(double), cudaMemcpyDefault));
+      if (converged_out)
+        for (int r = 0; r < nroots; ++r) converged_out[r] = 1;
+      if (residual_norms)
+        for (int r = 0; r < nroots; ++r) residual_norms[r] = 0.0;
+      if (iterations) *iterations = 1;
+      return;
+    }
+    // Initial subspace: unit vectors at the smallest gaps (davidson.rs:157-176).
+    std::vector<int> order(n);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return B->h_delta[a] < B->h_delta[b]; });
+    {
+      std::vector<double> init((size_t)nroots * ld, 0.0);
+      for (int i = 0; i < nroots; ++i) init[(size_t)i * ld + order[i]] = 1.0;
+      QX_CUDA(cudaMemcpyAsync(B->V.p, init.data(), init.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    }
+    int nv = nroots;
+    apply(0, nv);
+    std::vector<double> evals(nroots, 0.0), rnorm(nroots, std::numeric_limits<double>::max());
+    std::vector<int> conv(nroots, 0);
+    DevArr evecs;  // converged eigenvectors [nroots][ld]
+    evecs.alloc((size_t)nroots * ld);
+    QX_CUDA(cudaMemsetAsync(evecs.p, 0, (size_t)nroots * ld * sizeof(double), ctx->stream));
+    int iter = 0;
+    bool all = false;
+    std::vector<double> th(cap), nr(cap);
+    for (iter = 0; iter < cfg.max_iter; ++iter) {
+      rr(nv);
+      const int nr_ = std::min(nroots, nv);
+      // Ritz vectors X = V Y, AX = AV Y.
+      combine_rows(ctx, B->V.p, ld, nv, B->Z2.p, nv, nr_, n, B->X.p, ld, 1.0, 0.0);
+      combine_rows(ctx, B->AV.p, ld, nv, B->Z2.p, nv, nr_, n, B->AX.p, ld, 1.0, 0.0);
+      QX_CUDA(cudaMemsetAsync(d_nrm, 0, nr_ * sizeof(double), ctx->stream));
+      k_residual<<<dim3(nblk, nr_), nthreads, 0, ctx->stream>>>(B->AX.p, B->X.p, d_theta, ld, n, B->R.p, d_nrm);
+      check_launch(ctx);
+      QX_CUDA(cudaMemcpyAsync(th.data(), d_theta, nr_ * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+      QX_CUDA(cudaMemcpyAsync(nr.data(), d_nrm, nr_ * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+      sync_and_check(ctx);
+      std::vector<int> newr;
+      for (int j = 0; j < nroots; ++j) {
+        if (j >= nr_ || conv[j]) continue;
+        const double res = std::sqrt(nr[j]);
+        rnorm[j] = res;
+        if (res < cfg.tol_residual) {
+          conv[j] = 1;
+          evals[j] = th[j];
+          QX_CUDA(cudaMemcpyAsync(evecs.p + (size_t)j * ld, B->X.p + (size_t)j * ld, ld * sizeof(double),
+                                  cudaMemcpyDeviceToDevice, ctx->stream));
+          continue;
+        }
+        newr.push_back(j);
+      }
+      all = std::all_of(conv.begin(), conv.end(), [](int c) { return c != 0; });
+      if (all) {
+        ++iter;
+        break;
+      }
+      if (newr.empty()) continue;
+      // Preconditioned residuals t_j (davidson.rs:444-449), staged after V.
+      const int nnew = (int)newr.size();
+      for (int q = 0; q < nnew; ++q) {
+        const int j = newr[q];
+        double* t = B->V.p + (size_t)(nv + q) * ld;
+        QX_CUDA(cudaMemsetAsync(d_c, 0, sizeof(double), ctx->stream));
+        k_precond<<<nblk, nthreads, 0, ctx->stream>>>(B->R.p + (size_t)j * ld, B->delta.p, th[j], cfg.level_shift, n,
+                                                      t, d_c);
+        check_launch(ctx);
+        k_normalize<<<nblk, nthreads, 0, ctx->stream>>>(t, n, d_c, 1e-14);
+        check_launch(ctx);
+      }
+      if (nv + nnew > max_space) {
+        // Restart from the Ritz vectors, re-orthonormalised (davidson.rs:298-307).
+        QX_CUDA(cudaMemcpyAsync(B->V.p, B->X.p, (size_t)nr_ * ld * sizeof(double), cudaMemcpyDeviceToDevice,
+                                ctx->stream));
+        for (int i = 0; i < nr_; ++i) {
+          double* v = B->V.p + (size_t)i * ld;
+          for (int pass = 0; pass < 2 && i > 0; ++pass) {
+            GemmNT g{};
+            g.M = i;
+            g.N = 1;
+            g.K = n;
+            g.A = B->V.p;
+            g.lda = ld;
+            g.B = v;
+            g.ldb = ld;
+            g.C = d_c;
+            g.ldc = 1;
+            g.batch = 1;
+            g.alpha = 1.0;
+            g.splitk = 0;
+            gemm_nt_f64(ctx, g);
+            combine_rows(ctx, B->V.p, ld, i, d_c, 1, 1, n, v, ld, -1.0, 1.0);
+          }
+          QX_CUDA(cudaMemsetAsync(d_nrm, 0, sizeof(double), ctx->stream));
+          k_norm2<<<nblk, nthreads, 0, ctx->stream>>>(v, n, d_nrm);
+          check_launch(ctx);
+          k_normalize<<<nblk, nthreads, 0, ctx->stream>>>(v, n, d_nrm, -1.0);
+          check_launch(ctx);
+        }
+        nv = nr_;
+        QX_CUDA(cudaMemsetAsync(B->V.p + (size_t)nv * ld, 0, (size_t)(cap - nv) * ld * sizeof(double), ctx->stream));
+        apply(0, nv);
+        continue;
+      }
+      // Double Gram-Schmidt of each candidate against the subspace (davidson.rs:240-285).
+      int added = 0;
+      for (int q = 0; q < nnew; ++q) {
+        double* src = B->V.p + (size_t)(nv + q) * ld;
+        double* dst = B->V.p + (size_t)(nv + added) * ld;
+        if (src != dst)
+          QX_CUDA(cudaMemcpyAsync(dst, src, ld * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+        const int cur = nv + added;
+        for (int pass = 0; pass < 2; ++pass) {
+          GemmNT g{};
+          g.M = cur;
+          g.N = 1;
+          g.K = n;
+          g.A = B->V.p;
+          g.lda = ld;
+          g.B = dst;
+          g.ldb = ld;
+          g.C = d_c;
+          g.ldc = 1;
+          g.batch = 1;
+          g.alpha = 1.0;
+          g.splitk = 0;
+          gemm_nt_f64(ctx, g);
+          combine_rows(ctx, B->V.p, ld, cur, d_c, 1, 1, n, dst, ld, -1.0, 1.0);
+        }
+        QX_CUDA(cudaMemsetAsync(d_nrm, 0, sizeof(double), ctx->stream));
+        k_norm2<<<nblk, nthreads, 0, ctx->stream>>>(dst, n, d_nrm);
+        check_launch(ctx);
+        double h2 = 0.0;
+        QX_CUDA(cudaMemcpyAsync(&h2, d_nrm, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+        sync_and_check(ctx);
+        if (std::sqrt(h2) < cfg.lindep_threshold) continue;
+        k_normalize<<<nblk, nthreads, 0, ctx->stream>>>(dst, n, d_nrm, -1.0);
+        check_launch(ctx);
+        ++added;
+      }
+      QX_CUDA(cudaMemsetAsync(B->V.p + (size_t)(nv + added) * ld, 0, (size_t)(cap - nv - added) * ld * sizeof(double),
+                              ctx->stream));
+      if (added > 0) apply(nv, added);
+      nv += added;
+    }
+    // Not converged: the latest Ritz approximation for roots never stored
+    // (davidson.rs:480-496).
+    if (!all) {
+      rr(nv);
+      const int nr_ = std::min(nroots, nv);
+      combine_rows(ctx, B->V.p, ld, nv, B->Z2.p, nv, nr_, n, B->X.p, ld, 1.0, 0.0);
+      QX_CUDA(cudaMemcpyAsync(th.data(), d_theta, nr_ * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+      sync_and_check(ctx);
+      for (int j = 0; j < nr_; ++j)
+        if (!conv[j]) {
+          evals[j] = th[j];
+          QX_CUDA(cudaMemcpyAsync(evecs.p + (size_t)j * ld, B->X.p + (size_t)j * ld, ld * sizeof(double),
+                                  cudaMemcpyDeviceToDevice, ctx->stream));
+        }
+      iter = cfg.max_iter;
+    }
+    std::vector<double> hv((size_t)nroots * ld), ev((size_t)n * nroots);
+    QX_CUDA(cudaMemcpyAsync(hv.data(), evecs.p, hv.size() * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    sync_and_check(ctx);
+    for (int k = 0; k < n; ++k)
+      for (int r = 0; r < nroots; ++r) ev[(size_t)k * nroots + r] = hv[(size_t)r * ld + k];
+    QX_CUDA(cudaMemcpy(eigenvalues, evals.data(), nroots * sizeof(double), cudaMemcpyDefault));
+    QX_CUDA(cudaMemcpy(eigenvectors, ev.data(), ev.size() * sizeof(double), cudaMemcpyDefault));
+    if (converged_out)
+      for (int r = 0; r < nroots; ++r) converged_out[r] = conv[r];
+    if (residual_norms)
+      for (int r = 0; r < nroots; ++r) residual_norms[r] = rnorm[r];
+    if (iterations) *iterations = iter;
+  });
+}
+
+qx_status qx_bse_w0(qx_ctx* ctx, const double* mo_energy, const double* lpq_ov, int naux, int nocc, int nvir,
+                    double* w0) {
+  if (!ctx) return QX_ERR_INVALID_INPUT;
+  return bse_guard(ctx, [&] {
+    QX_REQUIRE(mo_energy && lpq_ov && w0 && naux > 0 && nocc > 0 && nvir > 0, QX_ERR_INVALID_INPUT,
+               "invalid arguments to bse_w0");
+    const int nov = nocc * nvir, ldov = round_up(nov, 8), ldn = round_up(naux, 8);
+    const double* d_lov = (const double*)device_view(ctx, WS_LPQ, lpq_ov, (size_t)naux * nov * sizeof(double));
+    ctx->ws[WS_SMALL].reserve((nocc + nvir + 8) * sizeof(double));
+    double* d_e = ctx->ws[WS_SMALL].as<double>();
+    double* d_f = d_e + nocc + nvir;
+    QX_CUDA(cudaMemcpyAsync(d_e, mo_energy, (nocc + nvir) * sizeof(double), cudaMemcpyDefault, ctx->stream));
+    QX_CUDA(cudaMemsetAsync(d_f, 0, sizeof(double), ctx->stream));
+    ctx->ws[WS_BOV].reserve((size_t)naux * ldov * sizeof(double));
+    double* bov = ctx->ws[WS_BOV].as<double>();
+    QX_CUDA(cudaMemcpy2DAsync(bov, ldov * sizeof(double), d_lov, nov * sizeof(double), nov * sizeof(double), naux,
+                              cudaMemcpyDeviceToDevice, ctx->stream));
+    if (ldov > nov)
+      QX_CUDA(cudaMemset2DAsync(bov + nov, ldov * sizeof(double), 0, (ldov - nov) * sizeof(double), naux, ctx->stream));
+    ctx->ws[WS_CHI].reserve((size_t)ldov * sizeof(double));
+    double* chi = ctx->ws[WS_CHI].as<double>();
+    const size_t stride = (size_t)naux * ldn;
+    ctx->ws[WS_EPS].reserve(stride * sizeof(double));
+    double* eps = ctx->ws[WS_EPS].as<double>();
+    launch_chi(ctx, d_e, nocc, nvir, d_f, 1, 0, chi, ldov);
+    launch_eps_fp64(ctx, bov, ldov, naux, nov, chi, 1, eps, ldn, stride);
+    launch_invert_wc(ctx, eps, naux, ldn, stride, 1);
+    std::vector<double> h(stride);
+    QX_CUDA(cudaMemcpyAsync(h.data(), eps, stride * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    sync_and_check(ctx);
+    std::vector<double> out((size_t)naux * naux);
+    for (int r = 0; r < naux; ++r)
+      for (int c = 0; c < naux; ++c) out[(size_t)r * naux + c] = h[(size_t)r * ldn + c] + (r == c ? 1.0 : 0.0);
+    QX_CUDA(cudaMemcpy(w0, out.data(), out.size() * sizeof(double), cudaMemcpyDefault));
+  });
+}
+
 qx_status qx_g0w0_cd(qx_ctx*, const double*, const double*, const double*, int, int, int, const int*, int, int, double,
                      double, int, int, double*, double*, double*, double*) {
   return QX_ERR_NOT_IMPLEMENTED;
 }
-}
+
+}  // extern "C"
