@@ -3,6 +3,7 @@
 #include <algorithm>
 #include <map>
 
+#include "qx_gw_sys.cuh"
 #include "qx_internal.cuh"
 
 #define QX_VERSION "qx-b200 0.1.0 (sm_100a)"
@@ -92,10 +93,6 @@ std::vector<int> pade_indices(int nws, int npade) {
   return idx;
 }
 
-// Self-energy grid (correlation_ac.rs:268-302).
-struct SigmaGrid {
-  std::vector<double> freqs, wts, iw;
-};
 SigmaGrid sigma_grid(int nw, double cutoff, double x0) {
   SigmaGrid g;
   g.freqs.resize(nw);
@@ -111,11 +108,6 @@ SigmaGrid sigma_grid(int nw, double cutoff, double x0) {
   return g;
 }
 
-// Unique unordered MO pairs touched by the target orbitals.
-struct PairSet {
-  std::vector<int2> pairs;
-  std::vector<int> index;  // [norbs][nmo]
-};
 PairSet build_pairs(const std::vector<int>& orbs, int nmo) {
   PairSet ps;
   std::vector<int> pid((size_t)nmo * nmo, -1);
@@ -134,21 +126,6 @@ PairSet build_pairs(const std::vector<int>& orbs, int nmo) {
   }
   return ps;
 }
-
-// Device-resident state of one GW system: pair tensor, B_ov and grids.
-struct GWSystem {
-  int nmo, nocc, nvir, naux, nov, ldk, ldov, ldn, npair, nw, nws, norbs;
-  int precision;
-  const double* lpq;
-  double *bpt, *bov, *chi, *eps, *v, *sigma;
-  double *d_freqs, *d_wts, *d_iw, *d_en;
-  int *d_pidx, *d_orbs;
-  size_t eps_stride;
-  std::vector<int> orbs;
-  SigmaGrid grid;
-  void *bpt_hi = nullptr, *bpt_lo = nullptr, *wc_hi = nullptr, *wc_lo = nullptr;
-  float* bpt_f32 = nullptr;
-};
 
 __global__ void k_to_f32(const double* __restrict__ s, float* __restrict__ d, size_t n) {
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
@@ -259,10 +236,9 @@ void accumulate_stage_times(qx_ctx* ctx) {
   }
 }
 
-// One imaginary-axis Sigma_c evaluation with energies e (host array [nmo]).
-void gw_sigma(qx_ctx* ctx, GWSystem& S, const double* e_host) {
+// Wc_nm(iw) for every pair of the system: v[w][pair] (energies e on the host).
+void gw_wc_pairs(qx_ctx* ctx, GWSystem& S, const double* e_host) {
   QX_CUDA(cudaMemcpyAsync(S.d_en, e_host, S.nmo * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
-  const double ef = 0.5 * (e_host[S.nocc - 1] + e_host[S.nocc]);
   record_stage(ctx, QX_ST_P0, true);
   launch_chi(ctx, S.d_en, S.nocc, S.nvir, S.d_freqs, S.nw, 0, S.chi, S.ldov);
   if (S.precision == QX_PREC_BF16X3)
@@ -282,6 +258,12 @@ void gw_sigma(qx_ctx* ctx, GWSystem& S, const double* e_host) {
     launch_pair_contract_fp64(ctx, S.bpt, S.ldk, S.npair, S.naux, S.eps, S.ldn, S.eps_stride, S.nw, S.v, S.npair);
   }
   record_stage(ctx, QX_ST_CONTRACT, false);
+}
+
+// One imaginary-axis Sigma_c evaluation with energies e (host array [nmo]).
+void gw_sigma(qx_ctx* ctx, GWSystem& S, const double* e_host) {
+  gw_wc_pairs(ctx, S, e_host);
+  const double ef = 0.5 * (e_host[S.nocc - 1] + e_host[S.nocc]);
   record_stage(ctx, QX_ST_SIGMA, true);
   launch_sigma_assemble(ctx, S.v, S.npair, S.nw, S.d_pidx, S.norbs, S.nmo, S.d_orbs, S.nocc, S.d_en, ef, S.d_freqs,
                         S.d_wts, S.d_iw, S.nws, S.sigma);

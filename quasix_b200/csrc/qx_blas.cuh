@@ -34,4 +34,8 @@ void combine_rows(qx_ctx* ctx, const double* V, int ldv, int nv, const double* c
 // (n x lda).  info[0] receives the number of sweeps.
 void jacobi_eigh(qx_ctx* ctx, double* A, double* V, int n, int lda, double* w, double* Z, int ldz, int* info);
 
+// out[b][c][r] = in[b][r][c] (rows x cols per batch), through 32x32 smem tiles.
+void transpose(qx_ctx* ctx, const double* in, int rows, int cols, int ldi, size_t si, double* out, int ldo, size_t so,
+               int batch);
+
 }  // namespace qx

@@ -28,8 +28,8 @@ __global__ void k_transpose(const double* __restrict__ in, int rows, int cols, i
   }
 }
 
-static void transpose(qx_ctx* ctx, const double* in, int rows, int cols, int ldi, size_t si, double* out, int ldo,
-                      size_t so, int batch) {
+void transpose(qx_ctx* ctx, const double* in, int rows, int cols, int ldi, size_t si, double* out, int ldo,
+               size_t so, int batch) {
   dim3 grid(ceil_div(cols, 32), ceil_div(rows, 32), batch);
   k_transpose<<<grid, dim3(32, 8), 0, ctx->stream>>>(in, rows, cols, ldi, si, out, ldo, so);
   check_launch(ctx);
@@ -687,11 +687,6 @@ qx_status qx_bse_w0(qx_ctx* ctx, const double* mo_energy, const double* lpq_ov, 
       for (int c = 0; c < naux; ++c) out[(size_t)r * naux + c] = h[(size_t)r * ldn + c] + (r == c ? 1.0 : 0.0);
     QX_CUDA(cudaMemcpy(w0, out.data(), out.size() * sizeof(double), cudaMemcpyDefault));
   });
-}
-
-qx_status qx_g0w0_cd(qx_ctx*, const double*, const double*, const double*, int, int, int, const int*, int, int, double,
-                     double, int, int, double*, double*, double*, double*) {
-  return QX_ERR_NOT_IMPLEMENTED;
 }
 
 }  // extern "C"

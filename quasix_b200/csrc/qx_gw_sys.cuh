@@ -1,0 +1,42 @@
+// Device-resident GW system state shared by the AC driver (qx_api.cu) and
+// the contour-deformation driver (qx_cd.cu).
+#pragma once
+#include "qx_internal.cuh"
+
+namespace qx {
+
+// Self-energy grid (correlation_ac.rs:268-302).
+struct SigmaGrid {
+  std::vector<double> freqs, wts, iw;
+};
+// Unique unordered MO pairs touched by the target orbitals.
+struct PairSet {
+  std::vector<int2> pairs;
+  std::vector<int> index;  // [norbs][nmo]
+};
+// Device-resident state of one GW system: pair tensor, B_ov and grids.
+struct GWSystem {
+  int nmo, nocc, nvir, naux, nov, ldk, ldov, ldn, npair, nw, nws, norbs;
+  int precision;
+  const double* lpq;
+  double *bpt, *bov, *chi, *eps, *v, *sigma;
+  double *d_freqs, *d_wts, *d_iw, *d_en;
+  int *d_pidx, *d_orbs;
+  size_t eps_stride;
+  std::vector<int> orbs;
+  SigmaGrid grid;
+  void *bpt_hi = nullptr, *bpt_lo = nullptr, *wc_hi = nullptr, *wc_lo = nullptr;
+  float* bpt_f32 = nullptr;
+};
+
+SigmaGrid sigma_grid(int nw, double cutoff, double x0);
+PairSet build_pairs(const std::vector<int>& orbs, int nmo);
+void gw_setup(qx_ctx* ctx, GWSystem& S, const double* d_lpq, int nmo, int nocc, int naux, const std::vector<int>& orbs,
+              int nw, double cutoff, double x0, int precision);
+void gw_wc_pairs(qx_ctx* ctx, GWSystem& S, const double* e_host);
+void gw_sigma(qx_ctx* ctx, GWSystem& S, const double* e_host);
+void record_stage(qx_ctx* ctx, int st, bool begin);
+void accumulate_stage_times(qx_ctx* ctx);
+void validate_common(int nmo, int nocc, int naux);
+
+}  // namespace qx
