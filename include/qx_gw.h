@@ -37,11 +37,13 @@ typedef enum {
   QX_ERR_NO_DEVICE = 7           /* no usable sm_100 device */
 } qx_status;
 
-/* Arithmetic form of the dense contractions (P0, Sigma_c pair contraction,
- * BSE matvecs).  FP64: the plain path.  BF16X3: tcgen05 tensor cores, each
- * FP64 operand split into bf16 hi + lo, three products hi*hi + hi*lo + lo*hi
- * accumulated in FP32 in TMEM; factorisations, Pade and QP stay FP64. */
-typedef enum { QX_PREC_FP64 = 0, QX_PREC_BF16X3 = 1 } qx_precision;
+/* Arithmetic form of the dense contractions (P0, Sigma_c pair contraction).
+ * FP64: the plain path.  BF16X3 / FP16X3: tcgen05 tensor cores, each FP64
+ * operand split into hi + lo (bf16, or fp16 after a per-matrix power-of-two
+ * scale), three products hi*hi + hi*lo + lo*hi accumulated in FP32 in TMEM;
+ * the factorisation of eps, Pade and QP stay FP64.  Relative error per product
+ * ~2^-17 (BF16X3) or ~2^-22 (FP16X3). */
+typedef enum { QX_PREC_FP64 = 0, QX_PREC_BF16X3 = 1, QX_PREC_FP16X3 = 2 } qx_precision;
 
 typedef struct qx_ctx qx_ctx;
 

@@ -19,7 +19,7 @@ STATUS_NAMES = {
     0: "OK", 1: "InvalidInput", 2: "DimensionMismatch", 3: "NumericalError", 4: "ConvergenceError",
     5: "NotImplemented", 6: "CudaError", 7: "NoDevice",
 }
-PREC = {"fp64": 0, "bf16x3": 1}
+PREC = {"fp64": 0, "bf16x3": 1, "fp16x3": 2}
 
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int)

@@ -58,7 +58,7 @@ def build(verbose: bool = False, force: bool = False) -> str:
             print(text)
     if failed:
         raise RuntimeError("nvcc failed:\n" + "\n".join(f"{s}:\n{t}" for s, t in failed))
-    cmd = [nvcc()] + ARCH + ["-shared", "-o", OUT] + objs
+    cmd = [nvcc()] + ARCH + ["-shared", "-Xlinker", "--no-undefined", "-o", OUT] + objs
     subprocess.check_call(cmd)
     return OUT
 

@@ -1,8 +1,11 @@
-// tcgen05 (5th-generation tensor core) kernels for the BF16x3 form.
+// tcgen05 (5th-generation tensor core) kernels for the split-operand forms.
 //
-// Each FP64 operand X is split into bf16 hi = bf16(X) and lo = bf16(X - hi);
-// a product is formed as hi*hi' + hi*lo' + lo*hi' with FP32 accumulation in
-// TMEM (relative error ~2^-17 per product, vs 2^-9 for one bf16 product).
+// Each FP64 operand X is split into hi = r(s X) and lo = r(s X - hi), with r()
+// rounding to bf16 (BF16X3, s = 1) or to fp16 (FP16X3, s a power of two per
+// matrix and frequency that puts max|s X| in [2^14, 2^15)).  A product is
+// formed as hi*hi' + hi*lo' + lo*hi' with FP32 accumulation in TMEM and the
+// scales divided out in the epilogue.  Relative error per product: ~2^-17
+// (bf16 pairs) or ~2^-22 (fp16 pairs), vs 2^-9 / 2^-12 for one product.
 //
 // One warp-specialised "NT" GEMM serves both contractions of the GW chain:
 //   C[m][n] = sum_k A[m][k] B[w][n][k]     (A, B K-major, bf16 hi/lo pairs)
@@ -14,6 +17,7 @@
 // on timeout the CTA records an error code and unwinds.
 #include <cuda.h>
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 
 #include "qx_internal.cuh"
 
@@ -94,12 +98,14 @@ __device__ __forceinline__ uint64_t umma_desc_sw128(uint32_t saddr) {
   return d;
 }
 
-// Instruction descriptor: kind::f16 with bf16 A/B, f32 accumulator, K-major A and B.
-__host__ __device__ constexpr uint32_t umma_idesc_bf16(int M, int N) {
-  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+// Instruction descriptor: kind::f16 with bf16 (fmt 1) or fp16 (fmt 0) A and B of
+// the same type, f32 accumulator, K-major A and B.
+__host__ __device__ constexpr uint32_t umma_idesc_f16(int M, int N, int fp16) {
+  return (1u << 4) | ((fp16 ? 0u : 1u) << 7) | ((fp16 ? 0u : 1u) << 10) | ((uint32_t)(N >> 3) << 17) |
+         ((uint32_t)(M >> 4) << 24);
 }
 
-__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+__device__ __forceinline__ void umma_f16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
                                           uint32_t accumulate) {
   asm volatile(
       "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(
@@ -130,7 +136,13 @@ enum { EPI_ROWDOT = 0, EPI_STORE = 1 };
 constexpr int TC_BM = 128;
 constexpr int TC_BK = 64;  // one 128-byte swizzle row of bf16
 constexpr int TC_STAGES = 2;
-constexpr int TC_THREADS = 192;
+// Epilogue warps: 4 (ROWDOT: one TMEM lane quarter each) or 8 (STORE: two
+// warps per lane quarter, 64 columns each).
+template <int EPI>
+struct TcWarps {
+  static constexpr int NEPI = (EPI == 1) ? 8 : 4;
+  static constexpr int THREADS = 64 + 32 * NEPI;
+};
 
 template <int BN>
 struct TcSmem {
@@ -153,11 +165,14 @@ struct TcArgs {
   int ldo;
   size_t out_stride;
   int lower_tiles;      // STORE: enumerate lower-triangular (m, n) tile pairs and mirror
+  int fp16;             // operand type: 0 bf16, 1 fp16
+  const float* scaleA;  // [1]      scale applied to A before the split
+  const float* scaleB;  // [nbatch] scale applied to B[w] before the split
   int* err;
 };
 
 template <int BN, int EPI>
-__global__ void __launch_bounds__(TC_THREADS, 1)
+__global__ void __launch_bounds__(TcWarps<EPI>::THREADS, 1)
     k_tc_gemm(const __grid_constant__ CUtensorMap mapAh, const __grid_constant__ CUtensorMap mapAl,
               const __grid_constant__ CUtensorMap mapBh, const __grid_constant__ CUtensorMap mapBl, TcArgs args) {
   using L = TcSmem<BN>;
@@ -211,7 +226,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     }
     for (int b = 0; b < 2; ++b) {
       mbar_init(&acc_full[b], 1);
-      mbar_init(&acc_empty[b], 4);  // one arrival per epilogue warp
+      mbar_init(&acc_empty[b], TcWarps<EPI>::NEPI);  // one arrival per epilogue warp
     }
     mbar_init(drain, 1);
     *abort_flag = 0;
@@ -261,39 +276,50 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
       }
     } else if (warp == 1) {
       // ---------------- MMA issuer ----------------
+      // Accumulation units: ROWDOT accumulates a whole N tile in one TMEM
+      // buffer; STORE restarts the accumulator every k-block (64 of K) and the
+      // epilogue sums the blocks in FP64, because the FP32 accumulation of the
+      // tensor pipe carries a small same-signed error per step that grows
+      // linearly over long positive sums (the diagonal of Pi over K = nov).
       if (lane == 0) {
-        constexpr uint32_t idesc = umma_idesc_bf16(TC_BM, BN);
-        int g = 0, t = 0;
-        for (int nt = nt_begin; nt < nt_end; ++nt, ++t) {
-          const int buf = t & 1;
-          if (t >= 2) {
-            if (!mbar_wait(&acc_empty[buf], ((t / 2) - 1) & 1, abort_flag, args.err, 2)) break;
-          }
-          tc_fence_after();
-          const uint32_t dacc = tmem_base + buf * BN;
-          bool ok = true;
+        const uint32_t idesc = umma_idesc_f16(TC_BM, BN, args.fp16);
+        int g = 0, u = 0;
+        bool ok = true;
+        for (int nt = nt_begin; nt < nt_end && ok; ++nt) {
           for (int kb = 0; kb < k_blocks; ++kb, ++g) {
+            const bool unit_start = (EPI == EPI_STORE) || kb == 0;
+            const bool unit_end = (EPI == EPI_STORE) || kb == k_blocks - 1;
+            const int buf = u & 1;
+            if (unit_start && u >= 2) {
+              if (!mbar_wait(&acc_empty[buf], ((u / 2) - 1) & 1, abort_flag, args.err, 2)) {
+                ok = false;
+                break;
+              }
+            }
             const int s = g % TC_STAGES;
             if (!mbar_wait(&full[s], (g / TC_STAGES) & 1, abort_flag, args.err, 3)) {
               ok = false;
               break;
             }
             tc_fence_after();
+            const uint32_t dacc = tmem_base + buf * BN;
             uint8_t* st = smem + s * L::STAGE_BYTES;
             const uint32_t ah = smem_u32(st), al = ah + L::A_BYTES;
             const uint32_t bh = ah + 2 * L::A_BYTES, bl = bh + L::B_BYTES;
 #pragma unroll
             for (int kk = 0; kk < TC_BK / 16; ++kk) {
               const uint32_t off = kk * 32;
-              const uint32_t acc0 = (kb > 0 || kk > 0) ? 1u : 0u;
-              umma_bf16(dacc, umma_desc_sw128(ah + off), umma_desc_sw128(bh + off), idesc, acc0);
-              umma_bf16(dacc, umma_desc_sw128(ah + off), umma_desc_sw128(bl + off), idesc, 1u);
-              umma_bf16(dacc, umma_desc_sw128(al + off), umma_desc_sw128(bh + off), idesc, 1u);
+              const uint32_t acc0 = (!unit_start || kk > 0) ? 1u : 0u;
+              umma_f16(dacc, umma_desc_sw128(ah + off), umma_desc_sw128(bh + off), idesc, acc0);
+              umma_f16(dacc, umma_desc_sw128(ah + off), umma_desc_sw128(bl + off), idesc, 1u);
+              umma_f16(dacc, umma_desc_sw128(al + off), umma_desc_sw128(bh + off), idesc, 1u);
             }
             umma_commit(&empty[s]);
+            if (unit_end) {
+              umma_commit(&acc_full[buf]);
+              ++u;
+            }
           }
-          if (!ok) break;
-          umma_commit(&acc_full[buf]);
         }
         // Wait until every MMA this thread issued has completed (TMEM and the
         // stages are released only after that).
@@ -301,11 +327,12 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         volatile int no_abort = 0;
         mbar_wait(drain, 0, &no_abort, args.err, 6);
       }
-    } else {
-      // ---------------- epilogue (warps 2..5) ----------------
+    } else if (EPI == EPI_ROWDOT) {
+      // ---------------- epilogue (warps 2..5): row dot products ----------------
       const int quarter = warp & 3;  // TMEM lane quarter this warp may access
       const int row = quarter * 32 + lane;
       const int m = m0 + row;
+      const double unscale = 1.0 / ((double)args.scaleA[0] * (double)args.scaleB[w]);
       double rowsum = 0.0;
       int t = 0;
       for (int nt = nt_begin; nt < nt_end; ++nt, ++t) {
@@ -318,35 +345,17 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         for (int c = 0; c < BN; c += 16) {
           float v[16];
           tmem_ld16(taddr + c, v);
-          if (EPI == EPI_ROWDOT) {
-            if (m < args.M) {
-              const float* xr = args.X + (size_t)m * args.ldx + n0 + c;
-              if (n0 + c + 16 <= args.N) {
+          if (m < args.M) {
+            const float* xr = args.X + (size_t)m * args.ldx + n0 + c;
+            if (n0 + c + 16 <= args.N) {
 #pragma unroll
-                for (int q = 0; q < 16; q += 4) {
-                  const float4 xx = *reinterpret_cast<const float4*>(xr + q);
-                  rowsum += (double)v[q] * xx.x + (double)v[q + 1] * xx.y + (double)v[q + 2] * xx.z +
-                            (double)v[q + 3] * xx.w;
-                }
-              } else {
-                for (int q = 0; q < 16 && n0 + c + q < args.N; ++q) rowsum += (double)v[q] * xr[q];
+              for (int q = 0; q < 16; q += 4) {
+                const float4 xx = *reinterpret_cast<const float4*>(xr + q);
+                rowsum += (double)v[q] * xx.x + (double)v[q + 1] * xx.y + (double)v[q + 2] * xx.z +
+                          (double)v[q + 3] * xx.w;
               }
-            }
-          } else {
-            if (m < args.M) {
-              double* orow = args.out + (size_t)w * args.out_stride + (size_t)m * args.ldo;
-#pragma unroll
-              for (int q = 0; q < 16; ++q) {
-                const int n = n0 + c + q;
-                // Lower-triangular mode writes the lower triangle and mirrors it,
-                // so the stored matrix is exactly symmetric.
-                if (n < args.N && !(args.lower_tiles && n > m)) {
-                  const double val = (double)v[q] + (m == n ? 1.0 : 0.0);
-                  orow[n] = val;
-                  if (args.lower_tiles && n != m)
-                    args.out[(size_t)w * args.out_stride + (size_t)n * args.ldo + m] = val;
-                }
-              }
+            } else {
+              for (int q = 0; q < 16 && n0 + c + q < args.N; ++q) rowsum += (double)v[q] * xr[q];
             }
           }
         }
@@ -354,8 +363,51 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         __syncwarp();
         if (lane == 0) mbar_arrive(&acc_empty[buf]);
       }
-      if (EPI == EPI_ROWDOT && m < args.M && t == nt_end - nt_begin)
-        args.out[(size_t)w * args.ldo + m] = rowsum;
+      if (m < args.M && t == nt_end - nt_begin) args.out[(size_t)w * args.ldo + m] = rowsum * unscale;
+    } else {
+      // ---------------- epilogue (warps 2..9): FP64 sum of k-block partials ----------------
+      const int quarter = warp & 3;
+      const int half = (warp - 2) >> 2;  // columns [64 half, 64 half + 64) of the tile
+      const int m = m0 + quarter * 32 + lane;
+      const double unscale = 1.0 / ((double)args.scaleA[0] * (double)args.scaleB[w]);
+      double acc[64];
+#pragma unroll
+      for (int c = 0; c < 64; ++c) acc[c] = 0.0;
+      bool ok = true;
+      for (int u = 0; u < k_blocks; ++u) {
+        const int buf = u & 1;
+        if (!mbar_wait(&acc_full[buf], (u / 2) & 1, abort_flag, args.err, 4)) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t taddr = tmem_base + ((uint32_t)(quarter * 32) << 16) + buf * BN + 64 * half;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          float v[16];
+          tmem_ld16(taddr + 16 * j, v);
+#pragma unroll
+          for (int q = 0; q < 16; ++q) acc[16 * j + q] += (double)v[q];
+        }
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&acc_empty[buf]);
+      }
+      if (ok && m < args.M) {
+        const int n0 = nt_begin * BN + 64 * half;
+        double* orow = args.out + (size_t)w * args.out_stride + (size_t)m * args.ldo;
+#pragma unroll
+        for (int c = 0; c < 64; ++c) {
+          const int n = n0 + c;
+          // Lower-triangular mode writes the lower triangle and mirrors it,
+          // so the stored matrix is exactly symmetric.
+          if (n < args.N && !(args.lower_tiles && n > m)) {
+            const double val = acc[c] * unscale + (m == n ? 1.0 : 0.0);
+            orow[n] = val;
+            if (args.lower_tiles && n != m) args.out[(size_t)w * args.out_stride + (size_t)n * args.ldo + m] = val;
+          }
+        }
+      }
     }
   }
   // Teardown: every warp reaches this point (all waits are bounded).
@@ -387,7 +439,8 @@ static EncodeTiledFn encode_fn() {
 }
 
 // bf16 matrix [batch][rows][ld] (K contiguous, K valid = cols) with box {64, box_rows, 1}.
-static CUtensorMap make_map(const void* base, int cols, int rows, int ld, int batch, int box_rows, int rank) {
+static CUtensorMap make_map(const void* base, int cols, int rows, int ld, int batch, int box_rows, int rank,
+                            int fp16) {
   QX_REQUIRE((reinterpret_cast<uintptr_t>(base) & 15) == 0 && (ld * 2) % 16 == 0, QX_ERR_INVALID_INPUT,
              "tensor map base/stride not 16-byte aligned");
   CUtensorMap m;
@@ -395,7 +448,7 @@ static CUtensorMap make_map(const void* base, int cols, int rows, int ld, int ba
   cuuint64_t strides[2] = {(cuuint64_t)ld * 2, (cuuint64_t)ld * 2 * rows};
   cuuint32_t box[3] = {(cuuint32_t)TC_BK, (cuuint32_t)box_rows, 1};
   cuuint32_t estr[3] = {1, 1, 1};
-  CUresult r = encode_fn()(&m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, rank, const_cast<void*>(base), dims, strides, box,
+  CUresult r = encode_fn()(&m, fp16 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, rank, const_cast<void*>(base), dims, strides, box,
                            estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
                            CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   QX_REQUIRE(r == CUDA_SUCCESS, QX_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
@@ -408,44 +461,108 @@ bool tc_supported(qx_ctx* ctx) {
   return p.major == 10;
 }
 
-// Split: hi = bf16(s x), lo = bf16(s x - hi), s = scale[batch][col] (or 1).
-__global__ void k_split_bf16(const double* __restrict__ src, int rows, int cols, int ld_src, size_t src_stride,
-                             __nv_bfloat16* __restrict__ hi, __nv_bfloat16* __restrict__ lo, int ld_dst,
-                             size_t dst_stride, const double* __restrict__ scale, int ld_scale) {
+// max|x| per batch (x >= 0 compares as its bit pattern).
+__global__ void k_amax(const double* __restrict__ src, int rows, int cols, int ld, size_t stride,
+                       unsigned long long* __restrict__ out) {
   const int b = blockIdx.y;
+  double m = 0.0;
+  const size_t total = (size_t)rows * cols;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+    const int r = (int)(i / cols), c = (int)(i % cols);
+    m = fmax(m, fabs(src[(size_t)b * stride + (size_t)r * ld + c]));
+  }
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(out + b, __double_as_longlong(m));
+}
+
+// Split s*x*c into hi/lo (bf16 or fp16).  c = colscale[b][col] (or 1); s is a
+// power of two from the bound amax_src * amax_col (fp16 only, else 1) and is
+// written to scale_out[b].
+__global__ void k_split(const double* __restrict__ src, int rows, int cols, int ld_src, size_t src_stride,
+                        const double* __restrict__ colscale, int ld_cs, void* __restrict__ hi_, void* __restrict__ lo_,
+                        int ld_dst, size_t dst_stride, int fp16, const unsigned long long* __restrict__ amax_src,
+                        const unsigned long long* __restrict__ amax_col, float* __restrict__ scale_out) {
+  const int b = blockIdx.y;
+  float s = 1.0f;
+  if (fp16) {
+    double bound = __longlong_as_double(amax_src[src_stride ? b : 0]);
+    if (amax_col) bound *= __longlong_as_double(amax_col[b]);
+    if (bound > 0.0 && isfinite(bound)) s = exp2f(floorf(log2f((float)(32768.0 / bound))));
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0 && scale_out) scale_out[b] = s;
   const size_t total = (size_t)rows * ld_dst;
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
     const int r = (int)(i / ld_dst), c = (int)(i % ld_dst);
     double x = 0.0;
     if (c < cols) {
       x = src[(size_t)b * src_stride + (size_t)r * ld_src + c];
-      if (scale) x *= scale[(size_t)b * ld_scale + c];
+      if (colscale) x *= colscale[(size_t)b * ld_cs + c];
     }
-    const __nv_bfloat16 h = __float2bfloat16_rn((float)x);
-    const double rem = x - (double)__bfloat162float(h);
-    hi[(size_t)b * dst_stride + i] = h;
-    lo[(size_t)b * dst_stride + i] = __float2bfloat16_rn((float)rem);
+    x *= (double)s;
+    if (fp16) {
+      const __half h = __float2half_rn((float)x);
+      const double rem = x - (double)__half2float(h);
+      reinterpret_cast<__half*>(hi_)[(size_t)b * dst_stride + i] = h;
+      reinterpret_cast<__half*>(lo_)[(size_t)b * dst_stride + i] = __float2half_rn((float)rem);
+    } else {
+      const __nv_bfloat16 h = __float2bfloat16_rn((float)x);
+      const double rem = x - (double)__bfloat162float(h);
+      reinterpret_cast<__nv_bfloat16*>(hi_)[(size_t)b * dst_stride + i] = h;
+      reinterpret_cast<__nv_bfloat16*>(lo_)[(size_t)b * dst_stride + i] = __float2bfloat16_rn((float)rem);
+    }
   }
 }
 
+// Scratch for the amax words and scales: [0, 1024) amax of sources, [1024, 2048)
+// amax of column scales, then float scales.
+struct SplitScratch {
+  unsigned long long* amax_src;
+  unsigned long long* amax_col;
+  float* scale;
+};
+static SplitScratch split_scratch(qx_ctx* ctx, int slot_offset) {
+  DevBuf& b = ctx->ws[WS_TCERR];
+  b.reserve(64 * 1024);
+  uint8_t* p = b.as<uint8_t>() + 256 + slot_offset * 20480;
+  SplitScratch s;
+  s.amax_src = reinterpret_cast<unsigned long long*>(p);
+  s.amax_col = s.amax_src + 1024;
+  s.scale = reinterpret_cast<float*>(s.amax_col + 1024);
+  return s;
+}
+
 static void split(qx_ctx* ctx, const double* src, int rows, int cols, int ld_src, size_t src_stride, void* hi,
-                  void* lo, int ld_dst, size_t dst_stride, int batch, const double* scale, int ld_scale) {
+                  void* lo, int ld_dst, size_t dst_stride, int batch, const double* colscale, int ld_cs, int fp16,
+                  int slot, float** scale_out) {
+  QX_REQUIRE(batch <= 1024, QX_ERR_INVALID_INPUT, "at most 1024 frequencies per split");
+  SplitScratch sc = split_scratch(ctx, slot);
+  if (fp16) {
+    const int nsrc = src_stride ? batch : 1;
+    QX_CUDA(cudaMemsetAsync(sc.amax_src, 0, 2048 * sizeof(unsigned long long), ctx->stream));
+    const size_t tot = (size_t)rows * cols;
+    dim3 g1((unsigned)std::min<size_t>((tot + 255) / 256, 1024), nsrc);
+    k_amax<<<g1, 256, 0, ctx->stream>>>(src, rows, cols, ld_src, src_stride, sc.amax_src);
+    check_launch(ctx);
+    if (colscale) {
+      dim3 g2(ceil_div(cols, 256), batch);
+      k_amax<<<g2, 256, 0, ctx->stream>>>(colscale, 1, cols, ld_cs, ld_cs, sc.amax_col);
+      check_launch(ctx);
+    }
+  }
   const size_t total = (size_t)rows * ld_dst;
   dim3 grid((unsigned)std::min<size_t>((total + 255) / 256, 4096), batch);
-  k_split_bf16<<<grid, 256, 0, ctx->stream>>>(src, rows, cols, ld_src, src_stride,
-                                              reinterpret_cast<__nv_bfloat16*>(hi),
-                                              reinterpret_cast<__nv_bfloat16*>(lo), ld_dst, dst_stride, scale,
-                                              ld_scale);
+  k_split<<<grid, 256, 0, ctx->stream>>>(src, rows, cols, ld_src, src_stride, colscale, ld_cs, hi, lo, ld_dst,
+                                         dst_stride, fp16, sc.amax_src, colscale ? sc.amax_col : nullptr, sc.scale);
   check_launch(ctx);
+  if (scale_out) *scale_out = sc.scale;
 }
 
-void launch_split_bf16(qx_ctx* ctx, const double* src, int rows, int cols, int ld_src, void* hi, void* lo,
-                       int ld_dst, size_t src_stride, size_t dst_stride, int batch) {
-  split(ctx, src, rows, cols, ld_src, src_stride, hi, lo, ld_dst, dst_stride, batch, nullptr, 0);
+void launch_split(qx_ctx* ctx, const double* src, int rows, int cols, int ld_src, void* hi, void* lo, int ld_dst,
+                  size_t src_stride, size_t dst_stride, int batch, int fp16, int slot, float** scale_out) {
+  split(ctx, src, rows, cols, ld_src, src_stride, hi, lo, ld_dst, dst_stride, batch, nullptr, 0, fp16, slot,
+        scale_out);
 }
 
-// Error words: one per tcgen05 GEMM kind, so both launches of an iteration
-// can be checked after a single synchronisation.
 static int* tc_err_slot(qx_ctx* ctx, int which) {
   DevBuf& b = ctx->ws[WS_TCERR];
   b.reserve(256);
@@ -463,20 +580,19 @@ static void launch_tc(qx_ctx* ctx, const CUtensorMap& ah, const CUtensorMap& al,
     QX_CUDA(cudaFuncSetAttribute(k_tc_gemm<BN, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, L::TOTAL));
     attr = true;
   }
-  k_tc_gemm<BN, EPI><<<grid, TC_THREADS, L::TOTAL, ctx->stream>>>(ah, al, bh, bl, a);
+  k_tc_gemm<BN, EPI><<<grid, TcWarps<EPI>::THREADS, L::TOTAL, ctx->stream>>>(ah, al, bh, bl, a);
   check_launch(ctx);
 }
 
-// v[w][p] = sum_Q X[p][Q] sum_P (Bh+Bl)[p][P] (Wh+Wl)[w][Q][P]   (three products)
-void launch_pair_contract_bf16x3(qx_ctx* ctx, const void* bpt_hi, const void* bpt_lo, const float* bpt_f32, int ldk,
-                                 int npair, int naux, const void* wc_hi, const void* wc_lo, int ldw,
-                                 size_t wc_stride, int nw, double* v, int ldv) {
+// v[w][p] = sum_Q X[p][Q] sum_P (Bh+Bl)[p][P] (Wh+Wl)[w][Q][P] / (sA sB[w])   (three products)
+void launch_pair_contract_tc(qx_ctx* ctx, const TcOperand& A, const float* bpt_f32, int ldk, int npair, int naux,
+                             const TcOperand& W, int ldw, size_t wc_stride, int nw, double* v, int ldv, int fp16) {
   constexpr int BN = 256;
   QX_REQUIRE(wc_stride == (size_t)naux * ldw, QX_ERR_INVALID_INPUT, "Wc stride must be naux*ldw");
-  CUtensorMap ah = make_map(bpt_hi, naux, npair, ldk, 1, TC_BM, 2);
-  CUtensorMap al = make_map(bpt_lo, naux, npair, ldk, 1, TC_BM, 2);
-  CUtensorMap bh = make_map(wc_hi, naux, naux, ldw, nw, BN, 3);
-  CUtensorMap bl = make_map(wc_lo, naux, naux, ldw, nw, BN, 3);
+  CUtensorMap ah = make_map(A.hi, naux, npair, ldk, 1, TC_BM, 2, fp16);
+  CUtensorMap al = make_map(A.lo, naux, npair, ldk, 1, TC_BM, 2, fp16);
+  CUtensorMap bh = make_map(W.hi, naux, naux, ldw, nw, BN, 3, fp16);
+  CUtensorMap bl = make_map(W.lo, naux, naux, ldw, nw, BN, 3, fp16);
   int* d_err = tc_err_slot(ctx, 0);
   QX_CUDA(cudaMemsetAsync(d_err, 0, sizeof(int), ctx->stream));
   TcArgs a{};
@@ -490,6 +606,9 @@ void launch_pair_contract_bf16x3(qx_ctx* ctx, const void* bpt_hi, const void* bp
   a.ldx = ldk;
   a.out = v;
   a.ldo = ldv;
+  a.fp16 = fp16;
+  a.scaleA = A.scale;
+  a.scaleB = W.scale;
   a.err = d_err;
   const int groups = ceil_div(nw, a.wgroup);
   launch_tc<BN, EPI_ROWDOT>(ctx, ah, al, bh, bl, a, dim3(groups * a.m_blocks * a.wgroup));
@@ -497,8 +616,8 @@ void launch_pair_contract_bf16x3(qx_ctx* ctx, const void* bpt_hi, const void* bp
 }
 
 // eps[w] = I + Bov diag(chi[w]) Bov^T with A = split(Bov), B = split(Bov * chi[w]).
-void launch_eps_bf16x3(qx_ctx* ctx, const double* bov, int ldov, int naux, int nov, const double* chi, int nw,
-                       double* eps, int ldn, size_t eps_stride) {
+void launch_eps_tc(qx_ctx* ctx, const double* bov, int ldov, int naux, int nov, const double* chi, int nw,
+                   double* eps, int ldn, size_t eps_stride, int fp16) {
   constexpr int BN = 128;
   const size_t a_elems = (size_t)naux * ldov;
   DevBuf& buf = ctx->ws[WS_BOV_HI];
@@ -508,12 +627,13 @@ void launch_eps_bf16x3(qx_ctx* ctx, const double* bov, int ldov, int naux, int n
   void* a_lo = p + a_elems * 2;
   void* b_hi = p + a_elems * 4;
   void* b_lo = p + a_elems * 4 + a_elems * 2 * nw;
-  split(ctx, bov, naux, nov, ldov, 0, a_hi, a_lo, ldov, 0, 1, nullptr, 0);
-  split(ctx, bov, naux, nov, ldov, 0, b_hi, b_lo, ldov, a_elems, nw, chi, ldov);
-  CUtensorMap ah = make_map(a_hi, nov, naux, ldov, 1, TC_BM, 2);
-  CUtensorMap al = make_map(a_lo, nov, naux, ldov, 1, TC_BM, 2);
-  CUtensorMap bh = make_map(b_hi, nov, naux, ldov, nw, BN, 3);
-  CUtensorMap bl = make_map(b_lo, nov, naux, ldov, nw, BN, 3);
+  float *sa = nullptr, *sb = nullptr;
+  split(ctx, bov, naux, nov, ldov, 0, a_hi, a_lo, ldov, 0, 1, nullptr, 0, fp16, 0, &sa);
+  split(ctx, bov, naux, nov, ldov, 0, b_hi, b_lo, ldov, a_elems, nw, chi, ldov, fp16, 1, &sb);
+  CUtensorMap ah = make_map(a_hi, nov, naux, ldov, 1, TC_BM, 2, fp16);
+  CUtensorMap al = make_map(a_lo, nov, naux, ldov, 1, TC_BM, 2, fp16);
+  CUtensorMap bh = make_map(b_hi, nov, naux, ldov, nw, BN, 3, fp16);
+  CUtensorMap bl = make_map(b_lo, nov, naux, ldov, nw, BN, 3, fp16);
   int* d_err = tc_err_slot(ctx, 1);
   QX_CUDA(cudaMemsetAsync(d_err, 0, sizeof(int), ctx->stream));
   TcArgs a{};
@@ -526,6 +646,9 @@ void launch_eps_bf16x3(qx_ctx* ctx, const double* bov, int ldov, int naux, int n
   a.ldo = ldn;
   a.out_stride = eps_stride;
   a.lower_tiles = 1;
+  a.fp16 = fp16;
+  a.scaleA = sa;
+  a.scaleB = sb;
   a.err = d_err;
   const int tiles = ceil_div(naux, TC_BM);  // BM == BN for the symmetric product
   static_assert(BN == TC_BM, "eps tiles are square");

@@ -187,23 +187,25 @@ void gw_setup(qx_ctx* ctx, GWSystem& S, const double* d_lpq, int nmo, int nocc, 
   QX_CUDA(cudaMemcpyAsync(S.d_orbs, orbs.data(), orbs.size() * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
   launch_gather_pairs(ctx, d_lpq, naux, nmo, d_pairs, S.npair, S.bpt, S.ldk);
   launch_gather_ov(ctx, d_lpq, naux, nmo, nocc, S.bov, S.ldov);
-  if (precision == QX_PREC_BF16X3) {
-    QX_REQUIRE(tc_supported(ctx), QX_ERR_NO_DEVICE, "BF16X3 precision needs an sm_100 device");
+  if (is_tc_precision(precision)) {
+    QX_REQUIRE(tc_supported(ctx), QX_ERR_NO_DEVICE, "tensor-core precision needs an sm_100 device");
+    const int fp16 = precision == QX_PREC_FP16X3;
     const size_t nb = (size_t)S.npair * S.ldk;
     ctx->ws[WS_BPT_HI].reserve(nb * 2);
     ctx->ws[WS_BPT_LO].reserve(nb * 2);
     ctx->ws[WS_BPT_F32].reserve(nb * 4);
-    S.bpt_hi = ctx->ws[WS_BPT_HI].ptr;
-    S.bpt_lo = ctx->ws[WS_BPT_LO].ptr;
+    S.bpt_split.hi = ctx->ws[WS_BPT_HI].ptr;
+    S.bpt_split.lo = ctx->ws[WS_BPT_LO].ptr;
     S.bpt_f32 = ctx->ws[WS_BPT_F32].as<float>();
-    launch_split_bf16(ctx, S.bpt, S.npair, S.ldk, S.ldk, S.bpt_hi, S.bpt_lo, S.ldk, 0, 0, 1);
+    launch_split(ctx, S.bpt, S.npair, S.ldk, S.ldk, S.bpt_split.hi, S.bpt_split.lo, S.ldk, 0, 0, 1, fp16, 2,
+                 &S.bpt_split.scale);
     k_to_f32<<<1184, 256, 0, ctx->stream>>>(S.bpt, S.bpt_f32, nb);
     check_launch(ctx);
     const size_t nwc = (size_t)nw * S.eps_stride;
     ctx->ws[WS_WC_HI].reserve(nwc * 2);
     ctx->ws[WS_WC_LO].reserve(nwc * 2);
-    S.wc_hi = ctx->ws[WS_WC_HI].ptr;
-    S.wc_lo = ctx->ws[WS_WC_LO].ptr;
+    S.wc_split.hi = ctx->ws[WS_WC_HI].ptr;
+    S.wc_split.lo = ctx->ws[WS_WC_LO].ptr;
   }
 }
 
@@ -241,8 +243,9 @@ void gw_wc_pairs(qx_ctx* ctx, GWSystem& S, const double* e_host) {
   QX_CUDA(cudaMemcpyAsync(S.d_en, e_host, S.nmo * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
   record_stage(ctx, QX_ST_P0, true);
   launch_chi(ctx, S.d_en, S.nocc, S.nvir, S.d_freqs, S.nw, 0, S.chi, S.ldov);
-  if (S.precision == QX_PREC_BF16X3)
-    launch_eps_bf16x3(ctx, S.bov, S.ldov, S.naux, S.nov, S.chi, S.nw, S.eps, S.ldn, S.eps_stride);
+  if (is_tc_precision(S.precision))
+    launch_eps_tc(ctx, S.bov, S.ldov, S.naux, S.nov, S.chi, S.nw, S.eps, S.ldn, S.eps_stride,
+                  S.precision == QX_PREC_FP16X3);
   else
     launch_eps_fp64(ctx, S.bov, S.ldov, S.naux, S.nov, S.chi, S.nw, S.eps, S.ldn, S.eps_stride);
   record_stage(ctx, QX_ST_P0, false);
@@ -250,10 +253,12 @@ void gw_wc_pairs(qx_ctx* ctx, GWSystem& S, const double* e_host) {
   launch_invert_wc(ctx, S.eps, S.naux, S.ldn, S.eps_stride, S.nw);
   record_stage(ctx, QX_ST_INV, false);
   record_stage(ctx, QX_ST_CONTRACT, true);
-  if (S.precision == QX_PREC_BF16X3) {
-    launch_split_bf16(ctx, S.eps, S.naux, S.naux, S.ldn, S.wc_hi, S.wc_lo, S.ldn, S.eps_stride, S.eps_stride, S.nw);
-    launch_pair_contract_bf16x3(ctx, S.bpt_hi, S.bpt_lo, S.bpt_f32, S.ldk, S.npair, S.naux, S.wc_hi, S.wc_lo, S.ldn,
-                                S.eps_stride, S.nw, S.v, S.npair);
+  if (is_tc_precision(S.precision)) {
+    const int fp16 = S.precision == QX_PREC_FP16X3;
+    launch_split(ctx, S.eps, S.naux, S.naux, S.ldn, S.wc_split.hi, S.wc_split.lo, S.ldn, S.eps_stride, S.eps_stride,
+                 S.nw, fp16, 0, &S.wc_split.scale);
+    launch_pair_contract_tc(ctx, S.bpt_split, S.bpt_f32, S.ldk, S.npair, S.naux, S.wc_split, S.ldn, S.eps_stride, S.nw,
+                            S.v, S.npair, fp16);
   } else {
     launch_pair_contract_fp64(ctx, S.bpt, S.ldk, S.npair, S.naux, S.eps, S.ldn, S.eps_stride, S.nw, S.v, S.npair);
   }
@@ -542,7 +547,8 @@ qx_status qx_get_rho_response(qx_ctx* ctx, int nfreq, const double* freqs, const
     ctx->ws[WS_EPS].reserve((size_t)nfreq * stride * sizeof(double));
     double* eps = ctx->ws[WS_EPS].as<double>();
     launch_chi(ctx, d_e, nocc, nvir, d_f, nfreq, 0, chi, ldov);
-    if (precision == QX_PREC_BF16X3) launch_eps_bf16x3(ctx, bov, ldov, naux, nov, chi, nfreq, eps, ldn, stride);
+    if (is_tc_precision(precision))
+      launch_eps_tc(ctx, bov, ldov, naux, nov, chi, nfreq, eps, ldn, stride, precision == QX_PREC_FP16X3);
     else launch_eps_fp64(ctx, bov, ldov, naux, nov, chi, nfreq, eps, ldn, stride);
     // Pi = I - eps.
     std::vector<double> h((size_t)nfreq * stride);

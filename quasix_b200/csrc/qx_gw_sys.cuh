@@ -25,7 +25,7 @@ struct GWSystem {
   size_t eps_stride;
   std::vector<int> orbs;
   SigmaGrid grid;
-  void *bpt_hi = nullptr, *bpt_lo = nullptr, *wc_hi = nullptr, *wc_lo = nullptr;
+  TcOperand bpt_split{}, wc_split{};
   float* bpt_f32 = nullptr;
 };
 

@@ -211,14 +211,22 @@ struct QPParams {
 };
 void launch_pade_qp(qx_ctx* ctx, const QPParams& p);
 
-// Mixed-precision (tcgen05) forms.
-void launch_split_bf16(qx_ctx* ctx, const double* src, int rows, int cols, int ld_src, void* hi, void* lo,
-                       int ld_dst, size_t src_stride, size_t dst_stride, int batch);
-void launch_eps_bf16x3(qx_ctx* ctx, const double* bov, int ldov, int naux, int nov, const double* chi, int nw,
-                       double* eps, int ldn, size_t eps_stride);
-void launch_pair_contract_bf16x3(qx_ctx* ctx, const void* bpt_hi, const void* bpt_lo, const float* bpt_f32,
-                                 int ldk, int npair, int naux, const void* wc_hi, const void* wc_lo, int ldw,
-                                 size_t wc_stride, int nw, double* v, int ldv);
+// Mixed-precision (tcgen05) forms.  An operand is a hi/lo pair of bf16 or
+// fp16 arrays plus the device scales (powers of two, one per batch) applied
+// before the split.
+struct TcOperand {
+  void* hi;
+  void* lo;
+  float* scale;
+};
+inline bool is_tc_precision(int p) { return p == QX_PREC_BF16X3 || p == QX_PREC_FP16X3; }
+// slot selects one of the scratch areas for the scales (0..2).
+void launch_split(qx_ctx* ctx, const double* src, int rows, int cols, int ld_src, void* hi, void* lo, int ld_dst,
+                  size_t src_stride, size_t dst_stride, int batch, int fp16, int slot, float** scale_out);
+void launch_eps_tc(qx_ctx* ctx, const double* bov, int ldov, int naux, int nov, const double* chi, int nw,
+                   double* eps, int ldn, size_t eps_stride, int fp16);
+void launch_pair_contract_tc(qx_ctx* ctx, const TcOperand& A, const float* bpt_f32, int ldk, int npair, int naux,
+                             const TcOperand& W, int ldw, size_t wc_stride, int nw, double* v, int ldv, int fp16);
 bool tc_supported(qx_ctx* ctx);
 
 
