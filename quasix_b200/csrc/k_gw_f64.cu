@@ -2,6 +2,7 @@
 // inversion to Wc = eps^-1 - I, pair gathers, exchange diagonal, the Sigma_c
 // pair contraction v = B_p^T Wc B_p, and the Sigma_c(iw) assembly.
 #include "gemm_f64.cuh"
+#include "qx_blas.cuh"
 #include "qx_internal.cuh"
 
 namespace qx {
@@ -106,51 +107,95 @@ void launch_eps_fp64(qx_ctx* ctx, const double* bov, int ldov, int naux, int nov
 constexpr int SWEEP_NB = 128;
 
 // The kb x kb diagonal block, padded with the identity to 128 x 128, is swept
-// element-wise in shared memory: thread t owns column j = t % 128 and rows
-// i = t / 128 + 4 k (k < 32), so a warp touches 32 consecutive doubles of a row.
+// in four sub-blocks of 32 (the block sweep applied recursively): warp 0 sweeps
+// the 32 x 32 sub-block element by element in registers (lane j holds column
+// j; pivot rows and columns travel by shuffles, so a pivot step costs no block
+// barrier), then the whole CTA applies the rank-32 update to the rest of the
+// 128 x 128 block through shared memory.
+__device__ __forceinline__ void sweep32_warp(double* S, int q0, int lane, bool& bad_any) {
+  // c[k] holds S[(p + k) % 32][lane] at pivot step p: the pivot row is always
+  // c[0] and the array rotates by one after each step, so every register index
+  // is a compile-time constant without unrolling the pivot loop.
+  double c[32];
+#pragma unroll
+  for (int i = 0; i < 32; ++i) c[i] = S[(q0 + i) * SWEEP_NB + q0 + lane];
+#pragma unroll 1
+  for (int p = 0; p < 32; ++p) {
+    const double d = __shfl_sync(0xffffffffu, c[0], p);
+    const bool bad = !(fabs(d) > 0.0) || !isfinite(d);
+    bad_any |= bad;
+    const double inv = bad ? 0.0 : 1.0 / d;
+    const double rj = c[0] * inv;  // S[p][lane] / d
+    const bool piv = (lane == p);
+#pragma unroll
+    for (int i = 1; i < 32; ++i) {
+      const double ci = __shfl_sync(0xffffffffu, c[i], p);  // S[p + i][p]
+      c[i] = piv ? ci * inv : c[i] - ci * rj;
+    }
+    c[0] = piv ? -inv : rj;
+    const double t = c[0];
+#pragma unroll
+    for (int i = 0; i < 31; ++i) c[i] = c[i + 1];
+    c[31] = t;
+  }
+#pragma unroll
+  for (int i = 0; i < 32; ++i) S[(q0 + i) * SWEEP_NB + q0 + lane] = c[i];
+}
+
 __global__ void __launch_bounds__(512) k_sweep_diag(const double* __restrict__ M, int ldn, size_t stride, int k0,
                                                     int kb, double* __restrict__ Dp, int* __restrict__ status) {
   static_assert(SWEEP_NB == 128, "thread mapping assumes 128 columns");
-  extern __shared__ double S[];  // [128][128]
-  __shared__ double rowp[SWEEP_NB], colp[SWEEP_NB];
+  constexpr int TLD = 33;                       // padded row stride of T
+  extern __shared__ double S[];                 // [128][128]
+  double* Tb = S + SWEEP_NB * SWEEP_NB;         // [128][33]
   const int w = blockIdx.x;
   const double* A = M + (size_t)w * stride;
-  const int j = threadIdx.x & 127, r0 = threadIdx.x >> 7;
-#pragma unroll 4
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int j = tid & 127, r0 = tid >> 7;
   for (int k = 0; k < 32; ++k) {
     const int i = r0 + 4 * k;
     S[i * SWEEP_NB + j] = (i < kb && j < kb) ? A[(size_t)(k0 + i) * ldn + k0 + j] : (i == j ? 1.0 : 0.0);
   }
-  __syncthreads();
   bool bad_any = false;
-  for (int p = 0; p < kb; ++p) {
-    if (threadIdx.x < SWEEP_NB) {
-      rowp[threadIdx.x] = S[p * SWEEP_NB + threadIdx.x];
-      colp[threadIdx.x] = S[threadIdx.x * SWEEP_NB + p];
-    }
+  for (int sb = 0; sb < 4; ++sb) {
+    const int q0 = 32 * sb;
     __syncthreads();
-    const double d = rowp[p];
-    // eps is positive definite on the imaginary axis; when energies reorder it
-    // can turn indefinite, and the sweep then still inverts it with negative
-    // pivots (the reference falls back from Cholesky to LU there,
-    // correlation_ac.rs:383-399).  Only a zero or non-finite pivot is singular.
-    const bool bad = !(fabs(d) > 0.0) || !isfinite(d);
-    bad_any |= bad;
-    const double inv = bad ? 0.0 : 1.0 / d;
-    const double rj = rowp[j] * inv;
+    if (warp == 0) sweep32_warp(S, q0, lane, bad_any);
+    __syncthreads();
+    // T[r][q] = S[r][Q] D1 = -S[r][Q] Sswept[Q][q] for rows outside Q.
+    {
+      const int q = tid & 31, rg = tid >> 5;  // 16 row groups
+      for (int r = rg; r < SWEEP_NB; r += 16) {
+        if (r >= q0 && r < q0 + 32) continue;
+        double t = 0.0;
 #pragma unroll 8
-    for (int k = 0; k < 32; ++k) {
-      const int i = r0 + 4 * k;
-      const double ci = colp[i];
-      double nv;
-      if (i == p) nv = (j == p) ? -inv : rj;
-      else if (j == p) nv = ci * inv;
-      else nv = S[i * SWEEP_NB + j] - ci * rj;
-      S[i * SWEEP_NB + j] = nv;
+        for (int p = 0; p < 32; ++p) t -= S[r * SWEEP_NB + q0 + p] * S[(q0 + p) * SWEEP_NB + q0 + q];
+        Tb[r * TLD + q] = t;
+      }
     }
     __syncthreads();
+    // S[r][c] -= T[r] . S[Q][c]  for r, c outside Q (old S[Q][c]).
+    for (int k = 0; k < 32; ++k) {
+      const int r = r0 + 4 * k;
+      if ((r >= q0 && r < q0 + 32) || (j >= q0 && j < q0 + 32)) continue;
+      double t = 0.0;
+#pragma unroll 8
+      for (int p = 0; p < 32; ++p) t += Tb[r * TLD + p] * S[(q0 + p) * SWEEP_NB + j];
+      S[r * SWEEP_NB + j] -= t;
+    }
+    __syncthreads();
+    // S[r][Q] = T[r] (lanes along q) and S[Q][r] = T[r]^T (lanes along r).
+    for (int idx = tid; idx < SWEEP_NB * 32; idx += blockDim.x) {
+      const int r = idx >> 5, q = idx & 31;
+      if (!(r >= q0 && r < q0 + 32)) S[r * SWEEP_NB + q0 + q] = Tb[r * TLD + q];
+    }
+    for (int idx = tid; idx < SWEEP_NB * 32; idx += blockDim.x) {
+      const int q = idx >> 7, r = idx & 127;
+      if (!(r >= q0 && r < q0 + 32)) S[(q0 + q) * SWEEP_NB + r] = Tb[r * TLD + q];
+    }
   }
-  if (bad_any && threadIdx.x == 0) atomicExch(status + w, 1);
+  __syncthreads();
+  if (lane == 0 && warp == 0 && bad_any) atomicExch(status + w, 1);
   // D = -S, zero outside the kb x kb block.
   double* D = Dp + (size_t)w * SWEEP_NB * SWEEP_NB;
   for (int k = 0; k < 32; ++k) {
@@ -246,19 +291,24 @@ __global__ void k_sweep_write(double* __restrict__ M, int n, int ldn, size_t str
 }
 
 // After the last sweep M = -eps^-1; Wc = eps^-1 - I = -M - I.  A frequency
-// whose eps was singular gets Wc = 0 (eps^-1 replaced by the identity).
-__global__ void k_finish_wc(double* __restrict__ M, int n, int ldn, size_t stride, const int* __restrict__ status) {
+// whose eps was singular gets Wc = 0 (eps^-1 replaced by the identity).  With
+// half_lower the output is W' = strict lower triangle of Wc + diag(Wc) / 2 and
+// zeros above, so that b^T Wc b = 2 b^T W' b needs only the lower triangle.
+__global__ void k_finish_wc(double* __restrict__ M, int n, int ldn, size_t stride, const int* __restrict__ status,
+                            int half_lower) {
   const int w = blockIdx.y;
   double* A = M + (size_t)w * stride;
   const bool singular = status[w] != 0;
   for (size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x; idx < (size_t)n * n;
        idx += (size_t)gridDim.x * blockDim.x) {
     int r = (int)(idx / n), c = (int)(idx % n);
-    A[(size_t)r * ldn + c] = singular ? 0.0 : -A[(size_t)r * ldn + c] - (r == c ? 1.0 : 0.0);
+    double v = singular ? 0.0 : -A[(size_t)r * ldn + c] - (r == c ? 1.0 : 0.0);
+    if (half_lower) v = (c < r) ? v : (c == r ? 0.5 * v : 0.0);
+    A[(size_t)r * ldn + c] = v;
   }
 }
 
-void launch_invert_wc(qx_ctx* ctx, double* eps, int n, int ldn, size_t stride, int nw) {
+void launch_invert_wc(qx_ctx* ctx, double* eps, int n, int ldn, size_t stride, int nw, int half_lower) {
   const size_t pstride = (size_t)n * SWEEP_NB;
   DevBuf& pan = ctx->ws[WS_PANEL];
   const size_t need = (pstride * nw + (size_t)nw * SWEEP_NB * SWEEP_NB) * sizeof(double) + nw * sizeof(int) + 256;
@@ -267,7 +317,7 @@ void launch_invert_wc(qx_ctx* ctx, double* eps, int n, int ldn, size_t stride, i
   double* Dp = Tp + pstride * nw;
   int* status = reinterpret_cast<int*>(Dp + (size_t)nw * SWEEP_NB * SWEEP_NB);
   QX_CUDA(cudaMemsetAsync(status, 0, nw * sizeof(int), ctx->stream));
-  const int diag_smem = SWEEP_NB * SWEEP_NB * sizeof(double);
+  const int diag_smem = (SWEEP_NB * SWEEP_NB + SWEEP_NB * 33) * sizeof(double);
   static bool attr = false;
   if (!attr) {
     QX_CUDA(cudaFuncSetAttribute(k_sweep_diag, cudaFuncAttributeMaxDynamicSharedMemorySize, diag_smem));
@@ -295,7 +345,7 @@ void launch_invert_wc(qx_ctx* ctx, double* eps, int n, int ldn, size_t stride, i
     check_launch(ctx);
   }
   dim3 fg(ceil_div(n * n, 256 * 4), nw);
-  k_finish_wc<<<fg, 256, 0, ctx->stream>>>(eps, n, ldn, stride, status);
+  k_finish_wc<<<fg, 256, 0, ctx->stream>>>(eps, n, ldn, stride, status, half_lower);
   check_launch(ctx);
   ctx->pending.push_back({status, nw, 1});
 }
@@ -378,7 +428,8 @@ void launch_exchange_diag(qx_ctx* ctx, const double* lpq, int naux, int nmo, int
 }
 
 // ---------------------------------------------------------------------------
-// Pair contraction: v[w][p] = sum_Q Bpt[p][Q] sum_P Wc[w][Q][P] Bpt[p][P].
+// Pair contraction: v[w][p] = 2 sum_Q Bpt[p][Q] sum_{P <= Q} W'[w][Q][P] Bpt[p][P]
+// with W' the half-lower form of Wc (k_finish_wc), i.e. Bpt[p]^T Wc[w] Bpt[p].
 // One CTA per (128-pair block, frequency); it walks every Q tile, so the
 // per-pair sums stay in shared memory and are written once (deterministic).
 // ---------------------------------------------------------------------------
@@ -406,7 +457,9 @@ __global__ void __launch_bounds__(PairTile::THREADS) k_pair_contract_f64(const d
     for (int i = 0; i < T::MI; ++i)
 #pragma unroll
       for (int j = 0; j < T::NJ; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
-    f64_mainloop<T>(acc, smem, Arow, ldk, npair - m0, Wc + (size_t)n0 * ldn, ldn, naux - n0, nullptr, naux);
+    // W' is lower triangular: rows Q of this tile need P <= Q < n0 + BN only.
+    f64_mainloop<T>(acc, smem, Arow, ldk, npair - m0, Wc + (size_t)n0 * ldn, ldn, naux - n0, nullptr,
+                    min(naux, n0 + T::BN));
     // Row partials: sum_n acc[m][n] * Bpt[m0+m][n0+n].
 #pragma unroll
     for (int i = 0; i < T::MI; ++i) {
@@ -439,7 +492,7 @@ __global__ void __launch_bounds__(PairTile::THREADS) k_pair_contract_f64(const d
     __syncthreads();
   }
   for (int r = threadIdx.x; r < T::BM; r += T::THREADS)
-    if (m0 + r < npair) v[(size_t)w * ldv + m0 + r] = rowacc[r];
+    if (m0 + r < npair) v[(size_t)w * ldv + m0 + r] = 2.0 * rowacc[r];
 }
 
 void launch_pair_contract_fp64(qx_ctx* ctx, const double* bpt, int ldk, int npair, int naux, const double* wc,
@@ -458,61 +511,94 @@ void launch_pair_contract_fp64(qx_ctx* ctx, const double* bpt, int ldk, int npai
 // ---------------------------------------------------------------------------
 // Sigma_c(iw_k) = -(1/pi) sum_w sum_m v[w][pair(t,m)] wts_w emo/(emo^2 + f_w^2),
 // emo = s i iw_k + ef - e_m, s = -1 for occupied targets, +1 for virtual
-// (correlation_ac.rs:286-314, 404-438).  One CTA per target; each warp takes
-// one k at a time, lanes stride over m, the frequency loop is outermost.
+// (correlation_ac.rs:286-314, 404-438).  The Green's-function factors depend
+// only on (s, k, w, m), so they are tabulated once per call as
+// G[(s, k, re/im)][(w, m)] and the sum becomes one DGEMM
+//   C[t][(s, k, c)] = sum_{(w,m)} V[t][(w,m)] G[(s, k, c)][(w,m)],
+// with V[t][(w,m)] = v[w][pair(t,m)] gathered first.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_sigma_assemble(const double* __restrict__ v, int ldv, int nw,
-                                                        const int* __restrict__ pair_index, int nmo,
-                                                        const int* __restrict__ orbs, int nocc,
-                                                        const double* __restrict__ en, double ef,
-                                                        const double* __restrict__ freqs,
-                                                        const double* __restrict__ wts,
-                                                        const double* __restrict__ iw, int nws,
-                                                        double* __restrict__ sigma) {
-  const int t = blockIdx.x;
-  const int n = orbs[t];
-  const double s = (n < nocc) ? -1.0 : 1.0;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
-  const int* pidx = pair_index + (size_t)t * nmo;
-  for (int k = warp; k < nws; k += nwarp) {
-    const double b = s * iw[k];
-    double re = 0.0, im = 0.0;
-    for (int w = 0; w < nw; ++w) {
-      const double f2 = freqs[w] * freqs[w];
-      const double wt = wts[w];
-      double sre = 0.0, sim = 0.0;
-      for (int m = lane; m < nmo; m += 32) {
-        const double a = ef - en[m];
-        // emo = a + ib ; den = emo^2 + f^2 = (a^2 - b^2 + f^2) + i 2ab
-        const double dr = a * a - b * b + f2, di = 2.0 * a * b;
-        const double dd = dr * dr + di * di;
-        const double gr = wt * (a * dr + b * di) / dd;
-        const double gi = wt * (b * dr - a * di) / dd;
-        const double vv = v[(size_t)w * ldv + pidx[m]];
-        sre += vv * gr;
-        sim += vv * gi;
-      }
-      re += sre;
-      im += sim;
+__global__ void k_sigma_gtab(const double* __restrict__ en, double ef, const double* __restrict__ freqs,
+                             const double* __restrict__ wts, const double* __restrict__ iw, int nw, int nmo, int nws,
+                             double* __restrict__ G, int ldg) {
+  const int row = blockIdx.y;  // (s, k, c): s in {occ, vir}
+  const int c = row & 1, k = (row >> 1) % nws, sidx = (row >> 1) / nws;
+  const double b = (sidx == 0 ? -1.0 : 1.0) * iw[k];
+  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < ldg; idx += gridDim.x * blockDim.x) {
+    double val = 0.0;
+    if (idx < nw * nmo) {
+      const int w = idx / nmo, m = idx % nmo;
+      const double a = ef - en[m], f2 = freqs[w] * freqs[w], wt = wts[w];
+      // emo = a + ib ; den = emo^2 + f^2 = (a^2 - b^2 + f^2) + i 2ab
+      const double dr = a * a - b * b + f2, di = 2.0 * a * b;
+      const double dd = dr * dr + di * di;
+      val = (c == 0) ? wt * (a * dr + b * di) / dd : wt * (b * dr - a * di) / dd;
     }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      re += __shfl_xor_sync(0xffffffffu, re, o);
-      im += __shfl_xor_sync(0xffffffffu, im, o);
-    }
-    if (lane == 0) {
-      sigma[((size_t)t * nws + k) * 2 + 0] = -re / M_PI;
-      sigma[((size_t)t * nws + k) * 2 + 1] = -im / M_PI;
-    }
+    G[(size_t)row * ldg + idx] = val;
   }
+}
+
+__global__ void k_sigma_gather(const double* __restrict__ v, int ldv, int nw, const int* __restrict__ pidx, int nmo,
+                               double* __restrict__ V, int ldg) {
+  const int t = blockIdx.y;
+  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < ldg; idx += gridDim.x * blockDim.x) {
+    double val = 0.0;
+    if (idx < nw * nmo) {
+      const int w = idx / nmo, m = idx % nmo;
+      val = v[(size_t)w * ldv + pidx[(size_t)t * nmo + m]];
+    }
+    V[(size_t)t * ldg + idx] = val;
+  }
+}
+
+__global__ void k_sigma_pick(const double* __restrict__ C, int ldc, const int* __restrict__ orbs, int nocc, int norbs,
+                             int nws, double* __restrict__ sigma) {
+  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < norbs * nws; idx += gridDim.x * blockDim.x) {
+    const int t = idx / nws, k = idx % nws;
+    const int sidx = orbs[t] < nocc ? 0 : 1;
+    const double* c = C + (size_t)t * ldc + 2 * (sidx * nws + k);
+    sigma[2 * (size_t)idx] = -c[0] / M_PI;
+    sigma[2 * (size_t)idx + 1] = -c[1] / M_PI;
+  }
+}
+
+size_t sigma_workspace_doubles(int norbs, int nws, int nw, int nmo) {
+  const size_t ldg = round_up(nw * nmo, 8), ng = 4 * (size_t)nws;
+  return round_up(norbs * nws * 2, 8) + ng * ldg + (size_t)norbs * ldg + (size_t)norbs * ng + 16;
 }
 
 void launch_sigma_assemble(qx_ctx* ctx, const double* v, int ldv, int nw, const int* pair_index, int norbs,
                            int nmo, const int* orbs, int nocc, const double* energies, double ef,
                            const double* freqs, const double* wts, const double* iw, int nws,
                            double* sigma) {
-  k_sigma_assemble<<<norbs, 256, 0, ctx->stream>>>(v, ldv, nw, pair_index, nmo, orbs, nocc, energies, ef, freqs, wts,
-                                                   iw, nws, sigma);
+  const int K = nw * nmo, ldg = round_up(K, 8), ng = 4 * nws;
+  DevBuf& sb = ctx->ws[WS_SIGMA];
+  const size_t out = (size_t)norbs * nws * 2;
+  QX_REQUIRE(sigma == sb.as<double>() && sb.bytes >= sigma_workspace_doubles(norbs, nws, nw, nmo) * sizeof(double),
+             QX_ERR_INVALID_INPUT, "sigma must live in the sized sigma workspace");
+  double* G = sb.as<double>() + round_up((int)out, 8);
+  double* V = G + (size_t)ng * ldg;
+  double* C = V + (size_t)norbs * ldg;
+  k_sigma_gtab<<<dim3(std::min(ceil_div(ldg, 256), 1024), ng), 256, 0, ctx->stream>>>(energies, ef, freqs, wts, iw,
+                                                                                      nw, nmo, nws, G, ldg);
+  check_launch(ctx);
+  k_sigma_gather<<<dim3(std::min(ceil_div(ldg, 256), 1024), norbs), 256, 0, ctx->stream>>>(v, ldv, nw, pair_index,
+                                                                                         nmo, V, ldg);
+  check_launch(ctx);
+  GemmNT g{};
+  g.M = norbs;
+  g.N = ng;
+  g.K = ldg;
+  g.A = V;
+  g.lda = ldg;
+  g.B = G;
+  g.ldb = ldg;
+  g.C = C;
+  g.ldc = ng;
+  g.batch = 1;
+  g.alpha = 1.0;
+  g.splitk = 0;
+  gemm_nt_f64(ctx, g);
+  k_sigma_pick<<<ceil_div(norbs * nws, 256), 256, 0, ctx->stream>>>(C, ng, orbs, nocc, norbs, nws, sigma);
   check_launch(ctx);
 }
 

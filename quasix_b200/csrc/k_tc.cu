@@ -166,6 +166,7 @@ struct TcArgs {
   size_t out_stride;
   int lower_tiles;      // STORE: enumerate lower-triangular (m, n) tile pairs and mirror
   int fp16;             // operand type: 0 bf16, 1 fp16
+  int tri;              // ROWDOT with lower-triangular B: N tile n0 needs K < n0 + BN, result x2
   const float* scaleA;  // [1]      scale applied to A before the split
   const float* scaleB;  // [nbatch] scale applied to B[w] before the split
   int* err;
@@ -250,7 +251,8 @@ __global__ void __launch_bounds__(TcWarps<EPI>::THREADS, 1)
         int issued = 0;
         for (int nt = nt_begin; nt < nt_end; ++nt) {
           const int n0 = nt * BN;
-          for (int kb = 0; kb < k_blocks; ++kb, ++g) {
+          const int kbe = args.tri ? min(k_blocks, (n0 + BN + TC_BK - 1) / TC_BK) : k_blocks;
+          for (int kb = 0; kb < kbe; ++kb, ++g) {
             const int s = g % TC_STAGES;
             if (g >= TC_STAGES) {
               if (!mbar_wait(&empty[s], ((g / TC_STAGES) - 1) & 1, abort_flag, args.err, 1)) goto producer_done;
@@ -286,9 +288,10 @@ __global__ void __launch_bounds__(TcWarps<EPI>::THREADS, 1)
         int g = 0, u = 0;
         bool ok = true;
         for (int nt = nt_begin; nt < nt_end && ok; ++nt) {
-          for (int kb = 0; kb < k_blocks; ++kb, ++g) {
+          const int kbe = args.tri ? min(k_blocks, (nt * BN + BN + TC_BK - 1) / TC_BK) : k_blocks;
+          for (int kb = 0; kb < kbe; ++kb, ++g) {
             const bool unit_start = (EPI == EPI_STORE) || kb == 0;
-            const bool unit_end = (EPI == EPI_STORE) || kb == k_blocks - 1;
+            const bool unit_end = (EPI == EPI_STORE) || kb == kbe - 1;
             const int buf = u & 1;
             if (unit_start && u >= 2) {
               if (!mbar_wait(&acc_empty[buf], ((u / 2) - 1) & 1, abort_flag, args.err, 2)) {
@@ -363,7 +366,8 @@ __global__ void __launch_bounds__(TcWarps<EPI>::THREADS, 1)
         __syncwarp();
         if (lane == 0) mbar_arrive(&acc_empty[buf]);
       }
-      if (m < args.M && t == nt_end - nt_begin) args.out[(size_t)w * args.ldo + m] = rowsum * unscale;
+      if (m < args.M && t == nt_end - nt_begin)
+        args.out[(size_t)w * args.ldo + m] = rowsum * unscale * (args.tri ? 2.0 : 1.0);
     } else {
       // ---------------- epilogue (warps 2..9): FP64 sum of k-block partials ----------------
       const int quarter = warp & 3;
@@ -584,7 +588,8 @@ static void launch_tc(qx_ctx* ctx, const CUtensorMap& ah, const CUtensorMap& al,
   check_launch(ctx);
 }
 
-// v[w][p] = sum_Q X[p][Q] sum_P (Bh+Bl)[p][P] (Wh+Wl)[w][Q][P] / (sA sB[w])   (three products)
+// v[w][p] = 2 sum_Q X[p][Q] sum_{P <= Q} (Bh+Bl)[p][P] (W'h+W'l)[w][Q][P] / (sA sB[w]),
+// W' the half-lower form of Wc (three products per term)
 void launch_pair_contract_tc(qx_ctx* ctx, const TcOperand& A, const float* bpt_f32, int ldk, int npair, int naux,
                              const TcOperand& W, int ldw, size_t wc_stride, int nw, double* v, int ldv, int fp16) {
   constexpr int BN = 256;
@@ -607,6 +612,7 @@ void launch_pair_contract_tc(qx_ctx* ctx, const TcOperand& A, const float* bpt_f
   a.out = v;
   a.ldo = ldv;
   a.fp16 = fp16;
+  a.tri = 1;
   a.scaleA = A.scale;
   a.scaleB = W.scale;
   a.err = d_err;

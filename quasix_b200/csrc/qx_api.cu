@@ -159,7 +159,7 @@ void gw_setup(qx_ctx* ctx, GWSystem& S, const double* d_lpq, int nmo, int nocc, 
   ctx->ws[WS_EPS].reserve((size_t)nw * S.eps_stride * sizeof(double));
   const int ldv = S.npair;
   ctx->ws[WS_VPAIR].reserve((size_t)nw * ldv * sizeof(double));
-  ctx->ws[WS_SIGMA].reserve((size_t)S.norbs * S.nws * 2 * sizeof(double));
+  ctx->ws[WS_SIGMA].reserve(sigma_workspace_doubles(S.norbs, S.nws, nw, nmo) * sizeof(double));
   size_t small = (3 * (size_t)nw + S.nws + nmo + 8) * sizeof(double) + (ps.index.size() + orbs.size()) * sizeof(int) +
                  ps.pairs.size() * sizeof(int2) + 1024;
   ctx->ws[WS_SMALL].reserve(small);
@@ -250,7 +250,7 @@ void gw_wc_pairs(qx_ctx* ctx, GWSystem& S, const double* e_host) {
     launch_eps_fp64(ctx, S.bov, S.ldov, S.naux, S.nov, S.chi, S.nw, S.eps, S.ldn, S.eps_stride);
   record_stage(ctx, QX_ST_P0, false);
   record_stage(ctx, QX_ST_INV, true);
-  launch_invert_wc(ctx, S.eps, S.naux, S.ldn, S.eps_stride, S.nw);
+  launch_invert_wc(ctx, S.eps, S.naux, S.ldn, S.eps_stride, S.nw, /*half_lower=*/1);
   record_stage(ctx, QX_ST_INV, false);
   record_stage(ctx, QX_ST_CONTRACT, true);
   if (is_tc_precision(S.precision)) {

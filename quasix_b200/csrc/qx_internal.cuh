@@ -166,9 +166,10 @@ void launch_eps_fp64(qx_ctx* ctx, const double* bov, int ldov, int naux, int nov
 
 // In-place inversion of nw SPD matrices by the block sweep operator;
 // output Wc = eps^-1 - I (FP64).
-void launch_invert_wc(qx_ctx* ctx, double* eps, int n, int ldn, size_t stride, int nw);
+// half_lower: return W' = strict-lower(Wc) + diag(Wc)/2 (zeros above) instead of Wc.
+void launch_invert_wc(qx_ctx* ctx, double* eps, int n, int ldn, size_t stride, int nw, int half_lower = 0);
 
-// v[w][p] = Bpt[p]^T Wc[w] Bpt[p] for all pairs (FP64).
+// v[w][p] = Bpt[p]^T Wc[w] Bpt[p] for all pairs (FP64), given W' (half-lower form).
 void launch_pair_contract_fp64(qx_ctx* ctx, const double* bpt, int ldk, int npair, int naux, const double* wc,
                                int ldn, size_t wc_stride, int nw, double* v, int ldv);
 
@@ -178,7 +179,9 @@ void launch_gather_pairs(qx_ctx* ctx, const double* lpq, int naux, int nmo, cons
 void launch_gather_ov(qx_ctx* ctx, const double* lpq, int naux, int nmo, int nocc, double* bov, int ldov);
 void launch_exchange_diag(qx_ctx* ctx, const double* lpq, int naux, int nmo, int nocc, double* sx);
 
-// Sigma_c(iw_k) assembly: sigma[t][k] (complex) for each target t.
+// Sigma_c(iw_k) assembly: sigma[t][k] (complex) for each target t.  sigma must
+// be the start of the WS_SIGMA slot sized by sigma_workspace_doubles.
+size_t sigma_workspace_doubles(int norbs, int nws, int nw, int nmo);
 void launch_sigma_assemble(qx_ctx* ctx, const double* v, int ldv, int nw, const int* pair_index, int norbs,
                            int nmo, const int* orbs, int nocc, const double* energies, double ef,
                            const double* freqs, const double* wts, const double* iw, int nws,
