@@ -80,6 +80,23 @@ qx_status qx_get_rho_response(qx_ctx* ctx, int nfreq, const double* freqs, const
  * pi, wc: [nfreq][naux][naux] (may alias). */
 qx_status qx_screened_interaction(qx_ctx* ctx, int nfreq, int naux, const double* pi, double* wc);
 
+/* qx_screened_interaction without any allocation.  No counterpart in the
+ * reference: it exists for callers that must not allocate device memory
+ * inside the call (e.g. a pre-sized serving process).  pi and wc must be
+ * device pointers of the context's device ([nfreq][naux][naux], may alias);
+ * all scratch lives in one file-scope device array of
+ * QX_NOALLOC_SCRATCH_BYTES, shared by every call on a device.  Limits:
+ * naux <= QX_NOALLOC_MAX_NAUX, nfreq <= QX_NOALLOC_MAX_NFREQ; larger sizes
+ * return QX_ERR_INVALID_INPUT.  The first call on each device resolves the
+ * scratch address and sets kernel attributes: make it before any stream
+ * capture.  Calls on one device that overlap in time (other threads, contexts
+ * or streams) race on the scratch and must be serialised by the caller.
+ * Synchronous: returns after wc is written. */
+#define QX_NOALLOC_SCRATCH_BYTES (32u << 20)
+#define QX_NOALLOC_MAX_NAUX 1024
+#define QX_NOALLOC_MAX_NFREQ 4096
+qx_status qx_screened_interaction_noalloc(qx_ctx* ctx, int nfreq, int naux, const double* pi, double* wc);
+
 /* ---- selfenergy ------------------------------------------------------------ */
 /* get_sigma_diag (correlation_ac.rs:241-449).  lpq: [naux][nmo][nmo] (symmetric
  * in the MO pair), orbs: [norbs].  Outputs sigma, omega: complex

@@ -74,6 +74,7 @@ SIGNATURES = {
     "qx_get_scaled_legendre_roots": (C.c_int, [C.c_int, C.c_double, _vp, _vp]),
     "qx_get_rho_response": (C.c_int, [_vp, C.c_int, _vp, _vp, _vp, C.c_int, C.c_int, C.c_int, C.c_int, _vp]),
     "qx_screened_interaction": (C.c_int, [_vp, C.c_int, C.c_int, _vp, _vp]),
+    "qx_screened_interaction_noalloc": (C.c_int, [_vp, C.c_int, C.c_int, _vp, _vp]),
     "qx_get_sigma_diag": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double,
                                     C.c_double, C.c_int, _vp, _vp, C.c_int, _ip]),
     "qx_ac_pade_thiele_diag": (C.c_int, [_vp, C.c_int, C.c_int, _vp, _vp, C.c_int, _vp, _vp, C.c_int, _ip]),

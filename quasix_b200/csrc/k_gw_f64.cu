@@ -350,6 +350,41 @@ void launch_invert_wc(qx_ctx* ctx, double* eps, int n, int ldn, size_t stride, i
   ctx->pending.push_back({status, nw, 1});
 }
 
+static_assert(kSweepPanelCols == SWEEP_NB, "panel width");
+
+void sweep_set_attributes() {
+  QX_CUDA(cudaFuncSetAttribute(k_sweep_diag, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)((SWEEP_NB * SWEEP_NB + SWEEP_NB * 33) * sizeof(double))));
+  QX_CUDA(cudaFuncSetAttribute(k_sweep_tpanel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PanelTile::SMEM));
+  QX_CUDA(cudaFuncSetAttribute(k_sweep_update, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SweepTile::SMEM));
+}
+
+void launch_invert_wc_panels(qx_ctx* ctx, double* eps, int n, int ldn, size_t stride, int nw, double* Tp,
+                             double* Dp, int* status) {
+  const size_t pstride = (size_t)n * SWEEP_NB;
+  const int diag_smem = (SWEEP_NB * SWEEP_NB + SWEEP_NB * 33) * sizeof(double);
+  const int tiles = ceil_div(n, SweepTile::BM);
+  for (int k0 = 0; k0 < n; k0 += SWEEP_NB) {
+    const int kb = min(SWEEP_NB, n - k0);
+    k_sweep_diag<<<nw, 512, diag_smem, ctx->stream>>>(eps, ldn, stride, k0, kb, Dp, status);
+    check_launch(ctx);
+    dim3 tg(ceil_div(n, PanelTile::BM), ceil_div(kb, PanelTile::BN), nw);
+    k_sweep_tpanel<<<tg, PanelTile::THREADS, PanelTile::SMEM, ctx->stream>>>(eps, n, ldn, stride, k0, kb, Dp, Tp,
+                                                                             pstride);
+    check_launch(ctx);
+    dim3 ug(tiles * (tiles + 1) / 2, nw);
+    k_sweep_update<<<ug, SweepTile::THREADS, SweepTile::SMEM, ctx->stream>>>(eps, n, ldn, stride, k0, kb, Tp,
+                                                                             pstride);
+    check_launch(ctx);
+    dim3 wg(ceil_div(n * kb, 256), nw);
+    k_sweep_write<<<wg, 256, 0, ctx->stream>>>(eps, n, ldn, stride, k0, kb, Tp, pstride, Dp);
+    check_launch(ctx);
+  }
+  dim3 fg(ceil_div(n * n, 256 * 4), nw);
+  k_finish_wc<<<fg, 256, 0, ctx->stream>>>(eps, n, ldn, stride, status, 0);
+  check_launch(ctx);
+}
+
 // ---------------------------------------------------------------------------
 // Gathers.
 // bpt[p][P] = lpq[P][pairs[p].x][pairs[p].y]   (tiled transpose through smem)
