@@ -168,6 +168,13 @@ qx_status qx_evgw(qx_ctx* ctx, const double* mo_energy, const double* lpq, const
                   int nocc, int naux, const qx_evgw_config* cfg, qx_evgw_result* res);
 
 /* ---- G0W0 by contour deformation -------------------------------------------- */
+/* QP solver of the CD entry points.  NEWTON: the step rule of
+ * NewtonQPSolver::solve (quasix_core/src/qp/newton_solver.rs:174-280; clipped
+ * step, adaptive damping) with the analytic slope of Sigma^CD, up to max_iter
+ * evaluations.  LINEARIZED: one evaluation at e_n, E = e_n + Z (Sx + Sigma(e_n)
+ * - Vxc) (qp/evgw.rs:784-821).  Z is clipped to [0.1, 0.999] in both. */
+typedef enum { QX_QP_NEWTON = 0, QX_QP_LINEARIZED = 1 } qx_qp_solver;
+
 /* Sigma_c(w) = imaginary-axis GL integral + residues at the real shifts
  * |w - e_m| (imaginary-axis integrand of compute_sigma_c_pyscf_cd,
  * quasix_core/src/selfenergy/correlation_pyscf_cd.rs:164-259; residues restated
@@ -175,8 +182,32 @@ qx_status qx_evgw(qx_ctx* ctx, const double* mo_energy, const double* lpq, const
  * root for each target.  Outputs [ntarget]. */
 qx_status qx_g0w0_cd(qx_ctx* ctx, const double* mo_energy, const double* lpq, const double* vxc, int nmo,
                      int nocc, int naux, const int* targets, int ntarget, int nw, double x0, double tol,
-                     int max_iter, int precision, double* qp_energies, double* z_factors,
+                     int max_iter, int qp_solver, int precision, double* qp_energies, double* z_factors,
                      double* sigma_c, double* sigma_x);
+
+/* Many independent G0W0-CD systems of uneven size in one call (no reference
+ * counterpart: the reference runs compute_sigma_c_pyscf_cd once per system).
+ * Each system is the argument set of qx_g0w0_cd; the library runs them on
+ * nworkers worker streams of the context (<= 0: 4; at most 16), largest P0
+ * cost first, each with its own workspace, so that small systems overlap the
+ * large ones.  Per-system status is written to systems[i].status; the call
+ * returns the first failure (by index). */
+typedef struct {
+  const double* mo_energy; /* [nmo] */
+  const double* lpq;       /* [naux][nmo][nmo] */
+  const double* vxc;       /* [nmo] or NULL (0) */
+  int nmo, nocc, naux;
+  const int* targets;      /* [ntarget] */
+  int ntarget;
+  double* qp_energies;     /* [ntarget] out */
+  double* z_factors;       /* [ntarget] out or NULL */
+  double* sigma_c;         /* [ntarget] out or NULL */
+  double* sigma_x;         /* [ntarget] out or NULL */
+  int status;              /* out: qx_status of this system */
+} qx_cd_system;
+
+qx_status qx_g0w0_cd_batch(qx_ctx* ctx, qx_cd_system* systems, int nsys, int nw, double x0, double tol,
+                           int max_iter, int qp_solver, int precision, int nworkers);
 
 /* ---- bse -------------------------------------------------------------------- */
 typedef struct qx_bse qx_bse;

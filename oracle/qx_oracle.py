@@ -856,11 +856,19 @@ def sigma_cd(omega: float, n: int, mo_energy, lpq, nocc, freqs, wts, wc_imag_n
 
 
 def g0w0_cd(mo_energy, lpq, nocc, targets, nw, x0=0.5, vxc=None, sigma_x=None,
-            tol=1e-8, max_iter=50) -> Dict:
-    """G0W0 by contour deformation for ``targets``: Newton on
-    f(E) = E - e_n - Sx_n - Sigma_c^CD(E) + Vxc_n with the analytic derivative,
-    full steps clipped to 1 Ha, |f| < tol.  Sigma_x from the exchange of
-    quasix_core/src/qp/evgw.rs:1167-1193; Vxc = 0 unless given."""
+            tol=1e-8, max_iter=50, qp_solver="newton", z_min=0.1, z_max=0.999) -> Dict:
+    """G0W0 by contour deformation for ``targets``, f(E) = E - e_n - Sx_n -
+    Sigma_c^CD(E) + Vxc_n, with the analytic slope of Sigma^CD.
+
+    qp_solver "newton": the step rule of NewtonQPSolver::solve
+    (quasix_core/src/qp/newton_solver.rs:174-280): step -f/f' (or
+    -sign(f) min(1, |f|) when |f'| < 1e-10) clipped to +-1 Ha, times an
+    adaptive damping that starts at 1, halves when |f| grew and grows by 1.2
+    when |f| more than halved, within [0.1, 1]; converged when |f| < tol.
+    qp_solver "linearized": E = e_n + Z (Sx_n + Sigma(e_n) - Vxc_n), the
+    linearized QP of qp/evgw.rs:784-821.  Z = 1/(1 - dSigma/dw) clipped to
+    [z_min, z_max] in both (newton_solver.rs:306-315).  Sigma_x from the
+    exchange of quasix_core/src/qp/evgw.rs:1167-1193; Vxc = 0 unless given."""
     nmo = mo_energy.shape[0]
     freqs, wts = get_scaled_legendre_roots(nw, x0)
     if sigma_x is None:
@@ -874,17 +882,33 @@ def g0w0_cd(mo_energy, lpq, nocc, targets, nw, x0=0.5, vxc=None, sigma_x=None,
     iters = np.zeros(len(targets), dtype=np.int64)
     for t, n in enumerate(targets):
         e = mo_energy[n]
+        if qp_solver == "linearized":
+            s, ds = sigma_cd(e, n, mo_energy, lpq, nocc, freqs, wts, wci[:, t])
+            z = min(max(1.0 / (1.0 - ds), z_min), z_max)
+            qp[t] = e + z * (sigma_x[n] + s - vxc[n])
+            zf[t] = z
+            sc_out[t] = s
+            iters[t] = 1
+            continue
+        damping, prev = 1.0, np.inf
+        it = 0
         for it in range(max_iter):
             s, ds = sigma_cd(e, n, mo_energy, lpq, nocc, freqs, wts, wci[:, t])
             f = e - mo_energy[n] - sigma_x[n] - s + vxc[n]
             if abs(f) < tol:
                 break
-            step = -f / (1.0 - ds)
+            fp = 1.0 - ds
+            step = -np.sign(f) * min(1.0, abs(f)) if abs(fp) < 1e-10 else -f / fp
             step = min(max(step, -1.0), 1.0)
-            e += step
+            if abs(f) > prev:
+                damping = max(damping * 0.5, 0.1)
+            elif abs(f) < 0.5 * prev and damping < 1.0:
+                damping = min(damping * 1.2, 1.0)
+            e += damping * step
+            prev = abs(f)
         s, ds = sigma_cd(e, n, mo_energy, lpq, nocc, freqs, wts, wci[:, t])
         qp[t] = e
-        zf[t] = 1.0 / (1.0 - ds)
+        zf[t] = min(max(1.0 / (1.0 - ds), z_min), z_max)
         sc_out[t] = s
         iters[t] = it + 1
     return dict(qp_energies=qp, z_factors=zf, sigma_c=sc_out, sigma_x=sigma_x[list(targets)],

@@ -8,12 +8,12 @@ Drop-in entry points with the reference's names and argument meaning:
 from . import _native, bse
 from .bse import BSETDAConfig, BSETDAKernel, BSETDAResult, DavidsonConfig, run_bse_tda
 from .gw import (ac_pade_thiele_diag, compute_epsilon_inverse_minus_identity, compute_exchange_diag,
-                 compute_polarizability_p0, evgw, g0w0_cd, get_rho_response, get_rho_response_batch,
+                 compute_polarizability_p0, evgw, g0w0_cd, g0w0_cd_batch, get_rho_response, get_rho_response_batch,
                  get_scaled_legendre_roots, get_sigma_diag, pade_thiele, run_evgw, run_evgw_blocks)
 
 __all__ = [
     "bse", "BSETDAConfig", "BSETDAKernel", "BSETDAResult", "DavidsonConfig", "run_bse_tda",
     "ac_pade_thiele_diag", "compute_epsilon_inverse_minus_identity", "compute_exchange_diag",
-    "compute_polarizability_p0", "evgw", "g0w0_cd", "get_rho_response", "get_rho_response_batch",
+    "compute_polarizability_p0", "evgw", "g0w0_cd", "g0w0_cd_batch", "get_rho_response", "get_rho_response_batch",
     "get_scaled_legendre_roots", "get_sigma_diag", "pade_thiele", "run_evgw", "run_evgw_blocks",
 ]

@@ -20,6 +20,7 @@ STATUS_NAMES = {
     5: "NotImplemented", 6: "CudaError", 7: "NoDevice",
 }
 PREC = {"fp64": 0, "bf16x3": 1, "fp16x3": 2}
+QP_SOLVER = {"newton": 0, "linearized": 1}
 
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int)
@@ -62,6 +63,14 @@ class DavidsonConfig(C.Structure):
                 ("tol_residual", C.c_double), ("lindep_threshold", C.c_double), ("level_shift", C.c_double)]
 
 
+class CdSystem(C.Structure):
+    _fields_ = [
+        ("mo_energy", _vp), ("lpq", _vp), ("vxc", _vp), ("nmo", C.c_int), ("nocc", C.c_int), ("naux", C.c_int),
+        ("targets", _vp), ("ntarget", C.c_int), ("qp_energies", _vp), ("z_factors", _vp), ("sigma_c", _vp),
+        ("sigma_x", _vp), ("status", C.c_int),
+    ]
+
+
 # Every symbol the header declares, with its ctypes signature.
 SIGNATURES = {
     "qx_ctx_create": (C.c_int, [C.POINTER(_vp), C.c_int]),
@@ -84,7 +93,9 @@ SIGNATURES = {
     "qx_evgw": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int, C.c_int, C.c_int, C.POINTER(EvgwConfig),
                           C.POINTER(EvgwResult)]),
     "qx_g0w0_cd": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int, C.c_int, C.c_int, _vp, C.c_int, C.c_int, C.c_double,
-                             C.c_double, C.c_int, C.c_int, _vp, _vp, _vp, _vp]),
+                             C.c_double, C.c_int, C.c_int, C.c_int, _vp, _vp, _vp, _vp]),
+    "qx_g0w0_cd_batch": (C.c_int, [_vp, C.POINTER(CdSystem), C.c_int, C.c_int, C.c_double, C.c_double, C.c_int,
+                                   C.c_int, C.c_int, C.c_int]),
     "qx_bse_create": (C.c_int, [_vp, C.POINTER(_vp), C.c_int, C.c_int, C.c_int, _vp, _vp, _vp, _vp, _vp, C.c_int,
                                 C.c_int]),
     "qx_bse_destroy": (C.c_int, [_vp]),

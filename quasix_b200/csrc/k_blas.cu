@@ -1,6 +1,8 @@
 // Generic FP64 building blocks on the DMMA mainloop: a batched "NT" GEMM with
 // split-K, small combination kernels and a one-CTA parallel Jacobi
 // eigensolver for the Davidson Rayleigh-Ritz step.
+#include <mutex>
+
 #include "gemm_f64.cuh"
 #include "qx_internal.cuh"
 #include "qx_blas.cuh"
@@ -64,11 +66,10 @@ void gemm_nt_f64(qx_ctx* ctx, GemmNT g) {
                  (reinterpret_cast<uintptr_t>(g.B) & 15) == 0 && g.sA % 2 == 0 && g.sB % 2 == 0,
              QX_ERR_INVALID_INPUT, "gemm_nt_f64: operands must be 16-byte aligned with even leading dimensions");
   if (g.M <= 0 || g.N <= 0 || g.batch <= 0) return;
-  static bool attr = false;
-  if (!attr) {
+  static std::once_flag attr_once;
+  std::call_once(attr_once, [&] {
     QX_CUDA(cudaFuncSetAttribute(k_gemm_nt, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::SMEM));
-    attr = true;
-  }
+  });
   if (g.splitk < 1) {
     // Enough CTAs to fill the GPU about twice.
     const long tiles = (long)ceil_div(g.M, T::BM) * ceil_div(g.N, T::BN) * g.batch;
@@ -255,11 +256,10 @@ __global__ void __launch_bounds__(1024) k_jacobi(double* __restrict__ A, double*
 void jacobi_eigh(qx_ctx* ctx, double* A, double* V, int n, int lda, double* w, double* Z, int ldz, int* info) {
   const int m = n + (n & 1);
   const size_t sh = (size_t)m * sizeof(double) + (size_t)m * sizeof(int) + 64;
-  static bool attr = false;
-  if (!attr) {
+  static std::once_flag attr_once;
+  std::call_once(attr_once, [&] {
     QX_CUDA(cudaFuncSetAttribute(k_jacobi, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024));
-    attr = true;
-  }
+  });
   QX_REQUIRE(sh <= 64 * 1024, QX_ERR_INVALID_INPUT, "subspace too large for the Jacobi kernel (%d)", n);
   k_jacobi<<<1, 1024, sh, ctx->stream>>>(A, V, n, lda, w, Z, ldz, 60, info);
   check_launch(ctx);

@@ -1,6 +1,8 @@
 // FP64 kernels of the GW chain: chi weights, eps = I + B chi B^T, block-sweep
 // inversion to Wc = eps^-1 - I, pair gathers, exchange diagonal, the Sigma_c
 // pair contraction v = B_p^T Wc B_p, and the Sigma_c(iw) assembly.
+#include <mutex>
+
 #include "gemm_f64.cuh"
 #include "qx_blas.cuh"
 #include "qx_internal.cuh"
@@ -83,11 +85,10 @@ void launch_eps_fp64(qx_ctx* ctx, const double* bov, int ldov, int naux, int nov
   using T = EpsTile;
   const int tiles = ceil_div(naux, T::BM);
   dim3 grid(tiles * (tiles + 1) / 2, nw);
-  static bool attr = false;
-  if (!attr) {
+  static std::once_flag attr_once;
+  std::call_once(attr_once, [&] {
     QX_CUDA(cudaFuncSetAttribute(k_eps_f64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::SMEM));
-    attr = true;
-  }
+  });
   k_eps_f64<<<grid, T::THREADS, T::SMEM, ctx->stream>>>(bov, ldov, naux, nov, chi, eps, ldn, eps_stride);
   check_launch(ctx);
 }
@@ -284,7 +285,11 @@ __global__ void k_sweep_write(double* __restrict__ M, int n, int ldn, size_t str
   const double* D = Dp + (size_t)w * SWEEP_NB * SWEEP_NB;
   for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < n * kb; idx += gridDim.x * blockDim.x) {
     const int r = idx / kb, q = idx % kb;
-    const double v = (r >= k0 && r < k0 + kb) ? -D[(r - k0) * SWEEP_NB + q] : Tw[(size_t)r * SWEEP_NB + q];
+    // Inside the K block both (r, q) and its mirror write the same element:
+    // take D's lower triangle for both, so the stored value does not depend on
+    // which write lands last.
+    const int a = r - k0;
+    const double v = (r >= k0 && r < k0 + kb) ? -D[max(a, q) * SWEEP_NB + min(a, q)] : Tw[(size_t)r * SWEEP_NB + q];
     A[(size_t)r * ldn + k0 + q] = v;
     A[(size_t)(k0 + q) * ldn + r] = v;
   }
@@ -318,15 +323,14 @@ void launch_invert_wc(qx_ctx* ctx, double* eps, int n, int ldn, size_t stride, i
   int* status = reinterpret_cast<int*>(Dp + (size_t)nw * SWEEP_NB * SWEEP_NB);
   QX_CUDA(cudaMemsetAsync(status, 0, nw * sizeof(int), ctx->stream));
   const int diag_smem = (SWEEP_NB * SWEEP_NB + SWEEP_NB * 33) * sizeof(double);
-  static bool attr = false;
-  if (!attr) {
+  static std::once_flag attr_once;
+  std::call_once(attr_once, [&] {
     QX_CUDA(cudaFuncSetAttribute(k_sweep_diag, cudaFuncAttributeMaxDynamicSharedMemorySize, diag_smem));
     QX_CUDA(cudaFuncSetAttribute(k_sweep_tpanel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)PanelTile::SMEM));
     QX_CUDA(cudaFuncSetAttribute(k_sweep_update, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)SweepTile::SMEM));
-    attr = true;
-  }
+  });
   const int tiles = ceil_div(n, SweepTile::BM);
   for (int k0 = 0; k0 < n; k0 += SWEEP_NB) {
     const int kb = min(SWEEP_NB, n - k0);
@@ -533,11 +537,10 @@ __global__ void __launch_bounds__(PairTile::THREADS) k_pair_contract_f64(const d
 void launch_pair_contract_fp64(qx_ctx* ctx, const double* bpt, int ldk, int npair, int naux, const double* wc,
                                int ldn, size_t wc_stride, int nw, double* v, int ldv) {
   using T = PairTile;
-  static bool attr = false;
-  if (!attr) {
+  static std::once_flag attr_once;
+  std::call_once(attr_once, [&] {
     QX_CUDA(cudaFuncSetAttribute(k_pair_contract_f64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::SMEM));
-    attr = true;
-  }
+  });
   dim3 grid(ceil_div(npair, T::BM), nw);
   k_pair_contract_f64<<<grid, T::THREADS, T::SMEM, ctx->stream>>>(bpt, ldk, npair, naux, wc, ldn, wc_stride, v, ldv);
   check_launch(ctx);

@@ -19,6 +19,8 @@
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
+#include <mutex>
+
 #include "qx_internal.cuh"
 
 namespace qx {
@@ -431,14 +433,15 @@ typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t,
                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
 
 static EncodeTiledFn encode_fn() {
+  static std::once_flag once;
   static EncodeTiledFn fn = nullptr;
-  if (!fn) {
+  std::call_once(once, [] {
     void* p = nullptr;
     cudaDriverEntryPointQueryResult q;
     QX_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q));
     QX_REQUIRE(p != nullptr && q == cudaDriverEntryPointSuccess, QX_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
     fn = reinterpret_cast<EncodeTiledFn>(p);
-  }
+  });
   return fn;
 }
 
@@ -579,11 +582,10 @@ template <int BN, int EPI>
 static void launch_tc(qx_ctx* ctx, const CUtensorMap& ah, const CUtensorMap& al, const CUtensorMap& bh,
                       const CUtensorMap& bl, const TcArgs& a, dim3 grid) {
   using L = TcSmem<BN>;
-  static bool attr = false;
-  if (!attr) {
+  static std::once_flag attr_once;
+  std::call_once(attr_once, [&] {
     QX_CUDA(cudaFuncSetAttribute(k_tc_gemm<BN, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, L::TOTAL));
-    attr = true;
-  }
+  });
   k_tc_gemm<BN, EPI><<<grid, TcWarps<EPI>::THREADS, L::TOTAL, ctx->stream>>>(ah, al, bh, bl, a);
   check_launch(ctx);
 }

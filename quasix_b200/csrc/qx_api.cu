@@ -465,8 +465,10 @@ qx_status qx_ctx_create(qx_ctx** out, int device) {
 
 qx_status qx_ctx_destroy(qx_ctx* c) {
   if (!c) return QX_OK;
+  for (qx_ctx* w : c->workers) qx_ctx_destroy(w);
+  c->workers.clear();
   cudaSetDevice(c->device);
-  cudaStreamSynchronize(c->stream);
+  if (c->stream) cudaStreamSynchronize(c->stream);
   for (auto& e : c->ev)
     if (e) cudaEventDestroy(e);
   if (c->own_stream) cudaStreamDestroy(c->own_stream);

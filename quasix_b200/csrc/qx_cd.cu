@@ -14,6 +14,9 @@
 // transition; the sweep needs no positive pivots).  The QP root is a Newton
 // iteration with the analytic derivative, all targets at once.
 #include <algorithm>
+#include <atomic>
+#include <mutex>
+#include <thread>
 
 #include "qx_blas.cuh"
 #include "qx_gw_sys.cuh"
@@ -113,112 +116,127 @@ __global__ void k_cd_dres(const double* __restrict__ tmat, int ldt, const double
   if (threadIdx.x == 0) out[r] = 4.0 * red[0];
 }
 
-}  // namespace qx
+// One G0W0-CD problem (the arguments of qx_g0w0_cd).
+struct CdProblem {
+  const double* mo_energy;
+  const double* lpq;
+  const double* vxc;
+  int nmo, nocc, naux;
+  const int* targets;
+  int ntarget, nw;
+  double x0, tol;
+  int max_iter, qp_solver, precision;
+  double *qp, *z, *sc, *sx;
+};
 
-using namespace qx;
-
-extern "C" qx_status qx_g0w0_cd(qx_ctx* ctx, const double* mo_energy, const double* lpq, const double* vxc, int nmo,
-                                int nocc, int naux, const int* targets, int ntarget, int nw, double x0, double tol,
-                                int max_iter, int precision, double* qp_energies, double* z_factors, double* sigma_c,
-                                double* sigma_x) {
-  if (!ctx) return QX_ERR_INVALID_INPUT;
-  try {
-    ctx->pending.clear();
-    ctx->launches = 0;
-    for (double& v : ctx->stage_ms) v = 0.0;
-    QX_CUDA(cudaSetDevice(ctx->device));
-    QX_REQUIRE(mo_energy && lpq && targets && qp_energies && ntarget > 0 && nw > 0 && max_iter > 0,
-               QX_ERR_INVALID_INPUT, "invalid arguments to g0w0_cd");
-    validate_common(nmo, nocc, naux);
-    const int nvir = nmo - nocc;
-    std::vector<double> e(nmo), vx(nmo, 0.0);
-    QX_CUDA(cudaMemcpy(e.data(), mo_energy, nmo * sizeof(double), cudaMemcpyDefault));
-    if (vxc) QX_CUDA(cudaMemcpy(vx.data(), vxc, nmo * sizeof(double), cudaMemcpyDefault));
-    std::vector<int> tg(ntarget);
-    QX_CUDA(cudaMemcpy(tg.data(), targets, ntarget * sizeof(int), cudaMemcpyDefault));
-    for (int t : tg) QX_REQUIRE(t >= 0 && t < nmo, QX_ERR_INVALID_INPUT, "target orbital %d out of range", t);
-    const double* d_lpq = (const double*)device_view(ctx, WS_LPQ, lpq, (size_t)naux * nmo * nmo * sizeof(double));
-    // Imaginary axis: Wc_nm(i f_k) for the target pairs (no cutoff: the sigma grid is unused).
-    GWSystem S;
-    gw_setup(ctx, S, d_lpq, nmo, nocc, naux, tg, nw, 1e300, x0, precision);
-    gw_wc_pairs(ctx, S, e.data());
-    // Exchange.
-    DevBuf& cb = ctx->ws[WS_CD0];
-    cb.reserve((size_t)(nmo + 4 * ntarget + 64) * sizeof(double));
-    double* d_sx = cb.as<double>();
-    double* d_om = d_sx + nmo;
-    double* d_imag = d_om + ntarget;
-    launch_exchange_diag(ctx, d_lpq, naux, nmo, nocc, d_sx);
-    std::vector<double> sx(nmo);
-    QX_CUDA(cudaMemcpyAsync(sx.data(), d_sx, nmo * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-    // B_ov^T [nov][ldn] for the residue derivatives.
-    const int nov = nocc * nvir, ldn = S.ldn;
-    DevBuf& bt = ctx->ws[WS_CD1];
-    bt.reserve((size_t)nov * ldn * sizeof(double));
-    double* bovT = bt.as<double>();
-    QX_CUDA(cudaMemsetAsync(bovT, 0, (size_t)nov * ldn * sizeof(double), ctx->stream));
-    transpose(ctx, S.bov, naux, nov, S.ldov, 0, bovT, ldn, 0, 1);
-    std::vector<double> om(ntarget), sig(ntarget, 0.0), dsig(ntarget, 0.0);
-    std::vector<int> done(ntarget, 0), iters(ntarget, 0);
-    for (int t = 0; t < ntarget; ++t) om[t] = e[tg[t]];
-    auto evaluate = [&](const std::vector<int>& act) {
-      // Imaginary-axis part for every target.
-      QX_CUDA(cudaMemcpyAsync(d_om, om.data(), ntarget * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
-      k_cd_imag<<<ntarget, 256, 0, ctx->stream>>>(S.v, S.npair, nw, S.d_pidx, nmo, S.d_en, S.d_freqs, S.d_wts, d_om,
-                                                   d_imag);
-      check_launch(ctx);
-      std::vector<double> hi(2 * ntarget);
-      QX_CUDA(cudaMemcpyAsync(hi.data(), d_imag, 2 * ntarget * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-      // Residue list.
-      std::vector<int2> nm;
-      std::vector<double> wr, sgn;
-      std::vector<int> owner;
-      for (int t : act) {
-        const int n = tg[t];
-        for (int m = 0; m < nmo; ++m) {
-          if (m < nocc && e[m] > om[t]) {
-            nm.push_back(make_int2(n, m));
-            wr.push_back(e[m] - om[t]);
-            sgn.push_back(-1.0);
-            owner.push_back(t);
-          } else if (m >= nocc && e[m] < om[t]) {
-            nm.push_back(make_int2(n, m));
-            wr.push_back(om[t] - e[m]);
-            sgn.push_back(1.0);
-            owner.push_back(t);
-          }
+// Runs one system on ctx (throws qx::Error).  Imaginary-axis Wc for the target
+// pairs once, then Newton steps; each evaluation adds the residues of the
+// poles between the target energy and the Fermi level.
+void g0w0_cd_run(qx_ctx* ctx, const CdProblem& p) {
+  const int nmo = p.nmo, nocc = p.nocc, naux = p.naux, ntarget = p.ntarget, nw = p.nw;
+  QX_REQUIRE(p.mo_energy && p.lpq && p.targets && p.qp && ntarget > 0 && nw > 0 && p.max_iter > 0,
+             QX_ERR_INVALID_INPUT, "invalid arguments to g0w0_cd");
+  QX_REQUIRE(p.qp_solver == QX_QP_NEWTON || p.qp_solver == QX_QP_LINEARIZED, QX_ERR_INVALID_INPUT,
+             "qp_solver %d", p.qp_solver);
+  validate_common(nmo, nocc, naux);
+  const int nvir = nmo - nocc;
+  std::vector<double> e(nmo), vx(nmo, 0.0);
+  QX_CUDA(cudaMemcpy(e.data(), p.mo_energy, nmo * sizeof(double), cudaMemcpyDefault));
+  if (p.vxc) QX_CUDA(cudaMemcpy(vx.data(), p.vxc, nmo * sizeof(double), cudaMemcpyDefault));
+  std::vector<int> tg(ntarget);
+  QX_CUDA(cudaMemcpy(tg.data(), p.targets, ntarget * sizeof(int), cudaMemcpyDefault));
+  for (int t : tg) QX_REQUIRE(t >= 0 && t < nmo, QX_ERR_INVALID_INPUT, "target orbital %d out of range", t);
+  const double* d_lpq = (const double*)device_view(ctx, WS_LPQ, p.lpq, (size_t)naux * nmo * nmo * sizeof(double));
+  const bool tc = is_tc_precision(p.precision);
+  // Imaginary axis: Wc_nm(i f_k) for the target pairs (no cutoff: the sigma grid is unused).
+  GWSystem S;
+  gw_setup(ctx, S, d_lpq, nmo, nocc, naux, tg, nw, 1e300, p.x0, p.precision);
+  gw_wc_pairs(ctx, S, e.data());
+  // Exchange.
+  DevBuf& cb = ctx->ws[WS_CD0];
+  cb.reserve((size_t)(nmo + 4 * ntarget + 64) * sizeof(double));
+  double* d_sx = cb.as<double>();
+  double* d_om = d_sx + nmo;
+  double* d_imag = d_om + ntarget;
+  launch_exchange_diag(ctx, d_lpq, naux, nmo, nocc, d_sx);
+  std::vector<double> sx(nmo);
+  QX_CUDA(cudaMemcpyAsync(sx.data(), d_sx, nmo * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  // B_ov^T [nov][ldn] for the residue derivatives.
+  const int nov = nocc * nvir, ldn = S.ldn;
+  DevBuf& bt = ctx->ws[WS_CD1];
+  bt.reserve((size_t)nov * ldn * sizeof(double));
+  double* bovT = bt.as<double>();
+  QX_CUDA(cudaMemsetAsync(bovT, 0, (size_t)nov * ldn * sizeof(double), ctx->stream));
+  transpose(ctx, S.bov, naux, nov, S.ldov, 0, bovT, ldn, 0, 1);
+  std::vector<double> om(ntarget), sig(ntarget, 0.0), dsig(ntarget, 0.0);
+  for (int t = 0; t < ntarget; ++t) om[t] = e[tg[t]];
+  auto evaluate = [&](const std::vector<int>& act) {
+    // Imaginary-axis part for every target.
+    QX_CUDA(cudaMemcpyAsync(d_om, om.data(), ntarget * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    k_cd_imag<<<ntarget, 256, 0, ctx->stream>>>(S.v, S.npair, nw, S.d_pidx, nmo, S.d_en, S.d_freqs, S.d_wts, d_om,
+                                                 d_imag);
+    check_launch(ctx);
+    std::vector<double> hi(2 * ntarget);
+    QX_CUDA(cudaMemcpyAsync(hi.data(), d_imag, 2 * ntarget * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    // Residue list.
+    std::vector<int2> nm;
+    std::vector<double> wr, sgn;
+    std::vector<int> owner;
+    for (int t : act) {
+      const int n = tg[t];
+      for (int m = 0; m < nmo; ++m) {
+        if (m < nocc && e[m] > om[t]) {
+          nm.push_back(make_int2(n, m));
+          wr.push_back(e[m] - om[t]);
+          sgn.push_back(-1.0);
+          owner.push_back(t);
+        } else if (m >= nocc && e[m] < om[t]) {
+          nm.push_back(make_int2(n, m));
+          wr.push_back(om[t] - e[m]);
+          sgn.push_back(1.0);
+          owner.push_back(t);
         }
       }
-      const int R = (int)nm.size();
-      std::vector<double> rv(R), rd(R);
-      if (R > 0) {
-        const size_t stride = (size_t)naux * ldn;
-        DevBuf& rb = ctx->ws[WS_CD2];
-        const size_t need = (size_t)R * (stride + 2 * ldn + S.ldov + 4) * sizeof(double) + R * sizeof(int2) + 1024;
-        rb.reserve(need);
-        double* eps = rb.as<double>();
-        double* b = eps + (size_t)R * stride;
-        double* x = b + (size_t)R * ldn;
-        double* tm = x + (size_t)R * ldn;
-        double* d_wr = tm + (size_t)R * S.ldov;
-        double* d_val = d_wr + R;
-        double* d_dv = d_val + R;
-        int2* d_nm = reinterpret_cast<int2*>(d_dv + R + 1);
-        QX_CUDA(cudaMemcpyAsync(d_wr, wr.data(), R * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
-        QX_CUDA(cudaMemcpyAsync(d_nm, nm.data(), R * sizeof(int2), cudaMemcpyHostToDevice, ctx->stream));
-        // eps(w_r) = I + B_ov diag(chi'(w_r)) B_ov^T, real axis (chi buffer reused).
-        ctx->ws[WS_CD3].reserve((size_t)R * S.ldov * sizeof(double));
-        double* chi = ctx->ws[WS_CD3].as<double>();
-        launch_chi(ctx, S.d_en, nocc, nvir, d_wr, R, 1, chi, S.ldov);
-        launch_eps_fp64(ctx, S.bov, S.ldov, naux, nov, chi, R, eps, ldn, stride);
-        launch_invert_wc(ctx, eps, naux, ldn, stride, R);
-        dim3 gg(ceil_div(ldn, 256), R);
-        k_cd_gather<<<gg, 256, 0, ctx->stream>>>(d_lpq, naux, nmo, d_nm, R, b, ldn);
+    }
+    const int R = (int)nm.size();
+    std::vector<double> rv(R), rd(R);
+    if (R > 0) {
+      // Residues in chunks of RC frequencies so that the eps matrices (and,
+      // for the split forms, the split operands) stay within ~2 GB.
+      const size_t stride = (size_t)naux * ldn;
+      const size_t per_res = (stride + S.ldov) * sizeof(double) + (tc ? (size_t)naux * S.ldov * 4 : 0);
+      const int RC = (int)std::max<size_t>(1, std::min<size_t>((size_t)R, ((size_t)2 << 30) / per_res));
+      DevBuf& rb = ctx->ws[WS_CD2];
+      const size_t need = (size_t)RC * (stride + 2 * ldn + S.ldov + 4) * sizeof(double) + RC * sizeof(int2) + 1024;
+      rb.reserve(need);
+      double* eps = rb.as<double>();
+      double* b = eps + (size_t)RC * stride;
+      double* x = b + (size_t)RC * ldn;
+      double* tm = x + (size_t)RC * ldn;
+      double* d_wr = tm + (size_t)RC * S.ldov;
+      double* d_val = d_wr + RC;
+      double* d_dv = d_val + RC;
+      int2* d_nm = reinterpret_cast<int2*>(d_dv + RC + 1);
+      ctx->ws[WS_CD3].reserve((size_t)RC * S.ldov * sizeof(double));
+      double* chi = ctx->ws[WS_CD3].as<double>();
+      for (int c0 = 0; c0 < R; c0 += RC) {
+        const int rc = std::min(RC, R - c0);
+        QX_CUDA(cudaMemcpyAsync(d_wr, wr.data() + c0, rc * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+        QX_CUDA(cudaMemcpyAsync(d_nm, nm.data() + c0, rc * sizeof(int2), cudaMemcpyHostToDevice, ctx->stream));
+        // eps(w_r) = I + B_ov diag(chi'(w_r)) B_ov^T, real axis.
+        launch_chi(ctx, S.d_en, nocc, nvir, d_wr, rc, 1, chi, S.ldov);
+        if (tc)
+          launch_eps_tc(ctx, S.bov, S.ldov, naux, nov, chi, rc, eps, ldn, stride, p.precision == QX_PREC_FP16X3);
+        else
+          launch_eps_fp64(ctx, S.bov, S.ldov, naux, nov, chi, rc, eps, ldn, stride);
+        launch_invert_wc(ctx, eps, naux, ldn, stride, rc);
+        dim3 gg(ceil_div(ldn, 256), rc);
+        k_cd_gather<<<gg, 256, 0, ctx->stream>>>(d_lpq, naux, nmo, d_nm, rc, b, ldn);
         check_launch(ctx);
-        k_cd_quad<<<R, 256, 0, ctx->stream>>>(eps, ldn, stride, b, naux, ldn, x, d_val);
+        k_cd_quad<<<rc, 256, 0, ctx->stream>>>(eps, ldn, stride, b, naux, ldn, x, d_val);
         check_launch(ctx);
         GemmNT g{};
-        g.M = R;
+        g.M = rc;
         g.N = nov;
         g.K = naux;
         g.A = x;
@@ -231,53 +249,194 @@ extern "C" qx_status qx_g0w0_cd(qx_ctx* ctx, const double* mo_energy, const doub
         g.alpha = 1.0;
         g.splitk = 0;
         gemm_nt_f64(ctx, g);
-        k_cd_dres<<<R, 256, 0, ctx->stream>>>(tm, S.ldov, S.d_en, nocc, nvir, d_wr, d_dv);
+        k_cd_dres<<<rc, 256, 0, ctx->stream>>>(tm, S.ldov, S.d_en, nocc, nvir, d_wr, d_dv);
         check_launch(ctx);
-        QX_CUDA(cudaMemcpyAsync(rv.data(), d_val, R * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-        QX_CUDA(cudaMemcpyAsync(rd.data(), d_dv, R * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+        QX_CUDA(cudaMemcpyAsync(rv.data() + c0, d_val, rc * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+        QX_CUDA(cudaMemcpyAsync(rd.data() + c0, d_dv, rc * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+        // The singular-eps flags live in one buffer per context: read them
+        // before the next chunk reuses it.
+        if (c0 + rc < R) sync_and_check(ctx);
       }
-      sync_and_check(ctx);
-      for (int t : act) {
-        sig[t] = hi[2 * t];
-        dsig[t] = hi[2 * t + 1];
-      }
-      for (int r = 0; r < R; ++r) {
-        sig[owner[r]] += sgn[r] * rv[r];
-        dsig[owner[r]] += rd[r];
-      }
-    };
-    std::vector<int> act;
-    for (int t = 0; t < ntarget; ++t) act.push_back(t);
-    for (int it = 0; it < max_iter && !act.empty(); ++it) {
+    }
+    sync_and_check(ctx);
+    for (int t : act) {
+      sig[t] = hi[2 * t];
+      dsig[t] = hi[2 * t + 1];
+    }
+    for (int r = 0; r < R; ++r) {
+      sig[owner[r]] += sgn[r] * rv[r];
+      dsig[owner[r]] += rd[r];
+    }
+  };
+  constexpr double z_min = 0.1, z_max = 0.999;  // newton_solver.rs:93-95
+  std::vector<double> zf(ntarget), sxo(ntarget);
+  std::vector<int> all;
+  for (int t = 0; t < ntarget; ++t) all.push_back(t);
+  if (p.qp_solver == QX_QP_LINEARIZED) {
+    // E = e_n + Z (Sx + Sigma(e_n) - Vxc), Z clipped (qp/evgw.rs:784-821).
+    evaluate(all);
+    for (int t = 0; t < ntarget; ++t) {
+      const int n = tg[t];
+      zf[t] = std::min(std::max(1.0 / (1.0 - dsig[t]), z_min), z_max);
+      om[t] = e[n] + zf[t] * (sx[n] + sig[t] - vx[n]);
+    }
+  } else {
+    // Newton with the step rule of NewtonQPSolver::solve (newton_solver.rs:174-280):
+    // clipped step, adaptive damping in [0.1, 1].  fresh[t]: sig/dsig of
+    // target t were evaluated at om[t].
+    std::vector<int> act = all, fresh(ntarget, 0);
+    std::vector<double> damping(ntarget, 1.0), prev(ntarget, HUGE_VAL);
+    for (int it = 0; it < p.max_iter && !act.empty(); ++it) {
       evaluate(act);
       std::vector<int> next;
       for (int t : act) {
         const int n = tg[t];
         const double f = om[t] - e[n] - sx[n] - sig[t] + vx[n];
-        iters[t] = it + 1;
-        if (std::fabs(f) < tol) continue;  // converged at om[t]
-        double step = -f / (1.0 - dsig[t]);
+        const double af = std::fabs(f);
+        fresh[t] = 1;
+        if (af < p.tol) continue;  // converged at om[t]
+        const double fp = 1.0 - dsig[t];
+        double step = (std::fabs(fp) < 1e-10) ? -std::copysign(std::min(1.0, af), f) : -f / fp;
         step = std::min(std::max(step, -1.0), 1.0);
-        om[t] += step;
+        if (af > prev[t])
+          damping[t] = std::max(damping[t] * 0.5, 0.1);
+        else if (af < 0.5 * prev[t] && damping[t] < 1.0)
+          damping[t] = std::min(damping[t] * 1.2, 1.0);
+        om[t] += damping[t] * step;
+        prev[t] = af;
+        fresh[t] = 0;
         next.push_back(t);
       }
       act.swap(next);
     }
-    // Final self-energy and slope at the returned energies.
-    std::vector<int> all;
-    for (int t = 0; t < ntarget; ++t) all.push_back(t);
-    evaluate(all);
-    std::vector<double> zf(ntarget), sxo(ntarget);
-    for (int t = 0; t < ntarget; ++t) {
-      zf[t] = 1.0 / (1.0 - dsig[t]);
-      sxo[t] = sx[tg[t]];
-      QX_REQUIRE(std::isfinite(om[t]) && std::isfinite(sig[t]), QX_ERR_NUMERICAL, "non-finite CD result for target %d",
-                 tg[t]);
+    // Self-energy and slope at the returned energies (targets whose last
+    // evaluation was before their final step).
+    std::vector<int> stale;
+    for (int t = 0; t < ntarget; ++t)
+      if (!fresh[t]) stale.push_back(t);
+    if (!stale.empty()) evaluate(stale);
+    for (int t = 0; t < ntarget; ++t) zf[t] = std::min(std::max(1.0 / (1.0 - dsig[t]), z_min), z_max);
+  }
+  for (int t = 0; t < ntarget; ++t) {
+    sxo[t] = sx[tg[t]];
+    QX_REQUIRE(std::isfinite(om[t]) && std::isfinite(sig[t]), QX_ERR_NUMERICAL, "non-finite CD result for target %d",
+               tg[t]);
+  }
+  QX_CUDA(cudaMemcpy(p.qp, om.data(), ntarget * sizeof(double), cudaMemcpyDefault));
+  if (p.z) QX_CUDA(cudaMemcpy(p.z, zf.data(), ntarget * sizeof(double), cudaMemcpyDefault));
+  if (p.sc) QX_CUDA(cudaMemcpy(p.sc, sig.data(), ntarget * sizeof(double), cudaMemcpyDefault));
+  if (p.sx) QX_CUDA(cudaMemcpy(p.sx, sxo.data(), ntarget * sizeof(double), cudaMemcpyDefault));
+}
+
+// Worker context of a batch: its own non-blocking stream and workspace, so
+// that systems on different workers overlap on the device.
+qx_ctx* make_worker(int device) {
+  qx_ctx* c = new qx_ctx();
+  c->device = device;
+  try {
+    cudaDeviceProp pr;
+    QX_CUDA(cudaGetDeviceProperties(&pr, device));
+    c->sm_count = pr.multiProcessorCount;
+    QX_CUDA(cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking));
+    c->stream = c->own_stream;
+    for (auto& ev : c->ev) QX_CUDA(cudaEventCreate(&ev));
+  } catch (...) {
+    qx_ctx_destroy(c);
+    throw;
+  }
+  return c;
+}
+
+}  // namespace qx
+
+using namespace qx;
+
+extern "C" qx_status qx_g0w0_cd(qx_ctx* ctx, const double* mo_energy, const double* lpq, const double* vxc, int nmo,
+                                int nocc, int naux, const int* targets, int ntarget, int nw, double x0, double tol,
+                                int max_iter, int qp_solver, int precision, double* qp_energies, double* z_factors,
+                                double* sigma_c, double* sigma_x) {
+  if (!ctx) return QX_ERR_INVALID_INPUT;
+  try {
+    ctx->pending.clear();
+    ctx->launches = 0;
+    for (double& v : ctx->stage_ms) v = 0.0;
+    QX_CUDA(cudaSetDevice(ctx->device));
+    CdProblem p{mo_energy, lpq, vxc, nmo, nocc, naux, targets, ntarget, nw, x0, tol, max_iter, qp_solver, precision,
+                qp_energies, z_factors, sigma_c, sigma_x};
+    g0w0_cd_run(ctx, p);
+    ctx->err.clear();
+    return QX_OK;
+  } catch (const Error& ex) {
+    ctx->err = ex.what();
+    return ex.status;
+  } catch (const std::exception& ex) {
+    ctx->err = ex.what();
+    return QX_ERR_INVALID_INPUT;
+  }
+}
+
+extern "C" qx_status qx_g0w0_cd_batch(qx_ctx* ctx, qx_cd_system* systems, int nsys, int nw, double x0, double tol,
+                                      int max_iter, int qp_solver, int precision, int nworkers) {
+  if (!ctx) return QX_ERR_INVALID_INPUT;
+  try {
+    ctx->pending.clear();
+    ctx->launches = 0;
+    for (double& v : ctx->stage_ms) v = 0.0;
+    QX_CUDA(cudaSetDevice(ctx->device));
+    QX_REQUIRE(systems && nsys > 0 && nw > 0 && max_iter > 0, QX_ERR_INVALID_INPUT, "invalid arguments to g0w0_cd_batch");
+    QX_REQUIRE(precision >= QX_PREC_FP64 && precision <= QX_PREC_FP16X3, QX_ERR_INVALID_INPUT, "precision %d",
+               precision);
+    if (nworkers <= 0) nworkers = 4;
+    nworkers = std::min(std::min(nworkers, 16), nsys);
+    // Inputs may have been produced on the caller's stream.
+    QX_CUDA(cudaStreamSynchronize(ctx->stream));
+    while ((int)ctx->workers.size() < nworkers) ctx->workers.push_back(make_worker(ctx->device));
+    // Largest systems first (P0 cost nov * naux^2 dominates), so that the
+    // small ones fill in behind them.
+    std::vector<int> order(nsys);
+    std::vector<double> cost(nsys);
+    for (int i = 0; i < nsys; ++i) {
+      const qx_cd_system& s = systems[i];
+      order[i] = i;
+      cost[i] = (double)s.nocc * (s.nmo - s.nocc) * s.naux * (double)s.naux + (double)s.naux * s.naux * s.naux;
+      systems[i].status = QX_ERR_INVALID_INPUT;
     }
-    QX_CUDA(cudaMemcpy(qp_energies, om.data(), ntarget * sizeof(double), cudaMemcpyDefault));
-    if (z_factors) QX_CUDA(cudaMemcpy(z_factors, zf.data(), ntarget * sizeof(double), cudaMemcpyDefault));
-    if (sigma_c) QX_CUDA(cudaMemcpy(sigma_c, sig.data(), ntarget * sizeof(double), cudaMemcpyDefault));
-    if (sigma_x) QX_CUDA(cudaMemcpy(sigma_x, sxo.data(), ntarget * sizeof(double), cudaMemcpyDefault));
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cost[a] > cost[b]; });
+    std::atomic<int> next{0};
+    std::mutex mu;
+    std::vector<std::string> msg(nsys);
+    auto work = [&](qx_ctx* w) {
+      if (cudaSetDevice(w->device) != cudaSuccess) return;
+      for (;;) {
+        const int k = next.fetch_add(1);
+        if (k >= nsys) break;
+        qx_cd_system& s = systems[order[k]];
+        w->pending.clear();
+        try {
+          CdProblem p{s.mo_energy, s.lpq, s.vxc,    s.nmo,      s.nocc,       s.naux,      s.targets,
+                      s.ntarget,   nw,    x0,      tol,      max_iter,   qp_solver,    precision,   s.qp_energies,
+                      s.z_factors, s.sigma_c, s.sigma_x};
+          g0w0_cd_run(w, p);
+          s.status = QX_OK;
+        } catch (const Error& ex) {
+          s.status = ex.status;
+          std::lock_guard<std::mutex> lock(mu);
+          msg[order[k]] = ex.what();
+        } catch (const std::exception& ex) {
+          s.status = QX_ERR_INVALID_INPUT;
+          std::lock_guard<std::mutex> lock(mu);
+          msg[order[k]] = ex.what();
+        }
+      }
+    };
+    for (auto* w : ctx->workers) w->launches = 0;
+    std::vector<std::thread> th;
+    for (int i = 0; i < nworkers; ++i) th.emplace_back(work, ctx->workers[i]);
+    for (auto& t : th) t.join();
+    for (int i = 0; i < nworkers; ++i) ctx->launches += ctx->workers[i]->launches;
+    for (int i = 0; i < nsys; ++i)
+      if (systems[i].status != QX_OK)
+        throw Error((qx_status)systems[i].status, fmt("system %d: %s", i, msg[i].c_str()));
     ctx->err.clear();
     return QX_OK;
   } catch (const Error& ex) {

@@ -89,6 +89,8 @@ struct qx_ctx {
     int kind;
   };
   std::vector<Pending> pending;
+  // Worker contexts of batched calls (own streams and workspaces), owned.
+  std::vector<qx_ctx*> workers;
 };
 
 namespace qx {

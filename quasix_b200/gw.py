@@ -17,7 +17,7 @@ Reference interfaces (QuasiX, by path within the project):
 from __future__ import annotations
 
 import ctypes as C
-from typing import Dict, Optional, Sequence
+from typing import Dict, List, Optional, Sequence
 
 import numpy as np
 
@@ -291,21 +291,61 @@ def run_evgw(config: Dict) -> Dict:
                 iw_cutoff=config.get("iw_cutoff", 5.0), precision=config.get("precision", "fp64"), device=config.get("device", 0))
 
 
+def _qp_solver(name) -> int:
+    try:
+        return N.QP_SOLVER[name]
+    except KeyError:
+        raise ValueError(f"qp_solver must be one of {list(N.QP_SOLVER)}") from None
+
+
 def g0w0_cd(mo_energy, lpq, nocc: int, targets: Sequence[int], nw: int = 100, x0: float = 0.5, vxc=None,
-            tol: float = 1e-8, max_iter: int = 50, precision="fp64", device: int = 0) -> Dict:
+            tol: float = 1e-8, max_iter: int = 50, precision="fp64", qp_solver: str = "newton",
+            device: int = 0) -> Dict:
     """G0W0 by contour deformation (imaginary-axis GL integral + residues) with a
-    Newton QP root per target."""
-    ctx = _ctx(device)
+    Newton (damped, as NewtonQPSolver) or linearized QP step per target."""
+    ctx = _ctx(device, lpq, mo_energy, vxc)
     lpq_a = lpq if hasattr(lpq, "data_ptr") else _f64(lpq)
     naux, nmo, _ = tuple(lpq_a.shape)
-    e = _f64(mo_energy)
-    vx = np.zeros(nmo) if vxc is None else _f64(vxc)
+    e = mo_energy if hasattr(mo_energy, "data_ptr") else _f64(mo_energy)
+    vx = np.zeros(nmo) if vxc is None else (vxc if hasattr(vxc, "data_ptr") else _f64(vxc))
     t = np.ascontiguousarray(np.asarray(targets, dtype=np.int32))
     qp = np.zeros(len(t))
     z = np.zeros(len(t))
     sc = np.zeros(len(t))
     sx = np.zeros(len(t))
     ctx.check(ctx.lib.qx_g0w0_cd(ctx.handle, N.ptr(e), N.ptr(lpq_a), N.ptr(vx), nmo, int(nocc), naux, N.ptr(t), len(t),
-                                 int(nw), float(x0), float(tol), int(max_iter), _prec(precision), N.ptr(qp), N.ptr(z),
+                                 int(nw), float(x0), float(tol), int(max_iter), _qp_solver(qp_solver),
+                                 _prec(precision), N.ptr(qp), N.ptr(z),
                                  N.ptr(sc), N.ptr(sx)))
     return dict(qp_energies=qp, z_factors=z, sigma_c=sc, sigma_x=sx)
+
+
+def g0w0_cd_batch(systems, nw: int = 24, x0: float = 0.5, tol: float = 1e-8, max_iter: int = 50,
+                  precision="fp64", qp_solver: str = "newton", nworkers: int = 4, device: int = 0) -> List[Dict]:
+    """G0W0-CD for many independent systems in one call (qx_g0w0_cd_batch).
+
+    ``systems``: sequence of dicts with keys mo_energy, lpq ([naux, nmo, nmo],
+    numpy or a CUDA tensor), nocc, targets and optionally vxc.  Returns one dict
+    per system with the keys of :func:`g0w0_cd`.  The systems run on
+    ``nworkers`` worker streams, largest first."""
+    ctx = _ctx(device, *[s["lpq"] for s in systems])
+    keep, outs = [], []
+    arr = (N.CdSystem * len(systems))()
+    for i, s in enumerate(systems):
+        lpq = s["lpq"] if hasattr(s["lpq"], "data_ptr") else _f64(s["lpq"])
+        naux, nmo, _ = tuple(lpq.shape)
+        e = s["mo_energy"]
+        e = e if hasattr(e, "data_ptr") else _f64(e)
+        vx = s.get("vxc")
+        vx = None if vx is None else (vx if hasattr(vx, "data_ptr") else _f64(vx))
+        t = np.ascontiguousarray(np.asarray(s["targets"], dtype=np.int32))
+        out = dict(qp_energies=np.zeros(len(t)), z_factors=np.zeros(len(t)), sigma_c=np.zeros(len(t)),
+                   sigma_x=np.zeros(len(t)))
+        keep += [lpq, e, vx, t]
+        outs.append(out)
+        arr[i] = N.CdSystem(N.ptr(e), N.ptr(lpq), N.ptr(vx), nmo, int(s["nocc"]), naux, N.ptr(t), len(t),
+                            N.ptr(out["qp_energies"]), N.ptr(out["z_factors"]), N.ptr(out["sigma_c"]),
+                            N.ptr(out["sigma_x"]), -1)
+    ctx.check(ctx.lib.qx_g0w0_cd_batch(ctx.handle, arr, len(systems), int(nw), float(x0), float(tol), int(max_iter),
+                                       _qp_solver(qp_solver), _prec(precision), int(nworkers)))
+    return outs

@@ -133,3 +133,27 @@ def grad_nmo200() -> SyntheticSystem:
 def bse_dim26400_bov() -> SyntheticSystem:
     """nocc 60, nvirt 440, naux 1800, seed 11, ||Pi(0)|| = 5 (full tensor is 3.6 GB)."""
     return make_system(60, 440, 1800, seed=11, pi_norm=5.0)
+
+
+def make_system_device(nocc: int, nvir: int, naux: int, seed: int, pi_norm: float, device: int = 0):
+    """The same distributions as :func:`make_system`, drawn on the GPU with
+    torch's seeded device generator (the draws differ from numpy's).  Returns
+    (mo_energy, lpq) as CUDA float64 tensors.  Used where the host draw is too
+    slow (the 64-system batch holds ~32 GB of lpq)."""
+    import torch
+    dev = torch.device("cuda", device)
+    g = torch.Generator(device=dev)
+    g.manual_seed(seed)
+    nmo = nocc + nvir
+    kw = dict(generator=g, device=dev, dtype=torch.float64)
+    e_occ = torch.sort(torch.rand(nocc, **kw) * 0.9 - 1.2).values
+    e_vir = torch.sort(torch.rand(nvir, **kw) * 2.95 + 0.05).values
+    e = torch.cat([e_occ, e_vir])
+    lpq = torch.randn(naux, nmo, nmo, **kw) * 0.05
+    lpq = torch.triu(lpq) + torch.triu(lpq, 1).transpose(1, 2)
+    bov = lpq[:, :nocc, nocc:].reshape(naux, -1)
+    e_ia = (e[:nocc, None] - e[None, nocc:]).reshape(-1)
+    pi0 = 4.0 * (bov / e_ia) @ bov.T
+    norm = torch.linalg.eigvalsh(pi0).abs().max()
+    lpq *= torch.sqrt(pi_norm / norm)
+    return e.contiguous(), lpq.contiguous()

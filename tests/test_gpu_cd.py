@@ -87,3 +87,72 @@ def test_cd_medium_first_steps_with_vxc_zero(q):
         ref = O.g0w0_cd(s.mo_energy, s.lpq, 12, targets, 24, tol=1e-8, max_iter=it)
         assert np.abs(got["qp_energies"] - ref["qp_energies"]).max() < 1e-8
         assert np.abs(got["sigma_c"] - ref["sigma_c"]).max() < 1e-8 * max(1.0, np.abs(ref["sigma_c"]).max())
+
+
+def _batch_members():
+    """Small members of the 64-system batch family (nocc = round(nmo/6),
+    naux = round(3.5 nmo), HOMO-2..LUMO+2, HF reference Vxc = Sigma_x)."""
+    out = []
+    for nmo, seed, pin in [(40, 100, 1.5), (57, 101, 4.0), (72, 102, 2.5), (46, 103, 6.0), (88, 104, 3.0)]:
+        nocc = int(round(nmo / 6))
+        s = make_system(nocc, nmo - nocc, int(round(3.5 * nmo)), seed=seed, pi_norm=pin)
+        out.append(dict(mo_energy=s.mo_energy, lpq=s.lpq, nocc=nocc, targets=list(range(nocc - 3, nocc + 3)),
+                        vxc=_sx(s, nocc)))
+    return out
+
+
+def test_cd_batch_matches_oracle_and_single_calls(q):
+    """Damped Newton on strongly screened systems: targets the oracle brings to
+    |f| < tol within max_iter agree to 1e-8; a target still wandering among the
+    poles of Sigma after max_iter is compared by neither side.  The batch
+    reproduces the single-system calls exactly."""
+    systems = _batch_members()
+    got = q.g0w0_cd_batch(systems, nw=24, tol=1e-8, max_iter=50, nworkers=3)
+    nconv = ntot = 0
+    for s, g in zip(systems, got):
+        ref = O.g0w0_cd(s["mo_energy"], s["lpq"], s["nocc"], s["targets"], 24, vxc=s["vxc"], tol=1e-8, max_iter=50)
+        conv = ref["iterations"] < 50
+        nconv += int(conv.sum())
+        ntot += conv.size
+        if conv.any():
+            assert np.abs(g["qp_energies"] - ref["qp_energies"])[conv].max() < 1e-8
+            assert np.abs(g["z_factors"] - ref["z_factors"])[conv].max() < 1e-6
+        one = q.g0w0_cd(s["mo_energy"], s["lpq"], s["nocc"], s["targets"], nw=24, vxc=s["vxc"], tol=1e-8, max_iter=50)
+        assert np.abs(g["qp_energies"] - one["qp_energies"]).max() < 1e-12
+    assert 2 * nconv >= ntot, (nconv, ntot)  # the comparison covers at least half the targets
+
+
+def test_cd_linearized_matches_oracle(q):
+    """One evaluation at e_n and the linearized QP step (batched G0W0)."""
+    systems = _batch_members()
+    got = q.g0w0_cd_batch(systems, nw=24, qp_solver="linearized", nworkers=2)
+    for s, g in zip(systems, got):
+        ref = O.g0w0_cd(s["mo_energy"], s["lpq"], s["nocc"], s["targets"], 24, vxc=s["vxc"], qp_solver="linearized")
+        assert np.abs(g["qp_energies"] - ref["qp_energies"]).max() < 1e-8
+        assert np.abs(g["sigma_c"] - ref["sigma_c"]).max() < 1e-8
+        assert np.abs(g["z_factors"] - ref["z_factors"]).max() < 1e-8
+
+
+@pytest.mark.parametrize("precision", ["fp16x3", "bf16x3"])
+def test_cd_batch_mixed_precision_within_one_mev(q, precision):
+    systems = _batch_members()
+    ref = q.g0w0_cd_batch(systems, nw=24, nworkers=2, qp_solver="linearized")
+    got = q.g0w0_cd_batch(systems, nw=24, nworkers=2, precision=precision, qp_solver="linearized")
+    err_mev = max(np.abs(g["qp_energies"] - r["qp_energies"]).max() for g, r in zip(got, ref)) * 27211.386
+    assert err_mev < 1.0, err_mev
+
+
+def test_cd_batch_device_inputs_and_per_system_status(q):
+    import torch
+    from quasix_b200._native import QxValueError
+    systems = _batch_members()[:3]
+    host = q.g0w0_cd_batch(systems, nw=16, tol=1e-8)
+    dev = [dict(s, lpq=torch.from_numpy(s["lpq"]).cuda(), mo_energy=torch.from_numpy(s["mo_energy"]).cuda())
+           for s in systems]
+    got = q.g0w0_cd_batch(dev, nw=16, tol=1e-8)
+    for g, h in zip(got, host):
+        assert np.abs(g["qp_energies"] - h["qp_energies"]).max() < 1e-12
+    bad = [dict(s) for s in systems]
+    bad[1]["targets"] = [0, 10_000]
+    with pytest.raises(QxValueError, match="system 1"):
+        q.g0w0_cd_batch(bad, nw=16, tol=1e-8)
