@@ -44,6 +44,7 @@ def parse():
     p.add_argument("--precision", choices=["fp16x3", "bf16x3", "fp64"], default=None)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-batch64", action="store_true")
+    p.add_argument("--no-grad", action="store_true")
     p.add_argument("--batch-workers", type=int, default=4)
     return p.parse_args()
 
@@ -247,6 +248,76 @@ def bench_batch64(q, dev, precision, steps, warmup, nworkers):
             "data": "synthetic, drawn on the device (torch generator, seeds 100-163)"}
 
 
+def bench_grad_nmo200(q, dev, precision, steps=3, warmup=1):
+    """Differentiation workload: nocc 30, nvirt 170, naux 700, seed 7, 24-point
+    grid, L = E_QP(HOMO) + E_QP(LUMO) by the CD Newton root, gradient with
+    respect to all orbital energies and lpq by the adjoint (P0/W rebuilt per
+    frequency).  Vxc is held fixed at values that put the roots 0.05 Ha inside
+    the gap.  One step = forward root + adjoint.  Also reports the max-norm
+    relative deviation from FP64 central differences at 8 seeded coordinates."""
+    import torch
+    from quasix_b200.synth import make_system
+    s = make_system(30, 170, 700, seed=7, pi_norm=2.0)
+    nocc, tg, nw = 30, [29, 30], 24
+    e_d = torch.from_numpy(s.mo_energy.copy()).to(f"cuda:{dev}")
+    l_d = torch.from_numpy(s.lpq.copy()).to(f"cuda:{dev}")
+    target = np.array([s.mo_energy[29] + 0.05, s.mo_energy[30] - 0.05])
+    cs = q.cd_sigma(e_d, l_d, nocc, tg, target, nw=nw, device=dev)
+    vxc = np.asarray(q.compute_exchange_diag(l_d, nocc, device=dev))
+    vxc[tg] = cs["sigma_x"] + cs["sigma_c"] - (target - s.mo_energy[tg])
+    v_d = torch.from_numpy(vxc).to(f"cuda:{dev}")
+
+    def step(prec, e=e_d, lpq=l_d, tol=1e-13, grad=True):
+        r = q.g0w0_cd(e, lpq, nocc, tg, nw=nw, vxc=v_d, tol=tol, max_iter=100, precision=prec, device=dev)
+        if not grad:
+            return float(r["qp_energies"].sum())
+        return q.g0w0_cd_grad(e, lpq, nocc, tg, r["qp_energies"], [1.0, 1.0], nw=nw, precision=prec, device=dev)
+
+    out = {"workload": "g0w0_cd_grad_nmo200_naux700_nw24", "loss": "E_QP(HOMO) + E_QP(LUMO)", "steps": steps,
+           "vxc": "fixed; roots 0.05 Ha inside the gap"}
+    grads = {}
+    for prec in (precision, "fp64"):
+        for _ in range(warmup):
+            step(prec)
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        ev0.record()
+        for _ in range(steps):
+            g = step(prec)
+        ev1.record()
+        torch.cuda.synchronize()
+        grads[prec] = (g[0].cpu().numpy(), g[1].cpu().numpy())
+        out[("" if prec == precision else "fp64_") + "ms_per_gradient"] = ev0.elapsed_time(ev1) / steps
+    out["precision"] = precision
+    out["speedup_vs_fp64_gpu"] = out["fp64_ms_per_gradient"] / out["ms_per_gradient"]
+    rng = np.random.default_rng(7)
+    ge64, gl64 = grads["fp64"]
+    fd, an = [], {precision: [], "fp64": []}
+    for p in rng.choice(200, 4, replace=False):
+        ep, em = e_d.clone(), e_d.clone()
+        ep[p] += 1e-5
+        em[p] -= 1e-5
+        fd.append((step("fp64", e=ep, grad=False) - step("fp64", e=em, grad=False)) / 2e-5)
+        for k in an:
+            an[k].append(grads[k][0][p])
+    mag = np.abs(gl64)
+    cand = np.argwhere(mag > 1e-3 * mag.max())
+    for k in rng.choice(len(cand), 4, replace=False):
+        P, a, b = (int(v) for v in cand[k])
+        d = torch.zeros_like(l_d)
+        d[P, a, b] += 1e-6
+        if a != b:
+            d[P, b, a] += 1e-6
+        fd.append((step("fp64", lpq=l_d + d, grad=False) - step("fp64", lpq=l_d - d, grad=False)) / 2e-6)
+        for kk in an:
+            an[kk].append(grads[kk][1][P, a, b] * (2 if a != b else 1))
+    fd = np.array(fd)
+    for k in an:
+        key = ("" if k == precision else "fp64_") + "fd_max_rel_err"
+        out[key] = float(np.abs(np.array(an[k]) - fd).max() / np.abs(fd).max())
+    return out
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -403,6 +474,8 @@ def main():
             "max_qp_err_meV_per_iteration": err_iter, "fp64_perturbation_1e-14_meV_per_iteration": sens_iter,
             "stage_ms_per_step": {k: v / args.steps for k, v in stage.items()},
             "roofline": roof, "clocks": clocks, "e2e": e2e, "gpu_launches": launches}
+    if not args.no_grad:
+        line["grad_nmo200"] = bench_grad_nmo200(q, dev, prec_main)
     if not args.no_batch64:
         line["batch64_g0w0_cd"] = bench_batch64(q, dev, prec_main, steps=1, warmup=1, nworkers=args.batch_workers)
     if rank == 0 and not args.no_cpu_baseline:

@@ -185,6 +185,15 @@ qx_status qx_g0w0_cd(qx_ctx* ctx, const double* mo_energy, const double* lpq, co
                      int max_iter, int qp_solver, int precision, double* qp_energies, double* z_factors,
                      double* sigma_c, double* sigma_x);
 
+/* Sigma_c^CD_n(w) and its slope dSigma/dw at caller-given real energies
+ * omega[t] for each target (compute_sigma_c_pyscf_cd,
+ * correlation_pyscf_cd.rs:164-259, which evaluates the imaginary-axis term at
+ * one energy; here with the residues).  sigma_x receives diag(Sigma_x) of the
+ * targets (may be NULL, as may dsigma_c). */
+qx_status qx_cd_sigma(qx_ctx* ctx, const double* mo_energy, const double* lpq, int nmo, int nocc, int naux,
+                      const int* targets, int ntarget, const double* omega, int nw, double x0, int precision,
+                      double* sigma_c, double* dsigma_c, double* sigma_x);
+
 /* Many independent G0W0-CD systems of uneven size in one call (no reference
  * counterpart: the reference runs compute_sigma_c_pyscf_cd once per system).
  * Each system is the argument set of qx_g0w0_cd; the library runs them on
@@ -208,6 +217,22 @@ typedef struct {
 
 qx_status qx_g0w0_cd_batch(qx_ctx* ctx, qx_cd_system* systems, int nsys, int nw, double x0, double tol,
                            int max_iter, int qp_solver, int precision, int nworkers);
+
+/* Adjoint of the CD QP roots (no reference counterpart: QuasiX has no
+ * derivative code).  Given the roots qp_energies[t] of f_t(E) = E - e_n - Sx_n
+ * - Sigma^CD_n(E) + Vxc_n (as returned by qx_g0w0_cd with Newton; Vxc is held
+ * fixed) and weights dl_dqp[t], returns the gradient of L = sum_t dl_dqp[t]
+ * E_t with respect to mo_energy (grad_energy [nmo]) and the symmetric tensor
+ * lpq (grad_lpq [naux][nmo][nmo], symmetric: dL = sum grad_lpq * dlpq for
+ * every symmetric dlpq).  Implicit differentiation with Z_t = 1/(1 -
+ * dSigma/dE) (unclipped, written to z_raw [ntarget] when non-NULL); P0 and W
+ * are rebuilt per frequency, not stored.  precision selects the P0 rebuild
+ * (FP64 or the split tcgen05 form); the adjoint GEMMs run in FP64.
+ * grad_energy or grad_lpq may be NULL (not both); targets must be distinct. */
+qx_status qx_g0w0_cd_grad(qx_ctx* ctx, const double* mo_energy, const double* lpq, int nmo, int nocc, int naux,
+                          const int* targets, int ntarget, const double* qp_energies, const double* dl_dqp,
+                          int nw, double x0, int precision, double* grad_energy, double* grad_lpq,
+                          double* z_raw);
 
 /* ---- bse -------------------------------------------------------------------- */
 typedef struct qx_bse qx_bse;

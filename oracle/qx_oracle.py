@@ -915,6 +915,86 @@ def g0w0_cd(mo_energy, lpq, nocc, targets, nw, x0=0.5, vxc=None, sigma_x=None,
                 iterations=iters)
 
 
+def g0w0_cd_grad(mo_energy, lpq, nocc, targets, qp, dl_dqp, nw, x0=0.5):
+    """Adjoint of the CD QP roots: gradient of L = sum_t dl_dqp[t] E_t with
+    respect to the orbital energies and the symmetric tensor lpq, where E_t
+    solves f_t(E) = E - e_n - Sx_n - Sigma_c^CD_n(E) + Vxc_n = 0 (Vxc held fixed).
+
+    Implicit differentiation: dE_t = Z_t (de_n + dSx_n + dSigma_n|_E) with
+    Z_t = 1 / (1 - dSigma_n/dE) unclipped, mu_t = dl_dqp[t] Z_t.  Sigma_n(E) =
+    I_n + R_n (sigma_cd); through Wc_nm = b^T (eps^-1 - I) b with
+    eps = I + B diag(chi) B^T, chi = -4 e_ia/(w^2 + e_ia^2) (imaginary axis) or
+    -4 e_ia/(e_ia^2 - w^2) (residue shifts):
+      dL/db_nm = 2 c (x - b),   dL/deps = G = -sum c x x^T,   x = eps^-1 b,
+      dL/dB_ov = 2 G B_ov diag(chi),   dL/dchi_ia = b_ia^T G b_ia,
+    with c the coefficient of Wc_nm in mu_t Sigma_n.  The residue shifts
+    w_r = s_r (E - e_m) contribute -mu_t dWc_r/dw to e_m.  P0 and W are rebuilt
+    per frequency.  Returns (grad_e [nmo], grad_lpq [naux, nmo, nmo] symmetric:
+    dL = sum grad_lpq * dlpq for every symmetric dlpq)."""
+    naux, nmo, _ = lpq.shape
+    nvir = nmo - nocc
+    freqs, wts = get_scaled_legendre_roots(nw, x0)
+    B = np.ascontiguousarray(lpq[:, :nocc, nocc:]).reshape(naux, -1)
+    e_ia = (mo_energy[:nocc, None] - mo_energy[None, nocc:]).reshape(-1)
+    wci = wc_pairs_imag(mo_energy, lpq, nocc, targets, freqs)
+    mu = np.zeros(len(targets))
+    for t, n in enumerate(targets):
+        _, ds = sigma_cd(qp[t], n, mo_energy, lpq, nocc, freqs, wts, wci[:, t])
+        mu[t] = dl_dqp[t] / (1.0 - ds)
+    g_e = np.zeros(nmo)
+    g_l = np.zeros_like(lpq)
+    g_b = np.zeros_like(B)
+    g_eia = np.zeros_like(e_ia)
+    for t, n in enumerate(targets):
+        g_e[n] += mu[t]
+        g_l[:, n, :nocc] += -2.0 * mu[t] * lpq[:, n, :nocc]
+    eye = np.eye(naux)
+    for k, f in enumerate(freqs):
+        chi = -4.0 * e_ia / (f * f + e_ia * e_ia)
+        dchi = -4.0 * (f * f - e_ia * e_ia) / (f * f + e_ia * e_ia) ** 2
+        inv = np.linalg.inv(eye + (B * chi) @ B.T)
+        G = np.zeros((naux, naux))
+        for t, n in enumerate(targets):
+            xr = qp[t] - mo_energy
+            den = xr * xr + f * f
+            c = mu[t] * (-1.0 / PI) * wts[k] * xr / den
+            g_e += mu[t] * (1.0 / PI) * wts[k] * wci[k, t] * (f * f - xr * xr) / den ** 2
+            bn = lpq[:, n, :]
+            X = inv @ bn
+            g_l[:, n, :] += 2.0 * c[None, :] * (X - bn)
+            G -= (X * c[None, :]) @ X.T
+        H = G @ B
+        g_eia += np.sum(B * H, axis=0) * dchi
+        g_b += 2.0 * H * chi[None, :]
+    for t, n in enumerate(targets):
+        E = qp[t]
+        for m in range(nmo):
+            em = mo_energy[m]
+            if m < nocc and em > E:
+                sgn, w = -1.0, em - E
+            elif m >= nocc and em < E:
+                sgn, w = 1.0, E - em
+            else:
+                continue
+            chi = -4.0 * e_ia / (e_ia * e_ia - w * w)
+            dchi_de = 4.0 * (e_ia * e_ia + w * w) / (e_ia * e_ia - w * w) ** 2
+            b = lpq[:, n, m]
+            x = np.linalg.solve(eye + (B * chi) @ B.T, b)
+            tv = B.T @ x
+            dwc = float(4.0 * np.sum(e_ia * 2.0 * w / (e_ia * e_ia - w * w) ** 2 * tv * tv))
+            c = mu[t] * sgn
+            g_e[m] += -mu[t] * dwc
+            g_l[:, n, m] += 2.0 * c * (x - b)
+            g_eia += -c * tv * tv * dchi_de
+            g_b += -2.0 * c * np.outer(x, tv * chi)
+    ge = g_eia.reshape(nocc, nvir)
+    g_e[:nocc] += ge.sum(axis=1)
+    g_e[nocc:] -= ge.sum(axis=0)
+    g_l[:, :nocc, nocc:] += g_b.reshape(naux, nocc, nvir)
+    g_l = 0.5 * (g_l + g_l.transpose(0, 2, 1))
+    return g_e, g_l
+
+
 # ---------------------------------------------------------------------------
 # a11-a13: BSE-TDA
 # ---------------------------------------------------------------------------

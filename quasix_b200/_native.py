@@ -96,6 +96,10 @@ SIGNATURES = {
                              C.c_double, C.c_int, C.c_int, C.c_int, _vp, _vp, _vp, _vp]),
     "qx_g0w0_cd_batch": (C.c_int, [_vp, C.POINTER(CdSystem), C.c_int, C.c_int, C.c_double, C.c_double, C.c_int,
                                    C.c_int, C.c_int, C.c_int]),
+    "qx_cd_sigma": (C.c_int, [_vp, _vp, _vp, C.c_int, C.c_int, C.c_int, _vp, C.c_int, _vp, C.c_int, C.c_double,
+                              C.c_int, _vp, _vp, _vp]),
+    "qx_g0w0_cd_grad": (C.c_int, [_vp, _vp, _vp, C.c_int, C.c_int, C.c_int, _vp, C.c_int, _vp, _vp, C.c_int,
+                                  C.c_double, C.c_int, _vp, _vp, _vp]),
     "qx_bse_create": (C.c_int, [_vp, C.POINTER(_vp), C.c_int, C.c_int, C.c_int, _vp, _vp, _vp, _vp, _vp, C.c_int,
                                 C.c_int]),
     "qx_bse_destroy": (C.c_int, [_vp]),

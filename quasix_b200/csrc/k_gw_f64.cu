@@ -316,11 +316,11 @@ __global__ void k_finish_wc(double* __restrict__ M, int n, int ldn, size_t strid
 void launch_invert_wc(qx_ctx* ctx, double* eps, int n, int ldn, size_t stride, int nw, int half_lower) {
   const size_t pstride = (size_t)n * SWEEP_NB;
   DevBuf& pan = ctx->ws[WS_PANEL];
-  const size_t need = (pstride * nw + (size_t)nw * SWEEP_NB * SWEEP_NB) * sizeof(double) + nw * sizeof(int) + 256;
+  const size_t need = (pstride * nw + (size_t)nw * SWEEP_NB * SWEEP_NB) * sizeof(double) + 256;
   pan.reserve(need);
   double* Tp = pan.as<double>();
   double* Dp = Tp + pstride * nw;
-  int* status = reinterpret_cast<int*>(Dp + (size_t)nw * SWEEP_NB * SWEEP_NB);
+  int* status = status_words(ctx, nw);
   QX_CUDA(cudaMemsetAsync(status, 0, nw * sizeof(int), ctx->stream));
   const int diag_smem = (SWEEP_NB * SWEEP_NB + SWEEP_NB * 33) * sizeof(double);
   static std::once_flag attr_once;

@@ -570,11 +570,8 @@ void launch_split(qx_ctx* ctx, const double* src, int rows, int cols, int ld_src
         scale_out);
 }
 
-static int* tc_err_slot(qx_ctx* ctx, int which) {
-  DevBuf& b = ctx->ws[WS_TCERR];
-  b.reserve(256);
-  return b.as<int>() + which;
-}
+// One error word per launch, from the context's status arena.
+static int* tc_err_slot(qx_ctx* ctx) { return status_words(ctx, 1); }
 
 static void check_tc_err(qx_ctx* ctx, int* d_err) { ctx->pending.push_back({d_err, 1, 0}); }
 
@@ -600,7 +597,7 @@ void launch_pair_contract_tc(qx_ctx* ctx, const TcOperand& A, const float* bpt_f
   CUtensorMap al = make_map(A.lo, naux, npair, ldk, 1, TC_BM, 2, fp16);
   CUtensorMap bh = make_map(W.hi, naux, naux, ldw, nw, BN, 3, fp16);
   CUtensorMap bl = make_map(W.lo, naux, naux, ldw, nw, BN, 3, fp16);
-  int* d_err = tc_err_slot(ctx, 0);
+  int* d_err = tc_err_slot(ctx);
   QX_CUDA(cudaMemsetAsync(d_err, 0, sizeof(int), ctx->stream));
   TcArgs a{};
   a.M = npair;
@@ -642,7 +639,7 @@ void launch_eps_tc(qx_ctx* ctx, const double* bov, int ldov, int naux, int nov, 
   CUtensorMap al = make_map(a_lo, nov, naux, ldov, 1, TC_BM, 2, fp16);
   CUtensorMap bh = make_map(b_hi, nov, naux, ldov, nw, BN, 3, fp16);
   CUtensorMap bl = make_map(b_lo, nov, naux, ldov, nw, BN, 3, fp16);
-  int* d_err = tc_err_slot(ctx, 1);
+  int* d_err = tc_err_slot(ctx);
   QX_CUDA(cudaMemsetAsync(d_err, 0, sizeof(int), ctx->stream));
   TcArgs a{};
   a.M = naux;

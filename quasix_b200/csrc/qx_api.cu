@@ -209,8 +209,19 @@ void gw_setup(qx_ctx* ctx, GWSystem& S, const double* d_lpq, int nmo, int nocc, 
   }
 }
 
+int* status_words(qx_ctx* ctx, int n) {
+  constexpr int kCap = 1 << 16;
+  QX_REQUIRE(n > 0 && n <= kCap, QX_ERR_INVALID_INPUT, "%d status words requested", n);
+  if (!ctx->status_arena.ptr) ctx->status_arena.reserve(kCap * sizeof(int));
+  if (ctx->status_used + n > kCap) sync_and_check(ctx);
+  int* p = ctx->status_arena.as<int>() + ctx->status_used;
+  ctx->status_used += n;
+  return p;
+}
+
 void sync_and_check(qx_ctx* ctx) {
   QX_CUDA(cudaStreamSynchronize(ctx->stream));
+  ctx->status_used = 0;
   std::vector<qx_ctx::Pending> pend;
   pend.swap(ctx->pending);
   for (const auto& pd : pend) {
@@ -407,7 +418,7 @@ template <class F>
 static qx_status guarded(qx_ctx* ctx, F&& f) {
   try {
     if (ctx) {
-      ctx->pending.clear();
+      reset_pending(ctx);
       ctx->launches = 0;
       for (double& v : ctx->stage_ms) v = 0.0;
       QX_CUDA(cudaSetDevice(ctx->device));

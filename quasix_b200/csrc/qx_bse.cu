@@ -261,7 +261,7 @@ static void bse_apply_rows(qx_bse* B, const double* X, double* Y, int nvec) {
 template <class F>
 static qx_status bse_guard(qx_ctx* ctx, F&& f) {
   try {
-    ctx->pending.clear();
+    reset_pending(ctx);
     ctx->launches = 0;
     QX_CUDA(cudaSetDevice(ctx->device));
     f();

@@ -18,9 +18,7 @@
 #include <mutex>
 #include <thread>
 
-#include "qx_blas.cuh"
-#include "qx_gw_sys.cuh"
-#include "qx_internal.cuh"
+#include "qx_cd.cuh"
 
 namespace qx {
 
@@ -116,6 +114,160 @@ __global__ void k_cd_dres(const double* __restrict__ tmat, int ldt, const double
   if (threadIdx.x == 0) out[r] = 4.0 * red[0];
 }
 
+void launch_cd_gather(qx_ctx* ctx, const double* lpq, int naux, int nmo, const int2* nm, int R, double* b, int ld) {
+  dim3 gg(ceil_div(ld, 256), R);
+  k_cd_gather<<<gg, 256, 0, ctx->stream>>>(lpq, naux, nmo, nm, R, b, ld);
+  check_launch(ctx);
+}
+
+void CdEngine::setup(const double* mo_energy, const double* lpq, const int* targets, int ntarget_, int nmo_,
+                     int nocc_, int naux_, int nw_, double x0, int precision_) {
+  nmo = nmo_;
+  nocc = nocc_;
+  naux = naux_;
+  ntarget = ntarget_;
+  nw = nw_;
+  precision = precision_;
+  QX_REQUIRE(mo_energy && lpq && targets && ntarget > 0 && nw > 0, QX_ERR_INVALID_INPUT, "invalid CD arguments");
+  validate_common(nmo, nocc, naux);
+  nvir = nmo - nocc;
+  nov = nocc * nvir;
+  tc = is_tc_precision(precision);
+  e.assign(nmo, 0.0);
+  QX_CUDA(cudaMemcpy(e.data(), mo_energy, nmo * sizeof(double), cudaMemcpyDefault));
+  tg.assign(ntarget, 0);
+  QX_CUDA(cudaMemcpy(tg.data(), targets, ntarget * sizeof(int), cudaMemcpyDefault));
+  for (int t : tg) QX_REQUIRE(t >= 0 && t < nmo, QX_ERR_INVALID_INPUT, "target orbital %d out of range", t);
+  d_lpq = (const double*)device_view(ctx, WS_LPQ, lpq, (size_t)naux * nmo * nmo * sizeof(double));
+  // Imaginary axis: Wc_nm(i f_k) for the target pairs (no cutoff: the sigma grid is unused).
+  gw_setup(ctx, S, d_lpq, nmo, nocc, naux, tg, nw, 1e300, x0, precision);
+  gw_wc_pairs(ctx, S, e.data());
+  ldn = S.ldn;
+  DevBuf& cb = ctx->ws[WS_CD0];
+  cb.reserve((size_t)(nmo + 4 * ntarget + 64) * sizeof(double));
+  double* d_sx = cb.as<double>();
+  d_om = d_sx + nmo;
+  d_imag = d_om + ntarget;
+  launch_exchange_diag(ctx, d_lpq, naux, nmo, nocc, d_sx);
+  sx.assign(nmo, 0.0);
+  QX_CUDA(cudaMemcpyAsync(sx.data(), d_sx, nmo * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  // B_ov^T [nov][ldn] for the residue derivatives.
+  DevBuf& bt = ctx->ws[WS_CD1];
+  bt.reserve((size_t)nov * ldn * sizeof(double));
+  bovT = bt.as<double>();
+  QX_CUDA(cudaMemsetAsync(bovT, 0, (size_t)nov * ldn * sizeof(double), ctx->stream));
+  transpose(ctx, S.bov, naux, nov, S.ldov, 0, bovT, ldn, 0, 1);
+  om.assign(ntarget, 0.0);
+  sig.assign(ntarget, 0.0);
+  dsig.assign(ntarget, 0.0);
+  for (int t = 0; t < ntarget; ++t) om[t] = e[tg[t]];
+}
+
+std::vector<CdResidue> CdEngine::residues(const std::vector<int>& act) const {
+  std::vector<CdResidue> out;
+  for (int t : act) {
+    for (int m = 0; m < nmo; ++m) {
+      if (m < nocc && e[m] > om[t])
+        out.push_back({t, m, -1.0, e[m] - om[t]});
+      else if (m >= nocc && e[m] < om[t])
+        out.push_back({t, m, 1.0, om[t] - e[m]});
+    }
+  }
+  return out;
+}
+
+CdResidueChunk CdEngine::residue_buffers(int R) {
+  // Chunks of RC frequencies keep the eps matrices (and, for the split forms,
+  // the split operands) within ~2 GB.
+  const size_t stride = (size_t)naux * ldn;
+  const size_t per_res = (stride + S.ldov) * sizeof(double) + (tc ? (size_t)naux * S.ldov * 4 : 0);
+  const int RC = (int)std::max<size_t>(1, std::min<size_t>((size_t)std::max(R, 1), ((size_t)2 << 30) / per_res));
+  DevBuf& rb = ctx->ws[WS_CD2];
+  rb.reserve((size_t)RC * (stride + 2 * ldn + S.ldov + 4) * sizeof(double) + RC * sizeof(int2) + 1024);
+  CdResidueChunk c;
+  c.cap = RC;
+  c.eps = rb.as<double>();
+  c.b = c.eps + (size_t)RC * stride;
+  c.x = c.b + (size_t)RC * ldn;
+  c.tm = c.x + (size_t)RC * ldn;
+  c.wr = c.tm + (size_t)RC * S.ldov;
+  c.val = c.wr + RC;
+  c.dv = c.val + RC;
+  c.nm = reinterpret_cast<int2*>(c.dv + RC + 1);
+  ctx->ws[WS_CD3].reserve((size_t)RC * S.ldov * sizeof(double));
+  c.chi = ctx->ws[WS_CD3].as<double>();
+  return c;
+}
+
+void CdEngine::residue_compute(CdResidueChunk& c, const CdResidue* list, int rc) {
+  const size_t stride = (size_t)naux * ldn;
+  std::vector<double> wr(rc);
+  std::vector<int2> nm(rc);
+  for (int r = 0; r < rc; ++r) {
+    wr[r] = list[r].w;
+    nm[r] = make_int2(tg[list[r].t], list[r].m);
+  }
+  QX_CUDA(cudaMemcpyAsync(c.wr, wr.data(), rc * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  QX_CUDA(cudaMemcpyAsync(c.nm, nm.data(), rc * sizeof(int2), cudaMemcpyHostToDevice, ctx->stream));
+  // eps(w_r) = I + B_ov diag(chi'(w_r)) B_ov^T, real axis.
+  launch_chi(ctx, S.d_en, nocc, nvir, c.wr, rc, 1, c.chi, S.ldov);
+  if (tc)
+    launch_eps_tc(ctx, S.bov, S.ldov, naux, nov, c.chi, rc, c.eps, ldn, stride, precision == QX_PREC_FP16X3);
+  else
+    launch_eps_fp64(ctx, S.bov, S.ldov, naux, nov, c.chi, rc, c.eps, ldn, stride);
+  launch_invert_wc(ctx, c.eps, naux, ldn, stride, rc);
+  launch_cd_gather(ctx, d_lpq, naux, nmo, c.nm, rc, c.b, ldn);
+  k_cd_quad<<<rc, 256, 0, ctx->stream>>>(c.eps, ldn, stride, c.b, naux, ldn, c.x, c.val);
+  check_launch(ctx);
+  GemmNT g{};
+  g.M = rc;
+  g.N = nov;
+  g.K = naux;
+  g.A = c.x;
+  g.lda = ldn;
+  g.B = bovT;
+  g.ldb = ldn;
+  g.C = c.tm;
+  g.ldc = S.ldov;
+  g.batch = 1;
+  g.alpha = 1.0;
+  g.splitk = 0;
+  gemm_nt_f64(ctx, g);
+  k_cd_dres<<<rc, 256, 0, ctx->stream>>>(c.tm, S.ldov, S.d_en, nocc, nvir, c.wr, c.dv);
+  check_launch(ctx);
+}
+
+void CdEngine::evaluate(const std::vector<int>& act) {
+  // Imaginary-axis part for every target.
+  QX_CUDA(cudaMemcpyAsync(d_om, om.data(), ntarget * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  k_cd_imag<<<ntarget, 256, 0, ctx->stream>>>(S.v, S.npair, nw, S.d_pidx, nmo, S.d_en, S.d_freqs, S.d_wts, d_om,
+                                               d_imag);
+  check_launch(ctx);
+  std::vector<double> hi(2 * ntarget);
+  QX_CUDA(cudaMemcpyAsync(hi.data(), d_imag, 2 * ntarget * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  const std::vector<CdResidue> res = residues(act);
+  const int R = (int)res.size();
+  std::vector<double> rv(R), rd(R);
+  if (R > 0) {
+    CdResidueChunk c = residue_buffers(R);
+    for (int c0 = 0; c0 < R; c0 += c.cap) {
+      const int rc = std::min(c.cap, R - c0);
+      residue_compute(c, res.data() + c0, rc);
+      QX_CUDA(cudaMemcpyAsync(rv.data() + c0, c.val, rc * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+      QX_CUDA(cudaMemcpyAsync(rd.data() + c0, c.dv, rc * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    }
+  }
+  sync_and_check(ctx);
+  for (int t : act) {
+    sig[t] = hi[2 * t];
+    dsig[t] = hi[2 * t + 1];
+  }
+  for (int r = 0; r < R; ++r) {
+    sig[res[r].t] += res[r].sgn * rv[r];
+    dsig[res[r].t] += rd[r];
+  }
+}
+
 // One G0W0-CD problem (the arguments of qx_g0w0_cd).
 struct CdProblem {
   const double* mo_energy;
@@ -129,152 +281,32 @@ struct CdProblem {
   double *qp, *z, *sc, *sx;
 };
 
-// Runs one system on ctx (throws qx::Error).  Imaginary-axis Wc for the target
-// pairs once, then Newton steps; each evaluation adds the residues of the
-// poles between the target energy and the Fermi level.
+// Runs one system on ctx (throws qx::Error): imaginary-axis Wc for the target
+// pairs once, then QP steps; each evaluation adds the residues of the poles
+// between the target energy and the Fermi level.
 void g0w0_cd_run(qx_ctx* ctx, const CdProblem& p) {
-  const int nmo = p.nmo, nocc = p.nocc, naux = p.naux, ntarget = p.ntarget, nw = p.nw;
-  QX_REQUIRE(p.mo_energy && p.lpq && p.targets && p.qp && ntarget > 0 && nw > 0 && p.max_iter > 0,
-             QX_ERR_INVALID_INPUT, "invalid arguments to g0w0_cd");
+  QX_REQUIRE(p.qp && p.max_iter > 0, QX_ERR_INVALID_INPUT, "invalid arguments to g0w0_cd");
   QX_REQUIRE(p.qp_solver == QX_QP_NEWTON || p.qp_solver == QX_QP_LINEARIZED, QX_ERR_INVALID_INPUT,
              "qp_solver %d", p.qp_solver);
-  validate_common(nmo, nocc, naux);
-  const int nvir = nmo - nocc;
-  std::vector<double> e(nmo), vx(nmo, 0.0);
-  QX_CUDA(cudaMemcpy(e.data(), p.mo_energy, nmo * sizeof(double), cudaMemcpyDefault));
-  if (p.vxc) QX_CUDA(cudaMemcpy(vx.data(), p.vxc, nmo * sizeof(double), cudaMemcpyDefault));
-  std::vector<int> tg(ntarget);
-  QX_CUDA(cudaMemcpy(tg.data(), p.targets, ntarget * sizeof(int), cudaMemcpyDefault));
-  for (int t : tg) QX_REQUIRE(t >= 0 && t < nmo, QX_ERR_INVALID_INPUT, "target orbital %d out of range", t);
-  const double* d_lpq = (const double*)device_view(ctx, WS_LPQ, p.lpq, (size_t)naux * nmo * nmo * sizeof(double));
-  const bool tc = is_tc_precision(p.precision);
-  // Imaginary axis: Wc_nm(i f_k) for the target pairs (no cutoff: the sigma grid is unused).
-  GWSystem S;
-  gw_setup(ctx, S, d_lpq, nmo, nocc, naux, tg, nw, 1e300, p.x0, p.precision);
-  gw_wc_pairs(ctx, S, e.data());
-  // Exchange.
-  DevBuf& cb = ctx->ws[WS_CD0];
-  cb.reserve((size_t)(nmo + 4 * ntarget + 64) * sizeof(double));
-  double* d_sx = cb.as<double>();
-  double* d_om = d_sx + nmo;
-  double* d_imag = d_om + ntarget;
-  launch_exchange_diag(ctx, d_lpq, naux, nmo, nocc, d_sx);
-  std::vector<double> sx(nmo);
-  QX_CUDA(cudaMemcpyAsync(sx.data(), d_sx, nmo * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-  // B_ov^T [nov][ldn] for the residue derivatives.
-  const int nov = nocc * nvir, ldn = S.ldn;
-  DevBuf& bt = ctx->ws[WS_CD1];
-  bt.reserve((size_t)nov * ldn * sizeof(double));
-  double* bovT = bt.as<double>();
-  QX_CUDA(cudaMemsetAsync(bovT, 0, (size_t)nov * ldn * sizeof(double), ctx->stream));
-  transpose(ctx, S.bov, naux, nov, S.ldov, 0, bovT, ldn, 0, 1);
-  std::vector<double> om(ntarget), sig(ntarget, 0.0), dsig(ntarget, 0.0);
-  for (int t = 0; t < ntarget; ++t) om[t] = e[tg[t]];
-  auto evaluate = [&](const std::vector<int>& act) {
-    // Imaginary-axis part for every target.
-    QX_CUDA(cudaMemcpyAsync(d_om, om.data(), ntarget * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
-    k_cd_imag<<<ntarget, 256, 0, ctx->stream>>>(S.v, S.npair, nw, S.d_pidx, nmo, S.d_en, S.d_freqs, S.d_wts, d_om,
-                                                 d_imag);
-    check_launch(ctx);
-    std::vector<double> hi(2 * ntarget);
-    QX_CUDA(cudaMemcpyAsync(hi.data(), d_imag, 2 * ntarget * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-    // Residue list.
-    std::vector<int2> nm;
-    std::vector<double> wr, sgn;
-    std::vector<int> owner;
-    for (int t : act) {
-      const int n = tg[t];
-      for (int m = 0; m < nmo; ++m) {
-        if (m < nocc && e[m] > om[t]) {
-          nm.push_back(make_int2(n, m));
-          wr.push_back(e[m] - om[t]);
-          sgn.push_back(-1.0);
-          owner.push_back(t);
-        } else if (m >= nocc && e[m] < om[t]) {
-          nm.push_back(make_int2(n, m));
-          wr.push_back(om[t] - e[m]);
-          sgn.push_back(1.0);
-          owner.push_back(t);
-        }
-      }
-    }
-    const int R = (int)nm.size();
-    std::vector<double> rv(R), rd(R);
-    if (R > 0) {
-      // Residues in chunks of RC frequencies so that the eps matrices (and,
-      // for the split forms, the split operands) stay within ~2 GB.
-      const size_t stride = (size_t)naux * ldn;
-      const size_t per_res = (stride + S.ldov) * sizeof(double) + (tc ? (size_t)naux * S.ldov * 4 : 0);
-      const int RC = (int)std::max<size_t>(1, std::min<size_t>((size_t)R, ((size_t)2 << 30) / per_res));
-      DevBuf& rb = ctx->ws[WS_CD2];
-      const size_t need = (size_t)RC * (stride + 2 * ldn + S.ldov + 4) * sizeof(double) + RC * sizeof(int2) + 1024;
-      rb.reserve(need);
-      double* eps = rb.as<double>();
-      double* b = eps + (size_t)RC * stride;
-      double* x = b + (size_t)RC * ldn;
-      double* tm = x + (size_t)RC * ldn;
-      double* d_wr = tm + (size_t)RC * S.ldov;
-      double* d_val = d_wr + RC;
-      double* d_dv = d_val + RC;
-      int2* d_nm = reinterpret_cast<int2*>(d_dv + RC + 1);
-      ctx->ws[WS_CD3].reserve((size_t)RC * S.ldov * sizeof(double));
-      double* chi = ctx->ws[WS_CD3].as<double>();
-      for (int c0 = 0; c0 < R; c0 += RC) {
-        const int rc = std::min(RC, R - c0);
-        QX_CUDA(cudaMemcpyAsync(d_wr, wr.data() + c0, rc * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
-        QX_CUDA(cudaMemcpyAsync(d_nm, nm.data() + c0, rc * sizeof(int2), cudaMemcpyHostToDevice, ctx->stream));
-        // eps(w_r) = I + B_ov diag(chi'(w_r)) B_ov^T, real axis.
-        launch_chi(ctx, S.d_en, nocc, nvir, d_wr, rc, 1, chi, S.ldov);
-        if (tc)
-          launch_eps_tc(ctx, S.bov, S.ldov, naux, nov, chi, rc, eps, ldn, stride, p.precision == QX_PREC_FP16X3);
-        else
-          launch_eps_fp64(ctx, S.bov, S.ldov, naux, nov, chi, rc, eps, ldn, stride);
-        launch_invert_wc(ctx, eps, naux, ldn, stride, rc);
-        dim3 gg(ceil_div(ldn, 256), rc);
-        k_cd_gather<<<gg, 256, 0, ctx->stream>>>(d_lpq, naux, nmo, d_nm, rc, b, ldn);
-        check_launch(ctx);
-        k_cd_quad<<<rc, 256, 0, ctx->stream>>>(eps, ldn, stride, b, naux, ldn, x, d_val);
-        check_launch(ctx);
-        GemmNT g{};
-        g.M = rc;
-        g.N = nov;
-        g.K = naux;
-        g.A = x;
-        g.lda = ldn;
-        g.B = bovT;
-        g.ldb = ldn;
-        g.C = tm;
-        g.ldc = S.ldov;
-        g.batch = 1;
-        g.alpha = 1.0;
-        g.splitk = 0;
-        gemm_nt_f64(ctx, g);
-        k_cd_dres<<<rc, 256, 0, ctx->stream>>>(tm, S.ldov, S.d_en, nocc, nvir, d_wr, d_dv);
-        check_launch(ctx);
-        QX_CUDA(cudaMemcpyAsync(rv.data() + c0, d_val, rc * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-        QX_CUDA(cudaMemcpyAsync(rd.data() + c0, d_dv, rc * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-        // The singular-eps flags live in one buffer per context: read them
-        // before the next chunk reuses it.
-        if (c0 + rc < R) sync_and_check(ctx);
-      }
-    }
-    sync_and_check(ctx);
-    for (int t : act) {
-      sig[t] = hi[2 * t];
-      dsig[t] = hi[2 * t + 1];
-    }
-    for (int r = 0; r < R; ++r) {
-      sig[owner[r]] += sgn[r] * rv[r];
-      dsig[owner[r]] += rd[r];
-    }
-  };
+  CdEngine E;
+  E.ctx = ctx;
+  E.setup(p.mo_energy, p.lpq, p.targets, p.ntarget, p.nmo, p.nocc, p.naux, p.nw, p.x0, p.precision);
+  const int ntarget = p.ntarget;
+  std::vector<double> vx(p.nmo, 0.0);
+  if (p.vxc) QX_CUDA(cudaMemcpy(vx.data(), p.vxc, p.nmo * sizeof(double), cudaMemcpyDefault));
+  const std::vector<double>& e = E.e;
+  const std::vector<double>& sx = E.sx;
+  const std::vector<int>& tg = E.tg;
+  std::vector<double>& om = E.om;
+  const std::vector<double>& sig = E.sig;
+  const std::vector<double>& dsig = E.dsig;
   constexpr double z_min = 0.1, z_max = 0.999;  // newton_solver.rs:93-95
   std::vector<double> zf(ntarget), sxo(ntarget);
   std::vector<int> all;
   for (int t = 0; t < ntarget; ++t) all.push_back(t);
   if (p.qp_solver == QX_QP_LINEARIZED) {
     // E = e_n + Z (Sx + Sigma(e_n) - Vxc), Z clipped (qp/evgw.rs:784-821).
-    evaluate(all);
+    E.evaluate(all);
     for (int t = 0; t < ntarget; ++t) {
       const int n = tg[t];
       zf[t] = std::min(std::max(1.0 / (1.0 - dsig[t]), z_min), z_max);
@@ -287,7 +319,7 @@ void g0w0_cd_run(qx_ctx* ctx, const CdProblem& p) {
     std::vector<int> act = all, fresh(ntarget, 0);
     std::vector<double> damping(ntarget, 1.0), prev(ntarget, HUGE_VAL);
     for (int it = 0; it < p.max_iter && !act.empty(); ++it) {
-      evaluate(act);
+      E.evaluate(act);
       std::vector<int> next;
       for (int t : act) {
         const int n = tg[t];
@@ -314,7 +346,7 @@ void g0w0_cd_run(qx_ctx* ctx, const CdProblem& p) {
     std::vector<int> stale;
     for (int t = 0; t < ntarget; ++t)
       if (!fresh[t]) stale.push_back(t);
-    if (!stale.empty()) evaluate(stale);
+    if (!stale.empty()) E.evaluate(stale);
     for (int t = 0; t < ntarget; ++t) zf[t] = std::min(std::max(1.0 / (1.0 - dsig[t]), z_min), z_max);
   }
   for (int t = 0; t < ntarget; ++t) {
@@ -357,7 +389,7 @@ extern "C" qx_status qx_g0w0_cd(qx_ctx* ctx, const double* mo_energy, const doub
                                 double* sigma_c, double* sigma_x) {
   if (!ctx) return QX_ERR_INVALID_INPUT;
   try {
-    ctx->pending.clear();
+    reset_pending(ctx);
     ctx->launches = 0;
     for (double& v : ctx->stage_ms) v = 0.0;
     QX_CUDA(cudaSetDevice(ctx->device));
@@ -375,11 +407,44 @@ extern "C" qx_status qx_g0w0_cd(qx_ctx* ctx, const double* mo_energy, const doub
   }
 }
 
+extern "C" qx_status qx_cd_sigma(qx_ctx* ctx, const double* mo_energy, const double* lpq, int nmo, int nocc,
+                                 int naux, const int* targets, int ntarget, const double* omega, int nw, double x0,
+                                 int precision, double* sigma_c, double* dsigma_c, double* sigma_x) {
+  if (!ctx) return QX_ERR_INVALID_INPUT;
+  try {
+    reset_pending(ctx);
+    ctx->launches = 0;
+    for (double& v : ctx->stage_ms) v = 0.0;
+    QX_CUDA(cudaSetDevice(ctx->device));
+    QX_REQUIRE(omega && sigma_c, QX_ERR_INVALID_INPUT, "invalid arguments to cd_sigma");
+    CdEngine E;
+    E.ctx = ctx;
+    E.setup(mo_energy, lpq, targets, ntarget, nmo, nocc, naux, nw, x0, precision);
+    QX_CUDA(cudaMemcpy(E.om.data(), omega, ntarget * sizeof(double), cudaMemcpyDefault));
+    std::vector<int> all(ntarget);
+    for (int t = 0; t < ntarget; ++t) all[t] = t;
+    E.evaluate(all);
+    std::vector<double> sxo(ntarget);
+    for (int t = 0; t < ntarget; ++t) sxo[t] = E.sx[E.tg[t]];
+    QX_CUDA(cudaMemcpy(sigma_c, E.sig.data(), ntarget * sizeof(double), cudaMemcpyDefault));
+    if (dsigma_c) QX_CUDA(cudaMemcpy(dsigma_c, E.dsig.data(), ntarget * sizeof(double), cudaMemcpyDefault));
+    if (sigma_x) QX_CUDA(cudaMemcpy(sigma_x, sxo.data(), ntarget * sizeof(double), cudaMemcpyDefault));
+    ctx->err.clear();
+    return QX_OK;
+  } catch (const Error& ex) {
+    ctx->err = ex.what();
+    return ex.status;
+  } catch (const std::exception& ex) {
+    ctx->err = ex.what();
+    return QX_ERR_INVALID_INPUT;
+  }
+}
+
 extern "C" qx_status qx_g0w0_cd_batch(qx_ctx* ctx, qx_cd_system* systems, int nsys, int nw, double x0, double tol,
                                       int max_iter, int qp_solver, int precision, int nworkers) {
   if (!ctx) return QX_ERR_INVALID_INPUT;
   try {
-    ctx->pending.clear();
+    reset_pending(ctx);
     ctx->launches = 0;
     for (double& v : ctx->stage_ms) v = 0.0;
     QX_CUDA(cudaSetDevice(ctx->device));
@@ -411,7 +476,7 @@ extern "C" qx_status qx_g0w0_cd_batch(qx_ctx* ctx, qx_cd_system* systems, int ns
         const int k = next.fetch_add(1);
         if (k >= nsys) break;
         qx_cd_system& s = systems[order[k]];
-        w->pending.clear();
+        reset_pending(w);
         try {
           CdProblem p{s.mo_energy, s.lpq, s.vxc,    s.nmo,      s.nocc,       s.naux,      s.targets,
                       s.ntarget,   nw,    x0,      tol,      max_iter,   qp_solver,    precision,   s.qp_energies,

@@ -1,0 +1,60 @@
+// Contour-deformation G0W0 engine shared by the forward driver (qx_cd.cu)
+// and the adjoint (qx_grad.cu).
+#pragma once
+#include "qx_blas.cuh"
+#include "qx_gw_sys.cuh"
+#include "qx_internal.cuh"
+
+namespace qx {
+
+// One residue of target t: Wc_{n_t m}(w) enters Sigma_n with sign sgn, at the
+// real shift w = sgn (E_t - e_m) (occupied m above E_t: sgn = -1; virtual m
+// below E_t: sgn = +1).
+struct CdResidue {
+  int t, m;
+  double sgn, w;
+};
+
+// Device buffers of one chunk of residues (rc <= the chunk capacity).
+struct CdResidueChunk {
+  double* eps;  // [rc][naux][ldn]: eps(w_r), then Wc(w_r) = eps^-1 - I
+  double* b;    // [rc][ldn]: b_r = lpq[:, n_t, m]
+  double* x;    // [rc][ldn]: eps(w_r)^-1 b_r
+  double* tm;   // [rc][ldov]: B_ov^T x_r
+  double* chi;  // [rc][ldov]: real-axis chi'(w_r)
+  double* wr;   // [rc]
+  double* val;  // [rc]: Wc_r = b^T Wc(w_r) b
+  double* dv;   // [rc]: dWc_r/dw
+  int2* nm;     // [rc]
+  int cap;
+};
+
+struct CdEngine {
+  qx_ctx* ctx = nullptr;
+  int nmo = 0, nocc = 0, nvir = 0, naux = 0, nov = 0, ldn = 0, ntarget = 0, nw = 0, precision = 0;
+  bool tc = false;
+  std::vector<double> e, sx, om, sig, dsig;
+  std::vector<int> tg;
+  const double* d_lpq = nullptr;
+  GWSystem S;
+  double* bovT = nullptr;   // [nov][ldn]
+  double* d_om = nullptr;   // [ntarget]
+  double* d_imag = nullptr; // [ntarget][2]
+
+  // Copies the inputs, builds the imaginary-axis Wc_nm(i f_k) of the target
+  // pairs, Sigma_x and B_ov^T.  om starts at the mean-field energies.
+  void setup(const double* mo_energy, const double* lpq, const int* targets, int ntarget, int nmo, int nocc,
+             int naux, int nw, double x0, int precision);
+  // Residues of the targets in act at their current om.
+  std::vector<CdResidue> residues(const std::vector<int>& act) const;
+  // Buffers for chunks of up to the returned capacity (~2 GB of eps).
+  CdResidueChunk residue_buffers(int R);
+  // Wc, x, B_ov^T x and dWc/dw for residues list[0..rc) (device, async).
+  void residue_compute(CdResidueChunk& c, const CdResidue* list, int rc);
+  // sig/dsig of the targets in act at om (synchronises).
+  void evaluate(const std::vector<int>& act);
+};
+
+void launch_cd_gather(qx_ctx* ctx, const double* lpq, int naux, int nmo, const int2* nm, int R, double* b, int ld);
+
+}  // namespace qx

@@ -79,7 +79,7 @@ struct qx_ctx {
   double stage_ms[QX_ST_COUNT] = {0, 0, 0, 0, 0};
   cudaEvent_t ev[2 * QX_ST_COUNT] = {};
   // Named workspace slots.
-  qx::DevBuf ws[32];
+  qx::DevBuf ws[40];
   // Device status words to inspect after the next stream synchronisation:
   // (pointer, count, kind) with kind 0 = tcgen05 pipeline error code,
   // kind 1 = per-frequency singular-eps flags.
@@ -89,6 +89,10 @@ struct qx_ctx {
     int kind;
   };
   std::vector<Pending> pending;
+  // Status words of the pending checks: a fixed arena, never reallocated
+  // while checks are pending; reset at every synchronisation.
+  qx::DevBuf status_arena;
+  int status_used = 0;
   // Worker contexts of batched calls (own streams and workspaces), owned.
   std::vector<qx_ctx*> workers;
 };
@@ -118,9 +122,10 @@ enum WsSlot {
   WS_BSE0, WS_BSE1, WS_BSE2, WS_BSE3, WS_BSE4, WS_BSE5, WS_BSE6, WS_BSE7,
   WS_CD0, WS_CD1, WS_CD2, WS_CD3,
   WS_TCERR,       // tcgen05 pipeline error word
+  WS_GRAD0, WS_GRAD1, WS_GRAD2,  // CD adjoint: accumulators, per-frequency chunk, lpq gradient
   WS_COUNT
 };
-static_assert(WS_COUNT <= 32, "workspace slots");
+static_assert(WS_COUNT <= 40, "workspace slots");
 
 // Is p a device-accessible pointer of the current device?
 bool is_device_ptr(const void* p);
@@ -140,6 +145,16 @@ inline void check_launch(qx_ctx* ctx) {
 
 // Synchronise the context stream and act on the pending device status words.
 void sync_and_check(qx_ctx* ctx);
+
+// n status words (int) from the context's arena, valid until the next
+// sync_and_check (which this call performs first when the arena is full).
+int* status_words(qx_ctx* ctx, int n);
+
+// Forget pending checks at the start of an entry point.
+inline void reset_pending(qx_ctx* ctx) {
+  ctx->pending.clear();
+  ctx->status_used = 0;
+}
 
 // Stage timer (CUDA events on the context stream).
 struct StageTimer {

@@ -320,6 +320,22 @@ def g0w0_cd(mo_energy, lpq, nocc: int, targets: Sequence[int], nw: int = 100, x0
     return dict(qp_energies=qp, z_factors=z, sigma_c=sc, sigma_x=sx)
 
 
+def cd_sigma(mo_energy, lpq, nocc: int, targets: Sequence[int], omega, nw: int = 24, x0: float = 0.5,
+             precision="fp64", device: int = 0) -> Dict:
+    """Sigma_c^CD_n(omega_t) and dSigma/dw per target at the given real energies
+    (qx_cd_sigma), plus diag(Sigma_x) of the targets."""
+    ctx = _ctx(device, lpq, mo_energy)
+    lpq_a = lpq if hasattr(lpq, "data_ptr") else _f64(lpq)
+    naux, nmo, _ = tuple(lpq_a.shape)
+    e = mo_energy if hasattr(mo_energy, "data_ptr") else _f64(mo_energy)
+    t = np.ascontiguousarray(np.asarray(targets, dtype=np.int32))
+    om = _f64(omega)
+    sc, ds, sx = np.zeros(len(t)), np.zeros(len(t)), np.zeros(len(t))
+    ctx.check(ctx.lib.qx_cd_sigma(ctx.handle, N.ptr(e), N.ptr(lpq_a), nmo, int(nocc), naux, N.ptr(t), len(t),
+                                  N.ptr(om), int(nw), float(x0), _prec(precision), N.ptr(sc), N.ptr(ds), N.ptr(sx)))
+    return dict(sigma_c=sc, dsigma_c=ds, sigma_x=sx)
+
+
 def g0w0_cd_batch(systems, nw: int = 24, x0: float = 0.5, tol: float = 1e-8, max_iter: int = 50,
                   precision="fp64", qp_solver: str = "newton", nworkers: int = 4, device: int = 0) -> List[Dict]:
     """G0W0-CD for many independent systems in one call (qx_g0w0_cd_batch).
