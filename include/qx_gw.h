@@ -261,6 +261,14 @@ qx_status qx_bse_davidson(qx_bse* bse, const qx_davidson_config* cfg, double* ei
                           double* eigenvectors, int* converged, double* residual_norms,
                           int* iterations);
 
+/* Gradient of an eigenvalue Omega of the kernel's matrix (eigenvector x [nov],
+ * any norm) with respect to the orbital energies, grad_energy [nocc+nvirt], by
+ * Hellmann-Feynman (no reference counterpart).  delta_qp is taken as
+ * e_a - e_i.  With mo_energy non-NULL, W0 is taken as (I - Pi(0))^-1 built
+ * from mo_energy and df_ia (qx_bse_w0) and its dependence is included; with
+ * NULL, W0 is held fixed.  W0 must be symmetric. */
+qx_status qx_bse_root_grad(qx_bse* bse, const double* x, const double* mo_energy, double* grad_energy);
+
 /* W(w=0) = (I - Pi(0))^-1 for the screened-direct kernel, from lpq_ov [naux][nocc][nvir]. */
 qx_status qx_bse_w0(qx_ctx* ctx, const double* mo_energy, const double* lpq_ov, int naux, int nocc,
                     int nvir, double* w0);

@@ -1035,6 +1035,42 @@ def bse_apply_tda(x: np.ndarray, delta_qp, df_ia, df_ij, df_ab, w0, nocc, nvirt,
     return Y[:, 0] if single else Y
 
 
+def bse_root_grad(x, df_ia, df_ij, df_ab, w0, nocc, nvirt, mo_energy=None) -> np.ndarray:
+    """dOmega/de_p for an eigenpair (Omega, x) of the BSE-TDA matrix
+    A = diag(Delta) + alpha_x K^x - K^d(W0) (kernel.rs:501-598), by
+    Hellmann-Feynman (no reference counterpart): dOmega = x^T dA x / x^T x.
+
+    Delta_ia = e_a - e_i gives -sum_a x_ia^2 on e_i and +sum_i x_ia^2 on e_a.
+    With mo_energy given, W0 = (I - Pi(0))^-1 is taken as built from mo_energy
+    and df_ia (bse_w0): dOmega/dW0 = -M, M_PQ = sum x_ia x_jb B_ij^P B_ab^Q;
+    through W0 = eps0^-1, dOmega/deps0 = W0 sym(M) W0 = G; eps0 = I + sum_ia
+    chi_ia b_ia b_ia^T with chi_ia = 4/Delta_ia, so dOmega/dDelta_ia gains
+    (b_ia^T G b_ia) (-4/Delta_ia^2)."""
+    nov = nocc * nvirt
+    x = np.asarray(x, dtype=np.float64).reshape(-1)
+    xx = x / np.sqrt(x @ x)
+    X = xx.reshape(nocc, nvirt)
+    nmo = nocc + nvirt
+    g = np.zeros(nmo)
+    g[:nocc] -= np.sum(X * X, axis=1)
+    g[nocc:] += np.sum(X * X, axis=0)
+    if mo_energy is None:
+        return g
+    naux = df_ia.shape[1]
+    ab = df_ab.reshape(nvirt, nvirt, naux)
+    ij = df_ij.reshape(nocc, nocc, naux)
+    T = np.einsum("ia,abQ,jb->ijQ", X, ab, X, optimize=True)
+    M = np.einsum("ijP,ijQ->PQ", ij, T, optimize=True)
+    Ms = 0.5 * (M + M.T)
+    G = w0 @ Ms @ w0
+    s = np.einsum("kP,PQ,kQ->k", df_ia, G, df_ia, optimize=True)
+    delta = (mo_energy[None, nocc:] - mo_energy[:nocc, None]).reshape(-1)
+    gd = (s * (-4.0 / delta ** 2)).reshape(nocc, nvirt)
+    g[:nocc] -= gd.sum(axis=1)
+    g[nocc:] += gd.sum(axis=0)
+    return g
+
+
 @dataclass
 class DavidsonConfig:
     """quasix_core/src/bse/davidson.rs:47-104."""

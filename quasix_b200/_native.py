@@ -106,6 +106,7 @@ SIGNATURES = {
     "qx_bse_apply": (C.c_int, [_vp, _vp, _vp, C.c_int]),
     "qx_davidson_config_default": (None, [C.POINTER(DavidsonConfig)]),
     "qx_bse_davidson": (C.c_int, [_vp, C.POINTER(DavidsonConfig), _vp, _vp, _vp, _vp, _ip]),
+    "qx_bse_root_grad": (C.c_int, [_vp, _vp, _vp, _vp]),
     "qx_bse_w0": (C.c_int, [_vp, _vp, _vp, C.c_int, C.c_int, C.c_int, _vp]),
 }
 

@@ -118,6 +118,20 @@ class BSETDAKernel:
         """quasix/src/bse.rs:286-300: max_space = 20 * n_roots."""
         return self.solve_davidson_with_config(DavidsonConfig(n_roots, max_iter, 20 * n_roots, tol_residual))
 
+    def root_gradient(self, x, mo_energy=None) -> np.ndarray:
+        """dOmega/de [nocc + nvirt] of the eigenvalue with eigenvector ``x``
+        (Hellmann-Feynman; qx_bse_root_grad).  delta_qp is taken as e_a - e_i;
+        with ``mo_energy`` the dependence of W0 = (I - Pi(0))^-1 on the
+        energies is included, otherwise W0 is held fixed."""
+        xv = _f64(x).reshape(-1)
+        if xv.shape[0] != self.dimension:
+            raise ValueError(f"Input vector length {xv.shape[0]} != BSE dimension {self.dimension}")
+        g = np.zeros(self._nocc + self._nvirt)
+        e = None if mo_energy is None else _f64(mo_energy)
+        self.ctx.check(self.ctx.lib.qx_bse_root_grad(self.handle, N.ptr(xv), N.ptr(e) if e is not None else None,
+                                                     N.ptr(g)))
+        return g
+
     def close(self):
         if getattr(self, "handle", None):
             self.ctx.lib.qx_bse_destroy(self.handle)

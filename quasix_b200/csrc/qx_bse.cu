@@ -132,6 +132,29 @@ __global__ void k_norm2(const double* __restrict__ x, int n, double* __restrict_
   }
 }
 
+// M <- (M + M^T) / 2 for an n x n matrix (ld).
+__global__ void k_symmetrize(double* __restrict__ M, int n, int ld) {
+  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < n * n; idx += gridDim.x * blockDim.x) {
+    const int r = idx / n, c = idx % n;
+    if (c < r) {
+      const double v = 0.5 * (M[(size_t)r * ld + c] + M[(size_t)c * ld + r]);
+      M[(size_t)r * ld + c] = v;
+      M[(size_t)c * ld + r] = v;
+    }
+  }
+}
+
+// s[k] = sum_Q U[k][Q] D[k][Q]   (one warp per row)
+__global__ void k_rowdot(const double* __restrict__ U, const double* __restrict__ D, int rows, int n, int ld,
+                         double* __restrict__ s) {
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (warp >= rows) return;
+  double acc = 0.0;
+  for (int q = lane; q < n; q += 32) acc += U[(size_t)warp * ld + q] * D[(size_t)warp * ld + q];
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if (lane == 0) s[warp] = acc;
+}
+
 }  // namespace qx
 
 using namespace qx;
@@ -158,7 +181,9 @@ struct qx_bse {
   int ldq, ldvp, ldov;
   double alpha_x;
   DevArr delta, dia, diaT, ijw, dabT;
+  DevArr w0T, dij;                   // kept for the root gradient (W0 term)
   DevArr xp, T, Yd, Z, Yx, Xr, Yr;  // matvec scratch
+  DevArr gTt, gTp, gTpT, gdijT, gM, gG1, gG, gU;  // root-gradient scratch
   DevArr V, AV, X, AX, R, heff, jv, Z2, small;
   std::vector<double> h_delta;
 };
@@ -334,7 +359,8 @@ qx_status qx_bse_create(qx_ctx* ctx, qx_bse** out, int nocc, int nvirt, int naux
     QX_CUDA(cudaMemsetAsync(B->diaT.p, 0, (size_t)naux * B->ldov * sizeof(double), ctx->stream));
     transpose(ctx, stage.p, nov, naux, naux, 0, B->diaT.p, B->ldov, 0, 1);
     // w0^T [Q][P] (ldq), df_ij [nocc^2][ldq]; ijw = df_ij w0 (kernel.rs:286-291).
-    DevArr w0T, dij;
+    DevArr& w0T = B->w0T;
+    DevArr& dij = B->dij;
     upload(ctx, stage.p, w0, (size_t)naux * naux);
     w0T.alloc((size_t)naux * B->ldq);
     QX_CUDA(cudaMemsetAsync(w0T.p, 0, (size_t)naux * B->ldq * sizeof(double), ctx->stream));
@@ -649,6 +675,99 @@ qx_status qx_bse_davidson(qx_bse* B, const qx_davidson_config* cfgp, double* eig
     if (residual_norms)
       for (int r = 0; r < nroots; ++r) residual_norms[r] = rnorm[r];
     if (iterations) *iterations = iter;
+  });
+}
+
+static void gemm_nt(qx_ctx* ctx, int M, int N, int K, const double* A, int lda, const double* Bm, int ldb, double* C,
+                    int ldc) {
+  GemmNT g{};
+  g.M = M;
+  g.N = N;
+  g.K = K;
+  g.A = A;
+  g.lda = lda;
+  g.B = Bm;
+  g.ldb = ldb;
+  g.C = C;
+  g.ldc = ldc;
+  g.batch = 1;
+  g.alpha = 1.0;
+  g.beta = 0.0;
+  g.splitk = 0;
+  gemm_nt_f64(ctx, g);
+}
+
+qx_status qx_bse_root_grad(qx_bse* B, const double* x, const double* mo_energy, double* grad_energy) {
+  if (!B) return QX_ERR_INVALID_INPUT;
+  return bse_guard(B->ctx, [&] {
+    QX_REQUIRE(x && grad_energy, QX_ERR_INVALID_INPUT, "invalid arguments to bse_root_grad");
+    qx_ctx* ctx = B->ctx;
+    const int nocc = B->nocc, nvir = B->nvir, naux = B->naux, nov = B->nov, ldq = B->ldq, ldvp = B->ldvp;
+    std::vector<double> hx(nov);
+    QX_CUDA(cudaMemcpy(hx.data(), x, nov * sizeof(double), cudaMemcpyDefault));
+    double n2 = 0.0;
+    for (double v : hx) n2 += v * v;
+    QX_REQUIRE(n2 > 0.0 && std::isfinite(n2), QX_ERR_NUMERICAL, "eigenvector has zero or non-finite norm");
+    for (double& v : hx) v /= std::sqrt(n2);
+    // Delta_ia = e_a - e_i.
+    std::vector<double> g(nocc + nvir, 0.0);
+    for (int i = 0; i < nocc; ++i)
+      for (int a = 0; a < nvir; ++a) {
+        const double w = hx[(size_t)i * nvir + a] * hx[(size_t)i * nvir + a];
+        g[i] -= w;
+        g[nocc + a] += w;
+      }
+    if (mo_energy) {
+      std::vector<double> e(nocc + nvir);
+      QX_CUDA(cudaMemcpy(e.data(), mo_energy, e.size() * sizeof(double), cudaMemcpyDefault));
+      // T[a][j][Q] = sum_b x[j][b] B_ab^Q: the first step of the matvec (nvec = 1).
+      std::vector<double> hr(B->ldov, 0.0);
+      std::copy(hx.begin(), hx.end(), hr.begin());
+      B->Xr.alloc(B->ldov);
+      B->Yr.alloc(B->ldov);
+      QX_CUDA(cudaMemcpyAsync(B->Xr.p, hr.data(), B->ldov * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+      bse_apply_rows(B, B->Xr.p, B->Yr.p, 1);
+      const int nq = nocc * ldq, n2o = nocc * nocc, ld2 = round_up(n2o, 8);
+      // T'[(i,j)][Q] = sum_a x[i][a] T[a][(j,Q)]
+      B->gTt.alloc((size_t)nq * ldvp);
+      QX_CUDA(cudaMemsetAsync(B->gTt.p, 0, (size_t)nq * ldvp * sizeof(double), ctx->stream));
+      transpose(ctx, B->T.p, nvir, nq, nq, 0, B->gTt.p, ldvp, 0, 1);
+      B->gTp.alloc((size_t)n2o * ldq);
+      gemm_nt(ctx, nocc, nq, nvir, B->xp.p, ldvp, B->gTt.p, ldvp, B->gTp.p, nq);
+      // M[P][Q] = sum_(ij) B_ij^P T'[(ij)][Q]
+      B->gdijT.alloc((size_t)naux * ld2);
+      B->gTpT.alloc((size_t)ldq * ld2);
+      QX_CUDA(cudaMemsetAsync(B->gdijT.p, 0, (size_t)naux * ld2 * sizeof(double), ctx->stream));
+      QX_CUDA(cudaMemsetAsync(B->gTpT.p, 0, (size_t)ldq * ld2 * sizeof(double), ctx->stream));
+      transpose(ctx, B->dij.p, n2o, naux, ldq, 0, B->gdijT.p, ld2, 0, 1);
+      transpose(ctx, B->gTp.p, n2o, naux, ldq, 0, B->gTpT.p, ld2, 0, 1);
+      B->gM.alloc((size_t)naux * ldq);
+      gemm_nt(ctx, naux, naux, n2o, B->gdijT.p, ld2, B->gTpT.p, ld2, B->gM.p, ldq);
+      k_symmetrize<<<std::min(ceil_div(naux * naux, 256), 4096), 256, 0, ctx->stream>>>(B->gM.p, naux, ldq);
+      check_launch(ctx);
+      // G = W0 sym(M) W0 (W0 symmetric, stored as its transpose)
+      B->gG1.alloc((size_t)naux * ldq);
+      B->gG.alloc((size_t)naux * ldq);
+      gemm_nt(ctx, naux, naux, naux, B->w0T.p, ldq, B->gM.p, ldq, B->gG1.p, ldq);
+      gemm_nt(ctx, naux, naux, naux, B->gG1.p, ldq, B->w0T.p, ldq, B->gG.p, ldq);
+      // s_ia = b_ia^T G b_ia
+      B->gU.alloc((size_t)nov * ldq + nov);
+      gemm_nt(ctx, nov, naux, naux, B->dia.p, ldq, B->gG.p, ldq, B->gU.p, ldq);
+      double* d_s = B->gU.p + (size_t)nov * ldq;
+      k_rowdot<<<ceil_div(nov * 32, 256), 256, 0, ctx->stream>>>(B->gU.p, B->dia.p, nov, naux, ldq, d_s);
+      check_launch(ctx);
+      std::vector<double> sv(nov);
+      QX_CUDA(cudaMemcpyAsync(sv.data(), d_s, nov * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+      sync_and_check(ctx);
+      for (int i = 0; i < nocc; ++i)
+        for (int a = 0; a < nvir; ++a) {
+          const double d = e[nocc + a] - e[i];
+          const double gd = sv[(size_t)i * nvir + a] * (-4.0 / (d * d));
+          g[i] -= gd;
+          g[nocc + a] += gd;
+        }
+    }
+    QX_CUDA(cudaMemcpy(grad_energy, g.data(), g.size() * sizeof(double), cudaMemcpyDefault));
   });
 }
 

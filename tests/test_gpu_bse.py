@@ -107,3 +107,18 @@ def test_run_bse_tda(q):
     delta = (s.mo_energy[None, 6:] - s.mo_energy[:6, None]).reshape(-1)
     H = O.bse_apply_tda(np.eye(180), delta, dia, dij, dab, w0, 6, 30)
     assert res.converged and np.abs(res.excitation_energies_Ha - np.linalg.eigvalsh(H)[:4]).max() < 1e-9
+
+
+@pytest.mark.parametrize("shape", [(6, 30, 80), (7, 13, 31)])
+def test_root_gradient_matches_oracle(q, shape):
+    """Hellmann-Feynman gradient of the lowest root (the oracle's is checked
+    against central differences in tests/test_oracle_bse_grad.py)."""
+    nocc, nvir, naux = shape
+    s, delta, dia, dij, dab, w0 = bse_inputs(nocc, nvir, naux, 4)
+    k = q.BSETDAKernel(nocc, nvir, naux, delta, dia, dij, dab, w0)
+    r = k.solve_davidson(n_roots=1, tol_residual=1e-9)
+    x = r["eigenvectors"][:, 0]
+    for e in (s.mo_energy, None):
+        got = k.root_gradient(3.0 * x, mo_energy=e)  # any norm
+        ref = O.bse_root_grad(x, dia, dij, dab, w0, nocc, nvir, mo_energy=e)
+        assert np.abs(got - ref).max() < 1e-10 * np.abs(ref).max()
