@@ -167,6 +167,7 @@ struct TcArgs {
   int ldo;
   size_t out_stride;
   int lower_tiles;      // STORE: enumerate lower-triangular (m, n) tile pairs and mirror
+  int add_identity;     // STORE: add delta_mn
   int fp16;             // operand type: 0 bf16, 1 fp16
   int tri;              // ROWDOT with lower-triangular B: N tile n0 needs K < n0 + BN, result x2
   const float* scaleA;  // [1]      scale applied to A before the split
@@ -408,7 +409,7 @@ __global__ void __launch_bounds__(TcWarps<EPI>::THREADS, 1)
           // Lower-triangular mode writes the lower triangle and mirrors it,
           // so the stored matrix is exactly symmetric.
           if (n < args.N && !(args.lower_tiles && n > m)) {
-            const double val = acc[c] * unscale + (m == n ? 1.0 : 0.0);
+            const double val = acc[c] * unscale + ((args.add_identity && m == n) ? 1.0 : 0.0);
             orow[n] = val;
             if (args.lower_tiles && n != m) args.out[(size_t)w * args.out_stride + (size_t)n * args.ldo + m] = val;
           }
@@ -651,6 +652,7 @@ void launch_eps_tc(qx_ctx* ctx, const double* bov, int ldov, int naux, int nov, 
   a.ldo = ldn;
   a.out_stride = eps_stride;
   a.lower_tiles = 1;
+  a.add_identity = 1;
   a.fp16 = fp16;
   a.scaleA = sa;
   a.scaleB = sb;
@@ -658,6 +660,37 @@ void launch_eps_tc(qx_ctx* ctx, const double* bov, int ldov, int naux, int nov, 
   const int tiles = ceil_div(naux, TC_BM);  // BM == BN for the symmetric product
   static_assert(BN == TC_BM, "eps tiles are square");
   launch_tc<BN, EPI_STORE>(ctx, ah, al, bh, bl, a, dim3(tiles * (tiles + 1) / 2, nw));
+  check_tc_err(ctx, d_err);
+}
+
+// out[w][m][n] = sum_k A[m][k] B[w][n][k] in FP64 from split operands:
+// A hi/lo [M][lda] (one scale), B hi/lo [nbatch][N][ldb] (a scale per batch).
+void launch_gemm_tc(qx_ctx* ctx, const TcOperand& A, int M, int lda, const TcOperand& B, int N, int ldb, int K,
+                    int nbatch, double* out, int ldo, size_t out_stride, int fp16) {
+  constexpr int BN = 128;
+  CUtensorMap ah = make_map(A.hi, K, M, lda, 1, TC_BM, 2, fp16);
+  CUtensorMap al = make_map(A.lo, K, M, lda, 1, TC_BM, 2, fp16);
+  CUtensorMap bh = make_map(B.hi, K, N, ldb, nbatch, BN, 3, fp16);
+  CUtensorMap bl = make_map(B.lo, K, N, ldb, nbatch, BN, 3, fp16);
+  int* d_err = tc_err_slot(ctx);
+  QX_CUDA(cudaMemsetAsync(d_err, 0, sizeof(int), ctx->stream));
+  TcArgs a{};
+  a.M = M;
+  a.N = N;
+  a.K = K;
+  a.nbatch = nbatch;
+  a.m_blocks = ceil_div(M, TC_BM);
+  a.out = out;
+  a.ldo = ldo;
+  a.out_stride = out_stride;
+  a.lower_tiles = 0;
+  a.add_identity = 0;
+  a.fp16 = fp16;
+  a.scaleA = A.scale;
+  a.scaleB = B.scale;
+  a.err = d_err;
+  QX_REQUIRE(nbatch <= 65535, QX_ERR_INVALID_INPUT, "at most 65535 batches");
+  launch_tc<BN, EPI_STORE>(ctx, ah, al, bh, bl, a, dim3(a.m_blocks * ceil_div(N, BN), nbatch));
   check_tc_err(ctx, d_err);
 }
 

@@ -182,6 +182,8 @@ struct qx_bse {
   double alpha_x;
   DevArr delta, dia, diaT, ijw, dabT;
   DevArr w0T, dij;                   // kept for the root gradient (W0 term)
+  DevArr dab_split, dab_scale;       // split forms: hi/lo of dabT [a][Q][ldvp], scale per a
+  DevArr x_split;                    // split forms: hi/lo of the packed vectors
   DevArr xp, T, Yd, Z, Yx, Xr, Yr;  // matvec scratch
   DevArr gTt, gTp, gTpT, gdijT, gM, gG1, gG, gU;  // root-gradient scratch
   DevArr V, AV, X, AX, R, heff, jv, Z2, small;
@@ -205,7 +207,19 @@ static void bse_apply_rows(qx_bse* B, const double* X, double* Y, int nvec) {
     B->T.alloc(tslab * nvir);
     QX_CUDA(cudaMemsetAsync(B->T.p, 0, tslab * nvir * sizeof(double), ctx->stream));  // Q padding stays zero
   }
-  {
+  if (is_tc_precision(B->precision)) {
+    // T on tcgen05: split packed X (one scale), dabT split at create.
+    const int fp16 = B->precision == QX_PREC_FP16X3;
+    const size_t xe = (size_t)nvec * nocc * B->ldvp;
+    B->x_split.alloc((xe * 2 * 2 + 7) / 8 + 64);
+    uint8_t* xs = reinterpret_cast<uint8_t*>(B->x_split.p);
+    TcOperand A{xs, xs + ((xe * 2 + 255) / 256) * 256, nullptr};
+    launch_split(ctx, B->xp.p, nvec * nocc, nvir, B->ldvp, A.hi, A.lo, B->ldvp, 0, 0, 1, fp16, 0, &A.scale);
+    const size_t de = (size_t)nvir * naux * B->ldvp;
+    uint8_t* ds = reinterpret_cast<uint8_t*>(B->dab_split.p);
+    TcOperand Bo{ds, ds + ((de * 2 + 255) / 256) * 256, reinterpret_cast<float*>(B->dab_scale.p)};
+    launch_gemm_tc(ctx, A, nvec * nocc, B->ldvp, Bo, naux, B->ldvp, nvir, nvir, B->T.p, B->ldq, tslab, fp16);
+  } else {
     GemmNT g{};
     g.M = nvec * nocc;
     g.N = naux;
@@ -327,7 +341,10 @@ qx_status qx_bse_create(qx_ctx* ctx, qx_bse** out, int nocc, int nvirt, int naux
                nocc, nvirt, naux);
     QX_REQUIRE(delta_qp && df_ia && df_ij && df_ab && w0, QX_ERR_INVALID_INPUT, "null BSE input");
     QX_REQUIRE(spin == 0 || spin == 1, QX_ERR_INVALID_INPUT, "Unknown spin type %d", spin);
-    QX_REQUIRE(precision == QX_PREC_FP64 || precision == QX_PREC_BF16X3, QX_ERR_INVALID_INPUT, "bad precision");
+    QX_REQUIRE(precision == QX_PREC_FP64 || is_tc_precision(precision), QX_ERR_INVALID_INPUT, "bad precision %d",
+               precision);
+    QX_REQUIRE(!is_tc_precision(precision) || nvirt <= 1024, QX_ERR_INVALID_INPUT,
+               "split forms support nvirt <= 1024 (one scale per virtual orbital)");
     B->ctx = ctx;
     B->nocc = nocc;
     B->nvir = nvirt;
@@ -396,6 +413,18 @@ qx_status qx_bse_create(qx_ctx* ctx, qx_bse** out, int nocc, int nvirt, int naux
     QX_CUDA(cudaMemsetAsync(B->dabT.p, 0, (size_t)nvirt * naux * B->ldvp * sizeof(double), ctx->stream));
     transpose(ctx, stage.p, nvirt, naux, naux, (size_t)nvirt * naux, B->dabT.p, B->ldvp, (size_t)naux * B->ldvp,
               nvirt);
+    if (is_tc_precision(precision)) {
+      // hi/lo of dabT with a power-of-two scale per virtual orbital a (kept).
+      const size_t de = (size_t)nvirt * naux * B->ldvp;
+      const size_t half = ((de * 2 + 255) / 256) * 256;
+      B->dab_split.alloc((2 * half + 7) / 8 + 64);
+      B->dab_scale.alloc((nvirt + 1) / 2 + 1);
+      uint8_t* ds = reinterpret_cast<uint8_t*>(B->dab_split.p);
+      float* sc = nullptr;
+      launch_split(ctx, B->dabT.p, naux, nvirt, B->ldvp, ds, ds + half, B->ldvp, (size_t)naux * B->ldvp,
+                   (size_t)naux * B->ldvp, nvirt, precision == QX_PREC_FP16X3, 2, &sc);
+      QX_CUDA(cudaMemcpyAsync(B->dab_scale.p, sc, nvirt * sizeof(float), cudaMemcpyDeviceToDevice, ctx->stream));
+    }
     sync_and_check(ctx);
   });
   if (st != QX_OK) {

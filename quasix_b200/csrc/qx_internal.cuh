@@ -255,6 +255,8 @@ void launch_split(qx_ctx* ctx, const double* src, int rows, int cols, int ld_src
                   size_t src_stride, size_t dst_stride, int batch, int fp16, int slot, float** scale_out);
 void launch_eps_tc(qx_ctx* ctx, const double* bov, int ldov, int naux, int nov, const double* chi, int nw,
                    double* eps, int ldn, size_t eps_stride, int fp16);
+void launch_gemm_tc(qx_ctx* ctx, const TcOperand& A, int M, int lda, const TcOperand& B, int N, int ldb, int K,
+                    int nbatch, double* out, int ldo, size_t out_stride, int fp16);
 void launch_pair_contract_tc(qx_ctx* ctx, const TcOperand& A, const float* bpt_f32, int ldk, int npair, int naux,
                              const TcOperand& W, int ldw, size_t wc_stride, int nw, double* v, int ldv, int fp16);
 bool tc_supported(qx_ctx* ctx);

@@ -122,3 +122,21 @@ def test_root_gradient_matches_oracle(q, shape):
         got = k.root_gradient(3.0 * x, mo_energy=e)  # any norm
         ref = O.bse_root_grad(x, dia, dij, dab, w0, nocc, nvir, mo_energy=e)
         assert np.abs(got - ref).max() < 1e-10 * np.abs(ref).max()
+
+
+@pytest.mark.parametrize("precision,tol", [("fp16x3", 2e-6), ("bf16x3", 3e-5)])
+def test_split_precision_matvec_and_roots(q, precision, tol):
+    """Direct-term GEMM T = X dab^T on tcgen05 (split operands, FP64 drain of
+    each 64-wide K block); the other GEMMs and the Rayleigh-Ritz step stay
+    FP64.  Matvec error relative to max|y|; roots within 1e-6 Ha of FP64."""
+    nocc, nvir, naux = 6, 30, 80
+    s, delta, dia, dij, dab, w0 = bse_inputs(nocc, nvir, naux, 2)
+    k = q.BSETDAKernel(nocc, nvir, naux, delta, dia, dij, dab, w0, precision=precision)
+    x = np.random.default_rng(0).normal(size=(nocc * nvir, 7))
+    ref = O.bse_apply_tda(x, delta, dia, dij, dab, w0, nocc, nvir)
+    got = k.apply_hamiltonian_batch(x)
+    assert np.abs(got - ref).max() < tol * np.abs(ref).max()
+    k64 = q.BSETDAKernel(nocc, nvir, naux, delta, dia, dij, dab, w0)
+    r64 = k64.solve_davidson(n_roots=4, tol_residual=1e-8)
+    r = k.solve_davidson(n_roots=4, tol_residual=1e-8)
+    assert np.abs(np.array(r["eigenvalues"]) - np.array(r64["eigenvalues"])).max() < 1e-6
