@@ -265,4 +265,256 @@ void jacobi_eigh(qx_ctx* ctx, double* A, double* V, int n, int lda, double* w, d
   check_launch(ctx);
 }
 
+// ---------------------------------------------------------------------------
+// Lowest k eigenpairs of a symmetric n x n matrix, one CTA of 1024 threads:
+// Householder tridiagonalisation (in place in W, through L2), Sturm-count
+// bisection for eigenvalues 0..k-1 (one thread each), inverse iteration on
+// the tridiagonal with partial pivoting (the dgttrf/dgttrs elimination),
+// modified Gram-Schmidt among the k vectors, and back-transformation with
+// the stored reflectors.  A is symmetrised on load ((A + A^T) / 2).
+// Work (doubles): n*n + 4n + k*n*5 + k*n; ints: k*n.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double cta_sum(double v, double* red) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0) red[warp] = v;
+  __syncthreads();
+  double t = 0.0;
+  for (int i = 0; i < (int)(blockDim.x >> 5); ++i) t += red[i];
+  return t;
+}
+
+__device__ int sturm_count(const double* d, const double* e, int n, double x, double pivmin) {
+  int c = 0;
+  double q = d[0] - x;
+  if (q < 0.0) ++c;
+  for (int i = 1; i < n; ++i) {
+    if (fabs(q) < pivmin) q = -pivmin;
+    q = d[i] - x - e[i - 1] * e[i - 1] / q;
+    if (q < 0.0) ++c;
+  }
+  return c;
+}
+
+__global__ void __launch_bounds__(1024) k_eigh_lowest(const double* __restrict__ A, int n, int lda, int k,
+                                                      double* __restrict__ W, double* __restrict__ work,
+                                                      int* __restrict__ iwork, double* __restrict__ w_out,
+                                                      double* __restrict__ Z, int ldz) {
+  __shared__ double red[32];
+  extern __shared__ double sm[];  // u [n], q [n]
+  double* u = sm;
+  double* q = sm + n;
+  double* tau = work;           // [n]
+  double* d = work + n;         // [n]
+  double* e = work + 2 * n;     // [n]
+  double* lam = work + 3 * n;   // [n]
+  double* Y = work + 4 * n;     // [k][n] eigenvectors of T, then of A
+  double* LU = Y + (size_t)k * n;  // [5][k][n] per-vector factors
+  const int tid = threadIdx.x, nt = blockDim.x;
+  for (int idx = tid; idx < n * n; idx += nt) {
+    const int r = idx / n, c = idx % n;
+    W[idx] = 0.5 * (A[(size_t)r * lda + c] + A[(size_t)c * lda + r]);
+  }
+  __syncthreads();
+  // Tridiagonalisation: H_j = I - tau_j u_j u_j^T on rows/cols j+1..n-1.
+  for (int j = 0; j + 2 < n; ++j) {
+    const int m = n - j - 1;
+    double s = 0.0;
+    for (int i = tid; i < m; i += nt) {
+      const double x = W[(size_t)(j + 1 + i) * n + j];
+      s += x * x;
+    }
+    const double alpha = sqrt(cta_sum(s, red));
+    const double x0 = W[(size_t)(j + 1) * n + j];
+    if (alpha == 0.0) {
+      if (tid == 0) {
+        tau[j] = 0.0;
+        d[j] = W[(size_t)j * n + j];
+        e[j] = 0.0;
+      }
+      __syncthreads();
+      continue;
+    }
+    const double as = (x0 >= 0.0) ? -alpha : alpha;
+    const double t = 1.0 / (alpha * (alpha + fabs(x0)));  // 2 / (u^T u)
+    for (int i = tid; i < m; i += nt) u[i] = W[(size_t)(j + 1 + i) * n + j] - (i == 0 ? as : 0.0);
+    __syncthreads();
+    // p = B u (B symmetric: column access is coalesced)
+    for (int i = tid; i < m; i += nt) {
+      double acc = 0.0;
+      for (int l = 0; l < m; ++l) acc += W[(size_t)(j + 1 + l) * n + j + 1 + i] * u[l];
+      q[i] = acc;
+    }
+    __syncthreads();
+    double up = 0.0;
+    for (int i = tid; i < m; i += nt) up += u[i] * q[i];
+    const double K = cta_sum(up, red);
+    for (int i = tid; i < m; i += nt) q[i] = t * q[i] - 0.5 * t * t * K * u[i];
+    __syncthreads();
+    for (int idx = tid; idx < m * m; idx += nt) {
+      const int r = idx / m, c = idx % m;
+      W[(size_t)(j + 1 + r) * n + j + 1 + c] -= u[r] * q[c] + q[r] * u[c];
+    }
+    // keep u in the column below the diagonal for the back-transformation
+    for (int i = tid; i < m; i += nt) W[(size_t)(j + 1 + i) * n + j] = u[i];
+    if (tid == 0) {
+      tau[j] = t;
+      d[j] = W[(size_t)j * n + j];
+      e[j] = as;
+    }
+    __syncthreads();
+  }
+  if (tid == 0) {
+    if (n >= 2) {
+      d[n - 2] = W[(size_t)(n - 2) * n + n - 2];
+      e[n - 2] = W[(size_t)(n - 1) * n + n - 2];
+      tau[n - 2] = 0.0;
+    }
+    d[n - 1] = W[(size_t)(n - 1) * n + n - 1];
+    tau[n - 1] = 0.0;
+  }
+  __syncthreads();
+  // Bisection for eigenvalues r = 0..k-1 (ascending).
+  double lo = 1e300, hi = -1e300, emax = 0.0;
+  for (int i = 0; i < n; ++i) {
+    const double r0 = (i > 0) ? fabs(e[i - 1]) : 0.0, r1 = (i + 1 < n) ? fabs(e[i]) : 0.0;
+    lo = fmin(lo, d[i] - r0 - r1);
+    hi = fmax(hi, d[i] + r0 + r1);
+    if (i + 1 < n) emax = fmax(emax, fabs(e[i]));
+  }
+  const double tnorm = fmax(fabs(lo), fabs(hi));
+  const double pivmin = fmax(1e-300, 1e-290 * fmax(1.0, emax * emax));
+  for (int r = tid; r < k; r += nt) {
+    double a = lo - 1e-14 * tnorm - 1e-300, b = hi + 1e-14 * tnorm + 1e-300;
+    for (int it = 0; it < 200; ++it) {
+      const double mid = 0.5 * (a + b);
+      if (b - a <= 2.0 * 2.2e-16 * fmax(fabs(a), fabs(b)) + 1e-300) break;
+      if (sturm_count(d, e, n, mid, pivmin) > r)
+        b = mid;
+      else
+        a = mid;
+    }
+    lam[r] = 0.5 * (a + b);
+  }
+  __syncthreads();
+  // Inverse iteration on T - lam I (partial pivoting), three solves.
+  for (int r = tid; r < k; r += nt) {
+    double* dl = LU + ((size_t)0 * k + r) * n;
+    double* dd = LU + ((size_t)1 * k + r) * n;
+    double* du = LU + ((size_t)2 * k + r) * n;
+    double* du2 = LU + ((size_t)3 * k + r) * n;
+    int* piv = iwork + (size_t)r * n;
+    double* y = Y + (size_t)r * n;
+    const double lr = lam[r];
+    for (int i = 0; i < n; ++i) {
+      dd[i] = d[i] - lr;
+      if (i + 1 < n) {
+        dl[i] = e[i];
+        du[i] = e[i];
+      }
+      du2[i] = 0.0;
+    }
+    for (int i = 0; i + 1 < n; ++i) {
+      if (fabs(dd[i]) >= fabs(dl[i])) {
+        piv[i] = i;
+        if (dd[i] != 0.0) {
+          const double f = dl[i] / dd[i];
+          dl[i] = f;
+          dd[i + 1] -= f * du[i];
+        }
+      } else {
+        piv[i] = i + 1;
+        const double f = dd[i] / dl[i];
+        dd[i] = dl[i];
+        dl[i] = f;
+        const double tmp = du[i];
+        du[i] = dd[i + 1];
+        dd[i + 1] = tmp - f * dd[i + 1];
+        if (i + 2 < n) {
+          du2[i] = du[i + 1];
+          du[i + 1] = -f * du[i + 1];
+        }
+      }
+    }
+    const double tiny = 2.2e-16 * fmax(tnorm, 1e-300);
+    for (int i = 0; i < n; ++i)
+      if (fabs(dd[i]) < tiny) dd[i] = (dd[i] < 0.0) ? -tiny : tiny;
+    for (int i = 0; i < n; ++i) y[i] = 1.0 + 0.01 * sin(0.7 * (i + 1) * (r + 1));
+    for (int sweep = 0; sweep < 3; ++sweep) {
+      for (int i = 0; i + 1 < n; ++i) {
+        if (piv[i] == i) {
+          y[i + 1] -= dl[i] * y[i];
+        } else {
+          const double tmp = y[i];
+          y[i] = y[i + 1];
+          y[i + 1] = tmp - dl[i] * y[i];
+        }
+      }
+      y[n - 1] /= dd[n - 1];
+      if (n >= 2) y[n - 2] = (y[n - 2] - du[n - 2] * y[n - 1]) / dd[n - 2];
+      for (int i = n - 3; i >= 0; --i) y[i] = (y[i] - du[i] * y[i + 1] - du2[i] * y[i + 2]) / dd[i];
+      double nrm = 0.0;
+      for (int i = 0; i < n; ++i) nrm += y[i] * y[i];
+      nrm = 1.0 / sqrt(nrm);
+      for (int i = 0; i < n; ++i) y[i] *= nrm;
+    }
+  }
+  __syncthreads();
+  // Modified Gram-Schmidt among the k vectors (in order of eigenvalue).
+  for (int r = 0; r < k; ++r) {
+    double* yr = Y + (size_t)r * n;
+    for (int s2 = 0; s2 < r; ++s2) {
+      const double* ys = Y + (size_t)s2 * n;
+      double dp = 0.0;
+      for (int i = tid; i < n; i += nt) dp += yr[i] * ys[i];
+      const double dot = cta_sum(dp, red);
+      for (int i = tid; i < n; i += nt) yr[i] -= dot * ys[i];
+      __syncthreads();
+    }
+    double nn = 0.0;
+    for (int i = tid; i < n; i += nt) nn += yr[i] * yr[i];
+    const double inv = 1.0 / sqrt(cta_sum(nn, red));
+    for (int i = tid; i < n; i += nt) yr[i] *= inv;
+    __syncthreads();
+  }
+  // z = H_0 H_1 ... H_{n-3} y: one warp per vector.
+  const int lane = tid & 31, warp = tid >> 5, nwarp = nt >> 5;
+  for (int r = warp; r < k; r += nwarp) {
+    double* y = Y + (size_t)r * n;
+    for (int j = n - 3; j >= 0; --j) {
+      const double tj = tau[j];
+      if (tj == 0.0) continue;
+      const int m = n - j - 1;
+      double dp = 0.0;
+      for (int i = lane; i < m; i += 32) dp += W[(size_t)(j + 1 + i) * n + j] * y[j + 1 + i];
+      for (int o = 16; o > 0; o >>= 1) dp += __shfl_xor_sync(0xffffffffu, dp, o);
+      for (int i = lane; i < m; i += 32) y[j + 1 + i] -= tj * dp * W[(size_t)(j + 1 + i) * n + j];
+      __syncwarp();
+    }
+  }
+  __syncthreads();
+  for (int r = tid; r < k; r += nt) w_out[r] = lam[r];
+  for (int idx = tid; idx < n * k; idx += nt) {
+    const int i = idx / k, r = idx % k;
+    Z[(size_t)i * ldz + r] = Y[(size_t)r * n + i];
+  }
+}
+
+size_t eigh_lowest_work_doubles(int n, int k) { return (size_t)n * n + 4 * (size_t)n + 6 * (size_t)k * n + 64; }
+
+void eigh_lowest(qx_ctx* ctx, const double* A, int n, int lda, int k, double* w, double* Z, int ldz, double* work,
+                 int* iwork) {
+  QX_REQUIRE(n >= 1 && k >= 1 && k <= n && n <= 4096, QX_ERR_INVALID_INPUT, "eigh_lowest: n=%d k=%d", n, k);
+  double* W = work;
+  double* rest = work + (size_t)n * n;
+  const size_t sh = 2 * (size_t)n * sizeof(double);
+  static std::once_flag attr_once;
+  std::call_once(attr_once, [&] {
+    QX_CUDA(cudaFuncSetAttribute(k_eigh_lowest, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * 4096 * 8));
+  });
+  k_eigh_lowest<<<1, 1024, sh, ctx->stream>>>(A, n, lda, k, W, rest, iwork, w, Z, ldz);
+  check_launch(ctx);
+}
+
 }  // namespace qx

@@ -34,6 +34,13 @@ void combine_rows(qx_ctx* ctx, const double* V, int ldv, int nv, const double* c
 // (n x lda).  info[0] receives the number of sweeps.
 void jacobi_eigh(qx_ctx* ctx, double* A, double* V, int n, int lda, double* w, double* Z, int ldz, int* info);
 
+// Lowest k eigenpairs of the symmetric part of A (n x n, lda), one CTA:
+// eigenvalues ascending in w[0..k), eigenvectors as the first k columns of Z
+// (ldz).  work: eigh_lowest_work_doubles(n, k) doubles; iwork: k * n ints.
+size_t eigh_lowest_work_doubles(int n, int k);
+void eigh_lowest(qx_ctx* ctx, const double* A, int n, int lda, int k, double* w, double* Z, int ldz, double* work,
+                 int* iwork);
+
 // out[b][c][r] = in[b][r][c] (rows x cols per batch), through 32x32 smem tiles.
 void transpose(qx_ctx* ctx, const double* in, int rows, int cols, int ldi, size_t si, double* out, int ldo, size_t so,
                int batch);

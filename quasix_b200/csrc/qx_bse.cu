@@ -186,7 +186,7 @@ struct qx_bse {
   DevArr x_split;                    // split forms: hi/lo of the packed vectors
   DevArr xp, T, Yd, Z, Yx, Xr, Yr;  // matvec scratch
   DevArr gTt, gTp, gTpT, gdijT, gM, gG1, gG, gU;  // root-gradient scratch
-  DevArr V, AV, X, AX, R, heff, jv, Z2, small;
+  DevArr V, AV, X, AX, R, heff, jv, Z2, small, eigi;
   std::vector<double> h_delta;
 };
 
@@ -487,17 +487,18 @@ qx_status qx_bse_davidson(qx_bse* B, const qx_davidson_config* cfgp, double* eig
     B->AX.alloc((size_t)nroots * ld);
     B->R.alloc((size_t)nroots * ld);
     B->heff.alloc((size_t)cap * cap);
-    B->jv.alloc((size_t)cap * cap);
+    B->jv.alloc(eigh_lowest_work_doubles(cap, cap));
+    B->eigi.alloc(((size_t)cap * cap + 1) / 2 + 1);
     B->Z2.alloc((size_t)cap * cap);
     B->small.alloc((size_t)4 * cap + 64);
     double* d_theta = B->small.p;
     double* d_nrm = d_theta + cap;
     double* d_c = d_nrm + cap;
-    int* d_info = reinterpret_cast<int*>(d_c + cap);
     QX_CUDA(cudaMemsetAsync(B->V.p, 0, (size_t)cap * ld * sizeof(double), ctx->stream));
     auto apply = [&](int first, int count) { bse_apply_rows(B, B->V.p + (size_t)first * ld, B->AV.p + (size_t)first * ld, count); };
-    auto rr = [&](int nv) {
-      // heff = V AV^T, then Jacobi (symmetrises) -> theta, Z2 (columns).
+    auto rr = [&](int nv, int k) {
+      // heff = V AV^T, then the lowest k eigenpairs of its symmetric part ->
+      // theta, Z2 (columns).
       GemmNT g{};
       g.M = nv;
       g.N = nv;
@@ -512,7 +513,7 @@ qx_status qx_bse_davidson(qx_bse* B, const qx_davidson_config* cfgp, double* eig
       g.alpha = 1.0;
       g.splitk = 0;
       gemm_nt_f64(ctx, g);
-      jacobi_eigh(ctx, B->heff.p, B->jv.p, nv, nv, d_theta, B->Z2.p, nv, d_info);
+      eigh_lowest(ctx, B->heff.p, nv, nv, k, d_theta, B->Z2.p, nv, B->jv.p, reinterpret_cast<int*>(B->eigi.p));
     };
     const int nthreads = 256, nblk = std::min(ceil_div(n, nthreads), 2 * ctx->sm_count);
     // Trivial case (davidson.rs:384-387, 510-540): the full matrix.
@@ -521,7 +522,7 @@ qx_status qx_bse_davidson(qx_bse* B, const qx_davidson_config* cfgp, double* eig
       for (int i = 0; i < n; ++i) id[(size_t)i * ld + i] = 1.0;
       QX_CUDA(cudaMemcpyAsync(B->V.p, id.data(), id.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
       apply(0, n);
-      rr(n);
+      rr(n, n);
       std::vector<double> th(n), zz((size_t)n * n);
       QX_CUDA(cudaMemcpyAsync(th.data(), d_theta, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
       QX_CUDA(cudaMemcpyAsync(zz.data(), B->Z2.p, zz.size() * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
@@ -558,8 +559,8 @@ qx_status qx_bse_davidson(qx_bse* B, const qx_davidson_config* cfgp, double* eig
     bool all = false;
     std::vector<double> th(cap), nr(cap);
     for (iter = 0; iter < cfg.max_iter; ++iter) {
-      rr(nv);
       const int nr_ = std::min(nroots, nv);
+      rr(nv, nr_);
       // Ritz vectors X = V Y, AX = AV Y.
       combine_rows(ctx, B->V.p, ld, nv, B->Z2.p, nv, nr_, n, B->X.p, ld, 1.0, 0.0);
       combine_rows(ctx, B->AV.p, ld, nv, B->Z2.p, nv, nr_, n, B->AX.p, ld, 1.0, 0.0);
@@ -679,8 +680,8 @@ qx_status qx_bse_davidson(qx_bse* B, const qx_davidson_config* cfgp, double* eig
     // Not converged: the latest Ritz approximation for roots never stored
     // (davidson.rs:480-496).
     if (!all) {
-      rr(nv);
       const int nr_ = std::min(nroots, nv);
+      rr(nv, nr_);
       combine_rows(ctx, B->V.p, ld, nv, B->Z2.p, nv, nr_, n, B->X.p, ld, 1.0, 0.0);
       QX_CUDA(cudaMemcpyAsync(th.data(), d_theta, nr_ * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
       sync_and_check(ctx);
