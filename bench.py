@@ -45,6 +45,7 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-batch64", action="store_true")
     p.add_argument("--no-grad", action="store_true")
+    p.add_argument("--no-bse", action="store_true")
     p.add_argument("--batch-workers", type=int, default=4)
     return p.parse_args()
 
@@ -75,7 +76,7 @@ class Clocks:
                 ["nvidia-smi", f"--id={self.index}",
                  "--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
                  "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
-                 "clocks_event_reasons.sw_power_cap", "--format=csv,noheader,nounits", "-lms", "100"],
+                 "clocks_event_reasons.sw_power_cap", "--format=csv,noheader,nounits", "-lms", "200"],
                 stdout=self.f, stderr=subprocess.DEVNULL)
         except FileNotFoundError:
             self.p = None
@@ -318,6 +319,43 @@ def bench_grad_nmo200(q, dev, precision, steps=3, warmup=1):
     return out
 
 
+def bench_bse_dim26400(q, precision):
+    """BSE-TDA: nocc 60, nvirt 440 (dimension 26 400), naux 1800, seed 11,
+    ||Pi(0)|| = 5, singlet, W0 = (I - Pi(0))^-1; the 10 lowest roots to a
+    1e-8 Ha residual by the device Davidson (max_space 200).  One step = one
+    Davidson solve from the unit-vector start.  Reports seconds to converge
+    for the split form and FP64 and the largest root difference in meV."""
+    import torch
+    from oracle import qx_oracle as O
+    from quasix_b200.synth import make_system
+    s = make_system(60, 440, 1800, seed=11, pi_norm=5.0)
+    nocc, nvir, naux = 60, 440, 1800
+    dia, dij, dab = O.bse_blocks(s.lpq, nocc)
+    w0 = q.bse.screened_w0(s.mo_energy, np.ascontiguousarray(s.lpq[:, :nocc, nocc:]))
+    delta = (s.mo_energy[None, nocc:] - s.mo_energy[:nocc, None]).reshape(-1)
+    out = {"workload": "bse_tda_dim26400_naux1800_10roots", "tol_residual": 1e-8, "precision": precision}
+    roots = {}
+    for prec in (precision, "fp64"):
+        k = q.BSETDAKernel(nocc, nvir, naux, delta, dia, dij, dab, w0, precision=prec)
+        cfg = q.DavidsonConfig(10, 400, 200, 1e-8)
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        ev0.record()
+        r = k.solve_davidson_with_config(cfg)
+        ev1.record()
+        torch.cuda.synchronize()
+        pre = "" if prec == precision else "fp64_"
+        out[pre + "s_to_converge"] = ev0.elapsed_time(ev1) * 1e-3
+        out[pre + "iterations"] = r["iterations"]
+        out[pre + "all_converged"] = r["all_converged"]
+        roots[prec] = np.array(r["eigenvalues"])
+        k.close()
+    out["speedup_vs_fp64_gpu"] = out["fp64_s_to_converge"] / out["s_to_converge"]
+    out["max_root_err_meV_vs_fp64"] = float(np.abs(roots[precision] - roots["fp64"]).max() * HA_TO_MEV)
+    out["roots_Ha"] = [float(v) for v in roots["fp64"]]
+    return out
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -476,8 +514,10 @@ def main():
             "roofline": roof, "clocks": clocks, "e2e": e2e, "gpu_launches": launches}
     if not args.no_grad:
         line["grad_nmo200"] = bench_grad_nmo200(q, dev, prec_main)
+    if not args.no_bse:
+        line["bse_dim26400"] = bench_bse_dim26400(q, prec_main)
     if not args.no_batch64:
-        line["batch64_g0w0_cd"] = bench_batch64(q, dev, prec_main, steps=1, warmup=1, nworkers=args.batch_workers)
+        line["batch64_g0w0_cd"] = bench_batch64(q, dev, prec_main, steps=3, warmup=1, nworkers=args.batch_workers)
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_reference_sample(sysm, budget_s=12.0)
     if rank == 0:

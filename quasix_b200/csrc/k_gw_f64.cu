@@ -101,9 +101,15 @@ void launch_eps_fp64(qx_ctx* ctx, const double* bov, int ldov, int naux, int nov
 // no pivot vanishes).  Per block of SWEEP_NB columns:
 //   k_sweep_diag   : D = inverse of the current diagonal block (one CTA per matrix)
 //   k_sweep_tpanel : T = M[:, K] D                      (DMMA GEMM, K = nb)
-//   k_sweep_update : M[r][c] -= T[r] . M[c][K]  for r, c outside K, lower
-//                    tiles only, mirrored (DMMA GEMM, K = nb)
-//   k_sweep_write  : M[r][K] = M[K][r] = T[r], M[K][K] = -D
+//   k_sweep_write  : P[r] = M[r][K] (old panel), then M[r][K] = M[K][r] = T[r],
+//                    M[K][K] = -D
+//   k_sweep_update : M[r][c] -= T[r] . P[c]  for r, c outside K, lower tiles
+//                    only, mirrored (DMMA GEMM, K = nb)
+// Because the update reads the saved panel P, the next block's diagonal and
+// panel can be swept while the rest of this block's update still runs: the
+// update is split into the tiles that touch the next block (on the critical
+// chain) and the others (on a low-priority stream), with T, P, D
+// double-buffered.
 // ---------------------------------------------------------------------------
 constexpr int SWEEP_NB = 128;
 
@@ -163,26 +169,72 @@ __global__ void __launch_bounds__(512) k_sweep_diag(const double* __restrict__ M
     __syncthreads();
     if (warp == 0) sweep32_warp(S, q0, lane, bad_any);
     __syncthreads();
-    // T[r][q] = S[r][Q] D1 = -S[r][Q] Sswept[Q][q] for rows outside Q.
+    // Both products below use register tiles (thread = 4 rows x 2 or 8
+    // columns), so each shared-memory operand feeds several FMAs.
+    const int rt = tid >> 4, ct = tid & 15, rb = 4 * rt;
+    // T[r][q] = S[r][Q] D1 = -S[r][Q] Sswept[Q][q] for rows outside Q (0 inside).
     {
-      const int q = tid & 31, rg = tid >> 5;  // 16 row groups
-      for (int r = rg; r < SWEEP_NB; r += 16) {
-        if (r >= q0 && r < q0 + 32) continue;
-        double t = 0.0;
-#pragma unroll 8
-        for (int p = 0; p < 32; ++p) t -= S[r * SWEEP_NB + q0 + p] * S[(q0 + p) * SWEEP_NB + q0 + q];
-        Tb[r * TLD + q] = t;
+      const int cb = 2 * ct;
+      double t[4][2];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) t[i][0] = t[i][1] = 0.0;
+#pragma unroll 4
+      for (int p = 0; p < 32; ++p) {
+        const double b0 = S[(q0 + p) * SWEEP_NB + q0 + cb], b1 = S[(q0 + p) * SWEEP_NB + q0 + cb + 1];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          const double a = S[(rb + i) * SWEEP_NB + q0 + p];
+          t[i][0] -= a * b0;
+          t[i][1] -= a * b1;
+        }
+      }
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const bool inq = (rb + i >= q0 && rb + i < q0 + 32);
+        Tb[(rb + i) * TLD + cb] = inq ? 0.0 : t[i][0];
+        Tb[(rb + i) * TLD + cb + 1] = inq ? 0.0 : t[i][1];
       }
     }
     __syncthreads();
-    // S[r][c] -= T[r] . S[Q][c]  for r, c outside Q (old S[Q][c]).
-    for (int k = 0; k < 32; ++k) {
-      const int r = r0 + 4 * k;
-      if ((r >= q0 && r < q0 + 32) || (j >= q0 && j < q0 + 32)) continue;
-      double t = 0.0;
-#pragma unroll 8
-      for (int p = 0; p < 32; ++p) t += Tb[r * TLD + p] * S[(q0 + p) * SWEEP_NB + j];
-      S[r * SWEEP_NB + j] -= t;
+    // S[r][c] -= T[r] . S[Q][c]  for r, c outside Q (old S[Q][c]; rows in Q
+    // are read, never written here).
+    {
+      // Columns 32 v + 2 ct + {0, 1}, v = 0..3: a warp's double2 loads are
+      // contiguous (conflict-free), and each 32-column group lies wholly
+      // inside or outside Q.
+      const int cb = 2 * ct;
+      double acc[4][8];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int c = 0; c < 8; ++c) acc[i][c] = 0.0;
+#pragma unroll 2
+      for (int p = 0; p < 32; ++p) {
+        double bv[8];
+        const double* brow = S + (q0 + p) * SWEEP_NB + cb;
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+          const double2 x2 = *reinterpret_cast<const double2*>(brow + 32 * v);
+          bv[2 * v] = x2.x;
+          bv[2 * v + 1] = x2.y;
+        }
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          const double a = Tb[(rb + i) * TLD + p];
+#pragma unroll
+          for (int c = 0; c < 8; ++c) acc[i][c] += a * bv[c];
+        }
+      }
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        if (rb + i >= q0 && rb + i < q0 + 32) continue;
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+          if (32 * v == q0) continue;
+          S[(rb + i) * SWEEP_NB + 32 * v + cb] -= acc[i][2 * v];
+          S[(rb + i) * SWEEP_NB + 32 * v + cb + 1] -= acc[i][2 * v + 1];
+        }
+      }
     }
     __syncthreads();
     // S[r][Q] = T[r] (lanes along q) and S[Q][r] = T[r]^T (lanes along r).
@@ -238,10 +290,13 @@ __global__ void __launch_bounds__(PanelTile::THREADS) k_sweep_tpanel(const doubl
 
 using SweepTile = F64Tile<64, 64, 2, 2, 3>;
 
+// mode 0: every lower tile; 1: tiles whose rows or columns meet the next
+// block [nk0, nk0 + nkb); 2: the other tiles.
 __global__ void __launch_bounds__(SweepTile::THREADS) k_sweep_update(double* __restrict__ M, int n, int ldn,
                                                                      size_t stride, int k0, int kb,
                                                                      const double* __restrict__ Tp,
-                                                                     size_t pstride) {
+                                                                     const double* __restrict__ Pp,
+                                                                     size_t pstride, int mode, int nk0, int nkb) {
   using T = SweepTile;
   extern __shared__ double smem[];
   const int t = blockIdx.x;
@@ -253,6 +308,10 @@ __global__ void __launch_bounds__(SweepTile::THREADS) k_sweep_update(double* __r
   const int m0 = tm * T::BM, n0 = tn * T::BN;
   // Tiles entirely inside the K block rows or columns have nothing to update.
   if ((m0 >= k0 && m0 + T::BM <= k0 + kb) || (n0 >= k0 && n0 + T::BN <= k0 + kb)) return;
+  if (mode != 0) {
+    const bool touches = (m0 < nk0 + nkb && m0 + T::BM > nk0) || (n0 < nk0 + nkb && n0 + T::BN > nk0);
+    if (touches != (mode == 1)) return;
+  }
   double* A = M + (size_t)w * stride;
   const double* Tw = Tp + (size_t)w * pstride;
   double acc[T::MI][T::NJ][2];
@@ -260,8 +319,8 @@ __global__ void __launch_bounds__(SweepTile::THREADS) k_sweep_update(double* __r
   for (int i = 0; i < T::MI; ++i)
 #pragma unroll
     for (int j = 0; j < T::NJ; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
-  f64_mainloop<T>(acc, smem, Tw + (size_t)m0 * SWEEP_NB, SWEEP_NB, n - m0, A + (size_t)n0 * ldn + k0, ldn, n - n0,
-                  nullptr, kb);
+  f64_mainloop<T>(acc, smem, Tw + (size_t)m0 * SWEEP_NB, SWEEP_NB, n - m0, Pp + (size_t)w * pstride + (size_t)n0 * SWEEP_NB,
+                  SWEEP_NB, n - n0, nullptr, kb);
 #pragma unroll
   for (int i = 0; i < T::MI; ++i)
 #pragma unroll
@@ -278,13 +337,18 @@ __global__ void __launch_bounds__(SweepTile::THREADS) k_sweep_update(double* __r
 }
 
 __global__ void k_sweep_write(double* __restrict__ M, int n, int ldn, size_t stride, int k0, int kb,
-                              const double* __restrict__ Tp, size_t pstride, const double* __restrict__ Dp) {
+                              const double* __restrict__ Tp, double* __restrict__ Pp, size_t pstride,
+                              const double* __restrict__ Dp) {
   const int w = blockIdx.y;
   double* A = M + (size_t)w * stride;
   const double* Tw = Tp + (size_t)w * pstride;
+  double* Pw = Pp + (size_t)w * pstride;
   const double* D = Dp + (size_t)w * SWEEP_NB * SWEEP_NB;
   for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < n * kb; idx += gridDim.x * blockDim.x) {
     const int r = idx / kb, q = idx % kb;
+    // Save the old panel for the update (rows outside K; their mirror
+    // writes below land in rows inside K, which no thread reads here).
+    if (r < k0 || r >= k0 + kb) Pw[(size_t)r * SWEEP_NB + q] = A[(size_t)r * ldn + k0 + q];
     // Inside the K block both (r, q) and its mirror write the same element:
     // take D's lower triangle for both, so the stored value does not depend on
     // which write lands last.
@@ -313,47 +377,6 @@ __global__ void k_finish_wc(double* __restrict__ M, int n, int ldn, size_t strid
   }
 }
 
-void launch_invert_wc(qx_ctx* ctx, double* eps, int n, int ldn, size_t stride, int nw, int half_lower) {
-  const size_t pstride = (size_t)n * SWEEP_NB;
-  DevBuf& pan = ctx->ws[WS_PANEL];
-  const size_t need = (pstride * nw + (size_t)nw * SWEEP_NB * SWEEP_NB) * sizeof(double) + 256;
-  pan.reserve(need);
-  double* Tp = pan.as<double>();
-  double* Dp = Tp + pstride * nw;
-  int* status = status_words(ctx, nw);
-  QX_CUDA(cudaMemsetAsync(status, 0, nw * sizeof(int), ctx->stream));
-  const int diag_smem = (SWEEP_NB * SWEEP_NB + SWEEP_NB * 33) * sizeof(double);
-  static std::once_flag attr_once;
-  std::call_once(attr_once, [&] {
-    QX_CUDA(cudaFuncSetAttribute(k_sweep_diag, cudaFuncAttributeMaxDynamicSharedMemorySize, diag_smem));
-    QX_CUDA(cudaFuncSetAttribute(k_sweep_tpanel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)PanelTile::SMEM));
-    QX_CUDA(cudaFuncSetAttribute(k_sweep_update, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)SweepTile::SMEM));
-  });
-  const int tiles = ceil_div(n, SweepTile::BM);
-  for (int k0 = 0; k0 < n; k0 += SWEEP_NB) {
-    const int kb = min(SWEEP_NB, n - k0);
-    k_sweep_diag<<<nw, 512, diag_smem, ctx->stream>>>(eps, ldn, stride, k0, kb, Dp, status);
-    check_launch(ctx);
-    dim3 tg(ceil_div(n, PanelTile::BM), ceil_div(kb, PanelTile::BN), nw);
-    k_sweep_tpanel<<<tg, PanelTile::THREADS, PanelTile::SMEM, ctx->stream>>>(eps, n, ldn, stride, k0, kb, Dp, Tp,
-                                                                             pstride);
-    check_launch(ctx);
-    dim3 ug(tiles * (tiles + 1) / 2, nw);
-    k_sweep_update<<<ug, SweepTile::THREADS, SweepTile::SMEM, ctx->stream>>>(eps, n, ldn, stride, k0, kb, Tp,
-                                                                             pstride);
-    check_launch(ctx);
-    dim3 wg(ceil_div(n * kb, 256), nw);
-    k_sweep_write<<<wg, 256, 0, ctx->stream>>>(eps, n, ldn, stride, k0, kb, Tp, pstride, Dp);
-    check_launch(ctx);
-  }
-  dim3 fg(ceil_div(n * n, 256 * 4), nw);
-  k_finish_wc<<<fg, 256, 0, ctx->stream>>>(eps, n, ldn, stride, status, half_lower);
-  check_launch(ctx);
-  ctx->pending.push_back({status, nw, 1});
-}
-
 static_assert(kSweepPanelCols == SWEEP_NB, "panel width");
 
 void sweep_set_attributes() {
@@ -363,26 +386,106 @@ void sweep_set_attributes() {
   QX_CUDA(cudaFuncSetAttribute(k_sweep_update, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SweepTile::SMEM));
 }
 
-void launch_invert_wc_panels(qx_ctx* ctx, double* eps, int n, int ldn, size_t stride, int nw, double* Tp,
-                             double* Dp, int* status) {
-  const size_t pstride = (size_t)n * SWEEP_NB;
+static void sweep_attributes_once() {
+  static std::once_flag attr_once;
+  std::call_once(attr_once, [] { sweep_set_attributes(); });
+}
+
+// One block step of the sweep on stream st: D, T, then P and the panel write.
+static void sweep_front(qx_ctx* ctx, cudaStream_t st, double* eps, int n, int ldn, size_t stride, int nw, int k0,
+                        int kb, double* Tp, double* Dp, double* Pp, size_t pstride, int* status) {
   const int diag_smem = (SWEEP_NB * SWEEP_NB + SWEEP_NB * 33) * sizeof(double);
+  k_sweep_diag<<<nw, 512, diag_smem, st>>>(eps, ldn, stride, k0, kb, Dp, status);
+  check_launch(ctx);
+  dim3 tg(ceil_div(n, PanelTile::BM), ceil_div(kb, PanelTile::BN), nw);
+  k_sweep_tpanel<<<tg, PanelTile::THREADS, PanelTile::SMEM, st>>>(eps, n, ldn, stride, k0, kb, Dp, Tp, pstride);
+  check_launch(ctx);
+  dim3 wg(ceil_div(n * kb, 256), nw);
+  k_sweep_write<<<wg, 256, 0, st>>>(eps, n, ldn, stride, k0, kb, Tp, Pp, pstride, Dp);
+  check_launch(ctx);
+}
+
+static void sweep_update(qx_ctx* ctx, cudaStream_t st, double* eps, int n, int ldn, size_t stride, int nw, int k0,
+                         int kb, const double* Tp, const double* Pp, size_t pstride, int mode, int nk0, int nkb) {
   const int tiles = ceil_div(n, SweepTile::BM);
+  dim3 ug(tiles * (tiles + 1) / 2, nw);
+  k_sweep_update<<<ug, SweepTile::THREADS, SweepTile::SMEM, st>>>(eps, n, ldn, stride, k0, kb, Tp, Pp, pstride, mode,
+                                                                  nk0, nkb);
+  check_launch(ctx);
+}
+
+void launch_invert_wc(qx_ctx* ctx, double* eps, int n, int ldn, size_t stride, int nw, int half_lower) {
+  const size_t pstride = (size_t)n * SWEEP_NB;
+  const size_t dsz = (size_t)nw * SWEEP_NB * SWEEP_NB;
+  DevBuf& pan = ctx->ws[WS_PANEL];
+  // T[2], P[2] (pstride per matrix), D[2]
+  pan.reserve((4 * pstride * nw + 2 * dsz) * sizeof(double) + 256);
+  double* T0 = pan.as<double>();
+  double* T1 = T0 + pstride * nw;
+  double* P0 = T1 + pstride * nw;
+  double* P1 = P0 + pstride * nw;
+  double* D0 = P1 + pstride * nw;
+  double* D1 = D0 + dsz;
+  double* Tb[2] = {T0, T1};
+  double* Pb[2] = {P0, P1};
+  double* Db[2] = {D0, D1};
+  int* status = status_words(ctx, nw);
+  QX_CUDA(cudaMemsetAsync(status, 0, nw * sizeof(int), ctx->stream));
+  sweep_attributes_once();
+  const int nsteps = ceil_div(n, SWEEP_NB);
+  if (nsteps == 1) {
+    sweep_front(ctx, ctx->stream, eps, n, ldn, stride, nw, 0, n, T0, D0, P0, pstride, status);
+  } else {
+    // Look-ahead: critical chain (D, T, write, next-block update) on a
+    // high-priority stream, the remaining trailing update on a low-priority one.
+    if (!ctx->sweep_hi) {
+      int lo = 0, hi = 0;
+      QX_CUDA(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+      if (ctx->worker) lo = hi = 0;
+      QX_CUDA(cudaStreamCreateWithPriority(&ctx->sweep_hi, cudaStreamNonBlocking, hi));
+      QX_CUDA(cudaStreamCreateWithPriority(&ctx->sweep_lo, cudaStreamNonBlocking, lo));
+      for (auto& e : ctx->sweep_ev) QX_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    }
+    cudaStream_t s0 = ctx->sweep_hi, s1 = ctx->sweep_lo;
+    cudaEvent_t ev_start = ctx->sweep_ev[0], ev_front = ctx->sweep_ev[1], ev_rest = ctx->sweep_ev[2],
+                ev_done = ctx->sweep_ev[3];
+    QX_CUDA(cudaEventRecord(ev_start, ctx->stream));
+    QX_CUDA(cudaStreamWaitEvent(s0, ev_start, 0));
+    QX_CUDA(cudaStreamWaitEvent(s1, ev_start, 0));
+    for (int step = 0; step < nsteps; ++step) {
+      const int k0 = step * SWEEP_NB, kb = min(SWEEP_NB, n - k0);
+      const int b = step & 1;
+      sweep_front(ctx, s0, eps, n, ldn, stride, nw, k0, kb, Tb[b], Db[b], Pb[b], pstride, status);
+      // The previous step's trailing update must be done before this step's
+      // updates touch the same tiles.
+      if (step > 0) QX_CUDA(cudaStreamWaitEvent(s0, ev_rest, 0));
+      if (step + 1 < nsteps) {
+        const int nk0 = k0 + SWEEP_NB, nkb = min(SWEEP_NB, n - nk0);
+        QX_CUDA(cudaEventRecord(ev_front, s0));
+        sweep_update(ctx, s0, eps, n, ldn, stride, nw, k0, kb, Tb[b], Pb[b], pstride, 1, nk0, nkb);
+        QX_CUDA(cudaStreamWaitEvent(s1, ev_front, 0));
+        sweep_update(ctx, s1, eps, n, ldn, stride, nw, k0, kb, Tb[b], Pb[b], pstride, 2, nk0, nkb);
+        QX_CUDA(cudaEventRecord(ev_rest, s1));
+      } else {
+        sweep_update(ctx, s0, eps, n, ldn, stride, nw, k0, kb, Tb[b], Pb[b], pstride, 0, 0, 0);
+      }
+    }
+    QX_CUDA(cudaEventRecord(ev_done, s0));
+    QX_CUDA(cudaStreamWaitEvent(ctx->stream, ev_done, 0));
+  }
+  dim3 fg(ceil_div(n * n, 256 * 4), nw);
+  k_finish_wc<<<fg, 256, 0, ctx->stream>>>(eps, n, ldn, stride, status, half_lower);
+  check_launch(ctx);
+  ctx->pending.push_back({status, nw, 1});
+}
+
+void launch_invert_wc_panels(qx_ctx* ctx, double* eps, int n, int ldn, size_t stride, int nw, double* Tp,
+                             double* Dp, double* Pp, int* status) {
+  const size_t pstride = (size_t)n * SWEEP_NB;
   for (int k0 = 0; k0 < n; k0 += SWEEP_NB) {
     const int kb = min(SWEEP_NB, n - k0);
-    k_sweep_diag<<<nw, 512, diag_smem, ctx->stream>>>(eps, ldn, stride, k0, kb, Dp, status);
-    check_launch(ctx);
-    dim3 tg(ceil_div(n, PanelTile::BM), ceil_div(kb, PanelTile::BN), nw);
-    k_sweep_tpanel<<<tg, PanelTile::THREADS, PanelTile::SMEM, ctx->stream>>>(eps, n, ldn, stride, k0, kb, Dp, Tp,
-                                                                             pstride);
-    check_launch(ctx);
-    dim3 ug(tiles * (tiles + 1) / 2, nw);
-    k_sweep_update<<<ug, SweepTile::THREADS, SweepTile::SMEM, ctx->stream>>>(eps, n, ldn, stride, k0, kb, Tp,
-                                                                             pstride);
-    check_launch(ctx);
-    dim3 wg(ceil_div(n * kb, 256), nw);
-    k_sweep_write<<<wg, 256, 0, ctx->stream>>>(eps, n, ldn, stride, k0, kb, Tp, pstride, Dp);
-    check_launch(ctx);
+    sweep_front(ctx, ctx->stream, eps, n, ldn, stride, nw, k0, kb, Tp, Dp, Pp, pstride, status);
+    sweep_update(ctx, ctx->stream, eps, n, ldn, stride, nw, k0, kb, Tp, Pp, pstride, 0, 0, 0);
   }
   dim3 fg(ceil_div(n * n, 256 * 4), nw);
   k_finish_wc<<<fg, 256, 0, ctx->stream>>>(eps, n, ldn, stride, status, 0);

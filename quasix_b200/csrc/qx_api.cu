@@ -480,6 +480,10 @@ qx_status qx_ctx_destroy(qx_ctx* c) {
   c->workers.clear();
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
+  for (auto& e : c->sweep_ev)
+    if (e) cudaEventDestroy(e);
+  if (c->sweep_hi) cudaStreamDestroy(c->sweep_hi);
+  if (c->sweep_lo) cudaStreamDestroy(c->sweep_lo);
   for (auto& e : c->ev)
     if (e) cudaEventDestroy(e);
   if (c->own_stream) cudaStreamDestroy(c->own_stream);

@@ -64,31 +64,39 @@ __global__ void k_cd_gather(const double* __restrict__ lpq, int naux, int nmo, c
     b[(size_t)r * ld + P] = (P < naux) ? lpq[(size_t)P * nmo * nmo + (size_t)p.x * nmo + p.y] : 0.0;
 }
 
-// x[r] = b[r] + Wc[r] b[r] (= eps^-1 b);  wc[r] = b^T Wc b.  One warp per row.
-__global__ void k_cd_quad(const double* __restrict__ wc, int ldn, size_t stride, const double* __restrict__ b, int n,
-                          int ld, double* __restrict__ x, double* __restrict__ val) {
-  const int r = blockIdx.x;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
-  const double* W = wc + (size_t)r * stride;
+// x[r][P] = b[r][P] + sum_Q Wc[r][P][Q] b[r][Q] (= eps^-1 b): one warp per
+// row P, many CTAs per residue.
+__global__ void k_cd_solve_rows(const double* __restrict__ wc, int ldn, size_t stride, const double* __restrict__ b,
+                                int n, int ld, double* __restrict__ x) {
+  const int r = blockIdx.y;
+  const int lane = threadIdx.x & 31;
+  const int P = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (P >= n) return;
+  const double* W = wc + (size_t)r * stride + (size_t)P * ldn;
   const double* br = b + (size_t)r * ld;
+  double s = 0.0;
+  for (int Q = lane; Q < n; Q += 32) s += W[Q] * br[Q];
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if (lane == 0) x[(size_t)r * ld + P] = br[P] + s;
+}
+
+// val[r] = b^T Wc b = sum_P b[P] (x[P] - b[P])   (one CTA per residue, fixed order)
+__global__ void k_cd_quad_reduce(const double* __restrict__ b, const double* __restrict__ x, int n, int ld,
+                                 double* __restrict__ val) {
+  const int r = blockIdx.x;
   double q = 0.0;
-  for (int P = warp; P < n; P += nwarp) {
-    double s = 0.0;
-    for (int Q = lane; Q < n; Q += 32) s += W[(size_t)P * ldn + Q] * br[Q];
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    if (lane == 0) {
-      x[(size_t)r * ld + P] = br[P] + s;
-      q += br[P] * s;
-    }
+  for (int P = threadIdx.x; P < n; P += blockDim.x) {
+    const double bv = b[(size_t)r * ld + P];
+    q += bv * (x[(size_t)r * ld + P] - bv);
   }
-  __shared__ double red[32];
-  if (lane == 0) red[warp] = q;
+  __shared__ double red[256];
+  red[threadIdx.x] = q;
   __syncthreads();
-  if (threadIdx.x == 0) {
-    double t = 0.0;
-    for (int i = 0; i < nwarp; ++i) t += red[i];
-    val[r] = t;
+  for (int o = 128; o > 0; o >>= 1) {
+    if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+    __syncthreads();
   }
+  if (threadIdx.x == 0) val[r] = red[0];
 }
 
 // dwc[r] = 4 sum_ia e_ia 2 w_r / (e_ia^2 - w_r^2)^2 (B_ia^T x_r)^2
@@ -217,7 +225,9 @@ void CdEngine::residue_compute(CdResidueChunk& c, const CdResidue* list, int rc)
     launch_eps_fp64(ctx, S.bov, S.ldov, naux, nov, c.chi, rc, c.eps, ldn, stride);
   launch_invert_wc(ctx, c.eps, naux, ldn, stride, rc);
   launch_cd_gather(ctx, d_lpq, naux, nmo, c.nm, rc, c.b, ldn);
-  k_cd_quad<<<rc, 256, 0, ctx->stream>>>(c.eps, ldn, stride, c.b, naux, ldn, c.x, c.val);
+  k_cd_solve_rows<<<dim3(ceil_div(naux, 8), rc), 256, 0, ctx->stream>>>(c.eps, ldn, stride, c.b, naux, ldn, c.x);
+  check_launch(ctx);
+  k_cd_quad_reduce<<<rc, 256, 0, ctx->stream>>>(c.b, c.x, naux, ldn, c.val);
   check_launch(ctx);
   GemmNT g{};
   g.M = rc;
@@ -365,6 +375,7 @@ void g0w0_cd_run(qx_ctx* ctx, const CdProblem& p) {
 qx_ctx* make_worker(int device) {
   qx_ctx* c = new qx_ctx();
   c->device = device;
+  c->worker = true;
   try {
     cudaDeviceProp pr;
     QX_CUDA(cudaGetDeviceProperties(&pr, device));

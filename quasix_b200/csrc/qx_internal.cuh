@@ -93,6 +93,14 @@ struct qx_ctx {
   // while checks are pending; reset at every synchronisation.
   qx::DevBuf status_arena;
   int status_used = 0;
+  // Streams of the look-ahead inversion (critical chain at high priority,
+  // trailing updates at low priority) and their events; created on first use.
+  cudaStream_t sweep_hi = nullptr, sweep_lo = nullptr;
+  // Batch workers share the GPU with each other: their look-ahead streams keep
+  // the default priority (a high-priority chain there stalls the other
+  // workers' kernels while SMs drain for its large-shared-memory CTAs).
+  bool worker = false;
+  cudaEvent_t sweep_ev[4] = {};
   // Worker contexts of batched calls (own streams and workspaces), owned.
   std::vector<qx_ctx*> workers;
 };
@@ -186,15 +194,15 @@ void launch_eps_fp64(qx_ctx* ctx, const double* bov, int ldov, int naux, int nov
 // half_lower: return W' = strict-lower(Wc) + diag(Wc)/2 (zeros above) instead of Wc.
 void launch_invert_wc(qx_ctx* ctx, double* eps, int n, int ldn, size_t stride, int nw, int half_lower = 0);
 
-// The same sweep on caller-provided panels (no workspace, full Wc): Tp holds
-// nw * n * SWEEP_NB doubles, Dp nw * SWEEP_NB^2 doubles, status nw ints that
+// The same sweep on caller-provided panels (no workspace, full Wc): Tp and Pp
+// hold nw * n * SWEEP_NB doubles each, Dp nw * SWEEP_NB^2, status nw ints that
 // must be zero on entry (nonzero on exit = singular eps, Wc set to 0).
 // sweep_set_attributes() raises the kernels' dynamic shared-memory limits on
 // the current device.
 constexpr int kSweepPanelCols = 128;
 void sweep_set_attributes();
 void launch_invert_wc_panels(qx_ctx* ctx, double* eps, int n, int ldn, size_t stride, int nw, double* Tp,
-                             double* Dp, int* status);
+                             double* Dp, double* Pp, int* status);
 
 // v[w][p] = Bpt[p]^T Wc[w] Bpt[p] for all pairs (FP64), given W' (half-lower form).
 void launch_pair_contract_fp64(qx_ctx* ctx, const double* bpt, int ldk, int npair, int naux, const double* wc,

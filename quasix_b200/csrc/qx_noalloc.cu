@@ -5,7 +5,8 @@
 // launch_invert_wc, correlation_ac.rs:377-401 in the reference), processed in
 // frequency chunks that fit the scratch array.  Scratch layout, each region
 // 256-byte aligned:
-//   status [kMaxFreq] int  | eps [c][naux][ldn] | T panels [c][naux][128] | D blocks [c][128][128]
+//   status [kMaxFreq] int | eps [c][naux][ldn] | T panels [c][naux][128] | P panels [c][naux][128] |
+//   D blocks [c][128][128]
 // with c the chunk length.  Only the status words must start at zero; they are
 // cleared at the start of every call.
 #include <mutex>
@@ -28,9 +29,9 @@ static __device__ __align__(256) double qx_noalloc_scratch[kScratchBytes / sizeo
 
 inline size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
 
-// Bytes one frequency needs (eps, T panel, D block), each region rounded.
+// Bytes one frequency needs (eps, T and P panels, D block), each region rounded.
 inline size_t per_freq_bytes(int n, int ldn) {
-  return align256((size_t)n * ldn * sizeof(double)) + align256((size_t)n * kSweepPanelCols * sizeof(double)) +
+  return align256((size_t)n * ldn * sizeof(double)) + 2 * align256((size_t)n * kSweepPanelCols * sizeof(double)) +
          align256((size_t)kSweepPanelCols * kSweepPanelCols * sizeof(double));
 }
 
@@ -98,7 +99,9 @@ void screened_noalloc(qx_ctx* ctx, int nfreq, int naux, const double* pi, double
   int* status = reinterpret_cast<int*>(base);
   double* eps = reinterpret_cast<double*>(base + kStatusBytes);
   double* Tp = reinterpret_cast<double*>(base + kStatusBytes + align256((size_t)chunk * stride * sizeof(double)));
-  double* Dp = reinterpret_cast<double*>(reinterpret_cast<char*>(Tp) +
+  double* Pp = reinterpret_cast<double*>(reinterpret_cast<char*>(Tp) +
+                                         align256((size_t)chunk * n * kSweepPanelCols * sizeof(double)));
+  double* Dp = reinterpret_cast<double*>(reinterpret_cast<char*>(Pp) +
                                          align256((size_t)chunk * n * kSweepPanelCols * sizeof(double)));
 
   QX_CUDA(cudaMemsetAsync(status, 0, (size_t)nfreq * sizeof(int), ctx->stream));
@@ -107,7 +110,7 @@ void screened_noalloc(qx_ctx* ctx, int nfreq, int naux, const double* pi, double
     dim3 g(std::min(ceil_div(n * ldn, 256), 4096), c);
     k_noalloc_load<<<g, 256, 0, ctx->stream>>>(pi + (size_t)w0 * n * n, n, ldn, stride, eps);
     check_launch(ctx);
-    launch_invert_wc_panels(ctx, eps, n, ldn, stride, c, Tp, Dp, status + w0);
+    launch_invert_wc_panels(ctx, eps, n, ldn, stride, c, Tp, Dp, Pp, status + w0);
     k_noalloc_store<<<g, 256, 0, ctx->stream>>>(eps, n, ldn, stride, wc + (size_t)w0 * n * n);
     check_launch(ctx);
   }
