@@ -142,7 +142,7 @@ constexpr int TC_STAGES = 2;
 // warps per lane quarter, 64 columns each).
 template <int EPI>
 struct TcWarps {
-  static constexpr int NEPI = (EPI == 1) ? 8 : 4;
+  static constexpr int NEPI = 8;
   static constexpr int THREADS = 64 + 32 * NEPI;
 };
 
@@ -152,7 +152,8 @@ struct TcSmem {
   static constexpr int B_BYTES = BN * TC_BK * 2;
   static constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;
   static constexpr int BAR_OFF = TC_STAGES * STAGE_BYTES;
-  static constexpr int TOTAL = BAR_OFF + 256 + 1024;  // barriers + misc + alignment slack
+  static constexpr int RED_OFF = BAR_OFF + 256;  // ROWDOT: partial row sums [2][128] doubles + 2 flags
+  static constexpr int TOTAL = RED_OFF + 2048 + 64 + 1024;  // + alignment slack
 };
 
 struct TcArgs {
@@ -174,6 +175,10 @@ struct TcArgs {
   const float* scaleB;  // [nbatch] scale applied to B[w] before the split
   int* err;
 };
+
+__device__ __forceinline__ double unscale_rowdot(const TcArgs& a, int w) {
+  return 1.0 / ((double)a.scaleA[0] * (double)a.scaleB[w]);
+}
 
 template <int BN, int EPI>
 __global__ void __launch_bounds__(TcWarps<EPI>::THREADS, 1)
@@ -334,21 +339,23 @@ __global__ void __launch_bounds__(TcWarps<EPI>::THREADS, 1)
         mbar_wait(drain, 0, &no_abort, args.err, 6);
       }
     } else if (EPI == EPI_ROWDOT) {
-      // ---------------- epilogue (warps 2..5): row dot products ----------------
+      // ---------------- epilogue (warps 2..9): row dot products ----------------
+      // Two warps per TMEM lane quarter, each over half of the N tile.
       const int quarter = warp & 3;  // TMEM lane quarter this warp may access
+      const int half = (warp - 2) >> 2;
       const int row = quarter * 32 + lane;
       const int m = m0 + row;
-      const double unscale = 1.0 / ((double)args.scaleA[0] * (double)args.scaleB[w]);
+      constexpr int HB = BN / 2;
       double rowsum = 0.0;
       int t = 0;
       for (int nt = nt_begin; nt < nt_end; ++nt, ++t) {
         const int buf = t & 1;
         if (!mbar_wait(&acc_full[buf], (t / 2) & 1, abort_flag, args.err, 4)) break;
         tc_fence_after();
-        const int n0 = nt * BN;
-        const uint32_t taddr = tmem_base + ((uint32_t)(quarter * 32) << 16) + buf * BN;
+        const int n0 = nt * BN + half * HB;
+        const uint32_t taddr = tmem_base + ((uint32_t)(quarter * 32) << 16) + buf * BN + half * HB;
 #pragma unroll 1
-        for (int c = 0; c < BN; c += 16) {
+        for (int c = 0; c < HB; c += 16) {
           float v[16];
           tmem_ld16(taddr + c, v);
           if (m < args.M) {
@@ -369,8 +376,15 @@ __global__ void __launch_bounds__(TcWarps<EPI>::THREADS, 1)
         __syncwarp();
         if (lane == 0) mbar_arrive(&acc_empty[buf]);
       }
-      if (m < args.M && t == nt_end - nt_begin)
-        args.out[(size_t)w * args.ldo + m] = rowsum * unscale * (args.tri ? 2.0 : 1.0);
+      // Combine the two halves (named barrier of the 8 epilogue warps; every
+      // one of them reaches it, also after an abort).
+      double* red = reinterpret_cast<double*>(smem + L::RED_OFF);
+      int* done = reinterpret_cast<int*>(red + 2 * TC_BM);  // two flags after the sums
+      red[half * TC_BM + row] = (t == nt_end - nt_begin) ? rowsum : 0.0;
+      if (lane == 0 && quarter == 0) done[half] = (t == nt_end - nt_begin) ? 1 : 0;
+      asm volatile("bar.sync 1, 256;\n" ::: "memory");
+      if (half == 0 && m < args.M && done[0] && done[1])
+        args.out[(size_t)w * args.ldo + m] = (red[row] + red[TC_BM + row]) * unscale_rowdot(args, w) * (args.tri ? 2.0 : 1.0);
     } else {
       // ---------------- epilogue (warps 2..9): FP64 sum of k-block partials ----------------
       const int quarter = warp & 3;
