@@ -62,6 +62,23 @@ def dist_setup(n):
     return 0, 1, 0
 
 
+def max_over_ranks(values, world, device):
+    """Element-wise maximum of per-rank timings (seconds) over the job: every
+    rank takes part in the same all-reduce, in the same order."""
+    if world == 1:
+        return [float(v) for v in values]
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(v) for v in t]
+
+
+def job_rate(units_per_rank, world, seconds_max):
+    """Whole-job throughput: units of all ranks over the slowest rank's time."""
+    return world * units_per_rank / seconds_max
+
+
 class Clocks:
     """nvidia-smi sampler for the timed region."""
 
@@ -152,8 +169,26 @@ def fp64_dgemm_peak_tflops():
 
 
 def contraction_flops(nmo, naux, nw):
+    """Algorithmic FLOPs of the Sigma_c contraction per iteration (all orbitals):
+    2 naux^2 norbs nmo per frequency (the per-unit figure of the reference's
+    per-orbital dgemm), norbs = nmo."""
+    return 2.0 * naux * naux * nmo * nmo * nw
+
+
+def contraction_mma_flops(nmo, naux, nw):
+    """MMA FLOPs the split tcgen05 contraction issues: unique pairs padded to
+    128 rows, N tiles of 256 over naux padded to 64, the half-lower K range
+    [0, n0 + 256) of each N tile, three products."""
     npair = nmo * (nmo + 1) // 2
-    return 2.0 * naux * naux * npair * nw + 2.0 * naux * npair * nw
+    m_pad = -(-npair // 128) * 128
+    kb = -(-naux // 64)
+    kn = sum(min(kb, -(-(n0 + 256) // 64)) * 64 for n0 in range(0, naux, 256))
+    return 3 * 2.0 * m_pad * 256 * kn * nw
+
+
+# DRAM bytes (read + write) of one pair-contraction launch at nmo 300 / naux 1000 /
+# nw 32, from one ncu capture (profiles/k_tc_gemm_evgw_nmo300.md).
+CONTRACTION_DRAM_BYTES = 1.564282e9 + 0.034871e9
 
 
 def iteration_flops(nocc, nvir, naux, nw):
@@ -442,13 +477,9 @@ def main():
     if prec_main != "fp64":
         run("fp64", min(args.warmup, 1), lpq_d)
         res_fp64, t_fp64 = timed("fp64", args.steps, lpq_d)
-    # max over ranks
-    if world > 1:
-        tt = torch.tensor([t_main, t_fp64], device=f"cuda:{dev}")
-        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
-        t_main, t_fp64 = float(tt[0]), float(tt[1])
-    value = world * args.steps / t_main
-    fp64_rate = world * args.steps / t_fp64
+    t_main, t_fp64 = max_over_ranks([t_main, t_fp64], world, f"cuda:{dev}")
+    value = job_rate(args.steps, world, t_main)
+    fp64_rate = job_rate(args.steps, world, t_fp64)
     err_iter = [float(np.abs(a - b).max() * HA_TO_MEV) for a, b in zip(res_main["energies"], res_fp64["energies"])]
     # Conditioning of the FP64 path itself: the same FP64 evGW on lpq
     # perturbed by ~1e-14 relative (symmetric noise).  Iterations whose FP64
@@ -473,12 +504,8 @@ def main():
     t0 = time.perf_counter()
     run(prec_main, args.steps, lpq_h.numpy())
     torch.cuda.synchronize()
-    t_e2e = time.perf_counter() - t0
-    if world > 1:
-        tt = torch.tensor([t_e2e], device=f"cuda:{dev}")
-        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
-        t_e2e = float(tt[0])
-    e2e = {"value": world * args.steps / t_e2e, "unit": "evGW iter/s",
+    t_e2e = max_over_ranks([time.perf_counter() - t0], world, f"cuda:{dev}")[0]
+    e2e = {"value": job_rate(args.steps, world, t_e2e), "unit": "evGW iter/s",
            "h2d_bytes_per_step": int((sysm.lpq.nbytes + 2 * nmo * 8) / args.steps + nmo * 8 * 2),
            "d2h_bytes_per_step": int(nmo * 8 * 4)}
 
@@ -486,6 +513,7 @@ def main():
     cflops = contraction_flops(nmo, NAUX, NW)
     ms_contract = stage["contraction"] / args.steps
     achieved = cflops / (ms_contract * 1e-3) / 1e12
+    executed = contraction_mma_flops(nmo, NAUX, NW) / (ms_contract * 1e-3) / 1e12
     if prec_main == "fp64":
         dpeak = fp64_dgemm_peak_tflops()
         roof = {"bound": "tensor", "achieved": achieved, "peak": dpeak, "unit": "TFLOP/s", "frac": achieved / dpeak,
@@ -494,9 +522,12 @@ def main():
     else:
         pk = peaks.get("bf16_tflops_sustained", peaks.get("bf16_tflops"))
         roof = {"bound": "tensor", "achieved": achieved, "peak": pk, "unit": "TFLOP/s", "frac": achieved / pk,
-                "traffic": None, "kernel": "k_tc_gemm<256,EPI_ROWDOT> (pair contraction)",
+                "traffic": CONTRACTION_DRAM_BYTES, "kernel": "k_tc_gemm<256,EPI_ROWDOT> (pair contraction)",
                 "peak_source": f"bf16_tflops_sustained, {peak_src}",
-                "mma_flops_per_algorithmic_flop": 3}
+                "algorithmic_flops_per_launch": cflops,
+                "executed_mma_tflops": executed, "executed_mma_frac": executed / pk,
+                "note": "algorithmic = 2 naux^2 norbs nmo nw; executed = 3 split products over the "
+                        "half-lower K range of unique pairs; stage time includes the Wc split"}
 
     line = {"metric": METRIC, "value": value, "unit": "evGW iter/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * t_main / args.steps, "higher_is_better": True,
