@@ -164,7 +164,11 @@ __global__ void __launch_bounds__(512) k_sweep_diag(const double* __restrict__ M
     S[i * SWEEP_NB + j] = (i < kb && j < kb) ? A[(size_t)(k0 + i) * ldn + k0 + j] : (i == j ? 1.0 : 0.0);
   }
   bool bad_any = false;
-  for (int sb = 0; sb < 4; ++sb) {
+  // Sub-blocks past kb are identity padding with no coupling to the block:
+  // sweeping them changes nothing inside it (D is zeroed outside kb), so a
+  // narrow last block sweeps only ceil(kb / 32) of them.
+  const int nsb = (kb + 31) / 32;
+  for (int sb = 0; sb < nsb; ++sb) {
     const int q0 = 32 * sb;
     __syncthreads();
     if (warp == 0) sweep32_warp(S, q0, lane, bad_any);

@@ -19,7 +19,10 @@
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
+#include <array>
+#include <map>
 #include <mutex>
+#include <vector>
 
 #include "qx_internal.cuh"
 
@@ -602,6 +605,47 @@ static void launch_tc(qx_ctx* ctx, const CUtensorMap& ah, const CUtensorMap& al,
   check_launch(ctx);
 }
 
+// Autotuned frequency-group size of the pair contraction, per (npair, naux,
+// nw, device): candidates 4, 8, 16, 32 (<= nw) are timed with CUDA events on
+// the first call of a shape; later calls reuse the fastest.
+template <class F>
+static int tuned_wgroup(qx_ctx* ctx, int npair, int naux, int nw, F&& launch_with) {
+  static std::mutex mu;
+  static std::map<std::array<int, 4>, int> table;
+  const std::array<int, 4> key{npair, naux, nw, ctx->device};
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = table.find(key);
+    if (it != table.end()) return it->second;
+  }
+  std::vector<int> cand;
+  for (int g : {4, 8, 16, 32})
+    if (g <= nw) cand.push_back(g);
+  if (cand.empty()) cand.push_back(nw);
+  cudaEvent_t e0, e1;
+  QX_CUDA(cudaEventCreate(&e0));
+  QX_CUDA(cudaEventCreate(&e1));
+  int best = cand[0];
+  float best_ms = 1e30f;
+  for (int g : cand) {
+    QX_CUDA(cudaEventRecord(e0, ctx->stream));
+    launch_with(g);
+    QX_CUDA(cudaEventRecord(e1, ctx->stream));
+    QX_CUDA(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    QX_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    if (ms < best_ms) {
+      best_ms = ms;
+      best = g;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  std::lock_guard<std::mutex> lock(mu);
+  table[key] = best;
+  return best;
+}
+
 // v[w][p] = 2 sum_Q X[p][Q] sum_{P <= Q} (Bh+Bl)[p][P] (W'h+W'l)[w][Q][P] / (sA sB[w]),
 // W' the half-lower form of Wc (three products per term)
 void launch_pair_contract_tc(qx_ctx* ctx, const TcOperand& A, const float* bpt_f32, int ldk, int npair, int naux,
@@ -630,8 +674,18 @@ void launch_pair_contract_tc(qx_ctx* ctx, const TcOperand& A, const float* bpt_f
   a.scaleA = A.scale;
   a.scaleB = W.scale;
   a.err = d_err;
-  const int groups = ceil_div(nw, a.wgroup);
-  launch_tc<BN, EPI_ROWDOT>(ctx, ah, al, bh, bl, a, dim3(groups * a.m_blocks * a.wgroup));
+  // CTA order: frequency groups of wgroup, pair blocks inside a group, the
+  // group's frequencies innermost.  The group size trades L2 residency of W
+  // (wgroup matrices) against re-reads of the pair tensor (nw / wgroup
+  // passes); every (frequency, pair block) is still one CTA with the same
+  // arithmetic, so the choice does not change the result.  It is tuned once
+  // per shape by timing the candidates on the call's own data.
+  auto launch_with = [&](int g) {
+    a.wgroup = g;
+    launch_tc<BN, EPI_ROWDOT>(ctx, ah, al, bh, bl, a, dim3(ceil_div(nw, g) * a.m_blocks * g));
+  };
+  a.wgroup = tuned_wgroup(ctx, npair, naux, nw, launch_with);
+  launch_with(a.wgroup);
   check_tc_err(ctx, d_err);
 }
 
