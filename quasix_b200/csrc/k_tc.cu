@@ -91,17 +91,21 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, u
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory"); }
 
-// SM100 shared-memory matrix descriptor: K-major, 128-byte swizzle, rows of
-// 128 bytes, 8-row groups 1024 bytes apart (SBO), version 1.
-__device__ __forceinline__ uint64_t umma_desc_sw128(uint32_t saddr) {
+// SM100 shared-memory matrix descriptor (version 1) for a K-major operand tile of BK 16-bit elements per row: BK = 64 uses the 128-byte
+// swizzle (layout 2, 8-row groups 1024 bytes apart), BK = 32 the 64-byte swizzle
+// (layout 4, 512 bytes apart).
+template <int BK>
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr) {
+  static_assert(BK == 32 || BK == 64, "K block of 32 or 64 elements");
   uint64_t d = 0;
-  d |= (uint64_t)((saddr & 0x3FFFF) >> 4);  // start address
-  d |= (uint64_t)1 << 16;                   // leading byte offset (unused for swizzled K-major)
-  d |= (uint64_t)(1024 >> 4) << 32;         // stride byte offset
-  d |= (uint64_t)1 << 46;                   // descriptor version (sm_100)
-  d |= (uint64_t)2 << 61;                   // SWIZZLE_128B
+  d |= (uint64_t)((saddr & 0x3FFFF) >> 4);          // start address
+  d |= (uint64_t)1 << 16;                           // leading byte offset (unused for swizzled K-major)
+  d |= (uint64_t)((8 * BK * 2) >> 4) << 32;         // stride byte offset: 8 rows
+  d |= (uint64_t)1 << 46;                           // descriptor version (sm_100)
+  d |= (uint64_t)(BK == 64 ? 2 : 4) << 61;          // SWIZZLE_128B / SWIZZLE_64B
   return d;
 }
+
 
 // Instruction descriptor: kind::f16 with bf16 (fmt 1) or fp16 (fmt 0) A and B of
 // the same type, f32 accumulator, K-major A and B.
@@ -139,8 +143,15 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
 enum { EPI_ROWDOT = 0, EPI_STORE = 1 };
 
 constexpr int TC_BM = 128;
-constexpr int TC_BK = 64;  // one 128-byte swizzle row of bf16
-constexpr int TC_STAGES = 2;
+// Pipeline shape per epilogue: 64-wide K blocks (the unit of the STORE
+// kernels' FP64 drain) in 2 stages.  32-wide blocks in 4 stages (the same
+// shared memory, more TMA requests in flight) measured slower for the pair
+// contraction (7.8 vs 6.1 ms at nmo 300 / naux 1000 / nw 32).
+template <int EPI>
+struct TcPipe {
+  static constexpr int BK = 64;
+  static constexpr int STAGES = 2;
+};
 // Epilogue warps: 4 (ROWDOT: one TMEM lane quarter each) or 8 (STORE: two
 // warps per lane quarter, 64 columns each).
 template <int EPI>
@@ -149,12 +160,12 @@ struct TcWarps {
   static constexpr int THREADS = 64 + 32 * NEPI;
 };
 
-template <int BN>
+template <int BN, int EPI>
 struct TcSmem {
-  static constexpr int A_BYTES = TC_BM * TC_BK * 2;
-  static constexpr int B_BYTES = BN * TC_BK * 2;
+  static constexpr int A_BYTES = TC_BM * TcPipe<EPI>::BK * 2;
+  static constexpr int B_BYTES = BN * TcPipe<EPI>::BK * 2;
   static constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;
-  static constexpr int BAR_OFF = TC_STAGES * STAGE_BYTES;
+  static constexpr int BAR_OFF = TcPipe<EPI>::STAGES * STAGE_BYTES;
   static constexpr int RED_OFF = BAR_OFF + 256;  // ROWDOT: partial row sums [2][128] doubles + 2 flags
   static constexpr int TOTAL = RED_OFF + 2048 + 64 + 1024;  // + alignment slack
 };
@@ -187,7 +198,9 @@ template <int BN, int EPI>
 __global__ void __launch_bounds__(TcWarps<EPI>::THREADS, 1)
     k_tc_gemm(const __grid_constant__ CUtensorMap mapAh, const __grid_constant__ CUtensorMap mapAl,
               const __grid_constant__ CUtensorMap mapBh, const __grid_constant__ CUtensorMap mapBl, TcArgs args) {
-  using L = TcSmem<BN>;
+  using L = TcSmem<BN, EPI>;
+  constexpr int TC_BK = TcPipe<EPI>::BK;
+  constexpr int TC_STAGES = TcPipe<EPI>::STAGES;
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + L::BAR_OFF);
@@ -324,9 +337,9 @@ __global__ void __launch_bounds__(TcWarps<EPI>::THREADS, 1)
             for (int kk = 0; kk < TC_BK / 16; ++kk) {
               const uint32_t off = kk * 32;
               const uint32_t acc0 = (!unit_start || kk > 0) ? 1u : 0u;
-              umma_f16(dacc, umma_desc_sw128(ah + off), umma_desc_sw128(bh + off), idesc, acc0);
-              umma_f16(dacc, umma_desc_sw128(ah + off), umma_desc_sw128(bl + off), idesc, 1u);
-              umma_f16(dacc, umma_desc_sw128(al + off), umma_desc_sw128(bh + off), idesc, 1u);
+              umma_f16(dacc, umma_desc<TC_BK>(ah + off), umma_desc<TC_BK>(bh + off), idesc, acc0);
+              umma_f16(dacc, umma_desc<TC_BK>(ah + off), umma_desc<TC_BK>(bl + off), idesc, 1u);
+              umma_f16(dacc, umma_desc<TC_BK>(al + off), umma_desc<TC_BK>(bh + off), idesc, 1u);
             }
             umma_commit(&empty[s]);
             if (unit_end) {
@@ -465,16 +478,17 @@ static EncodeTiledFn encode_fn() {
 
 // bf16 matrix [batch][rows][ld] (K contiguous, K valid = cols) with box {64, box_rows, 1}.
 static CUtensorMap make_map(const void* base, int cols, int rows, int ld, int batch, int box_rows, int rank,
-                            int fp16) {
+                            int fp16, int bk) {
   QX_REQUIRE((reinterpret_cast<uintptr_t>(base) & 15) == 0 && (ld * 2) % 16 == 0, QX_ERR_INVALID_INPUT,
              "tensor map base/stride not 16-byte aligned");
   CUtensorMap m;
   cuuint64_t dims[3] = {(cuuint64_t)cols, (cuuint64_t)rows, (cuuint64_t)batch};
   cuuint64_t strides[2] = {(cuuint64_t)ld * 2, (cuuint64_t)ld * 2 * rows};
-  cuuint32_t box[3] = {(cuuint32_t)TC_BK, (cuuint32_t)box_rows, 1};
+  cuuint32_t box[3] = {(cuuint32_t)bk, (cuuint32_t)box_rows, 1};
   cuuint32_t estr[3] = {1, 1, 1};
   CUresult r = encode_fn()(&m, fp16 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, rank, const_cast<void*>(base), dims, strides, box,
-                           estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                           estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                           bk == 64 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B,
                            CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   QX_REQUIRE(r == CUDA_SUCCESS, QX_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
   return m;
@@ -596,7 +610,7 @@ static void check_tc_err(qx_ctx* ctx, int* d_err) { ctx->pending.push_back({d_er
 template <int BN, int EPI>
 static void launch_tc(qx_ctx* ctx, const CUtensorMap& ah, const CUtensorMap& al, const CUtensorMap& bh,
                       const CUtensorMap& bl, const TcArgs& a, dim3 grid) {
-  using L = TcSmem<BN>;
+  using L = TcSmem<BN, EPI>;
   static std::once_flag attr_once;
   std::call_once(attr_once, [&] {
     QX_CUDA(cudaFuncSetAttribute(k_tc_gemm<BN, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, L::TOTAL));
@@ -652,10 +666,11 @@ void launch_pair_contract_tc(qx_ctx* ctx, const TcOperand& A, const float* bpt_f
                              const TcOperand& W, int ldw, size_t wc_stride, int nw, double* v, int ldv, int fp16) {
   constexpr int BN = 256;
   QX_REQUIRE(wc_stride == (size_t)naux * ldw, QX_ERR_INVALID_INPUT, "Wc stride must be naux*ldw");
-  CUtensorMap ah = make_map(A.hi, naux, npair, ldk, 1, TC_BM, 2, fp16);
-  CUtensorMap al = make_map(A.lo, naux, npair, ldk, 1, TC_BM, 2, fp16);
-  CUtensorMap bh = make_map(W.hi, naux, naux, ldw, nw, BN, 3, fp16);
-  CUtensorMap bl = make_map(W.lo, naux, naux, ldw, nw, BN, 3, fp16);
+  constexpr int BK = TcPipe<EPI_ROWDOT>::BK;
+  CUtensorMap ah = make_map(A.hi, naux, npair, ldk, 1, TC_BM, 2, fp16, BK);
+  CUtensorMap al = make_map(A.lo, naux, npair, ldk, 1, TC_BM, 2, fp16, BK);
+  CUtensorMap bh = make_map(W.hi, naux, naux, ldw, nw, BN, 3, fp16, BK);
+  CUtensorMap bl = make_map(W.lo, naux, naux, ldw, nw, BN, 3, fp16, BK);
   int* d_err = tc_err_slot(ctx);
   QX_CUDA(cudaMemsetAsync(d_err, 0, sizeof(int), ctx->stream));
   TcArgs a{};
@@ -704,10 +719,11 @@ void launch_eps_tc(qx_ctx* ctx, const double* bov, int ldov, int naux, int nov, 
   float *sa = nullptr, *sb = nullptr;
   split(ctx, bov, naux, nov, ldov, 0, a_hi, a_lo, ldov, 0, 1, nullptr, 0, fp16, 0, &sa);
   split(ctx, bov, naux, nov, ldov, 0, b_hi, b_lo, ldov, a_elems, nw, chi, ldov, fp16, 1, &sb);
-  CUtensorMap ah = make_map(a_hi, nov, naux, ldov, 1, TC_BM, 2, fp16);
-  CUtensorMap al = make_map(a_lo, nov, naux, ldov, 1, TC_BM, 2, fp16);
-  CUtensorMap bh = make_map(b_hi, nov, naux, ldov, nw, BN, 3, fp16);
-  CUtensorMap bl = make_map(b_lo, nov, naux, ldov, nw, BN, 3, fp16);
+  constexpr int BK = TcPipe<EPI_STORE>::BK;
+  CUtensorMap ah = make_map(a_hi, nov, naux, ldov, 1, TC_BM, 2, fp16, BK);
+  CUtensorMap al = make_map(a_lo, nov, naux, ldov, 1, TC_BM, 2, fp16, BK);
+  CUtensorMap bh = make_map(b_hi, nov, naux, ldov, nw, BN, 3, fp16, BK);
+  CUtensorMap bl = make_map(b_lo, nov, naux, ldov, nw, BN, 3, fp16, BK);
   int* d_err = tc_err_slot(ctx);
   QX_CUDA(cudaMemsetAsync(d_err, 0, sizeof(int), ctx->stream));
   TcArgs a{};
@@ -736,10 +752,11 @@ void launch_eps_tc(qx_ctx* ctx, const double* bov, int ldov, int naux, int nov, 
 void launch_gemm_tc(qx_ctx* ctx, const TcOperand& A, int M, int lda, const TcOperand& B, int N, int ldb, int K,
                     int nbatch, double* out, int ldo, size_t out_stride, int fp16) {
   constexpr int BN = 128;
-  CUtensorMap ah = make_map(A.hi, K, M, lda, 1, TC_BM, 2, fp16);
-  CUtensorMap al = make_map(A.lo, K, M, lda, 1, TC_BM, 2, fp16);
-  CUtensorMap bh = make_map(B.hi, K, N, ldb, nbatch, BN, 3, fp16);
-  CUtensorMap bl = make_map(B.lo, K, N, ldb, nbatch, BN, 3, fp16);
+  constexpr int BK = TcPipe<EPI_STORE>::BK;
+  CUtensorMap ah = make_map(A.hi, K, M, lda, 1, TC_BM, 2, fp16, BK);
+  CUtensorMap al = make_map(A.lo, K, M, lda, 1, TC_BM, 2, fp16, BK);
+  CUtensorMap bh = make_map(B.hi, K, N, ldb, nbatch, BN, 3, fp16, BK);
+  CUtensorMap bl = make_map(B.lo, K, N, ldb, nbatch, BN, 3, fp16, BK);
   int* d_err = tc_err_slot(ctx);
   QX_CUDA(cudaMemsetAsync(d_err, 0, sizeof(int), ctx->stream));
   TcArgs a{};
