@@ -7,9 +7,11 @@ Workload (one "step" = one evGW iteration over all orbitals):
   Inputs are synthetic (seeded), far larger than L2 (lpq is 720 MB), so no
   explicit L2 flush is needed between steps.
 
-The headline value is the mixed-precision (tcgen05 BF16x3) form; the plain FP64
-GPU path is timed in the same run and the QP-energy error of the mixed form
-against it is reported in meV.  ``--impl reference`` times the reference's
+The headline value is the split-precision tcgen05 form (FP16x3 by default);
+the plain FP64 GPU path is timed in the same run and the QP-energy error of
+the split form against it is reported in meV.  The same line carries the
+64-system batched G0W0 (batch64_g0w0_cd), the differentiation workload
+(grad_nmo200) and the BSE-TDA Davidson (bse_dim26400).  ``--impl reference`` times the reference's
 algorithm on the host cores (the CPU oracle restatement; the Rust reference
 cannot be built here).
 """
@@ -38,7 +40,9 @@ HA_TO_MEV = 27211.386
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=5)
+    # 50 evGW iterations (~0.6 s): long enough that a driver stall under the
+    # nvidia-smi clock sampler (up to ~0.1 s) cannot dominate the timed region.
+    p.add_argument("--steps", type=int, default=50)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--precision", choices=["fp16x3", "bf16x3", "fp64"], default=None)

@@ -190,6 +190,24 @@ struct TcArgs {
   int* err;
 };
 
+// x[q] = xr[q] for the columns col0 + q < N of a valid row, 0 otherwise
+// (vector loads for a full chunk; indices are compile-time, x stays in registers).
+__device__ __forceinline__ void load_x16(const float* xr, int col0, int N, bool row_ok, float (&x)[16]) {
+  if (row_ok && col0 + 16 <= N) {
+#pragma unroll
+    for (int q = 0; q < 16; q += 4) {
+      const float4 v = *reinterpret_cast<const float4*>(xr + q);
+      x[q] = v.x;
+      x[q + 1] = v.y;
+      x[q + 2] = v.z;
+      x[q + 3] = v.w;
+    }
+  } else {
+#pragma unroll
+    for (int q = 0; q < 16; ++q) x[q] = (row_ok && col0 + q < N) ? xr[q] : 0.0f;
+  }
+}
+
 __device__ __forceinline__ double unscale_rowdot(const TcArgs& a, int w) {
   return 1.0 / ((double)a.scaleA[0] * (double)a.scaleB[w]);
 }
@@ -370,23 +388,23 @@ __global__ void __launch_bounds__(TcWarps<EPI>::THREADS, 1)
         tc_fence_after();
         const int n0 = nt * BN + half * HB;
         const uint32_t taddr = tmem_base + ((uint32_t)(quarter * 32) << 16) + buf * BN + half * HB;
+        // The pair-row values of the next 16 columns are loaded before the
+        // TMEM load of the current ones, so the two latencies overlap.
+        const float* xrow = args.X + (size_t)(m < args.M ? m : 0) * args.ldx + n0;
+        float xn[16];
+        load_x16(xrow, n0, args.N, m < args.M, xn);
 #pragma unroll 1
         for (int c = 0; c < HB; c += 16) {
+          float xc[16];
+#pragma unroll
+          for (int q = 0; q < 16; ++q) xc[q] = xn[q];
+          if (c + 16 < HB) load_x16(xrow + c + 16, n0 + c + 16, args.N, m < args.M, xn);
           float v[16];
           tmem_ld16(taddr + c, v);
-          if (m < args.M) {
-            const float* xr = args.X + (size_t)m * args.ldx + n0 + c;
-            if (n0 + c + 16 <= args.N) {
 #pragma unroll
-              for (int q = 0; q < 16; q += 4) {
-                const float4 xx = *reinterpret_cast<const float4*>(xr + q);
-                rowsum += (double)v[q] * xx.x + (double)v[q + 1] * xx.y + (double)v[q + 2] * xx.z +
-                          (double)v[q + 3] * xx.w;
-              }
-            } else {
-              for (int q = 0; q < 16 && n0 + c + q < args.N; ++q) rowsum += (double)v[q] * xr[q];
-            }
-          }
+          for (int q = 0; q < 16; q += 4)
+            rowsum += (double)v[q] * xc[q] + (double)v[q + 1] * xc[q + 1] + (double)v[q + 2] * xc[q + 2] +
+                      (double)v[q + 3] * xc[q + 3];
         }
         tc_fence_before();
         __syncwarp();
