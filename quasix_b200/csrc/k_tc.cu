@@ -532,6 +532,20 @@ __global__ void k_amax(const double* __restrict__ src, int rows, int cols, int l
   if ((threadIdx.x & 31) == 0) atomicMax(out + b, __double_as_longlong(m));
 }
 
+// Power-of-two scale s for batch b: the largest 2^k with 2^k * bound <= 32768,
+// bound = amax_src * amax_col (fp16 only; 1 for bf16 or an empty bound).
+__device__ __forceinline__ float split_scale(int fp16, int b, size_t src_stride,
+                                             const unsigned long long* __restrict__ amax_src,
+                                             const unsigned long long* __restrict__ amax_col) {
+  float s = 1.0f;
+  if (fp16) {
+    double bound = __longlong_as_double(amax_src[src_stride ? b : 0]);
+    if (amax_col) bound *= __longlong_as_double(amax_col[b]);
+    if (bound > 0.0 && isfinite(bound)) s = exp2f(floorf(log2f((float)(32768.0 / bound))));
+  }
+  return s;
+}
+
 // Split s*x*c into hi/lo (bf16 or fp16).  c = colscale[b][col] (or 1); s is a
 // power of two from the bound amax_src * amax_col (fp16 only, else 1) and is
 // written to scale_out[b].
@@ -540,12 +554,7 @@ __global__ void k_split(const double* __restrict__ src, int rows, int cols, int 
                         int ld_dst, size_t dst_stride, int fp16, const unsigned long long* __restrict__ amax_src,
                         const unsigned long long* __restrict__ amax_col, float* __restrict__ scale_out) {
   const int b = blockIdx.y;
-  float s = 1.0f;
-  if (fp16) {
-    double bound = __longlong_as_double(amax_src[src_stride ? b : 0]);
-    if (amax_col) bound *= __longlong_as_double(amax_col[b]);
-    if (bound > 0.0 && isfinite(bound)) s = exp2f(floorf(log2f((float)(32768.0 / bound))));
-  }
+  const float s = split_scale(fp16, b, src_stride, amax_src, amax_col);
   if (blockIdx.x == 0 && threadIdx.x == 0 && scale_out) scale_out[b] = s;
   const size_t total = (size_t)rows * ld_dst;
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
@@ -567,6 +576,82 @@ __global__ void k_split(const double* __restrict__ src, int rows, int cols, int 
       reinterpret_cast<__nv_bfloat16*>(hi_)[(size_t)b * dst_stride + i] = h;
       reinterpret_cast<__nv_bfloat16*>(lo_)[(size_t)b * dst_stride + i] = __float2bfloat16_rn((float)rem);
     }
+  }
+}
+
+// k_split with eight destination columns per thread: double2 loads and one
+// 16-byte store each of hi and lo.  Same rounding as k_split, element for
+// element.  Requires ld_dst % 8 == 0 (a group never straddles rows), 16-byte
+// aligned hi/lo with dst_stride % 8 == 0, and 16-byte aligned src (and
+// colscale) with even ld_src, src_stride (and ld_cs).
+template <bool FP16>
+__global__ void k_split8(const double* __restrict__ src, int rows, int cols, int ld_src, size_t src_stride,
+                         const double* __restrict__ colscale, int ld_cs, void* __restrict__ hi_,
+                         void* __restrict__ lo_, int ld_dst, size_t dst_stride,
+                         const unsigned long long* __restrict__ amax_src,
+                         const unsigned long long* __restrict__ amax_col, float* __restrict__ scale_out) {
+  const int b = blockIdx.y;
+  const float s = split_scale(FP16, b, src_stride, amax_src, amax_col);
+  if (blockIdx.x == 0 && threadIdx.x == 0 && scale_out) scale_out[b] = s;
+  const int groups_per_row = ld_dst >> 3;
+  const size_t total = (size_t)rows * groups_per_row;
+  const double* S = src + (size_t)b * src_stride;
+  const double* CS = colscale ? colscale + (size_t)b * ld_cs : nullptr;
+  uint4* H = reinterpret_cast<uint4*>(reinterpret_cast<uint16_t*>(hi_) + (size_t)b * dst_stride);
+  uint4* L = reinterpret_cast<uint4*>(reinterpret_cast<uint16_t*>(lo_) + (size_t)b * dst_stride);
+  for (size_t g = (size_t)blockIdx.x * blockDim.x + threadIdx.x; g < total; g += (size_t)gridDim.x * blockDim.x) {
+    const int r = (int)(g / groups_per_row), c0 = (int)(g % groups_per_row) << 3;
+    const double* row = S + (size_t)r * ld_src + c0;
+    double x[8];
+    if (c0 + 8 <= cols) {
+#pragma unroll
+      for (int j = 0; j < 8; j += 2) {
+        const double2 v = *reinterpret_cast<const double2*>(row + j);
+        x[j] = v.x;
+        x[j + 1] = v.y;
+      }
+      if (CS) {
+#pragma unroll
+        for (int j = 0; j < 8; j += 2) {
+          const double2 v = *reinterpret_cast<const double2*>(CS + c0 + j);
+          x[j] *= v.x;
+          x[j + 1] *= v.y;
+        }
+      }
+    } else {
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        x[j] = 0.0;
+        if (c0 + j < cols) {
+          x[j] = row[j];
+          if (CS) x[j] *= CS[c0 + j];
+        }
+      }
+    }
+    uint32_t hw[4], lw[4];
+#pragma unroll
+    for (int j = 0; j < 8; j += 2) {
+      uint16_t hb[2], lb[2];
+#pragma unroll
+      for (int k = 0; k < 2; ++k) {
+        const double v = x[j + k] * (double)s;
+        if (FP16) {
+          const __half h = __float2half_rn((float)v);
+          const __half l = __float2half_rn((float)(v - (double)__half2float(h)));
+          hb[k] = __half_as_ushort(h);
+          lb[k] = __half_as_ushort(l);
+        } else {
+          const __nv_bfloat16 h = __float2bfloat16_rn((float)v);
+          const __nv_bfloat16 l = __float2bfloat16_rn((float)(v - (double)__bfloat162float(h)));
+          hb[k] = __bfloat16_as_ushort(h);
+          lb[k] = __bfloat16_as_ushort(l);
+        }
+      }
+      hw[j >> 1] = (uint32_t)hb[0] | ((uint32_t)hb[1] << 16);
+      lw[j >> 1] = (uint32_t)lb[0] | ((uint32_t)lb[1] << 16);
+    }
+    H[g] = make_uint4(hw[0], hw[1], hw[2], hw[3]);
+    L[g] = make_uint4(lw[0], lw[1], lw[2], lw[3]);
   }
 }
 
@@ -606,10 +691,25 @@ static void split(qx_ctx* ctx, const double* src, int rows, int cols, int ld_src
       check_launch(ctx);
     }
   }
-  const size_t total = (size_t)rows * ld_dst;
-  dim3 grid((unsigned)std::min<size_t>((total + 255) / 256, 4096), batch);
-  k_split<<<grid, 256, 0, ctx->stream>>>(src, rows, cols, ld_src, src_stride, colscale, ld_cs, hi, lo, ld_dst,
-                                         dst_stride, fp16, sc.amax_src, colscale ? sc.amax_col : nullptr, sc.scale);
+  auto a16 = [](const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; };
+  const bool vec = ld_dst % 8 == 0 && dst_stride % 8 == 0 && a16(hi) && a16(lo) && ld_src % 2 == 0 &&
+                   src_stride % 2 == 0 && a16(src) && (!colscale || (a16(colscale) && ld_cs % 2 == 0));
+  const unsigned long long* acol = colscale ? sc.amax_col : nullptr;
+  if (vec) {
+    const size_t groups = (size_t)rows * (ld_dst / 8);
+    dim3 grid((unsigned)std::min<size_t>((groups + 255) / 256, 4096), batch);
+    if (fp16)
+      k_split8<true><<<grid, 256, 0, ctx->stream>>>(src, rows, cols, ld_src, src_stride, colscale, ld_cs, hi, lo,
+                                                    ld_dst, dst_stride, sc.amax_src, acol, sc.scale);
+    else
+      k_split8<false><<<grid, 256, 0, ctx->stream>>>(src, rows, cols, ld_src, src_stride, colscale, ld_cs, hi, lo,
+                                                     ld_dst, dst_stride, sc.amax_src, acol, sc.scale);
+  } else {
+    const size_t total = (size_t)rows * ld_dst;
+    dim3 grid((unsigned)std::min<size_t>((total + 255) / 256, 4096), batch);
+    k_split<<<grid, 256, 0, ctx->stream>>>(src, rows, cols, ld_src, src_stride, colscale, ld_cs, hi, lo, ld_dst,
+                                           dst_stride, fp16, sc.amax_src, acol, sc.scale);
+  }
   check_launch(ctx);
   if (scale_out) *scale_out = sc.scale;
 }
