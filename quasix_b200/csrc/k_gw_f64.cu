@@ -351,8 +351,10 @@ __global__ void k_sweep_write(double* __restrict__ M, int n, int ldn, size_t str
   for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < n * kb; idx += gridDim.x * blockDim.x) {
     const int r = idx / kb, q = idx % kb;
     // Save the old panel for the update (rows outside K; their mirror
-    // writes below land in rows inside K, which no thread reads here).
-    if (r < k0 || r >= k0 + kb) Pw[(size_t)r * SWEEP_NB + q] = A[(size_t)r * ldn + k0 + q];
+    // writes below land in rows inside K, which no thread reads here).  The
+    // rows inside K are unused by the update and set to zero, so that a split
+    // of P (its scale bound) sees no stale values.
+    Pw[(size_t)r * SWEEP_NB + q] = (r < k0 || r >= k0 + kb) ? A[(size_t)r * ldn + k0 + q] : 0.0;
     // Inside the K block both (r, q) and its mirror write the same element:
     // take D's lower triangle for both, so the stored value does not depend on
     // which write lands last.
@@ -418,7 +420,8 @@ static void sweep_update(qx_ctx* ctx, cudaStream_t st, double* eps, int n, int l
   check_launch(ctx);
 }
 
-void launch_invert_wc(qx_ctx* ctx, double* eps, int n, int ldn, size_t stride, int nw, int half_lower) {
+void launch_invert_wc(qx_ctx* ctx, double* eps, int n, int ldn, size_t stride, int nw, int half_lower,
+                      int split_update) {
   const size_t pstride = (size_t)n * SWEEP_NB;
   const size_t dsz = (size_t)nw * SWEEP_NB * SWEEP_NB;
   DevBuf& pan = ctx->ws[WS_PANEL];
@@ -437,6 +440,18 @@ void launch_invert_wc(qx_ctx* ctx, double* eps, int n, int ldn, size_t stride, i
   QX_CUDA(cudaMemsetAsync(status, 0, nw * sizeof(int), ctx->stream));
   sweep_attributes_once();
   const int nsteps = ceil_div(n, SWEEP_NB);
+  // Split form: panel splits (two steps in flight) and one tcgen05 error word
+  // per update launch, zeroed here on the context stream.
+  const bool tc = split_update && nsteps > 1;
+  void* split_base = nullptr;
+  int* tc_err = nullptr;
+  if (tc) {
+    DevBuf& sb = ctx->ws[WS_SWEEP_SPLIT];
+    sb.reserve((size_t)2 * 4 * nw * n * SWEEP_NB * 2);
+    split_base = sb.ptr;
+    tc_err = status_words(ctx, 2 * nsteps);
+    QX_CUDA(cudaMemsetAsync(tc_err, 0, 2 * nsteps * sizeof(int), ctx->stream));
+  }
   if (nsteps == 1) {
     sweep_front(ctx, ctx->stream, eps, n, ldn, stride, nw, 0, n, T0, D0, P0, pstride, status);
   } else {
@@ -460,16 +475,26 @@ void launch_invert_wc(qx_ctx* ctx, double* eps, int n, int ldn, size_t stride, i
       const int k0 = step * SWEEP_NB, kb = min(SWEEP_NB, n - k0);
       const int b = step & 1;
       sweep_front(ctx, s0, eps, n, ldn, stride, nw, k0, kb, Tb[b], Db[b], Pb[b], pstride, status);
+      SweepSplit sp{};
+      if (tc) sp = launch_sweep_split(ctx, s0, Tb[b], Pb[b], n, kb, nw, b, split_base);
       // The previous step's trailing update must be done before this step's
       // updates touch the same tiles.
       if (step > 0) QX_CUDA(cudaStreamWaitEvent(s0, ev_rest, 0));
       if (step + 1 < nsteps) {
         const int nk0 = k0 + SWEEP_NB, nkb = min(SWEEP_NB, n - nk0);
         QX_CUDA(cudaEventRecord(ev_front, s0));
-        sweep_update(ctx, s0, eps, n, ldn, stride, nw, k0, kb, Tb[b], Pb[b], pstride, 1, nk0, nkb);
+        if (tc)
+          launch_sweep_update_tc(ctx, s0, eps, n, ldn, stride, nw, step, sp, 1, step + 1, tc_err + 2 * step);
+        else
+          sweep_update(ctx, s0, eps, n, ldn, stride, nw, k0, kb, Tb[b], Pb[b], pstride, 1, nk0, nkb);
         QX_CUDA(cudaStreamWaitEvent(s1, ev_front, 0));
-        sweep_update(ctx, s1, eps, n, ldn, stride, nw, k0, kb, Tb[b], Pb[b], pstride, 2, nk0, nkb);
+        if (tc)
+          launch_sweep_update_tc(ctx, s1, eps, n, ldn, stride, nw, step, sp, 2, step + 1, tc_err + 2 * step + 1);
+        else
+          sweep_update(ctx, s1, eps, n, ldn, stride, nw, k0, kb, Tb[b], Pb[b], pstride, 2, nk0, nkb);
         QX_CUDA(cudaEventRecord(ev_rest, s1));
+      } else if (tc) {
+        launch_sweep_update_tc(ctx, s0, eps, n, ldn, stride, nw, step, sp, 0, -1, tc_err + 2 * step);
       } else {
         sweep_update(ctx, s0, eps, n, ldn, stride, nw, k0, kb, Tb[b], Pb[b], pstride, 0, 0, 0);
       }
@@ -481,6 +506,7 @@ void launch_invert_wc(qx_ctx* ctx, double* eps, int n, int ldn, size_t stride, i
   k_finish_wc<<<fg, 256, 0, ctx->stream>>>(eps, n, ldn, stride, status, half_lower);
   check_launch(ctx);
   ctx->pending.push_back({status, nw, 1});
+  if (tc) ctx->pending.push_back({tc_err, 2 * nsteps, 0});
 }
 
 void launch_invert_wc_panels(qx_ctx* ctx, double* eps, int n, int ldn, size_t stride, int nw, double* Tp,

@@ -151,6 +151,26 @@ template <int EPI>
 struct TcPipe {
   static constexpr int BK = 64;
   static constexpr int STAGES = 2;
+  static constexpr int UNIT = 1;  // unused by ROWDOT (one accumulation unit per N tile)
+};
+// STORE (the FP64-output GEMMs: P0, the BSE direct term): the accumulator
+// restarts every UNIT k-blocks and the epilogue sums the units in FP64.  The
+// FP32 -> FP64 conversions of one drain cost about as much as the MMAs of one
+// 64-wide k-block, so a drain per block left P0 drain-bound: at nmo 300 /
+// naux 1000 / nw 32, P0 took 2.29 ms per evGW iteration with UNIT 1, 1.93 ms
+// with UNIT 2 and 1.72 ms with UNIT 4, at QP errors against FP64 of 0.024,
+// 0.036 and 0.068 meV.  A third stage measured no faster.
+#ifndef QX_TC_STORE_STAGES
+#define QX_TC_STORE_STAGES 2
+#endif
+#ifndef QX_TC_STORE_UNIT
+#define QX_TC_STORE_UNIT 2
+#endif
+template <>
+struct TcPipe<1> {
+  static constexpr int BK = 64;
+  static constexpr int STAGES = QX_TC_STORE_STAGES;
+  static constexpr int UNIT = QX_TC_STORE_UNIT;
 };
 // Epilogue warps: 4 (ROWDOT: one TMEM lane quarter each) or 8 (STORE: two
 // warps per lane quarter, 64 columns each).
@@ -185,9 +205,19 @@ struct TcArgs {
   int add_identity;     // STORE: add delta_mn
   int fp16;             // operand type: 0 bf16, 1 fp16
   int tri;              // ROWDOT with lower-triangular B: N tile n0 needs K < n0 + BN, result x2
-  const float* scaleA;  // [1]      scale applied to A before the split
+  const float* scaleA;  // [1] (or [nbatch] with a_batched) scale applied to A before the split
   const float* scaleB;  // [nbatch] scale applied to B[w] before the split
   int* err;
+  // STORE, trailing update of the block sweep (subtract = 1, with
+  // lower_tiles): out = out - C; the tiles whose row or column index is
+  // skip_tile are left alone; filter_mode 1 keeps only the tiles whose row or
+  // column index is filter_tile, 2 only the others (0: no filter).
+  // a_batched: A has a batch index (3D map) and a scale per batch.
+  int a_batched;
+  int subtract;
+  int skip_tile;
+  int filter_mode;
+  int filter_tile;
 };
 
 // x[q] = xr[q] for the columns col0 + q < N of a valid row, 0 otherwise
@@ -258,6 +288,14 @@ __global__ void __launch_bounds__(TcWarps<EPI>::THREADS, 1)
     }
     nt_end = nt_begin + 1;
   }
+  if (EPI == EPI_STORE && args.subtract) {
+    // Whole-CTA exit before any barrier or TMEM allocation.
+    if (mb == args.skip_tile || nt_begin == args.skip_tile) return;
+    if (args.filter_mode) {
+      const bool touches = (mb == args.filter_tile || nt_begin == args.filter_tile);
+      if (touches != (args.filter_mode == 1)) return;
+    }
+  }
   const bool active = (w < args.nbatch);
   const int m0 = mb * TC_BM;
   const int k_blocks = (args.K + TC_BK - 1) / TC_BK;
@@ -302,8 +340,13 @@ __global__ void __launch_bounds__(TcWarps<EPI>::THREADS, 1)
             uint8_t* st = smem + s * L::STAGE_BYTES;
             mbar_expect_tx(&full[s], L::STAGE_BYTES);
             const int k0 = kb * TC_BK;
-            tma_load_2d(st, &mapAh, &full[s], k0, m0);
-            tma_load_2d(st + L::A_BYTES, &mapAl, &full[s], k0, m0);
+            if (args.a_batched) {
+              tma_load_3d(st, &mapAh, &full[s], k0, m0, w);
+              tma_load_3d(st + L::A_BYTES, &mapAl, &full[s], k0, m0, w);
+            } else {
+              tma_load_2d(st, &mapAh, &full[s], k0, m0);
+              tma_load_2d(st + L::A_BYTES, &mapAl, &full[s], k0, m0);
+            }
             tma_load_3d(st + 2 * L::A_BYTES, &mapBh, &full[s], k0, n0, w);
             tma_load_3d(st + 2 * L::A_BYTES + L::B_BYTES, &mapBl, &full[s], k0, n0, w);
             issued = g + 1;
@@ -321,8 +364,8 @@ __global__ void __launch_bounds__(TcWarps<EPI>::THREADS, 1)
     } else if (warp == 1) {
       // ---------------- MMA issuer ----------------
       // Accumulation units: ROWDOT accumulates a whole N tile in one TMEM
-      // buffer; STORE restarts the accumulator every k-block (64 of K) and the
-      // epilogue sums the blocks in FP64, because the FP32 accumulation of the
+      // buffer; STORE restarts the accumulator every UNIT k-blocks and the
+      // epilogue sums the units in FP64, because the FP32 accumulation of the
       // tensor pipe carries a small same-signed error per step that grows
       // linearly over long positive sums (the diagonal of Pi over K = nov).
       if (lane == 0) {
@@ -332,8 +375,9 @@ __global__ void __launch_bounds__(TcWarps<EPI>::THREADS, 1)
         for (int nt = nt_begin; nt < nt_end && ok; ++nt) {
           const int kbe = args.tri ? min(k_blocks, (nt * BN + BN + TC_BK - 1) / TC_BK) : k_blocks;
           for (int kb = 0; kb < kbe; ++kb, ++g) {
-            const bool unit_start = (EPI == EPI_STORE) || kb == 0;
-            const bool unit_end = (EPI == EPI_STORE) || kb == kbe - 1;
+            constexpr int UNIT = TcPipe<EPI>::UNIT;
+            const bool unit_start = (EPI == EPI_STORE) ? (kb % UNIT == 0) : kb == 0;
+            const bool unit_end = (EPI == EPI_STORE) ? (kb % UNIT == UNIT - 1 || kb == kbe - 1) : kb == kbe - 1;
             const int buf = u & 1;
             if (unit_start && u >= 2) {
               if (!mbar_wait(&acc_empty[buf], ((u / 2) - 1) & 1, abort_flag, args.err, 2)) {
@@ -424,12 +468,13 @@ __global__ void __launch_bounds__(TcWarps<EPI>::THREADS, 1)
       const int quarter = warp & 3;
       const int half = (warp - 2) >> 2;  // columns [64 half, 64 half + 64) of the tile
       const int m = m0 + quarter * 32 + lane;
-      const double unscale = 1.0 / ((double)args.scaleA[0] * (double)args.scaleB[w]);
+      const double unscale = 1.0 / ((double)args.scaleA[args.a_batched ? w : 0] * (double)args.scaleB[w]);
       double acc[64];
 #pragma unroll
       for (int c = 0; c < 64; ++c) acc[c] = 0.0;
       bool ok = true;
-      for (int u = 0; u < k_blocks; ++u) {
+      const int n_units = (k_blocks + TcPipe<EPI>::UNIT - 1) / TcPipe<EPI>::UNIT;
+      for (int u = 0; u < n_units; ++u) {
         const int buf = u & 1;
         if (!mbar_wait(&acc_full[buf], (u / 2) & 1, abort_flag, args.err, 4)) {
           ok = false;
@@ -457,7 +502,8 @@ __global__ void __launch_bounds__(TcWarps<EPI>::THREADS, 1)
           // Lower-triangular mode writes the lower triangle and mirrors it,
           // so the stored matrix is exactly symmetric.
           if (n < args.N && !(args.lower_tiles && n > m)) {
-            const double val = acc[c] * unscale + ((args.add_identity && m == n) ? 1.0 : 0.0);
+            const double val = args.subtract ? orow[n] - acc[c] * unscale
+                                             : acc[c] * unscale + ((args.add_identity && m == n) ? 1.0 : 0.0);
             orow[n] = val;
             if (args.lower_tiles && n != m) args.out[(size_t)w * args.out_stride + (size_t)n * args.ldo + m] = val;
           }
@@ -518,18 +564,41 @@ bool tc_supported(qx_ctx* ctx) {
   return p.major == 10;
 }
 
-// max|x| per batch (x >= 0 compares as its bit pattern).
+// max|x| per batch (x >= 0 compares as its bit pattern).  Index type I: 32-bit
+// when rows * cols < 2^31 (the division per element is then cheap).  Four
+// independent loads per thread and step keep enough bytes in flight for HBM.
+template <typename I>
 __global__ void k_amax(const double* __restrict__ src, int rows, int cols, int ld, size_t stride,
                        unsigned long long* __restrict__ out) {
   const int b = blockIdx.y;
+  const double* S = src + (size_t)b * stride;
   double m = 0.0;
-  const size_t total = (size_t)rows * cols;
-  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
-    const int r = (int)(i / cols), c = (int)(i % cols);
-    m = fmax(m, fabs(src[(size_t)b * stride + (size_t)r * ld + c]));
+  const I total = (I)rows * (I)cols, ucols = (I)cols;
+  const I step = (I)gridDim.x * blockDim.x;
+  for (I i = (I)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += 4 * step) {
+    double v[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const I j = i + (I)u * step;
+      v[u] = 0.0;
+      if (j < total) {
+        const I r = j / ucols, c = j - r * ucols;
+        v[u] = fabs(S[(size_t)r * ld + c]);
+      }
+    }
+    m = fmax(m, fmax(fmax(v[0], v[1]), fmax(v[2], v[3])));
   }
+  // One atomic per block: same-address atomics serialise in L2, so a per-warp
+  // atomic over thousands of blocks costs more than the pass itself.
+  __shared__ double wmax[32];
   for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-  if ((threadIdx.x & 31) == 0) atomicMax(out + b, __double_as_longlong(m));
+  if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    m = threadIdx.x < (blockDim.x >> 5) ? wmax[threadIdx.x] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if (threadIdx.x == 0) atomicMax(out + b, __double_as_longlong(m));
+  }
 }
 
 // Power-of-two scale s for batch b: the largest 2^k with 2^k * bound <= 32768,
@@ -579,11 +648,72 @@ __global__ void k_split(const double* __restrict__ src, int rows, int cols, int 
   }
 }
 
+// Eight source values of row `row` from column c0 (zero past cols), times the
+// column scales cs[c0..] when cs is given.  16-byte loads for a full group.
+__device__ __forceinline__ void load8(const double* __restrict__ row, const double* __restrict__ cs, int c0,
+                                      int cols, double (&x)[8]) {
+  if (c0 + 8 <= cols) {
+#pragma unroll
+    for (int j = 0; j < 8; j += 2) {
+      const double2 v = *reinterpret_cast<const double2*>(row + c0 + j);
+      x[j] = v.x;
+      x[j + 1] = v.y;
+    }
+    if (cs) {
+#pragma unroll
+      for (int j = 0; j < 8; j += 2) {
+        const double2 v = *reinterpret_cast<const double2*>(cs + c0 + j);
+        x[j] *= v.x;
+        x[j + 1] *= v.y;
+      }
+    }
+  } else {
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      x[j] = 0.0;
+      if (c0 + j < cols) {
+        x[j] = row[c0 + j];
+        if (cs) x[j] *= cs[c0 + j];
+      }
+    }
+  }
+}
+
+// hi/lo of s*x[0..8) packed into one 16-byte word each (same rounding as k_split).
+template <bool FP16>
+__device__ __forceinline__ void split8_store(const double (&x)[8], float s, uint4* __restrict__ H,
+                                             uint4* __restrict__ L) {
+  uint32_t hw[4], lw[4];
+#pragma unroll
+  for (int j = 0; j < 8; j += 2) {
+    uint16_t hb[2], lb[2];
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+      const double v = x[j + k] * (double)s;
+      if (FP16) {
+        const __half h = __float2half_rn((float)v);
+        const __half l = __float2half_rn((float)(v - (double)__half2float(h)));
+        hb[k] = __half_as_ushort(h);
+        lb[k] = __half_as_ushort(l);
+      } else {
+        const __nv_bfloat16 h = __float2bfloat16_rn((float)v);
+        const __nv_bfloat16 l = __float2bfloat16_rn((float)(v - (double)__bfloat162float(h)));
+        hb[k] = __bfloat16_as_ushort(h);
+        lb[k] = __bfloat16_as_ushort(l);
+      }
+    }
+    hw[j >> 1] = (uint32_t)hb[0] | ((uint32_t)hb[1] << 16);
+    lw[j >> 1] = (uint32_t)lb[0] | ((uint32_t)lb[1] << 16);
+  }
+  *H = make_uint4(hw[0], hw[1], hw[2], hw[3]);
+  *L = make_uint4(lw[0], lw[1], lw[2], lw[3]);
+}
+
 // k_split with eight destination columns per thread: double2 loads and one
 // 16-byte store each of hi and lo.  Same rounding as k_split, element for
 // element.  Requires ld_dst % 8 == 0 (a group never straddles rows), 16-byte
-// aligned hi/lo with dst_stride % 8 == 0, and 16-byte aligned src (and
-// colscale) with even ld_src, src_stride (and ld_cs).
+// aligned hi/lo with dst_stride % 8 == 0, 16-byte aligned src (and colscale)
+// with even ld_src, src_stride (and ld_cs), and rows * ld_dst / 8 < 2^31.
 template <bool FP16>
 __global__ void k_split8(const double* __restrict__ src, int rows, int cols, int ld_src, size_t src_stride,
                          const double* __restrict__ colscale, int ld_cs, void* __restrict__ hi_,
@@ -593,65 +723,64 @@ __global__ void k_split8(const double* __restrict__ src, int rows, int cols, int
   const int b = blockIdx.y;
   const float s = split_scale(FP16, b, src_stride, amax_src, amax_col);
   if (blockIdx.x == 0 && threadIdx.x == 0 && scale_out) scale_out[b] = s;
-  const int groups_per_row = ld_dst >> 3;
-  const size_t total = (size_t)rows * groups_per_row;
+  const unsigned gpr = (unsigned)ld_dst >> 3;
+  const unsigned total = (unsigned)rows * gpr;
   const double* S = src + (size_t)b * src_stride;
   const double* CS = colscale ? colscale + (size_t)b * ld_cs : nullptr;
   uint4* H = reinterpret_cast<uint4*>(reinterpret_cast<uint16_t*>(hi_) + (size_t)b * dst_stride);
   uint4* L = reinterpret_cast<uint4*>(reinterpret_cast<uint16_t*>(lo_) + (size_t)b * dst_stride);
-  for (size_t g = (size_t)blockIdx.x * blockDim.x + threadIdx.x; g < total; g += (size_t)gridDim.x * blockDim.x) {
-    const int r = (int)(g / groups_per_row), c0 = (int)(g % groups_per_row) << 3;
-    const double* row = S + (size_t)r * ld_src + c0;
+  for (unsigned g = blockIdx.x * blockDim.x + threadIdx.x; g < total; g += gridDim.x * blockDim.x) {
+    const unsigned r = g / gpr;
+    const int c0 = (int)(g - r * gpr) << 3;
     double x[8];
-    if (c0 + 8 <= cols) {
-#pragma unroll
-      for (int j = 0; j < 8; j += 2) {
-        const double2 v = *reinterpret_cast<const double2*>(row + j);
-        x[j] = v.x;
-        x[j + 1] = v.y;
-      }
-      if (CS) {
+    load8(S + (size_t)r * ld_src, CS, c0, cols, x);
+    split8_store<FP16>(x, s, H + g, L + g);
+  }
+}
+
+// k_split8 for one source shared by every batch (src_stride == 0) with a
+// column scale per batch (the chi-scaled operand of P0): each thread reads its
+// eight source values once and writes the hi/lo groups of all batches, so the
+// FP64 source crosses memory once instead of once per batch.  The per-batch
+// scales sit in shared memory ([batch] floats, batch <= 1024).
+template <bool FP16>
+__global__ void k_split8_bcast(const double* __restrict__ src, int rows, int cols, int ld_src,
+                               const double* __restrict__ colscale, int ld_cs, void* __restrict__ hi_,
+                               void* __restrict__ lo_, int ld_dst, size_t dst_stride, int batch,
+                               const unsigned long long* __restrict__ amax_src,
+                               const unsigned long long* __restrict__ amax_col, float* __restrict__ scale_out) {
+  __shared__ float s_scale[1024];
+  for (int b = threadIdx.x; b < batch; b += blockDim.x) {
+    s_scale[b] = split_scale(FP16, b, 0, amax_src, amax_col);
+    if (blockIdx.x == 0 && scale_out) scale_out[b] = s_scale[b];
+  }
+  __syncthreads();
+  const unsigned gpr = (unsigned)ld_dst >> 3;
+  const unsigned total = (unsigned)rows * gpr;
+  uint4* H = reinterpret_cast<uint4*>(hi_);
+  uint4* L = reinterpret_cast<uint4*>(lo_);
+  const size_t bstride = dst_stride >> 3;  // in 16-byte groups
+  for (unsigned g = blockIdx.x * blockDim.x + threadIdx.x; g < total; g += gridDim.x * blockDim.x) {
+    const unsigned r = g / gpr;
+    const int c0 = (int)(g - r * gpr) << 3;
+    double x0[8];
+    load8(src + (size_t)r * ld_src, nullptr, c0, cols, x0);
+    for (int b = 0; b < batch; ++b) {
+      const double* cs = colscale + (size_t)b * ld_cs;
+      double x[8];
+      if (c0 + 8 <= cols) {
 #pragma unroll
         for (int j = 0; j < 8; j += 2) {
-          const double2 v = *reinterpret_cast<const double2*>(CS + c0 + j);
-          x[j] *= v.x;
-          x[j + 1] *= v.y;
+          const double2 v = *reinterpret_cast<const double2*>(cs + c0 + j);
+          x[j] = x0[j] * v.x;
+          x[j + 1] = x0[j + 1] * v.y;
         }
-      }
-    } else {
+      } else {
 #pragma unroll
-      for (int j = 0; j < 8; ++j) {
-        x[j] = 0.0;
-        if (c0 + j < cols) {
-          x[j] = row[j];
-          if (CS) x[j] *= CS[c0 + j];
-        }
+        for (int j = 0; j < 8; ++j) x[j] = (c0 + j < cols) ? x0[j] * cs[c0 + j] : 0.0;
       }
+      split8_store<FP16>(x, s_scale[b], H + b * bstride + g, L + b * bstride + g);
     }
-    uint32_t hw[4], lw[4];
-#pragma unroll
-    for (int j = 0; j < 8; j += 2) {
-      uint16_t hb[2], lb[2];
-#pragma unroll
-      for (int k = 0; k < 2; ++k) {
-        const double v = x[j + k] * (double)s;
-        if (FP16) {
-          const __half h = __float2half_rn((float)v);
-          const __half l = __float2half_rn((float)(v - (double)__half2float(h)));
-          hb[k] = __half_as_ushort(h);
-          lb[k] = __half_as_ushort(l);
-        } else {
-          const __nv_bfloat16 h = __float2bfloat16_rn((float)v);
-          const __nv_bfloat16 l = __float2bfloat16_rn((float)(v - (double)__bfloat162float(h)));
-          hb[k] = __bfloat16_as_ushort(h);
-          lb[k] = __bfloat16_as_ushort(l);
-        }
-      }
-      hw[j >> 1] = (uint32_t)hb[0] | ((uint32_t)hb[1] << 16);
-      lw[j >> 1] = (uint32_t)lb[0] | ((uint32_t)lb[1] << 16);
-    }
-    H[g] = make_uint4(hw[0], hw[1], hw[2], hw[3]);
-    L[g] = make_uint4(lw[0], lw[1], lw[2], lw[3]);
   }
 }
 
@@ -664,7 +793,7 @@ struct SplitScratch {
 };
 static SplitScratch split_scratch(qx_ctx* ctx, int slot_offset) {
   DevBuf& b = ctx->ws[WS_TCERR];
-  b.reserve(64 * 1024);
+  b.reserve(256 + 8 * 20480);
   uint8_t* p = b.as<uint8_t>() + 256 + slot_offset * 20480;
   SplitScratch s;
   s.amax_src = reinterpret_cast<unsigned long long*>(p);
@@ -675,19 +804,31 @@ static SplitScratch split_scratch(qx_ctx* ctx, int slot_offset) {
 
 static void split(qx_ctx* ctx, const double* src, int rows, int cols, int ld_src, size_t src_stride, void* hi,
                   void* lo, int ld_dst, size_t dst_stride, int batch, const double* colscale, int ld_cs, int fp16,
-                  int slot, float** scale_out) {
+                  int slot, float** scale_out, int reuse_src_amax_slot = -1, cudaStream_t stream = nullptr) {
   QX_REQUIRE(batch <= 1024, QX_ERR_INVALID_INPUT, "at most 1024 frequencies per split");
   SplitScratch sc = split_scratch(ctx, slot);
+  cudaStream_t st = stream ? stream : ctx->stream;
   if (fp16) {
     const int nsrc = src_stride ? batch : 1;
-    QX_CUDA(cudaMemsetAsync(sc.amax_src, 0, 2048 * sizeof(unsigned long long), ctx->stream));
-    const size_t tot = (size_t)rows * cols;
-    dim3 g1((unsigned)std::min<size_t>((tot + 255) / 256, 1024), nsrc);
-    k_amax<<<g1, 256, 0, ctx->stream>>>(src, rows, cols, ld_src, src_stride, sc.amax_src);
-    check_launch(ctx);
+    QX_CUDA(cudaMemsetAsync(sc.amax_src, 0, 2048 * sizeof(unsigned long long), st));
+    if (reuse_src_amax_slot >= 0) {
+      // The same source was split just before in that slot: take its bound.
+      sc.amax_src = split_scratch(ctx, reuse_src_amax_slot).amax_src;
+    } else {
+      // About eight blocks per SM over all batches, each thread four
+      // elements per step at least.
+      const size_t tot = (size_t)rows * cols;
+      const size_t per_batch = std::max<size_t>(1, 1184 / nsrc);
+      dim3 g1((unsigned)std::min<size_t>((tot + 1023) / 1024, per_batch), nsrc);
+      if (tot < (1u << 31))
+        k_amax<unsigned><<<g1, 256, 0, st>>>(src, rows, cols, ld_src, src_stride, sc.amax_src);
+      else
+        k_amax<size_t><<<g1, 256, 0, st>>>(src, rows, cols, ld_src, src_stride, sc.amax_src);
+      check_launch(ctx);
+    }
     if (colscale) {
-      dim3 g2(ceil_div(cols, 256), batch);
-      k_amax<<<g2, 256, 0, ctx->stream>>>(colscale, 1, cols, ld_cs, ld_cs, sc.amax_col);
+      dim3 g2(ceil_div(cols, 1024), batch);
+      k_amax<unsigned><<<g2, 256, 0, st>>>(colscale, 1, cols, ld_cs, ld_cs, sc.amax_col);
       check_launch(ctx);
     }
   }
@@ -695,19 +836,27 @@ static void split(qx_ctx* ctx, const double* src, int rows, int cols, int ld_src
   const bool vec = ld_dst % 8 == 0 && dst_stride % 8 == 0 && a16(hi) && a16(lo) && ld_src % 2 == 0 &&
                    src_stride % 2 == 0 && a16(src) && (!colscale || (a16(colscale) && ld_cs % 2 == 0));
   const unsigned long long* acol = colscale ? sc.amax_col : nullptr;
-  if (vec) {
-    const size_t groups = (size_t)rows * (ld_dst / 8);
+  const size_t groups = (size_t)rows * (ld_dst / 8);
+  if (vec && groups < (1u << 31) && src_stride == 0 && colscale && batch > 1) {
+    dim3 grid((unsigned)std::min<size_t>((groups + 255) / 256, 4096));
+    if (fp16)
+      k_split8_bcast<true><<<grid, 256, 0, st>>>(src, rows, cols, ld_src, colscale, ld_cs, hi, lo, ld_dst,
+                                                          dst_stride, batch, sc.amax_src, acol, sc.scale);
+    else
+      k_split8_bcast<false><<<grid, 256, 0, st>>>(src, rows, cols, ld_src, colscale, ld_cs, hi, lo, ld_dst,
+                                                           dst_stride, batch, sc.amax_src, acol, sc.scale);
+  } else if (vec && groups < (1u << 31)) {
     dim3 grid((unsigned)std::min<size_t>((groups + 255) / 256, 4096), batch);
     if (fp16)
-      k_split8<true><<<grid, 256, 0, ctx->stream>>>(src, rows, cols, ld_src, src_stride, colscale, ld_cs, hi, lo,
+      k_split8<true><<<grid, 256, 0, st>>>(src, rows, cols, ld_src, src_stride, colscale, ld_cs, hi, lo,
                                                     ld_dst, dst_stride, sc.amax_src, acol, sc.scale);
     else
-      k_split8<false><<<grid, 256, 0, ctx->stream>>>(src, rows, cols, ld_src, src_stride, colscale, ld_cs, hi, lo,
+      k_split8<false><<<grid, 256, 0, st>>>(src, rows, cols, ld_src, src_stride, colscale, ld_cs, hi, lo,
                                                      ld_dst, dst_stride, sc.amax_src, acol, sc.scale);
   } else {
     const size_t total = (size_t)rows * ld_dst;
     dim3 grid((unsigned)std::min<size_t>((total + 255) / 256, 4096), batch);
-    k_split<<<grid, 256, 0, ctx->stream>>>(src, rows, cols, ld_src, src_stride, colscale, ld_cs, hi, lo, ld_dst,
+    k_split<<<grid, 256, 0, st>>>(src, rows, cols, ld_src, src_stride, colscale, ld_cs, hi, lo, ld_dst,
                                            dst_stride, fp16, sc.amax_src, acol, sc.scale);
   }
   check_launch(ctx);
@@ -727,13 +876,13 @@ static void check_tc_err(qx_ctx* ctx, int* d_err) { ctx->pending.push_back({d_er
 
 template <int BN, int EPI>
 static void launch_tc(qx_ctx* ctx, const CUtensorMap& ah, const CUtensorMap& al, const CUtensorMap& bh,
-                      const CUtensorMap& bl, const TcArgs& a, dim3 grid) {
+                      const CUtensorMap& bl, const TcArgs& a, dim3 grid, cudaStream_t stream = nullptr) {
   using L = TcSmem<BN, EPI>;
   static std::once_flag attr_once;
   std::call_once(attr_once, [&] {
     QX_CUDA(cudaFuncSetAttribute(k_tc_gemm<BN, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, L::TOTAL));
   });
-  k_tc_gemm<BN, EPI><<<grid, TcWarps<EPI>::THREADS, L::TOTAL, ctx->stream>>>(ah, al, bh, bl, a);
+  k_tc_gemm<BN, EPI><<<grid, TcWarps<EPI>::THREADS, L::TOTAL, stream ? stream : ctx->stream>>>(ah, al, bh, bl, a);
   check_launch(ctx);
 }
 
@@ -836,7 +985,7 @@ void launch_eps_tc(qx_ctx* ctx, const double* bov, int ldov, int naux, int nov, 
   void* b_lo = p + a_elems * 4 + a_elems * 2 * nw;
   float *sa = nullptr, *sb = nullptr;
   split(ctx, bov, naux, nov, ldov, 0, a_hi, a_lo, ldov, 0, 1, nullptr, 0, fp16, 0, &sa);
-  split(ctx, bov, naux, nov, ldov, 0, b_hi, b_lo, ldov, a_elems, nw, chi, ldov, fp16, 1, &sb);
+  split(ctx, bov, naux, nov, ldov, 0, b_hi, b_lo, ldov, a_elems, nw, chi, ldov, fp16, 1, &sb, /*amax of bov*/ 0);
   constexpr int BK = TcPipe<EPI_STORE>::BK;
   CUtensorMap ah = make_map(a_hi, nov, naux, ldov, 1, TC_BM, 2, fp16, BK);
   CUtensorMap al = make_map(a_lo, nov, naux, ldov, 1, TC_BM, 2, fp16, BK);
@@ -895,6 +1044,66 @@ void launch_gemm_tc(qx_ctx* ctx, const TcOperand& A, int M, int lda, const TcOpe
   QX_REQUIRE(nbatch <= 65535, QX_ERR_INVALID_INPUT, "at most 65535 batches");
   launch_tc<BN, EPI_STORE>(ctx, ah, al, bh, bl, a, dim3(a.m_blocks * ceil_div(N, BN), nbatch));
   check_tc_err(ctx, d_err);
+}
+
+// Block sweep, FP16X3 trailing update.  The panels T = M[:, K] D and P = the
+// old M[:, K] ([nw][n][128] FP64; T is zero past column kb, P is zero in the
+// rows of K) are split into the half of `base` selected by buf, so that one
+// step can be split while the previous step's update still runs on the other
+// sweep stream; the scales go to split slots 3 + 2 buf (T) and 4 + 2 buf (P).
+SweepSplit launch_sweep_split(qx_ctx* ctx, cudaStream_t st, const double* Tp, const double* Pp, int n, int kb,
+                              int nw, int buf, void* base) {
+  const size_t elems = (size_t)nw * n * kSweepPanelCols;
+  const size_t ps = (size_t)n * kSweepPanelCols;
+  uint8_t* b = static_cast<uint8_t*>(base) + (size_t)buf * elems * 2 * 4;
+  SweepSplit sp;
+  sp.T.hi = b;
+  sp.T.lo = b + elems * 2;
+  sp.P.hi = b + elems * 4;
+  sp.P.lo = b + elems * 6;
+  split(ctx, Tp, n, kb, kSweepPanelCols, ps, sp.T.hi, sp.T.lo, kSweepPanelCols, ps, nw, nullptr, 0, 1, 3 + 2 * buf,
+        &sp.T.scale, -1, st);
+  split(ctx, Pp, n, kb, kSweepPanelCols, ps, sp.P.hi, sp.P.lo, kSweepPanelCols, ps, nw, nullptr, 0, 1, 4 + 2 * buf,
+        &sp.P.scale, -1, st);
+  return sp;
+}
+
+// M[w][r][c] -= sum_q T[w][r][q] P[w][c][q] on stream st over the lower
+// 128 x 128 tiles outside tile row/column kblk (the K block), mirrored;
+// mode / next_blk select the look-ahead subset (filter_mode of TcArgs).  err
+// is one status word, zero on entry.
+void launch_sweep_update_tc(qx_ctx* ctx, cudaStream_t st, double* eps, int n, int ldn, size_t stride, int nw,
+                            int kblk, const SweepSplit& sp, int mode, int next_blk, int* err) {
+  static_assert(kSweepPanelCols == TC_BM, "sweep block = tcgen05 tile");
+  constexpr int BN = 128;
+  constexpr int BK = TcPipe<EPI_STORE>::BK;
+  const int K = kSweepPanelCols;
+  CUtensorMap ah = make_map(sp.T.hi, K, n, K, nw, TC_BM, 3, 1, BK);
+  CUtensorMap al = make_map(sp.T.lo, K, n, K, nw, TC_BM, 3, 1, BK);
+  CUtensorMap bh = make_map(sp.P.hi, K, n, K, nw, BN, 3, 1, BK);
+  CUtensorMap bl = make_map(sp.P.lo, K, n, K, nw, BN, 3, 1, BK);
+  TcArgs a{};
+  a.M = n;
+  a.N = n;
+  a.K = K;
+  a.nbatch = nw;
+  a.m_blocks = ceil_div(n, TC_BM);
+  a.out = eps;
+  a.ldo = ldn;
+  a.out_stride = stride;
+  a.lower_tiles = 1;
+  a.subtract = 1;
+  a.a_batched = 1;
+  a.fp16 = 1;
+  a.scaleA = sp.T.scale;
+  a.scaleB = sp.P.scale;
+  a.err = err;
+  a.skip_tile = kblk;
+  a.filter_mode = mode;
+  a.filter_tile = next_blk;
+  const int tiles = ceil_div(n, TC_BM);
+  QX_REQUIRE(nw <= 65535, QX_ERR_INVALID_INPUT, "at most 65535 matrices per sweep");
+  launch_tc<BN, EPI_STORE>(ctx, ah, al, bh, bl, a, dim3(tiles * (tiles + 1) / 2, nw), st);
 }
 
 }  // namespace qx

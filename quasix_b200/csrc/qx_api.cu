@@ -261,7 +261,10 @@ void gw_wc_pairs(qx_ctx* ctx, GWSystem& S, const double* e_host) {
     launch_eps_fp64(ctx, S.bov, S.ldov, S.naux, S.nov, S.chi, S.nw, S.eps, S.ldn, S.eps_stride);
   record_stage(ctx, QX_ST_P0, false);
   record_stage(ctx, QX_ST_INV, true);
-  launch_invert_wc(ctx, S.eps, S.naux, S.ldn, S.eps_stride, S.nw, /*half_lower=*/1);
+  // Imaginary axis: eps is SPD with eigenvalues in [1, 1 + ||Pi||], so the
+  // split trailing update of the sweep keeps Wc within the split forms' error.
+  launch_invert_wc(ctx, S.eps, S.naux, S.ldn, S.eps_stride, S.nw, /*half_lower=*/1,
+                   /*split_update=*/is_tc_precision(S.precision));
   record_stage(ctx, QX_ST_INV, false);
   record_stage(ctx, QX_ST_CONTRACT, true);
   if (is_tc_precision(S.precision)) {

@@ -223,6 +223,8 @@ void CdEngine::residue_compute(CdResidueChunk& c, const CdResidue* list, int rc)
     launch_eps_tc(ctx, S.bov, S.ldov, naux, nov, c.chi, rc, c.eps, ldn, stride, precision == QX_PREC_FP16X3);
   else
     launch_eps_fp64(ctx, S.bov, S.ldov, naux, nov, c.chi, rc, c.eps, ldn, stride);
+  // Real axis: eps(w_r) is indefinite and can be ill-conditioned near an
+  // excitation, so the sweep stays FP64 here.
   launch_invert_wc(ctx, c.eps, naux, ldn, stride, rc);
   launch_cd_gather(ctx, d_lpq, naux, nmo, c.nm, rc, c.b, ldn);
   k_cd_solve_rows<<<dim3(ceil_div(naux, 8), rc), 256, 0, ctx->stream>>>(c.eps, ldn, stride, c.b, naux, ldn, c.x);

@@ -131,6 +131,7 @@ enum WsSlot {
   WS_CD0, WS_CD1, WS_CD2, WS_CD3,
   WS_TCERR,       // tcgen05 pipeline error word
   WS_GRAD0, WS_GRAD1, WS_GRAD2,  // CD adjoint: accumulators, per-frequency chunk, lpq gradient
+  WS_SWEEP_SPLIT,  // split sweep panels (two steps in flight)
   WS_COUNT
 };
 static_assert(WS_COUNT <= 40, "workspace slots");
@@ -192,7 +193,10 @@ void launch_eps_fp64(qx_ctx* ctx, const double* bov, int ldov, int naux, int nov
 // In-place inversion of nw SPD matrices by the block sweep operator;
 // output Wc = eps^-1 - I (FP64).
 // half_lower: return W' = strict-lower(Wc) + diag(Wc)/2 (zeros above) instead of Wc.
-void launch_invert_wc(qx_ctx* ctx, double* eps, int n, int ldn, size_t stride, int nw, int half_lower = 0);
+// split_update: run the trailing updates on tcgen05 in the FP16X3 form
+// (launch_sweep_update_tc); the diagonal blocks and panels stay FP64.
+void launch_invert_wc(qx_ctx* ctx, double* eps, int n, int ldn, size_t stride, int nw, int half_lower = 0,
+                      int split_update = 0);
 
 // The same sweep on caller-provided panels (no workspace, full Wc): Tp and Pp
 // hold nw * n * SWEEP_NB doubles each, Dp nw * SWEEP_NB^2, status nw ints that
@@ -258,7 +262,8 @@ struct TcOperand {
   float* scale;
 };
 inline bool is_tc_precision(int p) { return p == QX_PREC_BF16X3 || p == QX_PREC_FP16X3; }
-// slot selects one of the scratch areas for the scales (0..2).
+// slot selects one of the scratch areas for the scales (0..2; 3..6 belong to
+// the sweep).
 void launch_split(qx_ctx* ctx, const double* src, int rows, int cols, int ld_src, void* hi, void* lo, int ld_dst,
                   size_t src_stride, size_t dst_stride, int batch, int fp16, int slot, float** scale_out);
 void launch_eps_tc(qx_ctx* ctx, const double* bov, int ldov, int naux, int nov, const double* chi, int nw,
@@ -268,6 +273,18 @@ void launch_gemm_tc(qx_ctx* ctx, const TcOperand& A, int M, int lda, const TcOpe
 void launch_pair_contract_tc(qx_ctx* ctx, const TcOperand& A, const float* bpt_f32, int ldk, int npair, int naux,
                              const TcOperand& W, int ldw, size_t wc_stride, int nw, double* v, int ldv, int fp16);
 bool tc_supported(qx_ctx* ctx);
+
+// Block sweep in the FP16X3 form: split the step's panels (buffer half buf of
+// base, 2 * 4 * nw * n * 128 * 2 bytes in all), then the tcgen05 trailing
+// update on stream st (mode / next_blk as k_sweep_update; err: one zeroed
+// status word).
+struct SweepSplit {
+  TcOperand T, P;
+};
+SweepSplit launch_sweep_split(qx_ctx* ctx, cudaStream_t st, const double* Tp, const double* Pp, int n, int kb,
+                              int nw, int buf, void* base);
+void launch_sweep_update_tc(qx_ctx* ctx, cudaStream_t st, double* eps, int n, int ldn, size_t stride, int nw,
+                            int kblk, const SweepSplit& sp, int mode, int next_blk, int* err);
 
 
 }  // namespace qx
