@@ -50,7 +50,7 @@ def parse():
     p.add_argument("--no-batch64", action="store_true")
     p.add_argument("--no-grad", action="store_true")
     p.add_argument("--no-bse", action="store_true")
-    p.add_argument("--batch-workers", type=int, default=4)
+    p.add_argument("--batch-workers", type=int, default=0)
     return p.parse_args()
 
 
@@ -280,7 +280,9 @@ def bench_batch64(q, dev, precision, steps, warmup, nworkers):
     flops = batch64_flops(shapes, nw)
     del systems
     torch.cuda.empty_cache()
-    return {"workload": "g0w0_cd_batch64_nmo40-400_nw24", "systems": n, "nworkers": nworkers, "qp": "linearized",
+    return {"workload": "g0w0_cd_batch64_nmo40-400_nw24", "systems": n, "nworkers": nworkers,
+            "mode": "grouped (every inversion one grouped block sweep)" if nworkers == 0
+            else f"{nworkers} per-system worker streams", "qp": "linearized",
             "precision": precision, "steps": steps, "warmup": warmup,
             "systems_per_s": n * steps / t_mixed, "fp64_systems_per_s": n * steps / t_fp64,
             "speedup_vs_fp64_gpu": t_fp64 / t_mixed, "max_qp_err_meV_vs_fp64": err * HA_TO_MEV,

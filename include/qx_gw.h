@@ -196,11 +196,14 @@ qx_status qx_cd_sigma(qx_ctx* ctx, const double* mo_energy, const double* lpq, i
 
 /* Many independent G0W0-CD systems of uneven size in one call (no reference
  * counterpart: the reference runs compute_sigma_c_pyscf_cd once per system).
- * Each system is the argument set of qx_g0w0_cd; the library runs them on
- * nworkers worker streams of the context (<= 0: 4; at most 16), largest P0
- * cost first, each with its own workspace, so that small systems overlap the
- * large ones.  Per-system status is written to systems[i].status; the call
- * returns the first failure (by index). */
+ * Each system is the argument set of qx_g0w0_cd.  nworkers = 0: grouped
+ * mode -- the systems advance phase by phase on their own streams and every
+ * inversion (the imaginary-axis eps of all systems; the residue eps of all
+ * systems at each QP evaluation) runs as one grouped block sweep, in waves of
+ * at most 64 systems and ~48 GB of workspace.  nworkers > 0: each system runs
+ * whole on one of nworkers worker streams (at most 16), largest P0 cost
+ * first; < 0: 4 such streams.  Per-system status is written to
+ * systems[i].status; the call returns the first failure (by index). */
 typedef struct {
   const double* mo_energy; /* [nmo] */
   const double* lpq;       /* [naux][nmo][nmo] */

@@ -1,7 +1,9 @@
 // FP64 kernels of the GW chain: chi weights, eps = I + B chi B^T, block-sweep
 // inversion to Wc = eps^-1 - I, pair gathers, exchange diagonal, the Sigma_c
 // pair contraction v = B_p^T Wc B_p, and the Sigma_c(iw) assembly.
+#include <algorithm>
 #include <mutex>
+#include <vector>
 
 #include "gemm_f64.cuh"
 #include "qx_blas.cuh"
@@ -149,19 +151,20 @@ __device__ __forceinline__ void sweep32_warp(double* S, int q0, int lane, bool& 
   for (int i = 0; i < 32; ++i) S[(q0 + i) * SWEEP_NB + q0 + lane] = c[i];
 }
 
-__global__ void __launch_bounds__(512) k_sweep_diag(const double* __restrict__ M, int ldn, size_t stride, int k0,
-                                                    int kb, double* __restrict__ Dp, int* __restrict__ status) {
+// D = -(A_KK)^-1 for the kb x kb diagonal block whose first element is at
+// Akk (row stride ldn), zero outside kb x kb; *status_w = 1 when a pivot
+// vanishes.  512 threads; dynamic shared memory (128 * 128 + 128 * 33) doubles.
+__device__ __forceinline__ void sweep_diag_body(const double* __restrict__ Akk, int ldn, int kb,
+                                                double* __restrict__ D, int* __restrict__ status_w) {
   static_assert(SWEEP_NB == 128, "thread mapping assumes 128 columns");
   constexpr int TLD = 33;                       // padded row stride of T
   extern __shared__ double S[];                 // [128][128]
   double* Tb = S + SWEEP_NB * SWEEP_NB;         // [128][33]
-  const int w = blockIdx.x;
-  const double* A = M + (size_t)w * stride;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int j = tid & 127, r0 = tid >> 7;
   for (int k = 0; k < 32; ++k) {
     const int i = r0 + 4 * k;
-    S[i * SWEEP_NB + j] = (i < kb && j < kb) ? A[(size_t)(k0 + i) * ldn + k0 + j] : (i == j ? 1.0 : 0.0);
+    S[i * SWEEP_NB + j] = (i < kb && j < kb) ? Akk[(size_t)i * ldn + j] : (i == j ? 1.0 : 0.0);
   }
   bool bad_any = false;
   // Sub-blocks past kb are identity padding with no coupling to the block:
@@ -252,35 +255,38 @@ __global__ void __launch_bounds__(512) k_sweep_diag(const double* __restrict__ M
     }
   }
   __syncthreads();
-  if (lane == 0 && warp == 0 && bad_any) atomicExch(status + w, 1);
+  if (lane == 0 && warp == 0 && bad_any) atomicExch(status_w, 1);
   // D = -S, zero outside the kb x kb block.
-  double* D = Dp + (size_t)w * SWEEP_NB * SWEEP_NB;
   for (int k = 0; k < 32; ++k) {
     const int i = r0 + 4 * k;
     D[(size_t)i * SWEEP_NB + j] = (i < kb && j < kb) ? -S[i * SWEEP_NB + j] : 0.0;
   }
 }
 
+__global__ void __launch_bounds__(512) k_sweep_diag(const double* __restrict__ M, int ldn, size_t stride, int k0,
+                                                    int kb, double* __restrict__ Dp, int* __restrict__ status) {
+  const int w = blockIdx.x;
+  sweep_diag_body(M + (size_t)w * stride + (size_t)k0 * ldn + k0, ldn, kb, Dp + (size_t)w * SWEEP_NB * SWEEP_NB,
+                  status + w);
+}
+
 using PanelTile = F64Tile<64, 64, 2, 2, 3>;
 
-// T[w][r][:] = M[w][r][K] D[w]   (D symmetric: its rows serve as the B operand)
-__global__ void __launch_bounds__(PanelTile::THREADS) k_sweep_tpanel(const double* __restrict__ M, int n, int ldn,
-                                                                     size_t stride, int k0, int kb,
-                                                                     const double* __restrict__ Dp,
-                                                                     double* __restrict__ Tp, size_t pstride) {
+// Tile (m0, n0) of T[r][:] = M[r][K] D (D symmetric: its rows serve as the B
+// operand); columns past kb come out zero.
+__device__ __forceinline__ void sweep_tpanel_body(const double* __restrict__ M, int n, int ldn, int k0, int kb,
+                                                  const double* __restrict__ Dw, double* __restrict__ Tw, int m0,
+                                                  int n0) {
   using T = PanelTile;
   extern __shared__ double smem[];
-  const int w = blockIdx.z;
-  const int m0 = blockIdx.x * T::BM, n0 = blockIdx.y * T::BN;
   double acc[T::MI][T::NJ][2];
 #pragma unroll
   for (int i = 0; i < T::MI; ++i)
 #pragma unroll
     for (int j = 0; j < T::NJ; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
-  const double* A = M + (size_t)w * stride + (size_t)m0 * ldn + k0;
-  const double* D = Dp + (size_t)w * SWEEP_NB * SWEEP_NB + (size_t)n0 * SWEEP_NB;
+  const double* A = M + (size_t)m0 * ldn + k0;
+  const double* D = Dw + (size_t)n0 * SWEEP_NB;
   f64_mainloop<T>(acc, smem, A, ldn, n - m0, D, SWEEP_NB, kb - n0, nullptr, kb);
-  double* Tw = Tp + (size_t)w * pstride;
 #pragma unroll
   for (int i = 0; i < T::MI; ++i)
 #pragma unroll
@@ -292,23 +298,27 @@ __global__ void __launch_bounds__(PanelTile::THREADS) k_sweep_tpanel(const doubl
       }
 }
 
+// T[w][r][:] = M[w][r][K] D[w]
+__global__ void __launch_bounds__(PanelTile::THREADS) k_sweep_tpanel(const double* __restrict__ M, int n, int ldn,
+                                                                     size_t stride, int k0, int kb,
+                                                                     const double* __restrict__ Dp,
+                                                                     double* __restrict__ Tp, size_t pstride) {
+  const int w = blockIdx.z;
+  sweep_tpanel_body(M + (size_t)w * stride, n, ldn, k0, kb, Dp + (size_t)w * SWEEP_NB * SWEEP_NB,
+                    Tp + (size_t)w * pstride, blockIdx.x * PanelTile::BM, blockIdx.y * PanelTile::BN);
+}
+
 using SweepTile = F64Tile<64, 64, 2, 2, 3>;
 
-// mode 0: every lower tile; 1: tiles whose rows or columns meet the next
-// block [nk0, nk0 + nkb); 2: the other tiles.
-__global__ void __launch_bounds__(SweepTile::THREADS) k_sweep_update(double* __restrict__ M, int n, int ldn,
-                                                                     size_t stride, int k0, int kb,
-                                                                     const double* __restrict__ Tp,
-                                                                     const double* __restrict__ Pp,
-                                                                     size_t pstride, int mode, int nk0, int nkb) {
+// M[r][c] -= T[r] . P[c] over the 64 x 64 tile (tm, tn), lower part, mirrored;
+// rows and columns of the K block are left alone.  mode 0: any tile; 1: only
+// tiles whose rows or columns meet the next block [nk0, nk0 + nkb); 2: only
+// the other tiles.
+__device__ __forceinline__ void sweep_update_body(double* __restrict__ A, int n, int ldn, int k0, int kb,
+                                                  const double* __restrict__ Tw, const double* __restrict__ Pw,
+                                                  int tm, int tn, int mode, int nk0, int nkb) {
   using T = SweepTile;
   extern __shared__ double smem[];
-  const int t = blockIdx.x;
-  int tm = (int)floor((sqrt(8.0 * t + 1.0) - 1.0) * 0.5);
-  while ((tm + 1) * (tm + 2) / 2 <= t) ++tm;
-  while (tm * (tm + 1) / 2 > t) --tm;
-  const int tn = t - tm * (tm + 1) / 2;
-  const int w = blockIdx.y;
   const int m0 = tm * T::BM, n0 = tn * T::BN;
   // Tiles entirely inside the K block rows or columns have nothing to update.
   if ((m0 >= k0 && m0 + T::BM <= k0 + kb) || (n0 >= k0 && n0 + T::BN <= k0 + kb)) return;
@@ -316,15 +326,13 @@ __global__ void __launch_bounds__(SweepTile::THREADS) k_sweep_update(double* __r
     const bool touches = (m0 < nk0 + nkb && m0 + T::BM > nk0) || (n0 < nk0 + nkb && n0 + T::BN > nk0);
     if (touches != (mode == 1)) return;
   }
-  double* A = M + (size_t)w * stride;
-  const double* Tw = Tp + (size_t)w * pstride;
   double acc[T::MI][T::NJ][2];
 #pragma unroll
   for (int i = 0; i < T::MI; ++i)
 #pragma unroll
     for (int j = 0; j < T::NJ; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
-  f64_mainloop<T>(acc, smem, Tw + (size_t)m0 * SWEEP_NB, SWEEP_NB, n - m0, Pp + (size_t)w * pstride + (size_t)n0 * SWEEP_NB,
-                  SWEEP_NB, n - n0, nullptr, kb);
+  f64_mainloop<T>(acc, smem, Tw + (size_t)m0 * SWEEP_NB, SWEEP_NB, n - m0, Pw + (size_t)n0 * SWEEP_NB, SWEEP_NB,
+                  n - n0, nullptr, kb);
 #pragma unroll
   for (int i = 0; i < T::MI; ++i)
 #pragma unroll
@@ -340,6 +348,48 @@ __global__ void __launch_bounds__(SweepTile::THREADS) k_sweep_update(double* __r
       }
 }
 
+// Lower tile index t -> (tm, tn), tn <= tm.
+__device__ __forceinline__ void lower_tile(int t, int& tm, int& tn) {
+  tm = (int)floor((sqrt(8.0 * t + 1.0) - 1.0) * 0.5);
+  while ((tm + 1) * (tm + 2) / 2 <= t) ++tm;
+  while (tm * (tm + 1) / 2 > t) --tm;
+  tn = t - tm * (tm + 1) / 2;
+}
+
+__global__ void __launch_bounds__(SweepTile::THREADS) k_sweep_update(double* __restrict__ M, int n, int ldn,
+                                                                     size_t stride, int k0, int kb,
+                                                                     const double* __restrict__ Tp,
+                                                                     const double* __restrict__ Pp,
+                                                                     size_t pstride, int mode, int nk0, int nkb) {
+  int tm, tn;
+  lower_tile(blockIdx.x, tm, tn);
+  const int w = blockIdx.y;
+  sweep_update_body(M + (size_t)w * stride, n, ldn, k0, kb, Tp + (size_t)w * pstride, Pp + (size_t)w * pstride, tm,
+                    tn, mode, nk0, nkb);
+}
+
+// Element (r, q), q < 128, of the panel write: P[r][q] = the old M[r][k0 + q]
+// for rows outside K and q < kb, zero otherwise (a split of P then sees no
+// stale values); for q < kb, M[r][k0 + q] = M[k0 + q][r] = T[r][q] outside K
+// and -D inside.  The mirror writes of rows outside K land in rows inside K,
+// which no thread reads here.  Inside the K block both (r, q) and its mirror
+// write the same element: D's lower triangle serves both, so the stored value
+// does not depend on which write lands last.
+__device__ __forceinline__ void sweep_write_elem(double* __restrict__ A, int ldn, int k0, int kb,
+                                                 const double* __restrict__ Tw, double* __restrict__ Pw,
+                                                 const double* __restrict__ D, int r, int q) {
+  const bool in_k = (r >= k0 && r < k0 + kb);
+  if (q >= kb) {
+    Pw[(size_t)r * SWEEP_NB + q] = 0.0;
+    return;
+  }
+  Pw[(size_t)r * SWEEP_NB + q] = in_k ? 0.0 : A[(size_t)r * ldn + k0 + q];
+  const int a = r - k0;
+  const double v = in_k ? -D[max(a, q) * SWEEP_NB + min(a, q)] : Tw[(size_t)r * SWEEP_NB + q];
+  A[(size_t)r * ldn + k0 + q] = v;
+  A[(size_t)(k0 + q) * ldn + r] = v;
+}
+
 __global__ void k_sweep_write(double* __restrict__ M, int n, int ldn, size_t stride, int k0, int kb,
                               const double* __restrict__ Tp, double* __restrict__ Pp, size_t pstride,
                               const double* __restrict__ Dp) {
@@ -348,48 +398,49 @@ __global__ void k_sweep_write(double* __restrict__ M, int n, int ldn, size_t str
   const double* Tw = Tp + (size_t)w * pstride;
   double* Pw = Pp + (size_t)w * pstride;
   const double* D = Dp + (size_t)w * SWEEP_NB * SWEEP_NB;
-  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < n * kb; idx += gridDim.x * blockDim.x) {
-    const int r = idx / kb, q = idx % kb;
-    // Save the old panel for the update (rows outside K; their mirror
-    // writes below land in rows inside K, which no thread reads here).  The
-    // rows inside K are unused by the update and set to zero, so that a split
-    // of P (its scale bound) sees no stale values.
-    Pw[(size_t)r * SWEEP_NB + q] = (r < k0 || r >= k0 + kb) ? A[(size_t)r * ldn + k0 + q] : 0.0;
-    // Inside the K block both (r, q) and its mirror write the same element:
-    // take D's lower triangle for both, so the stored value does not depend on
-    // which write lands last.
-    const int a = r - k0;
-    const double v = (r >= k0 && r < k0 + kb) ? -D[max(a, q) * SWEEP_NB + min(a, q)] : Tw[(size_t)r * SWEEP_NB + q];
-    A[(size_t)r * ldn + k0 + q] = v;
-    A[(size_t)(k0 + q) * ldn + r] = v;
-  }
+  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < n * SWEEP_NB; idx += gridDim.x * blockDim.x)
+    sweep_write_elem(A, ldn, k0, kb, Tw, Pw, D, idx / SWEEP_NB, idx % SWEEP_NB);
 }
 
 // After the last sweep M = -eps^-1; Wc = eps^-1 - I = -M - I.  A frequency
 // whose eps was singular gets Wc = 0 (eps^-1 replaced by the identity).  With
 // half_lower the output is W' = strict lower triangle of Wc + diag(Wc) / 2 and
 // zeros above, so that b^T Wc b = 2 b^T W' b needs only the lower triangle.
+__device__ __forceinline__ void finish_wc_elem(double* __restrict__ A, int ldn, bool singular, int half_lower, int r,
+                                               int c) {
+  double v = singular ? 0.0 : -A[(size_t)r * ldn + c] - (r == c ? 1.0 : 0.0);
+  if (half_lower) v = (c < r) ? v : (c == r ? 0.5 * v : 0.0);
+  A[(size_t)r * ldn + c] = v;
+}
+
 __global__ void k_finish_wc(double* __restrict__ M, int n, int ldn, size_t stride, const int* __restrict__ status,
                             int half_lower) {
   const int w = blockIdx.y;
   double* A = M + (size_t)w * stride;
   const bool singular = status[w] != 0;
   for (size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x; idx < (size_t)n * n;
-       idx += (size_t)gridDim.x * blockDim.x) {
-    int r = (int)(idx / n), c = (int)(idx % n);
-    double v = singular ? 0.0 : -A[(size_t)r * ldn + c] - (r == c ? 1.0 : 0.0);
-    if (half_lower) v = (c < r) ? v : (c == r ? 0.5 * v : 0.0);
-    A[(size_t)r * ldn + c] = v;
-  }
+       idx += (size_t)gridDim.x * blockDim.x)
+    finish_wc_elem(A, ldn, singular, half_lower, (int)(idx / n), (int)(idx % n));
 }
 
 static_assert(kSweepPanelCols == SWEEP_NB, "panel width");
 
+// Grouped forms of the sweep kernels (defined below).
+__global__ void k_gsweep_diag(const GMat* __restrict__ mats, int k0, double* __restrict__ Dp,
+                              int* __restrict__ status);
+__global__ void k_gsweep_tpanel(const GMat* __restrict__ mats, const int* __restrict__ pre, int count, int k0,
+                                const double* __restrict__ Dp, double* __restrict__ Tcat);
+__global__ void k_gsweep_update(const GMat* __restrict__ mats, const int* __restrict__ pre, int count, int k0,
+                                const double* __restrict__ Tcat, const double* __restrict__ Pcat);
+
 void sweep_set_attributes() {
-  QX_CUDA(cudaFuncSetAttribute(k_sweep_diag, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)((SWEEP_NB * SWEEP_NB + SWEEP_NB * 33) * sizeof(double))));
+  const int diag_smem = (int)((SWEEP_NB * SWEEP_NB + SWEEP_NB * 33) * sizeof(double));
+  QX_CUDA(cudaFuncSetAttribute(k_sweep_diag, cudaFuncAttributeMaxDynamicSharedMemorySize, diag_smem));
   QX_CUDA(cudaFuncSetAttribute(k_sweep_tpanel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PanelTile::SMEM));
   QX_CUDA(cudaFuncSetAttribute(k_sweep_update, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SweepTile::SMEM));
+  QX_CUDA(cudaFuncSetAttribute(k_gsweep_diag, cudaFuncAttributeMaxDynamicSharedMemorySize, diag_smem));
+  QX_CUDA(cudaFuncSetAttribute(k_gsweep_tpanel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PanelTile::SMEM));
+  QX_CUDA(cudaFuncSetAttribute(k_gsweep_update, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SweepTile::SMEM));
 }
 
 static void sweep_attributes_once() {
@@ -406,7 +457,7 @@ static void sweep_front(qx_ctx* ctx, cudaStream_t st, double* eps, int n, int ld
   dim3 tg(ceil_div(n, PanelTile::BM), ceil_div(kb, PanelTile::BN), nw);
   k_sweep_tpanel<<<tg, PanelTile::THREADS, PanelTile::SMEM, st>>>(eps, n, ldn, stride, k0, kb, Dp, Tp, pstride);
   check_launch(ctx);
-  dim3 wg(ceil_div(n * kb, 256), nw);
+  dim3 wg(ceil_div(n * SWEEP_NB, 256), nw);
   k_sweep_write<<<wg, 256, 0, st>>>(eps, n, ldn, stride, k0, kb, Tp, Pp, pstride, Dp);
   check_launch(ctx);
 }
@@ -520,6 +571,199 @@ void launch_invert_wc_panels(qx_ctx* ctx, double* eps, int n, int ldn, size_t st
   dim3 fg(ceil_div(n * n, 256 * 4), nw);
   k_finish_wc<<<fg, 256, 0, ctx->stream>>>(eps, n, ldn, stride, status, 0);
   check_launch(ctx);
+}
+
+// ---------------------------------------------------------------------------
+// Grouped block sweep: the kernels above over a table of matrices of
+// different orders.  A CTA finds its matrix by binary search in a prefix
+// table of per-matrix CTA counts (matrices sorted by order, largest first, so
+// those still active at a step are a prefix).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int group_of(const int* __restrict__ pre, int count, int b) {
+  int lo = 0, hi = count - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (__ldg(pre + mid) <= b)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  return lo;
+}
+
+__global__ void __launch_bounds__(512) k_gsweep_diag(const GMat* __restrict__ mats, int k0, double* __restrict__ Dp,
+                                                     int* __restrict__ status) {
+  const int g = blockIdx.x;
+  const GMat m = mats[g];
+  sweep_diag_body(m.M + (size_t)k0 * m.ldn + k0, m.ldn, min(SWEEP_NB, m.n - k0), Dp + (size_t)g * SWEEP_NB * SWEEP_NB,
+                  status + g);
+}
+
+// Two 64-column tiles per 64 rows: all 128 panel columns are written (zero past kb).
+__global__ void __launch_bounds__(PanelTile::THREADS) k_gsweep_tpanel(const GMat* __restrict__ mats,
+                                                                      const int* __restrict__ pre, int count, int k0,
+                                                                      const double* __restrict__ Dp,
+                                                                      double* __restrict__ Tcat) {
+  const int g = group_of(pre, count, blockIdx.x);
+  const int t = blockIdx.x - pre[g];
+  const GMat m = mats[g];
+  sweep_tpanel_body(m.M, m.n, m.ldn, k0, min(SWEEP_NB, m.n - k0), Dp + (size_t)g * SWEEP_NB * SWEEP_NB,
+                    Tcat + (size_t)m.prow * SWEEP_NB, (t >> 1) * PanelTile::BM, (t & 1) * PanelTile::BN);
+}
+
+__global__ void k_gsweep_write(const GMat* __restrict__ mats, const int* __restrict__ pre, int count, int k0,
+                               const double* __restrict__ Tcat, double* __restrict__ Pcat,
+                               const double* __restrict__ Dp) {
+  const int g = group_of(pre, count, blockIdx.x);
+  const GMat m = mats[g];
+  const int idx = (blockIdx.x - pre[g]) * blockDim.x + threadIdx.x;
+  if (idx >= m.n * SWEEP_NB) return;
+  sweep_write_elem(m.M, m.ldn, k0, min(SWEEP_NB, m.n - k0), Tcat + (size_t)m.prow * SWEEP_NB,
+                   Pcat + (size_t)m.prow * SWEEP_NB, Dp + (size_t)g * SWEEP_NB * SWEEP_NB, idx / SWEEP_NB,
+                   idx % SWEEP_NB);
+}
+
+__global__ void __launch_bounds__(SweepTile::THREADS) k_gsweep_update(const GMat* __restrict__ mats,
+                                                                      const int* __restrict__ pre, int count, int k0,
+                                                                      const double* __restrict__ Tcat,
+                                                                      const double* __restrict__ Pcat) {
+  const int g = group_of(pre, count, blockIdx.x);
+  const GMat m = mats[g];
+  int tm, tn;
+  lower_tile(blockIdx.x - pre[g], tm, tn);
+  sweep_update_body(m.M, m.n, m.ldn, k0, min(SWEEP_NB, m.n - k0), Tcat + (size_t)m.prow * SWEEP_NB,
+                    Pcat + (size_t)m.prow * SWEEP_NB, tm, tn, 0, 0, 0);
+}
+
+__global__ void k_gfinish_wc(const GMat* __restrict__ mats, const int* __restrict__ pre, int count,
+                             const int* __restrict__ status, int half_lower) {
+  const int g = group_of(pre, count, blockIdx.x);
+  const GMat m = mats[g];
+  const int idx = (blockIdx.x - pre[g]) * blockDim.x + threadIdx.x;
+  if (idx >= m.n * m.n) return;
+  finish_wc_elem(m.M, m.ldn, status[g] != 0, half_lower, idx / m.n, idx % m.n);
+}
+
+// Zero the padding rows [n, n rounded up to 128) of each matrix's panels
+// (read by the tcgen05 tiles and the splits, written by no sweep kernel).
+__global__ void k_gzero_pad(const GMat* __restrict__ mats, double* __restrict__ Tcat, double* __restrict__ Pcat) {
+  const GMat m = mats[blockIdx.x];
+  const int rows = (m.n + SWEEP_NB - 1) / SWEEP_NB * SWEEP_NB - m.n;
+  for (int idx = threadIdx.x; idx < rows * SWEEP_NB; idx += blockDim.x) {
+    const size_t at = (size_t)(m.prow + m.n) * SWEEP_NB + idx;
+    Tcat[at] = 0.0;
+    Pcat[at] = 0.0;
+  }
+}
+
+void launch_invert_wc_group(qx_ctx* ctx, const GMat* mats_in, int G, int half_lower, int split_update) {
+  QX_REQUIRE(mats_in && G > 0, QX_ERR_INVALID_INPUT, "empty matrix group");
+  std::vector<int> ord(G);
+  for (int i = 0; i < G; ++i) ord[i] = i;
+  std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) { return mats_in[a].n > mats_in[b].n; });
+  std::vector<GMat> m(G);
+  int prow = 0;
+  for (int i = 0; i < G; ++i) {
+    m[i] = mats_in[ord[i]];
+    QX_REQUIRE(m[i].M && m[i].n > 0 && m[i].n <= 32768 && m[i].ldn >= m[i].n, QX_ERR_INVALID_INPUT,
+               "grouped sweep: matrix %d has n=%d ldn=%d", ord[i], m[i].n, m[i].ldn);
+    m[i].prow = prow;
+    QX_REQUIRE((size_t)prow + round_up(m[i].n, SWEEP_NB) < (1u << 30), QX_ERR_INVALID_INPUT,
+               "grouped sweep: too many panel rows");
+    prow += round_up(m[i].n, SWEEP_NB);
+  }
+  const int R = prow;
+  const int nsteps = ceil_div(m[0].n, SWEEP_NB);
+  const bool tc = split_update != 0;
+  // Prefix tables: per step the tpanel, write and update CTA counts of the
+  // active matrices, then the finish counts of all.
+  std::vector<int> tab;
+  auto add_table = [&](int count, auto tiles) {
+    const size_t off = tab.size();
+    long long acc = 0;
+    for (int g = 0; g < count; ++g) {
+      tab.push_back((int)acc);
+      acc += tiles(m[g]);
+    }
+    QX_REQUIRE(acc < (1ll << 31), QX_ERR_INVALID_INPUT, "grouped sweep: too many CTAs");
+    tab.push_back((int)acc);
+    return off;
+  };
+  std::vector<int> act(nsteps), rows_act(nsteps);
+  std::vector<size_t> off_tp(nsteps), off_wr(nsteps), off_up(nsteps);
+  for (int s = 0; s < nsteps; ++s) {
+    const int k0 = s * SWEEP_NB;
+    int a = 0;
+    while (a < G && m[a].n > k0) ++a;
+    act[s] = a;
+    rows_act[s] = m[a - 1].prow + round_up(m[a - 1].n, SWEEP_NB);
+    off_tp[s] = add_table(a, [](const GMat& x) { return (long long)ceil_div(x.n, PanelTile::BM) * 2; });
+    off_wr[s] = add_table(a, [](const GMat& x) { return (long long)ceil_div(x.n * SWEEP_NB, 256); });
+    if (tc)
+      off_up[s] = add_table(a, [](const GMat& x) {
+        const long long t = ceil_div(x.n, SWEEP_NB);
+        return t * (t + 1) / 2;
+      });
+    else
+      off_up[s] = add_table(a, [](const GMat& x) {
+        const long long t = ceil_div(x.n, SweepTile::BM);
+        return t * (t + 1) / 2;
+      });
+  }
+  const size_t off_fin = add_table(G, [](const GMat& x) { return ((long long)x.n * x.n + 255) / 256; });
+  // Workspace: T, P [R][128] FP64, D [G][128][128], the matrix and prefix tables.
+  const size_t pan = (size_t)R * SWEEP_NB;
+  const size_t dsz = (size_t)G * SWEEP_NB * SWEEP_NB;
+  DevBuf& wb = ctx->ws[WS_PANEL];
+  wb.reserve((2 * pan + dsz) * sizeof(double) + G * sizeof(GMat) + tab.size() * sizeof(int) + 512);
+  double* Tcat = wb.as<double>();
+  double* Pcat = Tcat + pan;
+  double* Dp = Pcat + pan;
+  GMat* d_mats = reinterpret_cast<GMat*>(Dp + dsz);
+  int* d_tab = reinterpret_cast<int*>(d_mats + G);
+  QX_CUDA(cudaMemcpyAsync(d_mats, m.data(), G * sizeof(GMat), cudaMemcpyHostToDevice, ctx->stream));
+  QX_CUDA(cudaMemcpyAsync(d_tab, tab.data(), tab.size() * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+  int* status = status_words(ctx, G);
+  QX_CUDA(cudaMemsetAsync(status, 0, G * sizeof(int), ctx->stream));
+  int* tc_err = nullptr;
+  void* split_base = nullptr;
+  if (tc) {
+    tc_err = status_words(ctx, nsteps);
+    QX_CUDA(cudaMemsetAsync(tc_err, 0, nsteps * sizeof(int), ctx->stream));
+    DevBuf& sb = ctx->ws[WS_SWEEP_SPLIT];
+    sb.reserve(pan * 2 * 4 + 256);
+    split_base = sb.ptr;
+  }
+  sweep_attributes_once();
+  k_gzero_pad<<<G, 256, 0, ctx->stream>>>(d_mats, Tcat, Pcat);
+  check_launch(ctx);
+  const int diag_smem = (SWEEP_NB * SWEEP_NB + SWEEP_NB * 33) * sizeof(double);
+  for (int s = 0; s < nsteps; ++s) {
+    const int k0 = s * SWEEP_NB, a = act[s];
+    k_gsweep_diag<<<a, 512, diag_smem, ctx->stream>>>(d_mats, k0, Dp, status);
+    check_launch(ctx);
+    k_gsweep_tpanel<<<tab[off_tp[s] + a], PanelTile::THREADS, PanelTile::SMEM, ctx->stream>>>(
+        d_mats, d_tab + off_tp[s], a, k0, Dp, Tcat);
+    check_launch(ctx);
+    k_gsweep_write<<<tab[off_wr[s] + a], 256, 0, ctx->stream>>>(d_mats, d_tab + off_wr[s], a, k0, Tcat, Pcat, Dp);
+    check_launch(ctx);
+    if (tc) {
+      uint8_t* b = static_cast<uint8_t*>(split_base);
+      TcOperand T{b, b + pan * 2, nullptr}, P{b + pan * 4, b + pan * 6, nullptr};
+      const int rows = rows_act[s];
+      launch_split(ctx, Tcat, rows, SWEEP_NB, SWEEP_NB, T.hi, T.lo, SWEEP_NB, 0, 0, 1, 1, 3, &T.scale);
+      launch_split(ctx, Pcat, rows, SWEEP_NB, SWEEP_NB, P.hi, P.lo, SWEEP_NB, 0, 0, 1, 1, 4, &P.scale);
+      launch_gsweep_update_tc(ctx, d_mats, d_tab + off_up[s], a, tab[off_up[s] + a], s, T, P, rows, tc_err + s);
+    } else {
+      k_gsweep_update<<<tab[off_up[s] + a], SweepTile::THREADS, SweepTile::SMEM, ctx->stream>>>(
+          d_mats, d_tab + off_up[s], a, k0, Tcat, Pcat);
+      check_launch(ctx);
+    }
+  }
+  k_gfinish_wc<<<tab[off_fin + G], 256, 0, ctx->stream>>>(d_mats, d_tab + off_fin, G, status, half_lower);
+  check_launch(ctx);
+  ctx->pending.push_back({status, G, 1});
+  if (tc) ctx->pending.push_back({tc_err, nsteps, 0});
 }
 
 // ---------------------------------------------------------------------------

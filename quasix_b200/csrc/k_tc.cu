@@ -218,6 +218,12 @@ struct TcArgs {
   int skip_tile;
   int filter_mode;
   int filter_tile;
+  // Grouped trailing update (with subtract): a CTA's matrix is found in the
+  // prefix table gpre over gcount matrices gmats; A and B rows are offset by
+  // the matrix's panel row, out / M / N / ldo come from the matrix.
+  const GMat* gmats;
+  const int* gpre;
+  int gcount;
 };
 
 // x[q] = xr[q] for the columns col0 + q < N of a valid row, 0 otherwise
@@ -263,6 +269,7 @@ __global__ void __launch_bounds__(TcWarps<EPI>::THREADS, 1)
 
   // CTA -> (m block, batch, n tile range).
   int mb, w, nt_begin, nt_end;
+  GMat gmat{};
   const int n_tiles = (args.N + BN - 1) / BN;
   if (EPI == EPI_ROWDOT) {
     const int g = args.wgroup;
@@ -275,7 +282,23 @@ __global__ void __launch_bounds__(TcWarps<EPI>::THREADS, 1)
     nt_end = n_tiles;
   } else {
     w = blockIdx.y;
-    if (args.lower_tiles) {
+    if (args.gmats) {
+      int lo = 0, hi = args.gcount - 1;
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(args.gpre + mid) <= (int)blockIdx.x)
+          lo = mid;
+        else
+          hi = mid - 1;
+      }
+      gmat = args.gmats[lo];
+      const int t = blockIdx.x - args.gpre[lo];
+      int tm = (int)floor((sqrt(8.0 * t + 1.0) - 1.0) * 0.5);
+      while ((tm + 1) * (tm + 2) / 2 <= t) ++tm;
+      while (tm * (tm + 1) / 2 > t) --tm;
+      mb = tm;
+      nt_begin = t - tm * (tm + 1) / 2;
+    } else if (args.lower_tiles) {
       const int t = blockIdx.x;
       int tm = (int)floor((sqrt(8.0 * t + 1.0) - 1.0) * 0.5);
       while ((tm + 1) * (tm + 2) / 2 <= t) ++tm;
@@ -298,6 +321,13 @@ __global__ void __launch_bounds__(TcWarps<EPI>::THREADS, 1)
   }
   const bool active = (w < args.nbatch);
   const int m0 = mb * TC_BM;
+  // STORE output shape and the panel row offsets of a grouped matrix.
+  const bool grouped = (EPI == EPI_STORE) && args.gmats != nullptr;
+  const int outM = grouped ? gmat.n : args.M, outN = grouped ? gmat.n : args.N;
+  const int out_ld = grouped ? gmat.ldn : args.ldo;
+  const size_t out_stride = grouped ? 0 : args.out_stride;
+  double* const out_base = grouped ? gmat.M : args.out;
+  const int row_off = grouped ? gmat.prow : 0;
   const int k_blocks = (args.K + TC_BK - 1) / TC_BK;
 
   if (threadIdx.x == 0) {
@@ -344,11 +374,11 @@ __global__ void __launch_bounds__(TcWarps<EPI>::THREADS, 1)
               tma_load_3d(st, &mapAh, &full[s], k0, m0, w);
               tma_load_3d(st + L::A_BYTES, &mapAl, &full[s], k0, m0, w);
             } else {
-              tma_load_2d(st, &mapAh, &full[s], k0, m0);
-              tma_load_2d(st + L::A_BYTES, &mapAl, &full[s], k0, m0);
+              tma_load_2d(st, &mapAh, &full[s], k0, row_off + m0);
+              tma_load_2d(st + L::A_BYTES, &mapAl, &full[s], k0, row_off + m0);
             }
-            tma_load_3d(st + 2 * L::A_BYTES, &mapBh, &full[s], k0, n0, w);
-            tma_load_3d(st + 2 * L::A_BYTES + L::B_BYTES, &mapBl, &full[s], k0, n0, w);
+            tma_load_3d(st + 2 * L::A_BYTES, &mapBh, &full[s], k0, row_off + n0, w);
+            tma_load_3d(st + 2 * L::A_BYTES + L::B_BYTES, &mapBl, &full[s], k0, row_off + n0, w);
             issued = g + 1;
           }
         }
@@ -493,19 +523,19 @@ __global__ void __launch_bounds__(TcWarps<EPI>::THREADS, 1)
         __syncwarp();
         if (lane == 0) mbar_arrive(&acc_empty[buf]);
       }
-      if (ok && m < args.M) {
+      if (ok && m < outM) {
         const int n0 = nt_begin * BN + 64 * half;
-        double* orow = args.out + (size_t)w * args.out_stride + (size_t)m * args.ldo;
+        double* orow = out_base + (size_t)w * out_stride + (size_t)m * out_ld;
 #pragma unroll
         for (int c = 0; c < 64; ++c) {
           const int n = n0 + c;
           // Lower-triangular mode writes the lower triangle and mirrors it,
           // so the stored matrix is exactly symmetric.
-          if (n < args.N && !(args.lower_tiles && n > m)) {
+          if (n < outN && !(args.lower_tiles && n > m)) {
             const double val = args.subtract ? orow[n] - acc[c] * unscale
                                              : acc[c] * unscale + ((args.add_identity && m == n) ? 1.0 : 0.0);
             orow[n] = val;
-            if (args.lower_tiles && n != m) args.out[(size_t)w * args.out_stride + (size_t)n * args.ldo + m] = val;
+            if (args.lower_tiles && n != m) out_base[(size_t)w * out_stride + (size_t)n * out_ld + m] = val;
           }
         }
       }
@@ -558,10 +588,11 @@ static CUtensorMap make_map(const void* base, int cols, int rows, int ld, int ba
   return m;
 }
 
+// (cudaDeviceGetAttribute: a full property query costs milliseconds per call.)
 bool tc_supported(qx_ctx* ctx) {
-  cudaDeviceProp p;
-  if (cudaGetDeviceProperties(&p, ctx->device) != cudaSuccess) return false;
-  return p.major == 10;
+  int major = 0;
+  if (cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, ctx->device) != cudaSuccess) return false;
+  return major == 10;
 }
 
 // max|x| per batch (x >= 0 compares as its bit pattern).  Index type I: 32-bit
@@ -1104,6 +1135,31 @@ void launch_sweep_update_tc(qx_ctx* ctx, cudaStream_t st, double* eps, int n, in
   const int tiles = ceil_div(n, TC_BM);
   QX_REQUIRE(nw <= 65535, QX_ERR_INVALID_INPUT, "at most 65535 matrices per sweep");
   launch_tc<BN, EPI_STORE>(ctx, ah, al, bh, bl, a, dim3(tiles * (tiles + 1) / 2, nw), st);
+}
+
+void launch_gsweep_update_tc(qx_ctx* ctx, const GMat* d_mats, const int* d_pre, int count, int ntiles, int step,
+                             const TcOperand& T, const TcOperand& P, int rows, int* err) {
+  constexpr int BN = 128;
+  constexpr int BK = TcPipe<EPI_STORE>::BK;
+  const int K = kSweepPanelCols;
+  CUtensorMap ah = make_map(T.hi, K, rows, K, 1, TC_BM, 2, 1, BK);
+  CUtensorMap al = make_map(T.lo, K, rows, K, 1, TC_BM, 2, 1, BK);
+  CUtensorMap bh = make_map(P.hi, K, rows, K, 1, BN, 3, 1, BK);
+  CUtensorMap bl = make_map(P.lo, K, rows, K, 1, BN, 3, 1, BK);
+  TcArgs a{};
+  a.K = K;
+  a.nbatch = 1;
+  a.lower_tiles = 1;
+  a.subtract = 1;
+  a.fp16 = 1;
+  a.scaleA = T.scale;
+  a.scaleB = P.scale;
+  a.err = err;
+  a.skip_tile = step;
+  a.gmats = d_mats;
+  a.gpre = d_pre;
+  a.gcount = count;
+  launch_tc<BN, EPI_STORE>(ctx, ah, al, bh, bl, a, dim3(ntiles, 1));
 }
 
 }  // namespace qx

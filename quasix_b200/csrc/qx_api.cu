@@ -249,8 +249,8 @@ void accumulate_stage_times(qx_ctx* ctx) {
   }
 }
 
-// Wc_nm(iw) for every pair of the system: v[w][pair] (energies e on the host).
-void gw_wc_pairs(qx_ctx* ctx, GWSystem& S, const double* e_host) {
+// eps(iw) = I - Pi(iw) for the grid of the system (energies e on the host).
+void gw_wc_p0(qx_ctx* ctx, GWSystem& S, const double* e_host) {
   QX_CUDA(cudaMemcpyAsync(S.d_en, e_host, S.nmo * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
   record_stage(ctx, QX_ST_P0, true);
   launch_chi(ctx, S.d_en, S.nocc, S.nvir, S.d_freqs, S.nw, 0, S.chi, S.ldov);
@@ -260,12 +260,10 @@ void gw_wc_pairs(qx_ctx* ctx, GWSystem& S, const double* e_host) {
   else
     launch_eps_fp64(ctx, S.bov, S.ldov, S.naux, S.nov, S.chi, S.nw, S.eps, S.ldn, S.eps_stride);
   record_stage(ctx, QX_ST_P0, false);
-  record_stage(ctx, QX_ST_INV, true);
-  // Imaginary axis: eps is SPD with eigenvalues in [1, 1 + ||Pi||], so the
-  // split trailing update of the sweep keeps Wc within the split forms' error.
-  launch_invert_wc(ctx, S.eps, S.naux, S.ldn, S.eps_stride, S.nw, /*half_lower=*/1,
-                   /*split_update=*/is_tc_precision(S.precision));
-  record_stage(ctx, QX_ST_INV, false);
+}
+
+// v[w][pair] = Wc_nm(iw) of every pair, from S.eps holding W' (half-lower Wc).
+void gw_wc_contract(qx_ctx* ctx, GWSystem& S) {
   record_stage(ctx, QX_ST_CONTRACT, true);
   if (is_tc_precision(S.precision)) {
     const int fp16 = S.precision == QX_PREC_FP16X3;
@@ -277,6 +275,18 @@ void gw_wc_pairs(qx_ctx* ctx, GWSystem& S, const double* e_host) {
     launch_pair_contract_fp64(ctx, S.bpt, S.ldk, S.npair, S.naux, S.eps, S.ldn, S.eps_stride, S.nw, S.v, S.npair);
   }
   record_stage(ctx, QX_ST_CONTRACT, false);
+}
+
+// Wc_nm(iw) for every pair of the system: v[w][pair] (energies e on the host).
+void gw_wc_pairs(qx_ctx* ctx, GWSystem& S, const double* e_host) {
+  gw_wc_p0(ctx, S, e_host);
+  record_stage(ctx, QX_ST_INV, true);
+  // Imaginary axis: eps is SPD with eigenvalues in [1, 1 + ||Pi||], so the
+  // split trailing update of the sweep keeps Wc within the split forms' error.
+  launch_invert_wc(ctx, S.eps, S.naux, S.ldn, S.eps_stride, S.nw, /*half_lower=*/1,
+                   /*split_update=*/is_tc_precision(S.precision));
+  record_stage(ctx, QX_ST_INV, false);
+  gw_wc_contract(ctx, S);
 }
 
 // One imaginary-axis Sigma_c evaluation with energies e (host array [nmo]).

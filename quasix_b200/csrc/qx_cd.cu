@@ -130,6 +130,15 @@ void launch_cd_gather(qx_ctx* ctx, const double* lpq, int naux, int nmo, const i
 
 void CdEngine::setup(const double* mo_energy, const double* lpq, const int* targets, int ntarget_, int nmo_,
                      int nocc_, int naux_, int nw_, double x0, int precision_) {
+  setup_begin(mo_energy, lpq, targets, ntarget_, nmo_, nocc_, naux_, nw_, x0, precision_);
+  record_stage(ctx, QX_ST_INV, true);
+  launch_invert_wc(ctx, S.eps, S.naux, S.ldn, S.eps_stride, S.nw, /*half_lower=*/1, /*split_update=*/tc);
+  record_stage(ctx, QX_ST_INV, false);
+  setup_end();
+}
+
+void CdEngine::setup_begin(const double* mo_energy, const double* lpq, const int* targets, int ntarget_, int nmo_,
+                           int nocc_, int naux_, int nw_, double x0, int precision_) {
   nmo = nmo_;
   nocc = nocc_;
   naux = naux_;
@@ -149,16 +158,33 @@ void CdEngine::setup(const double* mo_energy, const double* lpq, const int* targ
   d_lpq = (const double*)device_view(ctx, WS_LPQ, lpq, (size_t)naux * nmo * nmo * sizeof(double));
   // Imaginary axis: Wc_nm(i f_k) for the target pairs (no cutoff: the sigma grid is unused).
   gw_setup(ctx, S, d_lpq, nmo, nocc, naux, tg, nw, 1e300, x0, precision);
-  gw_wc_pairs(ctx, S, e.data());
+  gw_wc_p0(ctx, S, e.data());
   ldn = S.ldn;
+  // Pinned staging: diag(Sigma_x), the imaginary-axis values and the residue
+  // values (at most ntarget * nmo residues).
+  ctx->host_stage.reserve((size_t)(nmo + 2 * ntarget + 2 * (size_t)ntarget * nmo + 8) * sizeof(double));
+  h_sx = ctx->host_stage.as<double>();
+  h_hi = h_sx + nmo;
+  h_rv = h_hi + 2 * ntarget;
+  h_rd = h_rv + (size_t)ntarget * nmo;
+}
+
+void CdEngine::eps_matrices(std::vector<GMat>& out) const {
+  for (int w = 0; w < nw; ++w) out.push_back(GMat{S.eps + (size_t)w * S.eps_stride, naux, S.ldn, 0, 0});
+}
+
+void CdEngine::setup_end() {
+  gw_wc_contract(ctx, S);
   DevBuf& cb = ctx->ws[WS_CD0];
   cb.reserve((size_t)(nmo + 4 * ntarget + 64) * sizeof(double));
   double* d_sx = cb.as<double>();
   d_om = d_sx + nmo;
   d_imag = d_om + ntarget;
   launch_exchange_diag(ctx, d_lpq, naux, nmo, nocc, d_sx);
+  // Read into sx at the next evaluation's synchronisation.
   sx.assign(nmo, 0.0);
-  QX_CUDA(cudaMemcpyAsync(sx.data(), d_sx, nmo * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  QX_CUDA(cudaMemcpyAsync(h_sx, d_sx, nmo * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  sx_pending = true;
   // B_ov^T [nov][ldn] for the residue derivatives.
   DevBuf& bt = ctx->ws[WS_CD1];
   bt.reserve((size_t)nov * ldn * sizeof(double));
@@ -208,6 +234,14 @@ CdResidueChunk CdEngine::residue_buffers(int R) {
 }
 
 void CdEngine::residue_compute(CdResidueChunk& c, const CdResidue* list, int rc) {
+  residue_p0(c, list, rc);
+  // Real axis: eps(w_r) is indefinite and can be ill-conditioned near an
+  // excitation, so the sweep stays FP64 here.
+  launch_invert_wc(ctx, c.eps, naux, ldn, (size_t)naux * ldn, rc);
+  residue_post(c, rc);
+}
+
+void CdEngine::residue_p0(CdResidueChunk& c, const CdResidue* list, int rc) {
   const size_t stride = (size_t)naux * ldn;
   std::vector<double> wr(rc);
   std::vector<int2> nm(rc);
@@ -223,9 +257,10 @@ void CdEngine::residue_compute(CdResidueChunk& c, const CdResidue* list, int rc)
     launch_eps_tc(ctx, S.bov, S.ldov, naux, nov, c.chi, rc, c.eps, ldn, stride, precision == QX_PREC_FP16X3);
   else
     launch_eps_fp64(ctx, S.bov, S.ldov, naux, nov, c.chi, rc, c.eps, ldn, stride);
-  // Real axis: eps(w_r) is indefinite and can be ill-conditioned near an
-  // excitation, so the sweep stays FP64 here.
-  launch_invert_wc(ctx, c.eps, naux, ldn, stride, rc);
+}
+
+void CdEngine::residue_post(CdResidueChunk& c, int rc) {
+  const size_t stride = (size_t)naux * ldn;
   launch_cd_gather(ctx, d_lpq, naux, nmo, c.nm, rc, c.b, ldn);
   k_cd_solve_rows<<<dim3(ceil_div(naux, 8), rc), 256, 0, ctx->stream>>>(c.eps, ldn, stride, c.b, naux, ldn, c.x);
   check_launch(ctx);
@@ -250,33 +285,70 @@ void CdEngine::residue_compute(CdResidueChunk& c, const CdResidue* list, int rc)
 }
 
 void CdEngine::evaluate(const std::vector<int>& act) {
+  evaluate_begin(act, nullptr);
+  evaluate_end();
+}
+
+void CdEngine::evaluate_begin(const std::vector<int>& act, std::vector<GMat>* group) {
+  ev_act = act;
   // Imaginary-axis part for every target.
   QX_CUDA(cudaMemcpyAsync(d_om, om.data(), ntarget * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
   k_cd_imag<<<ntarget, 256, 0, ctx->stream>>>(S.v, S.npair, nw, S.d_pidx, nmo, S.d_en, S.d_freqs, S.d_wts, d_om,
                                                d_imag);
   check_launch(ctx);
-  std::vector<double> hi(2 * ntarget);
-  QX_CUDA(cudaMemcpyAsync(hi.data(), d_imag, 2 * ntarget * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-  const std::vector<CdResidue> res = residues(act);
-  const int R = (int)res.size();
-  std::vector<double> rv(R), rd(R);
-  if (R > 0) {
-    CdResidueChunk c = residue_buffers(R);
-    for (int c0 = 0; c0 < R; c0 += c.cap) {
-      const int rc = std::min(c.cap, R - c0);
-      residue_compute(c, res.data() + c0, rc);
-      QX_CUDA(cudaMemcpyAsync(rv.data() + c0, c.val, rc * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-      QX_CUDA(cudaMemcpyAsync(rd.data() + c0, c.dv, rc * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-    }
+  QX_CUDA(cudaMemcpyAsync(h_hi, d_imag, 2 * ntarget * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  ev_res = residues(act);
+  const int R = (int)ev_res.size();
+  ev_grouped = false;
+  if (R == 0) return;
+  ev_chunk = residue_buffers(R);
+  CdResidueChunk& c = ev_chunk;
+  if (group && R <= c.cap) {
+    // One chunk: its eps(w_r) join the caller's grouped inversion.
+    residue_p0(c, ev_res.data(), R);
+    for (int r = 0; r < R; ++r) group->push_back(GMat{c.eps + (size_t)r * naux * ldn, naux, ldn, 0, 0});
+    ev_grouped = true;
+    return;
   }
+  for (int c0 = 0; c0 < R; c0 += c.cap) {
+    const int rc = std::min(c.cap, R - c0);
+    residue_compute(c, ev_res.data() + c0, rc);
+    QX_CUDA(cudaMemcpyAsync(h_rv + c0, c.val, rc * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    QX_CUDA(cudaMemcpyAsync(h_rd + c0, c.dv, rc * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  }
+}
+
+void CdEngine::evaluate_end() {
+  evaluate_post();
+  evaluate_finish();
+}
+
+void CdEngine::evaluate_post() {
+  const int R = (int)ev_res.size();
+  if (ev_grouped) {
+    residue_post(ev_chunk, R);
+    QX_CUDA(cudaMemcpyAsync(h_rv, ev_chunk.val, R * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    QX_CUDA(cudaMemcpyAsync(h_rd, ev_chunk.dv, R * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  }
+}
+
+void CdEngine::evaluate_finish() {
+  const int R = (int)ev_res.size();
   sync_and_check(ctx);
-  for (int t : act) {
-    sig[t] = hi[2 * t];
-    dsig[t] = hi[2 * t + 1];
+  if (sx_pending) {
+    sx.assign(h_sx, h_sx + nmo);
+    sx_pending = false;
+  }
+  ev_hi.assign(h_hi, h_hi + 2 * ntarget);
+  ev_rv.assign(h_rv, h_rv + R);
+  ev_rd.assign(h_rd, h_rd + R);
+  for (int t : ev_act) {
+    sig[t] = ev_hi[2 * t];
+    dsig[t] = ev_hi[2 * t + 1];
   }
   for (int r = 0; r < R; ++r) {
-    sig[res[r].t] += res[r].sgn * rv[r];
-    dsig[res[r].t] += rd[r];
+    sig[ev_res[r].t] += ev_res[r].sgn * ev_rv[r];
+    dsig[ev_res[r].t] += ev_rd[r];
   }
 }
 
@@ -293,53 +365,63 @@ struct CdProblem {
   double *qp, *z, *sc, *sx;
 };
 
-// Runs one system on ctx (throws qx::Error): imaginary-axis Wc for the target
-// pairs once, then QP steps; each evaluation adds the residues of the poles
-// between the target energy and the Fermi level.
-void g0w0_cd_run(qx_ctx* ctx, const CdProblem& p) {
-  QX_REQUIRE(p.qp && p.max_iter > 0, QX_ERR_INVALID_INPUT, "invalid arguments to g0w0_cd");
-  QX_REQUIRE(p.qp_solver == QX_QP_NEWTON || p.qp_solver == QX_QP_LINEARIZED, QX_ERR_INVALID_INPUT,
-             "qp_solver %d", p.qp_solver);
+// QP root search of one system as a sequence of evaluations: first() gives
+// the targets to evaluate first, advance() consumes that evaluation (E.sig,
+// E.dsig at E.om) and gives the next list (empty: done), finish() writes the
+// outputs.  The single-system driver and the grouped batch step through it.
+struct CdRun {
   CdEngine E;
-  E.ctx = ctx;
-  E.setup(p.mo_energy, p.lpq, p.targets, p.ntarget, p.nmo, p.nocc, p.naux, p.nw, p.x0, p.precision);
-  const int ntarget = p.ntarget;
-  std::vector<double> vx(p.nmo, 0.0);
-  if (p.vxc) QX_CUDA(cudaMemcpy(vx.data(), p.vxc, p.nmo * sizeof(double), cudaMemcpyDefault));
-  const std::vector<double>& e = E.e;
-  const std::vector<double>& sx = E.sx;
-  const std::vector<int>& tg = E.tg;
-  std::vector<double>& om = E.om;
-  const std::vector<double>& sig = E.sig;
-  const std::vector<double>& dsig = E.dsig;
-  constexpr double z_min = 0.1, z_max = 0.999;  // newton_solver.rs:93-95
-  std::vector<double> zf(ntarget), sxo(ntarget);
-  std::vector<int> all;
-  for (int t = 0; t < ntarget; ++t) all.push_back(t);
-  if (p.qp_solver == QX_QP_LINEARIZED) {
-    // E = e_n + Z (Sx + Sigma(e_n) - Vxc), Z clipped (qp/evgw.rs:784-821).
-    E.evaluate(all);
-    for (int t = 0; t < ntarget; ++t) {
-      const int n = tg[t];
-      zf[t] = std::min(std::max(1.0 / (1.0 - dsig[t]), z_min), z_max);
-      om[t] = e[n] + zf[t] * (sx[n] + sig[t] - vx[n]);
+  const CdProblem* p = nullptr;
+  std::vector<double> vx, zf, damping, prev;
+  std::vector<int> fresh;
+  int it = 0;
+  bool final_pass = false;
+  static constexpr double z_min = 0.1, z_max = 0.999;  // newton_solver.rs:93-95
+
+  void init(const CdProblem& prob) {
+    p = &prob;
+    QX_REQUIRE(p->qp && p->max_iter > 0, QX_ERR_INVALID_INPUT, "invalid arguments to g0w0_cd");
+    QX_REQUIRE(p->qp_solver == QX_QP_NEWTON || p->qp_solver == QX_QP_LINEARIZED, QX_ERR_INVALID_INPUT,
+               "qp_solver %d", p->qp_solver);
+    vx.assign(p->nmo, 0.0);
+    if (p->vxc) QX_CUDA(cudaMemcpy(vx.data(), p->vxc, p->nmo * sizeof(double), cudaMemcpyDefault));
+    zf.assign(p->ntarget, 0.0);
+    damping.assign(p->ntarget, 1.0);
+    prev.assign(p->ntarget, HUGE_VAL);
+    fresh.assign(p->ntarget, 0);
+  }
+  std::vector<int> first() const {
+    std::vector<int> all(p->ntarget);
+    for (int t = 0; t < p->ntarget; ++t) all[t] = t;
+    return all;
+  }
+  std::vector<int> advance(const std::vector<int>& act) {
+    const std::vector<double>& e = E.e;
+    const std::vector<double>& sx = E.sx;
+    const std::vector<int>& tg = E.tg;
+    std::vector<double>& om = E.om;
+    const int ntarget = p->ntarget;
+    if (p->qp_solver == QX_QP_LINEARIZED) {
+      // E = e_n + Z (Sx + Sigma(e_n) - Vxc), Z clipped (qp/evgw.rs:784-821).
+      for (int t = 0; t < ntarget; ++t) {
+        const int n = tg[t];
+        zf[t] = std::min(std::max(1.0 / (1.0 - E.dsig[t]), z_min), z_max);
+        om[t] = e[n] + zf[t] * (sx[n] + E.sig[t] - vx[n]);
+      }
+      return {};
     }
-  } else {
-    // Newton with the step rule of NewtonQPSolver::solve (newton_solver.rs:174-280):
-    // clipped step, adaptive damping in [0.1, 1].  fresh[t]: sig/dsig of
-    // target t were evaluated at om[t].
-    std::vector<int> act = all, fresh(ntarget, 0);
-    std::vector<double> damping(ntarget, 1.0), prev(ntarget, HUGE_VAL);
-    for (int it = 0; it < p.max_iter && !act.empty(); ++it) {
-      E.evaluate(act);
+    if (!final_pass) {
+      // Newton with the step rule of NewtonQPSolver::solve
+      // (newton_solver.rs:174-280): clipped step, adaptive damping in
+      // [0.1, 1].  fresh[t]: sig/dsig of target t were evaluated at om[t].
       std::vector<int> next;
       for (int t : act) {
         const int n = tg[t];
-        const double f = om[t] - e[n] - sx[n] - sig[t] + vx[n];
+        const double f = om[t] - e[n] - sx[n] - E.sig[t] + vx[n];
         const double af = std::fabs(f);
         fresh[t] = 1;
-        if (af < p.tol) continue;  // converged at om[t]
-        const double fp = 1.0 - dsig[t];
+        if (af < p->tol) continue;  // converged at om[t]
+        const double fp = 1.0 - E.dsig[t];
         double step = (std::fabs(fp) < 1e-10) ? -std::copysign(std::min(1.0, af), f) : -f / fp;
         step = std::min(std::max(step, -1.0), 1.0);
         if (af > prev[t])
@@ -351,25 +433,48 @@ void g0w0_cd_run(qx_ctx* ctx, const CdProblem& p) {
         fresh[t] = 0;
         next.push_back(t);
       }
-      act.swap(next);
+      ++it;
+      if (!next.empty() && it < p->max_iter) return next;
+      // Self-energy and slope at the returned energies (targets whose last
+      // evaluation was before their final step).
+      final_pass = true;
+      std::vector<int> stale;
+      for (int t = 0; t < ntarget; ++t)
+        if (!fresh[t]) stale.push_back(t);
+      if (!stale.empty()) return stale;
     }
-    // Self-energy and slope at the returned energies (targets whose last
-    // evaluation was before their final step).
-    std::vector<int> stale;
-    for (int t = 0; t < ntarget; ++t)
-      if (!fresh[t]) stale.push_back(t);
-    if (!stale.empty()) E.evaluate(stale);
-    for (int t = 0; t < ntarget; ++t) zf[t] = std::min(std::max(1.0 / (1.0 - dsig[t]), z_min), z_max);
+    for (int t = 0; t < ntarget; ++t) zf[t] = std::min(std::max(1.0 / (1.0 - E.dsig[t]), z_min), z_max);
+    return {};
   }
-  for (int t = 0; t < ntarget; ++t) {
-    sxo[t] = sx[tg[t]];
-    QX_REQUIRE(std::isfinite(om[t]) && std::isfinite(sig[t]), QX_ERR_NUMERICAL, "non-finite CD result for target %d",
-               tg[t]);
+  void finish() {
+    const int ntarget = p->ntarget;
+    std::vector<double> sxo(ntarget);
+    for (int t = 0; t < ntarget; ++t) {
+      sxo[t] = E.sx[E.tg[t]];
+      QX_REQUIRE(std::isfinite(E.om[t]) && std::isfinite(E.sig[t]), QX_ERR_NUMERICAL,
+                 "non-finite CD result for target %d", E.tg[t]);
+    }
+    QX_CUDA(cudaMemcpy(p->qp, E.om.data(), ntarget * sizeof(double), cudaMemcpyDefault));
+    if (p->z) QX_CUDA(cudaMemcpy(p->z, zf.data(), ntarget * sizeof(double), cudaMemcpyDefault));
+    if (p->sc) QX_CUDA(cudaMemcpy(p->sc, E.sig.data(), ntarget * sizeof(double), cudaMemcpyDefault));
+    if (p->sx) QX_CUDA(cudaMemcpy(p->sx, sxo.data(), ntarget * sizeof(double), cudaMemcpyDefault));
   }
-  QX_CUDA(cudaMemcpy(p.qp, om.data(), ntarget * sizeof(double), cudaMemcpyDefault));
-  if (p.z) QX_CUDA(cudaMemcpy(p.z, zf.data(), ntarget * sizeof(double), cudaMemcpyDefault));
-  if (p.sc) QX_CUDA(cudaMemcpy(p.sc, sig.data(), ntarget * sizeof(double), cudaMemcpyDefault));
-  if (p.sx) QX_CUDA(cudaMemcpy(p.sx, sxo.data(), ntarget * sizeof(double), cudaMemcpyDefault));
+};
+
+// Runs one system on ctx (throws qx::Error): imaginary-axis Wc for the target
+// pairs once, then QP steps; each evaluation adds the residues of the poles
+// between the target energy and the Fermi level.
+void g0w0_cd_run(qx_ctx* ctx, const CdProblem& p) {
+  CdRun R;
+  R.init(p);
+  R.E.ctx = ctx;
+  R.E.setup(p.mo_energy, p.lpq, p.targets, p.ntarget, p.nmo, p.nocc, p.naux, p.nw, p.x0, p.precision);
+  std::vector<int> act = R.first();
+  while (!act.empty()) {
+    R.E.evaluate(act);
+    act = R.advance(act);
+  }
+  R.finish();
 }
 
 // Worker context of a batch: its own non-blocking stream and workspace, so
@@ -379,9 +484,7 @@ qx_ctx* make_worker(int device) {
   c->device = device;
   c->worker = true;
   try {
-    cudaDeviceProp pr;
-    QX_CUDA(cudaGetDeviceProperties(&pr, device));
-    c->sm_count = pr.multiProcessorCount;
+    QX_CUDA(cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device));
     QX_CUDA(cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking));
     c->stream = c->own_stream;
     for (auto& ev : c->ev) QX_CUDA(cudaEventCreate(&ev));
@@ -390,6 +493,143 @@ qx_ctx* make_worker(int device) {
     throw;
   }
   return c;
+}
+
+// Workspace estimate of one system in the grouped batch (bytes): eps of the
+// grid and of the residues, the P0 operands (split forms: hi/lo of B_ov and of
+// every chi-scaled copy), chi, B_ov^T and the pair tensors of the targets.
+static double cd_system_bytes(const qx_cd_system& s, int nw, bool tc) {
+  const double ldn = round_up(s.naux, 8), nov = (double)s.nocc * (s.nmo - s.nocc), ldov = round_up((int)nov, 8);
+  const double eps = (nw + 2.0 * s.ntarget) * s.naux * ldn * 8.0;
+  const double p0 = s.naux * ldov * 8.0 + nw * ldov * 8.0 + (tc ? (1.0 + nw) * s.naux * ldov * 4.0 : 0.0);
+  const double pairs = (double)s.ntarget * s.nmo * ldn * (tc ? 16.0 : 8.0) + nw * (double)s.ntarget * s.nmo * 8.0;
+  return eps + p0 + nov * ldn * 8.0 + pairs;
+}
+
+// Grouped batch.  The systems of a wave advance phase by phase, each on the
+// stream of its own worker context (setup, P0, contraction, residue P0 and
+// solves), and every inversion of the wave -- the imaginary-axis eps of all
+// systems, then at each QP evaluation the real-axis residue eps of all
+// systems -- runs as one grouped block sweep on the context stream, so that
+// each sweep step is one launch over hundreds of matrices instead of a
+// latency-bound launch per system.  Waves hold at most 64 systems and about
+// 48 GB of estimated workspace.  Per-system failures are recorded in
+// status / msg; a failure of a grouped step throws.
+static void cd_batch_grouped(qx_ctx* ctx, qx_cd_system* systems, int nsys, int nw, double x0, double tol,
+                             int max_iter, int qp_solver, int precision, std::vector<std::string>& msg) {
+  const bool tc = is_tc_precision(precision);
+  std::vector<int> order(nsys);
+  for (int i = 0; i < nsys; ++i) order[i] = i;
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+    return cd_system_bytes(systems[a], nw, tc) > cd_system_bytes(systems[b], nw, tc);
+  });
+  constexpr double kWaveBytes = 48e9;
+  constexpr int kWaveSystems = 64;
+  for (int k = 0; k < nsys;) {
+    std::vector<int> wave;
+    double used = 0.0;
+    while (k < nsys && (int)wave.size() < kWaveSystems) {
+      const double b = cd_system_bytes(systems[order[k]], nw, tc);
+      if (!wave.empty() && used + b > kWaveBytes) break;
+      wave.push_back(order[k++]);
+      used += b;
+    }
+    const int W = (int)wave.size();
+    while ((int)ctx->workers.size() < W) ctx->workers.push_back(make_worker(ctx->device));
+    std::vector<CdProblem> probs(W);
+    std::vector<CdRun> runs(W);
+    std::vector<char> ok(W, 1);
+    std::vector<std::vector<int>> act(W);
+    auto fail = [&](int j, qx_status st, const char* what) {
+      ok[j] = 0;
+      systems[wave[j]].status = st;
+      msg[wave[j]] = what;
+    };
+    auto guarded = [&](int j, auto&& f) {
+      try {
+        f();
+      } catch (const Error& ex) {
+        fail(j, ex.status, ex.what());
+      } catch (const std::exception& ex) {
+        fail(j, QX_ERR_INVALID_INPUT, ex.what());
+      }
+    };
+    std::vector<cudaEvent_t> evs(W + 1, nullptr);
+    for (auto& e : evs) QX_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    // One grouped inversion on the context stream between the work of the
+    // systems in `live` before and after it.
+    auto grouped_inversion = [&](const std::vector<int>& live, std::vector<GMat>& mats, int half_lower,
+                                 int split_update) {
+      for (int j : live) {
+        QX_CUDA(cudaEventRecord(evs[j], ctx->workers[j]->stream));
+        QX_CUDA(cudaStreamWaitEvent(ctx->stream, evs[j], 0));
+      }
+      if (!mats.empty()) launch_invert_wc_group(ctx, mats.data(), (int)mats.size(), half_lower, split_update);
+      QX_CUDA(cudaEventRecord(evs[W], ctx->stream));
+      for (int j : live) QX_CUDA(cudaStreamWaitEvent(ctx->workers[j]->stream, evs[W], 0));
+    };
+    try {
+      // Setup and P0 of every system, then one inversion of all their eps.
+      std::vector<GMat> mats;
+      std::vector<int> live;
+      for (int j = 0; j < W; ++j) {
+        qx_cd_system& s = systems[wave[j]];
+        qx_ctx* w = ctx->workers[j];
+        reset_pending(w);
+        w->launches = 0;
+        probs[j] = CdProblem{s.mo_energy, s.lpq, s.vxc, s.nmo, s.nocc, s.naux, s.targets, s.ntarget, nw, x0, tol,
+                             max_iter, qp_solver, precision, s.qp_energies, s.z_factors, s.sigma_c, s.sigma_x};
+        guarded(j, [&] {
+          runs[j].init(probs[j]);
+          runs[j].E.ctx = w;
+          runs[j].E.setup_begin(s.mo_energy, s.lpq, s.targets, s.ntarget, s.nmo, s.nocc, s.naux, nw, x0, precision);
+          runs[j].E.eps_matrices(mats);
+          live.push_back(j);
+        });
+      }
+      grouped_inversion(live, mats, /*half_lower=*/1, /*split_update=*/tc);
+      for (int j : live)
+        if (ok[j])
+          guarded(j, [&] {
+            runs[j].E.setup_end();
+            act[j] = runs[j].first();
+          });
+      // QP evaluations in lockstep; the residue eps of all systems of an
+      // evaluation are inverted together (FP64: real axis).
+      for (;;) {
+        mats.clear();
+        live.clear();
+        for (int j = 0; j < W; ++j)
+          if (ok[j] && !act[j].empty())
+            guarded(j, [&] {
+              runs[j].E.evaluate_begin(act[j], &mats);
+              live.push_back(j);
+            });
+        if (live.empty()) break;
+        grouped_inversion(live, mats, /*half_lower=*/0, /*split_update=*/0);
+        for (int j : live)
+          if (ok[j]) guarded(j, [&] { runs[j].E.evaluate_post(); });
+        for (int j : live)
+          if (ok[j])
+            guarded(j, [&] {
+              runs[j].E.evaluate_finish();
+              act[j] = runs[j].advance(act[j]);
+            });
+        sync_and_check(ctx);
+      }
+      for (int j = 0; j < W; ++j)
+        if (ok[j])
+          guarded(j, [&] {
+            runs[j].finish();
+            systems[wave[j]].status = QX_OK;
+          });
+    } catch (...) {
+      for (auto& e : evs) cudaEventDestroy(e);
+      throw;
+    }
+    for (int j = 0; j < W; ++j) ctx->launches += ctx->workers[j]->launches;
+    for (auto& e : evs) cudaEventDestroy(e);
+  }
 }
 
 }  // namespace qx
@@ -464,10 +704,20 @@ extern "C" qx_status qx_g0w0_cd_batch(qx_ctx* ctx, qx_cd_system* systems, int ns
     QX_REQUIRE(systems && nsys > 0 && nw > 0 && max_iter > 0, QX_ERR_INVALID_INPUT, "invalid arguments to g0w0_cd_batch");
     QX_REQUIRE(precision >= QX_PREC_FP64 && precision <= QX_PREC_FP16X3, QX_ERR_INVALID_INPUT, "precision %d",
                precision);
-    if (nworkers <= 0) nworkers = 4;
-    nworkers = std::min(std::min(nworkers, 16), nsys);
     // Inputs may have been produced on the caller's stream.
     QX_CUDA(cudaStreamSynchronize(ctx->stream));
+    if (nworkers == 0) {
+      std::vector<std::string> msg(nsys);
+      for (int i = 0; i < nsys; ++i) systems[i].status = QX_ERR_INVALID_INPUT;
+      cd_batch_grouped(ctx, systems, nsys, nw, x0, tol, max_iter, qp_solver, precision, msg);
+      for (int i = 0; i < nsys; ++i)
+        if (systems[i].status != QX_OK)
+          throw Error((qx_status)systems[i].status, fmt("system %d: %s", i, msg[i].c_str()));
+      ctx->err.clear();
+      return QX_OK;
+    }
+    if (nworkers < 0) nworkers = 4;
+    nworkers = std::min(std::min(nworkers, 16), nsys);
     while ((int)ctx->workers.size() < nworkers) ctx->workers.push_back(make_worker(ctx->device));
     // Largest systems first (P0 cost nov * naux^2 dominates), so that the
     // small ones fill in behind them.

@@ -45,14 +45,47 @@ struct CdEngine {
   // pairs, Sigma_x and B_ov^T.  om starts at the mean-field energies.
   void setup(const double* mo_energy, const double* lpq, const int* targets, int ntarget, int nmo, int nocc,
              int naux, int nw, double x0, int precision);
+  // setup in two halves around the inversion of the nw eps(i f_k) (to W',
+  // half-lower), for a caller that inverts the matrices of many systems at
+  // once: setup_begin ends with eps on the device (eps_matrices lists them),
+  // setup_end runs on the inverted matrices.
+  void setup_begin(const double* mo_energy, const double* lpq, const int* targets, int ntarget, int nmo, int nocc,
+                   int naux, int nw, double x0, int precision);
+  void eps_matrices(std::vector<GMat>& out) const;
+  void setup_end();
   // Residues of the targets in act at their current om.
   std::vector<CdResidue> residues(const std::vector<int>& act) const;
   // Buffers for chunks of up to the returned capacity (~2 GB of eps).
   CdResidueChunk residue_buffers(int R);
-  // Wc, x, B_ov^T x and dWc/dw for residues list[0..rc) (device, async).
+  // Wc, x, B_ov^T x and dWc/dw for residues list[0..rc) (device, async):
+  // residue_p0 (eps(w_r)), the FP64 inversion, residue_post (the rest).
   void residue_compute(CdResidueChunk& c, const CdResidue* list, int rc);
+  void residue_p0(CdResidueChunk& c, const CdResidue* list, int rc);
+  void residue_post(CdResidueChunk& c, int rc);
   // sig/dsig of the targets in act at om (synchronises).
   void evaluate(const std::vector<int>& act);
+  // evaluate in two halves.  With group given and the residues in one chunk,
+  // evaluate_begin stops after their eps(w_r) and appends them to group
+  // (FP64 inversion to Wc by the caller, half_lower = 0) before
+  // evaluate_end; otherwise it does the whole residue work itself.
+  void evaluate_begin(const std::vector<int>& act, std::vector<GMat>* group);
+  void evaluate_end();
+  // evaluate_end in two halves: enqueue the rest of the residue work and the
+  // copies, then synchronise and combine (so that a caller can enqueue the
+  // work of many systems before waiting on any).
+  void evaluate_post();
+  void evaluate_finish();
+
+  // State of an evaluation between its halves.
+  std::vector<int> ev_act;
+  std::vector<CdResidue> ev_res;
+  std::vector<double> ev_hi, ev_rv, ev_rd;
+  CdResidueChunk ev_chunk{};
+  bool ev_grouped = false;
+  // Pinned staging in ctx->host_stage (reserved by setup_begin); sx is
+  // filled from h_sx at the first evaluation's synchronisation.
+  double *h_sx = nullptr, *h_hi = nullptr, *h_rv = nullptr, *h_rd = nullptr;
+  bool sx_pending = false;
 };
 
 void launch_cd_gather(qx_ctx* ctx, const double* lpq, int naux, int nmo, const int2* nm, int R, double* b, int ld);

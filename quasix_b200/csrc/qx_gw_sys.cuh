@@ -34,6 +34,10 @@ PairSet build_pairs(const std::vector<int>& orbs, int nmo);
 void gw_setup(qx_ctx* ctx, GWSystem& S, const double* d_lpq, int nmo, int nocc, int naux, const std::vector<int>& orbs,
               int nw, double cutoff, double x0, int precision);
 void gw_wc_pairs(qx_ctx* ctx, GWSystem& S, const double* e_host);
+// The two halves of gw_wc_pairs around the inversion of S.eps (to W', the
+// half-lower Wc): P0 into S.eps, then the pair contraction.
+void gw_wc_p0(qx_ctx* ctx, GWSystem& S, const double* e_host);
+void gw_wc_contract(qx_ctx* ctx, GWSystem& S);
 void gw_sigma(qx_ctx* ctx, GWSystem& S, const double* e_host);
 void record_stage(qx_ctx* ctx, int st, bool begin);
 void accumulate_stage_times(qx_ctx* ctx);

@@ -64,6 +64,27 @@ struct DevBuf {
   }
 };
 
+// Grow-only page-locked host buffer: device-to-host copies into it stay
+// asynchronous (a copy into pageable memory blocks the host until the stream
+// reaches it).
+struct HostBuf {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+  void reserve(size_t n) {
+    if (n <= bytes) return;
+    if (ptr) cudaFreeHost(ptr);
+    ptr = nullptr;
+    bytes = 0;
+    QX_CUDA(cudaMallocHost(&ptr, n));
+    bytes = n;
+  }
+  template <class T>
+  T* as() const { return reinterpret_cast<T*>(ptr); }
+  ~HostBuf() {
+    if (ptr) cudaFreeHost(ptr);
+  }
+};
+
 }  // namespace qx
 
 // Stage indices for timing.
@@ -80,6 +101,7 @@ struct qx_ctx {
   cudaEvent_t ev[2 * QX_ST_COUNT] = {};
   // Named workspace slots.
   qx::DevBuf ws[40];
+  qx::HostBuf host_stage;  // pinned staging of small device-to-host results
   // Device status words to inspect after the next stream synchronisation:
   // (pointer, count, kind) with kind 0 = tcgen05 pipeline error code,
   // kind 1 = per-frequency singular-eps flags.
@@ -198,6 +220,24 @@ void launch_eps_fp64(qx_ctx* ctx, const double* bov, int ldov, int naux, int nov
 void launch_invert_wc(qx_ctx* ctx, double* eps, int n, int ldn, size_t stride, int nw, int half_lower = 0,
                       int split_update = 0);
 
+// One matrix of a grouped block sweep: M [n][ldn], symmetric, inverted in
+// place.  prow (its first row in the concatenated panel arrays, a multiple of
+// 128) is assigned by launch_invert_wc_group.
+struct GMat {
+  double* M;
+  int n;
+  int ldn;
+  int prow;
+  int unused;
+};
+
+// Wc = eps^-1 - I in place for G symmetric matrices of different orders (the
+// eps of many systems at once): each block step of the sweep is one launch of
+// each kernel over all matrices that still have that block, with the
+// (matrix, tile) of a CTA found in per-step prefix tables.  half_lower and
+// split_update as launch_invert_wc.  Runs on the context stream.
+void launch_invert_wc_group(qx_ctx* ctx, const GMat* mats, int G, int half_lower, int split_update);
+
 // The same sweep on caller-provided panels (no workspace, full Wc): Tp and Pp
 // hold nw * n * SWEEP_NB doubles each, Dp nw * SWEEP_NB^2, status nw ints that
 // must be zero on entry (nonzero on exit = singular eps, Wc set to 0).
@@ -285,6 +325,11 @@ SweepSplit launch_sweep_split(qx_ctx* ctx, cudaStream_t st, const double* Tp, co
                               int nw, int buf, void* base);
 void launch_sweep_update_tc(qx_ctx* ctx, cudaStream_t st, double* eps, int n, int ldn, size_t stride, int nw,
                             int kblk, const SweepSplit& sp, int mode, int next_blk, int* err);
+// Grouped form: lower 128 x 128 tiles of the count matrices of d_mats (prefix
+// table d_pre of tile counts, ntiles in all) minus the split panels T, P
+// ([rows][128], one scale each), skipping tile row/column `step`.
+void launch_gsweep_update_tc(qx_ctx* ctx, const GMat* d_mats, const int* d_pre, int count, int ntiles, int step,
+                             const TcOperand& T, const TcOperand& P, int rows, int* err);
 
 
 }  // namespace qx

@@ -337,13 +337,15 @@ def cd_sigma(mo_energy, lpq, nocc: int, targets: Sequence[int], omega, nw: int =
 
 
 def g0w0_cd_batch(systems, nw: int = 24, x0: float = 0.5, tol: float = 1e-8, max_iter: int = 50,
-                  precision="fp64", qp_solver: str = "newton", nworkers: int = 4, device: int = 0) -> List[Dict]:
+                  precision="fp64", qp_solver: str = "newton", nworkers: int = 0, device: int = 0) -> List[Dict]:
     """G0W0-CD for many independent systems in one call (qx_g0w0_cd_batch).
 
     ``systems``: sequence of dicts with keys mo_energy, lpq ([naux, nmo, nmo],
     numpy or a CUDA tensor), nocc, targets and optionally vxc.  Returns one dict
-    per system with the keys of :func:`g0w0_cd`.  The systems run on
-    ``nworkers`` worker streams, largest first."""
+    per system with the keys of :func:`g0w0_cd`.  ``nworkers=0`` (default)
+    runs the grouped mode (all systems phase by phase, every inversion as one
+    grouped block sweep); ``nworkers > 0`` runs each system whole on one of
+    that many worker streams, largest first."""
     ctx = _ctx(device, *[s["lpq"] for s in systems])
     keep, outs = [], []
     arr = (N.CdSystem * len(systems))()

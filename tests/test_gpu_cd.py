@@ -133,11 +133,26 @@ def test_cd_linearized_matches_oracle(q):
         assert np.abs(g["z_factors"] - ref["z_factors"]).max() < 1e-8
 
 
-@pytest.mark.parametrize("precision", ["fp16x3", "bf16x3"])
-def test_cd_batch_mixed_precision_within_one_mev(q, precision):
+@pytest.mark.parametrize("qp_solver", ["newton", "linearized"])
+def test_cd_batch_grouped_matches_per_system_streams(q, qp_solver):
+    """Grouped mode (every inversion one grouped block sweep over all systems)
+    against the per-system worker streams: the FP64 sweep kernels are shared,
+    so the roots agree to rounding."""
     systems = _batch_members()
-    ref = q.g0w0_cd_batch(systems, nw=24, nworkers=2, qp_solver="linearized")
-    got = q.g0w0_cd_batch(systems, nw=24, nworkers=2, precision=precision, qp_solver="linearized")
+    kw = dict(nw=24, tol=1e-8, max_iter=50, qp_solver=qp_solver)
+    grouped = q.g0w0_cd_batch(systems, nworkers=0, **kw)
+    threaded = q.g0w0_cd_batch(systems, nworkers=3, **kw)
+    for g, t in zip(grouped, threaded):
+        for k in ("qp_energies", "z_factors", "sigma_c", "sigma_x"):
+            assert np.abs(g[k] - t[k]).max() < 1e-12, k
+
+
+@pytest.mark.parametrize("nworkers", [0, 2])
+@pytest.mark.parametrize("precision", ["fp16x3", "bf16x3"])
+def test_cd_batch_mixed_precision_within_one_mev(q, precision, nworkers):
+    systems = _batch_members()
+    ref = q.g0w0_cd_batch(systems, nw=24, nworkers=nworkers, qp_solver="linearized")
+    got = q.g0w0_cd_batch(systems, nw=24, nworkers=nworkers, precision=precision, qp_solver="linearized")
     err_mev = max(np.abs(g["qp_energies"] - r["qp_energies"]).max() for g, r in zip(got, ref)) * 27211.386
     assert err_mev < 1.0, err_mev
 
