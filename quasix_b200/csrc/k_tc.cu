@@ -151,27 +151,18 @@ template <int EPI>
 struct TcPipe {
   static constexpr int BK = 64;
   static constexpr int STAGES = 2;
-  static constexpr int UNIT = 1;  // unused by ROWDOT (one accumulation unit per N tile)
 };
-// STORE (the FP64-output GEMMs: P0, the BSE direct term): the accumulator
-// restarts every UNIT k-blocks and the epilogue sums the units in FP64.  The
-// FP32 -> FP64 conversions of one drain cost about as much as the MMAs of one
-// 64-wide k-block, so a drain per block left P0 drain-bound: at nmo 300 /
-// naux 1000 / nw 32, P0 took 2.29 ms per evGW iteration with UNIT 1, 1.93 ms
-// with UNIT 2 and 1.72 ms with UNIT 4, at QP errors against FP64 of 0.024,
-// 0.036 and 0.068 meV.  A third stage measured no faster.
-#ifndef QX_TC_STORE_STAGES
-#define QX_TC_STORE_STAGES 2
-#endif
-#ifndef QX_TC_STORE_UNIT
-#define QX_TC_STORE_UNIT 2
-#endif
-template <>
-struct TcPipe<1> {
-  static constexpr int BK = 64;
-  static constexpr int STAGES = QX_TC_STORE_STAGES;
-  static constexpr int UNIT = QX_TC_STORE_UNIT;
-};
+// STORE (the FP64-output GEMMs: P0, the sweep update, the BSE direct term):
+// the accumulator restarts every TcArgs::unit k-blocks and the epilogue sums
+// the units in FP64.  The FP32 -> FP64 conversions of one drain cost about as
+// much as the MMAs of one 64-wide k-block, so a drain per block left P0
+// drain-bound: at nmo 300 / naux 1000 / nw 32, P0 took 2.29 ms per evGW
+// iteration with unit 1, 1.93 ms with unit 2 and 1.72 ms with unit 4, at QP
+// errors against FP64 of 0.024, 0.036 and 0.068 meV.  P0 and the sweep use
+// unit 2; the BSE direct term keeps unit 1, since with unit 2 the Davidson
+// residuals of the 26 400-dimensional problem stalled above 1e-8.  A third
+// stage measured no faster.
+constexpr int kP0Unit = 2;
 // Epilogue warps: 4 (ROWDOT: one TMEM lane quarter each) or 8 (STORE: two
 // warps per lane quarter, 64 columns each).
 template <int EPI>
@@ -224,6 +215,7 @@ struct TcArgs {
   const GMat* gmats;
   const int* gpre;
   int gcount;
+  int unit;  // STORE: k-blocks per FP32 accumulation unit (0 counts as 1)
 };
 
 // x[q] = xr[q] for the columns col0 + q < N of a valid row, 0 otherwise
@@ -405,9 +397,9 @@ __global__ void __launch_bounds__(TcWarps<EPI>::THREADS, 1)
         for (int nt = nt_begin; nt < nt_end && ok; ++nt) {
           const int kbe = args.tri ? min(k_blocks, (nt * BN + BN + TC_BK - 1) / TC_BK) : k_blocks;
           for (int kb = 0; kb < kbe; ++kb, ++g) {
-            constexpr int UNIT = TcPipe<EPI>::UNIT;
-            const bool unit_start = (EPI == EPI_STORE) ? (kb % UNIT == 0) : kb == 0;
-            const bool unit_end = (EPI == EPI_STORE) ? (kb % UNIT == UNIT - 1 || kb == kbe - 1) : kb == kbe - 1;
+            const int unit = args.unit > 0 ? args.unit : 1;
+            const bool unit_start = (EPI == EPI_STORE) ? (kb % unit == 0) : kb == 0;
+            const bool unit_end = (EPI == EPI_STORE) ? (kb % unit == unit - 1 || kb == kbe - 1) : kb == kbe - 1;
             const int buf = u & 1;
             if (unit_start && u >= 2) {
               if (!mbar_wait(&acc_empty[buf], ((u / 2) - 1) & 1, abort_flag, args.err, 2)) {
@@ -503,7 +495,8 @@ __global__ void __launch_bounds__(TcWarps<EPI>::THREADS, 1)
 #pragma unroll
       for (int c = 0; c < 64; ++c) acc[c] = 0.0;
       bool ok = true;
-      const int n_units = (k_blocks + TcPipe<EPI>::UNIT - 1) / TcPipe<EPI>::UNIT;
+      const int unit = args.unit > 0 ? args.unit : 1;
+      const int n_units = (k_blocks + unit - 1) / unit;
       for (int u = 0; u < n_units; ++u) {
         const int buf = u & 1;
         if (!mbar_wait(&acc_full[buf], (u / 2) & 1, abort_flag, args.err, 4)) {
@@ -1035,6 +1028,7 @@ void launch_eps_tc(qx_ctx* ctx, const double* bov, int ldov, int naux, int nov, 
   a.out_stride = eps_stride;
   a.lower_tiles = 1;
   a.add_identity = 1;
+  a.unit = kP0Unit;
   a.fp16 = fp16;
   a.scaleA = sa;
   a.scaleB = sb;
@@ -1125,6 +1119,7 @@ void launch_sweep_update_tc(qx_ctx* ctx, cudaStream_t st, double* eps, int n, in
   a.lower_tiles = 1;
   a.subtract = 1;
   a.a_batched = 1;
+  a.unit = kP0Unit;
   a.fp16 = 1;
   a.scaleA = sp.T.scale;
   a.scaleB = sp.P.scale;
@@ -1152,6 +1147,7 @@ void launch_gsweep_update_tc(qx_ctx* ctx, const GMat* d_mats, const int* d_pre, 
   a.lower_tiles = 1;
   a.subtract = 1;
   a.fp16 = 1;
+  a.unit = kP0Unit;
   a.scaleA = T.scale;
   a.scaleB = P.scale;
   a.err = err;
