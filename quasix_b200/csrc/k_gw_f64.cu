@@ -368,38 +368,48 @@ __global__ void __launch_bounds__(SweepTile::THREADS) k_sweep_update(double* __r
                     tn, mode, nk0, nkb);
 }
 
-// Element (r, q), q < 128, of the panel write: P[r][q] = the old M[r][k0 + q]
-// for rows outside K and q < kb, zero otherwise (a split of P then sees no
-// stale values); for q < kb, M[r][k0 + q] = M[k0 + q][r] = T[r][q] outside K
-// and -D inside.  The mirror writes of rows outside K land in rows inside K,
-// which no thread reads here.  Inside the K block both (r, q) and its mirror
-// write the same element: D's lower triangle serves both, so the stored value
-// does not depend on which write lands last.
-__device__ __forceinline__ void sweep_write_elem(double* __restrict__ A, int ldn, int k0, int kb,
+// Rows [r0, r0 + 32) of the panel write (256 threads).  P[r][q] = the old
+// M[r][k0 + q] for rows outside K and q < kb, zero otherwise (a split of P
+// then sees no stale values); for q < kb, M[r][k0 + q] = M[k0 + q][r] =
+// T[r][q] outside K and -D inside.  The row-major part runs along q; the
+// mirror goes through a shared-memory transpose so that it runs along r.  No
+// thread reads what another writes: rows outside K read and write only their
+// own row, the mirror writes land in rows inside K, and the rows inside K
+// read no old value.  Inside the K block both (r, q) and its mirror write the
+// same element: D's lower triangle serves both, so the stored value does not
+// depend on which write lands last.
+constexpr int kWriteRows = 32;
+__device__ __forceinline__ void sweep_write_tile(double* __restrict__ A, int n, int ldn, int k0, int kb,
                                                  const double* __restrict__ Tw, double* __restrict__ Pw,
-                                                 const double* __restrict__ D, int r, int q) {
-  const bool in_k = (r >= k0 && r < k0 + kb);
-  if (q >= kb) {
-    Pw[(size_t)r * SWEEP_NB + q] = 0.0;
-    return;
+                                                 const double* __restrict__ D, int r0) {
+  __shared__ double S[kWriteRows][SWEEP_NB + 1];
+  for (int e = threadIdx.x; e < kWriteRows * SWEEP_NB; e += blockDim.x) {
+    const int rr = e / SWEEP_NB, q = e % SWEEP_NB, r = r0 + rr;
+    if (r >= n) continue;
+    if (q >= kb) {
+      Pw[(size_t)r * SWEEP_NB + q] = 0.0;
+      continue;
+    }
+    const bool in_k = (r >= k0 && r < k0 + kb);
+    Pw[(size_t)r * SWEEP_NB + q] = in_k ? 0.0 : A[(size_t)r * ldn + k0 + q];
+    const int a = r - k0;
+    const double v = in_k ? -D[max(a, q) * SWEEP_NB + min(a, q)] : Tw[(size_t)r * SWEEP_NB + q];
+    A[(size_t)r * ldn + k0 + q] = v;
+    S[rr][q] = v;
   }
-  Pw[(size_t)r * SWEEP_NB + q] = in_k ? 0.0 : A[(size_t)r * ldn + k0 + q];
-  const int a = r - k0;
-  const double v = in_k ? -D[max(a, q) * SWEEP_NB + min(a, q)] : Tw[(size_t)r * SWEEP_NB + q];
-  A[(size_t)r * ldn + k0 + q] = v;
-  A[(size_t)(k0 + q) * ldn + r] = v;
+  __syncthreads();
+  for (int e = threadIdx.x; e < kWriteRows * SWEEP_NB; e += blockDim.x) {
+    const int q = e / kWriteRows, rr = e % kWriteRows, r = r0 + rr;
+    if (q < kb && r < n) A[(size_t)(k0 + q) * ldn + r] = S[rr][q];
+  }
 }
 
-__global__ void k_sweep_write(double* __restrict__ M, int n, int ldn, size_t stride, int k0, int kb,
-                              const double* __restrict__ Tp, double* __restrict__ Pp, size_t pstride,
-                              const double* __restrict__ Dp) {
+__global__ void __launch_bounds__(256) k_sweep_write(double* __restrict__ M, int n, int ldn, size_t stride, int k0,
+                                                     int kb, const double* __restrict__ Tp, double* __restrict__ Pp,
+                                                     size_t pstride, const double* __restrict__ Dp) {
   const int w = blockIdx.y;
-  double* A = M + (size_t)w * stride;
-  const double* Tw = Tp + (size_t)w * pstride;
-  double* Pw = Pp + (size_t)w * pstride;
-  const double* D = Dp + (size_t)w * SWEEP_NB * SWEEP_NB;
-  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < n * SWEEP_NB; idx += gridDim.x * blockDim.x)
-    sweep_write_elem(A, ldn, k0, kb, Tw, Pw, D, idx / SWEEP_NB, idx % SWEEP_NB);
+  sweep_write_tile(M + (size_t)w * stride, n, ldn, k0, kb, Tp + (size_t)w * pstride, Pp + (size_t)w * pstride,
+                   Dp + (size_t)w * SWEEP_NB * SWEEP_NB, blockIdx.x * kWriteRows);
 }
 
 // After the last sweep M = -eps^-1; Wc = eps^-1 - I = -M - I.  A frequency
@@ -457,7 +467,7 @@ static void sweep_front(qx_ctx* ctx, cudaStream_t st, double* eps, int n, int ld
   dim3 tg(ceil_div(n, PanelTile::BM), ceil_div(kb, PanelTile::BN), nw);
   k_sweep_tpanel<<<tg, PanelTile::THREADS, PanelTile::SMEM, st>>>(eps, n, ldn, stride, k0, kb, Dp, Tp, pstride);
   check_launch(ctx);
-  dim3 wg(ceil_div(n * SWEEP_NB, 256), nw);
+  dim3 wg(ceil_div(n, kWriteRows), nw);
   k_sweep_write<<<wg, 256, 0, st>>>(eps, n, ldn, stride, k0, kb, Tp, Pp, pstride, Dp);
   check_launch(ctx);
 }
@@ -611,16 +621,14 @@ __global__ void __launch_bounds__(PanelTile::THREADS) k_gsweep_tpanel(const GMat
                     Tcat + (size_t)m.prow * SWEEP_NB, (t >> 1) * PanelTile::BM, (t & 1) * PanelTile::BN);
 }
 
-__global__ void k_gsweep_write(const GMat* __restrict__ mats, const int* __restrict__ pre, int count, int k0,
-                               const double* __restrict__ Tcat, double* __restrict__ Pcat,
-                               const double* __restrict__ Dp) {
+__global__ void __launch_bounds__(256) k_gsweep_write(const GMat* __restrict__ mats, const int* __restrict__ pre,
+                                                      int count, int k0, const double* __restrict__ Tcat,
+                                                      double* __restrict__ Pcat, const double* __restrict__ Dp) {
   const int g = group_of(pre, count, blockIdx.x);
   const GMat m = mats[g];
-  const int idx = (blockIdx.x - pre[g]) * blockDim.x + threadIdx.x;
-  if (idx >= m.n * SWEEP_NB) return;
-  sweep_write_elem(m.M, m.ldn, k0, min(SWEEP_NB, m.n - k0), Tcat + (size_t)m.prow * SWEEP_NB,
-                   Pcat + (size_t)m.prow * SWEEP_NB, Dp + (size_t)g * SWEEP_NB * SWEEP_NB, idx / SWEEP_NB,
-                   idx % SWEEP_NB);
+  sweep_write_tile(m.M, m.n, m.ldn, k0, min(SWEEP_NB, m.n - k0), Tcat + (size_t)m.prow * SWEEP_NB,
+                   Pcat + (size_t)m.prow * SWEEP_NB, Dp + (size_t)g * SWEEP_NB * SWEEP_NB,
+                   (blockIdx.x - pre[g]) * kWriteRows);
 }
 
 __global__ void __launch_bounds__(SweepTile::THREADS) k_gsweep_update(const GMat* __restrict__ mats,
@@ -698,7 +706,7 @@ void launch_invert_wc_group(qx_ctx* ctx, const GMat* mats_in, int G, int half_lo
     act[s] = a;
     rows_act[s] = m[a - 1].prow + round_up(m[a - 1].n, SWEEP_NB);
     off_tp[s] = add_table(a, [](const GMat& x) { return (long long)ceil_div(x.n, PanelTile::BM) * 2; });
-    off_wr[s] = add_table(a, [](const GMat& x) { return (long long)ceil_div(x.n * SWEEP_NB, 256); });
+    off_wr[s] = add_table(a, [](const GMat& x) { return (long long)ceil_div(x.n, kWriteRows); });
     if (tc)
       off_up[s] = add_table(a, [](const GMat& x) {
         const long long t = ceil_div(x.n, SWEEP_NB);

@@ -163,8 +163,10 @@ struct TcPipe {
 // residuals of the 26 400-dimensional problem stalled above 1e-8.  A third
 // stage measured no faster.
 constexpr int kP0Unit = 2;
-// Epilogue warps: 4 (ROWDOT: one TMEM lane quarter each) or 8 (STORE: two
-// warps per lane quarter, 64 columns each).
+// Epilogue warps: 8, two per TMEM lane quarter (ROWDOT: half an N tile each;
+// STORE: 64 columns each).  For STORE, 16 warps of 32 columns (FP64 or
+// Kahan-compensated FP32 drain) measured no faster for P0 and slower for the
+// BSE direct term.
 template <int EPI>
 struct TcWarps {
   static constexpr int NEPI = 8;
@@ -487,13 +489,14 @@ __global__ void __launch_bounds__(TcWarps<EPI>::THREADS, 1)
         args.out[(size_t)w * args.ldo + m] = (red[row] + red[TC_BM + row]) * unscale_rowdot(args, w) * (args.tri ? 2.0 : 1.0);
     } else {
       // ---------------- epilogue (warps 2..9): FP64 sum of k-block partials ----------------
+      constexpr int CPW = BN * 4 / TcWarps<EPI>::NEPI;  // columns per epilogue warp
       const int quarter = warp & 3;
-      const int half = (warp - 2) >> 2;  // columns [64 half, 64 half + 64) of the tile
+      const int part = (warp - 2) >> 2;  // columns [CPW part, CPW part + CPW) of the tile
       const int m = m0 + quarter * 32 + lane;
       const double unscale = 1.0 / ((double)args.scaleA[args.a_batched ? w : 0] * (double)args.scaleB[w]);
-      double acc[64];
+      double acc[CPW];
 #pragma unroll
-      for (int c = 0; c < 64; ++c) acc[c] = 0.0;
+      for (int c = 0; c < CPW; ++c) acc[c] = 0.0;
       bool ok = true;
       const int unit = args.unit > 0 ? args.unit : 1;
       const int n_units = (k_blocks + unit - 1) / unit;
@@ -504,9 +507,9 @@ __global__ void __launch_bounds__(TcWarps<EPI>::THREADS, 1)
           break;
         }
         tc_fence_after();
-        const uint32_t taddr = tmem_base + ((uint32_t)(quarter * 32) << 16) + buf * BN + 64 * half;
+        const uint32_t taddr = tmem_base + ((uint32_t)(quarter * 32) << 16) + buf * BN + CPW * part;
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
+        for (int j = 0; j < CPW / 16; ++j) {
           float v[16];
           tmem_ld16(taddr + 16 * j, v);
 #pragma unroll
@@ -517,10 +520,10 @@ __global__ void __launch_bounds__(TcWarps<EPI>::THREADS, 1)
         if (lane == 0) mbar_arrive(&acc_empty[buf]);
       }
       if (ok && m < outM) {
-        const int n0 = nt_begin * BN + 64 * half;
+        const int n0 = nt_begin * BN + CPW * part;
         double* orow = out_base + (size_t)w * out_stride + (size_t)m * out_ld;
 #pragma unroll
-        for (int c = 0; c < 64; ++c) {
+        for (int c = 0; c < CPW; ++c) {
           const int n = n0 + c;
           // Lower-triangular mode writes the lower triangle and mirrors it,
           // so the stored matrix is exactly symmetric.
