@@ -416,21 +416,21 @@ __global__ void __launch_bounds__(256) k_sweep_write(double* __restrict__ M, int
 // whose eps was singular gets Wc = 0 (eps^-1 replaced by the identity).  With
 // half_lower the output is W' = strict lower triangle of Wc + diag(Wc) / 2 and
 // zeros above, so that b^T Wc b = 2 b^T W' b needs only the lower triangle.
-__device__ __forceinline__ void finish_wc_elem(double* __restrict__ A, int ldn, bool singular, int half_lower, int r,
-                                               int c) {
-  double v = singular ? 0.0 : -A[(size_t)r * ldn + c] - (r == c ? 1.0 : 0.0);
-  if (half_lower) v = (c < r) ? v : (c == r ? 0.5 * v : 0.0);
-  A[(size_t)r * ldn + c] = v;
+// Row r of the finish (one block per row).
+__device__ __forceinline__ void finish_wc_row(double* __restrict__ A, int n, int ldn, bool singular, int half_lower,
+                                              int r) {
+  double* row = A + (size_t)r * ldn;
+  for (int c = threadIdx.x; c < n; c += blockDim.x) {
+    double v = singular ? 0.0 : -row[c] - (r == c ? 1.0 : 0.0);
+    if (half_lower) v = (c < r) ? v : (c == r ? 0.5 * v : 0.0);
+    row[c] = v;
+  }
 }
 
 __global__ void k_finish_wc(double* __restrict__ M, int n, int ldn, size_t stride, const int* __restrict__ status,
                             int half_lower) {
   const int w = blockIdx.y;
-  double* A = M + (size_t)w * stride;
-  const bool singular = status[w] != 0;
-  for (size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x; idx < (size_t)n * n;
-       idx += (size_t)gridDim.x * blockDim.x)
-    finish_wc_elem(A, ldn, singular, half_lower, (int)(idx / n), (int)(idx % n));
+  finish_wc_row(M + (size_t)w * stride, n, ldn, status[w] != 0, half_lower, blockIdx.x);
 }
 
 static_assert(kSweepPanelCols == SWEEP_NB, "panel width");
@@ -563,7 +563,7 @@ void launch_invert_wc(qx_ctx* ctx, double* eps, int n, int ldn, size_t stride, i
     QX_CUDA(cudaEventRecord(ev_done, s0));
     QX_CUDA(cudaStreamWaitEvent(ctx->stream, ev_done, 0));
   }
-  dim3 fg(ceil_div(n * n, 256 * 4), nw);
+  dim3 fg(n, nw);
   k_finish_wc<<<fg, 256, 0, ctx->stream>>>(eps, n, ldn, stride, status, half_lower);
   check_launch(ctx);
   ctx->pending.push_back({status, nw, 1});
@@ -578,7 +578,7 @@ void launch_invert_wc_panels(qx_ctx* ctx, double* eps, int n, int ldn, size_t st
     sweep_front(ctx, ctx->stream, eps, n, ldn, stride, nw, k0, kb, Tp, Dp, Pp, pstride, status);
     sweep_update(ctx, ctx->stream, eps, n, ldn, stride, nw, k0, kb, Tp, Pp, pstride, 0, 0, 0);
   }
-  dim3 fg(ceil_div(n * n, 256 * 4), nw);
+  dim3 fg(n, nw);
   k_finish_wc<<<fg, 256, 0, ctx->stream>>>(eps, n, ldn, stride, status, 0);
   check_launch(ctx);
 }
@@ -647,9 +647,7 @@ __global__ void k_gfinish_wc(const GMat* __restrict__ mats, const int* __restric
                              const int* __restrict__ status, int half_lower) {
   const int g = group_of(pre, count, blockIdx.x);
   const GMat m = mats[g];
-  const int idx = (blockIdx.x - pre[g]) * blockDim.x + threadIdx.x;
-  if (idx >= m.n * m.n) return;
-  finish_wc_elem(m.M, m.ldn, status[g] != 0, half_lower, idx / m.n, idx % m.n);
+  finish_wc_row(m.M, m.n, m.ldn, status[g] != 0, half_lower, blockIdx.x - pre[g]);
 }
 
 // Zero the padding rows [n, n rounded up to 128) of each matrix's panels
@@ -718,7 +716,7 @@ void launch_invert_wc_group(qx_ctx* ctx, const GMat* mats_in, int G, int half_lo
         return t * (t + 1) / 2;
       });
   }
-  const size_t off_fin = add_table(G, [](const GMat& x) { return ((long long)x.n * x.n + 255) / 256; });
+  const size_t off_fin = add_table(G, [](const GMat& x) { return (long long)x.n; });
   // Workspace: T, P [R][128] FP64, D [G][128][128], the matrix and prefix tables.
   const size_t pan = (size_t)R * SWEEP_NB;
   const size_t dsz = (size_t)G * SWEEP_NB * SWEEP_NB;
@@ -828,8 +826,9 @@ void launch_gather_ov(qx_ctx* ctx, const double* lpq, int naux, int nmo, int noc
 }
 
 // sx[p] = -sum_{R,i} lpq[R][p][i]^2   (qp/evgw.rs:1167-1193)
-__global__ void k_exchange_diag(const double* __restrict__ lpq, int naux, int nmo, int nocc, double* __restrict__ sx) {
-  const int p = blockIdx.x;
+__global__ void k_exchange_diag(const double* __restrict__ lpq, int naux, int nmo, int nocc,
+                                const int* __restrict__ orbs, double* __restrict__ sx) {
+  const int p = orbs ? orbs[blockIdx.x] : blockIdx.x;
   double s = 0.0;
   for (int idx = threadIdx.x; idx < naux * nocc; idx += blockDim.x) {
     int R = idx / nocc, i = idx % nocc;
@@ -846,8 +845,9 @@ __global__ void k_exchange_diag(const double* __restrict__ lpq, int naux, int nm
   if (threadIdx.x == 0) sx[p] = -red[0];
 }
 
-void launch_exchange_diag(qx_ctx* ctx, const double* lpq, int naux, int nmo, int nocc, double* sx) {
-  k_exchange_diag<<<nmo, 256, 0, ctx->stream>>>(lpq, naux, nmo, nocc, sx);
+void launch_exchange_diag(qx_ctx* ctx, const double* lpq, int naux, int nmo, int nocc, double* sx,
+                          const int* orbs, int norbs) {
+  k_exchange_diag<<<orbs ? norbs : nmo, 256, 0, ctx->stream>>>(lpq, naux, nmo, nocc, orbs, sx);
   check_launch(ctx);
 }
 

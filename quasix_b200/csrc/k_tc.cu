@@ -1000,19 +1000,26 @@ void launch_pair_contract_tc(qx_ctx* ctx, const TcOperand& A, const float* bpt_f
 
 // eps[w] = I + Bov diag(chi[w]) Bov^T with A = split(Bov), B = split(Bov * chi[w]).
 void launch_eps_tc(qx_ctx* ctx, const double* bov, int ldov, int naux, int nov, const double* chi, int nw,
-                   double* eps, int ldn, size_t eps_stride, int fp16) {
+                   double* eps, int ldn, size_t eps_stride, int fp16, int reuse_a) {
   constexpr int BN = 128;
   const size_t a_elems = (size_t)naux * ldov;
   DevBuf& buf = ctx->ws[WS_BOV_HI];
-  buf.reserve(a_elems * 2 * 2 * (1 + (size_t)nw));
+  const size_t need = a_elems * 2 * 2 * (1 + (size_t)nw);
+  // The A split (and its scale in split slot 7) survive from the previous
+  // call on this context only if the buffer is not reallocated now.
+  reuse_a = reuse_a && buf.bytes >= need;
+  buf.reserve(need);
   uint8_t* p = buf.as<uint8_t>();
   void* a_hi = p;
   void* a_lo = p + a_elems * 2;
   void* b_hi = p + a_elems * 4;
   void* b_lo = p + a_elems * 4 + a_elems * 2 * nw;
   float *sa = nullptr, *sb = nullptr;
-  split(ctx, bov, naux, nov, ldov, 0, a_hi, a_lo, ldov, 0, 1, nullptr, 0, fp16, 0, &sa);
-  split(ctx, bov, naux, nov, ldov, 0, b_hi, b_lo, ldov, a_elems, nw, chi, ldov, fp16, 1, &sb, /*amax of bov*/ 0);
+  if (reuse_a)
+    sa = split_scratch(ctx, 7).scale;
+  else
+    split(ctx, bov, naux, nov, ldov, 0, a_hi, a_lo, ldov, 0, 1, nullptr, 0, fp16, 7, &sa);
+  split(ctx, bov, naux, nov, ldov, 0, b_hi, b_lo, ldov, a_elems, nw, chi, ldov, fp16, 1, &sb, /*amax of bov*/ 7);
   constexpr int BK = TcPipe<EPI_STORE>::BK;
   CUtensorMap ah = make_map(a_hi, nov, naux, ldov, 1, TC_BM, 2, fp16, BK);
   CUtensorMap al = make_map(a_lo, nov, naux, ldov, 1, TC_BM, 2, fp16, BK);

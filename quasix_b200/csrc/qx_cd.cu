@@ -180,7 +180,9 @@ void CdEngine::setup_end() {
   double* d_sx = cb.as<double>();
   d_om = d_sx + nmo;
   d_imag = d_om + ntarget;
-  launch_exchange_diag(ctx, d_lpq, naux, nmo, nocc, d_sx);
+  // Sigma_x of the targets only (the other entries of sx stay zero).
+  QX_CUDA(cudaMemsetAsync(d_sx, 0, nmo * sizeof(double), ctx->stream));
+  launch_exchange_diag(ctx, d_lpq, naux, nmo, nocc, d_sx, S.d_orbs, ntarget);
   // Read into sx at the next evaluation's synchronisation.
   sx.assign(nmo, 0.0);
   QX_CUDA(cudaMemcpyAsync(h_sx, d_sx, nmo * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
@@ -254,7 +256,8 @@ void CdEngine::residue_p0(CdResidueChunk& c, const CdResidue* list, int rc) {
   // eps(w_r) = I + B_ov diag(chi'(w_r)) B_ov^T, real axis.
   launch_chi(ctx, S.d_en, nocc, nvir, c.wr, rc, 1, c.chi, S.ldov);
   if (tc)
-    launch_eps_tc(ctx, S.bov, S.ldov, naux, nov, c.chi, rc, c.eps, ldn, stride, precision == QX_PREC_FP16X3);
+    launch_eps_tc(ctx, S.bov, S.ldov, naux, nov, c.chi, rc, c.eps, ldn, stride, precision == QX_PREC_FP16X3,
+                  /*reuse_a=*/1);
   else
     launch_eps_fp64(ctx, S.bov, S.ldov, naux, nov, c.chi, rc, c.eps, ldn, stride);
 }

@@ -256,7 +256,10 @@ void launch_pair_contract_fp64(qx_ctx* ctx, const double* bpt, int ldk, int npai
 void launch_gather_pairs(qx_ctx* ctx, const double* lpq, int naux, int nmo, const int2* pairs, int npair,
                          double* bpt, int ldk);
 void launch_gather_ov(qx_ctx* ctx, const double* lpq, int naux, int nmo, int nocc, double* bov, int ldov);
-void launch_exchange_diag(qx_ctx* ctx, const double* lpq, int naux, int nmo, int nocc, double* sx);
+// sx[p] = -sum_{R,i} lpq[R][p][i]^2 for every orbital, or only for the norbs
+// orbitals orbs (device array) when given.
+void launch_exchange_diag(qx_ctx* ctx, const double* lpq, int naux, int nmo, int nocc, double* sx,
+                          const int* orbs = nullptr, int norbs = 0);
 
 // Sigma_c(iw_k) assembly: sigma[t][k] (complex) for each target t.  sigma must
 // be the start of the WS_SIGMA slot sized by sigma_workspace_doubles.
@@ -303,11 +306,13 @@ struct TcOperand {
 };
 inline bool is_tc_precision(int p) { return p == QX_PREC_BF16X3 || p == QX_PREC_FP16X3; }
 // slot selects one of the scratch areas for the scales (0..2; 3..6 belong to
-// the sweep).
+// the sweep, 7 to the B_ov split of P0).
 void launch_split(qx_ctx* ctx, const double* src, int rows, int cols, int ld_src, void* hi, void* lo, int ld_dst,
                   size_t src_stride, size_t dst_stride, int batch, int fp16, int slot, float** scale_out);
+// reuse_a: B_ov is the one split by the previous call on this context; its
+// hi/lo split is reused (unless the operand buffer has to grow).
 void launch_eps_tc(qx_ctx* ctx, const double* bov, int ldov, int naux, int nov, const double* chi, int nw,
-                   double* eps, int ldn, size_t eps_stride, int fp16);
+                   double* eps, int ldn, size_t eps_stride, int fp16, int reuse_a = 0);
 void launch_gemm_tc(qx_ctx* ctx, const TcOperand& A, int M, int lda, const TcOperand& B, int N, int ldb, int K,
                     int nbatch, double* out, int ldo, size_t out_stride, int fp16);
 void launch_pair_contract_tc(qx_ctx* ctx, const TcOperand& A, const float* bpt_f32, int ldk, int npair, int naux,
