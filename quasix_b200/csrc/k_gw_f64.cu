@@ -272,11 +272,25 @@ __global__ void __launch_bounds__(512) k_sweep_diag(const double* __restrict__ M
 
 using PanelTile = F64Tile<64, 64, 2, 2, 3>;
 
+// *out = max(*out, max over the block of m) (m >= 0 compares as its bit
+// pattern); every thread of the block calls it; red holds one double per warp.
+__device__ __forceinline__ void block_amax(double m, double* red, unsigned long long* out) {
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    m = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if (threadIdx.x == 0) atomicMax(out, __double_as_longlong(m));
+  }
+}
+
 // Tile (m0, n0) of T[r][:] = M[r][K] D (D symmetric: its rows serve as the B
-// operand); columns past kb come out zero.
+// operand); columns past kb come out zero.  amax (optional): max|T| of the
+// tile joins *amax (the bound of a later split of T).
 __device__ __forceinline__ void sweep_tpanel_body(const double* __restrict__ M, int n, int ldn, int k0, int kb,
                                                   const double* __restrict__ Dw, double* __restrict__ Tw, int m0,
-                                                  int n0) {
+                                                  int n0, unsigned long long* amax) {
   using T = PanelTile;
   extern __shared__ double smem[];
   double acc[T::MI][T::NJ][2];
@@ -296,16 +310,30 @@ __device__ __forceinline__ void sweep_tpanel_body(const double* __restrict__ M, 
         const int r = m0 + f64_row<T>(i), c = n0 + f64_col<T>(j, e);
         if (r < n && c < SWEEP_NB) Tw[(size_t)r * SWEEP_NB + c] = acc[i][j][e];
       }
+  if (amax) {
+    // The mainloop has drained its stages: smem is free for the reduction.
+    double mx = 0.0;
+#pragma unroll
+    for (int i = 0; i < T::MI; ++i)
+#pragma unroll
+      for (int j = 0; j < T::NJ; ++j)
+#pragma unroll
+        for (int e = 0; e < 2; ++e)
+          if (m0 + f64_row<T>(i) < n) mx = fmax(mx, fabs(acc[i][j][e]));
+    block_amax(mx, smem, amax);
+  }
 }
 
 // T[w][r][:] = M[w][r][K] D[w]
 __global__ void __launch_bounds__(PanelTile::THREADS) k_sweep_tpanel(const double* __restrict__ M, int n, int ldn,
                                                                      size_t stride, int k0, int kb,
                                                                      const double* __restrict__ Dp,
-                                                                     double* __restrict__ Tp, size_t pstride) {
+                                                                     double* __restrict__ Tp, size_t pstride,
+                                                                     unsigned long long* amax) {
   const int w = blockIdx.z;
   sweep_tpanel_body(M + (size_t)w * stride, n, ldn, k0, kb, Dp + (size_t)w * SWEEP_NB * SWEEP_NB,
-                    Tp + (size_t)w * pstride, blockIdx.x * PanelTile::BM, blockIdx.y * PanelTile::BN);
+                    Tp + (size_t)w * pstride, blockIdx.x * PanelTile::BM, blockIdx.y * PanelTile::BN,
+                    amax ? amax + w : nullptr);
 }
 
 using SweepTile = F64Tile<64, 64, 2, 2, 3>;
@@ -381,8 +409,10 @@ __global__ void __launch_bounds__(SweepTile::THREADS) k_sweep_update(double* __r
 constexpr int kWriteRows = 32;
 __device__ __forceinline__ void sweep_write_tile(double* __restrict__ A, int n, int ldn, int k0, int kb,
                                                  const double* __restrict__ Tw, double* __restrict__ Pw,
-                                                 const double* __restrict__ D, int r0) {
+                                                 const double* __restrict__ D, int r0, unsigned long long* amax) {
   __shared__ double S[kWriteRows][SWEEP_NB + 1];
+  __shared__ double red[8];
+  double mx = 0.0;  // max|P| of the tile (amax, optional: the bound of a later split of P)
   for (int e = threadIdx.x; e < kWriteRows * SWEEP_NB; e += blockDim.x) {
     const int rr = e / SWEEP_NB, q = e % SWEEP_NB, r = r0 + rr;
     if (r >= n) continue;
@@ -391,7 +421,9 @@ __device__ __forceinline__ void sweep_write_tile(double* __restrict__ A, int n, 
       continue;
     }
     const bool in_k = (r >= k0 && r < k0 + kb);
-    Pw[(size_t)r * SWEEP_NB + q] = in_k ? 0.0 : A[(size_t)r * ldn + k0 + q];
+    const double old = in_k ? 0.0 : A[(size_t)r * ldn + k0 + q];
+    Pw[(size_t)r * SWEEP_NB + q] = old;
+    mx = fmax(mx, fabs(old));
     const int a = r - k0;
     const double v = in_k ? -D[max(a, q) * SWEEP_NB + min(a, q)] : Tw[(size_t)r * SWEEP_NB + q];
     A[(size_t)r * ldn + k0 + q] = v;
@@ -402,14 +434,16 @@ __device__ __forceinline__ void sweep_write_tile(double* __restrict__ A, int n, 
     const int q = e / kWriteRows, rr = e % kWriteRows, r = r0 + rr;
     if (q < kb && r < n) A[(size_t)(k0 + q) * ldn + r] = S[rr][q];
   }
+  if (amax) block_amax(mx, red, amax);
 }
 
 __global__ void __launch_bounds__(256) k_sweep_write(double* __restrict__ M, int n, int ldn, size_t stride, int k0,
                                                      int kb, const double* __restrict__ Tp, double* __restrict__ Pp,
-                                                     size_t pstride, const double* __restrict__ Dp) {
+                                                     size_t pstride, const double* __restrict__ Dp,
+                                                     unsigned long long* amax) {
   const int w = blockIdx.y;
   sweep_write_tile(M + (size_t)w * stride, n, ldn, k0, kb, Tp + (size_t)w * pstride, Pp + (size_t)w * pstride,
-                   Dp + (size_t)w * SWEEP_NB * SWEEP_NB, blockIdx.x * kWriteRows);
+                   Dp + (size_t)w * SWEEP_NB * SWEEP_NB, blockIdx.x * kWriteRows, amax ? amax + w : nullptr);
 }
 
 // After the last sweep M = -eps^-1; Wc = eps^-1 - I = -M - I.  A frequency
@@ -439,7 +473,7 @@ static_assert(kSweepPanelCols == SWEEP_NB, "panel width");
 __global__ void k_gsweep_diag(const GMat* __restrict__ mats, int k0, double* __restrict__ Dp,
                               int* __restrict__ status);
 __global__ void k_gsweep_tpanel(const GMat* __restrict__ mats, const int* __restrict__ pre, int count, int k0,
-                                const double* __restrict__ Dp, double* __restrict__ Tcat);
+                                const double* __restrict__ Dp, double* __restrict__ Tcat, unsigned long long* amax);
 __global__ void k_gsweep_update(const GMat* __restrict__ mats, const int* __restrict__ pre, int count, int k0,
                                 const double* __restrict__ Tcat, const double* __restrict__ Pcat);
 
@@ -459,16 +493,22 @@ static void sweep_attributes_once() {
 }
 
 // One block step of the sweep on stream st: D, T, then P and the panel write.
+// amax_t / amax_p (optional): [nw] words that receive max|T|, max|P| per
+// matrix (zeroed here first) for the split of the trailing update.
 static void sweep_front(qx_ctx* ctx, cudaStream_t st, double* eps, int n, int ldn, size_t stride, int nw, int k0,
-                        int kb, double* Tp, double* Dp, double* Pp, size_t pstride, int* status) {
+                        int kb, double* Tp, double* Dp, double* Pp, size_t pstride, int* status,
+                        unsigned long long* amax_t = nullptr, unsigned long long* amax_p = nullptr) {
+  if (amax_t) QX_CUDA(cudaMemsetAsync(amax_t, 0, nw * sizeof(unsigned long long), st));
+  if (amax_p) QX_CUDA(cudaMemsetAsync(amax_p, 0, nw * sizeof(unsigned long long), st));
   const int diag_smem = (SWEEP_NB * SWEEP_NB + SWEEP_NB * 33) * sizeof(double);
   k_sweep_diag<<<nw, 512, diag_smem, st>>>(eps, ldn, stride, k0, kb, Dp, status);
   check_launch(ctx);
   dim3 tg(ceil_div(n, PanelTile::BM), ceil_div(kb, PanelTile::BN), nw);
-  k_sweep_tpanel<<<tg, PanelTile::THREADS, PanelTile::SMEM, st>>>(eps, n, ldn, stride, k0, kb, Dp, Tp, pstride);
+  k_sweep_tpanel<<<tg, PanelTile::THREADS, PanelTile::SMEM, st>>>(eps, n, ldn, stride, k0, kb, Dp, Tp, pstride,
+                                                                   amax_t);
   check_launch(ctx);
   dim3 wg(ceil_div(n, kWriteRows), nw);
-  k_sweep_write<<<wg, 256, 0, st>>>(eps, n, ldn, stride, k0, kb, Tp, Pp, pstride, Dp);
+  k_sweep_write<<<wg, 256, 0, st>>>(eps, n, ldn, stride, k0, kb, Tp, Pp, pstride, Dp, amax_p);
   check_launch(ctx);
 }
 
@@ -535,7 +575,8 @@ void launch_invert_wc(qx_ctx* ctx, double* eps, int n, int ldn, size_t stride, i
     for (int step = 0; step < nsteps; ++step) {
       const int k0 = step * SWEEP_NB, kb = min(SWEEP_NB, n - k0);
       const int b = step & 1;
-      sweep_front(ctx, s0, eps, n, ldn, stride, nw, k0, kb, Tb[b], Db[b], Pb[b], pstride, status);
+      sweep_front(ctx, s0, eps, n, ldn, stride, nw, k0, kb, Tb[b], Db[b], Pb[b], pstride, status,
+                  tc ? split_amax_words(ctx, 3 + 2 * b) : nullptr, tc ? split_amax_words(ctx, 4 + 2 * b) : nullptr);
       SweepSplit sp{};
       if (tc) sp = launch_sweep_split(ctx, s0, Tb[b], Pb[b], n, kb, nw, b, split_base);
       // The previous step's trailing update must be done before this step's
@@ -613,22 +654,24 @@ __global__ void __launch_bounds__(512) k_gsweep_diag(const GMat* __restrict__ ma
 __global__ void __launch_bounds__(PanelTile::THREADS) k_gsweep_tpanel(const GMat* __restrict__ mats,
                                                                       const int* __restrict__ pre, int count, int k0,
                                                                       const double* __restrict__ Dp,
-                                                                      double* __restrict__ Tcat) {
+                                                                      double* __restrict__ Tcat,
+                                                                      unsigned long long* amax) {
   const int g = group_of(pre, count, blockIdx.x);
   const int t = blockIdx.x - pre[g];
   const GMat m = mats[g];
   sweep_tpanel_body(m.M, m.n, m.ldn, k0, min(SWEEP_NB, m.n - k0), Dp + (size_t)g * SWEEP_NB * SWEEP_NB,
-                    Tcat + (size_t)m.prow * SWEEP_NB, (t >> 1) * PanelTile::BM, (t & 1) * PanelTile::BN);
+                    Tcat + (size_t)m.prow * SWEEP_NB, (t >> 1) * PanelTile::BM, (t & 1) * PanelTile::BN, amax);
 }
 
 __global__ void __launch_bounds__(256) k_gsweep_write(const GMat* __restrict__ mats, const int* __restrict__ pre,
                                                       int count, int k0, const double* __restrict__ Tcat,
-                                                      double* __restrict__ Pcat, const double* __restrict__ Dp) {
+                                                      double* __restrict__ Pcat, const double* __restrict__ Dp,
+                                                      unsigned long long* amax) {
   const int g = group_of(pre, count, blockIdx.x);
   const GMat m = mats[g];
   sweep_write_tile(m.M, m.n, m.ldn, k0, min(SWEEP_NB, m.n - k0), Tcat + (size_t)m.prow * SWEEP_NB,
                    Pcat + (size_t)m.prow * SWEEP_NB, Dp + (size_t)g * SWEEP_NB * SWEEP_NB,
-                   (blockIdx.x - pre[g]) * kWriteRows);
+                   (blockIdx.x - pre[g]) * kWriteRows, amax);
 }
 
 __global__ void __launch_bounds__(SweepTile::THREADS) k_gsweep_update(const GMat* __restrict__ mats,
@@ -748,17 +791,26 @@ void launch_invert_wc_group(qx_ctx* ctx, const GMat* mats_in, int G, int half_lo
     const int k0 = s * SWEEP_NB, a = act[s];
     k_gsweep_diag<<<a, 512, diag_smem, ctx->stream>>>(d_mats, k0, Dp, status);
     check_launch(ctx);
+    // Split form: the panel and write kernels accumulate max|T|, max|P| over
+    // all matrices (one scale each) for the splits.
+    unsigned long long* amax_t = tc ? split_amax_words(ctx, 3) : nullptr;
+    unsigned long long* amax_p = tc ? split_amax_words(ctx, 4) : nullptr;
+    if (tc) {
+      QX_CUDA(cudaMemsetAsync(amax_t, 0, sizeof(unsigned long long), ctx->stream));
+      QX_CUDA(cudaMemsetAsync(amax_p, 0, sizeof(unsigned long long), ctx->stream));
+    }
     k_gsweep_tpanel<<<tab[off_tp[s] + a], PanelTile::THREADS, PanelTile::SMEM, ctx->stream>>>(
-        d_mats, d_tab + off_tp[s], a, k0, Dp, Tcat);
+        d_mats, d_tab + off_tp[s], a, k0, Dp, Tcat, amax_t);
     check_launch(ctx);
-    k_gsweep_write<<<tab[off_wr[s] + a], 256, 0, ctx->stream>>>(d_mats, d_tab + off_wr[s], a, k0, Tcat, Pcat, Dp);
+    k_gsweep_write<<<tab[off_wr[s] + a], 256, 0, ctx->stream>>>(d_mats, d_tab + off_wr[s], a, k0, Tcat, Pcat, Dp,
+                                                                amax_p);
     check_launch(ctx);
     if (tc) {
       uint8_t* b = static_cast<uint8_t*>(split_base);
       TcOperand T{b, b + pan * 2, nullptr}, P{b + pan * 4, b + pan * 6, nullptr};
       const int rows = rows_act[s];
-      launch_split(ctx, Tcat, rows, SWEEP_NB, SWEEP_NB, T.hi, T.lo, SWEEP_NB, 0, 0, 1, 1, 3, &T.scale);
-      launch_split(ctx, Pcat, rows, SWEEP_NB, SWEEP_NB, P.hi, P.lo, SWEEP_NB, 0, 0, 1, 1, 4, &P.scale);
+      launch_split(ctx, Tcat, rows, SWEEP_NB, SWEEP_NB, T.hi, T.lo, SWEEP_NB, 0, 0, 1, 1, 3, &T.scale, amax_t);
+      launch_split(ctx, Pcat, rows, SWEEP_NB, SWEEP_NB, P.hi, P.lo, SWEEP_NB, 0, 0, 1, 1, 4, &P.scale, amax_p);
       launch_gsweep_update_tc(ctx, d_mats, d_tab + off_up[s], a, tab[off_up[s] + a], s, T, P, rows, tc_err + s);
     } else {
       k_gsweep_update<<<tab[off_up[s] + a], SweepTile::THREADS, SweepTile::SMEM, ctx->stream>>>(

@@ -140,7 +140,9 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
 // ---------------------------------------------------------------------------
 // The GEMM kernel.
 // ---------------------------------------------------------------------------
-enum { EPI_ROWDOT = 0, EPI_STORE = 1 };
+// EPI_UPDATE is the STORE epilogue in its subtract form (the sweep's trailing
+// update), instantiated apart so that profiles tell it from P0.
+enum { EPI_ROWDOT = 0, EPI_STORE = 1, EPI_UPDATE = 2 };
 
 constexpr int TC_BM = 128;
 // Pipeline shape per epilogue: 64-wide K blocks (the unit of the STORE
@@ -305,7 +307,7 @@ __global__ void __launch_bounds__(TcWarps<EPI>::THREADS, 1)
     }
     nt_end = nt_begin + 1;
   }
-  if (EPI == EPI_STORE && args.subtract) {
+  if (EPI != EPI_ROWDOT && args.subtract) {
     // Whole-CTA exit before any barrier or TMEM allocation.
     if (mb == args.skip_tile || nt_begin == args.skip_tile) return;
     if (args.filter_mode) {
@@ -316,7 +318,7 @@ __global__ void __launch_bounds__(TcWarps<EPI>::THREADS, 1)
   const bool active = (w < args.nbatch);
   const int m0 = mb * TC_BM;
   // STORE output shape and the panel row offsets of a grouped matrix.
-  const bool grouped = (EPI == EPI_STORE) && args.gmats != nullptr;
+  const bool grouped = (EPI != EPI_ROWDOT) && args.gmats != nullptr;
   const int outM = grouped ? gmat.n : args.M, outN = grouped ? gmat.n : args.N;
   const int out_ld = grouped ? gmat.ldn : args.ldo;
   const size_t out_stride = grouped ? 0 : args.out_stride;
@@ -400,8 +402,8 @@ __global__ void __launch_bounds__(TcWarps<EPI>::THREADS, 1)
           const int kbe = args.tri ? min(k_blocks, (nt * BN + BN + TC_BK - 1) / TC_BK) : k_blocks;
           for (int kb = 0; kb < kbe; ++kb, ++g) {
             const int unit = args.unit > 0 ? args.unit : 1;
-            const bool unit_start = (EPI == EPI_STORE) ? (kb % unit == 0) : kb == 0;
-            const bool unit_end = (EPI == EPI_STORE) ? (kb % unit == unit - 1 || kb == kbe - 1) : kb == kbe - 1;
+            const bool unit_start = (EPI != EPI_ROWDOT) ? (kb % unit == 0) : kb == 0;
+            const bool unit_end = (EPI != EPI_ROWDOT) ? (kb % unit == unit - 1 || kb == kbe - 1) : kb == kbe - 1;
             const int buf = u & 1;
             if (unit_start && u >= 2) {
               if (!mbar_wait(&acc_empty[buf], ((u / 2) - 1) & 1, abort_flag, args.err, 2)) {
@@ -519,7 +521,79 @@ __global__ void __launch_bounds__(TcWarps<EPI>::THREADS, 1)
         __syncwarp();
         if (lane == 0) mbar_arrive(&acc_empty[buf]);
       }
-      if (ok && m < outM) {
+      if (EPI == EPI_UPDATE) {
+        // One FP32 accumulation unit covers K here (the launchers ask for
+        // it), so the tile C is exactly FP32.  It is staged in the drained
+        // stage buffers, then the lower tile and its mirror are updated in
+        // row-wise passes that are coalesced along the rows of M; the mirror
+        // reads its old value from the upper element itself, M being stored
+        // exactly symmetric.  Every epilogue thread reaches the barrier; after
+        // an abort nothing is written.
+        constexpr int CLD = BN + 1;
+        static_assert(TC_BM * CLD * 4 <= TC_STAGES * L::STAGE_BYTES, "staged tile fits the stage buffers");
+        float* Cs = reinterpret_cast<float*>(smem);
+        const int rl = quarter * 32 + lane;
+#pragma unroll
+        for (int c = 0; c < CPW; ++c) Cs[rl * CLD + CPW * part + c] = (float)acc[c];
+        asm volatile("bar.sync 1, 256;\n" ::: "memory");
+        if (!*abort_flag) {
+          // Warp e takes rows e, e + 8, ... of each pass, four at a time, and
+          // issues all 16 loads of a lane before its stores (enough bytes in
+          // flight per SM for HBM).
+          const int e = warp - 2;
+          const int nb = nt_begin * BN;
+          double* outw = out_base + (size_t)w * out_stride;
+          static_assert(EPI != EPI_UPDATE || (TC_BM == 128 && BN == 128), "row passes assume 128 x 128 tiles");
+          // Lower tile: row mm = m0 + r, columns n = nb + lane + 32 q, n <= mm.
+#pragma unroll 1
+          for (int r0 = e; r0 < TC_BM; r0 += 32) {
+            double x[4][4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+              const int mm = m0 + r0 + 8 * k;
+#pragma unroll
+              for (int q = 0; q < 4; ++q) {
+                const int n = nb + lane + 32 * q;
+                x[k][q] = (mm < outM && n < outN && n <= mm) ? outw[(size_t)mm * out_ld + n] : 0.0;
+              }
+            }
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+              const int r = r0 + 8 * k, mm = m0 + r;
+#pragma unroll
+              for (int q = 0; q < 4; ++q) {
+                const int cc = lane + 32 * q, n = nb + cc;
+                if (mm < outM && n < outN && n <= mm)
+                  outw[(size_t)mm * out_ld + n] = x[k][q] - (double)Cs[r * CLD + cc] * unscale;
+              }
+            }
+          }
+          // Mirror: row n = nb + cc, columns mm = m0 + lane + 32 q, n < mm.
+#pragma unroll 1
+          for (int c0 = e; c0 < BN; c0 += 32) {
+            double x[4][4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+              const int n = nb + c0 + 8 * k;
+#pragma unroll
+              for (int q = 0; q < 4; ++q) {
+                const int mm = m0 + lane + 32 * q;
+                x[k][q] = (mm < outM && n < outN && n < mm) ? outw[(size_t)n * out_ld + mm] : 0.0;
+              }
+            }
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+              const int cc = c0 + 8 * k, n = nb + cc;
+#pragma unroll
+              for (int q = 0; q < 4; ++q) {
+                const int r = lane + 32 * q, mm = m0 + r;
+                if (mm < outM && n < outN && n < mm)
+                  outw[(size_t)n * out_ld + mm] = x[k][q] - (double)Cs[r * CLD + cc] * unscale;
+              }
+            }
+          }
+        }
+      } else if (ok && m < outM) {
         const int n0 = nt_begin * BN + CPW * part;
         double* orow = out_base + (size_t)w * out_stride + (size_t)m * out_ld;
 #pragma unroll
@@ -831,17 +905,20 @@ static SplitScratch split_scratch(qx_ctx* ctx, int slot_offset) {
 
 static void split(qx_ctx* ctx, const double* src, int rows, int cols, int ld_src, size_t src_stride, void* hi,
                   void* lo, int ld_dst, size_t dst_stride, int batch, const double* colscale, int ld_cs, int fp16,
-                  int slot, float** scale_out, int reuse_src_amax_slot = -1, cudaStream_t stream = nullptr) {
+                  int slot, float** scale_out, const unsigned long long* given_amax = nullptr,
+                  cudaStream_t stream = nullptr) {
   QX_REQUIRE(batch <= 1024, QX_ERR_INVALID_INPUT, "at most 1024 frequencies per split");
   SplitScratch sc = split_scratch(ctx, slot);
   cudaStream_t st = stream ? stream : ctx->stream;
   if (fp16) {
     const int nsrc = src_stride ? batch : 1;
-    QX_CUDA(cudaMemsetAsync(sc.amax_src, 0, 2048 * sizeof(unsigned long long), st));
-    if (reuse_src_amax_slot >= 0) {
-      // The same source was split just before in that slot: take its bound.
-      sc.amax_src = split_scratch(ctx, reuse_src_amax_slot).amax_src;
+    if (given_amax) {
+      // The source's bound is already on the device (the same source split
+      // before, or accumulated by the kernel that wrote it).
+      sc.amax_src = const_cast<unsigned long long*>(given_amax);
+      if (colscale) QX_CUDA(cudaMemsetAsync(sc.amax_col, 0, 1024 * sizeof(unsigned long long), st));
     } else {
+      QX_CUDA(cudaMemsetAsync(sc.amax_src, 0, 2048 * sizeof(unsigned long long), st));
       // About eight blocks per SM over all batches, each thread four
       // elements per step at least.
       const size_t tot = (size_t)rows * cols;
@@ -891,10 +968,13 @@ static void split(qx_ctx* ctx, const double* src, int rows, int cols, int ld_src
 }
 
 void launch_split(qx_ctx* ctx, const double* src, int rows, int cols, int ld_src, void* hi, void* lo, int ld_dst,
-                  size_t src_stride, size_t dst_stride, int batch, int fp16, int slot, float** scale_out) {
+                  size_t src_stride, size_t dst_stride, int batch, int fp16, int slot, float** scale_out,
+                  const unsigned long long* given_amax) {
   split(ctx, src, rows, cols, ld_src, src_stride, hi, lo, ld_dst, dst_stride, batch, nullptr, 0, fp16, slot,
-        scale_out);
+        scale_out, given_amax);
 }
+
+unsigned long long* split_amax_words(qx_ctx* ctx, int slot) { return split_scratch(ctx, slot).amax_src; }
 
 // One error word per launch, from the context's status arena.
 static int* tc_err_slot(qx_ctx* ctx) { return status_words(ctx, 1); }
@@ -1019,7 +1099,8 @@ void launch_eps_tc(qx_ctx* ctx, const double* bov, int ldov, int naux, int nov, 
     sa = split_scratch(ctx, 7).scale;
   else
     split(ctx, bov, naux, nov, ldov, 0, a_hi, a_lo, ldov, 0, 1, nullptr, 0, fp16, 7, &sa);
-  split(ctx, bov, naux, nov, ldov, 0, b_hi, b_lo, ldov, a_elems, nw, chi, ldov, fp16, 1, &sb, /*amax of bov*/ 7);
+  split(ctx, bov, naux, nov, ldov, 0, b_hi, b_lo, ldov, a_elems, nw, chi, ldov, fp16, 1, &sb,
+        /*the bound of bov*/ split_scratch(ctx, 7).amax_src);
   constexpr int BK = TcPipe<EPI_STORE>::BK;
   CUtensorMap ah = make_map(a_hi, nov, naux, ldov, 1, TC_BM, 2, fp16, BK);
   CUtensorMap al = make_map(a_lo, nov, naux, ldov, 1, TC_BM, 2, fp16, BK);
@@ -1096,10 +1177,11 @@ SweepSplit launch_sweep_split(qx_ctx* ctx, cudaStream_t st, const double* Tp, co
   sp.T.lo = b + elems * 2;
   sp.P.hi = b + elems * 4;
   sp.P.lo = b + elems * 6;
+  // The bounds of T and P were accumulated by the panel and write kernels.
   split(ctx, Tp, n, kb, kSweepPanelCols, ps, sp.T.hi, sp.T.lo, kSweepPanelCols, ps, nw, nullptr, 0, 1, 3 + 2 * buf,
-        &sp.T.scale, -1, st);
+        &sp.T.scale, split_amax_words(ctx, 3 + 2 * buf), st);
   split(ctx, Pp, n, kb, kSweepPanelCols, ps, sp.P.hi, sp.P.lo, kSweepPanelCols, ps, nw, nullptr, 0, 1, 4 + 2 * buf,
-        &sp.P.scale, -1, st);
+        &sp.P.scale, split_amax_words(ctx, 4 + 2 * buf), st);
   return sp;
 }
 
@@ -1138,8 +1220,9 @@ void launch_sweep_update_tc(qx_ctx* ctx, cudaStream_t st, double* eps, int n, in
   a.filter_mode = mode;
   a.filter_tile = next_blk;
   const int tiles = ceil_div(n, TC_BM);
+  static_assert(kSweepPanelCols <= kP0Unit * TcPipe<EPI_UPDATE>::BK, "one accumulation unit covers the panel");
   QX_REQUIRE(nw <= 65535, QX_ERR_INVALID_INPUT, "at most 65535 matrices per sweep");
-  launch_tc<BN, EPI_STORE>(ctx, ah, al, bh, bl, a, dim3(tiles * (tiles + 1) / 2, nw), st);
+  launch_tc<BN, EPI_UPDATE>(ctx, ah, al, bh, bl, a, dim3(tiles * (tiles + 1) / 2, nw), st);
 }
 
 void launch_gsweep_update_tc(qx_ctx* ctx, const GMat* d_mats, const int* d_pre, int count, int ntiles, int step,
@@ -1165,7 +1248,7 @@ void launch_gsweep_update_tc(qx_ctx* ctx, const GMat* d_mats, const int* d_pre, 
   a.gmats = d_mats;
   a.gpre = d_pre;
   a.gcount = count;
-  launch_tc<BN, EPI_STORE>(ctx, ah, al, bh, bl, a, dim3(ntiles, 1));
+  launch_tc<BN, EPI_UPDATE>(ctx, ah, al, bh, bl, a, dim3(ntiles, 1));
 }
 
 }  // namespace qx

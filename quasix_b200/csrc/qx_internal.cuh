@@ -307,8 +307,14 @@ struct TcOperand {
 inline bool is_tc_precision(int p) { return p == QX_PREC_BF16X3 || p == QX_PREC_FP16X3; }
 // slot selects one of the scratch areas for the scales (0..2; 3..6 belong to
 // the sweep, 7 to the B_ov split of P0).
+// given_amax: the bounds max|src| per batch ([batch] words, a double's bits)
+// are already on the device; no amax pass.
 void launch_split(qx_ctx* ctx, const double* src, int rows, int cols, int ld_src, void* hi, void* lo, int ld_dst,
-                  size_t src_stride, size_t dst_stride, int batch, int fp16, int slot, float** scale_out);
+                  size_t src_stride, size_t dst_stride, int batch, int fp16, int slot, float** scale_out,
+                  const unsigned long long* given_amax = nullptr);
+// The amax words of split slot `slot` (1024, for kernels that accumulate a
+// bound before the split).
+unsigned long long* split_amax_words(qx_ctx* ctx, int slot);
 // reuse_a: B_ov is the one split by the previous call on this context; its
 // hi/lo split is reused (unless the operand buffer has to grow).
 void launch_eps_tc(qx_ctx* ctx, const double* bov, int ldov, int naux, int nov, const double* chi, int nw,
@@ -320,9 +326,10 @@ void launch_pair_contract_tc(qx_ctx* ctx, const TcOperand& A, const float* bpt_f
 bool tc_supported(qx_ctx* ctx);
 
 // Block sweep in the FP16X3 form: split the step's panels (buffer half buf of
-// base, 2 * 4 * nw * n * 128 * 2 bytes in all), then the tcgen05 trailing
-// update on stream st (mode / next_blk as k_sweep_update; err: one zeroed
-// status word).
+// base, 2 * 4 * nw * n * 128 * 2 bytes in all; the bounds max|T|, max|P| per
+// matrix must be in the amax words of split slots 3 + 2 buf and 4 + 2 buf),
+// then the tcgen05 trailing update on stream st (mode / next_blk as
+// k_sweep_update; err: one zeroed status word).
 struct SweepSplit {
   TcOperand T, P;
 };
