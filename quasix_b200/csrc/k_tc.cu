@@ -537,19 +537,20 @@ __global__ void __launch_bounds__(TcWarps<EPI>::THREADS, 1)
         for (int c = 0; c < CPW; ++c) Cs[rl * CLD + CPW * part + c] = (float)acc[c];
         asm volatile("bar.sync 1, 256;\n" ::: "memory");
         if (!*abort_flag) {
-          // Warp e takes rows e, e + 8, ... of each pass, four at a time, and
-          // issues all 16 loads of a lane before its stores (enough bytes in
-          // flight per SM for HBM).
+          // Warp e takes rows e, e + 8, ... of each pass, RB = 8 at a time, and
+          // issues all 32 loads of a lane before its stores, so that enough
+          // bytes are in flight per SM for HBM (4 and 16 rows measured slower).
+          constexpr int RB = 8;
           const int e = warp - 2;
           const int nb = nt_begin * BN;
           double* outw = out_base + (size_t)w * out_stride;
           static_assert(EPI != EPI_UPDATE || (TC_BM == 128 && BN == 128), "row passes assume 128 x 128 tiles");
           // Lower tile: row mm = m0 + r, columns n = nb + lane + 32 q, n <= mm.
 #pragma unroll 1
-          for (int r0 = e; r0 < TC_BM; r0 += 32) {
-            double x[4][4];
+          for (int r0 = e; r0 < TC_BM; r0 += 8 * RB) {
+            double x[RB][4];
 #pragma unroll
-            for (int k = 0; k < 4; ++k) {
+            for (int k = 0; k < RB; ++k) {
               const int mm = m0 + r0 + 8 * k;
 #pragma unroll
               for (int q = 0; q < 4; ++q) {
@@ -558,7 +559,7 @@ __global__ void __launch_bounds__(TcWarps<EPI>::THREADS, 1)
               }
             }
 #pragma unroll
-            for (int k = 0; k < 4; ++k) {
+            for (int k = 0; k < RB; ++k) {
               const int r = r0 + 8 * k, mm = m0 + r;
 #pragma unroll
               for (int q = 0; q < 4; ++q) {
@@ -570,10 +571,10 @@ __global__ void __launch_bounds__(TcWarps<EPI>::THREADS, 1)
           }
           // Mirror: row n = nb + cc, columns mm = m0 + lane + 32 q, n < mm.
 #pragma unroll 1
-          for (int c0 = e; c0 < BN; c0 += 32) {
-            double x[4][4];
+          for (int c0 = e; c0 < BN; c0 += 8 * RB) {
+            double x[RB][4];
 #pragma unroll
-            for (int k = 0; k < 4; ++k) {
+            for (int k = 0; k < RB; ++k) {
               const int n = nb + c0 + 8 * k;
 #pragma unroll
               for (int q = 0; q < 4; ++q) {
@@ -582,7 +583,7 @@ __global__ void __launch_bounds__(TcWarps<EPI>::THREADS, 1)
               }
             }
 #pragma unroll
-            for (int k = 0; k < 4; ++k) {
+            for (int k = 0; k < RB; ++k) {
               const int cc = c0 + 8 * k, n = nb + cc;
 #pragma unroll
               for (int q = 0; q < 4; ++q) {
