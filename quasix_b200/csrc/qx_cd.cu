@@ -303,6 +303,12 @@ void CdEngine::evaluate_begin(const std::vector<int>& act, std::vector<GMat>* gr
   ev_res = residues(act);
   const int R = (int)ev_res.size();
   ev_grouped = false;
+  // eps(w) = I + B diag(chi'(w)) B^T with chi'_ia(w) = -4 e_ia / (e_ia^2 - w^2)
+  // is SPD when every shift is below the smallest transition |e_ia| (chi' >
+  // 0); with a 0.9 margin its eigenvalues lie in [1, 1 + ||Pi(0)|| / 0.19].
+  double wmax = 0.0;
+  for (const CdResidue& r : ev_res) wmax = std::max(wmax, std::fabs(r.w));
+  ev_spd = wmax < 0.9 * (e[nocc] - e[nocc - 1]);
   if (R == 0) return;
   ev_chunk = residue_buffers(R);
   CdResidueChunk& c = ev_chunk;
@@ -609,7 +615,11 @@ static void cd_batch_grouped(qx_ctx* ctx, qx_cd_system* systems, int nsys, int n
               live.push_back(j);
             });
         if (live.empty()) break;
-        grouped_inversion(live, mats, /*half_lower=*/0, /*split_update=*/0);
+        // The split trailing update needs SPD matrices: all residue eps of
+        // the wave below the smallest transition of their system.
+        bool spd = tc;
+        for (int j : live) spd = spd && runs[j].E.ev_spd;
+        grouped_inversion(live, mats, /*half_lower=*/0, /*split_update=*/spd);
         for (int j : live)
           if (ok[j]) guarded(j, [&] { runs[j].E.evaluate_post(); });
         for (int j : live)

@@ -82,6 +82,7 @@ struct CdEngine {
   std::vector<double> ev_hi, ev_rv, ev_rd;
   CdResidueChunk ev_chunk{};
   bool ev_grouped = false;
+  bool ev_spd = false;  // every residue eps of this evaluation is SPD (see evaluate_begin)
   // Pinned staging in ctx->host_stage (reserved by setup_begin); sx is
   // filled from h_sx at the first evaluation's synchronisation.
   double *h_sx = nullptr, *h_hi = nullptr, *h_rv = nullptr, *h_rd = nullptr;
