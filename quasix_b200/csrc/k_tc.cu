@@ -160,11 +160,15 @@ struct TcPipe {
 // much as the MMAs of one 64-wide k-block, so a drain per block left P0
 // drain-bound: at nmo 300 / naux 1000 / nw 32, P0 took 2.29 ms per evGW
 // iteration with unit 1, 1.93 ms with unit 2 and 1.72 ms with unit 4, at QP
-// errors against FP64 of 0.024, 0.036 and 0.068 meV.  P0 and the sweep use
-// unit 2; the BSE direct term keeps unit 1, since with unit 2 the Davidson
-// residuals of the 26 400-dimensional problem stalled above 1e-8.  A third
-// stage measured no faster.
+// errors against FP64 of 0.024, 0.036 and 0.068 meV.  Once the chi-scaled
+// operand was split in one pass for all frequencies, unit 4 no longer beat
+// unit 2 (1.86 vs 1.89 ms) and doubled the error, so P0 uses unit 2; the
+// sweep's update uses unit 2 too (one unit covers its K of 128); the BSE
+// direct term keeps unit 1, since with unit 2 the Davidson residuals of the
+// 26 400-dimensional problem stalled above 1e-8.  A third stage measured no
+// faster.
 constexpr int kP0Unit = 2;
+constexpr int kUpdateUnit = 2;
 // Epilogue warps: 8, two per TMEM lane quarter (ROWDOT: half an N tile each;
 // STORE: 64 columns each).  For STORE, 16 warps of 32 columns (FP64 or
 // Kahan-compensated FP32 drain) measured no faster for P0 and slower for the
@@ -1212,7 +1216,7 @@ void launch_sweep_update_tc(qx_ctx* ctx, cudaStream_t st, double* eps, int n, in
   a.lower_tiles = 1;
   a.subtract = 1;
   a.a_batched = 1;
-  a.unit = kP0Unit;
+  a.unit = kUpdateUnit;
   a.fp16 = 1;
   a.scaleA = sp.T.scale;
   a.scaleB = sp.P.scale;
@@ -1221,7 +1225,7 @@ void launch_sweep_update_tc(qx_ctx* ctx, cudaStream_t st, double* eps, int n, in
   a.filter_mode = mode;
   a.filter_tile = next_blk;
   const int tiles = ceil_div(n, TC_BM);
-  static_assert(kSweepPanelCols <= kP0Unit * TcPipe<EPI_UPDATE>::BK, "one accumulation unit covers the panel");
+  static_assert(kSweepPanelCols <= kUpdateUnit * TcPipe<EPI_UPDATE>::BK, "one accumulation unit covers the panel");
   QX_REQUIRE(nw <= 65535, QX_ERR_INVALID_INPUT, "at most 65535 matrices per sweep");
   launch_tc<BN, EPI_UPDATE>(ctx, ah, al, bh, bl, a, dim3(tiles * (tiles + 1) / 2, nw), st);
 }
@@ -1241,7 +1245,7 @@ void launch_gsweep_update_tc(qx_ctx* ctx, const GMat* d_mats, const int* d_pre, 
   a.lower_tiles = 1;
   a.subtract = 1;
   a.fp16 = 1;
-  a.unit = kP0Unit;
+  a.unit = kUpdateUnit;
   a.scaleA = T.scale;
   a.scaleB = P.scale;
   a.err = err;
