@@ -191,8 +191,9 @@ def contraction_mma_flops(nmo, naux, nw):
 
 
 # DRAM bytes (read + write) of one pair-contraction launch at nmo 300 / naux 1000 /
-# nw 32, from one ncu capture (profiles/k_tc_gemm_evgw_nmo300.md).
-CONTRACTION_DRAM_BYTES = 1.564282e9 + 0.034871e9
+# nw 32, from one ncu capture of the bench's own command (dram__bytes_read.sum +
+# dram__bytes_write.sum of the launch the bench keeps).
+CONTRACTION_DRAM_BYTES = 1.563380e9 + 0.015538e9
 
 
 def iteration_flops(nocc, nvir, naux, nw):
