@@ -145,15 +145,18 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
 enum { EPI_ROWDOT = 0, EPI_STORE = 1, EPI_UPDATE = 2 };
 
 constexpr int TC_BM = 128;
-// Pipeline shape per epilogue: 64-wide K blocks (the unit of the STORE
-// kernels' FP64 drain) in 2 stages.  32-wide blocks in 4 stages (the same
-// shared memory, more TMA requests in flight) measured slower for the pair
-// contraction (7.8 vs 6.1 ms at nmo 300 / naux 1000 / nw 32).
+// Pipeline shape per epilogue: 64-wide K blocks in 2 stages.  32-wide blocks
+// in 4 stages (the same shared memory, more TMA requests in flight) measured
+// slower for the pair contraction (7.8 vs 6.1 ms at nmo 300 / naux 1000 /
+// nw 32); for P0, 3 stages of 64 gave 1.87 vs 1.91 ms and 6 stages of 32 were
+// slower: its limit is the operand traffic from shared memory of the
+// 128-wide tile, not the pipeline depth.
 template <int EPI>
 struct TcPipe {
   static constexpr int BK = 64;
   static constexpr int STAGES = 2;
 };
+
 // STORE (the FP64-output GEMMs: P0, the sweep update, the BSE direct term):
 // the accumulator restarts every TcArgs::unit k-blocks and the epilogue sums
 // the units in FP64.  The FP32 -> FP64 conversions of one drain cost about as
@@ -167,7 +170,8 @@ struct TcPipe {
 // direct term keeps unit 1, since with unit 2 the Davidson residuals of the
 // 26 400-dimensional problem stalled above 1e-8.  A third stage measured no
 // faster.
-constexpr int kP0Unit = 2;
+constexpr int kP0Unit = 128 / TcPipe<EPI_STORE>::BK;
+constexpr int kBseUnit = 64 / TcPipe<EPI_STORE>::BK;
 constexpr int kUpdateUnit = 2;
 // Epilogue warps: 8, two per TMEM lane quarter (ROWDOT: half an N tile each;
 // STORE: 64 columns each).  For STORE, 16 warps of 32 columns (FP64 or
@@ -1161,6 +1165,7 @@ void launch_gemm_tc(qx_ctx* ctx, const TcOperand& A, int M, int lda, const TcOpe
   a.fp16 = fp16;
   a.scaleA = A.scale;
   a.scaleB = B.scale;
+  a.unit = kBseUnit;
   a.err = d_err;
   QX_REQUIRE(nbatch <= 65535, QX_ERR_INVALID_INPUT, "at most 65535 batches");
   launch_tc<BN, EPI_STORE>(ctx, ah, al, bh, bl, a, dim3(a.m_blocks * ceil_div(N, BN), nbatch));
@@ -1198,7 +1203,7 @@ void launch_sweep_update_tc(qx_ctx* ctx, cudaStream_t st, double* eps, int n, in
                             int kblk, const SweepSplit& sp, int mode, int next_blk, int* err) {
   static_assert(kSweepPanelCols == TC_BM, "sweep block = tcgen05 tile");
   constexpr int BN = 128;
-  constexpr int BK = TcPipe<EPI_STORE>::BK;
+  constexpr int BK = TcPipe<EPI_UPDATE>::BK;
   const int K = kSweepPanelCols;
   CUtensorMap ah = make_map(sp.T.hi, K, n, K, nw, TC_BM, 3, 1, BK);
   CUtensorMap al = make_map(sp.T.lo, K, n, K, nw, TC_BM, 3, 1, BK);
@@ -1233,7 +1238,7 @@ void launch_sweep_update_tc(qx_ctx* ctx, cudaStream_t st, double* eps, int n, in
 void launch_gsweep_update_tc(qx_ctx* ctx, const GMat* d_mats, const int* d_pre, int count, int ntiles, int step,
                              const TcOperand& T, const TcOperand& P, int rows, int* err) {
   constexpr int BN = 128;
-  constexpr int BK = TcPipe<EPI_STORE>::BK;
+  constexpr int BK = TcPipe<EPI_UPDATE>::BK;
   const int K = kSweepPanelCols;
   CUtensorMap ah = make_map(T.hi, K, rows, K, 1, TC_BM, 2, 1, BK);
   CUtensorMap al = make_map(T.lo, K, rows, K, 1, TC_BM, 2, 1, BK);
