@@ -520,6 +520,9 @@ __global__ void __launch_bounds__(TcWarps<EPI>::THREADS, 1)
         const uint32_t taddr = tmem_base + ((uint32_t)(quarter * 32) << 16) + buf * BN + CPW * part;
 #pragma unroll
         for (int j = 0; j < CPW / 16; ++j) {
+          // Columns past N (a narrow GEMM, e.g. a few vectors) are not
+          // drained; the condition is warp-uniform.
+          if (nt_begin * BN + CPW * part + 16 * j >= outN) continue;
           float v[16];
           tmem_ld16(taddr + 16 * j, v);
 #pragma unroll

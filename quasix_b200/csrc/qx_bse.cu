@@ -3,7 +3,11 @@
 // Davidson of davidson_bse (quasix_core/src/bse/davidson.rs:372-508) with the
 // subspace, Rayleigh-Ritz (parallel Jacobi) and re-orthonormalisation on the
 // device; the host only steers (convergence flags, subspace size).
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
 #include <algorithm>
+#include <cmath>
 #include <numeric>
 
 #include "qx_blas.cuh"
@@ -159,6 +163,52 @@ __global__ void k_rowdot(const double* __restrict__ U, const double* __restrict_
 
 using namespace qx;
 
+// max|x| over n doubles (a double's bits; x >= 0 compares as its pattern).
+__global__ void k_absmax(const double* __restrict__ x, size_t n, unsigned long long* __restrict__ out) {
+  double m = 0.0;
+  for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x)
+    m = fmax(m, fabs(x[k]));
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  __shared__ double red[32];
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    m = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if (threadIdx.x == 0) atomicMax(out, __double_as_longlong(m));
+  }
+}
+
+// Row (i,a) of the direct kernel K^d[(i,a)][(j,b)] = C[(i,j)][(a,b)], scaled
+// by s and split into hi/lo (fp16 or bf16, the rounding of the other splits),
+// row stride ldg, zero past nov.  One block per row.
+template <bool FP16>
+__global__ void k_kd_split(const double* __restrict__ C, int nocc, int nvir, int ldg, double s,
+                           uint16_t* __restrict__ hi, uint16_t* __restrict__ lo) {
+  const int row = blockIdx.x, i = row / nvir, a = row % nvir;
+  const size_t ldc = (size_t)nvir * nvir;
+  const int nov = nocc * nvir;
+  for (int c = threadIdx.x; c < ldg; c += blockDim.x) {
+    double v = 0.0;
+    if (c < nov) {
+      const int j = c / nvir, b = c % nvir;
+      v = C[(size_t)(i * nocc + j) * ldc + (size_t)a * nvir + b] * s;
+    }
+    uint16_t h, l;
+    if (FP16) {
+      const __half hh = __float2half_rn((float)v);
+      h = __half_as_ushort(hh);
+      l = __half_as_ushort(__float2half_rn((float)(v - (double)__half2float(hh))));
+    } else {
+      const __nv_bfloat16 hh = __float2bfloat16_rn((float)v);
+      h = __bfloat16_as_ushort(hh);
+      l = __bfloat16_as_ushort(__float2bfloat16_rn((float)(v - (double)__bfloat162float(hh))));
+    }
+    hi[(size_t)row * ldg + c] = h;
+    lo[(size_t)row * ldg + c] = l;
+  }
+}
+
 struct DevArr {
   double* p = nullptr;
   size_t n = 0;
@@ -183,6 +233,11 @@ struct qx_bse {
   DevArr delta, dia, diaT, ijw, dabT;
   DevArr w0T, dij;                   // kept for the root gradient (W0 term)
   DevArr dab_split, dab_scale;       // split forms: hi/lo of dabT [a][Q][ldvp], scale per a
+  // Split forms, when it fits: the direct kernel K^d [nov][ldg] as hi/lo with
+  // one scale, so that a matvec's direct term is one GEMM.
+  DevArr kd_split, kd_scale;
+  int ldg = 0;
+  bool kd = false;
   DevArr x_split;                    // split forms: hi/lo of the packed vectors
   DevArr xp, T, Yd, Z, Yx, Xr, Yr;  // matvec scratch
   DevArr gTt, gTp, gTpT, gdijT, gM, gG1, gG, gU;  // root-gradient scratch
@@ -191,9 +246,27 @@ struct qx_bse {
 };
 
 // y[v] = H x[v] for nvec vectors in row layout [nvec][ldov] (device).
-static void bse_apply_rows(qx_bse* B, const double* X, double* Y, int nvec) {
+// need_T: take the factored direct term even when K^d is held (the root
+// gradient reads its first step T).
+static void bse_apply_rows(qx_bse* B, const double* X, double* Y, int nvec, bool need_T = false) {
   qx_ctx* ctx = B->ctx;
   const int nocc = B->nocc, nvir = B->nvir, naux = B->naux;
+  B->Yd.alloc((size_t)nocc * nvir * nvec);
+  if (B->kd && !need_T) {
+    // Direct term as one GEMM: Yd[(i,a)][v] = sum_(j,b) K^d[(i,a)][(j,b)] X[v][(j,b)]
+    // (the layout Yd[i][(a,v)] of the factored form).
+    const int fp16 = B->precision == QX_PREC_FP16X3;
+    const size_t xe = (size_t)nvec * B->ldov;
+    const size_t xhalf = ((xe * 2 + 255) / 256) * 256;
+    B->x_split.alloc((2 * xhalf + 7) / 8 + 64);
+    uint8_t* xs = reinterpret_cast<uint8_t*>(B->x_split.p);
+    TcOperand Xo{xs, xs + xhalf, nullptr};
+    launch_split(ctx, X, nvec, B->nov, B->ldov, Xo.hi, Xo.lo, B->ldov, 0, 0, 1, fp16, 0, &Xo.scale);
+    const size_t ge = (size_t)B->nov * B->ldg;
+    uint8_t* gs = reinterpret_cast<uint8_t*>(B->kd_split.p);
+    TcOperand Go{gs, gs + ((ge * 2 + 255) / 256) * 256, reinterpret_cast<float*>(B->kd_scale.p)};
+    launch_gemm_tc(ctx, Go, B->nov, B->ldg, Xo, nvec, B->ldov, B->nov, 1, B->Yd.p, nvec, 0, fp16);
+  } else {
   // Direct term, step 1: T[a][(v,j)][Q] = sum_b X[v][j,b] dab[a][b][Q].
   B->xp.alloc((size_t)nvec * nocc * B->ldvp);
   {
@@ -240,7 +313,6 @@ static void bse_apply_rows(qx_bse* B, const double* X, double* Y, int nvec) {
     gemm_nt_f64(ctx, g);
   }
   // Step 2: Yd[i][(a,v)] = sum_{(j,Q)} ijw[i][(j,Q)] T[a][v][(j,Q)].
-  B->Yd.alloc((size_t)nocc * nvir * nvec);
   {
     GemmNT g{};
     g.M = nocc;
@@ -257,6 +329,7 @@ static void bse_apply_rows(qx_bse* B, const double* X, double* Y, int nvec) {
     g.beta = 0.0;
     g.splitk = 0;
     gemm_nt_f64(ctx, g);
+  }
   }
   // Exchange: Z[v][Q] = sum_ia X[v][ia] dia[ia][Q]; Yx[v][ia] = sum_Q Z[v][Q] dia[ia][Q].
   if (B->alpha_x != 0.0) {
@@ -409,6 +482,58 @@ qx_status qx_bse_create(qx_ctx* ctx, qx_bse** out, int nocc, int nvirt, int naux
     // df_ab [a][b][Q] -> dabT [a][Q][b] (ldvp).
     QX_CUDA(cudaStreamSynchronize(ctx->stream));
     upload(ctx, stage.p, df_ab, (size_t)nvirt * nvirt * naux);
+    // Split forms: hold K^d[(i,a)][(j,b)] = sum_Q ijw[(i,j)][Q] B_ab[(a,b)][Q]
+    // (kernel.rs:391-462 contracted once) when its FP64 build (nov^2 doubles,
+    // freed after the split) fits 16 GB: every matvec's direct term is then
+    // one GEMM that streams the 4 nov^2 bytes of hi/lo, instead of the
+    // 2 nov nvir naux-FLOP factored product per vector.
+    if (is_tc_precision(precision) && (size_t)nov * nov * sizeof(double) <= ((size_t)16 << 30)) {
+      const int fp16 = precision == QX_PREC_FP16X3;
+      DevArr cmat;
+      cmat.alloc((size_t)nov * nov);
+      GemmNT g{};
+      g.M = nocc * nocc;
+      g.N = nvirt * nvirt;
+      g.K = naux;
+      g.A = B->ijw.p;
+      g.lda = B->ldq;
+      g.B = stage.p;
+      g.ldb = naux;
+      g.C = cmat.p;
+      g.ldc = nvirt * nvirt;
+      g.batch = 1;
+      g.alpha = 1.0;
+      g.beta = 0.0;
+      g.splitk = 0;
+      gemm_nt_f64(ctx, g);
+      DevArr amax;
+      amax.alloc(1);
+      QX_CUDA(cudaMemsetAsync(amax.p, 0, sizeof(double), ctx->stream));
+      k_absmax<<<1184, 256, 0, ctx->stream>>>(cmat.p, (size_t)nov * nov,
+                                              reinterpret_cast<unsigned long long*>(amax.p));
+      check_launch(ctx);
+      double bound = 0.0;
+      QX_CUDA(cudaMemcpyAsync(&bound, amax.p, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+      QX_CUDA(cudaStreamSynchronize(ctx->stream));
+      // Power-of-two scale as in the other fp16 splits (largest entry in [2^14, 2^15)).
+      const double s = (fp16 && bound > 0.0 && std::isfinite(bound)) ? std::exp2(std::floor(std::log2(32768.0 / bound)))
+                                                                     : 1.0;
+      B->ldg = round_up(nov, 8);
+      const size_t ge = (size_t)nov * B->ldg;
+      const size_t ghalf = ((ge * 2 + 255) / 256) * 256;
+      B->kd_split.alloc((2 * ghalf + 7) / 8 + 64);
+      uint16_t* gs = reinterpret_cast<uint16_t*>(B->kd_split.p);
+      if (fp16)
+        k_kd_split<true><<<nov, 256, 0, ctx->stream>>>(cmat.p, nocc, nvirt, B->ldg, s, gs, gs + ghalf / 2);
+      else
+        k_kd_split<false><<<nov, 256, 0, ctx->stream>>>(cmat.p, nocc, nvirt, B->ldg, s, gs, gs + ghalf / 2);
+      check_launch(ctx);
+      const float sf = (float)s;
+      B->kd_scale.alloc(1);
+      QX_CUDA(cudaMemcpyAsync(B->kd_scale.p, &sf, sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+      QX_CUDA(cudaStreamSynchronize(ctx->stream));  // cmat is freed on return
+      B->kd = true;
+    }
     B->dabT.alloc((size_t)nvirt * naux * B->ldvp);
     QX_CUDA(cudaMemsetAsync(B->dabT.p, 0, (size_t)nvirt * naux * B->ldvp * sizeof(double), ctx->stream));
     transpose(ctx, stage.p, nvirt, naux, naux, (size_t)nvirt * naux, B->dabT.p, B->ldvp, (size_t)naux * B->ldvp,
@@ -756,7 +881,7 @@ qx_status qx_bse_root_grad(qx_bse* B, const double* x, const double* mo_energy, 
       B->Xr.alloc(B->ldov);
       B->Yr.alloc(B->ldov);
       QX_CUDA(cudaMemcpyAsync(B->Xr.p, hr.data(), B->ldov * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
-      bse_apply_rows(B, B->Xr.p, B->Yr.p, 1);
+      bse_apply_rows(B, B->Xr.p, B->Yr.p, 1, /*need_T=*/true);
       const int nq = nocc * ldq, n2o = nocc * nocc, ld2 = round_up(n2o, 8);
       // T'[(i,j)][Q] = sum_a x[i][a] T[a][(j,Q)]
       B->gTt.alloc((size_t)nq * ldvp);
