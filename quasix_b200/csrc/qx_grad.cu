@@ -315,6 +315,23 @@ extern "C" qx_status qx_g0w0_cd_grad(qx_ctx* ctx, const double* mo_energy, const
     double* G = XsT + (size_t)naux * ldT * fc_max;
     double* H = G + stride * fc_max;
     double* chi = H + (size_t)naux * ldov * fc_max;
+    // Split forms: H_f^T = B_ov^T G_f on tcgen05 (G_f is symmetric), from
+    // B_ov^T split once and G_f split per chunk, then transposed to H_f.
+    TcOperand bovT_split{}, g_split{};
+    double* Ht = nullptr;
+    const int fp16 = precision == QX_PREC_FP16X3;
+    if (E.tc) {
+      const size_t ae = (size_t)nov * ldn, ge = (size_t)fc_max * naux * ldn;
+      const size_t ab = ((ae * 2 + 255) / 256) * 256, gb = ((ge * 2 + 255) / 256) * 256;
+      DevBuf& g2 = ctx->ws[WS_GRAD2];
+      g2.reserve(2 * ab + 2 * gb + (size_t)fc_max * nov * ldn * sizeof(double) + 1024);
+      uint8_t* p2 = g2.as<uint8_t>();
+      bovT_split = TcOperand{p2, p2 + ab, nullptr};
+      g_split = TcOperand{p2 + 2 * ab, p2 + 2 * ab + gb, nullptr};
+      Ht = reinterpret_cast<double*>(p2 + 2 * ab + 2 * gb);
+      launch_split(ctx, E.bovT, nov, naux, ldn, bovT_split.hi, bovT_split.lo, ldn, 0, 0, 1, fp16, 0,
+                   &bovT_split.scale);
+    }
     for (int f0 = 0; f0 < nw; f0 += fc_max) {
       const int fc = std::min(fc_max, nw - f0);
       launch_chi(ctx, E.S.d_en, nocc, nvir, E.S.d_freqs + f0, fc, 0, chi, ldov);
@@ -334,7 +351,14 @@ extern "C" qx_status qx_g0w0_cd_grad(qx_ctx* ctx, const double* mo_energy, const
       check_launch(ctx);
       // G_f = -sum_p c X X^T;  H_f = G_f B_ov
       gemm(ctx, naux, naux, Tn, XsT, ldT, (size_t)naux * ldT, XT, ldT, (size_t)naux * ldT, G, ldn, stride, fc, -1.0);
-      gemm(ctx, naux, nov, naux, G, ldn, stride, E.bovT, ldn, 0, H, ldov, (size_t)naux * ldov, fc, 1.0);
+      if (E.tc) {
+        launch_split(ctx, G, naux, naux, ldn, g_split.hi, g_split.lo, ldn, stride, (size_t)naux * ldn, fc, fp16, 2,
+                     &g_split.scale);
+        launch_gemm_tc(ctx, bovT_split, nov, ldn, g_split, naux, ldn, naux, fc, Ht, ldn, (size_t)nov * ldn, fp16);
+        transpose(ctx, Ht, nov, naux, ldn, (size_t)nov * ldn, H, ldov, (size_t)naux * ldov, fc);
+      } else {
+        gemm(ctx, naux, nov, naux, G, ldn, stride, E.bovT, ldn, 0, H, ldov, (size_t)naux * ldov, fc, 1.0);
+      }
       k_grad_ov_imag<<<dim3(ceil_div(nov, 128), npb), 128, 0, ctx->stream>>>(E.S.bov, ldov, naux, nov, H, chi, fc,
                                                                              g_bov, part, npb);
       check_launch(ctx);
