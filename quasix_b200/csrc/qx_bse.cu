@@ -641,6 +641,9 @@ qx_status qx_bse_davidson(qx_bse* B, const qx_davidson_config* cfgp, double* eig
       eigh_lowest(ctx, B->heff.p, nv, nv, k, d_theta, B->Z2.p, nv, B->jv.p, reinterpret_cast<int*>(B->eigi.p));
     };
     const int nthreads = 256, nblk = std::min(ceil_div(n, nthreads), 2 * ctx->sm_count);
+    // The norm reductions run in one block of 1024 threads each, so that their
+    // summation order (and the Davidson path) is the same on every run.
+    constexpr int kRedThreads = 1024;
     // Trivial case (davidson.rs:384-387, 510-540): the full matrix.
     if (n <= nroots) {
       std::vector<double> id((size_t)n * ld, 0.0);
@@ -690,7 +693,7 @@ qx_status qx_bse_davidson(qx_bse* B, const qx_davidson_config* cfgp, double* eig
       combine_rows(ctx, B->V.p, ld, nv, B->Z2.p, nv, nr_, n, B->X.p, ld, 1.0, 0.0);
       combine_rows(ctx, B->AV.p, ld, nv, B->Z2.p, nv, nr_, n, B->AX.p, ld, 1.0, 0.0);
       QX_CUDA(cudaMemsetAsync(d_nrm, 0, nr_ * sizeof(double), ctx->stream));
-      k_residual<<<dim3(nblk, nr_), nthreads, 0, ctx->stream>>>(B->AX.p, B->X.p, d_theta, ld, n, B->R.p, d_nrm);
+      k_residual<<<dim3(1, nr_), kRedThreads, 0, ctx->stream>>>(B->AX.p, B->X.p, d_theta, ld, n, B->R.p, d_nrm);
       check_launch(ctx);
       QX_CUDA(cudaMemcpyAsync(th.data(), d_theta, nr_ * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
       QX_CUDA(cudaMemcpyAsync(nr.data(), d_nrm, nr_ * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
@@ -721,7 +724,7 @@ qx_status qx_bse_davidson(qx_bse* B, const qx_davidson_config* cfgp, double* eig
         const int j = newr[q];
         double* t = B->V.p + (size_t)(nv + q) * ld;
         QX_CUDA(cudaMemsetAsync(d_c, 0, sizeof(double), ctx->stream));
-        k_precond<<<nblk, nthreads, 0, ctx->stream>>>(B->R.p + (size_t)j * ld, B->delta.p, th[j], cfg.level_shift, n,
+        k_precond<<<1, kRedThreads, 0, ctx->stream>>>(B->R.p + (size_t)j * ld, B->delta.p, th[j], cfg.level_shift, n,
                                                       t, d_c);
         check_launch(ctx);
         k_normalize<<<nblk, nthreads, 0, ctx->stream>>>(t, n, d_c, 1e-14);
@@ -751,7 +754,7 @@ qx_status qx_bse_davidson(qx_bse* B, const qx_davidson_config* cfgp, double* eig
             combine_rows(ctx, B->V.p, ld, i, d_c, 1, 1, n, v, ld, -1.0, 1.0);
           }
           QX_CUDA(cudaMemsetAsync(d_nrm, 0, sizeof(double), ctx->stream));
-          k_norm2<<<nblk, nthreads, 0, ctx->stream>>>(v, n, d_nrm);
+          k_norm2<<<1, kRedThreads, 0, ctx->stream>>>(v, n, d_nrm);
           check_launch(ctx);
           k_normalize<<<nblk, nthreads, 0, ctx->stream>>>(v, n, d_nrm, -1.0);
           check_launch(ctx);
@@ -787,7 +790,7 @@ qx_status qx_bse_davidson(qx_bse* B, const qx_davidson_config* cfgp, double* eig
           combine_rows(ctx, B->V.p, ld, cur, d_c, 1, 1, n, dst, ld, -1.0, 1.0);
         }
         QX_CUDA(cudaMemsetAsync(d_nrm, 0, sizeof(double), ctx->stream));
-        k_norm2<<<nblk, nthreads, 0, ctx->stream>>>(dst, n, d_nrm);
+        k_norm2<<<1, kRedThreads, 0, ctx->stream>>>(dst, n, d_nrm);
         check_launch(ctx);
         double h2 = 0.0;
         QX_CUDA(cudaMemcpyAsync(&h2, d_nrm, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));

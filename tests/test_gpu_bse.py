@@ -124,11 +124,25 @@ def test_root_gradient_matches_oracle(q, shape):
         assert np.abs(got - ref).max() < 1e-10 * np.abs(ref).max()
 
 
+@pytest.mark.parametrize("precision", ["fp64", "fp16x3"])
+def test_davidson_is_deterministic(q, precision):
+    """Two solves from the same start take the same path: identical iteration
+    counts and bit-identical roots (the norm reductions have a fixed order)."""
+    nocc, nvir, naux = 12, 60, 150
+    s, delta, dia, dij, dab, w0 = bse_inputs(nocc, nvir, naux, 3)
+    k = q.BSETDAKernel(nocc, nvir, naux, delta, dia, dij, dab, w0, precision=precision)
+    r1 = k.solve_davidson(n_roots=5, tol_residual=1e-8)
+    r2 = k.solve_davidson(n_roots=5, tol_residual=1e-8)
+    assert r1["iterations"] == r2["iterations"]
+    assert np.array_equal(np.array(r1["eigenvalues"]), np.array(r2["eigenvalues"]))
+
+
 @pytest.mark.parametrize("precision,tol", [("fp16x3", 2e-6), ("bf16x3", 3e-5)])
 def test_split_precision_matvec_and_roots(q, precision, tol):
-    """Direct-term GEMM T = X dab^T on tcgen05 (split operands, FP64 drain of
-    each 64-wide K block); the other GEMMs and the Rayleigh-Ritz step stay
-    FP64.  Matvec error relative to max|y|; roots within 1e-6 Ha of FP64."""
+    """Split forms: the direct kernel K^d is held as hi/lo and the direct term
+    is one tcgen05 GEMM (FP64 drain of each 64-wide K block); the exchange
+    term and the Rayleigh-Ritz step stay FP64.  Matvec error relative to
+    max|y|; roots within 1e-6 Ha of FP64."""
     nocc, nvir, naux = 6, 30, 80
     s, delta, dia, dij, dab, w0 = bse_inputs(nocc, nvir, naux, 2)
     k = q.BSETDAKernel(nocc, nvir, naux, delta, dia, dij, dab, w0, precision=precision)
