@@ -66,8 +66,8 @@ void gemm_nt_f64(qx_ctx* ctx, GemmNT g) {
                  (reinterpret_cast<uintptr_t>(g.B) & 15) == 0 && g.sA % 2 == 0 && g.sB % 2 == 0,
              QX_ERR_INVALID_INPUT, "gemm_nt_f64: operands must be 16-byte aligned with even leading dimensions");
   if (g.M <= 0 || g.N <= 0 || g.batch <= 0) return;
-  static std::once_flag attr_once;
-  std::call_once(attr_once, [&] {
+  static PerDeviceOnce attr_once;
+  attr_once(ctx->device, [&] {
     QX_CUDA(cudaFuncSetAttribute(k_gemm_nt, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::SMEM));
   });
   if (g.splitk < 1) {
@@ -256,8 +256,8 @@ __global__ void __launch_bounds__(1024) k_jacobi(double* __restrict__ A, double*
 void jacobi_eigh(qx_ctx* ctx, double* A, double* V, int n, int lda, double* w, double* Z, int ldz, int* info) {
   const int m = n + (n & 1);
   const size_t sh = (size_t)m * sizeof(double) + (size_t)m * sizeof(int) + 64;
-  static std::once_flag attr_once;
-  std::call_once(attr_once, [&] {
+  static PerDeviceOnce attr_once;
+  attr_once(ctx->device, [&] {
     QX_CUDA(cudaFuncSetAttribute(k_jacobi, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024));
   });
   QX_REQUIRE(sh <= 64 * 1024, QX_ERR_INVALID_INPUT, "subspace too large for the Jacobi kernel (%d)", n);
@@ -509,8 +509,8 @@ void eigh_lowest(qx_ctx* ctx, const double* A, int n, int lda, int k, double* w,
   double* W = work;
   double* rest = work + (size_t)n * n;
   const size_t sh = 2 * (size_t)n * sizeof(double);
-  static std::once_flag attr_once;
-  std::call_once(attr_once, [&] {
+  static PerDeviceOnce attr_once;
+  attr_once(ctx->device, [&] {
     QX_CUDA(cudaFuncSetAttribute(k_eigh_lowest, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * 4096 * 8));
   });
   k_eigh_lowest<<<1, 1024, sh, ctx->stream>>>(A, n, lda, k, W, rest, iwork, w, Z, ldz);

@@ -87,8 +87,8 @@ void launch_eps_fp64(qx_ctx* ctx, const double* bov, int ldov, int naux, int nov
   using T = EpsTile;
   const int tiles = ceil_div(naux, T::BM);
   dim3 grid(tiles * (tiles + 1) / 2, nw);
-  static std::once_flag attr_once;
-  std::call_once(attr_once, [&] {
+  static PerDeviceOnce attr_once;
+  attr_once(ctx->device, [&] {
     QX_CUDA(cudaFuncSetAttribute(k_eps_f64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::SMEM));
   });
   k_eps_f64<<<grid, T::THREADS, T::SMEM, ctx->stream>>>(bov, ldov, naux, nov, chi, eps, ldn, eps_stride);
@@ -487,9 +487,9 @@ void sweep_set_attributes() {
   QX_CUDA(cudaFuncSetAttribute(k_gsweep_update, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SweepTile::SMEM));
 }
 
-static void sweep_attributes_once() {
-  static std::once_flag attr_once;
-  std::call_once(attr_once, [] { sweep_set_attributes(); });
+static void sweep_attributes_once(int device) {
+  static PerDeviceOnce attr_once;
+  attr_once(device, [] { sweep_set_attributes(); });
 }
 
 // One block step of the sweep on stream st: D, T, then P and the panel write.
@@ -539,7 +539,7 @@ void launch_invert_wc(qx_ctx* ctx, double* eps, int n, int ldn, size_t stride, i
   double* Db[2] = {D0, D1};
   int* status = status_words(ctx, nw);
   QX_CUDA(cudaMemsetAsync(status, 0, nw * sizeof(int), ctx->stream));
-  sweep_attributes_once();
+  sweep_attributes_once(ctx->device);
   const int nsteps = ceil_div(n, SWEEP_NB);
   // Split form: panel splits (two steps in flight) and one tcgen05 error word
   // per update launch, zeroed here on the context stream.
@@ -783,7 +783,7 @@ void launch_invert_wc_group(qx_ctx* ctx, const GMat* mats_in, int G, int half_lo
     sb.reserve(pan * 2 * 4 + 256);
     split_base = sb.ptr;
   }
-  sweep_attributes_once();
+  sweep_attributes_once(ctx->device);
   k_gzero_pad<<<G, 256, 0, ctx->stream>>>(d_mats, Tcat, Pcat);
   check_launch(ctx);
   const int diag_smem = (SWEEP_NB * SWEEP_NB + SWEEP_NB * 33) * sizeof(double);
@@ -974,8 +974,8 @@ __global__ void __launch_bounds__(PairTile::THREADS) k_pair_contract_f64(const d
 void launch_pair_contract_fp64(qx_ctx* ctx, const double* bpt, int ldk, int npair, int naux, const double* wc,
                                int ldn, size_t wc_stride, int nw, double* v, int ldv) {
   using T = PairTile;
-  static std::once_flag attr_once;
-  std::call_once(attr_once, [&] {
+  static PerDeviceOnce attr_once;
+  attr_once(ctx->device, [&] {
     QX_CUDA(cudaFuncSetAttribute(k_pair_contract_f64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::SMEM));
   });
   dim3 grid(ceil_div(npair, T::BM), nw);

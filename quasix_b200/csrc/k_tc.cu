@@ -997,8 +997,8 @@ template <int BN, int EPI>
 static void launch_tc(qx_ctx* ctx, const CUtensorMap& ah, const CUtensorMap& al, const CUtensorMap& bh,
                       const CUtensorMap& bl, const TcArgs& a, dim3 grid, cudaStream_t stream = nullptr) {
   using L = TcSmem<BN, EPI>;
-  static std::once_flag attr_once;
-  std::call_once(attr_once, [&] {
+  static PerDeviceOnce attr_once;
+  attr_once(ctx->device, [&] {
     QX_CUDA(cudaFuncSetAttribute(k_tc_gemm<BN, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, L::TOTAL));
   });
   k_tc_gemm<BN, EPI><<<grid, TcWarps<EPI>::THREADS, L::TOTAL, stream ? stream : ctx->stream>>>(ah, al, bh, bl, a);

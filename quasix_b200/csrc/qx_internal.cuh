@@ -9,6 +9,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -157,6 +158,18 @@ enum WsSlot {
   WS_COUNT
 };
 static_assert(WS_COUNT <= 40, "workspace slots");
+
+// Runs f once per device (per call site): kernel attributes such as the
+// dynamic shared-memory limit are set per device, with that device current.
+struct PerDeviceOnce {
+  static constexpr int kMaxDevices = 64;
+  std::once_flag flags[kMaxDevices];
+  template <class F>
+  void operator()(int device, F&& f) {
+    QX_REQUIRE(device >= 0 && device < kMaxDevices, QX_ERR_INVALID_INPUT, "device %d out of range", device);
+    std::call_once(flags[device], std::forward<F>(f));
+  }
+};
 
 // Is p a device-accessible pointer of the current device?
 bool is_device_ptr(const void* p);
