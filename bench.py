@@ -554,6 +554,10 @@ def main():
             "max_qp_err_meV_per_iteration": err_iter, "fp64_perturbation_1e-14_meV_per_iteration": sens_iter,
             "stage_ms_per_step": {k: v / args.steps for k, v in stage.items()},
             "roofline": roof, "clocks": clocks, "e2e": e2e, "gpu_launches": launches}
+    if prec_main != "fp64":
+        # Tensor-core utilisation of the dominant kernel: the MMA work it issues
+        # per second over the measured sustained tcgen05 (bf16/fp16) peak.
+        line["tc_util_pct"] = 100.0 * roof["executed_mma_frac"]
     if not args.no_grad:
         line["grad_nmo200"] = bench_grad_nmo200(q, dev, prec_main)
     if not args.no_bse:
