@@ -1,7 +1,7 @@
 """GPU parity of the FP64 GW chain against the CPU oracle (same seeded inputs).
 
 Tolerances: the plain path is all FP64; P0/Wc agree to ~1e-12 relative, Sigma_c
-to 1e-10 Ha absolute, QP energies to 1e-8 Ha.
+to 1e-10 Ha absolute, QP energies to 1e-8 Ha (the parity bar of the plain FP64 path).
 """
 import numpy as np
 import pytest
