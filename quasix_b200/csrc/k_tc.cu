@@ -25,6 +25,7 @@
 #include <vector>
 
 #include "qx_internal.cuh"
+#include "split_round.cuh"
 
 namespace qx {
 
@@ -747,17 +748,13 @@ __global__ void k_split(const double* __restrict__ src, int rows, int cols, int 
       if (colscale) x *= colscale[(size_t)b * ld_cs + c];
     }
     x *= (double)s;
-    if (fp16) {
-      const __half h = __float2half_rn((float)x);
-      const double rem = x - (double)__half2float(h);
-      reinterpret_cast<__half*>(hi_)[(size_t)b * dst_stride + i] = h;
-      reinterpret_cast<__half*>(lo_)[(size_t)b * dst_stride + i] = __float2half_rn((float)rem);
-    } else {
-      const __nv_bfloat16 h = __float2bfloat16_rn((float)x);
-      const double rem = x - (double)__bfloat162float(h);
-      reinterpret_cast<__nv_bfloat16*>(hi_)[(size_t)b * dst_stride + i] = h;
-      reinterpret_cast<__nv_bfloat16*>(lo_)[(size_t)b * dst_stride + i] = __float2bfloat16_rn((float)rem);
-    }
+    uint16_t h, l;
+    if (fp16)
+      split_round<true>(x, h, l);
+    else
+      split_round<false>(x, h, l);
+    reinterpret_cast<uint16_t*>(hi_)[(size_t)b * dst_stride + i] = h;
+    reinterpret_cast<uint16_t*>(lo_)[(size_t)b * dst_stride + i] = l;
   }
 }
 
@@ -792,32 +789,14 @@ __device__ __forceinline__ void load8(const double* __restrict__ row, const doub
   }
 }
 
-// hi/lo of s*x[0..8) packed into one 16-byte word each (same rounding as k_split).
+// hi/lo of s*x[0..8) packed into one 16-byte word each (split_round, as k_split).
 template <bool FP16>
 __device__ __forceinline__ void split8_store(const double (&x)[8], float s, uint4* __restrict__ H,
                                              uint4* __restrict__ L) {
   uint32_t hw[4], lw[4];
+  const double sd = (double)s;
 #pragma unroll
-  for (int j = 0; j < 8; j += 2) {
-    uint16_t hb[2], lb[2];
-#pragma unroll
-    for (int k = 0; k < 2; ++k) {
-      const double v = x[j + k] * (double)s;
-      if (FP16) {
-        const __half h = __float2half_rn((float)v);
-        const __half l = __float2half_rn((float)(v - (double)__half2float(h)));
-        hb[k] = __half_as_ushort(h);
-        lb[k] = __half_as_ushort(l);
-      } else {
-        const __nv_bfloat16 h = __float2bfloat16_rn((float)v);
-        const __nv_bfloat16 l = __float2bfloat16_rn((float)(v - (double)__bfloat162float(h)));
-        hb[k] = __bfloat16_as_ushort(h);
-        lb[k] = __bfloat16_as_ushort(l);
-      }
-    }
-    hw[j >> 1] = (uint32_t)hb[0] | ((uint32_t)hb[1] << 16);
-    lw[j >> 1] = (uint32_t)lb[0] | ((uint32_t)lb[1] << 16);
-  }
+  for (int j = 0; j < 8; j += 2) split_round2<FP16>(x[j] * sd, x[j + 1] * sd, hw[j >> 1], lw[j >> 1]);
   *H = make_uint4(hw[0], hw[1], hw[2], hw[3]);
   *L = make_uint4(lw[0], lw[1], lw[2], lw[3]);
 }

@@ -12,6 +12,7 @@
 
 #include "qx_blas.cuh"
 #include "qx_internal.cuh"
+#include "split_round.cuh"
 
 namespace qx {
 
@@ -195,15 +196,7 @@ __global__ void k_kd_split(const double* __restrict__ C, int nocc, int nvir, int
       v = C[(size_t)(i * nocc + j) * ldc + (size_t)a * nvir + b] * s;
     }
     uint16_t h, l;
-    if (FP16) {
-      const __half hh = __float2half_rn((float)v);
-      h = __half_as_ushort(hh);
-      l = __half_as_ushort(__float2half_rn((float)(v - (double)__half2float(hh))));
-    } else {
-      const __nv_bfloat16 hh = __float2bfloat16_rn((float)v);
-      h = __bfloat16_as_ushort(hh);
-      l = __bfloat16_as_ushort(__float2bfloat16_rn((float)(v - (double)__bfloat162float(hh))));
-    }
+    split_round<FP16>(v, h, l);
     hi[(size_t)row * ldg + c] = h;
     lo[(size_t)row * ldg + c] = l;
   }
