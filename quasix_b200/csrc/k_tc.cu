@@ -831,16 +831,19 @@ __global__ void k_split8(const double* __restrict__ src, int rows, int cols, int
 }
 
 // k_split8 for one source shared by every batch (src_stride == 0) with a
-// column scale per batch (the chi-scaled operand of P0): each thread reads its
-// eight source values once and writes the hi/lo groups of all batches, so the
-// FP64 source crosses memory once instead of once per batch.  The per-batch
-// scales sit in shared memory ([batch] floats, batch <= 1024).
-template <bool FP16>
-__global__ void k_split8_bcast(const double* __restrict__ src, int rows, int cols, int ld_src,
-                               const double* __restrict__ colscale, int ld_cs, void* __restrict__ hi_,
-                               void* __restrict__ lo_, int ld_dst, size_t dst_stride, int batch,
-                               const unsigned long long* __restrict__ amax_src,
-                               const unsigned long long* __restrict__ amax_col, float* __restrict__ scale_out) {
+// column scale per batch (the chi-scaled operand of P0): each thread reads the
+// eight source values of RB rows once and writes the hi/lo groups of all
+// batches, so the FP64 source crosses memory once instead of once per batch,
+// and each batch's eight column scales are loaded once for the RB rows (with
+// RB = 1 the scale loads are twice the hi/lo bytes stored and the kernel is
+// bound by L1 traffic).  The per-batch scales sit in shared memory ([batch]
+// floats, batch <= 1024).
+template <bool FP16, int RB>
+__global__ void __launch_bounds__(256, 2)
+    k_split8_bcast(const double* __restrict__ src, int rows, int cols, int ld_src,
+                   const double* __restrict__ colscale, int ld_cs, void* __restrict__ hi_, void* __restrict__ lo_,
+                   int ld_dst, size_t dst_stride, int batch, const unsigned long long* __restrict__ amax_src,
+                   const unsigned long long* __restrict__ amax_col, float* __restrict__ scale_out) {
   __shared__ float s_scale[1024];
   for (int b = threadIdx.x; b < batch; b += blockDim.x) {
     s_scale[b] = split_scale(FP16, b, 0, amax_src, amax_col);
@@ -848,30 +851,53 @@ __global__ void k_split8_bcast(const double* __restrict__ src, int rows, int col
   }
   __syncthreads();
   const unsigned gpr = (unsigned)ld_dst >> 3;
-  const unsigned total = (unsigned)rows * gpr;
+  const unsigned total = ((unsigned)rows + RB - 1) / RB * gpr;
   uint4* H = reinterpret_cast<uint4*>(hi_);
   uint4* L = reinterpret_cast<uint4*>(lo_);
   const size_t bstride = dst_stride >> 3;  // in 16-byte groups
   for (unsigned g = blockIdx.x * blockDim.x + threadIdx.x; g < total; g += gridDim.x * blockDim.x) {
-    const unsigned r = g / gpr;
-    const int c0 = (int)(g - r * gpr) << 3;
-    double x0[8];
-    load8(src + (size_t)r * ld_src, nullptr, c0, cols, x0);
+    const unsigned rb = g / gpr;
+    const unsigned cg = g - rb * gpr;
+    const int c0 = (int)cg << 3;
+    const int r0 = (int)rb * RB;
+    const int nr = min(RB, rows - r0);
+    double x0[RB][8];
+#pragma unroll
+    for (int i = 0; i < RB; ++i) {
+      if (i < nr) {
+        load8(src + (size_t)(r0 + i) * ld_src, nullptr, c0, cols, x0[i]);
+      } else {
+#pragma unroll
+        for (int j = 0; j < 8; ++j) x0[i][j] = 0.0;
+      }
+    }
+    const bool full = c0 + 8 <= cols;
+    const size_t g0 = (size_t)r0 * gpr + cg;  // group of (r0, c0) in one batch
     for (int b = 0; b < batch; ++b) {
       const double* cs = colscale + (size_t)b * ld_cs;
-      double x[8];
-      if (c0 + 8 <= cols) {
+      double c[8];
+      if (full) {
 #pragma unroll
         for (int j = 0; j < 8; j += 2) {
           const double2 v = *reinterpret_cast<const double2*>(cs + c0 + j);
-          x[j] = x0[j] * v.x;
-          x[j + 1] = x0[j + 1] * v.y;
+          c[j] = v.x;
+          c[j + 1] = v.y;
         }
       } else {
 #pragma unroll
-        for (int j = 0; j < 8; ++j) x[j] = (c0 + j < cols) ? x0[j] * cs[c0 + j] : 0.0;
+        for (int j = 0; j < 8; ++j) c[j] = (c0 + j < cols) ? cs[c0 + j] : 0.0;
       }
-      split8_store<FP16>(x, s_scale[b], H + b * bstride + g, L + b * bstride + g);
+      const float sb = s_scale[b];
+      const size_t gb = (size_t)b * bstride + g0;
+#pragma unroll
+      for (int i = 0; i < RB; ++i) {
+        if (i < nr) {
+          double x[8];
+#pragma unroll
+          for (int j = 0; j < 8; ++j) x[j] = x0[i][j] * c[j];
+          split8_store<FP16>(x, sb, H + gb + (size_t)i * gpr, L + gb + (size_t)i * gpr);
+        }
+      }
     }
   }
 }
@@ -933,13 +959,25 @@ static void split(qx_ctx* ctx, const double* src, int rows, int cols, int ld_src
   const unsigned long long* acol = colscale ? sc.amax_col : nullptr;
   const size_t groups = (size_t)rows * (ld_dst / 8);
   if (vec && groups < (1u << 31) && src_stride == 0 && colscale && batch > 1) {
-    dim3 grid((unsigned)std::min<size_t>((groups + 255) / 256, 4096));
-    if (fp16)
-      k_split8_bcast<true><<<grid, 256, 0, st>>>(src, rows, cols, ld_src, colscale, ld_cs, hi, lo, ld_dst,
-                                                          dst_stride, batch, sc.amax_src, acol, sc.scale);
+    // Four rows per thread when that still gives every SM two full blocks
+    // (the kernel's residency), else one; a grid-stride loop over at most
+    // those resident blocks.
+    const size_t resident = 2 * (size_t)std::max(ctx->sm_count, 1);
+    const bool rb4 = (groups + 3) / 4 >= resident * 256;
+    const size_t items = rb4 ? ((size_t)(rows + 3) / 4) * (ld_dst / 8) : groups;
+    dim3 grid((unsigned)std::min<size_t>((items + 255) / 256, rb4 ? resident : 4096));
+    if (fp16 && rb4)
+      k_split8_bcast<true, 4><<<grid, 256, 0, st>>>(src, rows, cols, ld_src, colscale, ld_cs, hi, lo, ld_dst,
+                                                    dst_stride, batch, sc.amax_src, acol, sc.scale);
+    else if (fp16)
+      k_split8_bcast<true, 1><<<grid, 256, 0, st>>>(src, rows, cols, ld_src, colscale, ld_cs, hi, lo, ld_dst,
+                                                    dst_stride, batch, sc.amax_src, acol, sc.scale);
+    else if (rb4)
+      k_split8_bcast<false, 4><<<grid, 256, 0, st>>>(src, rows, cols, ld_src, colscale, ld_cs, hi, lo, ld_dst,
+                                                     dst_stride, batch, sc.amax_src, acol, sc.scale);
     else
-      k_split8_bcast<false><<<grid, 256, 0, st>>>(src, rows, cols, ld_src, colscale, ld_cs, hi, lo, ld_dst,
-                                                           dst_stride, batch, sc.amax_src, acol, sc.scale);
+      k_split8_bcast<false, 1><<<grid, 256, 0, st>>>(src, rows, cols, ld_src, colscale, ld_cs, hi, lo, ld_dst,
+                                                     dst_stride, batch, sc.amax_src, acol, sc.scale);
   } else if (vec && groups < (1u << 31)) {
     dim3 grid((unsigned)std::min<size_t>((groups + 255) / 256, 4096), batch);
     if (fp16)
