@@ -77,8 +77,22 @@ qx_status qx_get_rho_response(qx_ctx* ctx, int nfreq, const double* freqs, const
                               double* pi);
 
 /* Wc = (I - Pi)^-1 - I for nfreq matrices (correlation_ac.rs:377-401).
- * pi, wc: [nfreq][naux][naux] (may alias). */
+ * pi, wc: [nfreq][naux][naux] (may alias).  The reference inverts eps by
+ * Cholesky, then by LU with partial pivoting, then substitutes the identity;
+ * here a block Gauss-Jordan sweep runs first, guarded: a matrix with a pivot
+ * below 1e-6 max|eps|, element growth above 1e4 max|eps|, or a probe-vector
+ * backward error max|eps X v - v| / (n max|eps| max|X|) above 1e-15 is
+ * inverted again by Gauss-Jordan elimination with partial pivoting, and one
+ * that is singular there gets Wc = 0 (with a warning on stderr). */
 qx_status qx_screened_interaction(qx_ctx* ctx, int nfreq, int naux, const double* pi, double* wc);
+
+/* 1 when eps(w) = I + B diag(chi'(w)) B^T >= I is guaranteed for these
+ * orbital energies at every real shift |w| <= wmax (wmax = 0: the imaginary
+ * axis): every occupied level lies below every virtual one and wmax is below
+ * that gap, so every chi' > 0.  The library's own inversions skip the guard
+ * of qx_screened_interaction exactly then.  No reference counterpart (the
+ * reference tries Cholesky first and falls back on failure); host-only. */
+int qx_eps_at_least_identity(const double* mo_energy, int nocc, int nvir, double wmax);
 
 /* qx_screened_interaction without any allocation.  No counterpart in the
  * reference: it exists for callers that must not allocate device memory
@@ -107,17 +121,52 @@ qx_status qx_get_sigma_diag(qx_ctx* ctx, const double* mo_energy, const double* 
                             int precision, double* sigma, double* omega, int nw_sigma_max,
                             int* nw_sigma);
 
-/* thiele + ac_pade_thiele_diag (correlation_ac.rs:470-509, 587-654).
- * sigma, omega: complex [norbs][nw_sigma].  npade < 0 selects the reference's
- * point rule; npade = k selects 2k points (the [k/k] form).
- * coeff: complex [nfit][norbs], omega_fit: complex [norbs][nfit]; *nfit out. */
+/* thiele + ac_pade_thiele_diag (correlation_ac.rs:470-509, 587-654), one
+ * device thread per orbital.  sigma, omega: complex [norbs][nw_sigma].
+ * npade < 0 selects the reference's point rule; npade = k selects 2k points
+ * (the [k/k] form, nfit <= 64).  coeff: complex [nfit][norbs], omega_fit:
+ * complex [norbs][nfit]; *nfit out. */
 qx_status qx_ac_pade_thiele_diag(qx_ctx* ctx, int norbs, int nw_sigma, const double* sigma,
                                  const double* omega, int npade, double* coeff, double* omega_fit,
                                  int nfit_max, int* nfit);
 
-/* pade_thiele (correlation_ac.rs:530-566) at nomega real points for one orbital. */
-qx_status qx_pade_thiele(int nfit, const double* zn, const double* coeff, int nomega,
+/* pade_thiele (correlation_ac.rs:530-566) at nomega real points for one
+ * orbital, on the device: zn, coeff complex [nfit]; out complex [nomega]. */
+qx_status qx_pade_thiele(qx_ctx* ctx, int nfit, const double* zn, const double* coeff, int nomega,
                          const double* omega, double* out);
+
+/* ---- analysis: spectral functions ------------------------------------------- */
+/* SpectralAnalyzer::compute_spectral_function (quasix_core/src/analysis/
+ * spectral.rs:235-325, profiles 327-545): weights[q] = sum_i Z_i P(omega[q] -
+ * E_i) with P Gaussian (voigt_mixing < 0.01), Lorentzian (> 0.99) or the
+ * mixture (1 - a) G + a L.  kind 0: every state; 1: generate_pes_spectrum
+ * (states E <= fermi_energy at binding energy fermi_energy - E); 2:
+ * generate_ipes_spectrum (states E > fermi_energy at E - fermi_energy)
+ * (spectral.rs:557-656).  Rejects Z outside [0, 1], widths <= 0, mixing
+ * outside [0, 1] and an empty grid (QX_ERR_INVALID_INPUT), as the reference's
+ * validate() does.  total_weight (may be NULL): sum(weights) * (omega[1] -
+ * omega[0]), the reference's normalisation figure. */
+qx_status qx_spectral_function(qx_ctx* ctx, const double* qp_energies, const double* z_factors, int n_states,
+                               double fermi_energy, int kind, const double* omega, int n_omega,
+                               double gaussian_width, double lorentzian_width, double voigt_mixing,
+                               double* weights, double* total_weight);
+
+/* EvGWResult.spectral_function (quasix/quasix/evgw.py:124-134): per state,
+ * A[i][q] = Z_i eta / ((omega[q] - E_i)^2 + eta^2) / pi; A [n_states][n_omega]. */
+qx_status qx_spectral_function_states(qx_ctx* ctx, const double* qp_energies, const double* z_factors, int n_states,
+                                      const double* omega, int n_omega, double eta, double* A);
+
+/* Spectral function of each orbital from the Pade continuation of its
+ * Sigma_c (the fits of qx_ac_pade_thiele_diag; no reference counterpart, the
+ * reference broadens the QP peaks only): with S(w) the continued fraction of
+ * orbital t at w - ef,
+ *   A[t][q] = (1/pi) G / ((w - e_ref[t] - sigma_x[t] + vxc[t] - Re S)^2 + G^2),
+ *   G = |Im S| + eta,  w = omega[q].
+ * coeff complex [nfit][norbs], omega_fit complex [norbs][nfit]; vxc may be
+ * NULL (0); A [norbs][n_omega]. */
+qx_status qx_spectral_function_pade(qx_ctx* ctx, int norbs, int nfit, const double* coeff, const double* omega_fit,
+                                    const double* e_ref, const double* sigma_x, const double* vxc, double ef,
+                                    const double* omega, int n_omega, double eta, double* A);
 
 /* Exchange self-energy diagonal (qp/evgw.rs:1167-1193):
  * sigma_x[p] = -sum_{i,R} lpq[R][p][i]^2. */
@@ -237,6 +286,33 @@ qx_status qx_g0w0_cd_grad(qx_ctx* ctx, const double* mo_energy, const double* lp
                           int nw, double x0, int precision, double* grad_energy, double* grad_lpq,
                           double* z_raw);
 
+/* ---- df: density-fitting tensors ---------------------------------------------- */
+/* transform_mo_3center (quasix_core/src/df/mo_transform.rs:136-282):
+ * out[i*nvir + a][P] = sum_{u,v} C_occ[u][i] (uv|P) C_vir[v][a] on FP64 DMMA
+ * GEMMs.  j3c_ao [nao][nao][naux] (symmetric in u, v), c_occ [nao][nocc],
+ * c_vir [nao][nvir]. */
+qx_status qx_transform_mo_3center(qx_ctx* ctx, const double* j3c_ao, const double* c_occ, const double* c_vir,
+                                  int nao, int nocc, int nvir, int naux, double* out);
+
+/* J^-1/2 and J^1/2 of the Coulomb metric J = (P|Q) (quasix/quasix/evgw.py:
+ * 1014-1046, there by eigh with eigenvalues clamped at thresh_df) by the
+ * coupled Newton-Schulz iteration on the device.  A metric with an eigenvalue
+ * at or below thresh returns QX_ERR_NUMERICAL (the clamping is not
+ * reproduced).  metric, inv_sqrt, sqrt_metric (may be NULL): [naux][naux]. */
+qx_status qx_metric_inv_sqrt(qx_ctx* ctx, const double* metric, int naux, double thresh, double* inv_sqrt,
+                             double* sqrt_metric);
+
+/* The RI-normalised tensor of the DF tensor build (quasix/quasix/evgw.py:
+ * 1007-1100): lpq[P][p][q] = sum_Q J^-1/2[P][Q] sum_{u,v} C[u][p] (uv|Q)
+ * C[v][q], the lpq every GW and BSE entry point here takes.  Exactly one of
+ * metric (J, then J^-1/2 as qx_metric_inv_sqrt with thresh) and
+ * metric_inv_sqrt (J^-1/2 given) is non-NULL; chol_v (J^1/2, the
+ * reference's chol_v; may be NULL) needs the metric.  j3c_ao
+ * [nao][nao][naux], mo_coeff [nao][nmo], lpq [naux][nmo][nmo]. */
+qx_status qx_build_lpq(qx_ctx* ctx, const double* j3c_ao, const double* mo_coeff, const double* metric,
+                       const double* metric_inv_sqrt, int nao, int nmo, int naux, double thresh, double* lpq,
+                       double* chol_v);
+
 /* ---- bse -------------------------------------------------------------------- */
 typedef struct qx_bse qx_bse;
 /* BSETDAKernel::new (quasix_core/src/bse/kernel.rs:259-337; PyO3
@@ -271,6 +347,34 @@ qx_status qx_bse_davidson(qx_bse* bse, const qx_davidson_config* cfg, double* ei
  * from mo_energy and df_ia (qx_bse_w0) and its dependence is included; with
  * NULL, W0 is held fixed.  W0 must be symmetric. */
 qx_status qx_bse_root_grad(qx_bse* bse, const double* x, const double* mo_energy, double* grad_energy);
+
+/* ---- bse: optical properties ------------------------------------------------- */
+/* compute_transition_dipoles (quasix/quasix/bse_driver.py:249-298) with the
+ * AO dipole integrals given (the reference takes them from PySCF's
+ * int1e_r): mu[i*nvir + a][c] = sum_{m,n} C[m][i] D[c][m][n] C[n][nocc + a].
+ * mo_coeff [nao][nmo], ao_dipoles [3][nao][nao], mu [nocc*nvir][3]. */
+qx_status qx_compute_transition_dipoles(qx_ctx* ctx, const double* mo_coeff, const double* ao_dipoles, int nao,
+                                        int nmo, int nocc, double* mu);
+
+/* compute_oscillator_strengths (quasix_core/src/bse/optical.rs:179-247):
+ * d[n][c] = sum_t X[t][n] mu[t][c], f[n] = 2/3 E_n |d_n|^2, f_sum = sum f.
+ * eigenvectors [n_trans][n_roots], transition_dipoles [n_trans][3];
+ * root_dipoles [n_roots][3] and f_sum may be NULL.  A negative or non-finite
+ * eigenvalue returns QX_ERR_NUMERICAL, as the reference does. */
+qx_status qx_compute_oscillator_strengths(qx_ctx* ctx, const double* eigenvalues, const double* eigenvectors,
+                                          const double* transition_dipoles, int n_trans, int n_roots,
+                                          double* oscillator_strengths, double* root_dipoles, double* f_sum);
+
+/* compute_absorption_spectrum (optical.rs:305-385): intensities[q] = sum_n
+ * f_n L(E_q - E_n) on E_q = e_min + q (e_max - e_min) / (n_points - 1), L =
+ * gamma / (x^2 + gamma^2) (broadening_type 0, Lorentzian) or exp(-x^2 / (2
+ * gamma^2)) (1, Gaussian), gamma = broadening in Hartree.  has_range = 0
+ * picks the reference's automatic range (eigenvalue span padded by max(0.2
+ * span, 5 gamma), clipped at 0). */
+qx_status qx_compute_absorption_spectrum(qx_ctx* ctx, const double* eigenvalues, const double* oscillator_strengths,
+                                         int n_roots, int broadening_type, double broadening, int has_range,
+                                         double e_min, double e_max, int n_points, double* energies,
+                                         double* intensities);
 
 /* W(w=0) = (I - Pi(0))^-1 for the screened-direct kernel, from lpq_ov [naux][nocc][nvir]. */
 qx_status qx_bse_w0(qx_ctx* ctx, const double* mo_energy, const double* lpq_ov, int naux, int nocc,

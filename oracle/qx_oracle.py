@@ -1163,3 +1163,163 @@ def _gs(V: np.ndarray, t: np.ndarray) -> np.ndarray:
     for j in range(V.shape[1]):
         t = t - float(t @ V[:, j]) * V[:, j]
     return t
+
+
+# ---------------------------------------------------------------------------
+# f4: spectral functions (quasix_core/src/analysis/spectral.rs)
+# ---------------------------------------------------------------------------
+def gaussian_broadening(omega, energy, sigma):
+    """spectral.rs:779-784 (scalar form; the reference's AVX2 path uses a fast exp)."""
+    d = np.asarray(omega) - energy
+    return np.exp(-d * d / (2.0 * sigma * sigma)) / (sigma * math.sqrt(2.0 * PI))
+
+
+def lorentzian_broadening(omega, energy, gamma):
+    """spectral.rs:796-799."""
+    d = np.asarray(omega) - energy
+    return (gamma / PI) / (d * d + gamma * gamma)
+
+
+def voigt_profile(omega, energy, sigma, gamma, alpha):
+    """spectral.rs:814-818: (1 - alpha) G + alpha L."""
+    return (1.0 - alpha) * gaussian_broadening(omega, energy, sigma) + alpha * lorentzian_broadening(omega, energy,
+                                                                                                   gamma)
+
+
+def spectral_function(qp_energies, z_factors, omega, gaussian_width=0.1, lorentzian_width=0.05, voigt_mixing=0.5,
+                      fermi_energy=0.0, kind=0):
+    """SpectralAnalyzer::compute_spectral_function (spectral.rs:283-325) with the
+    profile choice of :291-302 (Gaussian below mixing 0.01, Lorentzian above
+    0.99, else Voigt) and, for kind 1 / 2, the state filter and energy shift of
+    generate_pes_spectrum / generate_ipes_spectrum (:557-656).  Returns
+    (weights [nomega], total_weight = sum * (omega[1] - omega[0]))."""
+    e = np.asarray(qp_energies, float)
+    z = np.asarray(z_factors, float)
+    w = np.asarray(omega, float)
+    if kind == 1:
+        m = e <= fermi_energy
+        e, z = fermi_energy - e[m], z[m]
+    elif kind == 2:
+        m = e > fermi_energy
+        e, z = e[m] - fermi_energy, z[m]
+    out = np.zeros_like(w)
+    for ei, zi in zip(e, z):
+        if voigt_mixing < 0.01:
+            p = gaussian_broadening(w, ei, gaussian_width)
+        elif voigt_mixing > 0.99:
+            p = lorentzian_broadening(w, ei, lorentzian_width)
+        else:
+            p = voigt_profile(w, ei, gaussian_width, lorentzian_width, voigt_mixing)
+        out += zi * p
+    dw = w[1] - w[0] if w.shape[0] > 1 else 1.0
+    return out, float(out.sum() * dw)
+
+
+def spectral_function_states(qp_energies, z_factors, omega, eta=0.01):
+    """EvGWResult.spectral_function (quasix/quasix/evgw.py:124-134): per state
+    A[i, w] = Z_i eta / ((w - E_i)^2 + eta^2) / pi."""
+    e = np.asarray(qp_energies, float)[:, None]
+    z = np.asarray(z_factors, float)[:, None]
+    w = np.asarray(omega, float)[None, :]
+    return z * eta / ((w - e) ** 2 + eta ** 2) / PI
+
+
+def spectral_function_pade(coeff, omega_fit, e_ref, sigma_x, vxc, ef, omega, eta):
+    """A_t(w) = (1/pi) G / ((w - e_t - Sx_t + Vxc_t - Re S)^2 + G^2), G = |Im S| + eta,
+    S = pade_thiele(w - ef) of orbital t (correlation_ac.rs:530-566 for S); no
+    reference counterpart for A itself (the reference broadens QP peaks only)."""
+    norbs = coeff.shape[1]
+    out = np.zeros((norbs, len(omega)))
+    for t in range(norbs):
+        for q, w in enumerate(omega):
+            s = pade_thiele(w - ef, omega_fit[t], coeff[:, t])
+            re = w - e_ref[t] - sigma_x[t] + vxc[t] - s.real
+            g = abs(s.imag) + eta
+            out[t, q] = g / (PI * (re * re + g * g))
+    return out
+
+
+# ---------------------------------------------------------------------------
+# f2: BSE optical properties (quasix_core/src/bse/optical.rs)
+# ---------------------------------------------------------------------------
+def compute_transition_dipoles(mo_coeff, ao_dipoles, nocc):
+    """<i|r_c|a> = C_occ^T D_c C_vir, [nocc * nvirt, 3] (quasix/quasix/bse_driver.py:249-298)."""
+    c = np.asarray(mo_coeff, float)
+    out = np.zeros((nocc * (c.shape[1] - nocc), 3))
+    for k in range(3):
+        out[:, k] = (c[:, :nocc].T @ ao_dipoles[k] @ c[:, nocc:]).ravel()
+    return out
+
+
+def compute_oscillator_strengths(eigenvalues, eigenvectors, transition_dipoles):
+    """optical.rs:179-247: d = X^T mu, f_n = 2/3 E_n |d_n|^2, with the
+    reference's validation (dimension mismatch, 3 components, finite and
+    non-negative eigenvalues)."""
+    e = np.asarray(eigenvalues, float)
+    x = np.asarray(eigenvectors, float)
+    mu = np.asarray(transition_dipoles, float)
+    if x.shape[1] != e.shape[0] or x.shape[0] != mu.shape[0] or mu.shape[1] != 3:
+        raise ValueError("dimension mismatch")
+    if not np.all(np.isfinite(e)) or np.any(e < 0.0):
+        raise ValueError("eigenvalues must be finite and non-negative")
+    d = x.T @ mu
+    f = (2.0 / 3.0) * e * np.sum(d * d, axis=1)
+    return f, d, float(f.sum())
+
+
+def absorption_lorentzian(x, gamma):
+    """optical.rs:121-123: gamma / (x^2 + gamma^2)."""
+    return gamma / (x * x + gamma * gamma)
+
+
+def absorption_gaussian(x, sigma):
+    """optical.rs:131-133: exp(-x^2 / (2 sigma^2))."""
+    return np.exp(-0.5 * x * x / (sigma * sigma))
+
+
+def compute_absorption_spectrum(eigenvalues, oscillator_strengths, broadening, gaussian=False, energy_range=None,
+                                n_points=1000):
+    """optical.rs:305-385 (broadening in Hartree; automatic range :332-340)."""
+    e = np.asarray(eigenvalues, float)
+    f = np.asarray(oscillator_strengths, float)
+    if energy_range is None:
+        lo, hi = e.min(), e.max()
+        pad = max((hi - lo) * 0.2, broadening * 5.0)
+        e_min, e_max = max(lo - pad, 0.0), hi + pad
+    else:
+        e_min, e_max = energy_range
+    de = (e_max - e_min) / (n_points - 1) if n_points > 1 else 0.0
+    grid = e_min + np.arange(n_points) * de
+    out = np.zeros(n_points)
+    for en, fn in zip(e, f):
+        x = grid - en
+        out += fn * (absorption_gaussian(x, broadening) if gaussian else absorption_lorentzian(x, broadening))
+    return grid, out
+
+
+# ---------------------------------------------------------------------------
+# f1: density-fitting tensors (quasix/quasix/evgw.py:1007-1100,
+#     quasix_core/src/df/mo_transform.rs:136-282)
+# ---------------------------------------------------------------------------
+def metric_inv_sqrt(metric, thresh_df=1e-10):
+    """J^-1/2 and J^1/2 by eigh with the eigenvalues clamped at thresh_df
+    (evgw.py:1014-1046)."""
+    lam, u = np.linalg.eigh(metric)
+    lam = np.maximum(lam, thresh_df)
+    return (u / np.sqrt(lam)) @ u.T, (u * np.sqrt(lam)) @ u.T
+
+
+def transform_mo_3center(j3c_ao, c_occ, c_vir):
+    """(ia|P) as [nocc*nvir, naux] (mo_transform.rs:136-282)."""
+    out = np.einsum("uvP,ui,va->iaP", j3c_ao, c_occ, c_vir, optimize=True)
+    return out.reshape(c_occ.shape[1] * c_vir.shape[1], j3c_ao.shape[2])
+
+
+def build_lpq(j3c_ao, mo_coeff, metric, thresh_df=1e-10):
+    """lpq[P, p, q] = sum_Q J^-1/2[Q, P] (C^T (uv|Q) C)[p, q] and chol_v = J^1/2:
+    the J^-1/2 transformation of the AO integrals (evgw.py:1041-1050) followed
+    by the per-P MO transform (:1068-1083), in the reference's order."""
+    jm, jp = metric_inv_sqrt(metric, thresh_df)
+    int3c = np.einsum("uvQ,QP->uvP", j3c_ao, jm, optimize=True)
+    lpq = np.einsum("up,uvP,vq->Ppq", mo_coeff, int3c, mo_coeff, optimize=True)
+    return lpq, jp

@@ -4,9 +4,11 @@ Drop-in entry points with the reference's names and argument meaning:
 ``run_evgw`` / ``evgw`` (quasix/src/evgw.rs), ``get_sigma_diag`` and friends
 (quasix_core/src/selfenergy/correlation_ac.rs), ``g0w0_cd``, and the BSE-TDA
 ``bse.BSETDAKernel`` / ``run_bse_tda`` (quasix/src/bse.rs, quasix/quasix/bse_driver.py),
+the spectral functions of quasix_core/src/analysis/spectral.rs (``spectral``),
+the density-fitting tensor build (``df``),
 and the adjoint of the CD QP roots (``grad``), which the reference does not have.
 """
-from . import _native, bse, grad
+from . import _native, bse, df, grad, spectral
 from .bse import BSETDAConfig, BSETDAKernel, BSETDAResult, DavidsonConfig, run_bse_tda
 from .gw import (ac_pade_thiele_diag, compute_epsilon_inverse_minus_identity, compute_exchange_diag,
                  cd_sigma, compute_polarizability_p0, evgw, g0w0_cd, g0w0_cd_batch, get_rho_response, get_rho_response_batch,
@@ -14,7 +16,7 @@ from .gw import (ac_pade_thiele_diag, compute_epsilon_inverse_minus_identity, co
 from .grad import G0W0CDQP, g0w0_cd_grad, g0w0_cd_qp
 
 __all__ = [
-    "bse", "BSETDAConfig", "BSETDAKernel", "BSETDAResult", "DavidsonConfig", "run_bse_tda",
+    "bse", "df", "spectral", "BSETDAConfig", "BSETDAKernel", "BSETDAResult", "DavidsonConfig", "run_bse_tda",
     "ac_pade_thiele_diag", "compute_epsilon_inverse_minus_identity", "compute_exchange_diag",
     "cd_sigma", "compute_polarizability_p0", "evgw", "g0w0_cd", "g0w0_cd_batch", "get_rho_response", "get_rho_response_batch",
     "get_scaled_legendre_roots", "get_sigma_diag", "pade_thiele", "run_evgw", "run_evgw_blocks",

@@ -84,10 +84,16 @@ SIGNATURES = {
     "qx_get_rho_response": (C.c_int, [_vp, C.c_int, _vp, _vp, _vp, C.c_int, C.c_int, C.c_int, C.c_int, _vp]),
     "qx_screened_interaction": (C.c_int, [_vp, C.c_int, C.c_int, _vp, _vp]),
     "qx_screened_interaction_noalloc": (C.c_int, [_vp, C.c_int, C.c_int, _vp, _vp]),
+    "qx_eps_at_least_identity": (C.c_int, [_vp, C.c_int, C.c_int, C.c_double]),
     "qx_get_sigma_diag": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double,
                                     C.c_double, C.c_int, _vp, _vp, C.c_int, _ip]),
     "qx_ac_pade_thiele_diag": (C.c_int, [_vp, C.c_int, C.c_int, _vp, _vp, C.c_int, _vp, _vp, C.c_int, _ip]),
-    "qx_pade_thiele": (C.c_int, [C.c_int, _vp, _vp, C.c_int, _vp, _vp]),
+    "qx_pade_thiele": (C.c_int, [_vp, C.c_int, _vp, _vp, C.c_int, _vp, _vp]),
+    "qx_spectral_function": (C.c_int, [_vp, _vp, _vp, C.c_int, C.c_double, C.c_int, _vp, C.c_int, C.c_double,
+                                       C.c_double, C.c_double, _vp, _dp]),
+    "qx_spectral_function_states": (C.c_int, [_vp, _vp, _vp, C.c_int, _vp, C.c_int, C.c_double, _vp]),
+    "qx_spectral_function_pade": (C.c_int, [_vp, C.c_int, C.c_int, _vp, _vp, _vp, _vp, _vp, C.c_double, _vp,
+                                            C.c_int, C.c_double, _vp]),
     "qx_compute_exchange_diag": (C.c_int, [_vp, _vp, C.c_int, C.c_int, C.c_int, _vp]),
     "qx_evgw_config_default": (None, [C.POINTER(EvgwConfig)]),
     "qx_evgw": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int, C.c_int, C.c_int, C.POINTER(EvgwConfig),
@@ -108,6 +114,13 @@ SIGNATURES = {
     "qx_bse_davidson": (C.c_int, [_vp, C.POINTER(DavidsonConfig), _vp, _vp, _vp, _vp, _ip]),
     "qx_bse_root_grad": (C.c_int, [_vp, _vp, _vp, _vp]),
     "qx_bse_w0": (C.c_int, [_vp, _vp, _vp, C.c_int, C.c_int, C.c_int, _vp]),
+    "qx_compute_transition_dipoles": (C.c_int, [_vp, _vp, _vp, C.c_int, C.c_int, C.c_int, _vp]),
+    "qx_transform_mo_3center": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int, C.c_int, C.c_int, C.c_int, _vp]),
+    "qx_metric_inv_sqrt": (C.c_int, [_vp, _vp, C.c_int, C.c_double, _vp, _vp]),
+    "qx_build_lpq": (C.c_int, [_vp, _vp, _vp, _vp, _vp, C.c_int, C.c_int, C.c_int, C.c_double, _vp, _vp]),
+    "qx_compute_oscillator_strengths": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int, C.c_int, _vp, _vp, _dp]),
+    "qx_compute_absorption_spectrum": (C.c_int, [_vp, _vp, _vp, C.c_int, C.c_int, C.c_double, C.c_int, C.c_double,
+                                                 C.c_double, C.c_int, _vp, _vp]),
 }
 
 _lib = None

@@ -7,6 +7,10 @@
   quasix/quasix/bse_driver.py:55-155, 782-982, taking the density-fitted
   tensors directly (the reference builds them from PySCF, which is not part of
   this path).  The screened-direct kernel uses W(w=0) = (I - Pi(0))^-1.
+* ``compute_transition_dipoles`` / ``compute_oscillator_strengths`` /
+  ``compute_absorption_spectrum``: bse_driver.py:249-298 (with the AO dipole
+  integrals given) and the ``quasix.bse`` functions of quasix/src/bse.rs:413-565
+  over quasix_core/src/bse/optical.rs.
 
 All arithmetic runs in libqxgpu; there is no CPU fallback.
 """
@@ -154,6 +158,66 @@ def screened_w0(mo_energy, lpq_ov, device: int = 0) -> np.ndarray:
     return out
 
 
+def compute_transition_dipoles(mo_coeff, ao_dipoles, nocc: int, device: int = 0) -> np.ndarray:
+    """<i|r|a> in the MO basis, [nocc * nvirt, 3] with row i * nvirt + a
+    (bse_driver.py:249-298); ``ao_dipoles`` [3, nao, nao] are the AO integrals
+    the reference takes from PySCF's ``int1e_r``."""
+    c, d = _f64(mo_coeff), _f64(ao_dipoles)
+    nao, nmo = c.shape
+    if d.shape != (3, nao, nao):
+        raise ValueError(f"ao_dipoles must be [3, {nao}, {nao}], got {list(d.shape)}")
+    ctx = N.context(device)
+    out = np.zeros((int(nocc) * (nmo - int(nocc)), 3))
+    ctx.check(ctx.lib.qx_compute_transition_dipoles(ctx.handle, N.ptr(c), N.ptr(d), nao, nmo, int(nocc), N.ptr(out)))
+    return out
+
+
+def compute_oscillator_strengths(eigenvalues, eigenvectors, transition_dipoles, device: int = 0) -> Dict[str, Any]:
+    """quasix.bse.compute_oscillator_strengths (quasix/src/bse.rs:413-459,
+    optical.rs:179-247): {oscillator_strengths [n_roots], transition_dipoles
+    [n_roots, 3], f_sum}."""
+    e, x, mu = _f64(eigenvalues), _f64(eigenvectors), _f64(transition_dipoles)
+    if x.ndim != 2 or x.shape[1] != e.shape[0]:
+        raise ValueError(f"Eigenvalues length {e.shape[0]} != eigenvectors columns {x.shape[-1]}")
+    if mu.ndim != 2 or mu.shape[0] != x.shape[0]:
+        raise ValueError(f"Eigenvectors rows {x.shape[0]} != transition_dipoles rows {mu.shape[0]}")
+    if mu.shape[1] != 3:
+        raise ValueError(f"Transition dipoles must have 3 components (x,y,z), got {mu.shape[1]}")
+    ctx = N.context(device)
+    f = np.zeros(e.shape[0])
+    d = np.zeros((e.shape[0], 3))
+    fs = C.c_double(0.0)
+    st = ctx.lib.qx_compute_oscillator_strengths(ctx.handle, N.ptr(e), N.ptr(x), N.ptr(mu), x.shape[0], e.shape[0],
+                                                 N.ptr(f), N.ptr(d), C.byref(fs))
+    if st != 0:
+        raise RuntimeError("Failed to compute oscillator strengths: "
+                           + ctx.lib.qx_last_error(ctx.handle).decode(errors="replace"))
+    return {"oscillator_strengths": f, "transition_dipoles": d, "f_sum": fs.value}
+
+
+def compute_absorption_spectrum(eigenvalues, oscillator_strengths, energy_range=None, n_points: int = 1000,
+                                broadening: float = 0.1, broadening_type: str = "lorentzian",
+                                device: int = 0) -> Dict[str, Any]:
+    """quasix.bse.compute_absorption_spectrum (quasix/src/bse.rs:461-565,
+    optical.rs:305-385); ``broadening`` in eV, energies in Hartree."""
+    e, f = _f64(eigenvalues), _f64(oscillator_strengths)
+    if f.shape != e.shape:
+        raise ValueError(f"Eigenvalues length {e.shape[0]} != oscillator_strengths length {f.shape[0]}")
+    bt = broadening_type.lower()
+    if bt not in ("lorentzian", "gaussian"):
+        raise ValueError(f"Unknown broadening type: {broadening_type}. Use 'lorentzian' or 'gaussian'")
+    ctx = N.context(device)
+    w = np.zeros(int(n_points))
+    out = np.zeros(int(n_points))
+    lo, hi = (0.0, 0.0) if energy_range is None else (float(energy_range[0]), float(energy_range[1]))
+    ctx.check(ctx.lib.qx_compute_absorption_spectrum(ctx.handle, N.ptr(e), N.ptr(f), e.shape[0],
+                                                     0 if bt == "lorentzian" else 1, broadening / HARTREE_TO_EV,
+                                                     0 if energy_range is None else 1, lo, hi, int(n_points),
+                                                     N.ptr(w), N.ptr(out)))
+    return {"energies": w, "energies_eV": w * HARTREE_TO_EV, "intensities": out, "broadening_eV": broadening,
+            "broadening_type": bt}
+
+
 @dataclass
 class BSETDAConfig:
     """quasix/quasix/bse_driver.py:55-104."""
@@ -178,8 +242,9 @@ class BSETDAConfig:
 
 @dataclass
 class BSETDAResult:
-    """quasix/quasix/bse_driver.py:106-155 (oscillator strengths need dipole
-    integrals from PySCF and are returned as zeros)."""
+    """quasix/quasix/bse_driver.py:106-155.  Without dipole integrals (the
+    reference takes them from PySCF) the oscillator strengths, transition
+    dipoles and f_sum are NaN, not zeros."""
     excitation_energies_Ha: np.ndarray
     excitation_energies_eV: np.ndarray
     oscillator_strengths: np.ndarray
@@ -206,12 +271,16 @@ class BSETDAResult:
 
 def run_bse_tda(mol=None, mf=None, nstates: int = 5, tol: float = 1e-6, max_iter: int = 100, auxbasis=None,
                 qp_energies=None, verbose: bool = True, config: Optional[BSETDAConfig] = None, *, lpq=None,
-                mo_energy=None, nocc: Optional[int] = None, w0=None, device: int = 0, **kwargs) -> BSETDAResult:
+                mo_energy=None, nocc: Optional[int] = None, w0=None, transition_dipoles=None, mo_coeff=None,
+                ao_dipoles=None, device: int = 0, **kwargs) -> BSETDAResult:
     """Drop-in for quasix.run_bse_tda (bse_driver.py:782-982) on given DF tensors.
 
     ``lpq`` is the RI-normalized [naux, nmo, nmo] tensor, ``mo_energy`` the
     mean-field energies, ``qp_energies`` optional QP energies for the
-    diagonal.  W0 defaults to (I - Pi(0))^-1 built from ``mo_energy``."""
+    diagonal.  W0 defaults to (I - Pi(0))^-1 built from ``mo_energy``.
+    Oscillator strengths (bse_driver.py:938-959) need the transition dipoles
+    <i|r|a> [nocc * nvirt, 3], given directly or as ``mo_coeff`` [nao, nmo]
+    plus ``ao_dipoles`` [3, nao, nao]; without them they are NaN."""
     if mol is not None or mf is not None:
         raise NotImplementedError("PySCF mean-field objects are outside this path; pass lpq/mo_energy/nocc")
     if config is None:
@@ -235,9 +304,19 @@ def run_bse_tda(mol=None, mf=None, nstates: int = 5, tol: float = 1e-6, max_iter
     r = k.solve_davidson_with_config(DavidsonConfig(config.nstates, config.max_iter, config.max_space, config.tol))
     t2 = time.perf_counter()
     ev = r["eigenvalues"]
+    timing = {"setup": t1 - t0, "davidson": t2 - t1}
+    if transition_dipoles is None and mo_coeff is not None and ao_dipoles is not None:
+        transition_dipoles = compute_transition_dipoles(mo_coeff, ao_dipoles, nocc, device=device)
+        timing["dipoles"] = time.perf_counter() - t2
+    if transition_dipoles is not None:
+        opt = compute_oscillator_strengths(ev, r["eigenvectors"], transition_dipoles, device=device)
+        osc, tdip, f_sum = opt["oscillator_strengths"], opt["transition_dipoles"], opt["f_sum"]
+    else:
+        osc, tdip, f_sum = np.full_like(ev, np.nan), np.full((len(ev), 3), np.nan), float("nan")
+    timing["total"] = time.perf_counter() - t0
     return BSETDAResult(excitation_energies_Ha=ev, excitation_energies_eV=ev * HARTREE_TO_EV,
-                        oscillator_strengths=np.zeros_like(ev), transition_dipoles=np.zeros((len(ev), 3)),
+                        oscillator_strengths=osc, transition_dipoles=tdip,
                         eigenvectors=r["eigenvectors"], converged=r["all_converged"],
                         n_converged=int(sum(r["converged"])), n_iterations=r["iterations"],
                         residual_norms=r["residual_norms"], config=config,
-                        timing={"setup": t1 - t0, "davidson": t2 - t1}, f_sum=0.0, nocc=nocc, nvirt=nvir)
+                        timing=timing, f_sum=f_sum, nocc=nocc, nvirt=nvir)

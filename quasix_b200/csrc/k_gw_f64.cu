@@ -121,7 +121,11 @@ constexpr int SWEEP_NB = 128;
 // j; pivot rows and columns travel by shuffles, so a pivot step costs no block
 // barrier), then the whole CTA applies the rank-32 update to the rest of the
 // 128 x 128 block through shared memory.
-__device__ __forceinline__ void sweep32_warp(double* S, int q0, int lane, bool& bad_any) {
+// A pivot at or below tol (0 unguarded: an exact zero), or a non-finite one,
+// sets bad_any.  GUARD: gm also takes max |entry| of the columns not yet
+// swept after each pivot step (the element growth of the elimination).
+template <bool GUARD>
+__device__ __forceinline__ void sweep32_warp(double* S, int q0, int lane, bool& bad_any, double tol, double& gm) {
   // c[k] holds S[(p + k) % 32][lane] at pivot step p: the pivot row is always
   // c[0] and the array rotates by one after each step, so every register index
   // is a compile-time constant without unrolling the pivot loop.
@@ -131,7 +135,7 @@ __device__ __forceinline__ void sweep32_warp(double* S, int q0, int lane, bool& 
 #pragma unroll 1
   for (int p = 0; p < 32; ++p) {
     const double d = __shfl_sync(0xffffffffu, c[0], p);
-    const bool bad = !(fabs(d) > 0.0) || !isfinite(d);
+    const bool bad = !(fabs(d) > tol) || !isfinite(d);
     bad_any |= bad;
     const double inv = bad ? 0.0 : 1.0 / d;
     const double rj = c[0] * inv;  // S[p][lane] / d
@@ -142,6 +146,10 @@ __device__ __forceinline__ void sweep32_warp(double* S, int q0, int lane, bool& 
       c[i] = piv ? ci * inv : c[i] - ci * rj;
     }
     c[0] = piv ? -inv : rj;
+    if (GUARD && lane > p) {
+#pragma unroll
+      for (int i = 0; i < 32; ++i) gm = fmax(gm, isfinite(c[i]) ? fabs(c[i]) : INFINITY);
+    }
     const double t = c[0];
 #pragma unroll
     for (int i = 0; i < 31; ++i) c[i] = c[i + 1];
@@ -152,19 +160,27 @@ __device__ __forceinline__ void sweep32_warp(double* S, int q0, int lane, bool& 
 }
 
 // D = -(A_KK)^-1 for the kb x kb diagonal block whose first element is at
-// Akk (row stride ldn), zero outside kb x kb; *status_w = 1 when a pivot
-// vanishes.  512 threads; dynamic shared memory (128 * 128 + 128 * 33) doubles.
+// Akk (row stride ldn), zero outside kb x kb; *status_w = 1 when a pivot is at
+// or below tol (guarded sweep) or vanishes.  growth_w (guarded sweep, else
+// null): max |A_KK| of the not-yet-swept block joins it.  512 threads;
+// dynamic shared memory (128 * 128 + 128 * 33) doubles.
+__device__ __forceinline__ void block_amax(double m, double* red, unsigned long long* out);
+template <bool GUARD>
 __device__ __forceinline__ void sweep_diag_body(const double* __restrict__ Akk, int ldn, int kb,
-                                                double* __restrict__ D, int* __restrict__ status_w) {
+                                                double* __restrict__ D, int* __restrict__ status_w, double tol,
+                                                unsigned long long* growth_w) {
   static_assert(SWEEP_NB == 128, "thread mapping assumes 128 columns");
   constexpr int TLD = 33;                       // padded row stride of T
   extern __shared__ double S[];                 // [128][128]
   double* Tb = S + SWEEP_NB * SWEEP_NB;         // [128][33]
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int j = tid & 127, r0 = tid >> 7;
+  double gm = 0.0;  // GUARD: max |entry| met in the unswept part
   for (int k = 0; k < 32; ++k) {
     const int i = r0 + 4 * k;
-    S[i * SWEEP_NB + j] = (i < kb && j < kb) ? Akk[(size_t)i * ldn + j] : (i == j ? 1.0 : 0.0);
+    const double v = (i < kb && j < kb) ? Akk[(size_t)i * ldn + j] : (i == j ? 1.0 : 0.0);
+    S[i * SWEEP_NB + j] = v;
+    if (GUARD) gm = fmax(gm, isfinite(v) ? fabs(v) : INFINITY);
   }
   bool bad_any = false;
   // Sub-blocks past kb are identity padding with no coupling to the block:
@@ -174,7 +190,7 @@ __device__ __forceinline__ void sweep_diag_body(const double* __restrict__ Akk, 
   for (int sb = 0; sb < nsb; ++sb) {
     const int q0 = 32 * sb;
     __syncthreads();
-    if (warp == 0) sweep32_warp(S, q0, lane, bad_any);
+    if (warp == 0) sweep32_warp<GUARD>(S, q0, lane, bad_any, tol, gm);
     __syncthreads();
     // Both products below use register tiles (thread = 4 rows x 2 or 8
     // columns), so each shared-memory operand feeds several FMAs.
@@ -238,8 +254,15 @@ __device__ __forceinline__ void sweep_diag_body(const double* __restrict__ Akk, 
 #pragma unroll
         for (int v = 0; v < 4; ++v) {
           if (32 * v == q0) continue;
-          S[(rb + i) * SWEEP_NB + 32 * v + cb] -= acc[i][2 * v];
-          S[(rb + i) * SWEEP_NB + 32 * v + cb + 1] -= acc[i][2 * v + 1];
+          const double s0 = S[(rb + i) * SWEEP_NB + 32 * v + cb] - acc[i][2 * v];
+          const double s1 = S[(rb + i) * SWEEP_NB + 32 * v + cb + 1] - acc[i][2 * v + 1];
+          S[(rb + i) * SWEEP_NB + 32 * v + cb] = s0;
+          S[(rb + i) * SWEEP_NB + 32 * v + cb + 1] = s1;
+          // Rows and columns past this sub-block: the Schur complement.
+          if (GUARD && rb + i >= q0 + 32 && 32 * v > q0) {
+            gm = fmax(gm, isfinite(s0) ? fabs(s0) : INFINITY);
+            gm = fmax(gm, isfinite(s1) ? fabs(s1) : INFINITY);
+          }
         }
       }
     }
@@ -256,6 +279,10 @@ __device__ __forceinline__ void sweep_diag_body(const double* __restrict__ Akk, 
   }
   __syncthreads();
   if (lane == 0 && warp == 0 && bad_any) atomicExch(status_w, 1);
+  if (GUARD && growth_w) {
+    __shared__ double gred[16];
+    block_amax(gm, gred, growth_w);
+  }
   // D = -S, zero outside the kb x kb block.
   for (int k = 0; k < 32; ++k) {
     const int i = r0 + 4 * k;
@@ -263,11 +290,21 @@ __device__ __forceinline__ void sweep_diag_body(const double* __restrict__ Akk, 
   }
 }
 
+// Pivot tolerance of matrix w: kGuardPivot * max|eps_w| in a guarded sweep
+// (gamax: the words of the guard's copy kernel), an exact zero otherwise.
+__device__ __forceinline__ double guard_tol(const unsigned long long* gamax, int w) {
+  return gamax ? kGuardPivot * __longlong_as_double((long long)gamax[w]) : 0.0;
+}
+
+template <bool GUARD>
 __global__ void __launch_bounds__(512) k_sweep_diag(const double* __restrict__ M, int ldn, size_t stride, int k0,
-                                                    int kb, double* __restrict__ Dp, int* __restrict__ status) {
+                                                    int kb, double* __restrict__ Dp, int* __restrict__ status,
+                                                    const unsigned long long* __restrict__ gamax,
+                                                    unsigned long long* __restrict__ growth) {
   const int w = blockIdx.x;
-  sweep_diag_body(M + (size_t)w * stride + (size_t)k0 * ldn + k0, ldn, kb, Dp + (size_t)w * SWEEP_NB * SWEEP_NB,
-                  status + w);
+  sweep_diag_body<GUARD>(M + (size_t)w * stride + (size_t)k0 * ldn + k0, ldn, kb,
+                         Dp + (size_t)w * SWEEP_NB * SWEEP_NB, status + w, guard_tol(gamax, w),
+                         growth ? growth + w : nullptr);
 }
 
 using PanelTile = F64Tile<64, 64, 2, 2, 3>;
@@ -407,12 +444,16 @@ __global__ void __launch_bounds__(SweepTile::THREADS) k_sweep_update(double* __r
 // same element: D's lower triangle serves both, so the stored value does not
 // depend on which write lands last.
 constexpr int kWriteRows = 32;
+// growth (guarded sweep, else null): max |P| over the rows not yet swept
+// (r >= k0 + kb, entries of the Schur complement) joins it.
 __device__ __forceinline__ void sweep_write_tile(double* __restrict__ A, int n, int ldn, int k0, int kb,
                                                  const double* __restrict__ Tw, double* __restrict__ Pw,
-                                                 const double* __restrict__ D, int r0, unsigned long long* amax) {
+                                                 const double* __restrict__ D, int r0, unsigned long long* amax,
+                                                 unsigned long long* growth) {
   __shared__ double S[kWriteRows][SWEEP_NB + 1];
   __shared__ double red[8];
   double mx = 0.0;  // max|P| of the tile (amax, optional: the bound of a later split of P)
+  double gx = 0.0;  // the same over the unswept rows
   for (int e = threadIdx.x; e < kWriteRows * SWEEP_NB; e += blockDim.x) {
     const int rr = e / SWEEP_NB, q = e % SWEEP_NB, r = r0 + rr;
     if (r >= n) continue;
@@ -424,6 +465,7 @@ __device__ __forceinline__ void sweep_write_tile(double* __restrict__ A, int n, 
     const double old = in_k ? 0.0 : A[(size_t)r * ldn + k0 + q];
     Pw[(size_t)r * SWEEP_NB + q] = old;
     mx = fmax(mx, fabs(old));
+    if (r >= k0 + kb) gx = fmax(gx, isfinite(old) ? fabs(old) : INFINITY);
     const int a = r - k0;
     const double v = in_k ? -D[max(a, q) * SWEEP_NB + min(a, q)] : Tw[(size_t)r * SWEEP_NB + q];
     A[(size_t)r * ldn + k0 + q] = v;
@@ -435,15 +477,20 @@ __device__ __forceinline__ void sweep_write_tile(double* __restrict__ A, int n, 
     if (q < kb && r < n) A[(size_t)(k0 + q) * ldn + r] = S[rr][q];
   }
   if (amax) block_amax(mx, red, amax);
+  if (growth) {
+    __syncthreads();  // red is reused
+    block_amax(gx, red, growth);
+  }
 }
 
 __global__ void __launch_bounds__(256) k_sweep_write(double* __restrict__ M, int n, int ldn, size_t stride, int k0,
                                                      int kb, const double* __restrict__ Tp, double* __restrict__ Pp,
                                                      size_t pstride, const double* __restrict__ Dp,
-                                                     unsigned long long* amax) {
+                                                     unsigned long long* amax, unsigned long long* growth) {
   const int w = blockIdx.y;
   sweep_write_tile(M + (size_t)w * stride, n, ldn, k0, kb, Tp + (size_t)w * pstride, Pp + (size_t)w * pstride,
-                   Dp + (size_t)w * SWEEP_NB * SWEEP_NB, blockIdx.x * kWriteRows, amax ? amax + w : nullptr);
+                   Dp + (size_t)w * SWEEP_NB * SWEEP_NB, blockIdx.x * kWriteRows, amax ? amax + w : nullptr,
+                   growth ? growth + w : nullptr);
 }
 
 // After the last sweep M = -eps^-1; Wc = eps^-1 - I = -M - I.  A frequency
@@ -470,8 +517,10 @@ __global__ void k_finish_wc(double* __restrict__ M, int n, int ldn, size_t strid
 static_assert(kSweepPanelCols == SWEEP_NB, "panel width");
 
 // Grouped forms of the sweep kernels (defined below).
+template <bool GUARD>
 __global__ void k_gsweep_diag(const GMat* __restrict__ mats, int k0, double* __restrict__ Dp,
-                              int* __restrict__ status);
+                              int* __restrict__ status, const unsigned long long* __restrict__ gamax,
+                              unsigned long long* __restrict__ growth);
 __global__ void k_gsweep_tpanel(const GMat* __restrict__ mats, const int* __restrict__ pre, int count, int k0,
                                 const double* __restrict__ Dp, double* __restrict__ Tcat, unsigned long long* amax);
 __global__ void k_gsweep_update(const GMat* __restrict__ mats, const int* __restrict__ pre, int count, int k0,
@@ -479,10 +528,12 @@ __global__ void k_gsweep_update(const GMat* __restrict__ mats, const int* __rest
 
 void sweep_set_attributes() {
   const int diag_smem = (int)((SWEEP_NB * SWEEP_NB + SWEEP_NB * 33) * sizeof(double));
-  QX_CUDA(cudaFuncSetAttribute(k_sweep_diag, cudaFuncAttributeMaxDynamicSharedMemorySize, diag_smem));
+  QX_CUDA(cudaFuncSetAttribute(k_sweep_diag<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, diag_smem));
+  QX_CUDA(cudaFuncSetAttribute(k_sweep_diag<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, diag_smem));
   QX_CUDA(cudaFuncSetAttribute(k_sweep_tpanel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PanelTile::SMEM));
   QX_CUDA(cudaFuncSetAttribute(k_sweep_update, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SweepTile::SMEM));
-  QX_CUDA(cudaFuncSetAttribute(k_gsweep_diag, cudaFuncAttributeMaxDynamicSharedMemorySize, diag_smem));
+  QX_CUDA(cudaFuncSetAttribute(k_gsweep_diag<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, diag_smem));
+  QX_CUDA(cudaFuncSetAttribute(k_gsweep_diag<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, diag_smem));
   QX_CUDA(cudaFuncSetAttribute(k_gsweep_tpanel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PanelTile::SMEM));
   QX_CUDA(cudaFuncSetAttribute(k_gsweep_update, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SweepTile::SMEM));
 }
@@ -494,22 +545,45 @@ static void sweep_attributes_once(int device) {
 
 // One block step of the sweep on stream st: D, T, then P and the panel write.
 // amax_t / amax_p (optional): [nw] words that receive max|T|, max|P| per
-// matrix (zeroed here first) for the split of the trailing update.
+// matrix (zeroed here first) for the split of the trailing update.  gs
+// (guarded sweep, else null): its max|eps| words set the pivot tolerance and
+// its growth words receive the unswept maxima.
 static void sweep_front(qx_ctx* ctx, cudaStream_t st, double* eps, int n, int ldn, size_t stride, int nw, int k0,
                         int kb, double* Tp, double* Dp, double* Pp, size_t pstride, int* status,
-                        unsigned long long* amax_t = nullptr, unsigned long long* amax_p = nullptr) {
+                        unsigned long long* amax_t = nullptr, unsigned long long* amax_p = nullptr,
+                        const GuardSet* gs = nullptr) {
   if (amax_t) QX_CUDA(cudaMemsetAsync(amax_t, 0, nw * sizeof(unsigned long long), st));
   if (amax_p) QX_CUDA(cudaMemsetAsync(amax_p, 0, nw * sizeof(unsigned long long), st));
   const int diag_smem = (SWEEP_NB * SWEEP_NB + SWEEP_NB * 33) * sizeof(double);
-  k_sweep_diag<<<nw, 512, diag_smem, st>>>(eps, ldn, stride, k0, kb, Dp, status);
+  unsigned long long* gamax = gs ? gs->amax : nullptr;
+  unsigned long long* growth = gs ? gs->growth : nullptr;
+  if (gs)
+    k_sweep_diag<true><<<nw, 512, diag_smem, st>>>(eps, ldn, stride, k0, kb, Dp, status, gamax, growth);
+  else
+    k_sweep_diag<false><<<nw, 512, diag_smem, st>>>(eps, ldn, stride, k0, kb, Dp, status, nullptr, nullptr);
   check_launch(ctx);
   dim3 tg(ceil_div(n, PanelTile::BM), ceil_div(kb, PanelTile::BN), nw);
   k_sweep_tpanel<<<tg, PanelTile::THREADS, PanelTile::SMEM, st>>>(eps, n, ldn, stride, k0, kb, Dp, Tp, pstride,
                                                                    amax_t);
   check_launch(ctx);
   dim3 wg(ceil_div(n, kWriteRows), nw);
-  k_sweep_write<<<wg, 256, 0, st>>>(eps, n, ldn, stride, k0, kb, Tp, Pp, pstride, Dp, amax_p);
+  k_sweep_write<<<wg, 256, 0, st>>>(eps, n, ldn, stride, k0, kb, Tp, Pp, pstride, Dp, amax_p, growth);
   check_launch(ctx);
+}
+
+// The guarded matrices of a uniform sweep: all nw of them.
+static void guard_uniform(GuardSet& gs, double* eps, int n, int ldn, size_t stride, int nw, int* status) {
+  gs.nall = nw;
+  gs.mats.resize(nw);
+  for (int w = 0; w < nw; ++w) {
+    GuardMat& g = gs.mats[w];
+    g = GuardMat{};
+    g.M = eps + (size_t)w * stride;
+    g.n = n;
+    g.ldn = ldn;
+    g.idx = w;
+    g.status = status + w;
+  }
 }
 
 static void sweep_update(qx_ctx* ctx, cudaStream_t st, double* eps, int n, int ldn, size_t stride, int nw, int k0,
@@ -521,8 +595,9 @@ static void sweep_update(qx_ctx* ctx, cudaStream_t st, double* eps, int n, int l
   check_launch(ctx);
 }
 
-void launch_invert_wc(qx_ctx* ctx, double* eps, int n, int ldn, size_t stride, int nw, int half_lower,
+void launch_invert_wc(qx_ctx* ctx, double* eps, int n, int ldn, size_t stride, int nw, int guard, int half_lower,
                       int split_update) {
+  QX_REQUIRE(nw >= 1 && nw <= 65535, QX_ERR_INVALID_INPUT, "%d matrices in one sweep (1 to 65535)", nw);
   const size_t pstride = (size_t)n * SWEEP_NB;
   const size_t dsz = (size_t)nw * SWEEP_NB * SWEEP_NB;
   DevBuf& pan = ctx->ws[WS_PANEL];
@@ -540,6 +615,15 @@ void launch_invert_wc(qx_ctx* ctx, double* eps, int n, int ldn, size_t stride, i
   int* status = status_words(ctx, nw);
   QX_CUDA(cudaMemsetAsync(status, 0, nw * sizeof(int), ctx->stream));
   sweep_attributes_once(ctx->device);
+  GuardSet gs;
+  if (guard) {
+    guard_uniform(gs, eps, n, ldn, stride, nw, status);
+    DevBuf& gb = ctx->ws[WS_GUARD];
+    gb.reserve(guard_bytes(n, ldn, nw));
+    guard_layout(gs, gb.ptr, gb.bytes);
+    guard_begin(ctx, gs);
+  }
+  const GuardSet* gp = guard ? &gs : nullptr;
   const int nsteps = ceil_div(n, SWEEP_NB);
   // Split form: panel splits (two steps in flight) and one tcgen05 error word
   // per update launch, zeroed here on the context stream.
@@ -554,7 +638,7 @@ void launch_invert_wc(qx_ctx* ctx, double* eps, int n, int ldn, size_t stride, i
     QX_CUDA(cudaMemsetAsync(tc_err, 0, 2 * nsteps * sizeof(int), ctx->stream));
   }
   if (nsteps == 1) {
-    sweep_front(ctx, ctx->stream, eps, n, ldn, stride, nw, 0, n, T0, D0, P0, pstride, status);
+    sweep_front(ctx, ctx->stream, eps, n, ldn, stride, nw, 0, n, T0, D0, P0, pstride, status, nullptr, nullptr, gp);
   } else {
     // Look-ahead: critical chain (D, T, write, next-block update) on a
     // high-priority stream, the remaining trailing update on a low-priority one.
@@ -576,7 +660,8 @@ void launch_invert_wc(qx_ctx* ctx, double* eps, int n, int ldn, size_t stride, i
       const int k0 = step * SWEEP_NB, kb = min(SWEEP_NB, n - k0);
       const int b = step & 1;
       sweep_front(ctx, s0, eps, n, ldn, stride, nw, k0, kb, Tb[b], Db[b], Pb[b], pstride, status,
-                  tc ? split_amax_words(ctx, 3 + 2 * b) : nullptr, tc ? split_amax_words(ctx, 4 + 2 * b) : nullptr);
+                  tc ? split_amax_words(ctx, 3 + 2 * b) : nullptr, tc ? split_amax_words(ctx, 4 + 2 * b) : nullptr,
+                  gp);
       SweepSplit sp{};
       if (tc) sp = launch_sweep_split(ctx, s0, Tb[b], Pb[b], n, kb, nw, b, split_base);
       // The previous step's trailing update must be done before this step's
@@ -604,6 +689,8 @@ void launch_invert_wc(qx_ctx* ctx, double* eps, int n, int ldn, size_t stride, i
     QX_CUDA(cudaEventRecord(ev_done, s0));
     QX_CUDA(cudaStreamWaitEvent(ctx->stream, ev_done, 0));
   }
+  // Guarded: the flagged matrices are inverted again with pivoting.
+  if (guard) guard_end(ctx, gs);
   dim3 fg(n, nw);
   k_finish_wc<<<fg, 256, 0, ctx->stream>>>(eps, n, ldn, stride, status, half_lower);
   check_launch(ctx);
@@ -612,13 +699,21 @@ void launch_invert_wc(qx_ctx* ctx, double* eps, int n, int ldn, size_t stride, i
 }
 
 void launch_invert_wc_panels(qx_ctx* ctx, double* eps, int n, int ldn, size_t stride, int nw, double* Tp,
-                             double* Dp, double* Pp, int* status) {
+                             double* Dp, double* Pp, int* status, void* guard_mem, size_t guard_mem_bytes) {
   const size_t pstride = (size_t)n * SWEEP_NB;
+  GuardSet gs;
+  if (guard_mem) {
+    guard_uniform(gs, eps, n, ldn, stride, nw, status);
+    guard_layout(gs, guard_mem, guard_mem_bytes);
+    guard_begin(ctx, gs);
+  }
+  const GuardSet* gp = guard_mem ? &gs : nullptr;
   for (int k0 = 0; k0 < n; k0 += SWEEP_NB) {
     const int kb = min(SWEEP_NB, n - k0);
-    sweep_front(ctx, ctx->stream, eps, n, ldn, stride, nw, k0, kb, Tp, Dp, Pp, pstride, status);
+    sweep_front(ctx, ctx->stream, eps, n, ldn, stride, nw, k0, kb, Tp, Dp, Pp, pstride, status, nullptr, nullptr, gp);
     sweep_update(ctx, ctx->stream, eps, n, ldn, stride, nw, k0, kb, Tp, Pp, pstride, 0, 0, 0);
   }
+  if (guard_mem) guard_end(ctx, gs);
   dim3 fg(n, nw);
   k_finish_wc<<<fg, 256, 0, ctx->stream>>>(eps, n, ldn, stride, status, 0);
   check_launch(ctx);
@@ -642,12 +737,17 @@ __device__ __forceinline__ int group_of(const int* __restrict__ pre, int count, 
   return lo;
 }
 
+template <bool GUARD>
 __global__ void __launch_bounds__(512) k_gsweep_diag(const GMat* __restrict__ mats, int k0, double* __restrict__ Dp,
-                                                     int* __restrict__ status) {
+                                                     int* __restrict__ status,
+                                                     const unsigned long long* __restrict__ gamax,
+                                                     unsigned long long* __restrict__ growth) {
   const int g = blockIdx.x;
   const GMat m = mats[g];
-  sweep_diag_body(m.M + (size_t)k0 * m.ldn + k0, m.ldn, min(SWEEP_NB, m.n - k0), Dp + (size_t)g * SWEEP_NB * SWEEP_NB,
-                  status + g);
+  const bool guarded = GUARD && m.guard;
+  sweep_diag_body<GUARD>(m.M + (size_t)k0 * m.ldn + k0, m.ldn, min(SWEEP_NB, m.n - k0),
+                         Dp + (size_t)g * SWEEP_NB * SWEEP_NB, status + g, guarded ? guard_tol(gamax, g) : 0.0,
+                         guarded ? growth + g : nullptr);
 }
 
 // Two 64-column tiles per 64 rows: all 128 panel columns are written (zero past kb).
@@ -666,12 +766,12 @@ __global__ void __launch_bounds__(PanelTile::THREADS) k_gsweep_tpanel(const GMat
 __global__ void __launch_bounds__(256) k_gsweep_write(const GMat* __restrict__ mats, const int* __restrict__ pre,
                                                       int count, int k0, const double* __restrict__ Tcat,
                                                       double* __restrict__ Pcat, const double* __restrict__ Dp,
-                                                      unsigned long long* amax) {
+                                                      unsigned long long* amax, unsigned long long* growth) {
   const int g = group_of(pre, count, blockIdx.x);
   const GMat m = mats[g];
   sweep_write_tile(m.M, m.n, m.ldn, k0, min(SWEEP_NB, m.n - k0), Tcat + (size_t)m.prow * SWEEP_NB,
                    Pcat + (size_t)m.prow * SWEEP_NB, Dp + (size_t)g * SWEEP_NB * SWEEP_NB,
-                   (blockIdx.x - pre[g]) * kWriteRows, amax);
+                   (blockIdx.x - pre[g]) * kWriteRows, amax, (growth && m.guard) ? growth + g : nullptr);
 }
 
 __global__ void __launch_bounds__(SweepTile::THREADS) k_gsweep_update(const GMat* __restrict__ mats,
@@ -774,6 +874,31 @@ void launch_invert_wc_group(qx_ctx* ctx, const GMat* mats_in, int G, int half_lo
   QX_CUDA(cudaMemcpyAsync(d_tab, tab.data(), tab.size() * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
   int* status = status_words(ctx, G);
   QX_CUDA(cudaMemsetAsync(status, 0, G * sizeof(int), ctx->stream));
+  // Guarded matrices (those the caller cannot show to be >= I).
+  GuardSet gs;
+  gs.nall = G;
+  for (int g = 0; g < G; ++g)
+    if (m[g].guard) {
+      GuardMat gm{};
+      gm.M = m[g].M;
+      gm.n = m[g].n;
+      gm.ldn = m[g].ldn;
+      gm.idx = g;
+      gm.status = status + g;
+      gs.mats.push_back(gm);
+    }
+  const bool guarded = !gs.mats.empty();
+  if (guarded) {
+    size_t bytes = 0;
+    for (const GuardMat& gm : gs.mats) bytes += guard_bytes(gm.n, gm.ldn, 1);
+    bytes += guard_bytes(0, 0, G);
+    DevBuf& gb = ctx->ws[WS_GUARD];
+    gb.reserve(bytes);
+    guard_layout(gs, gb.ptr, gb.bytes);
+    guard_begin(ctx, gs);
+  }
+  unsigned long long* gamax = guarded ? gs.amax : nullptr;
+  unsigned long long* ggrowth = guarded ? gs.growth : nullptr;
   int* tc_err = nullptr;
   void* split_base = nullptr;
   if (tc) {
@@ -789,7 +914,10 @@ void launch_invert_wc_group(qx_ctx* ctx, const GMat* mats_in, int G, int half_lo
   const int diag_smem = (SWEEP_NB * SWEEP_NB + SWEEP_NB * 33) * sizeof(double);
   for (int s = 0; s < nsteps; ++s) {
     const int k0 = s * SWEEP_NB, a = act[s];
-    k_gsweep_diag<<<a, 512, diag_smem, ctx->stream>>>(d_mats, k0, Dp, status);
+    if (guarded)
+      k_gsweep_diag<true><<<a, 512, diag_smem, ctx->stream>>>(d_mats, k0, Dp, status, gamax, ggrowth);
+    else
+      k_gsweep_diag<false><<<a, 512, diag_smem, ctx->stream>>>(d_mats, k0, Dp, status, nullptr, nullptr);
     check_launch(ctx);
     // Split form: the panel and write kernels accumulate max|T|, max|P| over
     // all matrices (one scale each) for the splits.
@@ -803,7 +931,7 @@ void launch_invert_wc_group(qx_ctx* ctx, const GMat* mats_in, int G, int half_lo
         d_mats, d_tab + off_tp[s], a, k0, Dp, Tcat, amax_t);
     check_launch(ctx);
     k_gsweep_write<<<tab[off_wr[s] + a], 256, 0, ctx->stream>>>(d_mats, d_tab + off_wr[s], a, k0, Tcat, Pcat, Dp,
-                                                                amax_p);
+                                                                amax_p, ggrowth);
     check_launch(ctx);
     if (tc) {
       uint8_t* b = static_cast<uint8_t*>(split_base);
@@ -818,6 +946,7 @@ void launch_invert_wc_group(qx_ctx* ctx, const GMat* mats_in, int G, int half_lo
       check_launch(ctx);
     }
   }
+  if (guarded) guard_end(ctx, gs);
   k_gfinish_wc<<<tab[off_fin + G], 256, 0, ctx->stream>>>(d_mats, d_tab + off_fin, G, status, half_lower);
   check_launch(ctx);
   ctx->pending.push_back({status, G, 1});

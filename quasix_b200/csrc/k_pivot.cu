@@ -1,0 +1,410 @@
+// Guarded eps inversion: pivot and growth checks around the block sweep, and
+// the pivoted re-inversion of the matrices they flag.
+//
+// The block sweep (k_gw_f64.cu) is Gauss-Jordan elimination without pivoting.
+// It is stable when eps >= I -- the imaginary axis with every occupied level
+// below every virtual one, or real shifts below the smallest transition --
+// and the callers that can show this run it unguarded.  Otherwise eps may be
+// indefinite with a tiny or zero leading minor while still nonsingular, and
+// the reference would then take its LU fallback: `invc` (Cholesky) fails and
+// `inv` (LAPACK dgetrf/dgetri, partial pivoting) inverts it
+// (quasix_core/src/selfenergy/correlation_ac.rs:383-399; the CD path calls
+// `inv` directly, selfenergy/correlation_pyscf_cd.rs:126-159).
+//
+// A guarded inversion therefore
+//   1. copies each eps aside and records amax = max |eps| (k_guard_backup);
+//   2. sweeps, flagging a matrix whose pivot is below kGuardPivot * amax or
+//      whose not-yet-swept entries grow past kGuardGrowth * amax;
+//   2b. checks every result against its copy with one probe vector v of
+//      +-1 entries: eta = max|eps X v - v| / (n amax max|X|) is the normwise
+//      backward error of X in the direction v, ~1e-17 for a stable inverse
+//      whatever the conditioning, and it exceeds kGuardResidual when the
+//      unpivoted elimination lost digits to element growth that the pivot
+//      and growth checks did not see;
+//   3. re-inverts every flagged matrix from its copy by Gauss-Jordan
+//      elimination with partial (row) pivoting, in panels of PIV_NB columns
+//      (k_piv_panel: the pivoted exchanges on the panel, one CTA per matrix;
+//      k_piv_update: the rank-PIV_NB update of the other columns on DMMA
+//      tiles; k_piv_permute: undo the pivot permutation into -eps^-1, the
+//      sweep's own output convention).
+// A zero or non-finite pivot in step 3 leaves the matrix flagged singular
+// (Wc = 0, the reference's identity fallback after a failed LU).
+#include <algorithm>
+#include <climits>
+
+#include "gemm_f64.cuh"
+#include "qx_internal.cuh"
+
+namespace qx {
+
+namespace {
+
+constexpr int PIV_NB = 32;
+using PivTile = F64Tile<64, 64, 2, 2, 3>;
+
+// Block-wide argmax of (v, r): largest v, ties to the smallest r (every
+// thread calls it; the result is returned to all threads).
+__device__ __forceinline__ void block_argmax(double& v, int& r, double* sv, int* sr) {
+  for (int o = 16; o > 0; o >>= 1) {
+    const double ov = __shfl_xor_sync(0xffffffffu, v, o);
+    const int orr = __shfl_xor_sync(0xffffffffu, r, o);
+    if (ov > v || (ov == v && orr < r)) {
+      v = ov;
+      r = orr;
+    }
+  }
+  const int warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) {
+    sv[warp] = v;
+    sr[warp] = r;
+  }
+  __syncthreads();
+  v = sv[0];
+  r = sr[0];
+  for (int k = 1; k < nwarp; ++k)
+    if (sv[k] > v || (sv[k] == v && sr[k] < r)) {
+      v = sv[k];
+      r = sr[k];
+    }
+}
+
+__device__ __forceinline__ void atomic_max_abs(unsigned long long* out, double m) {
+  // m >= 0 compares as its bit pattern.
+  atomicMax(out, (unsigned long long)__double_as_longlong(m));
+}
+
+// bk = M over the n x n part, amax[idx] = max |M|.  grid (count, y).
+__global__ void k_guard_backup(const GuardMat* __restrict__ tab, unsigned long long* __restrict__ amax) {
+  const GuardMat g = tab[blockIdx.x];
+  double m = 0.0;
+  const size_t total = (size_t)g.n * g.n;
+  for (size_t e = (size_t)blockIdx.y * blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.y * blockDim.x) {
+    const size_t r = e / g.n, c = e % g.n;
+    const double v = g.M[r * g.ldn + c];
+    g.bk[r * g.ldn + c] = v;
+    m = fmax(m, fabs(v));
+    if (!isfinite(v)) m = INFINITY;
+  }
+  __shared__ double red[32];
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    m = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if (threadIdx.x == 0) atomic_max_abs(amax + g.idx, m);
+  }
+}
+
+// Entry j of the probe vector: +-1 from a fixed integer hash of j.
+__device__ __forceinline__ double probe_entry(int j) {
+  unsigned h = (unsigned)j * 2654435761u;
+  h ^= h >> 15;
+  h *= 2246822519u;
+  h ^= h >> 13;
+  return (h & 1u) ? 1.0 : -1.0;
+}
+
+// y = X v with X = -M (the sweep's output is -eps^-1), xmax[idx] = max |X|.
+// One warp per row; y in rbuf.  grid (count, y).
+__global__ void k_guard_probe_xv(const GuardMat* __restrict__ tab, unsigned long long* __restrict__ xmax) {
+  const GuardMat g = tab[blockIdx.x];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+  double mx = 0.0;
+  for (int i = blockIdx.y * nwarp + warp; i < g.n; i += gridDim.y * nwarp) {
+    const double* row = g.M + (size_t)i * g.ldn;
+    double s = 0.0;
+    for (int j = lane; j < g.n; j += 32) {
+      const double x = -row[j];
+      s += x * probe_entry(j);
+      mx = fmax(mx, isfinite(x) ? fabs(x) : INFINITY);
+    }
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) g.rbuf[i] = s;
+  }
+  for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  if (lane == 0) atomic_max_abs(xmax + g.idx, mx);
+}
+
+// rmax[idx] = max_i |(eps y)_i - v_i| with eps the copy bk.  grid (count, y).
+__global__ void k_guard_probe_res(const GuardMat* __restrict__ tab, unsigned long long* __restrict__ rmax) {
+  const GuardMat g = tab[blockIdx.x];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+  double mx = 0.0;
+  for (int i = blockIdx.y * nwarp + warp; i < g.n; i += gridDim.y * nwarp) {
+    const double* row = g.bk + (size_t)i * g.ldn;
+    double s = 0.0;
+    for (int j = lane; j < g.n; j += 32) s += row[j] * g.rbuf[j];
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    const double r = s - probe_entry(i);
+    mx = fmax(mx, isfinite(r) ? fabs(r) : INFINITY);
+  }
+  if (lane == 0) atomic_max_abs(rmax + g.idx, mx);
+}
+
+// Row state (-1: not yet a pivot row) for every flagged matrix; status
+// cleared (the fallback decides it anew).
+__global__ void k_piv_init(const GuardMat* __restrict__ tab) {
+  const GuardMat g = tab[blockIdx.x];
+  for (int r = threadIdx.x; r < g.n; r += blockDim.x) g.ints[r] = -1;
+  if (threadIdx.x == 0) *g.status = 0;
+}
+
+// Panel [k0, k0 + kb) of the pivoted Gauss-Jordan exchange on bk, one CTA of
+// 512 threads per matrix.  Exchange on pivot (p, c), d = T[p][c]:
+//   T[p][c] = 1/d, T[p][j] = -T[p][j]/d, T[i][c] = T[i][c]/d,
+//   T[i][j] -= T[i][c] T[p][j]/d        (i != p, j != c),
+// applied here to the panel columns only (they depend on nothing else).  The
+// pivot row of column c is the unused row of largest |T[r][c]|.  Afterwards
+// rbuf[j][b] = the old row piv[k0 + b] outside the panel (zero inside), the
+// operand of the update of the other columns.
+__global__ void __launch_bounds__(512) k_piv_panel(const GuardMat* __restrict__ tab, int k0) {
+  const GuardMat g = tab[blockIdx.x];
+  const int n = g.n;
+  if (k0 >= n || *g.status != 0) return;
+  const int kb = min(PIV_NB, n - k0), lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int nwarp = blockDim.x >> 5;
+  int* state = g.ints;
+  int* piv = g.ints + n;
+  double* A = g.bk;
+  const size_t ld = g.ldn;
+  __shared__ double prow[PIV_NB];
+  __shared__ double sv[32];
+  __shared__ int sr[32];
+  // Candidate pivot of the panel's first column.
+  double best = -1.0;
+  int bi = INT_MAX;
+  for (int r = threadIdx.x; r < n; r += blockDim.x)
+    if (state[r] < 0) {
+      const double v = fabs(A[(size_t)r * ld + k0]);
+      if (v > best || (v == best && r < bi)) {
+        best = v;
+        bi = r;
+      }
+    }
+  for (int j = 0; j < kb; ++j) {
+    block_argmax(best, bi, sv, sr);
+    const int p = bi;
+    const double d = (p == INT_MAX) ? 0.0 : A[(size_t)p * ld + k0 + j];
+    if (!(fabs(d) > 0.0) || !isfinite(d)) {  // uniform: p and d are the same in every thread
+      if (threadIdx.x == 0) *g.status = 1;
+      return;
+    }
+    if (warp == 0) prow[lane] = lane < kb ? A[(size_t)p * ld + k0 + lane] : 0.0;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      state[p] = k0;
+      piv[k0 + j] = p;
+    }
+    const double inv = 1.0 / d;
+    best = -1.0;
+    bi = INT_MAX;
+    for (int r = warp; r < n; r += nwarp) {
+      double* row = A + (size_t)r * ld + k0;
+      double v = lane < kb ? row[lane] : 0.0;
+      if (r == p) {
+        v = (lane == j) ? inv : -prow[lane] * inv;
+      } else {
+        const double t = __shfl_sync(0xffffffffu, v, j) * inv;
+        v = (lane == j) ? t : v - t * prow[lane];
+      }
+      if (lane < kb) row[lane] = v;
+      if (j + 1 < kb && r != p) {
+        const double cv = fabs(__shfl_sync(0xffffffffu, v, j + 1));
+        if (state[r] < 0 && (cv > best || (cv == best && r < bi))) {
+          best = cv;
+          bi = r;
+        }
+      }
+    }
+    __syncthreads();
+  }
+  // rbuf[j][b] = A[piv[k0 + b]][j] for columns outside the panel.
+  for (int b = warp; b < kb; b += nwarp) {
+    const double* src = A + (size_t)piv[k0 + b] * ld;
+    for (int j = lane; j < n; j += 32)
+      g.rbuf[(size_t)j * PIV_NB + b] = (j >= k0 && j < k0 + kb) ? 0.0 : src[j];
+  }
+}
+
+// Columns outside the panel: with C = A[:, panel] (new) rbuf^T,
+//   A[r][j] = -C[r][j]         for the panel's pivot rows r,
+//   A[r][j] -= C[r][j]         otherwise.
+// grid (tiles, tiles, count).
+__global__ void __launch_bounds__(PivTile::THREADS) k_piv_update(const GuardMat* __restrict__ tab, int k0) {
+  using T = PivTile;
+  const GuardMat g = tab[blockIdx.z];
+  const int n = g.n;
+  if (k0 >= n || *g.status != 0) return;
+  const int kb = min(PIV_NB, n - k0);
+  const int m0 = blockIdx.y * T::BM, n0 = blockIdx.x * T::BN;
+  if (m0 >= n || n0 >= n) return;
+  if (n0 >= k0 && n0 + T::BN <= k0 + kb) return;
+  extern __shared__ double smem[];
+  double acc[T::MI][T::NJ][2];
+#pragma unroll
+  for (int i = 0; i < T::MI; ++i)
+#pragma unroll
+    for (int j = 0; j < T::NJ; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+  const size_t ld = g.ldn;
+  f64_mainloop<T>(acc, smem, g.bk + (size_t)m0 * ld + k0, (int)ld, n - m0, g.rbuf + (size_t)n0 * PIV_NB, PIV_NB,
+                  n - n0, nullptr, kb);
+  const int* state = g.ints;
+#pragma unroll
+  for (int i = 0; i < T::MI; ++i) {
+    const int r = m0 + f64_row<T>(i);
+    if (r >= n) continue;
+    const bool prow = state[r] == k0;
+#pragma unroll
+    for (int j = 0; j < T::NJ; ++j)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int c = n0 + f64_col<T>(j, e);
+        if (c >= n || (c >= k0 && c < k0 + kb)) continue;
+        double* a = g.bk + (size_t)r * ld + c;
+        *a = prow ? -acc[i][j][e] : *a - acc[i][j][e];
+      }
+  }
+}
+
+// pinv[piv[b]] = b.
+__global__ void k_piv_inverse_perm(const GuardMat* __restrict__ tab) {
+  const GuardMat g = tab[blockIdx.x];
+  if (*g.status != 0) return;
+  for (int b = threadIdx.x; b < g.n; b += blockDim.x) g.ints[2 * g.n + g.ints[g.n + b]] = b;
+}
+
+// After every exchange the element at (piv[a], b) is (eps^-1)[a][piv[b]], so
+// M[a][c] = -bk[piv[a]][pinv[c]] is the sweep's -eps^-1.  grid (n, count).
+__global__ void k_piv_permute(const GuardMat* __restrict__ tab) {
+  const GuardMat g = tab[blockIdx.y];
+  const int a = blockIdx.x;
+  if (a >= g.n || *g.status != 0) return;
+  const int* piv = g.ints + g.n;
+  const int* pinv = g.ints + 2 * g.n;
+  const double* src = g.bk + (size_t)piv[a] * g.ldn;
+  double* dst = g.M + (size_t)a * g.ldn;
+  for (int c = threadIdx.x; c < g.n; c += blockDim.x) dst[c] = -src[pinv[c]];
+}
+
+inline size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
+
+}  // namespace
+
+size_t guard_bytes(int n, int ldn, int count) {
+  const size_t per = align256((size_t)n * ldn * sizeof(double)) + align256((size_t)3 * n * sizeof(int)) +
+                     align256((size_t)n * PIV_NB * sizeof(double));
+  return per * count + align256(count * sizeof(GuardMat)) + 4 * align256(count * sizeof(unsigned long long)) + 256;
+}
+
+void guard_layout(GuardSet& gs, void* mem, size_t bytes) {
+  size_t need = align256(gs.mats.size() * sizeof(GuardMat)) + 4 * align256(gs.nall * sizeof(unsigned long long));
+  for (const GuardMat& g : gs.mats)
+    need += align256((size_t)g.n * g.ldn * sizeof(double)) + align256((size_t)3 * g.n * sizeof(int)) +
+            align256((size_t)g.n * PIV_NB * sizeof(double));
+  QX_REQUIRE(need <= bytes, QX_ERR_INVALID_INPUT, "guarded inversion needs %zu bytes of workspace, have %zu", need,
+             bytes);
+  char* p = static_cast<char*>(mem);
+  gs.d_tab = reinterpret_cast<GuardMat*>(p);
+  p += align256(gs.mats.size() * sizeof(GuardMat));
+  gs.amax = reinterpret_cast<unsigned long long*>(p);
+  p += align256(gs.nall * sizeof(unsigned long long));
+  gs.growth = reinterpret_cast<unsigned long long*>(p);
+  p += align256(gs.nall * sizeof(unsigned long long));
+  gs.xmax = reinterpret_cast<unsigned long long*>(p);
+  p += align256(gs.nall * sizeof(unsigned long long));
+  gs.rmax = reinterpret_cast<unsigned long long*>(p);
+  p += align256(gs.nall * sizeof(unsigned long long));
+  for (GuardMat& g : gs.mats) {
+    g.bk = reinterpret_cast<double*>(p);
+    p += align256((size_t)g.n * g.ldn * sizeof(double));
+    g.ints = reinterpret_cast<int*>(p);
+    p += align256((size_t)3 * g.n * sizeof(int));
+    g.rbuf = reinterpret_cast<double*>(p);
+    p += align256((size_t)g.n * PIV_NB * sizeof(double));
+  }
+}
+
+void guard_begin(qx_ctx* ctx, GuardSet& gs) {
+  if (gs.mats.empty()) return;
+  static PerDeviceOnce attr_once;
+  attr_once(ctx->device, [] {
+    QX_CUDA(cudaFuncSetAttribute(k_piv_update, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PivTile::SMEM));
+  });
+  QX_CUDA(cudaMemsetAsync(gs.amax, 0, gs.nall * sizeof(unsigned long long), ctx->stream));
+  QX_CUDA(cudaMemsetAsync(gs.growth, 0, gs.nall * sizeof(unsigned long long), ctx->stream));
+  QX_CUDA(cudaMemsetAsync(gs.xmax, 0, gs.nall * sizeof(unsigned long long), ctx->stream));
+  QX_CUDA(cudaMemsetAsync(gs.rmax, 0, gs.nall * sizeof(unsigned long long), ctx->stream));
+  QX_CUDA(cudaMemcpyAsync(gs.d_tab, gs.mats.data(), gs.mats.size() * sizeof(GuardMat), cudaMemcpyHostToDevice,
+                          ctx->stream));
+  int nmax = 0;
+  for (const GuardMat& g : gs.mats) nmax = std::max(nmax, g.n);
+  dim3 grid((unsigned)gs.mats.size(), std::max(1, std::min(ceil_div(nmax * nmax, 256 * 8), 512)));
+  k_guard_backup<<<grid, 256, 0, ctx->stream>>>(gs.d_tab, gs.amax);
+  check_launch(ctx);
+}
+
+int guard_end(qx_ctx* ctx, GuardSet& gs) {
+  if (gs.mats.empty()) return 0;
+  const int G = (int)gs.mats.size();
+  // Probe residual of every result against its copy.
+  int nmax = 0;
+  for (const GuardMat& g : gs.mats) nmax = std::max(nmax, g.n);
+  const dim3 pg((unsigned)G, std::max(1, std::min(ceil_div(nmax, 8), 64)));
+  k_guard_probe_xv<<<pg, 256, 0, ctx->stream>>>(gs.d_tab, gs.xmax);
+  check_launch(ctx);
+  k_guard_probe_res<<<pg, 256, 0, ctx->stream>>>(gs.d_tab, gs.rmax);
+  check_launch(ctx);
+  // Read the flags: the status word of each guarded matrix and its bounds.
+  std::vector<unsigned long long> amax(gs.nall), growth(gs.nall), xmax(gs.nall), rmax(gs.nall);
+  std::vector<int> st(G);
+  QX_CUDA(cudaMemcpyAsync(amax.data(), gs.amax, gs.nall * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                          ctx->stream));
+  QX_CUDA(cudaMemcpyAsync(growth.data(), gs.growth, gs.nall * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                          ctx->stream));
+  QX_CUDA(cudaMemcpyAsync(xmax.data(), gs.xmax, gs.nall * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                          ctx->stream));
+  QX_CUDA(cudaMemcpyAsync(rmax.data(), gs.rmax, gs.nall * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                          ctx->stream));
+  for (int i = 0; i < G; ++i)
+    QX_CUDA(cudaMemcpyAsync(&st[i], gs.mats[i].status, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  QX_CUDA(cudaStreamSynchronize(ctx->stream));
+  auto as_double = [](unsigned long long u) {
+    double d;
+    memcpy(&d, &u, sizeof d);
+    return d;
+  };
+  std::vector<GuardMat> flagged;
+  nmax = 0;
+  for (int i = 0; i < G; ++i) {
+    const GuardMat& g = gs.mats[i];
+    const double a = as_double(amax[g.idx]), gr = as_double(growth[g.idx]);
+    const double eta = as_double(rmax[g.idx]) / ((double)g.n * a * as_double(xmax[g.idx]));
+    if (st[i] != 0 || !(gr <= kGuardGrowth * a) || !(eta <= kGuardResidual)) {
+      flagged.push_back(g);
+      nmax = std::max(nmax, g.n);
+    }
+  }
+  gs.nflagged = (int)flagged.size();
+  if (flagged.empty()) return 0;
+  const int F = (int)flagged.size();
+  QX_REQUIRE(F <= 65535, QX_ERR_INVALID_INPUT, "%d matrices to re-invert in one call (at most 65535)", F);
+  QX_CUDA(cudaMemcpyAsync(gs.d_tab, flagged.data(), F * sizeof(GuardMat), cudaMemcpyHostToDevice, ctx->stream));
+  k_piv_init<<<F, 256, 0, ctx->stream>>>(gs.d_tab);
+  check_launch(ctx);
+  const int tiles = ceil_div(nmax, PivTile::BM);
+  for (int k0 = 0; k0 < nmax; k0 += PIV_NB) {
+    k_piv_panel<<<F, 512, 0, ctx->stream>>>(gs.d_tab, k0);
+    check_launch(ctx);
+    k_piv_update<<<dim3(tiles, tiles, F), PivTile::THREADS, PivTile::SMEM, ctx->stream>>>(gs.d_tab, k0);
+    check_launch(ctx);
+  }
+  k_piv_inverse_perm<<<F, 256, 0, ctx->stream>>>(gs.d_tab);
+  check_launch(ctx);
+  k_piv_permute<<<dim3(nmax, F), 256, 0, ctx->stream>>>(gs.d_tab);
+  check_launch(ctx);
+  return F;
+}
+
+}  // namespace qx

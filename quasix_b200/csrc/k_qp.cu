@@ -1,42 +1,10 @@
 // Per-orbital FP64 kernels: Thiele coefficients, Pade evaluation, linearized
 // and Newton quasiparticle roots.  One thread per orbital; latency-bound by
 // nature (O(nfit^2) complex work per orbital).
+#include "pade.cuh"
 #include "qx_internal.cuh"
 
 namespace qx {
-
-struct cplx {
-  double re, im;
-};
-__device__ __forceinline__ cplx cmk(double r, double i) { return cplx{r, i}; }
-__device__ __forceinline__ cplx cadd(cplx a, cplx b) { return cplx{a.re + b.re, a.im + b.im}; }
-__device__ __forceinline__ cplx csub(cplx a, cplx b) { return cplx{a.re - b.re, a.im - b.im}; }
-__device__ __forceinline__ cplx cmul(cplx a, cplx b) {
-  return cplx{a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re};
-}
-__device__ __forceinline__ cplx cdiv(cplx a, cplx b) {
-  const double n = b.re * b.re + b.im * b.im;
-  return cplx{(a.re * b.re + a.im * b.im) / n, (a.im * b.re - a.re * b.im) / n};
-}
-__device__ __forceinline__ double cabs_(cplx a) { return hypot(a.re, a.im); }
-
-constexpr int MAX_FIT = 64;
-
-// Pade continued fraction at real omega (correlation_ac.rs:530-566).
-__device__ cplx pade_eval(double omega, const cplx* zn, const cplx* a, int nfit) {
-  if (nfit == 0) return cmk(0, 0);
-  if (nfit == 1) return a[0];
-  const cplx z = cmk(omega, 0.0);
-  cplx x = cmul(a[nfit - 1], csub(z, zn[nfit - 2]));
-  for (int i = nfit - 2; i >= 1; --i) {
-    cplx den = cadd(cmk(1.0, 0.0), x);
-    if (cabs_(den) < 1e-14) x = cmk(1e10, 0.0);
-    else x = cdiv(cmul(a[i], csub(z, zn[i - 1])), den);
-  }
-  cplx den = cadd(cmk(1.0, 0.0), x);
-  if (cabs_(den) < 1e-14) return a[0];
-  return cdiv(a[0], den);
-}
 
 struct Orbital {
   const cplx* zn;
@@ -66,16 +34,7 @@ __global__ void k_pade_qp(QPParams p) {
     zn[j] = cmk(0.0, s * p.iw[k]);
     a[j] = cmk(p.sigma[((size_t)t * p.nws + k) * 2], p.sigma[((size_t)t * p.nws + k) * 2 + 1]);
   }
-  // Reciprocal differences in place (correlation_ac.rs:470-509): after column
-  // j, a[j] = g[j][j] and a[i > j] = g[i][j].
-  for (int j = 1; j < nfit; ++j) {
-    const cplx gd = a[j - 1];
-    for (int i = j; i < nfit; ++i) {
-      const cplx den = cmul(csub(zn[i], zn[j - 1]), a[i]);
-      if (cabs_(den) < 1e-14) a[i] = cmk(1e10, 0.0);
-      else a[i] = cdiv(csub(gd, a[i]), den);
-    }
-  }
+  thiele_fit(a, zn, nfit);
   for (int j = 0; j < nfit; ++j) {
     p.coeff[((size_t)j * p.norbs + t) * 2] = a[j].re;
     p.coeff[((size_t)j * p.norbs + t) * 2 + 1] = a[j].im;

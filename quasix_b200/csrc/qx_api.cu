@@ -281,9 +281,12 @@ void gw_wc_contract(qx_ctx* ctx, GWSystem& S) {
 void gw_wc_pairs(qx_ctx* ctx, GWSystem& S, const double* e_host) {
   gw_wc_p0(ctx, S, e_host);
   record_stage(ctx, QX_ST_INV, true);
-  // Imaginary axis: eps is SPD with eigenvalues in [1, 1 + ||Pi||], so the
-  // split trailing update of the sweep keeps Wc within the split forms' error.
-  launch_invert_wc(ctx, S.eps, S.naux, S.ldn, S.eps_stride, S.nw, /*half_lower=*/1,
+  // Imaginary axis with ordered levels: eps is SPD with eigenvalues in
+  // [1, 1 + ||Pi||], so the split trailing update of the sweep keeps Wc within
+  // the split forms' error.  Once levels cross, eps may be indefinite and the
+  // sweep runs guarded (with the pivoted fallback).
+  launch_invert_wc(ctx, S.eps, S.naux, S.ldn, S.eps_stride, S.nw,
+                   !eps_at_least_identity(e_host, S.nocc, S.nvir, 0.0), /*half_lower=*/1,
                    /*split_update=*/is_tc_precision(S.precision));
   record_stage(ctx, QX_ST_INV, false);
   gw_wc_contract(ctx, S);
@@ -416,6 +419,16 @@ void convergence_window(const double* e, int nmo, int nocc, const qx_evgw_config
     if (e[i] <= lumo + w) en = i + 1;
     else break;
   }
+}
+
+bool eps_at_least_identity(const double* energies, int nocc, int nvir, double wmax) {
+  double homo = -INFINITY, lumo = INFINITY;
+  for (int i = 0; i < nocc + nvir; ++i)
+    if (!std::isfinite(energies[i])) return false;
+  for (int i = 0; i < nocc; ++i) homo = std::max(homo, energies[i]);
+  for (int a = 0; a < nvir; ++a) lumo = std::min(lumo, energies[nocc + a]);
+  const double gap = lumo - homo;
+  return std::isfinite(gap) && gap > 0.0 && gap > std::fabs(wmax);
 }
 
 void validate_common(int nmo, int nocc, int naux) {
@@ -593,6 +606,11 @@ qx_status qx_get_rho_response(qx_ctx* ctx, int nfreq, const double* freqs, const
   });
 }
 
+int qx_eps_at_least_identity(const double* mo_energy, int nocc, int nvir, double wmax) {
+  if (!mo_energy || nocc <= 0 || nvir <= 0) return 0;
+  return eps_at_least_identity(mo_energy, nocc, nvir, wmax) ? 1 : 0;
+}
+
 qx_status qx_screened_interaction(qx_ctx* ctx, int nfreq, int naux, const double* pi, double* wc) {
   return guarded(ctx, [&] {
     QX_REQUIRE(ctx && nfreq > 0 && naux > 0 && pi && wc, QX_ERR_INVALID_INPUT, "invalid arguments");
@@ -608,7 +626,8 @@ qx_status qx_screened_interaction(qx_ctx* ctx, int nfreq, int naux, const double
     ctx->ws[WS_EPS].reserve(he.size() * sizeof(double));
     double* eps = ctx->ws[WS_EPS].as<double>();
     QX_CUDA(cudaMemcpyAsync(eps, he.data(), he.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
-    launch_invert_wc(ctx, eps, naux, ldn, stride, nfreq);
+    // Pi comes from the caller: eps >= I cannot be assumed.
+    launch_invert_wc(ctx, eps, naux, ldn, stride, nfreq, /*guard=*/1);
     QX_CUDA(cudaMemcpyAsync(he.data(), eps, he.size() * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     sync_and_check(ctx);
     for (int w = 0; w < nfreq; ++w)
@@ -652,82 +671,6 @@ qx_status qx_get_sigma_diag(qx_ctx* ctx, const double* mo_energy, const double* 
     QX_CUDA(cudaMemcpy(omega, om.data(), om.size() * sizeof(double), cudaMemcpyDefault));
     *nw_sigma = S.nws;
   });
-}
-
-// Host-side Thiele (used by qx_ac_pade_thiele_diag; the evGW loop uses the
-// device kernel).
-static void thiele_host(const std::vector<std::complex<double>>& f, const std::vector<std::complex<double>>& z,
-                        std::vector<std::complex<double>>& a) {
-  const int n = (int)f.size();
-  a = f;
-  for (int j = 1; j < n; ++j) {
-    const std::complex<double> gd = a[j - 1];
-    for (int i = j; i < n; ++i) {
-      std::complex<double> den = (z[i] - z[j - 1]) * a[i];
-      if (std::abs(den) < 1e-14) a[i] = 1e10;
-      else a[i] = (gd - a[i]) / den;
-    }
-  }
-}
-
-qx_status qx_ac_pade_thiele_diag(qx_ctx* ctx, int norbs, int nws, const double* sigma, const double* omega, int npade,
-                                 double* coeff, double* omega_fit, int nfit_max, int* nfit) {
-  return guarded(ctx, [&] {
-    QX_REQUIRE(norbs > 0 && nws > 0 && sigma && omega && nfit, QX_ERR_INVALID_INPUT, "invalid arguments");
-    std::vector<int> idx = pade_indices(nws, npade);
-    const int nf = (int)idx.size();
-    *nfit = nf;
-    if (nf == 0) return;
-    QX_REQUIRE(nfit_max >= nf && coeff && omega_fit, QX_ERR_INVALID_INPUT, "nfit_max %d < %d", nfit_max, nf);
-    std::vector<double> hs((size_t)norbs * nws * 2), ho((size_t)norbs * nws * 2);
-    QX_CUDA(cudaMemcpy(hs.data(), sigma, hs.size() * sizeof(double), cudaMemcpyDefault));
-    QX_CUDA(cudaMemcpy(ho.data(), omega, ho.size() * sizeof(double), cudaMemcpyDefault));
-    std::vector<double> hc((size_t)nf * norbs * 2), hf((size_t)norbs * nf * 2);
-    for (int p = 0; p < norbs; ++p) {
-      std::vector<std::complex<double>> f(nf), z(nf), a;
-      for (int j = 0; j < nf; ++j) {
-        size_t q = ((size_t)p * nws + idx[j]) * 2;
-        f[j] = {hs[q], hs[q + 1]};
-        z[j] = {ho[q], ho[q + 1]};
-        hf[((size_t)p * nf + j) * 2] = ho[q];
-        hf[((size_t)p * nf + j) * 2 + 1] = ho[q + 1];
-      }
-      thiele_host(f, z, a);
-      for (int j = 0; j < nf; ++j) {
-        hc[((size_t)j * norbs + p) * 2] = a[j].real();
-        hc[((size_t)j * norbs + p) * 2 + 1] = a[j].imag();
-      }
-    }
-    QX_CUDA(cudaMemcpy(coeff, hc.data(), hc.size() * sizeof(double), cudaMemcpyDefault));
-    QX_CUDA(cudaMemcpy(omega_fit, hf.data(), hf.size() * sizeof(double), cudaMemcpyDefault));
-  });
-}
-
-qx_status qx_pade_thiele(int nfit, const double* zn, const double* coeff, int nomega, const double* omega,
-                         double* out) {
-  if (nfit < 0 || nomega < 0 || (nfit > 0 && (!zn || !coeff)) || (nomega > 0 && (!omega || !out)))
-    return QX_ERR_INVALID_INPUT;
-  for (int q = 0; q < nomega; ++q) {
-    std::complex<double> r;
-    if (nfit == 0) r = 0.0;
-    else if (nfit == 1) r = {coeff[0], coeff[1]};
-    else {
-      auto Z = [&](int i) { return std::complex<double>(zn[2 * i], zn[2 * i + 1]); };
-      auto C = [&](int i) { return std::complex<double>(coeff[2 * i], coeff[2 * i + 1]); };
-      std::complex<double> z(omega[q], 0.0);
-      std::complex<double> x = C(nfit - 1) * (z - Z(nfit - 2));
-      for (int i = nfit - 2; i >= 1; --i) {
-        std::complex<double> den = 1.0 + x;
-        if (std::abs(den) < 1e-14) x = 1e10;
-        else x = C(i) * (z - Z(i - 1)) / den;
-      }
-      std::complex<double> den = 1.0 + x;
-      r = (std::abs(den) < 1e-14) ? C(0) : C(0) / den;
-    }
-    out[2 * q] = r.real();
-    out[2 * q + 1] = r.imag();
-  }
-  return QX_OK;
 }
 
 qx_status qx_compute_exchange_diag(qx_ctx* ctx, const double* lpq, int naux, int nmo, int nocc, double* sigma_x) {

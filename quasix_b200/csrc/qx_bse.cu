@@ -948,7 +948,9 @@ qx_status qx_bse_w0(qx_ctx* ctx, const double* mo_energy, const double* lpq_ov, 
     double* eps = ctx->ws[WS_EPS].as<double>();
     launch_chi(ctx, d_e, nocc, nvir, d_f, 1, 0, chi, ldov);
     launch_eps_fp64(ctx, bov, ldov, naux, nov, chi, 1, eps, ldn, stride);
-    launch_invert_wc(ctx, eps, naux, ldn, stride, 1);
+    std::vector<double> he(nocc + nvir);
+    QX_CUDA(cudaMemcpy(he.data(), mo_energy, (nocc + nvir) * sizeof(double), cudaMemcpyDefault));
+    launch_invert_wc(ctx, eps, naux, ldn, stride, 1, !eps_at_least_identity(he.data(), nocc, nvir, 0.0));
     std::vector<double> h(stride);
     QX_CUDA(cudaMemcpyAsync(h.data(), eps, stride * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     sync_and_check(ctx);

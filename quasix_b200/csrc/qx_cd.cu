@@ -132,7 +132,8 @@ void CdEngine::setup(const double* mo_energy, const double* lpq, const int* targ
                      int nocc_, int naux_, int nw_, double x0, int precision_) {
   setup_begin(mo_energy, lpq, targets, ntarget_, nmo_, nocc_, naux_, nw_, x0, precision_);
   record_stage(ctx, QX_ST_INV, true);
-  launch_invert_wc(ctx, S.eps, S.naux, S.ldn, S.eps_stride, S.nw, /*half_lower=*/1, /*split_update=*/tc);
+  launch_invert_wc(ctx, S.eps, S.naux, S.ldn, S.eps_stride, S.nw, !eps_at_least_identity(e.data(), nocc, nvir, 0.0),
+                   /*half_lower=*/1, /*split_update=*/tc);
   record_stage(ctx, QX_ST_INV, false);
   setup_end();
 }
@@ -170,7 +171,8 @@ void CdEngine::setup_begin(const double* mo_energy, const double* lpq, const int
 }
 
 void CdEngine::eps_matrices(std::vector<GMat>& out) const {
-  for (int w = 0; w < nw; ++w) out.push_back(GMat{S.eps + (size_t)w * S.eps_stride, naux, S.ldn, 0, 0});
+  const int guard = !eps_at_least_identity(e.data(), nocc, nvir, 0.0);
+  for (int w = 0; w < nw; ++w) out.push_back(GMat{S.eps + (size_t)w * S.eps_stride, naux, S.ldn, 0, guard});
 }
 
 void CdEngine::setup_end() {
@@ -237,9 +239,12 @@ CdResidueChunk CdEngine::residue_buffers(int R) {
 
 void CdEngine::residue_compute(CdResidueChunk& c, const CdResidue* list, int rc) {
   residue_p0(c, list, rc);
-  // Real axis: eps(w_r) is indefinite and can be ill-conditioned near an
-  // excitation, so the sweep stays FP64 here.
-  launch_invert_wc(ctx, c.eps, naux, ldn, (size_t)naux * ldn, rc);
+  // Real axis: eps(w_r) is indefinite once a shift passes the smallest
+  // transition, and can be ill-conditioned near an excitation, so the sweep
+  // stays FP64 here, guarded unless every shift lies below the gap.
+  double wmax = 0.0;
+  for (int r = 0; r < rc; ++r) wmax = std::max(wmax, std::fabs(list[r].w));
+  launch_invert_wc(ctx, c.eps, naux, ldn, (size_t)naux * ldn, rc, !eps_at_least_identity(e.data(), nocc, nvir, wmax));
   residue_post(c, rc);
 }
 
@@ -308,14 +313,16 @@ void CdEngine::evaluate_begin(const std::vector<int>& act, std::vector<GMat>* gr
   // 0); with a 0.9 margin its eigenvalues lie in [1, 1 + ||Pi(0)|| / 0.19].
   double wmax = 0.0;
   for (const CdResidue& r : ev_res) wmax = std::max(wmax, std::fabs(r.w));
-  ev_spd = wmax < 0.9 * (e[nocc] - e[nocc - 1]);
+  // The gap is min(virtual) - max(occupied): QP levels need not stay ordered.
+  ev_spd = eps_at_least_identity(e.data(), nocc, nvir, wmax / 0.9);
+  const int guard = !eps_at_least_identity(e.data(), nocc, nvir, wmax);
   if (R == 0) return;
   ev_chunk = residue_buffers(R);
   CdResidueChunk& c = ev_chunk;
   if (group && R <= c.cap) {
     // One chunk: its eps(w_r) join the caller's grouped inversion.
     residue_p0(c, ev_res.data(), R);
-    for (int r = 0; r < R; ++r) group->push_back(GMat{c.eps + (size_t)r * naux * ldn, naux, ldn, 0, 0});
+    for (int r = 0; r < R; ++r) group->push_back(GMat{c.eps + (size_t)r * naux * ldn, naux, ldn, 0, guard});
     ev_grouped = true;
     return;
   }

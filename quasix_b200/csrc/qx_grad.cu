@@ -339,7 +339,8 @@ extern "C" qx_status qx_g0w0_cd_grad(qx_ctx* ctx, const double* mo_energy, const
         launch_eps_tc(ctx, E.S.bov, ldov, naux, nov, chi, fc, eps, ldn, stride, precision == QX_PREC_FP16X3);
       else
         launch_eps_fp64(ctx, E.S.bov, ldov, naux, nov, chi, fc, eps, ldn, stride);
-      launch_invert_wc(ctx, eps, naux, ldn, stride, fc, 0, /*split_update=*/E.tc);
+      launch_invert_wc(ctx, eps, naux, ldn, stride, fc, !eps_at_least_identity(E.e.data(), nocc, nvir, 0.0), 0,
+                       /*split_update=*/E.tc);
       // Y[f][p] = Wc_f b_p
       gemm(ctx, Tn, naux, naux, bp, ldn, 0, eps, ldn, stride, Yb, ldn, (size_t)Tn * ldn, fc, 1.0);
       k_grad_imag_pairs<<<dim3(Tn, fc), 256, 0, ctx->stream>>>(bp, ldn, Yb, Tn, naux, nmo, d_qp, d_mu, E.S.d_en,

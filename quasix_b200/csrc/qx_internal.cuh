@@ -155,6 +155,7 @@ enum WsSlot {
   WS_TCERR,       // tcgen05 pipeline error word
   WS_GRAD0, WS_GRAD1, WS_GRAD2,  // CD adjoint: accumulators, per-frequency chunk, lpq gradient
   WS_SWEEP_SPLIT,  // split sweep panels (two steps in flight)
+  WS_GUARD,        // guarded inversion: copies of eps and the pivoted fallback's work arrays
   WS_COUNT
 };
 static_assert(WS_COUNT <= 40, "workspace slots");
@@ -225,23 +226,78 @@ void launch_chi(qx_ctx* ctx, const double* energies, int nocc, int nvir, const d
 void launch_eps_fp64(qx_ctx* ctx, const double* bov, int ldov, int naux, int nov, const double* chi, int nw,
                      double* eps, int ldn, size_t eps_stride);
 
-// In-place inversion of nw SPD matrices by the block sweep operator;
+// ---------------------------------------------------------------------------
+// Guarded inversion (k_pivot.cu).  The block sweep has no pivoting; when eps
+// >= I cannot be shown, each eps is copied aside, the sweep flags a pivot
+// below kGuardPivot * max|eps| or an unswept entry above kGuardGrowth *
+// max|eps|, and the flagged matrices are inverted again from their copies by
+// Gauss-Jordan elimination with partial pivoting.
+// ---------------------------------------------------------------------------
+constexpr double kGuardPivot = 1e-6;
+constexpr double kGuardGrowth = 1e4;
+// Probe backward error max|eps X v - v| / (n max|eps| max|X|) above which the
+// sweep's inverse is redone with pivoting (a stable inverse gives ~1e-17).
+constexpr double kGuardResidual = 1e-15;
+
+// One guarded matrix.  The caller sets M, n, ldn, idx and status;
+// guard_layout places bk, ints and rbuf.
+struct GuardMat {
+  double* M;     // the matrix being inverted ([n][ldn], -eps^-1 after the sweep or the fallback)
+  double* bk;    // its copy, worked in place by the fallback
+  int n, ldn;
+  int idx;       // its index in the sweep (its max|eps| and growth words)
+  int unused_;
+  int* status;   // the sweep's status word of the matrix (nonzero: singular, Wc = 0)
+  int* ints;     // 3 n ints: row state, pivot row of each column, inverse permutation
+  double* rbuf;  // [n][32] the current panel's old pivot rows
+};
+struct GuardSet {
+  std::vector<GuardMat> mats;  // the guarded matrices
+  int nall = 0;                // matrices in the sweep (length of amax and growth)
+  GuardMat* d_tab = nullptr;
+  unsigned long long* amax = nullptr;    // [nall] max|eps| as a double's bits (0: not guarded)
+  unsigned long long* growth = nullptr;  // [nall] max over the unswept entries met by the sweep
+  unsigned long long* xmax = nullptr;    // [nall] max|eps^-1| of the sweep's result
+  unsigned long long* rmax = nullptr;    // [nall] probe residual max|eps X v - v|
+  int nflagged = 0;                      // matrices re-inverted by the last guard_end
+};
+// Workspace bytes of count guarded n x ldn matrices (an upper bound).
+size_t guard_bytes(int n, int ldn, int count);
+// Carve the workspace for gs.mats (and gs.nall words) out of mem.
+void guard_layout(GuardSet& gs, void* mem, size_t bytes);
+// Before the sweep, on the context stream: copies and max|eps|.
+void guard_begin(qx_ctx* ctx, GuardSet& gs);
+// After the sweep: synchronises the context stream, reads the flags and
+// re-inverts the flagged matrices with pivoting (queued on the context
+// stream).  Returns the number re-inverted.
+int guard_end(qx_ctx* ctx, GuardSet& gs);
+
+// eps >= I holds for eps = I + B diag(chi') B^T when every chi' >= 0: on the
+// imaginary axis when no occupied level lies above a virtual one, on the real
+// axis when in addition every shift |w| is below the smallest transition.
+// energies: [nocc + nvir] host array; wmax: largest |real shift| (0: imaginary
+// axis).  Strict inequalities keep chi' finite.
+bool eps_at_least_identity(const double* energies, int nocc, int nvir, double wmax);
+
+// In-place inversion of nw symmetric matrices by the block sweep operator;
 // output Wc = eps^-1 - I (FP64).
+// guard: the caller cannot show eps >= I (see eps_at_least_identity); the
+// sweep then runs guarded, with the pivoted fallback.
 // half_lower: return W' = strict-lower(Wc) + diag(Wc)/2 (zeros above) instead of Wc.
 // split_update: run the trailing updates on tcgen05 in the FP16X3 form
 // (launch_sweep_update_tc); the diagonal blocks and panels stay FP64.
-void launch_invert_wc(qx_ctx* ctx, double* eps, int n, int ldn, size_t stride, int nw, int half_lower = 0,
-                      int split_update = 0);
+void launch_invert_wc(qx_ctx* ctx, double* eps, int n, int ldn, size_t stride, int nw, int guard,
+                      int half_lower = 0, int split_update = 0);
 
 // One matrix of a grouped block sweep: M [n][ldn], symmetric, inverted in
 // place.  prow (its first row in the concatenated panel arrays, a multiple of
-// 128) is assigned by launch_invert_wc_group.
+// 128) is assigned by launch_invert_wc_group; guard as launch_invert_wc.
 struct GMat {
   double* M;
   int n;
   int ldn;
   int prow;
-  int unused;
+  int guard;
 };
 
 // Wc = eps^-1 - I in place for G symmetric matrices of different orders (the
@@ -254,12 +310,14 @@ void launch_invert_wc_group(qx_ctx* ctx, const GMat* mats, int G, int half_lower
 // The same sweep on caller-provided panels (no workspace, full Wc): Tp and Pp
 // hold nw * n * SWEEP_NB doubles each, Dp nw * SWEEP_NB^2, status nw ints that
 // must be zero on entry (nonzero on exit = singular eps, Wc set to 0).
+// guard_mem (guard_bytes(n, ldn, nw) bytes, or null for an unguarded sweep)
+// holds the guarded inversion's copies and work arrays.
 // sweep_set_attributes() raises the kernels' dynamic shared-memory limits on
 // the current device.
 constexpr int kSweepPanelCols = 128;
 void sweep_set_attributes();
 void launch_invert_wc_panels(qx_ctx* ctx, double* eps, int n, int ldn, size_t stride, int nw, double* Tp,
-                             double* Dp, double* Pp, int* status);
+                             double* Dp, double* Pp, int* status, void* guard_mem, size_t guard_mem_bytes);
 
 // v[w][p] = Bpt[p]^T Wc[w] Bpt[p] for all pairs (FP64), given W' (half-lower form).
 void launch_pair_contract_fp64(qx_ctx* ctx, const double* bpt, int ldk, int npair, int naux, const double* wc,

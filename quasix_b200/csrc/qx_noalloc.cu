@@ -1,14 +1,14 @@
 // qx_screened_interaction_noalloc: Wc = (I - Pi)^-1 - I on device arrays with
 // all scratch in one file-scope device array (no allocation in the call).
 //
-// Same arithmetic as qx_screened_interaction (the block sweep of
-// launch_invert_wc, correlation_ac.rs:377-401 in the reference), processed in
-// frequency chunks that fit the scratch array.  Scratch layout, each region
-// 256-byte aligned:
+// Same arithmetic as qx_screened_interaction (the guarded block sweep of
+// launch_invert_wc with its pivoted fallback, correlation_ac.rs:377-401 in the
+// reference), processed in frequency chunks that fit the scratch array.
+// Scratch layout, each region 256-byte aligned:
 //   status [kMaxFreq] int | eps [c][naux][ldn] | T panels [c][naux][128] | P panels [c][naux][128] |
-//   D blocks [c][128][128]
-// with c the chunk length.  Only the status words must start at zero; they are
-// cleared at the start of every call.
+//   D blocks [c][128][128] | guard (copies of eps and the fallback's work arrays, guard_bytes)
+// with c the chunk length.  Only the status words and the guard's bound words
+// must start at zero; both are cleared by every call before use.
 #include <mutex>
 
 #include "qx_internal.cuh"
@@ -29,11 +29,15 @@ static __device__ __align__(256) double qx_noalloc_scratch[kScratchBytes / sizeo
 
 inline size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
 
-// Bytes one frequency needs (eps, T and P panels, D block), each region rounded.
+// Bytes one frequency of the sweep needs (eps, T and P panels, D block),
+// each region rounded.
 inline size_t per_freq_bytes(int n, int ldn) {
   return align256((size_t)n * ldn * sizeof(double)) + 2 * align256((size_t)n * kSweepPanelCols * sizeof(double)) +
          align256((size_t)kSweepPanelCols * kSweepPanelCols * sizeof(double));
 }
+
+// Bytes of a chunk of c frequencies: the sweep's regions plus the guard's.
+inline size_t chunk_bytes(int n, int ldn, int c) { return (size_t)c * per_freq_bytes(n, ldn) + guard_bytes(n, ldn, c); }
 
 // Device address of the scratch array, resolved once per device with that
 // device current (the module holding it is loaded on first use).
@@ -87,12 +91,23 @@ void screened_noalloc(qx_ctx* ctx, int nfreq, int naux, const double* pi, double
   QX_REQUIRE(nfreq <= kMaxFreq, QX_ERR_INVALID_INPUT,
              "nfreq=%d exceeds the scratch limit of qx_screened_interaction_noalloc (nfreq <= %d)", nfreq,
              kMaxFreq);
-  QX_REQUIRE(is_device_ptr(pi) && is_device_ptr(wc), QX_ERR_INVALID_INPUT,
-             "qx_screened_interaction_noalloc takes device pointers only");
+  // Device (or managed) memory of the context's device: a kernel handed a
+  // pointer of another device, or a host pointer, would fault.
+  for (const void* p : {static_cast<const void*>(pi), static_cast<const void*>(wc)}) {
+    cudaPointerAttributes at;
+    const cudaError_t e = cudaPointerGetAttributes(&at, p);
+    if (e != cudaSuccess) cudaGetLastError();
+    QX_REQUIRE(e == cudaSuccess && (at.type == cudaMemoryTypeManaged ||
+                                    (at.type == cudaMemoryTypeDevice && at.device == ctx->device)),
+               QX_ERR_INVALID_INPUT,
+               "qx_screened_interaction_noalloc takes device pointers of the context's device (%d) only",
+               ctx->device);
+  }
   const int n = naux, ldn = round_up(naux, 8);
   const size_t stride = (size_t)n * ldn;
-  const size_t per = per_freq_bytes(n, ldn);
-  const int chunk = (int)std::min<size_t>((size_t)nfreq, (kScratchBytes - kStatusBytes) / per);
+  const size_t avail = kScratchBytes - kStatusBytes;
+  int chunk = (int)std::min<size_t>((size_t)nfreq, avail / per_freq_bytes(n, ldn));
+  while (chunk > 0 && chunk_bytes(n, ldn, chunk) > avail) --chunk;
   QX_REQUIRE(chunk >= 1, QX_ERR_INVALID_INPUT, "naux=%d does not fit the %zu-byte scratch", naux, kScratchBytes);
 
   char* base = reinterpret_cast<char*>(scratch_for_device(ctx->device));
@@ -103,6 +118,9 @@ void screened_noalloc(qx_ctx* ctx, int nfreq, int naux, const double* pi, double
                                          align256((size_t)chunk * n * kSweepPanelCols * sizeof(double)));
   double* Dp = reinterpret_cast<double*>(reinterpret_cast<char*>(Pp) +
                                          align256((size_t)chunk * n * kSweepPanelCols * sizeof(double)));
+  char* guard_mem = reinterpret_cast<char*>(Dp) +
+                    align256((size_t)chunk * kSweepPanelCols * kSweepPanelCols * sizeof(double));
+  const size_t guard_len = guard_bytes(n, ldn, chunk);
 
   QX_CUDA(cudaMemsetAsync(status, 0, (size_t)nfreq * sizeof(int), ctx->stream));
   for (int w0 = 0; w0 < nfreq; w0 += chunk) {
@@ -110,7 +128,8 @@ void screened_noalloc(qx_ctx* ctx, int nfreq, int naux, const double* pi, double
     dim3 g(std::min(ceil_div(n * ldn, 256), 4096), c);
     k_noalloc_load<<<g, 256, 0, ctx->stream>>>(pi + (size_t)w0 * n * n, n, ldn, stride, eps);
     check_launch(ctx);
-    launch_invert_wc_panels(ctx, eps, n, ldn, stride, c, Tp, Dp, Pp, status + w0);
+    // Pi comes from the caller: the sweep runs guarded (eps >= I cannot be assumed).
+    launch_invert_wc_panels(ctx, eps, n, ldn, stride, c, Tp, Dp, Pp, status + w0, guard_mem, guard_len);
     k_noalloc_store<<<g, 256, 0, ctx->stream>>>(eps, n, ldn, stride, wc + (size_t)w0 * n * n);
     check_launch(ctx);
   }
@@ -132,6 +151,7 @@ extern "C" qx_status qx_screened_interaction_noalloc(qx_ctx* ctx, int nfreq, int
                                                      double* wc) {
   if (!ctx) return QX_ERR_INVALID_INPUT;
   try {
+    reset_pending(ctx);
     ctx->launches = 0;
     QX_CUDA(cudaSetDevice(ctx->device));
     screened_noalloc(ctx, nfreq, naux, pi, wc);

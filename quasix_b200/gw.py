@@ -136,16 +136,16 @@ def ac_pade_thiele_diag(sigma, omega, npade: Optional[int] = None, device: int =
     return c, o
 
 
-def pade_thiele(omega, zn, coeff):
-    """Evaluate the continued fraction at real omega (scalar or array)."""
-    lib = N.load()
+def pade_thiele(omega, zn, coeff, device: int = 0):
+    """Evaluate the continued fraction of one orbital at real omega (scalar or
+    array) on the device."""
+    ctx = _ctx(device)
     zn = np.ascontiguousarray(zn, dtype=np.complex128)
     coeff = np.ascontiguousarray(coeff, dtype=np.complex128)
     w = _f64(np.atleast_1d(omega))
     out = np.zeros(w.shape[0], dtype=np.complex128)
-    st = lib.qx_pade_thiele(coeff.shape[0], N.ptr(zn), N.ptr(coeff), w.shape[0], N.ptr(w), N.ptr(out))
-    if st != 0:
-        raise N.QxValueError(st, "pade_thiele")
+    ctx.check(ctx.lib.qx_pade_thiele(ctx.handle, coeff.shape[0], N.ptr(zn), N.ptr(coeff), w.shape[0], N.ptr(w),
+                                     N.ptr(out)))
     return out[0] if np.ndim(omega) == 0 else out
 
 

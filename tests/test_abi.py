@@ -55,7 +55,3 @@ def test_host_only_entry_points():
         f, w = q.get_scaled_legendre_roots(nw, 0.5)
         f2, w2 = O.get_scaled_legendre_roots(nw, 0.5)
         assert np.allclose(f, f2, rtol=1e-11, atol=0) and np.allclose(w, w2, rtol=1e-11, atol=0)
-    zn = np.array([0.5j, 1j, 2j, 4j])
-    c = O.thiele(1.0 / (1.0 + zn), zn)
-    for om in (0.0, 0.1, -0.3):
-        assert abs(q.pade_thiele(om, zn, c) - O.pade_thiele(om, zn, c)) < 1e-14
