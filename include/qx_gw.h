@@ -376,6 +376,20 @@ qx_status qx_compute_absorption_spectrum(qx_ctx* ctx, const double* eigenvalues,
                                          double e_min, double e_max, int n_points, double* energies,
                                          double* intensities);
 
+/* qx_bse_root_grad with the gradient of Omega with respect to the DF blocks as
+ * passed to qx_bse_create (no reference counterpart): grad_ia [nov][naux],
+ * grad_ij [nocc*nocc][naux], grad_ab [nvirt*nvirt][naux], each entry the
+ * derivative with respect to that input entry (Hellmann-Feynman on the
+ * normalised x):
+ *   d/dB_ia^P = 2 alpha_x x_ia (B_ia^T x)_P [+ 8/Delta_ia (G B_ia)_P],
+ *   d/dB_ij^P = -(T W0)_(ij)P, T^Q_ij = sum_ab x_ia B_ab^Q x_jb,
+ *   d/dB_ab^Q = -sum_ij x_ia (B_ij W0)^Q_ij x_jb,
+ * the bracket (G = W0 sym(M) W0, M_PQ = sum_ij B_ij^P T^Q_ij) when mo_energy is
+ * given and W0 = (I - Pi(0))^-1 is taken to follow df_ia and the energies.
+ * Any output may be NULL (not all). */
+qx_status qx_bse_root_grad_b(qx_bse* bse, const double* x, const double* mo_energy, double* grad_energy,
+                             double* grad_ia, double* grad_ij, double* grad_ab);
+
 /* W(w=0) = (I - Pi(0))^-1 for the screened-direct kernel, from lpq_ov [naux][nocc][nvir]. */
 qx_status qx_bse_w0(qx_ctx* ctx, const double* mo_energy, const double* lpq_ov, int naux, int nocc,
                     int nvir, double* w0);

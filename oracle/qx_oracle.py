@@ -197,6 +197,41 @@ def get_sigma_diag(mo_energy: np.ndarray, lpq: np.ndarray, orbs: Sequence[int], 
     return sigma, omega
 
 
+def get_sigma_diag_threaded(mo_energy, lpq, orbs, nocc, nw=100, iw_cutoff=5.0, x0=0.5, workers=1):
+    """get_sigma_diag with its frequency loop on a thread pool, as the reference
+    runs it (rayon into_par_iter over frequencies, correlation_ac.rs:367-441):
+    each worker returns the contribution of its frequencies, summed afterwards
+    in frequency order.  Same arithmetic as get_sigma_diag per frequency."""
+    from concurrent.futures import ThreadPoolExecutor
+    naux, nmo, _ = lpq.shape
+    freqs, wts, iw = sigma_grid(nw, iw_cutoff, x0)
+    ef = 0.5 * (mo_energy[nocc - 1] + mo_energy[nocc])
+    emo_occ = (-1j * iw)[None, :] + ef - mo_energy[:, None]
+    emo_vir = (1j * iw)[None, :] + ef - mo_energy[:, None]
+    lpq_ov = lpq[:, :nocc, nocc:]
+    orbs = list(orbs)
+
+    def one(w):
+        pi = get_rho_response(freqs[w], mo_energy, lpq_ov)
+        wc = epsilon_inverse_minus_identity(pi)
+        g0_occ = wts[w] * emo_occ / (emo_occ * emo_occ + freqs[w] ** 2)
+        g0_vir = wts[w] * emo_vir / (emo_vir * emo_vir + freqs[w] ** 2)
+        part = np.zeros((len(orbs), iw.shape[0]), dtype=np.complex128)
+        for ni, n in enumerate(orbs):
+            q = wc.T @ lpq[:, n, :]
+            wmn = np.sum(q * lpq[:, :, n], axis=0)
+            part[ni] = (-1.0 / PI) * (wmn @ (g0_occ if n < nocc else g0_vir))
+        return part
+
+    with ThreadPoolExecutor(max(1, workers)) as ex:
+        parts = list(ex.map(one, range(nw)))
+    sigma = np.zeros((len(orbs), iw.shape[0]), dtype=np.complex128)
+    for part in parts:
+        sigma += part
+    omega = np.array([-1j * iw if o < nocc else 1j * iw for o in orbs])
+    return sigma, omega
+
+
 # ---------------------------------------------------------------------------
 # a6: Thiele / Pade analytic continuation
 # ---------------------------------------------------------------------------
@@ -1069,6 +1104,36 @@ def bse_root_grad(x, df_ia, df_ij, df_ab, w0, nocc, nvirt, mo_energy=None) -> np
     g[:nocc] -= gd.sum(axis=1)
     g[nocc:] += gd.sum(axis=0)
     return g
+
+
+def bse_root_grad_blocks(x, df_ia, df_ij, df_ab, w0, nocc, nvirt, mo_energy=None, alpha_x=2.0):
+    """dOmega/d(df_ia, df_ij, df_ab) for an eigenpair of A = diag(Delta) +
+    alpha_x B_ia B_ia^T - K^d(W0) (kernel.rs:344-462), by Hellmann-Feynman on
+    the normalised x (no reference counterpart):
+      d/dB_ia^P = 2 alpha_x x_ia (B_ia^T x)_P [+ 8/Delta_ia (G B_ia)_P],
+      d/dB_ij^P = -(T W0)_(ij)P,   T^Q_ij = sum_ab x_ia B_ab^Q x_jb,
+      d/dB_ab^Q = -sum_ij x_ia (B_ij W0)^Q_ij x_jb,
+    the bracket (G = W0 sym(M) W0, M_PQ = sum_ij B_ij^P T^Q_ij) when
+    W0 = (I - Pi(0))^-1 follows df_ia (mo_energy given), as in bse_root_grad.
+    Returns (grad_ia [nov, naux], grad_ij [nocc^2, naux], grad_ab [nvir^2, naux])."""
+    x = np.asarray(x, dtype=np.float64).reshape(-1)
+    xx = x / np.sqrt(x @ x)
+    X = xx.reshape(nocc, nvirt)
+    naux = df_ia.shape[1]
+    ab = df_ab.reshape(nvirt, nvirt, naux)
+    ij = df_ij.reshape(nocc, nocc, naux)
+    u = df_ia.T @ xx
+    g_ia = 2.0 * alpha_x * np.outer(xx, u)
+    T = np.einsum("ia,abQ,jb->ijQ", X, ab, X, optimize=True)
+    g_ij = -(T.reshape(nocc * nocc, naux) @ w0)
+    U = (df_ij @ w0).reshape(nocc, nocc, naux)
+    g_ab = -np.einsum("ia,ijQ,jb->abQ", X, U, X, optimize=True).reshape(nvirt * nvirt, naux)
+    if mo_energy is not None:
+        M = np.einsum("ijP,ijQ->PQ", ij, T, optimize=True)
+        G = w0 @ (0.5 * (M + M.T)) @ w0
+        delta = (mo_energy[None, nocc:] - mo_energy[:nocc, None]).reshape(-1)
+        g_ia += (8.0 / delta)[:, None] * (df_ia @ G)
+    return g_ia, g_ij, g_ab
 
 
 @dataclass

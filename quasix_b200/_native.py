@@ -113,6 +113,7 @@ SIGNATURES = {
     "qx_davidson_config_default": (None, [C.POINTER(DavidsonConfig)]),
     "qx_bse_davidson": (C.c_int, [_vp, C.POINTER(DavidsonConfig), _vp, _vp, _vp, _vp, _ip]),
     "qx_bse_root_grad": (C.c_int, [_vp, _vp, _vp, _vp]),
+    "qx_bse_root_grad_b": (C.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "qx_bse_w0": (C.c_int, [_vp, _vp, _vp, C.c_int, C.c_int, C.c_int, _vp]),
     "qx_compute_transition_dipoles": (C.c_int, [_vp, _vp, _vp, C.c_int, C.c_int, C.c_int, _vp]),
     "qx_transform_mo_3center": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int, C.c_int, C.c_int, C.c_int, _vp]),

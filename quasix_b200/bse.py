@@ -32,6 +32,19 @@ def _f64(a):
     return np.ascontiguousarray(np.asarray(a, dtype=np.float64))
 
 
+def _arr(a):
+    """A float64 CUDA tensor passes through (the library reads device memory);
+    anything else becomes a contiguous float64 numpy array."""
+    if hasattr(a, "data_ptr") and getattr(a, "is_cuda", False):
+        import torch
+        return a.to(torch.float64).contiguous()
+    return _f64(a)
+
+
+def _count(a) -> int:
+    return int(a.numel()) if hasattr(a, "numel") else int(a.size)
+
+
 def _prec(p) -> int:
     return p if isinstance(p, int) else N.PREC[p.lower()]
 
@@ -64,11 +77,14 @@ class BSETDAKernel:
         self.ctx = N.context(device)
         self._nocc, self._nvirt, self._naux = int(nocc), int(nvirt), int(naux)
         nov = self._nocc * self._nvirt
-        arrs = [_f64(delta_qp), _f64(df_ia), _f64(df_ij), _f64(df_ab), _f64(w0)]
+        arrs = [_arr(delta_qp), _arr(df_ia), _arr(df_ij), _arr(df_ab), _arr(w0)]
         expect = [(nov,), (nov, naux), (nocc * nocc, naux), (nvirt * nvirt, naux), (naux, naux)]
         for a, e, name in zip(arrs, expect, ["delta_qp", "df_ia", "df_ij", "df_ab", "w0"]):
-            if a.size != int(np.prod(e)):
-                raise ValueError(f"Failed to create BSE-TDA kernel: {name} has {a.size} elements, expected {e}")
+            if _count(a) != int(np.prod(e)):
+                raise ValueError(f"Failed to create BSE-TDA kernel: {name} has {_count(a)} elements, expected {e}")
+        if any(hasattr(a, "data_ptr") for a in arrs):
+            import torch
+            torch.cuda.current_stream().synchronize()
         h = C.c_void_p()
         self.ctx.check(self.ctx.lib.qx_bse_create(self.ctx.handle, C.byref(h), self._nocc, self._nvirt, self._naux,
                                                   *[N.ptr(a) for a in arrs], 0 if s == "singlet" else 1,
@@ -135,6 +151,23 @@ class BSETDAKernel:
         self.ctx.check(self.ctx.lib.qx_bse_root_grad(self.handle, N.ptr(xv), N.ptr(e) if e is not None else None,
                                                      N.ptr(g)))
         return g
+
+    def root_gradient_blocks(self, x, mo_energy=None):
+        """(dOmega/de [nocc + nvirt], dOmega/d df_ia [nov, naux], dOmega/d df_ij
+        [nocc^2, naux], dOmega/d df_ab [nvirt^2, naux]) of the eigenvalue with
+        eigenvector ``x`` (qx_bse_root_grad_b).  With ``mo_energy`` W0 is taken
+        as (I - Pi(0))^-1 of mo_energy and df_ia and its dependence on both is
+        included; otherwise W0 is held fixed."""
+        xv = _f64(x).reshape(-1)
+        if xv.shape[0] != self.dimension:
+            raise ValueError(f"Input vector length {xv.shape[0]} != BSE dimension {self.dimension}")
+        no, nv, na = self._nocc, self._nvirt, self._naux
+        ge = np.zeros(no + nv)
+        gia, gij, gab = np.zeros((no * nv, na)), np.zeros((no * no, na)), np.zeros((nv * nv, na))
+        e = None if mo_energy is None else _f64(mo_energy)
+        self.ctx.check(self.ctx.lib.qx_bse_root_grad_b(self.handle, N.ptr(xv), N.ptr(e) if e is not None else None,
+                                                       N.ptr(ge), N.ptr(gia), N.ptr(gij), N.ptr(gab)))
+        return ge, gia, gij, gab
 
     def close(self):
         if getattr(self, "handle", None):

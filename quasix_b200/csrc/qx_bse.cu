@@ -234,6 +234,7 @@ struct qx_bse {
   DevArr x_split;                    // split forms: hi/lo of the packed vectors
   DevArr xp, T, Yd, Z, Yx, Xr, Yr;  // matvec scratch
   DevArr gTt, gTp, gTpT, gdijT, gM, gG1, gG, gU;  // root-gradient scratch
+  DevArr gGrad;                                     // root-gradient scratch of the DF blocks
   DevArr V, AV, X, AX, R, heff, jv, Z2, small, eigi;
   std::vector<double> h_delta;
 };
@@ -848,10 +849,42 @@ static void gemm_nt(qx_ctx* ctx, int M, int N, int K, const double* A, int lda, 
   gemm_nt_f64(ctx, g);
 }
 
-qx_status qx_bse_root_grad(qx_bse* B, const double* x, const double* mo_energy, double* grad_energy) {
-  if (!B) return QX_ERR_INVALID_INPUT;
-  return bse_guard(B->ctx, [&] {
-    QX_REQUIRE(x && grad_energy, QX_ERR_INVALID_INPUT, "invalid arguments to bse_root_grad");
+}  // extern "C"
+
+// grad_ia[ia][P] = 2 alpha_x x_ia u_P - c_ia U[ia][P], u = B_ia^T x; c_ia = 8 / e_ia
+// (e_ia = e_i - e_a) when W0's dependence on B_ia is included, else 0.
+__global__ void k_grad_ia(const double* __restrict__ x, const double* __restrict__ u,
+                          const double* __restrict__ U, int ldu, const double* __restrict__ c, int nov, int naux,
+                          double alpha_x, double* __restrict__ out) {
+  for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < (size_t)nov * naux;
+       k += (size_t)gridDim.x * blockDim.x) {
+    const int ia = (int)(k / naux), P = (int)(k % naux);
+    double g = 2.0 * alpha_x * x[ia] * u[P];
+    if (c) g -= c[ia] * U[(size_t)ia * ldu + P];
+    out[k] = g;
+  }
+}
+
+// out[r][c] = in[r][c] for c < cols (drops the row padding).
+__global__ void k_unpad(const double* __restrict__ in, size_t rows, int cols, int ld, double* __restrict__ out) {
+  for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < rows * cols; k += (size_t)gridDim.x * blockDim.x)
+    out[k] = in[(k / cols) * ld + k % cols];
+}
+
+// Gradients of a root Omega = x^T H x (|x| = 1, Hellmann-Feynman) of the
+// kernel's matrix with respect to the orbital energies and, when requested,
+// to the DF blocks df_ia, df_ij, df_ab as given to qx_bse_create:
+//   H = diag(Delta) + alpha_x B_ia B_ia^T - K^d,  K^d_(ia)(jb) = sum_PQ B_ij^P W0_PQ B_ab^Q.
+// With T'^Q_ij = sum_ab x_ia B_ab^Q x_jb and M_PQ = sum_ij B_ij^P T'^Q_ij:
+//   dOmega/dB_ij^P = -(T' W0)_(ij)P,
+//   dOmega/dB_ab^Q = -sum_ij x_ia (B_ij W0)^Q_ij x_jb,
+//   dOmega/dB_ia^P = 2 alpha_x x_ia (B_ia^T x)_P [- 8 / e_ia (B_ia G)_P],
+// the bracket (with G = W0 sym(M) W0) when W0 = (I - Pi(0))^-1 follows B_ia
+// (mo_energy given), as for the energies: dW0 = W0 dPi W0, Pi(0) = 4 sum_ia
+// B_ia B_ia^T / e_ia.
+static void bse_root_grad_impl(qx_bse* B, const double* x, const double* mo_energy, double* grad_energy,
+                               double* grad_ia, double* grad_ij, double* grad_ab) {
+  {
     qx_ctx* ctx = B->ctx;
     const int nocc = B->nocc, nvir = B->nvir, naux = B->naux, nov = B->nov, ldq = B->ldq, ldvp = B->ldvp;
     std::vector<double> hx(nov);
@@ -868,9 +901,14 @@ qx_status qx_bse_root_grad(qx_bse* B, const double* x, const double* mo_energy, 
         g[i] -= w;
         g[nocc + a] += w;
       }
+    const bool want_b = grad_ia || grad_ij || grad_ab;
+    const int nq = nocc * ldq, n2o = nocc * nocc, ld2 = round_up(n2o, 8);
+    std::vector<double> e;
     if (mo_energy) {
-      std::vector<double> e(nocc + nvir);
+      e.resize(nocc + nvir);
       QX_CUDA(cudaMemcpy(e.data(), mo_energy, e.size() * sizeof(double), cudaMemcpyDefault));
+    }
+    if (mo_energy || want_b) {
       // T[a][j][Q] = sum_b x[j][b] B_ab^Q: the first step of the matvec (nvec = 1).
       std::vector<double> hr(B->ldov, 0.0);
       std::copy(hx.begin(), hx.end(), hr.begin());
@@ -878,13 +916,14 @@ qx_status qx_bse_root_grad(qx_bse* B, const double* x, const double* mo_energy, 
       B->Yr.alloc(B->ldov);
       QX_CUDA(cudaMemcpyAsync(B->Xr.p, hr.data(), B->ldov * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
       bse_apply_rows(B, B->Xr.p, B->Yr.p, 1, /*need_T=*/true);
-      const int nq = nocc * ldq, n2o = nocc * nocc, ld2 = round_up(n2o, 8);
       // T'[(i,j)][Q] = sum_a x[i][a] T[a][(j,Q)]
       B->gTt.alloc((size_t)nq * ldvp);
       QX_CUDA(cudaMemsetAsync(B->gTt.p, 0, (size_t)nq * ldvp * sizeof(double), ctx->stream));
       transpose(ctx, B->T.p, nvir, nq, nq, 0, B->gTt.p, ldvp, 0, 1);
       B->gTp.alloc((size_t)n2o * ldq);
       gemm_nt(ctx, nocc, nq, nvir, B->xp.p, ldvp, B->gTt.p, ldvp, B->gTp.p, nq);
+    }
+    if (mo_energy) {
       // M[P][Q] = sum_(ij) B_ij^P T'[(ij)][Q]
       B->gdijT.alloc((size_t)naux * ld2);
       B->gTpT.alloc((size_t)ldq * ld2);
@@ -918,7 +957,146 @@ qx_status qx_bse_root_grad(qx_bse* B, const double* x, const double* mo_energy, 
           g[nocc + a] += gd;
         }
     }
-    QX_CUDA(cudaMemcpy(grad_energy, g.data(), g.size() * sizeof(double), cudaMemcpyDefault));
+    if (grad_energy) QX_CUDA(cudaMemcpy(grad_energy, g.data(), g.size() * sizeof(double), cudaMemcpyDefault));
+    if (!want_b) return;
+    // Scratch for the block gradients: u, c, the padded ij and ab results.
+    const int ldo8 = round_up(nocc, 8);
+    DevArr& gs = B->gGrad;
+    const size_t n_u = ldq, n_c = B->ldov, n_ij = (size_t)n2o * ldq, n_xt = (size_t)nvir * ldo8,
+                 n_ut = (size_t)nocc * naux * ldo8, n_v = (size_t)nocc * nvir * ldq, n_vt = (size_t)nvir * ldq * ldo8,
+                 n_ab = (size_t)nvir * nvir * ldq, n_out = std::max({(size_t)nov, (size_t)n2o, (size_t)nvir * nvir}) * naux;
+    gs.alloc(n_u + n_c + n_ij + n_xt + n_ut + n_v + n_vt + n_ab + n_out + 64);
+    double* u = gs.p;
+    double* cia = u + n_u;
+    double* gij = cia + n_c;
+    double* xt = gij + n_ij;
+    double* ut = xt + n_xt;
+    double* v = ut + n_ut;
+    double* vt = v + n_v;
+    double* gab = vt + n_vt;
+    double* outb = gab + n_ab;
+    auto copy_out = [&](const double* src, size_t rows, int ld, double* dst) {
+      const double* s = src;
+      if (ld != naux) {
+        k_unpad<<<(unsigned)std::min<size_t>((rows * naux + 255) / 256, 8192), 256, 0, ctx->stream>>>(src, rows, naux,
+                                                                                                     ld, outb);
+        check_launch(ctx);
+        s = outb;
+      }
+      QX_CUDA(cudaMemcpyAsync(dst, s, rows * naux * sizeof(double), cudaMemcpyDefault, ctx->stream));
+      sync_and_check(ctx);  // outb is reused by the next block
+    };
+    if (grad_ia) {
+      // u[P] = sum_ia x_ia B_ia^P.
+      GemmNT gu{};
+      gu.M = 1;
+      gu.N = naux;
+      gu.K = nov;
+      gu.A = B->Xr.p;
+      gu.lda = B->ldov;
+      gu.B = B->diaT.p;
+      gu.ldb = B->ldov;
+      gu.C = u;
+      gu.ldc = ldq;
+      gu.batch = 1;
+      gu.alpha = 1.0;
+      gu.splitk = 0;
+      gemm_nt_f64(ctx, gu);
+      const double* cptr = nullptr;
+      if (mo_energy) {
+        std::vector<double> hc(nov);
+        for (int i = 0; i < nocc; ++i)
+          for (int a = 0; a < nvir; ++a) hc[(size_t)i * nvir + a] = 8.0 / (e[i] - e[nocc + a]);
+        QX_CUDA(cudaMemcpyAsync(cia, hc.data(), nov * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+        cptr = cia;
+      }
+      k_grad_ia<<<(unsigned)std::min<size_t>(((size_t)nov * naux + 255) / 256, 8192), 256, 0, ctx->stream>>>(
+          B->Xr.p, u, B->gU.p, ldq, cptr, nov, naux, B->alpha_x, outb);
+      check_launch(ctx);
+      QX_CUDA(cudaMemcpyAsync(grad_ia, outb, (size_t)nov * naux * sizeof(double), cudaMemcpyDefault, ctx->stream));
+      sync_and_check(ctx);
+    }
+    if (grad_ij) {
+      // grad_ij[(ij)][P] = -sum_Q T'[(ij)][Q] W0[Q][P]  (w0T rows are W0's columns).
+      GemmNT gg{};
+      gg.M = n2o;
+      gg.N = naux;
+      gg.K = naux;
+      gg.A = B->gTp.p;
+      gg.lda = ldq;
+      gg.B = B->w0T.p;
+      gg.ldb = ldq;
+      gg.C = gij;
+      gg.ldc = ldq;
+      gg.batch = 1;
+      gg.alpha = -1.0;
+      gg.splitk = 0;
+      gemm_nt_f64(ctx, gg);
+      copy_out(gij, n2o, ldq, grad_ij);
+    }
+    if (grad_ab) {
+      // x^T [b][j] and U^T[i][Q][j] with U = ijw = B_ij W0 ([(i,j)][Q]).
+      QX_CUDA(cudaMemsetAsync(xt, 0, n_xt * sizeof(double), ctx->stream));
+      QX_CUDA(cudaMemsetAsync(ut, 0, n_ut * sizeof(double), ctx->stream));
+      transpose(ctx, B->xp.p, nocc, nvir, ldvp, 0, xt, ldo8, 0, 1);
+      transpose(ctx, B->ijw.p, nocc, naux, ldq, (size_t)nocc * ldq, ut, ldo8, (size_t)naux * ldo8, nocc);
+      // V[i][b][Q] = sum_j x[j][b] U[(i,j)][Q]
+      GemmNT ga{};
+      ga.M = nvir;
+      ga.N = naux;
+      ga.K = nocc;
+      ga.A = xt;
+      ga.lda = ldo8;
+      ga.sA = 0;
+      ga.B = ut;
+      ga.ldb = ldo8;
+      ga.sB = (size_t)naux * ldo8;
+      ga.C = v;
+      ga.ldc = ldq;
+      ga.sC = (size_t)nvir * ldq;
+      ga.batch = nocc;
+      ga.alpha = 1.0;
+      ga.splitk = 1;
+      gemm_nt_f64(ctx, ga);
+      // grad_ab[a][(b,Q)] = -sum_i x[i][a] V[i][(b,Q)]
+      QX_CUDA(cudaMemsetAsync(vt, 0, n_vt * sizeof(double), ctx->stream));
+      transpose(ctx, v, nocc, nvir * ldq, nvir * ldq, 0, vt, ldo8, 0, 1);
+      GemmNT gb{};
+      gb.M = nvir;
+      gb.N = nvir * ldq;
+      gb.K = nocc;
+      gb.A = xt;
+      gb.lda = ldo8;
+      gb.B = vt;
+      gb.ldb = ldo8;
+      gb.C = gab;
+      gb.ldc = nvir * ldq;
+      gb.batch = 1;
+      gb.alpha = -1.0;
+      gb.splitk = 1;
+      gemm_nt_f64(ctx, gb);
+      copy_out(gab, (size_t)nvir * nvir, ldq, grad_ab);
+    }
+  }
+}
+
+extern "C" {
+
+qx_status qx_bse_root_grad(qx_bse* B, const double* x, const double* mo_energy, double* grad_energy) {
+  if (!B) return QX_ERR_INVALID_INPUT;
+  return bse_guard(B->ctx, [&] {
+    QX_REQUIRE(x && grad_energy, QX_ERR_INVALID_INPUT, "invalid arguments to bse_root_grad");
+    bse_root_grad_impl(B, x, mo_energy, grad_energy, nullptr, nullptr, nullptr);
+  });
+}
+
+qx_status qx_bse_root_grad_b(qx_bse* B, const double* x, const double* mo_energy, double* grad_energy,
+                             double* grad_ia, double* grad_ij, double* grad_ab) {
+  if (!B) return QX_ERR_INVALID_INPUT;
+  return bse_guard(B->ctx, [&] {
+    QX_REQUIRE(x && (grad_energy || grad_ia || grad_ij || grad_ab), QX_ERR_INVALID_INPUT,
+               "invalid arguments to bse_root_grad_b");
+    bse_root_grad_impl(B, x, mo_energy, grad_energy, grad_ia, grad_ij, grad_ab);
   });
 }
 

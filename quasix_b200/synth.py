@@ -78,15 +78,23 @@ def pi0_spectral_norm(mo_energy: np.ndarray, lpq: np.ndarray, nocc: int) -> floa
     return float(np.abs(np.linalg.eigvalsh(pi0)).max())
 
 
-def make_system(nocc: int, nvir: int, naux: int, seed: int, pi_norm: float) -> SyntheticSystem:
-    """Build one seeded synthetic system (see module docstring)."""
+def draw_system(nocc: int, nvir: int, naux: int, seed: int):
+    """The seeded draws of one system, in the order (occupied energies, virtual
+    energies, upper triangle of B by (P, then row-major p <= q)): returns
+    (mo_energy [nmo], upper [naux, nmo (nmo + 1) / 2]) before the rescaling."""
     rng = np.random.default_rng(seed)
     nmo = nocc + nvir
     e_occ = np.sort(rng.uniform(-1.2, -0.3, nocc))
     e_vir = np.sort(rng.uniform(0.05, 3.0, nvir))
-    mo_energy = np.concatenate([e_occ, e_vir])
+    upper = rng.normal(0.0, 0.05, size=(naux, nmo * (nmo + 1) // 2))
+    return np.concatenate([e_occ, e_vir]), upper
+
+
+def make_system(nocc: int, nvir: int, naux: int, seed: int, pi_norm: float) -> SyntheticSystem:
+    """Build one seeded synthetic system (see module docstring)."""
+    nmo = nocc + nvir
+    mo_energy, upper = draw_system(nocc, nvir, naux, seed)
     iu, ju = np.triu_indices(nmo)
-    upper = rng.normal(0.0, 0.05, size=(naux, iu.shape[0]))
     lpq = np.empty((naux, nmo, nmo))
     lpq[:, iu, ju] = upper
     lpq[:, ju, iu] = upper
@@ -133,6 +141,56 @@ def grad_nmo200() -> SyntheticSystem:
 def bse_dim26400_bov() -> SyntheticSystem:
     """nocc 60, nvirt 440, naux 1800, seed 11, ||Pi(0)|| = 5 (full tensor is 3.6 GB)."""
     return make_system(60, 440, 1800, seed=11, pi_norm=5.0)
+
+
+def bse_blocks(lpq: np.ndarray, nocc: int):
+    """The BSE kernel's DF blocks in the layouts of BSETDAKernel::new
+    (quasix_core/src/bse/kernel.rs:259-337): df_ia [nocc*nvir, naux],
+    df_ij [nocc*nocc, naux], df_ab [nvir*nvir, naux]."""
+    naux = lpq.shape[0]
+    t = lpq.transpose(1, 2, 0)
+    dia = np.ascontiguousarray(t[:nocc, nocc:]).reshape(-1, naux)
+    dij = np.ascontiguousarray(t[:nocc, :nocc]).reshape(-1, naux)
+    dab = np.ascontiguousarray(t[nocc:, nocc:]).reshape(-1, naux)
+    return dia, dij, dab
+
+
+def systems_on_device(shapes, device: int = 0, threads: int = 8):
+    """make_system for many shapes, resident on the GPU: the seeded numpy draws
+    of draw_system (the same numbers make_system uses) run on a thread pool
+    (numpy's generators release the GIL), and each system is mirrored and
+    rescaled on the device.  shapes: (seed, nocc, nvir, naux, pi_norm) tuples.
+    Returns [(mo_energy, lpq)] as CUDA float64 tensors; the rescaling's
+    spectral norm comes from the device eigensolver, so lpq equals
+    make_system's to rounding."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    import torch
+    dev = torch.device("cuda", device)
+    out = [None] * len(shapes)
+
+    def draw(i):
+        seed, nocc, nvir, naux, _ = shapes[i]
+        return i, draw_system(nocc, nvir, naux, seed)
+
+    with ThreadPoolExecutor(max(1, threads)) as ex:
+        for i, (e, upper) in ex.map(draw, range(len(shapes))):
+            seed, nocc, nvir, naux, pin = shapes[i]
+            nmo = nocc + nvir
+            up = torch.from_numpy(upper).to(dev)
+            del upper
+            iu, ju = torch.triu_indices(nmo, nmo, device=dev)
+            lpq = torch.empty((naux, nmo, nmo), dtype=torch.float64, device=dev)
+            lpq[:, iu, ju] = up
+            lpq[:, ju, iu] = up
+            del up
+            ed = torch.from_numpy(e).to(dev)
+            bov = lpq[:, :nocc, nocc:].reshape(naux, -1)
+            e_ia = (ed[:nocc, None] - ed[None, nocc:]).reshape(-1)
+            pi0 = 4.0 * (bov / e_ia) @ bov.T
+            lpq *= torch.sqrt(pin / torch.linalg.eigvalsh(pi0).abs().max())
+            out[i] = (ed, lpq)
+    return out
 
 
 def make_system_device(nocc: int, nvir: int, naux: int, seed: int, pi_norm: float, device: int = 0):

@@ -1,9 +1,11 @@
 """Device Thiele/Pade entry points and spectral functions against the oracle.
 
 Tolerances: the Pade fit and evaluation are the same FP64 recursion as the
-oracle's (1e-12 relative on coefficients of the well-conditioned reference
-point rule); the broadened spectral sums are FP64 sums of exp / rational
-terms (1e-13 relative to max|A|).
+oracle's; the reciprocal differences amplify the last-bit differences of the
+complex divisions (the device divides by b conj(b), numpy scales first), so
+the coefficients agree to 1e-11 relative and the continued fraction's values
+to 1e-12; the broadened spectral sums are FP64 sums of exp / rational terms
+(1e-13 relative to max|A|).
 """
 import numpy as np
 import pytest
@@ -42,7 +44,12 @@ def test_thiele_fit_on_device_matches_oracle(q):
         c, f = q.ac_pade_thiele_diag(sig, om, npade)
         c2, f2 = O.ac_pade_thiele_diag(sig, om, npade)
         assert np.array_equal(f, f2)
-        assert rel(c, c2) < 1e-12
+        assert rel(c, c2) < 1e-11
+        w = np.linspace(-1.0, 1.0, 7)
+        for p in (0, 4, 5, 23):
+            got = q.pade_thiele(w, f[p], c[:, p])
+            ref = np.array([O.pade_thiele(x, f2[p], c2[:, p]) for x in w])
+            assert rel(got, ref) < 1e-12
 
 
 def test_spectral_function_matches_oracle(q):
