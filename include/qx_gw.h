@@ -59,6 +59,10 @@ qx_status qx_ctx_last_timings(const qx_ctx* ctx, double* ms_p0, double* ms_inv, 
                               double* ms_sigma, double* ms_qp);
 /* Number of kernel launches issued by the last call. */
 int64_t qx_ctx_last_launches(const qx_ctx* ctx);
+/* eps inversions of the last call that ran guarded (eps >= I not certain),
+ * and how many of those were re-inverted with pivoting (no reference
+ * counterpart).  Either pointer may be NULL. */
+qx_status qx_ctx_last_guard_stats(const qx_ctx* ctx, int64_t* guarded, int64_t* reinverted);
 /* Library version string. */
 const char* qx_version(void);
 
@@ -296,7 +300,7 @@ qx_status qx_transform_mo_3center(qx_ctx* ctx, const double* j3c_ao, const doubl
 
 /* J^-1/2 and J^1/2 of the Coulomb metric J = (P|Q) (quasix/quasix/evgw.py:
  * 1014-1046, there by eigh with eigenvalues clamped at thresh_df) by the
- * coupled Newton-Schulz iteration on the device.  A metric with an eigenvalue
+ * scaled Denman-Beavers iteration on the device.  A metric with an eigenvalue
  * at or below thresh returns QX_ERR_NUMERICAL (the clamping is not
  * reproduced).  metric, inv_sqrt, sqrt_metric (may be NULL): [naux][naux]. */
 qx_status qx_metric_inv_sqrt(qx_ctx* ctx, const double* metric, int naux, double thresh, double* inv_sqrt,

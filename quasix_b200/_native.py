@@ -79,6 +79,7 @@ SIGNATURES = {
     "qx_ctx_set_stream": (C.c_int, [_vp, _vp]),
     "qx_ctx_last_timings": (C.c_int, [_vp, _dp, _dp, _dp, _dp, _dp]),
     "qx_ctx_last_launches": (C.c_int64, [_vp]),
+    "qx_ctx_last_guard_stats": (C.c_int, [_vp, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
     "qx_version": (C.c_char_p, []),
     "qx_get_scaled_legendre_roots": (C.c_int, [C.c_int, C.c_double, _vp, _vp]),
     "qx_get_rho_response": (C.c_int, [_vp, C.c_int, _vp, _vp, _vp, C.c_int, C.c_int, C.c_int, C.c_int, _vp]),
@@ -186,6 +187,13 @@ class Context:
 
     def launches(self) -> int:
         return int(self.lib.qx_ctx_last_launches(self.handle))
+
+    def guard_stats(self):
+        """(guarded, reinverted): eps inversions of the last call that ran
+        guarded, and those re-inverted with pivoting."""
+        g, r = C.c_int64(0), C.c_int64(0)
+        self.check(self.lib.qx_ctx_last_guard_stats(self.handle, C.byref(g), C.byref(r)))
+        return int(g.value), int(r.value)
 
     def set_stream(self, stream_handle: int | None):
         self.check(self.lib.qx_ctx_set_stream(self.handle, stream_handle))

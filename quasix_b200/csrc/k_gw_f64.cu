@@ -598,6 +598,9 @@ static void sweep_update(qx_ctx* ctx, cudaStream_t st, double* eps, int n, int l
 void launch_invert_wc(qx_ctx* ctx, double* eps, int n, int ldn, size_t stride, int nw, int guard, int half_lower,
                       int split_update) {
   QX_REQUIRE(nw >= 1 && nw <= 65535, QX_ERR_INVALID_INPUT, "%d matrices in one sweep (1 to 65535)", nw);
+  // The split trailing update's error bound needs eps >= I: guarded matrices
+  // are swept with FP64 updates.
+  if (guard) split_update = 0;
   const size_t pstride = (size_t)n * SWEEP_NB;
   const size_t dsz = (size_t)nw * SWEEP_NB * SWEEP_NB;
   DevBuf& pan = ctx->ws[WS_PANEL];
@@ -823,7 +826,9 @@ void launch_invert_wc_group(qx_ctx* ctx, const GMat* mats_in, int G, int half_lo
   }
   const int R = prow;
   const int nsteps = ceil_div(m[0].n, SWEEP_NB);
-  const bool tc = split_update != 0;
+  bool any_guard = false;
+  for (int i = 0; i < G; ++i) any_guard = any_guard || m[i].guard;
+  const bool tc = split_update != 0 && !any_guard;
   // Prefix tables: per step the tpanel, write and update CTA counts of the
   // active matrices, then the finish counts of all.
   std::vector<int> tab;
@@ -888,6 +893,8 @@ void launch_invert_wc_group(qx_ctx* ctx, const GMat* mats_in, int G, int half_lo
       gs.mats.push_back(gm);
     }
   const bool guarded = !gs.mats.empty();
+  // As launch_invert_wc: no split trailing update once any matrix is guarded.
+  if (guarded) split_update = 0;
   if (guarded) {
     size_t bytes = 0;
     for (const GuardMat& gm : gs.mats) bytes += guard_bytes(gm.n, gm.ldn, 1);

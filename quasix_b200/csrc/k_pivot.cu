@@ -39,7 +39,10 @@ namespace qx {
 
 namespace {
 
-constexpr int PIV_NB = 32;
+constexpr int PIV_NB = 16;
+// Rows of a panel held in shared memory ([n][PIV_NB] doubles plus n row states).
+constexpr int kPivSmemRows = 1700;
+constexpr size_t kPivSmemBytes = (size_t)kPivSmemRows * (PIV_NB * sizeof(double) + sizeof(int)) + 1024;
 using PivTile = F64Tile<64, 64, 2, 2, 3>;
 
 // Block-wide argmax of (v, r): largest v, ties to the smallest r (every
@@ -156,19 +159,41 @@ __global__ void k_piv_init(const GuardMat* __restrict__ tab) {
 //   T[p][c] = 1/d, T[p][j] = -T[p][j]/d, T[i][c] = T[i][c]/d,
 //   T[i][j] -= T[i][c] T[p][j]/d        (i != p, j != c),
 // applied here to the panel columns only (they depend on nothing else).  The
-// pivot row of column c is the unused row of largest |T[r][c]|.  Afterwards
-// rbuf[j][b] = the old row piv[k0 + b] outside the panel (zero inside), the
-// operand of the update of the other columns.
+// pivot row of column c is the unused row of largest |T[r][c]| (ties to the
+// lowest row).  SMEM: the panel and the row states sit in shared memory for
+// the kb steps (n <= kPivSmemRows); otherwise every step works on bk itself.
+// Each half-warp holds one row, a lane one column.  Afterwards rbuf[j][b] =
+// the old row piv[k0 + b] outside the panel (zero inside), the operand of the
+// update of the other columns.
+template <bool SMEM>
 __global__ void __launch_bounds__(512) k_piv_panel(const GuardMat* __restrict__ tab, int k0) {
   const GuardMat g = tab[blockIdx.x];
   const int n = g.n;
   if (k0 >= n || *g.status != 0) return;
   const int kb = min(PIV_NB, n - k0), lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int nwarp = blockDim.x >> 5;
-  int* state = g.ints;
+  const int half = lane >> 4, col = lane & 15;
+  int* gstate = g.ints;
   int* piv = g.ints + n;
-  double* A = g.bk;
-  const size_t ld = g.ldn;
+  extern __shared__ __align__(16) uint8_t pan_smem[];
+  double* P;  // panel element (r, c) at P[r * pld + c]
+  int* state;
+  size_t pld;
+  if (SMEM) {
+    P = reinterpret_cast<double*>(pan_smem);
+    state = reinterpret_cast<int*>(P + (size_t)n * PIV_NB);
+    pld = PIV_NB;
+    for (int e = threadIdx.x; e < n * PIV_NB; e += blockDim.x) {
+      const int r = e / PIV_NB, c = e % PIV_NB;
+      P[e] = c < kb ? g.bk[(size_t)r * g.ldn + k0 + c] : 0.0;
+    }
+    for (int r = threadIdx.x; r < n; r += blockDim.x) state[r] = gstate[r];
+    __syncthreads();
+  } else {
+    P = g.bk + k0;
+    state = gstate;
+    pld = g.ldn;
+  }
   __shared__ double prow[PIV_NB];
   __shared__ double sv[32];
   __shared__ int sr[32];
@@ -177,7 +202,7 @@ __global__ void __launch_bounds__(512) k_piv_panel(const GuardMat* __restrict__ 
   int bi = INT_MAX;
   for (int r = threadIdx.x; r < n; r += blockDim.x)
     if (state[r] < 0) {
-      const double v = fabs(A[(size_t)r * ld + k0]);
+      const double v = fabs(P[(size_t)r * pld]);
       if (v > best || (v == best && r < bi)) {
         best = v;
         bi = r;
@@ -186,12 +211,12 @@ __global__ void __launch_bounds__(512) k_piv_panel(const GuardMat* __restrict__ 
   for (int j = 0; j < kb; ++j) {
     block_argmax(best, bi, sv, sr);
     const int p = bi;
-    const double d = (p == INT_MAX) ? 0.0 : A[(size_t)p * ld + k0 + j];
+    const double d = (p == INT_MAX) ? 0.0 : P[(size_t)p * pld + j];
     if (!(fabs(d) > 0.0) || !isfinite(d)) {  // uniform: p and d are the same in every thread
       if (threadIdx.x == 0) *g.status = 1;
       return;
     }
-    if (warp == 0) prow[lane] = lane < kb ? A[(size_t)p * ld + k0 + lane] : 0.0;
+    if (threadIdx.x < PIV_NB) prow[threadIdx.x] = threadIdx.x < kb ? P[(size_t)p * pld + threadIdx.x] : 0.0;
     __syncthreads();
     if (threadIdx.x == 0) {
       state[p] = k0;
@@ -200,19 +225,24 @@ __global__ void __launch_bounds__(512) k_piv_panel(const GuardMat* __restrict__ 
     const double inv = 1.0 / d;
     best = -1.0;
     bi = INT_MAX;
-    for (int r = warp; r < n; r += nwarp) {
-      double* row = A + (size_t)r * ld + k0;
-      double v = lane < kb ? row[lane] : 0.0;
+    // Row r of this half-warp (the loop bound is warp-uniform: both halves
+    // run every iteration, a half past n holding a dummy row).
+    for (int r0 = 2 * warp; r0 < n; r0 += 2 * nwarp) {
+      const int r = r0 + half;
+      const bool live = r < n;
+      double* row = P + (size_t)(live ? r : 0) * pld;
+      double v = (live && col < kb) ? row[col] : 0.0;
+      const double arj = __shfl_sync(0xffffffffu, v, (lane & 16) | j);
       if (r == p) {
-        v = (lane == j) ? inv : -prow[lane] * inv;
+        v = (col == j) ? inv : -prow[col] * inv;
       } else {
-        const double t = __shfl_sync(0xffffffffu, v, j) * inv;
-        v = (lane == j) ? t : v - t * prow[lane];
+        const double t = arj * inv;
+        v = (col == j) ? t : v - t * prow[col];
       }
-      if (lane < kb) row[lane] = v;
-      if (j + 1 < kb && r != p) {
-        const double cv = fabs(__shfl_sync(0xffffffffu, v, j + 1));
-        if (state[r] < 0 && (cv > best || (cv == best && r < bi))) {
+      if (live && col < kb) row[col] = v;
+      if (j + 1 < kb) {
+        const double cv = fabs(__shfl_sync(0xffffffffu, v, (lane & 16) | (j + 1)));
+        if (live && r != p && state[r] < 0 && (cv > best || (cv == best && r < bi))) {
           best = cv;
           bi = r;
         }
@@ -220,11 +250,19 @@ __global__ void __launch_bounds__(512) k_piv_panel(const GuardMat* __restrict__ 
     }
     __syncthreads();
   }
-  // rbuf[j][b] = A[piv[k0 + b]][j] for columns outside the panel.
+  if (SMEM) {
+    for (int e = threadIdx.x; e < n * PIV_NB; e += blockDim.x) {
+      const int r = e / PIV_NB, c = e % PIV_NB;
+      if (c < kb) g.bk[(size_t)r * g.ldn + k0 + c] = P[e];
+    }
+    for (int r = threadIdx.x; r < n; r += blockDim.x) gstate[r] = state[r];
+  }
+  // rbuf[j][b] = A[piv[k0 + b]][j] for columns outside the panel (A's columns
+  // outside the panel are untouched so far).
   for (int b = warp; b < kb; b += nwarp) {
-    const double* src = A + (size_t)piv[k0 + b] * ld;
-    for (int j = lane; j < n; j += 32)
-      g.rbuf[(size_t)j * PIV_NB + b] = (j >= k0 && j < k0 + kb) ? 0.0 : src[j];
+    const double* src = g.bk + (size_t)piv[k0 + b] * g.ldn;
+    for (int jj = lane; jj < n; jj += 32)
+      g.rbuf[(size_t)jj * PIV_NB + b] = (jj >= k0 && jj < k0 + kb) ? 0.0 : src[jj];
   }
 }
 
@@ -331,6 +369,8 @@ void guard_begin(qx_ctx* ctx, GuardSet& gs) {
   static PerDeviceOnce attr_once;
   attr_once(ctx->device, [] {
     QX_CUDA(cudaFuncSetAttribute(k_piv_update, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PivTile::SMEM));
+    QX_CUDA(cudaFuncSetAttribute(k_piv_panel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)kPivSmemBytes));
   });
   QX_CUDA(cudaMemsetAsync(gs.amax, 0, gs.nall * sizeof(unsigned long long), ctx->stream));
   QX_CUDA(cudaMemsetAsync(gs.growth, 0, gs.nall * sizeof(unsigned long long), ctx->stream));
@@ -387,6 +427,8 @@ int guard_end(qx_ctx* ctx, GuardSet& gs) {
     }
   }
   gs.nflagged = (int)flagged.size();
+  ctx->guard_matrices += G;
+  ctx->guard_reinverted += gs.nflagged;
   if (flagged.empty()) return 0;
   const int F = (int)flagged.size();
   QX_REQUIRE(F <= 65535, QX_ERR_INVALID_INPUT, "%d matrices to re-invert in one call (at most 65535)", F);
@@ -394,8 +436,13 @@ int guard_end(qx_ctx* ctx, GuardSet& gs) {
   k_piv_init<<<F, 256, 0, ctx->stream>>>(gs.d_tab);
   check_launch(ctx);
   const int tiles = ceil_div(nmax, PivTile::BM);
+  const bool smem_panel = nmax <= kPivSmemRows;
+  const size_t panel_smem = (size_t)nmax * (PIV_NB * sizeof(double) + sizeof(int));
   for (int k0 = 0; k0 < nmax; k0 += PIV_NB) {
-    k_piv_panel<<<F, 512, 0, ctx->stream>>>(gs.d_tab, k0);
+    if (smem_panel)
+      k_piv_panel<true><<<F, 512, panel_smem, ctx->stream>>>(gs.d_tab, k0);
+    else
+      k_piv_panel<false><<<F, 512, 0, ctx->stream>>>(gs.d_tab, k0);
     check_launch(ctx);
     k_piv_update<<<dim3(tiles, tiles, F), PivTile::THREADS, PivTile::SMEM, ctx->stream>>>(gs.d_tab, k0);
     check_launch(ctx);

@@ -183,6 +183,14 @@ struct TcWarps {
   static constexpr int NEPI = 8;
   static constexpr int THREADS = 64 + 32 * NEPI;
 };
+// Converter warps of the STORE form whose B operand is built in shared memory
+// (CONVB): the FP32 source times a per-batch column scale, split into hi/lo
+// and written in the 128-byte-swizzled layout that TMA would have written.
+constexpr int kConvWarps = 2;
+template <int EPI, bool CONVB>
+struct TcThreads {
+  static constexpr int VALUE = TcWarps<EPI>::THREADS + (CONVB ? 32 * kConvWarps : 0);
+};
 
 template <int BN, int EPI>
 struct TcSmem {
@@ -229,7 +237,21 @@ struct TcArgs {
   const int* gpre;
   int gcount;
   int unit;  // STORE: k-blocks per FP32 accumulation unit (0 counts as 1)
+  // CONVB: B[w][n][k] = convB[n][k] * convC[w][k] (FP32, both zero past K),
+  // converted to hi/lo by the converter warps instead of TMA loads.
+  const float* convB;
+  int ldconv;
+  const float* convC;
+  int ldcc;
 };
+
+// Byte offset of the 16-bit element (row r, column c) in a 64-wide K-major
+// tile with the 128-byte swizzle (the layout TMA's SWIZZLE_128B writes into a
+// 1024-byte-aligned buffer, umma_desc<64>): rows of 128 bytes, whose 16-byte
+// chunks are permuted by chunk ^ (r % 8).
+__device__ __forceinline__ uint32_t sw128_offset(int r, int c) {
+  return (uint32_t)r * 128u + ((uint32_t)((c >> 3) ^ (r & 7)) << 4) + (uint32_t)(c & 7) * 2u;
+}
 
 // x[q] = xr[q] for the columns col0 + q < N of a valid row, 0 otherwise
 // (vector loads for a full chunk; indices are compile-time, x stays in registers).
@@ -253,10 +275,11 @@ __device__ __forceinline__ double unscale_rowdot(const TcArgs& a, int w) {
   return 1.0 / ((double)a.scaleA[0] * (double)a.scaleB[w]);
 }
 
-template <int BN, int EPI>
-__global__ void __launch_bounds__(TcWarps<EPI>::THREADS, 1)
+template <int BN, int EPI, bool CONVB = false>
+__global__ void __launch_bounds__(TcThreads<EPI, CONVB>::VALUE, 1)
     k_tc_gemm(const __grid_constant__ CUtensorMap mapAh, const __grid_constant__ CUtensorMap mapAl,
               const __grid_constant__ CUtensorMap mapBh, const __grid_constant__ CUtensorMap mapBl, TcArgs args) {
+  static_assert(!CONVB || (EPI == EPI_STORE && BN == 128), "the converted B operand serves P0's STORE tiles");
   using L = TcSmem<BN, EPI>;
   constexpr int TC_BK = TcPipe<EPI>::BK;
   constexpr int TC_STAGES = TcPipe<EPI>::STAGES;
@@ -337,7 +360,8 @@ __global__ void __launch_bounds__(TcWarps<EPI>::THREADS, 1)
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < TC_STAGES; ++s) {
-      mbar_init(&full[s], 1);
+      // CONVB: the TMA of A plus one arrival per converter warp.
+      mbar_init(&full[s], CONVB ? 1 + kConvWarps : 1);
       mbar_init(&empty[s], 1);
     }
     for (int b = 0; b < 2; ++b) {
@@ -373,7 +397,7 @@ __global__ void __launch_bounds__(TcWarps<EPI>::THREADS, 1)
               if (!mbar_wait(&empty[s], ((g / TC_STAGES) - 1) & 1, abort_flag, args.err, 1)) goto producer_done;
             }
             uint8_t* st = smem + s * L::STAGE_BYTES;
-            mbar_expect_tx(&full[s], L::STAGE_BYTES);
+            mbar_expect_tx(&full[s], CONVB ? 2 * L::A_BYTES : L::STAGE_BYTES);
             const int k0 = kb * TC_BK;
             if (args.a_batched) {
               tma_load_3d(st, &mapAh, &full[s], k0, m0, w);
@@ -382,8 +406,10 @@ __global__ void __launch_bounds__(TcWarps<EPI>::THREADS, 1)
               tma_load_2d(st, &mapAh, &full[s], k0, row_off + m0);
               tma_load_2d(st + L::A_BYTES, &mapAl, &full[s], k0, row_off + m0);
             }
-            tma_load_3d(st + 2 * L::A_BYTES, &mapBh, &full[s], k0, row_off + n0, w);
-            tma_load_3d(st + 2 * L::A_BYTES + L::B_BYTES, &mapBl, &full[s], k0, row_off + n0, w);
+            if (!CONVB) {
+              tma_load_3d(st + 2 * L::A_BYTES, &mapBh, &full[s], k0, row_off + n0, w);
+              tma_load_3d(st + 2 * L::A_BYTES + L::B_BYTES, &mapBl, &full[s], k0, row_off + n0, w);
+            }
             issued = g + 1;
           }
         }
@@ -450,6 +476,62 @@ __global__ void __launch_bounds__(TcWarps<EPI>::THREADS, 1)
         umma_commit(drain);
         volatile int no_abort = 0;
         mbar_wait(drain, 0, &no_abort, args.err, 6);
+      }
+    } else if (CONVB && warp >= 2 + TcWarps<EPI>::NEPI) {
+      // ---------------- B operand converters (CONVB) ----------------
+      // Warp cw builds rows cw, cw + 4, ... of the 128-row B tile for each k
+      // block: lane l takes columns 2l, 2l + 1 (one coalesced 256-byte row
+      // read per warp), x = b * c in FP32, hi = rn16(x), lo = rn16(x - hi)
+      // (split_round's rounding), both as one 32-bit word per row into the
+      // swizzled tile.  The generic-proxy stores are made visible to the
+      // tensor core's async proxy before the warp's arrival on the stage.
+      const int cw = warp - (2 + TcWarps<EPI>::NEPI);
+      const int n0 = nt_begin * BN;
+      const float* cw_scale = args.convC + (size_t)w * args.ldcc;
+      int g = 0;
+      for (int kb = 0; kb < k_blocks; ++kb, ++g) {
+        const int s = g % TC_STAGES;
+        if (g >= TC_STAGES) {
+          if (!mbar_wait(&empty[s], ((g / TC_STAGES) - 1) & 1, abort_flag, args.err, 7)) break;
+        }
+        const int k = kb * TC_BK + 2 * lane;
+        const bool kin = k < args.K;  // K even: k + 1 < K as well
+        const float2 c = kin ? *reinterpret_cast<const float2*>(cw_scale + k) : make_float2(0.f, 0.f);
+        constexpr int RPW = BN / kConvWarps;  // rows per converter warp
+        float2 v[RPW];
+#pragma unroll
+        for (int i = 0; i < RPW; ++i) {
+          const int row = n0 + cw + kConvWarps * i;
+          v[i] = (kin && row < args.N) ? __ldg(reinterpret_cast<const float2*>(args.convB + (size_t)row * args.ldconv + k))
+                                        : make_float2(0.f, 0.f);
+        }
+        uint8_t* st = smem + s * L::STAGE_BYTES + 2 * L::A_BYTES;
+        const uint32_t bh = smem_u32(st), bl = bh + L::B_BYTES;
+#pragma unroll
+        for (int i = 0; i < RPW; ++i) {
+          const int r = cw + kConvWarps * i;
+          const float x0 = v[i].x * c.x, x1 = v[i].y * c.y;
+          uint32_t hw, lw;
+          if (args.fp16) {
+            const __half2 hh = __floats2half2_rn(x0, x1);
+            const float2 hf = __half22float2(hh);
+            const __half2 ll = __floats2half2_rn(x0 - hf.x, x1 - hf.y);
+            hw = *reinterpret_cast<const uint32_t*>(&hh);
+            lw = *reinterpret_cast<const uint32_t*>(&ll);
+          } else {
+            const __nv_bfloat162 hh = __floats2bfloat162_rn(x0, x1);
+            const float2 hf = __bfloat1622float2(hh);
+            const __nv_bfloat162 ll = __floats2bfloat162_rn(x0 - hf.x, x1 - hf.y);
+            hw = *reinterpret_cast<const uint32_t*>(&hh);
+            lw = *reinterpret_cast<const uint32_t*>(&ll);
+          }
+          const uint32_t off = sw128_offset(r, 2 * lane);
+          asm volatile("st.shared.b32 [%0], %1;\n" ::"r"(bh + off), "r"(hw) : "memory");
+          asm volatile("st.shared.b32 [%0], %1;\n" ::"r"(bl + off), "r"(lw) : "memory");
+        }
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&full[s]);
       }
     } else if (EPI == EPI_ROWDOT) {
       // ---------------- epilogue (warps 2..9): row dot products ----------------
@@ -1010,15 +1092,16 @@ static int* tc_err_slot(qx_ctx* ctx) { return status_words(ctx, 1); }
 
 static void check_tc_err(qx_ctx* ctx, int* d_err) { ctx->pending.push_back({d_err, 1, 0}); }
 
-template <int BN, int EPI>
+template <int BN, int EPI, bool CONVB = false>
 static void launch_tc(qx_ctx* ctx, const CUtensorMap& ah, const CUtensorMap& al, const CUtensorMap& bh,
                       const CUtensorMap& bl, const TcArgs& a, dim3 grid, cudaStream_t stream = nullptr) {
   using L = TcSmem<BN, EPI>;
   static PerDeviceOnce attr_once;
   attr_once(ctx->device, [&] {
-    QX_CUDA(cudaFuncSetAttribute(k_tc_gemm<BN, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, L::TOTAL));
+    QX_CUDA(cudaFuncSetAttribute(k_tc_gemm<BN, EPI, CONVB>, cudaFuncAttributeMaxDynamicSharedMemorySize, L::TOTAL));
   });
-  k_tc_gemm<BN, EPI><<<grid, TcWarps<EPI>::THREADS, L::TOTAL, stream ? stream : ctx->stream>>>(ah, al, bh, bl, a);
+  k_tc_gemm<BN, EPI, CONVB><<<grid, TcThreads<EPI, CONVB>::VALUE, L::TOTAL, stream ? stream : ctx->stream>>>(
+      ah, al, bh, bl, a);
   check_launch(ctx);
 }
 
@@ -1108,33 +1191,73 @@ void launch_pair_contract_tc(qx_ctx* ctx, const TcOperand& A, const float* bpt_f
 }
 
 // eps[w] = I + Bov diag(chi[w]) Bov^T with A = split(Bov), B = split(Bov * chi[w]).
+// bf[r][c] = (float)b[r][c] for c < cols, 0 in the padding columns [cols, ld).
+__global__ void k_f32_rows(const double* __restrict__ b, int rows, int cols, int ld, float* __restrict__ bf) {
+  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < (size_t)rows * ld;
+       e += (size_t)gridDim.x * blockDim.x) {
+    const int c = (int)(e % ld);
+    bf[e] = c < cols ? (float)b[e] : 0.0f;
+  }
+}
+
+// Per frequency w (one block each): s_w, the power of two of the fp16 split
+// of B diag(chi'_w) (largest 2^k with 2^k amax(B) max|chi'_w| <= 32768; 1 for
+// bf16), and the FP32 column scales cs[w][k] = chi'_w[k] s_w (0 past nov).
+__global__ void k_chi_cols(const double* __restrict__ chi, int nov, int ldov, const unsigned long long* amax_b,
+                           int fp16, float* __restrict__ cs, float* __restrict__ scale) {
+  const int w = blockIdx.x;
+  const double* cw = chi + (size_t)w * ldov;
+  double m = 0.0;
+  for (int k = threadIdx.x; k < nov; k += blockDim.x) m = fmax(m, fabs(cw[k]));
+  __shared__ double red[32];
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    m = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if (threadIdx.x == 0) red[0] = m;
+  }
+  __syncthreads();
+  const double bound = __longlong_as_double((long long)*amax_b) * red[0];
+  const double s = (fp16 && bound > 0.0 && isfinite(bound)) ? exp2(floor(log2(32768.0 / bound))) : 1.0;
+  if (threadIdx.x == 0) scale[w] = (float)s;
+  for (int k = threadIdx.x; k < ldov; k += blockDim.x) cs[(size_t)w * ldov + k] = k < nov ? (float)(cw[k] * s) : 0.f;
+}
+
 void launch_eps_tc(qx_ctx* ctx, const double* bov, int ldov, int naux, int nov, const double* chi, int nw,
                    double* eps, int ldn, size_t eps_stride, int fp16, int reuse_a) {
   constexpr int BN = 128;
   const size_t a_elems = (size_t)naux * ldov;
+  // A: the hi/lo split of B_ov (one scale, slot 7), reusable across calls.
+  // B: built in shared memory by the kernel's converter warps from an FP32
+  // copy of B_ov and the per-frequency column scales chi' s_w, so that no
+  // chi-scaled operand is written to memory.
   DevBuf& buf = ctx->ws[WS_BOV_HI];
-  const size_t need = a_elems * 2 * 2 * (1 + (size_t)nw);
-  // The A split (and its scale in split slot 7) survive from the previous
-  // call on this context only if the buffer is not reallocated now.
+  const size_t need = a_elems * 2 * 2 + a_elems * 4 + (size_t)nw * ldov * 4 + (size_t)nw * 4 + 1024;
   reuse_a = reuse_a && buf.bytes >= need;
   buf.reserve(need);
   uint8_t* p = buf.as<uint8_t>();
   void* a_hi = p;
   void* a_lo = p + a_elems * 2;
-  void* b_hi = p + a_elems * 4;
-  void* b_lo = p + a_elems * 4 + a_elems * 2 * nw;
-  float *sa = nullptr, *sb = nullptr;
-  if (reuse_a)
+  float* bf = reinterpret_cast<float*>(p + a_elems * 4);
+  float* cs = bf + a_elems;
+  float* sb = cs + (size_t)nw * ldov;
+  float* sa = nullptr;
+  if (reuse_a) {
     sa = split_scratch(ctx, 7).scale;
-  else
+  } else {
     split(ctx, bov, naux, nov, ldov, 0, a_hi, a_lo, ldov, 0, 1, nullptr, 0, fp16, 7, &sa);
-  split(ctx, bov, naux, nov, ldov, 0, b_hi, b_lo, ldov, a_elems, nw, chi, ldov, fp16, 1, &sb,
-        /*the bound of bov*/ split_scratch(ctx, 7).amax_src);
+    k_f32_rows<<<(unsigned)std::min<size_t>((a_elems + 255) / 256, 4 * (size_t)ctx->sm_count * 8), 256, 0,
+                 ctx->stream>>>(bov, naux, nov, ldov, bf);
+    check_launch(ctx);
+  }
+  k_chi_cols<<<nw, 256, 0, ctx->stream>>>(chi, nov, ldov, split_scratch(ctx, 7).amax_src, fp16, cs, sb);
+  check_launch(ctx);
   constexpr int BK = TcPipe<EPI_STORE>::BK;
   CUtensorMap ah = make_map(a_hi, nov, naux, ldov, 1, TC_BM, 2, fp16, BK);
   CUtensorMap al = make_map(a_lo, nov, naux, ldov, 1, TC_BM, 2, fp16, BK);
-  CUtensorMap bh = make_map(b_hi, nov, naux, ldov, nw, BN, 3, fp16, BK);
-  CUtensorMap bl = make_map(b_lo, nov, naux, ldov, nw, BN, 3, fp16, BK);
+  QX_REQUIRE(nov % 2 == 0 || ldov > nov, QX_ERR_INVALID_INPUT, "B_ov needs a padding column for odd nov");
   int* d_err = tc_err_slot(ctx);
   QX_CUDA(cudaMemsetAsync(d_err, 0, sizeof(int), ctx->stream));
   TcArgs a{};
@@ -1153,9 +1276,14 @@ void launch_eps_tc(qx_ctx* ctx, const double* bov, int ldov, int naux, int nov, 
   a.scaleA = sa;
   a.scaleB = sb;
   a.err = d_err;
+  a.convB = bf;
+  a.ldconv = ldov;
+  a.convC = cs;
+  a.ldcc = ldov;
   const int tiles = ceil_div(naux, TC_BM);  // BM == BN for the symmetric product
   static_assert(BN == TC_BM, "eps tiles are square");
-  launch_tc<BN, EPI_STORE>(ctx, ah, al, bh, bl, a, dim3(tiles * (tiles + 1) / 2, nw));
+  // The B maps are not read in this form (the converters build B).
+  launch_tc<BN, EPI_STORE, true>(ctx, ah, al, ah, al, a, dim3(tiles * (tiles + 1) / 2, nw));
   check_tc_err(ctx, d_err);
 }
 

@@ -537,6 +537,18 @@ qx_status qx_ctx_last_timings(const qx_ctx* c, double* a, double* b, double* d, 
 
 int64_t qx_ctx_last_launches(const qx_ctx* c) { return c ? c->launches : 0; }
 
+qx_status qx_ctx_last_guard_stats(const qx_ctx* c, int64_t* guarded, int64_t* reinverted) {
+  if (!c) return QX_ERR_INVALID_INPUT;
+  int64_t g = c->guard_matrices, r = c->guard_reinverted;
+  for (const qx_ctx* w : c->workers) {
+    g += w->guard_matrices;
+    r += w->guard_reinverted;
+  }
+  if (guarded) *guarded = g;
+  if (reinverted) *reinverted = r;
+  return QX_OK;
+}
+
 qx_status qx_get_scaled_legendre_roots(int nw, double x0, double* freqs, double* wts) {
   if (nw < 0 || (nw > 0 && (!freqs || !wts))) return QX_ERR_INVALID_INPUT;
   if (nw == 0) return QX_OK;

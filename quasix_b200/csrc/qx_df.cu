@@ -20,11 +20,10 @@
 // (the reference does it after): the two are linear and commute, and this
 // order contracts the metric over nmo^2 instead of nao^2 columns.
 //
-// J^-1/2 comes from the coupled Newton-Schulz iteration on J / c (c = ||J||_F):
-//   T = (3 I - Z Y) / 2,  Y <- Y T,  Z <- T Z,  Y0 = J / c, Z0 = I,
-// with Y -> (J / c)^1/2 and Z -> (J / c)^-1/2 (all GEMMs); it equals the
-// eigendecomposition form of the reference whenever no eigenvalue of J lies
-// below thresh_df.  That is checked with lambda_min(J) >= 1 / trace(J^-1)
+// J^-1/2 and J^1/2 come from the scaled Denman-Beavers iteration (product
+// form, see metric_inv_sqrt: one SPD inverse by the block sweep and two DMMA
+// GEMMs per step, 5-8 steps); it equals the eigendecomposition form of the
+// reference whenever no eigenvalue of J lies below thresh_df.  That is checked with lambda_min(J) >= 1 / trace(J^-1)
 // and, when this bound is inconclusive, by power iteration on J^-1/2 (the
 // reference's clamping of such eigenvalues is not reproduced: those metrics
 // are rejected with QX_ERR_NUMERICAL).
@@ -92,28 +91,32 @@ void transpose_gs(qx_ctx* ctx, const double* in, long long rows, int cols, int l
   check_launch(ctx);
 }
 
-// Y = s J (s = 1 / c), Z = I (both [n][ld]); sum of squares of J for c.
-__global__ void k_ns_init(const double* __restrict__ J, int n, int ldj, double s, double* __restrict__ Y,
-                          double* __restrict__ Z, int ld) {
-  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < (size_t)n * ld;
+// out = s * in (+ t I) over the n x n part (row stride ld); padding untouched.
+__global__ void k_axpi(const double* __restrict__ in, int n, int ldi, double s, double t, double* __restrict__ out,
+                       int ldo) {
+  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < (size_t)n * n;
        e += (size_t)gridDim.x * blockDim.x) {
-    const int r = (int)(e / ld), c = (int)(e % ld);
-    Y[e] = c < n ? s * J[(size_t)r * ldj + c] : 0.0;
-    Z[e] = (r == c) ? 1.0 : 0.0;
+    const size_t r = e / n, c = e % n;
+    out[r * ldo + c] = s * in[r * ldi + c] + (r == c ? t : 0.0);
   }
 }
 
-// T = 1.5 I - 0.5 P in place (P = Z Y), and *res = max |I - P| (bits).
-__global__ void k_ns_step(double* __restrict__ P, int n, int ld, unsigned long long* __restrict__ res) {
+// M <- (I + (a M + b Mi) / 2) / 2, symmetrised (each thread owns the pair
+// (r, c), (c, r) with c <= r), and *res = max |M - I| (bits).
+__global__ void k_db_m(double* __restrict__ M, const double* __restrict__ Mi, int n, int ld, double a, double b,
+                       unsigned long long* __restrict__ res) {
   double m = 0.0;
-  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < (size_t)n * ld;
+  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < (size_t)n * n;
        e += (size_t)gridDim.x * blockDim.x) {
-    const int r = (int)(e / ld), c = (int)(e % ld);
-    if (c >= n) continue;
+    const size_t r = e / n, c = e % n;
+    if (c > r) continue;
     const double id = (r == c) ? 1.0 : 0.0;
-    const double p = P[e];
-    m = fmax(m, isfinite(p) ? fabs(id - p) : INFINITY);
-    P[e] = 1.5 * id - 0.5 * p;
+    const double v1 = 0.5 * (id + 0.5 * (a * M[r * ld + c] + b * Mi[r * ld + c]));
+    const double v2 = 0.5 * (id + 0.5 * (a * M[c * ld + r] + b * Mi[c * ld + r]));
+    const double v = 0.5 * (v1 + v2);
+    M[r * ld + c] = v;
+    M[c * ld + r] = v;
+    m = fmax(m, isfinite(v) ? fabs(v - id) : INFINITY);
   }
   for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
   if ((threadIdx.x & 31) == 0) atomicMax(res, (unsigned long long)__double_as_longlong(m));
@@ -201,75 +204,91 @@ void gemm(qx_ctx* ctx, int M, int N, int K, const double* A, int lda, size_t sA,
   gemm_nt_f64(ctx, g);
 }
 
+// Frobenius norm of an n x n matrix (row stride ld), deterministic.
+double frob(qx_ctx* ctx, const double* A, int n, int ld, double* part, int blocks) {
+  k_sumsq<<<blocks, 256, 0, ctx->stream>>>(A, n, ld, part);
+  check_launch(ctx);
+  std::vector<double> h(blocks);
+  QX_CUDA(cudaMemcpyAsync(h.data(), part, blocks * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  QX_CUDA(cudaStreamSynchronize(ctx->stream));
+  double s = 0.0;
+  for (double v : h) s += v;
+  return std::sqrt(s);
+}
+
 // J^-1/2 and J^1/2 ([n][ld] each, symmetrised) of the SPD metric J ([n][ldj],
-// device).  Returns a lower bound on the smallest eigenvalue of J that is
-// tight whenever it is near thresh (1 / ||J^-1/2||_F^2, else the power
-// iteration's 1 / lambda_max(J^-1/2)^2).
+// device), by the scaled product form of the Denman-Beavers iteration:
+//   Mi = M^-1,  mu = (||Mi||_F / ||M||_F)^(1/4),  X = (I + Mi / mu^2) / 2,
+//   Y <- mu Y X,  Z <- mu Z X,  M <- (I + (mu^2 M + Mi / mu^2) / 2) / 2,
+// from M = Y = J, Z = I; M -> I, Y -> J^1/2, Z -> J^-1/2 (numerically stable;
+// M stays SPD, so its inverse is the unguarded block sweep).  Returns a lower
+// bound on the smallest eigenvalue of J that is tight whenever it is near
+// thresh (1 / ||J^-1/2||_F^2, else the power iteration's
+// 1 / lambda_max(J^-1/2)^2).
 double metric_inv_sqrt(qx_ctx* ctx, const double* J, int n, int ldj, double* Jm, double* Jp, int ld, double* work,
                        double thresh) {
   const size_t nn = (size_t)n * ld;
+  double* M = work;
+  double* Mi = work + nn;
+  double* X = work + 2 * nn;
+  double* small = work + 3 * nn;  // [512] block partials | residual word | power vectors
   double* Y = Jp;
   double* Z = Jm;
-  double* P = work;
-  double* Y2 = work + nn;
-  double* Z2 = work + 2 * nn;
-  double* small = work + 3 * nn;  // [512] block partials | residual word | power vectors
   const int blocks = std::min<int>((int)((nn + 255) / 256), 2 * ctx->sm_count);
-  k_sumsq<<<blocks, 256, 0, ctx->stream>>>(J, n, ldj, small);
+  QX_CUDA(cudaMemsetAsync(M, 0, 3 * nn * sizeof(double), ctx->stream));
+  QX_CUDA(cudaMemsetAsync(Jm, 0, nn * sizeof(double), ctx->stream));
+  QX_CUDA(cudaMemsetAsync(Jp, 0, nn * sizeof(double), ctx->stream));
+  k_axpi<<<blocks, 256, 0, ctx->stream>>>(J, n, ldj, 1.0, 0.0, M, ld);
   check_launch(ctx);
-  std::vector<double> part(blocks);
-  QX_CUDA(cudaMemcpyAsync(part.data(), small, blocks * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-  QX_CUDA(cudaStreamSynchronize(ctx->stream));
-  double fro = 0.0;
-  for (double v : part) fro += v;
-  fro = std::sqrt(fro);
-  QX_REQUIRE(std::isfinite(fro) && fro > 0.0, QX_ERR_NUMERICAL, "metric is zero or not finite");
-  k_ns_init<<<blocks, 256, 0, ctx->stream>>>(J, n, ldj, 1.0 / fro, Y, Z, ld);
+  k_axpi<<<blocks, 256, 0, ctx->stream>>>(J, n, ldj, 1.0, 0.0, Y, ld);
   check_launch(ctx);
+  k_axpi<<<blocks, 256, 0, ctx->stream>>>(J, n, ldj, 0.0, 1.0, Z, ld);
+  check_launch(ctx);
+  const double fj = frob(ctx, J, n, ldj, small, blocks);
+  QX_REQUIRE(std::isfinite(fj) && fj > 0.0, QX_ERR_NUMERICAL, "metric is zero or not finite");
   unsigned long long* res = reinterpret_cast<unsigned long long*>(small + 512);
-  double prev = INFINITY;
+  // Scratch for the products: the work buffer after small.
+  double* T = small + 520 + 2 * ((size_t)n + 8) + 64;
   bool done = false;
-  for (int it = 0; it < 200 && !done; ++it) {
-    gemm(ctx, n, n, n, Z, ld, 0, Y, ld, 0, P, ld, 0, 1);  // P = Z Y (both symmetric: Y's rows are its columns)
+  for (int it = 0; it < 100 && !done; ++it) {
+    // Mi = M^-1 (the sweep leaves M^-1 - I in place; M is SPD).
+    QX_CUDA(cudaMemcpyAsync(Mi, M, nn * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+    launch_invert_wc(ctx, Mi, n, ld, nn, 1, /*guard=*/0);
+    k_axpi<<<blocks, 256, 0, ctx->stream>>>(Mi, n, ld, 1.0, 1.0, Mi, ld);
+    check_launch(ctx);
+    const double mu = std::pow(frob(ctx, Mi, n, ld, small, blocks) / frob(ctx, M, n, ld, small, blocks), 0.25);
+    QX_REQUIRE(std::isfinite(mu) && mu > 0.0, QX_ERR_NUMERICAL, "Denman-Beavers iteration of the metric diverged");
+    // X = (I + Mi / mu^2) / 2;  Y <- mu Y X,  Z <- mu Z X (X symmetric: its rows are its columns).
+    k_axpi<<<blocks, 256, 0, ctx->stream>>>(Mi, n, ld, 0.5 / (mu * mu), 0.5, X, ld);
+    check_launch(ctx);
+    gemm(ctx, n, n, n, Y, ld, 0, X, ld, 0, T, ld, 0, 1);
+    k_axpi<<<blocks, 256, 0, ctx->stream>>>(T, n, ld, mu, 0.0, Y, ld);
+    check_launch(ctx);
+    gemm(ctx, n, n, n, Z, ld, 0, X, ld, 0, T, ld, 0, 1);
+    k_axpi<<<blocks, 256, 0, ctx->stream>>>(T, n, ld, mu, 0.0, Z, ld);
+    check_launch(ctx);
     QX_CUDA(cudaMemsetAsync(res, 0, sizeof(unsigned long long), ctx->stream));
-    k_ns_step<<<blocks, 256, 0, ctx->stream>>>(P, n, ld, res);  // P <- T = (3I - ZY)/2
+    k_db_m<<<blocks, 256, 0, ctx->stream>>>(M, Mi, n, ld, mu * mu, 1.0 / (mu * mu), res);
     check_launch(ctx);
     unsigned long long h = 0;
     QX_CUDA(cudaMemcpyAsync(&h, res, sizeof h, cudaMemcpyDeviceToHost, ctx->stream));
-    gemm(ctx, n, n, n, Y, ld, 0, P, ld, 0, Y2, ld, 0, 1);  // Y T   (T symmetric)
-    gemm(ctx, n, n, n, P, ld, 0, Z, ld, 0, Z2, ld, 0, 1);  // T Z   (Z symmetric)
-    QX_CUDA(cudaStreamSynchronize(ctx->stream));
-    std::swap(Y, Y2);
-    std::swap(Z, Z2);
+    sync_and_check(ctx);
     double r;
     memcpy(&r, &h, sizeof r);
-    QX_REQUIRE(std::isfinite(r), QX_ERR_NUMERICAL, "Newton-Schulz iteration of the metric diverged");
-    // Quadratic convergence: stop at rounding level, or once the residual
-    // stops falling (it then sits at rounding level for this conditioning).
-    if (r < 1e-14 || (r < 1e-8 && r > 0.5 * prev)) done = true;
-    prev = r;
+    QX_REQUIRE(std::isfinite(r), QX_ERR_NUMERICAL, "Denman-Beavers iteration of the metric diverged");
+    if (r < 1e-14) done = true;
   }
-  QX_REQUIRE(done, QX_ERR_CONVERGENCE, "Newton-Schulz iteration of the metric did not converge");
-  // Results into Jm, Jp, rescaled and symmetrised (the products only keep
-  // them symmetric to rounding).  Y and Z may sit in the work buffers after
-  // the swaps; P is free.
-  const double sc = std::sqrt(fro);
-  k_scale_copy<<<blocks, 256, 0, ctx->stream>>>(Z, n, ld, 1.0 / sc, P, ld);
+  QX_REQUIRE(done, QX_ERR_CONVERGENCE, "Denman-Beavers iteration of the metric did not converge");
+  // Symmetrised results (the products keep them symmetric only to rounding).
+  k_symmetrize<<<blocks, 256, 0, ctx->stream>>>(Z, n, ld, T);
   check_launch(ctx);
-  k_symmetrize<<<blocks, 256, 0, ctx->stream>>>(P, n, ld, Jm);
+  QX_CUDA(cudaMemcpyAsync(Jm, T, nn * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+  k_symmetrize<<<blocks, 256, 0, ctx->stream>>>(Y, n, ld, T);
   check_launch(ctx);
-  k_scale_copy<<<blocks, 256, 0, ctx->stream>>>(Y, n, ld, sc, P, ld);
-  check_launch(ctx);
-  k_symmetrize<<<blocks, 256, 0, ctx->stream>>>(P, n, ld, Jp);
-  check_launch(ctx);
+  QX_CUDA(cudaMemcpyAsync(Jp, T, nn * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
   // lambda_min(J) >= 1 / ||J^-1/2||_F^2 (= 1 / trace J^-1).
-  k_sumsq<<<blocks, 256, 0, ctx->stream>>>(Jm, n, ld, small);
-  check_launch(ctx);
-  QX_CUDA(cudaMemcpyAsync(part.data(), small, blocks * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-  QX_CUDA(cudaStreamSynchronize(ctx->stream));
-  double tr = 0.0;
-  for (double v : part) tr += v;
-  if (1.0 / tr > thresh) return 1.0 / tr;
+  const double fz = frob(ctx, Jm, n, ld, small, blocks);
+  if (1.0 / (fz * fz) > thresh) return 1.0 / (fz * fz);
   // Otherwise 1 / lambda_max(J^-1/2)^2 by power iteration from a fixed start.
   double* x = small + 520;
   double* y = x + n + 8;
@@ -289,8 +308,7 @@ double metric_inv_sqrt(qx_ctx* ctx, const double* J, int n, int ldj, double* Jm,
   return 1.0 / (lam * lam);
 }
 
-size_t metric_work_doubles(int n, int ld) { return 3 * (size_t)n * ld + 520 + 2 * ((size_t)n + 8) + 64; }
-
+size_t metric_work_doubles(int n, int ld) { return 4 * (size_t)n * ld + 520 + 2 * ((size_t)n + 8) + 64; }
 }  // namespace
 }  // namespace qx
 

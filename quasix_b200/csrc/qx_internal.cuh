@@ -126,6 +126,9 @@ struct qx_ctx {
   cudaEvent_t sweep_ev[4] = {};
   // Worker contexts of batched calls (own streams and workspaces), owned.
   std::vector<qx_ctx*> workers;
+  // Guarded inversions of the last call: matrices checked, and matrices
+  // re-inverted with pivoting.
+  int64_t guard_matrices = 0, guard_reinverted = 0;
 };
 
 namespace qx {
@@ -195,10 +198,12 @@ void sync_and_check(qx_ctx* ctx);
 // sync_and_check (which this call performs first when the arena is full).
 int* status_words(qx_ctx* ctx, int n);
 
-// Forget pending checks at the start of an entry point.
+// Forget pending checks (and the guard counts) at the start of an entry point.
 inline void reset_pending(qx_ctx* ctx) {
   ctx->pending.clear();
   ctx->status_used = 0;
+  ctx->guard_matrices = 0;
+  ctx->guard_reinverted = 0;
 }
 
 // Stage timer (CUDA events on the context stream).

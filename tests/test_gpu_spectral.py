@@ -3,8 +3,8 @@
 Tolerances: the Pade fit and evaluation are the same FP64 recursion as the
 oracle's; the reciprocal differences amplify the last-bit differences of the
 complex divisions (the device divides by b conj(b), numpy scales first), so
-the coefficients agree to 1e-11 relative and the continued fraction's values
-to 1e-12; the broadened spectral sums are FP64 sums of exp / rational terms
+the coefficients and the continued fraction's values agree to 1e-11
+relative; the broadened spectral sums are FP64 sums of exp / rational terms
 (1e-13 relative to max|A|).
 """
 import numpy as np
@@ -49,7 +49,7 @@ def test_thiele_fit_on_device_matches_oracle(q):
         for p in (0, 4, 5, 23):
             got = q.pade_thiele(w, f[p], c[:, p])
             ref = np.array([O.pade_thiele(x, f2[p], c2[:, p]) for x in w])
-            assert rel(got, ref) < 1e-12
+            assert rel(got, ref) < 1e-11
 
 
 def test_spectral_function_matches_oracle(q):
