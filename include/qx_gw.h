@@ -98,6 +98,19 @@ qx_status qx_screened_interaction(qx_ctx* ctx, int nfreq, int naux, const double
  * reference tries Cholesky first and falls back on failure); host-only. */
 int qx_eps_at_least_identity(const double* mo_energy, int nocc, int nvir, double wmax);
 
+/* compute_screened_interaction(P0, v_aux, freqs) (quasix_core/src/dielectric/
+ * screening.rs:164-236, the S3-3 form used by the CD path): per frequency
+ * W = v^1/2 (I - v^1/2 P0 v^1/2)^-1 v^1/2 with the symmetric square root of
+ * v_aux, eps and W symmetrised by averaging as the reference does.
+ * p0, w: [nfreq][naux][naux]; v_aux: [naux][naux] (host or device; w must
+ * not alias p0).  The frequencies themselves are not needed (the reference
+ * ignores its freqs argument too).  eps^-1 comes from the guarded sweep of
+ * qx_screened_interaction.  Errors: QX_ERR_NUMERICAL when v_aux has an
+ * eigenvalue at or below 1e-14 (the reference clamps those) or W is not
+ * finite. */
+qx_status qx_compute_screened_interaction(qx_ctx* ctx, int nfreq, int naux, const double* p0, const double* v_aux,
+                                          double* w);
+
 /* qx_screened_interaction without any allocation.  No counterpart in the
  * reference: it exists for callers that must not allocate device memory
  * inside the call (e.g. a pre-sized serving process).  pi and wc must be
@@ -138,6 +151,34 @@ qx_status qx_ac_pade_thiele_diag(qx_ctx* ctx, int norbs, int nw_sigma, const dou
  * orbital, on the device: zn, coeff complex [nfit]; out complex [nomega]. */
 qx_status qx_pade_thiele(qx_ctx* ctx, int nfit, const double* zn, const double* coeff, int nomega,
                          const double* omega, double* out);
+
+/* NewtonSolverConfig (quasix_core/src/qp/newton_solver.rs:52-103; defaults
+ * 50, 1e-8, 1.0, 0.1, 1.0, 1.0, 1e-6, 1, 0.1, 0.999, 1, 30). */
+typedef struct {
+  int max_iterations;
+  double energy_tolerance;
+  double initial_damping, min_damping, max_damping;
+  double max_step;
+  double derivative_delta;
+  int use_richardson;
+  double z_min, z_max;
+  int use_bisection_fallback;
+  int max_bisection_iterations;
+} qx_newton_config;
+
+/* NewtonQPSolver::new + solve (newton_solver.rs:141-402) for norbs orbitals at
+ * once, one device thread each, with the Pade continuation of Sigma_c as the
+ * evaluator (the SigmaCEvaluator of newton_solver.rs:133; coeff complex
+ * [nfit][norbs] and omega_fit complex [norbs][nfit], the layout
+ * qx_ac_pade_thiele_diag writes).  epsilon_hf, sigma_x, vxc, initial_guess:
+ * [norbs]; fermi_level shared.  Outputs per orbital: qp_energy, residual
+ * |f(E)|, iterations, method (0 Newton, 1 bisection fallback, -1 not
+ * converged: the reference's ConvergenceError, with the last Newton iterate
+ * in qp_energy), sigma_c complex [norbs], z_factor. */
+qx_status qx_newton_qp_solve(qx_ctx* ctx, const qx_newton_config* cfg, int norbs, int nfit, const double* coeff,
+                             const double* omega_fit, const double* epsilon_hf, const double* sigma_x,
+                             const double* vxc, double fermi_level, const double* initial_guess, double* qp_energy,
+                             double* residual, int* iterations, int* method, double* sigma_c, double* z_factor);
 
 /* ---- analysis: spectral functions ------------------------------------------- */
 /* SpectralAnalyzer::compute_spectral_function (quasix_core/src/analysis/
@@ -343,6 +384,26 @@ void qx_davidson_config_default(qx_davidson_config* cfg);
 qx_status qx_bse_davidson(qx_bse* bse, const qx_davidson_config* cfg, double* eigenvalues,
                           double* eigenvectors, int* converged, double* residual_norms,
                           int* iterations);
+
+/* Operator for qx_davidson: y[v][0..n) = H x[v][0..n) for v < nvec.  x and y
+ * are device pointers on the context's device, the vectors rows of stride ld
+ * (ld >= n, a multiple of 8).  The callback runs on the thread that called
+ * qx_davidson, after the library's work on x is complete; the library
+ * synchronises the device after it returns, so y may be written on any
+ * stream.  A nonzero return aborts the solve with that status
+ * (QX_ERR_INVALID_INPUT when it is not a qx_status value). */
+typedef int (*qx_apply_fn)(void* user, const double* x, double* y, int nvec, int ld);
+
+/* davidson_bse(apply_h, qp_gaps, config) (quasix_core/src/bse/davidson.rs:
+ * 372-508) with a caller-supplied operator: the same device Davidson as
+ * qx_bse_davidson (unit-vector start at the smallest qp_gaps, preconditioner
+ * 1 / (qp_gaps - theta + level_shift) with the reference's clamp, double
+ * Gram-Schmidt, restart from the Ritz vectors past max_space).
+ * qp_gaps: [n] (host or device); outputs as qx_bse_davidson with n in place
+ * of nov. */
+qx_status qx_davidson(qx_ctx* ctx, int n, const double* qp_gaps, qx_apply_fn apply_h, void* user,
+                      const qx_davidson_config* cfg, double* eigenvalues, double* eigenvectors, int* converged,
+                      double* residual_norms, int* iterations);
 
 /* Gradient of an eigenvalue Omega of the kernel's matrix (eigenvector x [nov],
  * any norm) with respect to the orbital energies, grad_energy [nocc+nvirt], by

@@ -132,12 +132,14 @@ def compute_screened_interaction(p0: np.ndarray, v_aux: np.ndarray) -> np.ndarra
     symmetric v^1/2 from eigh.  quasix_core/src/dielectric/screening.rs:164-236,
     334-410, 580-639.  p0 is [nfreq, naux, naux]."""
     lam, U = np.linalg.eigh(v_aux)
-    vs = (U * np.sqrt(np.maximum(lam, 0.0))) @ U.T
+    vs = (U * np.sqrt(np.maximum(lam, 1e-14))) @ U.T   # the clamp of screening.rs:606-607
     out = np.empty_like(p0)
     n = v_aux.shape[0]
     for k in range(p0.shape[0]):
         m = np.eye(n) - vs @ p0[k] @ vs
-        out[k] = vs @ np.linalg.solve(m, vs)
+        m = 0.5 * (m + m.T)
+        w = vs @ np.linalg.inv(m) @ vs
+        out[k] = 0.5 * (w + w.T)
     return out
 
 

@@ -63,12 +63,25 @@ class DavidsonConfig(C.Structure):
                 ("tol_residual", C.c_double), ("lindep_threshold", C.c_double), ("level_shift", C.c_double)]
 
 
+class NewtonConfig(C.Structure):
+    _fields_ = [
+        ("max_iterations", C.c_int), ("energy_tolerance", C.c_double), ("initial_damping", C.c_double),
+        ("min_damping", C.c_double), ("max_damping", C.c_double), ("max_step", C.c_double),
+        ("derivative_delta", C.c_double), ("use_richardson", C.c_int), ("z_min", C.c_double),
+        ("z_max", C.c_double), ("use_bisection_fallback", C.c_int), ("max_bisection_iterations", C.c_int),
+    ]
+
+
 class CdSystem(C.Structure):
     _fields_ = [
         ("mo_energy", _vp), ("lpq", _vp), ("vxc", _vp), ("nmo", C.c_int), ("nocc", C.c_int), ("naux", C.c_int),
         ("targets", _vp), ("ntarget", C.c_int), ("qp_energies", _vp), ("z_factors", _vp), ("sigma_c", _vp),
         ("sigma_x", _vp), ("status", C.c_int),
     ]
+
+
+# qx_apply_fn: int (*)(void* user, const double* x, double* y, int nvec, int ld).
+APPLY_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int)
 
 
 # Every symbol the header declares, with its ctypes signature.
@@ -86,10 +99,13 @@ SIGNATURES = {
     "qx_screened_interaction": (C.c_int, [_vp, C.c_int, C.c_int, _vp, _vp]),
     "qx_screened_interaction_noalloc": (C.c_int, [_vp, C.c_int, C.c_int, _vp, _vp]),
     "qx_eps_at_least_identity": (C.c_int, [_vp, C.c_int, C.c_int, C.c_double]),
+    "qx_compute_screened_interaction": (C.c_int, [_vp, C.c_int, C.c_int, _vp, _vp, _vp]),
     "qx_get_sigma_diag": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double,
                                     C.c_double, C.c_int, _vp, _vp, C.c_int, _ip]),
     "qx_ac_pade_thiele_diag": (C.c_int, [_vp, C.c_int, C.c_int, _vp, _vp, C.c_int, _vp, _vp, C.c_int, _ip]),
     "qx_pade_thiele": (C.c_int, [_vp, C.c_int, _vp, _vp, C.c_int, _vp, _vp]),
+    "qx_newton_qp_solve": (C.c_int, [_vp, C.POINTER(NewtonConfig), C.c_int, C.c_int, _vp, _vp, _vp, _vp, _vp,
+                                     C.c_double, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "qx_spectral_function": (C.c_int, [_vp, _vp, _vp, C.c_int, C.c_double, C.c_int, _vp, C.c_int, C.c_double,
                                        C.c_double, C.c_double, _vp, _dp]),
     "qx_spectral_function_states": (C.c_int, [_vp, _vp, _vp, C.c_int, _vp, C.c_int, C.c_double, _vp]),
@@ -113,6 +129,7 @@ SIGNATURES = {
     "qx_bse_apply": (C.c_int, [_vp, _vp, _vp, C.c_int]),
     "qx_davidson_config_default": (None, [C.POINTER(DavidsonConfig)]),
     "qx_bse_davidson": (C.c_int, [_vp, C.POINTER(DavidsonConfig), _vp, _vp, _vp, _vp, _ip]),
+    "qx_davidson": (C.c_int, [_vp, C.c_int, _vp, APPLY_FN, _vp, C.POINTER(DavidsonConfig), _vp, _vp, _vp, _vp, _ip]),
     "qx_bse_root_grad": (C.c_int, [_vp, _vp, _vp, _vp]),
     "qx_bse_root_grad_b": (C.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "qx_bse_w0": (C.c_int, [_vp, _vp, _vp, C.c_int, C.c_int, C.c_int, _vp]),

@@ -3,6 +3,7 @@
 * ``BSETDAKernel`` / ``DavidsonConfig``: the PyO3 classes of quasix/src/bse.rs
   (BSETDAKernel :139-330, DavidsonConfig :43-70) over
   quasix_core/src/bse/kernel.rs and davidson.rs.
+* ``davidson_bse``: davidson.rs:372-508 with a caller-supplied operator.
 * ``run_bse_tda`` / ``BSETDAConfig`` / ``BSETDAResult``: the Python driver of
   quasix/quasix/bse_driver.py:55-155, 782-982, taking the density-fitted
   tensors directly (the reference builds them from PySCF, which is not part of
@@ -64,6 +65,71 @@ class DavidsonConfig:
     def _c(self) -> N.DavidsonConfig:
         return N.DavidsonConfig(self.n_roots, self.max_iter, self.max_space, self.tol_residual,
                                 self.lindep_threshold, self.level_shift)
+
+
+class _DeviceRows:
+    """A [nvec, ld] FP64 device array at a raw pointer, for torch.as_tensor."""
+
+    def __init__(self, ptr: int, nvec: int, ld: int, readonly: bool):
+        self.__cuda_array_interface__ = {"shape": (nvec, ld), "typestr": "<f8", "data": (ptr, readonly),
+                                         "strides": None, "version": 3}
+
+
+def davidson_bse(apply_h, qp_gaps, config: Optional[DavidsonConfig] = None, tensors: str = "numpy",
+                 device: int = 0) -> Dict[str, Any]:
+    """davidson_bse(apply_h, qp_gaps, config) (quasix_core/src/bse/davidson.rs:372-508)
+    with a caller-supplied operator: the library's device Davidson calls
+    ``apply_h(X)`` with X [n, k] (one column per vector, as the reference) and
+    expects H X of the same shape.  ``tensors="numpy"`` hands X over as a numpy
+    array (a device-to-host copy per call); ``"torch"`` hands over a CUDA
+    tensor view of the subspace rows, so a device-resident operator never
+    leaves the GPU.  Returns the keys of ``BSETDAKernel.solve_davidson``."""
+    import torch
+    if tensors not in ("numpy", "torch"):
+        raise ValueError(f"tensors must be 'numpy' or 'torch', got {tensors!r}")
+    config = config or DavidsonConfig()
+    gaps = _f64(qp_gaps).reshape(-1)
+    n = gaps.shape[0]
+    # A context of its own: the operator may call the library (e.g. a
+    # BSETDAKernel's matvec) while the solve holds this one.
+    ctx = N.Context(device)
+    dev = torch.device("cuda", device)
+    failure = []
+
+    def cb(_user, x, y, nvec, ld):
+        try:
+            X = torch.as_tensor(_DeviceRows(x, nvec, ld, False), device=dev)[:, :n].T
+            Y = torch.as_tensor(_DeviceRows(y, nvec, ld, False), device=dev)
+            if tensors == "numpy":
+                r = np.asarray(apply_h(X.cpu().numpy()), dtype=np.float64)
+            else:
+                r = apply_h(X)
+            r = torch.as_tensor(r, dtype=torch.float64, device=dev)
+            if tuple(r.shape) != (n, nvec):
+                raise ValueError(f"apply_h returned shape {tuple(r.shape)}, expected {(n, nvec)}")
+            Y[:, :n].copy_(r.T)
+            torch.cuda.current_stream(dev).synchronize()
+            return 0
+        except BaseException as e:  # reported after the call returns
+            failure.append(e)
+            return 1
+
+    fn = N.APPLY_FN(cb)
+    nr = min(config.n_roots, n)
+    ev, vec = np.zeros(nr), np.zeros((n, nr))
+    conv, res = np.zeros(nr, dtype=np.int32), np.zeros(nr)
+    it = C.c_int(0)
+    cfg = config._c()
+    st = ctx.lib.qx_davidson(ctx.handle, n, N.ptr(gaps), fn, None, C.byref(cfg), N.ptr(ev), N.ptr(vec), N.ptr(conv),
+                             N.ptr(res), C.byref(it))
+    try:
+        if failure:
+            raise failure[0]
+        ctx.check(st)
+    finally:
+        ctx.close()
+    return dict(eigenvalues=ev, eigenvectors=vec, converged=[bool(c) for c in conv], iterations=it.value,
+                residual_norms=list(res), all_converged=bool(np.all(conv)))
 
 
 class BSETDAKernel:

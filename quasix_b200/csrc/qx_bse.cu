@@ -8,6 +8,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <functional>
 #include <numeric>
 
 #include "qx_blas.cuh"
@@ -218,6 +219,11 @@ struct DevArr {
   }
 };
 
+// Davidson subspace and scratch (grown on demand, reused across solves).
+struct DavWork {
+  DevArr V, AV, X, AX, R, heff, jv, Z2, small, eigi;
+};
+
 struct qx_bse {
   qx_ctx* ctx;
   int nocc, nvir, naux, nov, precision;
@@ -235,7 +241,7 @@ struct qx_bse {
   DevArr xp, T, Yd, Z, Yx, Xr, Yr;  // matvec scratch
   DevArr gTt, gTp, gTpT, gdijT, gM, gG1, gG, gU;  // root-gradient scratch
   DevArr gGrad;                                     // root-gradient scratch of the DF blocks
-  DevArr V, AV, X, AX, R, heff, jv, Z2, small, eigi;
+  DavWork dav;
   std::vector<double> h_delta;
 };
 
@@ -588,192 +594,158 @@ qx_status qx_bse_apply(qx_bse* B, const double* x, double* y, int nvec) {
   });
 }
 
-qx_status qx_bse_davidson(qx_bse* B, const qx_davidson_config* cfgp, double* eigenvalues, double* eigenvectors,
-                          int* converged_out, double* residual_norms, int* iterations) {
-  if (!B || !cfgp) return QX_ERR_INVALID_INPUT;
-  return bse_guard(B->ctx, [&] {
-    qx_ctx* ctx = B->ctx;
-    const qx_davidson_config cfg = *cfgp;
-    const int n = B->nov, ld = B->ldov;
-    const int nroots = std::min(cfg.n_roots, n);
-    const int max_space = std::min(cfg.max_space, n);
-    QX_REQUIRE(nroots > 0 && eigenvalues && eigenvectors, QX_ERR_INVALID_INPUT, "invalid Davidson arguments");
-    QX_REQUIRE(max_space <= 1024, QX_ERR_INVALID_INPUT, "max_space %d exceeds 1024", max_space);
-    const int cap = std::max(max_space, nroots) + nroots + 1;
-    B->V.alloc((size_t)cap * ld);
-    B->AV.alloc((size_t)cap * ld);
-    B->X.alloc((size_t)nroots * ld);
-    B->AX.alloc((size_t)nroots * ld);
-    B->R.alloc((size_t)nroots * ld);
-    B->heff.alloc((size_t)cap * cap);
-    B->jv.alloc(eigh_lowest_work_doubles(cap, cap));
-    B->eigi.alloc(((size_t)cap * cap + 1) / 2 + 1);
-    B->Z2.alloc((size_t)cap * cap);
-    B->small.alloc((size_t)4 * cap + 64);
-    double* d_theta = B->small.p;
-    double* d_nrm = d_theta + cap;
-    double* d_c = d_nrm + cap;
-    QX_CUDA(cudaMemsetAsync(B->V.p, 0, (size_t)cap * ld * sizeof(double), ctx->stream));
-    auto apply = [&](int first, int count) { bse_apply_rows(B, B->V.p + (size_t)first * ld, B->AV.p + (size_t)first * ld, count); };
-    auto rr = [&](int nv, int k) {
-      // heff = V AV^T, then the lowest k eigenpairs of its symmetric part ->
-      // theta, Z2 (columns).
-      GemmNT g{};
-      g.M = nv;
-      g.N = nv;
-      g.K = n;
-      g.A = B->V.p;
-      g.lda = ld;
-      g.B = B->AV.p;
-      g.ldb = ld;
-      g.C = B->heff.p;
-      g.ldc = nv;
-      g.batch = 1;
-      g.alpha = 1.0;
-      g.splitk = 0;
-      gemm_nt_f64(ctx, g);
-      eigh_lowest(ctx, B->heff.p, nv, nv, k, d_theta, B->Z2.p, nv, B->jv.p, reinterpret_cast<int*>(B->eigi.p));
-    };
-    const int nthreads = 256, nblk = std::min(ceil_div(n, nthreads), 2 * ctx->sm_count);
-    // The norm reductions run in one block of 1024 threads each, so that their
-    // summation order (and the Davidson path) is the same on every run.
-    constexpr int kRedThreads = 1024;
-    // Trivial case (davidson.rs:384-387, 510-540): the full matrix.
-    if (n <= nroots) {
-      std::vector<double> id((size_t)n * ld, 0.0);
-      for (int i = 0; i < n; ++i) id[(size_t)i * ld + i] = 1.0;
-      QX_CUDA(cudaMemcpyAsync(B->V.p, id.data(), id.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
-      apply(0, n);
-      rr(n, n);
-      std::vector<double> th(n), zz((size_t)n * n);
-      QX_CUDA(cudaMemcpyAsync(th.data(), d_theta, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-      QX_CUDA(cudaMemcpyAsync(zz.data(), B->Z2.p, zz.size() * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-      sync_and_check(ctx);
-      std::vector<double> ev((size_t)n * nroots);
-      for (int k = 0; k < n; ++k)
-        for (int r = 0; r < nroots; ++r) ev[(size_t)k * nroots + r] = zz[(size_t)k * n + r];
-      QX_CUDA(cudaMemcpy(eigenvalues, th.data(), nroots * sizeof(double), cudaMemcpyDefault));
-      QX_CUDA(cudaMemcpy(eigenvectors, ev.data(), ev.size() * sizeof(double), cudaMemcpyDefault));
-      if (converged_out)
-        for (int r = 0; r < nroots; ++r) converged_out[r] = 1;
-      if (residual_norms)
-        for (int r = 0; r < nroots; ++r) residual_norms[r] = 0.0;
-      if (iterations) *iterations = 1;
-      return;
-    }
-    // Initial subspace: unit vectors at the smallest gaps (davidson.rs:157-176).
-    std::vector<int> order(n);
-    std::iota(order.begin(), order.end(), 0);
-    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return B->h_delta[a] < B->h_delta[b]; });
-    {
-      std::vector<double> init((size_t)nroots * ld, 0.0);
-      for (int i = 0; i < nroots; ++i) init[(size_t)i * ld + order[i]] = 1.0;
-      QX_CUDA(cudaMemcpyAsync(B->V.p, init.data(), init.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
-    }
-    int nv = nroots;
-    apply(0, nv);
-    std::vector<double> evals(nroots, 0.0), rnorm(nroots, std::numeric_limits<double>::max());
-    std::vector<int> conv(nroots, 0);
-    DevArr evecs;  // converged eigenvectors [nroots][ld]
-    evecs.alloc((size_t)nroots * ld);
-    QX_CUDA(cudaMemsetAsync(evecs.p, 0, (size_t)nroots * ld * sizeof(double), ctx->stream));
-    int iter = 0;
-    bool all = false;
-    std::vector<double> th(cap), nr(cap);
-    for (iter = 0; iter < cfg.max_iter; ++iter) {
-      const int nr_ = std::min(nroots, nv);
-      rr(nv, nr_);
-      // Ritz vectors X = V Y, AX = AV Y.
-      combine_rows(ctx, B->V.p, ld, nv, B->Z2.p, nv, nr_, n, B->X.p, ld, 1.0, 0.0);
-      combine_rows(ctx, B->AV.p, ld, nv, B->Z2.p, nv, nr_, n, B->AX.p, ld, 1.0, 0.0);
-      QX_CUDA(cudaMemsetAsync(d_nrm, 0, nr_ * sizeof(double), ctx->stream));
-      k_residual<<<dim3(1, nr_), kRedThreads, 0, ctx->stream>>>(B->AX.p, B->X.p, d_theta, ld, n, B->R.p, d_nrm);
-      check_launch(ctx);
-      QX_CUDA(cudaMemcpyAsync(th.data(), d_theta, nr_ * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-      QX_CUDA(cudaMemcpyAsync(nr.data(), d_nrm, nr_ * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-      sync_and_check(ctx);
-      std::vector<int> newr;
-      for (int j = 0; j < nroots; ++j) {
-        if (j >= nr_ || conv[j]) continue;
-        const double res = std::sqrt(nr[j]);
-        rnorm[j] = res;
-        if (res < cfg.tol_residual) {
-          conv[j] = 1;
-          evals[j] = th[j];
-          QX_CUDA(cudaMemcpyAsync(evecs.p + (size_t)j * ld, B->X.p + (size_t)j * ld, ld * sizeof(double),
-                                  cudaMemcpyDeviceToDevice, ctx->stream));
-          continue;
-        }
-        newr.push_back(j);
-      }
-      all = std::all_of(conv.begin(), conv.end(), [](int c) { return c != 0; });
-      if (all) {
-        ++iter;
-        break;
-      }
-      if (newr.empty()) continue;
-      // Preconditioned residuals t_j (davidson.rs:444-449), staged after V.
-      const int nnew = (int)newr.size();
-      for (int q = 0; q < nnew; ++q) {
-        const int j = newr[q];
-        double* t = B->V.p + (size_t)(nv + q) * ld;
-        QX_CUDA(cudaMemsetAsync(d_c, 0, sizeof(double), ctx->stream));
-        k_precond<<<1, kRedThreads, 0, ctx->stream>>>(B->R.p + (size_t)j * ld, B->delta.p, th[j], cfg.level_shift, n,
-                                                      t, d_c);
-        check_launch(ctx);
-        k_normalize<<<nblk, nthreads, 0, ctx->stream>>>(t, n, d_c, 1e-14);
-        check_launch(ctx);
-      }
-      if (nv + nnew > max_space) {
-        // Restart from the Ritz vectors, re-orthonormalised (davidson.rs:298-307).
-        QX_CUDA(cudaMemcpyAsync(B->V.p, B->X.p, (size_t)nr_ * ld * sizeof(double), cudaMemcpyDeviceToDevice,
-                                ctx->stream));
-        for (int i = 0; i < nr_; ++i) {
-          double* v = B->V.p + (size_t)i * ld;
-          for (int pass = 0; pass < 2 && i > 0; ++pass) {
-            GemmNT g{};
-            g.M = i;
-            g.N = 1;
-            g.K = n;
-            g.A = B->V.p;
-            g.lda = ld;
-            g.B = v;
-            g.ldb = ld;
-            g.C = d_c;
-            g.ldc = 1;
-            g.batch = 1;
-            g.alpha = 1.0;
-            g.splitk = 0;
-            gemm_nt_f64(ctx, g);
-            combine_rows(ctx, B->V.p, ld, i, d_c, 1, 1, n, v, ld, -1.0, 1.0);
-          }
-          QX_CUDA(cudaMemsetAsync(d_nrm, 0, sizeof(double), ctx->stream));
-          k_norm2<<<1, kRedThreads, 0, ctx->stream>>>(v, n, d_nrm);
-          check_launch(ctx);
-          k_normalize<<<nblk, nthreads, 0, ctx->stream>>>(v, n, d_nrm, -1.0);
-          check_launch(ctx);
-        }
-        nv = nr_;
-        QX_CUDA(cudaMemsetAsync(B->V.p + (size_t)nv * ld, 0, (size_t)(cap - nv) * ld * sizeof(double), ctx->stream));
-        apply(0, nv);
+// Davidson of davidson_bse (davidson.rs:372-508) on an n-dimensional operator
+// whose vectors are rows of stride ld on the device: apply_rows(x, y, count)
+// writes y[v] = H x[v] on the context stream; d_delta / h_delta are the QP
+// gaps (the preconditioner's diagonal and the initial subspace's order).
+static void davidson_run(qx_ctx* ctx, DavWork& W, int n, int ld, const double* d_delta,
+                         const std::vector<double>& h_delta,
+                         const std::function<void(const double*, double*, int)>& apply_rows,
+                         const qx_davidson_config& cfg, double* eigenvalues, double* eigenvectors, int* converged_out,
+                         double* residual_norms, int* iterations) {
+  const int nroots = std::min(cfg.n_roots, n);
+  const int max_space = std::min(cfg.max_space, n);
+  QX_REQUIRE(nroots > 0 && eigenvalues && eigenvectors, QX_ERR_INVALID_INPUT, "invalid Davidson arguments");
+  QX_REQUIRE(max_space <= 1024, QX_ERR_INVALID_INPUT, "max_space %d exceeds 1024", max_space);
+  const int cap = std::max(max_space, nroots) + nroots + 1;
+  W.V.alloc((size_t)cap * ld);
+  W.AV.alloc((size_t)cap * ld);
+  W.X.alloc((size_t)nroots * ld);
+  W.AX.alloc((size_t)nroots * ld);
+  W.R.alloc((size_t)nroots * ld);
+  W.heff.alloc((size_t)cap * cap);
+  W.jv.alloc(eigh_lowest_work_doubles(cap, cap));
+  W.eigi.alloc(((size_t)cap * cap + 1) / 2 + 1);
+  W.Z2.alloc((size_t)cap * cap);
+  W.small.alloc((size_t)4 * cap + 64);
+  double* d_theta = W.small.p;
+  double* d_nrm = d_theta + cap;
+  double* d_c = d_nrm + cap;
+  QX_CUDA(cudaMemsetAsync(W.V.p, 0, (size_t)cap * ld * sizeof(double), ctx->stream));
+  auto apply = [&](int first, int count) { apply_rows(W.V.p + (size_t)first * ld, W.AV.p + (size_t)first * ld, count); };
+  auto rr = [&](int nv, int k) {
+    // heff = V AV^T, then the lowest k eigenpairs of its symmetric part ->
+    // theta, Z2 (columns).
+    GemmNT g{};
+    g.M = nv;
+    g.N = nv;
+    g.K = n;
+    g.A = W.V.p;
+    g.lda = ld;
+    g.B = W.AV.p;
+    g.ldb = ld;
+    g.C = W.heff.p;
+    g.ldc = nv;
+    g.batch = 1;
+    g.alpha = 1.0;
+    g.splitk = 0;
+    gemm_nt_f64(ctx, g);
+    eigh_lowest(ctx, W.heff.p, nv, nv, k, d_theta, W.Z2.p, nv, W.jv.p, reinterpret_cast<int*>(W.eigi.p));
+  };
+  const int nthreads = 256, nblk = std::min(ceil_div(n, nthreads), 2 * ctx->sm_count);
+  // The norm reductions run in one block of 1024 threads each, so that their
+  // summation order (and the Davidson path) is the same on every run.
+  constexpr int kRedThreads = 1024;
+  // Trivial case (davidson.rs:384-387, 510-540): the full matrix.
+  if (n <= nroots) {
+    std::vector<double> id((size_t)n * ld, 0.0);
+    for (int i = 0; i < n; ++i) id[(size_t)i * ld + i] = 1.0;
+    QX_CUDA(cudaMemcpyAsync(W.V.p, id.data(), id.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    apply(0, n);
+    rr(n, n);
+    std::vector<double> th(n), zz((size_t)n * n);
+    QX_CUDA(cudaMemcpyAsync(th.data(), d_theta, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    QX_CUDA(cudaMemcpyAsync(zz.data(), W.Z2.p, zz.size() * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    sync_and_check(ctx);
+    std::vector<double> ev((size_t)n * nroots);
+    for (int k = 0; k < n; ++k)
+      for (int r = 0; r < nroots; ++r) ev[(size_t)k * nroots + r] = zz[(size_t)k * n + r];
+    QX_CUDA(cudaMemcpy(eigenvalues, th.data(), nroots * sizeof(double), cudaMemcpyDefault));
+    QX_CUDA(cudaMemcpy(eigenvectors, ev.data(), ev.size() * sizeof(double), cudaMemcpyDefault));
+    if (converged_out)
+      for (int r = 0; r < nroots; ++r) converged_out[r] = 1;
+    if (residual_norms)
+      for (int r = 0; r < nroots; ++r) residual_norms[r] = 0.0;
+    if (iterations) *iterations = 1;
+    return;
+  }
+  // Initial subspace: unit vectors at the smallest gaps (davidson.rs:157-176).
+  std::vector<int> order(n);
+  std::iota(order.begin(), order.end(), 0);
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return h_delta[a] < h_delta[b]; });
+  {
+    std::vector<double> init((size_t)nroots * ld, 0.0);
+    for (int i = 0; i < nroots; ++i) init[(size_t)i * ld + order[i]] = 1.0;
+    QX_CUDA(cudaMemcpyAsync(W.V.p, init.data(), init.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  }
+  int nv = nroots;
+  apply(0, nv);
+  std::vector<double> evals(nroots, 0.0), rnorm(nroots, std::numeric_limits<double>::max());
+  std::vector<int> conv(nroots, 0);
+  DevArr evecs;  // converged eigenvectors [nroots][ld]
+  evecs.alloc((size_t)nroots * ld);
+  QX_CUDA(cudaMemsetAsync(evecs.p, 0, (size_t)nroots * ld * sizeof(double), ctx->stream));
+  int iter = 0;
+  bool all = false;
+  std::vector<double> th(cap), nr(cap);
+  for (iter = 0; iter < cfg.max_iter; ++iter) {
+    const int nr_ = std::min(nroots, nv);
+    rr(nv, nr_);
+    // Ritz vectors X = V Y, AX = AV Y.
+    combine_rows(ctx, W.V.p, ld, nv, W.Z2.p, nv, nr_, n, W.X.p, ld, 1.0, 0.0);
+    combine_rows(ctx, W.AV.p, ld, nv, W.Z2.p, nv, nr_, n, W.AX.p, ld, 1.0, 0.0);
+    QX_CUDA(cudaMemsetAsync(d_nrm, 0, nr_ * sizeof(double), ctx->stream));
+    k_residual<<<dim3(1, nr_), kRedThreads, 0, ctx->stream>>>(W.AX.p, W.X.p, d_theta, ld, n, W.R.p, d_nrm);
+    check_launch(ctx);
+    QX_CUDA(cudaMemcpyAsync(th.data(), d_theta, nr_ * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    QX_CUDA(cudaMemcpyAsync(nr.data(), d_nrm, nr_ * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    sync_and_check(ctx);
+    std::vector<int> newr;
+    for (int j = 0; j < nroots; ++j) {
+      if (j >= nr_ || conv[j]) continue;
+      const double res = std::sqrt(nr[j]);
+      rnorm[j] = res;
+      if (res < cfg.tol_residual) {
+        conv[j] = 1;
+        evals[j] = th[j];
+        QX_CUDA(cudaMemcpyAsync(evecs.p + (size_t)j * ld, W.X.p + (size_t)j * ld, ld * sizeof(double),
+                                cudaMemcpyDeviceToDevice, ctx->stream));
         continue;
       }
-      // Double Gram-Schmidt of each candidate against the subspace (davidson.rs:240-285).
-      int added = 0;
-      for (int q = 0; q < nnew; ++q) {
-        double* src = B->V.p + (size_t)(nv + q) * ld;
-        double* dst = B->V.p + (size_t)(nv + added) * ld;
-        if (src != dst)
-          QX_CUDA(cudaMemcpyAsync(dst, src, ld * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
-        const int cur = nv + added;
-        for (int pass = 0; pass < 2; ++pass) {
+      newr.push_back(j);
+    }
+    all = std::all_of(conv.begin(), conv.end(), [](int c) { return c != 0; });
+    if (all) {
+      ++iter;
+      break;
+    }
+    if (newr.empty()) continue;
+    // Preconditioned residuals t_j (davidson.rs:444-449), staged after V.
+    const int nnew = (int)newr.size();
+    for (int q = 0; q < nnew; ++q) {
+      const int j = newr[q];
+      double* t = W.V.p + (size_t)(nv + q) * ld;
+      QX_CUDA(cudaMemsetAsync(d_c, 0, sizeof(double), ctx->stream));
+      k_precond<<<1, kRedThreads, 0, ctx->stream>>>(W.R.p + (size_t)j * ld, d_delta, th[j], cfg.level_shift, n,
+                                                    t, d_c);
+      check_launch(ctx);
+      k_normalize<<<nblk, nthreads, 0, ctx->stream>>>(t, n, d_c, 1e-14);
+      check_launch(ctx);
+    }
+    if (nv + nnew > max_space) {
+      // Restart from the Ritz vectors, re-orthonormalised (davidson.rs:298-307).
+      QX_CUDA(cudaMemcpyAsync(W.V.p, W.X.p, (size_t)nr_ * ld * sizeof(double), cudaMemcpyDeviceToDevice,
+                              ctx->stream));
+      for (int i = 0; i < nr_; ++i) {
+        double* v = W.V.p + (size_t)i * ld;
+        for (int pass = 0; pass < 2 && i > 0; ++pass) {
           GemmNT g{};
-          g.M = cur;
+          g.M = i;
           g.N = 1;
           g.K = n;
-          g.A = B->V.p;
+          g.A = W.V.p;
           g.lda = ld;
-          g.B = dst;
+          g.B = v;
           g.ldb = ld;
           g.C = d_c;
           g.ldc = 1;
@@ -781,52 +753,124 @@ qx_status qx_bse_davidson(qx_bse* B, const qx_davidson_config* cfgp, double* eig
           g.alpha = 1.0;
           g.splitk = 0;
           gemm_nt_f64(ctx, g);
-          combine_rows(ctx, B->V.p, ld, cur, d_c, 1, 1, n, dst, ld, -1.0, 1.0);
+          combine_rows(ctx, W.V.p, ld, i, d_c, 1, 1, n, v, ld, -1.0, 1.0);
         }
         QX_CUDA(cudaMemsetAsync(d_nrm, 0, sizeof(double), ctx->stream));
-        k_norm2<<<1, kRedThreads, 0, ctx->stream>>>(dst, n, d_nrm);
+        k_norm2<<<1, kRedThreads, 0, ctx->stream>>>(v, n, d_nrm);
         check_launch(ctx);
-        double h2 = 0.0;
-        QX_CUDA(cudaMemcpyAsync(&h2, d_nrm, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-        sync_and_check(ctx);
-        if (std::sqrt(h2) < cfg.lindep_threshold) continue;
-        k_normalize<<<nblk, nthreads, 0, ctx->stream>>>(dst, n, d_nrm, -1.0);
+        k_normalize<<<nblk, nthreads, 0, ctx->stream>>>(v, n, d_nrm, -1.0);
         check_launch(ctx);
-        ++added;
       }
-      QX_CUDA(cudaMemsetAsync(B->V.p + (size_t)(nv + added) * ld, 0, (size_t)(cap - nv - added) * ld * sizeof(double),
-                              ctx->stream));
-      if (added > 0) apply(nv, added);
-      nv += added;
+      nv = nr_;
+      QX_CUDA(cudaMemsetAsync(W.V.p + (size_t)nv * ld, 0, (size_t)(cap - nv) * ld * sizeof(double), ctx->stream));
+      apply(0, nv);
+      continue;
     }
-    // Not converged: the latest Ritz approximation for roots never stored
-    // (davidson.rs:480-496).
-    if (!all) {
-      const int nr_ = std::min(nroots, nv);
-      rr(nv, nr_);
-      combine_rows(ctx, B->V.p, ld, nv, B->Z2.p, nv, nr_, n, B->X.p, ld, 1.0, 0.0);
-      QX_CUDA(cudaMemcpyAsync(th.data(), d_theta, nr_ * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    // Double Gram-Schmidt of each candidate against the subspace (davidson.rs:240-285).
+    int added = 0;
+    for (int q = 0; q < nnew; ++q) {
+      double* src = W.V.p + (size_t)(nv + q) * ld;
+      double* dst = W.V.p + (size_t)(nv + added) * ld;
+      if (src != dst)
+        QX_CUDA(cudaMemcpyAsync(dst, src, ld * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+      const int cur = nv + added;
+      for (int pass = 0; pass < 2; ++pass) {
+        GemmNT g{};
+        g.M = cur;
+        g.N = 1;
+        g.K = n;
+        g.A = W.V.p;
+        g.lda = ld;
+        g.B = dst;
+        g.ldb = ld;
+        g.C = d_c;
+        g.ldc = 1;
+        g.batch = 1;
+        g.alpha = 1.0;
+        g.splitk = 0;
+        gemm_nt_f64(ctx, g);
+        combine_rows(ctx, W.V.p, ld, cur, d_c, 1, 1, n, dst, ld, -1.0, 1.0);
+      }
+      QX_CUDA(cudaMemsetAsync(d_nrm, 0, sizeof(double), ctx->stream));
+      k_norm2<<<1, kRedThreads, 0, ctx->stream>>>(dst, n, d_nrm);
+      check_launch(ctx);
+      double h2 = 0.0;
+      QX_CUDA(cudaMemcpyAsync(&h2, d_nrm, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
       sync_and_check(ctx);
-      for (int j = 0; j < nr_; ++j)
-        if (!conv[j]) {
-          evals[j] = th[j];
-          QX_CUDA(cudaMemcpyAsync(evecs.p + (size_t)j * ld, B->X.p + (size_t)j * ld, ld * sizeof(double),
-                                  cudaMemcpyDeviceToDevice, ctx->stream));
-        }
-      iter = cfg.max_iter;
+      if (std::sqrt(h2) < cfg.lindep_threshold) continue;
+      k_normalize<<<nblk, nthreads, 0, ctx->stream>>>(dst, n, d_nrm, -1.0);
+      check_launch(ctx);
+      ++added;
     }
-    std::vector<double> hv((size_t)nroots * ld), ev((size_t)n * nroots);
-    QX_CUDA(cudaMemcpyAsync(hv.data(), evecs.p, hv.size() * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    QX_CUDA(cudaMemsetAsync(W.V.p + (size_t)(nv + added) * ld, 0, (size_t)(cap - nv - added) * ld * sizeof(double),
+                            ctx->stream));
+    if (added > 0) apply(nv, added);
+    nv += added;
+  }
+  // Not converged: the latest Ritz approximation for roots never stored
+  // (davidson.rs:480-496).
+  if (!all) {
+    const int nr_ = std::min(nroots, nv);
+    rr(nv, nr_);
+    combine_rows(ctx, W.V.p, ld, nv, W.Z2.p, nv, nr_, n, W.X.p, ld, 1.0, 0.0);
+    QX_CUDA(cudaMemcpyAsync(th.data(), d_theta, nr_ * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     sync_and_check(ctx);
-    for (int k = 0; k < n; ++k)
-      for (int r = 0; r < nroots; ++r) ev[(size_t)k * nroots + r] = hv[(size_t)r * ld + k];
-    QX_CUDA(cudaMemcpy(eigenvalues, evals.data(), nroots * sizeof(double), cudaMemcpyDefault));
-    QX_CUDA(cudaMemcpy(eigenvectors, ev.data(), ev.size() * sizeof(double), cudaMemcpyDefault));
-    if (converged_out)
-      for (int r = 0; r < nroots; ++r) converged_out[r] = conv[r];
-    if (residual_norms)
-      for (int r = 0; r < nroots; ++r) residual_norms[r] = rnorm[r];
-    if (iterations) *iterations = iter;
+    for (int j = 0; j < nr_; ++j)
+      if (!conv[j]) {
+        evals[j] = th[j];
+        QX_CUDA(cudaMemcpyAsync(evecs.p + (size_t)j * ld, W.X.p + (size_t)j * ld, ld * sizeof(double),
+                                cudaMemcpyDeviceToDevice, ctx->stream));
+      }
+    iter = cfg.max_iter;
+  }
+  std::vector<double> hv((size_t)nroots * ld), ev((size_t)n * nroots);
+  QX_CUDA(cudaMemcpyAsync(hv.data(), evecs.p, hv.size() * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  sync_and_check(ctx);
+  for (int k = 0; k < n; ++k)
+    for (int r = 0; r < nroots; ++r) ev[(size_t)k * nroots + r] = hv[(size_t)r * ld + k];
+  QX_CUDA(cudaMemcpy(eigenvalues, evals.data(), nroots * sizeof(double), cudaMemcpyDefault));
+  QX_CUDA(cudaMemcpy(eigenvectors, ev.data(), ev.size() * sizeof(double), cudaMemcpyDefault));
+  if (converged_out)
+    for (int r = 0; r < nroots; ++r) converged_out[r] = conv[r];
+  if (residual_norms)
+    for (int r = 0; r < nroots; ++r) residual_norms[r] = rnorm[r];
+  if (iterations) *iterations = iter;
+}
+
+qx_status qx_bse_davidson(qx_bse* B, const qx_davidson_config* cfgp, double* eigenvalues, double* eigenvectors,
+                          int* converged_out, double* residual_norms, int* iterations) {
+  if (!B || !cfgp) return QX_ERR_INVALID_INPUT;
+  return bse_guard(B->ctx, [&] {
+    davidson_run(B->ctx, B->dav, B->nov, B->ldov, B->delta.p, B->h_delta,
+                 [&](const double* x, double* y, int count) { bse_apply_rows(B, x, y, count); }, *cfgp, eigenvalues,
+                 eigenvectors, converged_out, residual_norms, iterations);
+  });
+}
+
+qx_status qx_davidson(qx_ctx* ctx, int n, const double* qp_gaps, qx_apply_fn apply_h, void* user,
+                      const qx_davidson_config* cfgp, double* eigenvalues, double* eigenvectors, int* converged_out,
+                      double* residual_norms, int* iterations) {
+  if (!ctx || !cfgp || !apply_h) return QX_ERR_INVALID_INPUT;
+  return bse_guard(ctx, [&] {
+    QX_REQUIRE(n > 0 && qp_gaps, QX_ERR_INVALID_INPUT, "davidson needs n > 0 (got %d) and qp_gaps", n);
+    const int ld = round_up(n, 8);
+    std::vector<double> h(n);
+    QX_CUDA(cudaMemcpy(h.data(), qp_gaps, n * sizeof(double), cudaMemcpyDefault));
+    for (double v : h) QX_REQUIRE(std::isfinite(v), QX_ERR_INVALID_INPUT, "qp_gaps contains NaN or Inf");
+    DevArr d;
+    d.alloc(ld);
+    QX_CUDA(cudaMemsetAsync(d.p, 0, ld * sizeof(double), ctx->stream));
+    upload(ctx, d.p, h.data(), n);
+    DavWork W;
+    davidson_run(ctx, W, n, ld, d.p, h,
+                 [&](const double* x, double* y, int count) {
+                   sync_and_check(ctx);
+                   const int rc = apply_h(user, x, y, count, ld);
+                   QX_CUDA(cudaDeviceSynchronize());
+                   QX_REQUIRE(rc == 0, (rc > 0 && rc <= (int)QX_ERR_NO_DEVICE) ? (qx_status)rc : QX_ERR_INVALID_INPUT,
+                              "apply_h returned %d", rc);
+                 },
+                 *cfgp, eigenvalues, eigenvectors, converged_out, residual_norms, iterations);
   });
 }
 

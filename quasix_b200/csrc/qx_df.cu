@@ -309,6 +309,33 @@ double metric_inv_sqrt(qx_ctx* ctx, const double* J, int n, int ldj, double* Jm,
 }
 
 size_t metric_work_doubles(int n, int ld) { return 4 * (size_t)n * ld + 520 + 2 * ((size_t)n + 8) + 64; }
+
+// out[b] = s (in[b] + in[b]^T) / 2 + t I over n x n matrices (row stride ld,
+// batch stride st; in and out distinct).  grid (x, batch).
+__global__ void k_sym_batch(const double* __restrict__ in, int n, int ld, size_t st, double s, double t,
+                            double* __restrict__ out) {
+  const double* a = in + blockIdx.y * st;
+  double* o = out + blockIdx.y * st;
+  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < (size_t)n * n;
+       e += (size_t)gridDim.x * blockDim.x) {
+    const size_t r = e / n, c = e % n;
+    o[r * ld + c] = s * (0.5 * (a[r * ld + c] + a[c * ld + r])) + (r == c ? t : 0.0);
+  }
+}
+
+// A[b] += t I in place.  grid (x, batch).
+__global__ void k_add_diag_batch(double* __restrict__ A, int n, int ld, size_t st, double t) {
+  double* a = A + blockIdx.y * st;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) a[(size_t)i * ld + i] += t;
+}
+
+// Any non-finite entry of the n x n matrices (row stride ld) sets *flag.
+__global__ void k_nonfinite(const double* __restrict__ A, int n, int ld, size_t st, int* __restrict__ flag) {
+  const double* a = A + blockIdx.y * st;
+  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < (size_t)n * n;
+       e += (size_t)gridDim.x * blockDim.x)
+    if (!isfinite(a[(e / n) * ld + e % n])) *flag = 1;
+}
 }  // namespace
 }  // namespace qx
 
@@ -356,6 +383,73 @@ qx_status qx_metric_inv_sqrt(qx_ctx* ctx, const double* metric, int naux, double
       QX_CUDA(cudaMemcpy2DAsync(sqrt_metric, naux * sizeof(double), jp, ld * sizeof(double), naux * sizeof(double),
                                 naux, cudaMemcpyDefault, ctx->stream));
     sync_and_check(ctx);
+  });
+}
+
+// The S3-3 screened interaction W(w) = v^1/2 (I - v^1/2 P0(w) v^1/2)^-1 v^1/2
+// (quasix_core/src/dielectric/screening.rs:164-236 compute_screened_interaction,
+// :334-410 compute_W_single_frequency, :580-639 compute_metric_sqrt).
+// v^1/2 is the symmetric square root (the Denman-Beavers iterate, equal to
+// the reference's eigendecomposition form when no eigenvalue of v lies at or
+// below its clamp 1e-14; such metrics are rejected).  Per frequency, as the
+// reference: eps = I - v^1/2 P0 v^1/2, symmetrised by averaging; eps^-1 by
+// the guarded block sweep (pivoted fallback where the reference would fall
+// from Cholesky to LU); W = v^1/2 eps^-1 v^1/2, symmetrised.  All products
+// are FP64 DMMA GEMMs, batched over the frequencies of a chunk.
+qx_status qx_compute_screened_interaction(qx_ctx* ctx, int nfreq, int naux, const double* p0, const double* v_aux,
+                                          double* w) {
+  return run_df(ctx, [&] {
+    QX_REQUIRE(p0 && v_aux && w && nfreq > 0 && naux > 0, QX_ERR_INVALID_INPUT,
+               "invalid arguments to compute_screened_interaction (nfreq=%d naux=%d)", nfreq, naux);
+    const int ld = round_up(naux, 8);
+    const size_t nn = (size_t)naux * ld, dense = (size_t)naux * naux;
+    const double* d_v = (const double*)device_view(ctx, WS_LPQ, v_aux, dense * sizeof(double));
+    DevBuf& mb = ctx->ws[WS_BSE2];
+    mb.reserve((2 * nn + metric_work_doubles(naux, ld)) * sizeof(double));
+    double* vm = mb.as<double>();
+    double* vs = vm + nn;
+    const double clamp = 1e-14;
+    const double lmin = metric_inv_sqrt(ctx, d_v, naux, naux, vm, vs, ld, vs + nn, clamp);
+    QX_REQUIRE(lmin > clamp, QX_ERR_NUMERICAL,
+               "v_aux has an eigenvalue (%.3e) at or below %.0e: it is not positive definite", lmin, clamp);
+    const double* d_p = (const double*)device_view(ctx, WS_BSE4, p0, (size_t)nfreq * dense * sizeof(double));
+    // Three [fc][naux][ld] buffers per chunk of fc frequencies, at most ~3 GB.
+    const size_t cap = std::max<size_t>(1, ((size_t)3 << 30) / (3 * nn * sizeof(double)));
+    const int fc = (int)std::min<size_t>({(size_t)nfreq, cap, (size_t)65535});
+    DevBuf& wb = ctx->ws[WS_BSE3];
+    wb.reserve((3 * (size_t)fc * nn + 64) * sizeof(double));
+    double* A = wb.as<double>();
+    double* B = A + (size_t)fc * nn;
+    double* E = B + (size_t)fc * nn;
+    int* flag = reinterpret_cast<int*>(E + (size_t)fc * nn);
+    QX_CUDA(cudaMemsetAsync(A, 0, (3 * (size_t)fc * nn + 64) * sizeof(double), ctx->stream));
+    const int blocks = std::max(1, std::min<int>((int)((dense + 255) / 256), 2 * ctx->sm_count / std::max(1, fc) + 1));
+    for (int f0 = 0; f0 < nfreq; f0 += fc) {
+      const int nb = std::min(fc, nfreq - f0);
+      // A = P0^T; B = v^1/2 P0; A = M = v^1/2 P0 v^1/2; E = eps = I - sym(M).
+      transpose(ctx, d_p + (size_t)f0 * dense, naux, naux, naux, dense, A, ld, nn, nb);
+      gemm(ctx, naux, naux, naux, vs, ld, 0, A, ld, nn, B, ld, nn, nb);
+      gemm(ctx, naux, naux, naux, B, ld, nn, vs, ld, 0, A, ld, nn, nb);
+      k_sym_batch<<<dim3(blocks, nb), 256, 0, ctx->stream>>>(A, naux, ld, nn, -1.0, 1.0, E);
+      check_launch(ctx);
+      // The sweep leaves eps^-1 - I in place.
+      launch_invert_wc(ctx, E, naux, ld, nn, nb, /*guard=*/1);
+      k_add_diag_batch<<<dim3(ceil_div(naux, 256), nb), 256, 0, ctx->stream>>>(E, naux, ld, nn, 1.0);
+      check_launch(ctx);
+      // B = v^1/2 eps^-T; A = v^1/2 eps^-T v^1/2; E = W = sym(A) (= sym(v^1/2 eps^-1 v^1/2)).
+      gemm(ctx, naux, naux, naux, vs, ld, 0, E, ld, nn, B, ld, nn, nb);
+      gemm(ctx, naux, naux, naux, B, ld, nn, vs, ld, 0, A, ld, nn, nb);
+      k_sym_batch<<<dim3(blocks, nb), 256, 0, ctx->stream>>>(A, naux, ld, nn, 1.0, 0.0, E);
+      check_launch(ctx);
+      k_nonfinite<<<dim3(blocks, nb), 256, 0, ctx->stream>>>(E, naux, ld, nn, flag);
+      check_launch(ctx);
+      QX_CUDA(cudaMemcpy2DAsync(w + (size_t)f0 * dense, naux * sizeof(double), E, ld * sizeof(double),
+                                naux * sizeof(double), (size_t)nb * naux, cudaMemcpyDefault, ctx->stream));
+    }
+    int hf = 0;
+    QX_CUDA(cudaMemcpyAsync(&hf, flag, sizeof hf, cudaMemcpyDeviceToHost, ctx->stream));
+    sync_and_check(ctx);
+    QX_REQUIRE(hf == 0, QX_ERR_NUMERICAL, "W contains NaN or Inf values");
   });
 }
 

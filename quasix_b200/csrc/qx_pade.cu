@@ -8,6 +8,7 @@
 // each orbital's coefficients, or a tile of states, in shared memory and run
 // one thread per output element.
 #include <algorithm>
+#include <cfloat>
 
 #include "pade.cuh"
 #include "qx_internal.cuh"
@@ -149,6 +150,104 @@ __global__ void k_spectral_states(const double* __restrict__ e, const double* __
     const double d = omega[q] - e[i];
     A[k] = z[i] * eta / (d * d + eta * eta) / M_PI;
   }
+}
+
+// NewtonQPSolver::solve with the Pade-continued Sigma_c as its evaluator
+// (quasix_core/src/qp/newton_solver.rs:174-280 Newton with adaptive damping,
+// :282-315 derivative and Z, :317-392 bisection fallback, :394-401 residual),
+// one thread per orbital.  method: 0 Newton, 1 bisection, -1 neither
+// converged (the reference's ConvergenceError).
+struct NewtonArgs {
+  qx_newton_config cfg;
+  int norbs, nfit;
+  const cplx* coeff;  // [nfit][norbs]
+  const cplx* zfit;   // [norbs][nfit]
+  const double *eps, *sx, *vxc, *guess;
+  double ef;
+  double *qp, *res, *z;
+  cplx* sc;
+  int *iters, *method;
+};
+
+__global__ void k_newton_qp(NewtonArgs p) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= p.norbs) return;
+  const int nfit = p.nfit;
+  cplx zn[MAX_FIT], a[MAX_FIT];
+  for (int j = 0; j < nfit; ++j) {
+    zn[j] = p.zfit[(size_t)t * nfit + j];
+    a[j] = p.coeff[(size_t)j * p.norbs + t];
+  }
+  const qx_newton_config& c = p.cfg;
+  const double eps = p.eps[t], sx = p.sx[t], vxc = p.vxc[t], ef = p.ef, guess = p.guess[t];
+  auto sig = [&](double w) { return pade_eval(w, zn, a, nfit); };
+  auto deriv = [&](double w) {
+    const double de = c.derivative_delta;
+    if (c.use_richardson) {
+      const double p1 = sig(w + de).re, m1 = sig(w - de).re, p2 = sig(w + 2.0 * de).re, m2 = sig(w - 2.0 * de).re;
+      return (8.0 * (p1 - m1) - (p2 - m2)) / (12.0 * de);
+    }
+    return (sig(w + de).re - sig(w - de).re) / (2.0 * de);
+  };
+  auto zfac = [&](double e) { return fmin(fmax(1.0 / (1.0 - deriv(e - ef)), c.z_min), c.z_max); };
+  auto resid = [&](double e) { return e - eps - sx - sig(e - ef).re + vxc; };
+  double energy = guess, damping = c.initial_damping, prev = DBL_MAX, ares = 0.0;
+  for (int it = 0; it < c.max_iterations; ++it) {
+    const double omega = energy - ef;
+    const cplx s = sig(omega);
+    const double r = energy - eps - sx - s.re + vxc;
+    ares = fabs(r);
+    if (ares < c.energy_tolerance) {
+      p.qp[t] = energy;
+      p.res[t] = ares;
+      p.iters[t] = it + 1;
+      p.method[t] = 0;
+      p.sc[t] = s;
+      p.z[t] = zfac(energy);
+      return;
+    }
+    const double fp = 1.0 - deriv(omega);
+    const double step = fabs(fp) < 1e-10 ? -copysign(1.0, r) * fmin(c.max_step, ares) : -r / fp;
+    const double clipped = fmin(fmax(step, -c.max_step), c.max_step);
+    if (ares > prev) damping = fmax(damping * 0.5, c.min_damping);
+    else if (ares < 0.5 * prev && damping < c.max_damping) damping = fmin(damping * 1.2, c.max_damping);
+    energy += damping * clipped;
+    prev = ares;
+  }
+  if (c.use_bisection_fallback) {
+    const double width = 2.0;
+    double lo = guess - width, hi = guess + width;
+    if (resid(lo) * resid(hi) > 0.0) {
+      for (int e = 1; e < 5; ++e) {
+        const double wd = width * (double)(1 << e);
+        lo = guess - wd;
+        hi = guess + wd;
+        if (resid(lo) * resid(hi) <= 0.0) break;
+      }
+    }
+    for (int it = 0; it < c.max_bisection_iterations; ++it) {
+      const double mid = 0.5 * (lo + hi);
+      const double fm = resid(mid);
+      if (fabs(fm) < c.energy_tolerance || 0.5 * (hi - lo) < c.energy_tolerance) {
+        p.qp[t] = mid;
+        p.res[t] = fabs(fm);
+        p.iters[t] = it + 1;
+        p.method[t] = 1;
+        p.sc[t] = sig(mid - ef);
+        p.z[t] = zfac(mid);
+        return;
+      }
+      if (fm * resid(lo) < 0.0) hi = mid;
+      else lo = mid;
+    }
+  }
+  // Not converged: the last Newton iterate, its residual and Z.
+  p.qp[t] = energy;
+  p.res[t] = prev;
+  p.iters[t] = c.max_iterations;
+  p.method[t] = -1;
+  p.sc[t] = sig(energy - ef);
+  p.z[t] = zfac(energy);
 }
 
 // Device copies of small caller arrays, carved from one workspace slot.
@@ -371,6 +470,58 @@ qx_status qx_spectral_function_pade(qx_ctx* ctx, int norbs, int nfit, const doub
                                                                                  d_vx, ef, d_w, n_omega, eta, d_a);
     check_launch(ctx);
     if (d_a != A) QX_CUDA(cudaMemcpyAsync(A, d_a, ab, cudaMemcpyDeviceToHost, ctx->stream));
+    sync_and_check(ctx);
+  });
+}
+
+qx_status qx_newton_qp_solve(qx_ctx* ctx, const qx_newton_config* cfg, int norbs, int nfit, const double* coeff,
+                             const double* omega_fit, const double* epsilon_hf, const double* sigma_x,
+                             const double* vxc, double fermi_level, const double* initial_guess, double* qp_energy,
+                             double* residual, int* iterations, int* method, double* sigma_c, double* z_factor) {
+  return run(ctx, [&] {
+    QX_REQUIRE(cfg && norbs >= 0 && nfit >= 1, QX_ERR_INVALID_INPUT, "invalid arguments to newton_qp_solve");
+    QX_REQUIRE(nfit <= MAX_FIT, QX_ERR_INVALID_INPUT, "nfit %d exceeds %d", nfit, MAX_FIT);
+    QX_REQUIRE(cfg->max_iterations >= 0 && cfg->max_bisection_iterations >= 0 && cfg->derivative_delta > 0.0 &&
+                   cfg->max_step > 0.0,
+               QX_ERR_INVALID_INPUT, "invalid Newton configuration");
+    if (norbs == 0) return;
+    QX_REQUIRE(coeff && omega_fit && epsilon_hf && sigma_x && vxc && initial_guess && qp_energy && residual &&
+                   iterations && method && sigma_c && z_factor,
+               QX_ERR_INVALID_INPUT, "null argument to newton_qp_solve");
+    const size_t cb = (size_t)nfit * norbs * 2 * sizeof(double), ob = (size_t)norbs * sizeof(double);
+    DevBuf& wb = ctx->ws[WS_QPOUT];
+    wb.reserve(carve_bytes({cb, cb, ob, ob, ob, ob, ob, ob, ob, 2 * ob, norbs * sizeof(int), norbs * sizeof(int)}));
+    Carve cv{wb.as<char>()};
+    NewtonArgs a;
+    a.cfg = *cfg;
+    a.norbs = norbs;
+    a.nfit = nfit;
+    auto in = [&](const double* src, size_t n) {
+      double* d = cv.take<double>(n);
+      QX_CUDA(cudaMemcpyAsync(d, src, n * sizeof(double), cudaMemcpyDefault, ctx->stream));
+      return d;
+    };
+    a.coeff = reinterpret_cast<const cplx*>(in(coeff, (size_t)nfit * norbs * 2));
+    a.zfit = reinterpret_cast<const cplx*>(in(omega_fit, (size_t)nfit * norbs * 2));
+    a.eps = in(epsilon_hf, norbs);
+    a.sx = in(sigma_x, norbs);
+    a.vxc = in(vxc, norbs);
+    a.guess = in(initial_guess, norbs);
+    a.ef = fermi_level;
+    a.qp = cv.take<double>(norbs);
+    a.res = cv.take<double>(norbs);
+    a.z = cv.take<double>(norbs);
+    a.sc = cv.take<cplx>(norbs);
+    a.iters = cv.take<int>(norbs);
+    a.method = cv.take<int>(norbs);
+    k_newton_qp<<<ceil_div(norbs, 64), 64, 0, ctx->stream>>>(a);
+    check_launch(ctx);
+    QX_CUDA(cudaMemcpyAsync(qp_energy, a.qp, ob, cudaMemcpyDefault, ctx->stream));
+    QX_CUDA(cudaMemcpyAsync(residual, a.res, ob, cudaMemcpyDefault, ctx->stream));
+    QX_CUDA(cudaMemcpyAsync(z_factor, a.z, ob, cudaMemcpyDefault, ctx->stream));
+    QX_CUDA(cudaMemcpyAsync(sigma_c, a.sc, 2 * ob, cudaMemcpyDefault, ctx->stream));
+    QX_CUDA(cudaMemcpyAsync(iterations, a.iters, norbs * sizeof(int), cudaMemcpyDefault, ctx->stream));
+    QX_CUDA(cudaMemcpyAsync(method, a.method, norbs * sizeof(int), cudaMemcpyDefault, ctx->stream));
     sync_and_check(ctx);
   });
 }

@@ -7,9 +7,11 @@ Reference interfaces (QuasiX, by path within the project):
 * ``get_rho_response`` / ``compute_polarizability_p0``
                                  correlation_ac.rs:184-211, dielectric/polarizability.rs:169-275
 * ``compute_epsilon_inverse``    correlation_ac.rs:377-401 (quasix/src/lib.rs:1694)
+* ``compute_screened_interaction``  dielectric/screening.rs:164-236
 * ``get_sigma_diag``             correlation_ac.rs:241-449
 * ``ac_pade_thiele_diag`` / ``pade_thiele``  correlation_ac.rs:470-654
 * ``compute_exchange_diag``      quasix_core/src/qp/evgw.rs:1167-1193
+* ``NewtonQPSolver`` / ``newton_qp_solve``  quasix_core/src/qp/newton_solver.rs:52-402
 * ``evgw`` / ``run_evgw``        quasix/src/evgw.rs:22-677
 * ``g0w0_cd``                    contour deformation (imaginary-axis term of
                                  selfenergy/correlation_pyscf_cd.rs:164-259 plus residues)
@@ -17,6 +19,7 @@ Reference interfaces (QuasiX, by path within the project):
 from __future__ import annotations
 
 import ctypes as C
+from dataclasses import dataclass, fields
 from typing import Dict, List, Optional, Sequence
 
 import numpy as np
@@ -94,6 +97,26 @@ def compute_epsilon_inverse_minus_identity(pi, device: int = 0) -> np.ndarray:
     return out[0] if single else out
 
 
+def compute_screened_interaction(p0, v_aux, freqs=None, device: int = 0) -> np.ndarray:
+    """W(w) = v^1/2 (I - v^1/2 P0(w) v^1/2)^-1 v^1/2 for P0 [nfreq, naux, naux]
+    (or one [naux, naux]) and the metric v_aux, with the symmetric square root
+    of v_aux (dielectric/screening.rs:164-236).  ``freqs`` is accepted for the
+    reference's signature and, as there, not used."""
+    ctx = _ctx(device)
+    p0 = _f64(p0)
+    v = np.ascontiguousarray(_f64(v_aux))
+    single = p0.ndim == 2
+    p = np.ascontiguousarray(p0[None] if single else p0)
+    if v.ndim != 2 or v.shape[0] != v.shape[1]:
+        raise ValueError(f"v_aux must be square, got {v.shape}")
+    if p.ndim != 3 or p.shape[1] != v.shape[0] or p.shape[2] != v.shape[0]:
+        raise ValueError(f"P0 dimension mismatch: expected [freq, {v.shape[0]}, {v.shape[0]}], got {p0.shape}")
+    out = np.zeros_like(p)
+    ctx.check(ctx.lib.qx_compute_screened_interaction(ctx.handle, p.shape[0], p.shape[1], N.ptr(p), N.ptr(v),
+                                                      N.ptr(out)))
+    return out[0] if single else out
+
+
 def get_sigma_diag(mo_energy, lpq, orbs: Sequence[int], nocc: int, nw: int = 100, iw_cutoff: float = 5.0,
                    x0: float = 0.5, precision="fp64", device: int = 0):
     """Sigma_c(iw) [norbs, nw_sigma] and the omega grid, both complex."""
@@ -147,6 +170,102 @@ def pade_thiele(omega, zn, coeff, device: int = 0):
     ctx.check(ctx.lib.qx_pade_thiele(ctx.handle, coeff.shape[0], N.ptr(zn), N.ptr(coeff), w.shape[0], N.ptr(w),
                                      N.ptr(out)))
     return out[0] if np.ndim(omega) == 0 else out
+
+
+@dataclass
+class NewtonSolverConfig:
+    """NewtonSolverConfig (qp/newton_solver.rs:52-103), same fields and
+    defaults (``verbose`` has no counterpart: the solve runs on the device)."""
+    max_iterations: int = 50
+    energy_tolerance: float = 1e-8
+    initial_damping: float = 1.0
+    min_damping: float = 0.1
+    max_damping: float = 1.0
+    max_step: float = 1.0
+    derivative_delta: float = 1e-6
+    use_richardson: bool = True
+    z_min: float = 0.1
+    z_max: float = 0.999
+    use_bisection_fallback: bool = True
+    max_bisection_iterations: int = 30
+
+    def native(self) -> N.NewtonConfig:
+        return N.NewtonConfig(**{f.name: (int(v) if isinstance(v, bool) else v)
+                                 for f in fields(self) for v in [getattr(self, f.name)]})
+
+
+@dataclass
+class NewtonSolverResult:
+    """NewtonSolverResult (qp/newton_solver.rs:105-122)."""
+    qp_energy: float
+    residual: float
+    iterations: int
+    converged: bool
+    sigma_c: complex
+    z_factor: float
+    method: str
+
+
+class ConvergenceError(N.QxError):
+    """The reference's QuasixError::ConvergenceError for one QP equation."""
+
+    def __init__(self, message: str):
+        super().__init__(4, message)
+
+
+_METHOD = {0: "newton", 1: "bisection", -1: "none"}
+
+
+def newton_qp_solve(coeff, omega_fit, epsilon_hf, sigma_x, vxc, fermi_level: float, initial_guess,
+                    config: Optional[NewtonSolverConfig] = None, device: int = 0) -> Dict[str, np.ndarray]:
+    """Solve E = eps + Sigma_x + Re Sigma_c(E - ef) - Vxc for every orbital at
+    once, one device thread each, with Sigma_c the Pade continuation given by
+    ``coeff`` [nfit, norbs] and ``omega_fit`` [norbs, nfit] (the output of
+    ``ac_pade_thiele_diag``).  Returns arrays ``qp_energy``, ``residual``,
+    ``iterations``, ``method`` (0 Newton, 1 bisection, -1 not converged),
+    ``converged``, ``sigma_c`` and ``z_factor``."""
+    cfg = (config or NewtonSolverConfig()).native()
+    ctx = _ctx(device)
+    coeff = np.ascontiguousarray(coeff, dtype=np.complex128)
+    ofit = np.ascontiguousarray(omega_fit, dtype=np.complex128)
+    if coeff.ndim != 2 or ofit.shape != (coeff.shape[1], coeff.shape[0]):
+        raise ValueError(f"coeff [nfit, norbs] and omega_fit [norbs, nfit] disagree: {coeff.shape}, {ofit.shape}")
+    nfit, norbs = coeff.shape
+    vec = [np.ascontiguousarray(np.broadcast_to(_f64(x), (norbs,))) for x in (epsilon_hf, sigma_x, vxc,
+                                                                               initial_guess)]
+    qp, res, z = np.zeros(norbs), np.zeros(norbs), np.zeros(norbs)
+    sc = np.zeros(norbs, dtype=np.complex128)
+    its, meth = np.zeros(norbs, dtype=np.int32), np.zeros(norbs, dtype=np.int32)
+    ctx.check(ctx.lib.qx_newton_qp_solve(ctx.handle, C.byref(cfg), norbs, nfit, N.ptr(coeff), N.ptr(ofit),
+                                         *[N.ptr(v) for v in vec[:3]], float(fermi_level), N.ptr(vec[3]),
+                                         N.ptr(qp), N.ptr(res), N.ptr(its), N.ptr(meth), N.ptr(sc), N.ptr(z)))
+    return {"qp_energy": qp, "residual": res, "iterations": its, "method": meth, "converged": meth >= 0,
+            "sigma_c": sc, "z_factor": z}
+
+
+class NewtonQPSolver:
+    """NewtonQPSolver (qp/newton_solver.rs:124-402) for one orbital.  The
+    reference's evaluator is any closure Sigma_c(w); on the device it is the
+    Pade continuation of that orbital, passed to ``solve`` as ``(zn, coeff)``
+    (complex [nfit] each, one column of ``ac_pade_thiele_diag``'s output)."""
+
+    def __init__(self, epsilon_hf: float, sigma_x: float, vxc: float, fermi_level: float,
+                 config: Optional[NewtonSolverConfig] = None, device: int = 0):
+        self.epsilon_hf, self.sigma_x, self.vxc = float(epsilon_hf), float(sigma_x), float(vxc)
+        self.fermi_level = float(fermi_level)
+        self.config = config or NewtonSolverConfig()
+        self.device = device
+
+    def solve(self, pade, initial_guess: float) -> NewtonSolverResult:
+        zn, coeff = (np.asarray(a, dtype=np.complex128).reshape(-1) for a in pade)
+        r = newton_qp_solve(coeff[:, None], zn[None, :], self.epsilon_hf, self.sigma_x, self.vxc, self.fermi_level,
+                            float(initial_guess), self.config, self.device)
+        m = int(r["method"][0])
+        if m < 0:
+            what = "Bisection fallback" if self.config.use_bisection_fallback else "Newton-Raphson"
+            raise ConvergenceError(f"{what} failed to converge (residual = {r['residual'][0]:.2e})")
+        return NewtonSolverResult(float(r["qp_energy"][0]), float(r["residual"][0]), int(r["iterations"][0]), True,
+                                  complex(r["sigma_c"][0]), float(r["z_factor"][0]), _METHOD[m])
 
 
 def compute_exchange_diag(lpq, nocc: int, device: int = 0) -> np.ndarray:
