@@ -502,7 +502,9 @@ def bse_grad_fd_check(q, s, nocc, npoints):
         if a != b:
             d[P, b, a] += 1e-6
         fd.append((f(e, lpq + d) - f(e, lpq - d)) / 2e-6)
-        an.append(float(gl[P, a, b]) * (2 if a != b else 1))
+        # The symmetric step moves both entries: its derivative is the sum of
+        # the two gradient entries (the forward reads one triangle of some blocks).
+        an.append(float(gl[P, a, b]) + (float(gl[P, b, a]) if a != b else 0.0))
     an, fd = np.array(an), np.array(fd)
     return {"points": npoints, "max_rel_err": float(np.abs(an - fd).max() / np.abs(fd).max()),
             "s_forward_and_backward_fp64": t_fwd_bwd,

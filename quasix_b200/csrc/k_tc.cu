@@ -192,11 +192,14 @@ struct TcThreads {
   static constexpr int VALUE = TcWarps<EPI>::THREADS + (CONVB ? 32 * kConvWarps : 0);
 };
 
-template <int BN, int EPI>
+template <int BN, int EPI, bool CONVB = false>
 struct TcSmem {
   static constexpr int A_BYTES = TC_BM * TcPipe<EPI>::BK * 2;
   static constexpr int B_BYTES = BN * TcPipe<EPI>::BK * 2;
-  static constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;
+  // CONVB: the FP32 B tile as TMA lands it, two 32-column boxes with the
+  // 128-byte swizzle, read by the converter warps.
+  static constexpr int F32_BYTES = CONVB ? BN * TcPipe<EPI>::BK * 4 : 0;
+  static constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES + F32_BYTES;
   static constexpr int BAR_OFF = TcPipe<EPI>::STAGES * STAGE_BYTES;
   static constexpr int RED_OFF = BAR_OFF + 256;  // ROWDOT: partial row sums [2][128] doubles + 2 flags
   static constexpr int TOTAL = RED_OFF + 2048 + 64 + 1024;  // + alignment slack
@@ -237,10 +240,9 @@ struct TcArgs {
   const int* gpre;
   int gcount;
   int unit;  // STORE: k-blocks per FP32 accumulation unit (0 counts as 1)
-  // CONVB: B[w][n][k] = convB[n][k] * convC[w][k] (FP32, both zero past K),
-  // converted to hi/lo by the converter warps instead of TMA loads.
-  const float* convB;
-  int ldconv;
+  // CONVB: B[w][n][k] = convB[n][k] * convC[w][k] (FP32, zero past K): the
+  // FP32 tile of convB arrives by TMA (map in the mapBh slot), and the
+  // converter warps scale and split it into the hi/lo tile the MMA reads.
   const float* convC;
   int ldcc;
 };
@@ -280,7 +282,7 @@ __global__ void __launch_bounds__(TcThreads<EPI, CONVB>::VALUE, 1)
     k_tc_gemm(const __grid_constant__ CUtensorMap mapAh, const __grid_constant__ CUtensorMap mapAl,
               const __grid_constant__ CUtensorMap mapBh, const __grid_constant__ CUtensorMap mapBl, TcArgs args) {
   static_assert(!CONVB || (EPI == EPI_STORE && BN == 128), "the converted B operand serves P0's STORE tiles");
-  using L = TcSmem<BN, EPI>;
+  using L = TcSmem<BN, EPI, CONVB>;
   constexpr int TC_BK = TcPipe<EPI>::BK;
   constexpr int TC_STAGES = TcPipe<EPI>::STAGES;
   extern __shared__ __align__(1024) uint8_t smem_raw[];
@@ -290,7 +292,8 @@ __global__ void __launch_bounds__(TcThreads<EPI, CONVB>::VALUE, 1)
   uint64_t* acc_full = empty + TC_STAGES;   // [2]
   uint64_t* acc_empty = acc_full + 2;       // [2]
   uint64_t* drain = acc_empty + 2;          // all issued MMAs complete
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain + 1);
+  uint64_t* conv = drain + 1;               // CONVB: [TC_STAGES] converted B tile ready
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(conv + TC_STAGES);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -360,9 +363,10 @@ __global__ void __launch_bounds__(TcThreads<EPI, CONVB>::VALUE, 1)
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < TC_STAGES; ++s) {
-      // CONVB: the TMA of A plus one arrival per converter warp.
-      mbar_init(&full[s], CONVB ? 1 + kConvWarps : 1);
+      mbar_init(&full[s], 1);
       mbar_init(&empty[s], 1);
+      // CONVB: one arrival per converter warp once the hi/lo B tile is written.
+      if (CONVB) mbar_init(&conv[s], kConvWarps);
     }
     for (int b = 0; b < 2; ++b) {
       mbar_init(&acc_full[b], 1);
@@ -397,7 +401,7 @@ __global__ void __launch_bounds__(TcThreads<EPI, CONVB>::VALUE, 1)
               if (!mbar_wait(&empty[s], ((g / TC_STAGES) - 1) & 1, abort_flag, args.err, 1)) goto producer_done;
             }
             uint8_t* st = smem + s * L::STAGE_BYTES;
-            mbar_expect_tx(&full[s], CONVB ? 2 * L::A_BYTES : L::STAGE_BYTES);
+            mbar_expect_tx(&full[s], CONVB ? 2 * L::A_BYTES + L::F32_BYTES : L::STAGE_BYTES);
             const int k0 = kb * TC_BK;
             if (args.a_batched) {
               tma_load_3d(st, &mapAh, &full[s], k0, m0, w);
@@ -406,7 +410,11 @@ __global__ void __launch_bounds__(TcThreads<EPI, CONVB>::VALUE, 1)
               tma_load_2d(st, &mapAh, &full[s], k0, row_off + m0);
               tma_load_2d(st + L::A_BYTES, &mapAl, &full[s], k0, row_off + m0);
             }
-            if (!CONVB) {
+            if (CONVB) {
+              uint8_t* f32 = st + 2 * L::A_BYTES + 2 * L::B_BYTES;
+              tma_load_2d(f32, &mapBh, &full[s], k0, n0);
+              tma_load_2d(f32 + L::F32_BYTES / 2, &mapBh, &full[s], k0 + TC_BK / 2, n0);
+            } else {
               tma_load_3d(st + 2 * L::A_BYTES, &mapBh, &full[s], k0, row_off + n0, w);
               tma_load_3d(st + 2 * L::A_BYTES + L::B_BYTES, &mapBl, &full[s], k0, row_off + n0, w);
             }
@@ -447,7 +455,7 @@ __global__ void __launch_bounds__(TcThreads<EPI, CONVB>::VALUE, 1)
               }
             }
             const int s = g % TC_STAGES;
-            if (!mbar_wait(&full[s], (g / TC_STAGES) & 1, abort_flag, args.err, 3)) {
+            if (!mbar_wait(CONVB ? &conv[s] : &full[s], (g / TC_STAGES) & 1, abort_flag, args.err, 3)) {
               ok = false;
               break;
             }
@@ -479,59 +487,83 @@ __global__ void __launch_bounds__(TcThreads<EPI, CONVB>::VALUE, 1)
       }
     } else if (CONVB && warp >= 2 + TcWarps<EPI>::NEPI) {
       // ---------------- B operand converters (CONVB) ----------------
-      // Warp cw builds rows cw, cw + 4, ... of the 128-row B tile for each k
-      // block: lane l takes columns 2l, 2l + 1 (one coalesced 256-byte row
-      // read per warp), x = b * c in FP32, hi = rn16(x), lo = rn16(x - hi)
-      // (split_round's rounding), both as one 32-bit word per row into the
-      // swizzled tile.  The generic-proxy stores are made visible to the
-      // tensor core's async proxy before the warp's arrival on the stage.
-      const int cw = warp - (2 + TcWarps<EPI>::NEPI);
-      const int n0 = nt_begin * BN;
-      const float* cw_scale = args.convC + (size_t)w * args.ldcc;
+      // Thread t owns the 8-column chunk cc = t % 8 of rows t / 8 + 8 i of
+      // the 128-row tile.  Per k block it reads the FP32 tile that TMA
+      // landed (two 32-column boxes, 128-byte swizzle: the chunk of 4 floats
+      // q of row r sits at r * 128 + ((q ^ r % 8) << 4)), forms x = b * c in
+      // FP32, hi = rn16(x), lo = rn16(x - hi) (split_round's rounding) and
+      // stores both 16-byte chunks into the swizzled hi/lo tile.  A warp's
+      // stores cover four whole rows and its loads two 128-byte row halves
+      // per box, so neither has bank conflicts beyond the 4 wavefronts of a
+      // 512-byte access.  The generic-proxy stores are made visible to the
+      // tensor core's async proxy before the warp arrives on conv[s].
+      const int ct = threadIdx.x - 32 * (2 + TcWarps<EPI>::NEPI);
+      const int cc = ct & 7, rg = ct >> 3;
+      constexpr int ROWS_PER_PASS = 4 * kConvWarps;  // row groups of 8 chunk threads
+      const float* cw_scale = args.convC + (size_t)w * args.ldcc + 8 * cc;
+      // Column scales of the next k block, loaded one block ahead.
+      float4 cn0 = make_float4(0.f, 0.f, 0.f, 0.f), cn1 = cn0;
+      if (8 * cc < args.K) {
+        cn0 = __ldg(reinterpret_cast<const float4*>(cw_scale));
+        cn1 = __ldg(reinterpret_cast<const float4*>(cw_scale + 4));
+      }
+      const int h = cc >> 2, q0 = 2 * (cc & 3);
       int g = 0;
       for (int kb = 0; kb < k_blocks; ++kb, ++g) {
+        const float4 c0 = cn0, c1 = cn1;
+        const int kn = (kb + 1) * TC_BK + 8 * cc;
+        if (kb + 1 < k_blocks && kn < args.K) {
+          cn0 = __ldg(reinterpret_cast<const float4*>(cw_scale + (size_t)(kb + 1) * TC_BK));
+          cn1 = __ldg(reinterpret_cast<const float4*>(cw_scale + (size_t)(kb + 1) * TC_BK + 4));
+        } else {
+          cn0 = cn1 = make_float4(0.f, 0.f, 0.f, 0.f);
+        }
         const int s = g % TC_STAGES;
-        if (g >= TC_STAGES) {
-          if (!mbar_wait(&empty[s], ((g / TC_STAGES) - 1) & 1, abort_flag, args.err, 7)) break;
-        }
-        const int k = kb * TC_BK + 2 * lane;
-        const bool kin = k < args.K;  // K even: k + 1 < K as well
-        const float2 c = kin ? *reinterpret_cast<const float2*>(cw_scale + k) : make_float2(0.f, 0.f);
-        constexpr int RPW = BN / kConvWarps;  // rows per converter warp
-        float2 v[RPW];
+        if (!mbar_wait(&full[s], (g / TC_STAGES) & 1, abort_flag, args.err, 7)) break;
+        uint8_t* st = smem + s * L::STAGE_BYTES;
+        const uint32_t bh = smem_u32(st + 2 * L::A_BYTES), bl = bh + L::B_BYTES;
+        const uint32_t f32 = bh + 2 * L::B_BYTES + h * (L::F32_BYTES / 2);
+#pragma unroll 4
+        for (int i = 0; i < BN / ROWS_PER_PASS; ++i) {
+          const int r = rg + ROWS_PER_PASS * i;
+          const uint32_t rb = f32 + r * 128;
+          float4 v0, v1;
+          asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];\n"
+                       : "=f"(v0.x), "=f"(v0.y), "=f"(v0.z), "=f"(v0.w)
+                       : "r"(rb + ((q0 ^ (r & 7)) << 4)));
+          asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];\n"
+                       : "=f"(v1.x), "=f"(v1.y), "=f"(v1.z), "=f"(v1.w)
+                       : "r"(rb + (((q0 + 1) ^ (r & 7)) << 4)));
+          const float x[8] = {v0.x * c0.x, v0.y * c0.y, v0.z * c0.z, v0.w * c0.w,
+                              v1.x * c1.x, v1.y * c1.y, v1.z * c1.z, v1.w * c1.w};
+          uint32_t hw[4], lw[4];
 #pragma unroll
-        for (int i = 0; i < RPW; ++i) {
-          const int row = n0 + cw + kConvWarps * i;
-          v[i] = (kin && row < args.N) ? __ldg(reinterpret_cast<const float2*>(args.convB + (size_t)row * args.ldconv + k))
-                                        : make_float2(0.f, 0.f);
-        }
-        uint8_t* st = smem + s * L::STAGE_BYTES + 2 * L::A_BYTES;
-        const uint32_t bh = smem_u32(st), bl = bh + L::B_BYTES;
-#pragma unroll
-        for (int i = 0; i < RPW; ++i) {
-          const int r = cw + kConvWarps * i;
-          const float x0 = v[i].x * c.x, x1 = v[i].y * c.y;
-          uint32_t hw, lw;
-          if (args.fp16) {
-            const __half2 hh = __floats2half2_rn(x0, x1);
-            const float2 hf = __half22float2(hh);
-            const __half2 ll = __floats2half2_rn(x0 - hf.x, x1 - hf.y);
-            hw = *reinterpret_cast<const uint32_t*>(&hh);
-            lw = *reinterpret_cast<const uint32_t*>(&ll);
-          } else {
-            const __nv_bfloat162 hh = __floats2bfloat162_rn(x0, x1);
-            const float2 hf = __bfloat1622float2(hh);
-            const __nv_bfloat162 ll = __floats2bfloat162_rn(x0 - hf.x, x1 - hf.y);
-            hw = *reinterpret_cast<const uint32_t*>(&hh);
-            lw = *reinterpret_cast<const uint32_t*>(&ll);
+          for (int p = 0; p < 4; ++p) {
+            if (args.fp16) {
+              const __half2 hh = __floats2half2_rn(x[2 * p], x[2 * p + 1]);
+              const float2 hf = __half22float2(hh);
+              const __half2 ll = __floats2half2_rn(x[2 * p] - hf.x, x[2 * p + 1] - hf.y);
+              hw[p] = *reinterpret_cast<const uint32_t*>(&hh);
+              lw[p] = *reinterpret_cast<const uint32_t*>(&ll);
+            } else {
+              const __nv_bfloat162 hh = __floats2bfloat162_rn(x[2 * p], x[2 * p + 1]);
+              const float2 hf = __bfloat1622float2(hh);
+              const __nv_bfloat162 ll = __floats2bfloat162_rn(x[2 * p] - hf.x, x[2 * p + 1] - hf.y);
+              hw[p] = *reinterpret_cast<const uint32_t*>(&hh);
+              lw[p] = *reinterpret_cast<const uint32_t*>(&ll);
+            }
           }
-          const uint32_t off = sw128_offset(r, 2 * lane);
-          asm volatile("st.shared.b32 [%0], %1;\n" ::"r"(bh + off), "r"(hw) : "memory");
-          asm volatile("st.shared.b32 [%0], %1;\n" ::"r"(bl + off), "r"(lw) : "memory");
+          const uint32_t off = sw128_offset(r, 8 * cc);
+          asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};\n" ::"r"(bh + off), "r"(hw[0]), "r"(hw[1]),
+                       "r"(hw[2]), "r"(hw[3])
+                       : "memory");
+          asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};\n" ::"r"(bl + off), "r"(lw[0]), "r"(lw[1]),
+                       "r"(lw[2]), "r"(lw[3])
+                       : "memory");
         }
         asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
         __syncwarp();
-        if (lane == 0) mbar_arrive(&full[s]);
+        if (lane == 0) mbar_arrive(&conv[s]);
       }
     } else if (EPI == EPI_ROWDOT) {
       // ---------------- epilogue (warps 2..9): row dot products ----------------
@@ -748,6 +780,23 @@ static CUtensorMap make_map(const void* base, int cols, int rows, int ld, int ba
   CUresult r = encode_fn()(&m, fp16 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, rank, const_cast<void*>(base), dims, strides, box,
                            estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
                            bk == 64 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B,
+                           CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  QX_REQUIRE(r == CUDA_SUCCESS, QX_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+  return m;
+}
+
+// 2D FP32 map over a [rows][ld] array (cols valid), box 32 columns x box_rows
+// with the 128-byte swizzle (32 floats = one 128-byte row of the atom).
+static CUtensorMap make_map_f32(const float* base, int cols, int rows, int ld, int box_rows) {
+  QX_REQUIRE((reinterpret_cast<uintptr_t>(base) & 15) == 0 && (ld * 4) % 16 == 0, QX_ERR_INVALID_INPUT,
+             "tensor map base/stride not 16-byte aligned");
+  CUtensorMap m;
+  cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
+  cuuint64_t strides[1] = {(cuuint64_t)ld * 4};
+  cuuint32_t box[2] = {32, (cuuint32_t)box_rows};
+  cuuint32_t estr[2] = {1, 1};
+  CUresult r = encode_fn()(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(base), dims, strides, box, estr,
+                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
                            CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   QX_REQUIRE(r == CUDA_SUCCESS, QX_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
   return m;
@@ -1095,7 +1144,7 @@ static void check_tc_err(qx_ctx* ctx, int* d_err) { ctx->pending.push_back({d_er
 template <int BN, int EPI, bool CONVB = false>
 static void launch_tc(qx_ctx* ctx, const CUtensorMap& ah, const CUtensorMap& al, const CUtensorMap& bh,
                       const CUtensorMap& bl, const TcArgs& a, dim3 grid, cudaStream_t stream = nullptr) {
-  using L = TcSmem<BN, EPI>;
+  using L = TcSmem<BN, EPI, CONVB>;
   static PerDeviceOnce attr_once;
   attr_once(ctx->device, [&] {
     QX_CUDA(cudaFuncSetAttribute(k_tc_gemm<BN, EPI, CONVB>, cudaFuncAttributeMaxDynamicSharedMemorySize, L::TOTAL));
@@ -1276,14 +1325,13 @@ void launch_eps_tc(qx_ctx* ctx, const double* bov, int ldov, int naux, int nov, 
   a.scaleA = sa;
   a.scaleB = sb;
   a.err = d_err;
-  a.convB = bf;
-  a.ldconv = ldov;
   a.convC = cs;
   a.ldcc = ldov;
   const int tiles = ceil_div(naux, TC_BM);  // BM == BN for the symmetric product
   static_assert(BN == TC_BM, "eps tiles are square");
-  // The B maps are not read in this form (the converters build B).
-  launch_tc<BN, EPI_STORE, true>(ctx, ah, al, ah, al, a, dim3(tiles * (tiles + 1) / 2, nw));
+  // The B slot carries the FP32 map of B_ov; the converters build hi/lo.
+  const CUtensorMap bm = make_map_f32(bf, nov, naux, ldov, BN);
+  launch_tc<BN, EPI_STORE, true>(ctx, ah, al, bm, bm, a, dim3(tiles * (tiles + 1) / 2, nw));
   check_tc_err(ctx, d_err);
 }
 

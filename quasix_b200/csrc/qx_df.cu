@@ -21,9 +21,10 @@
 // order contracts the metric over nmo^2 instead of nao^2 columns.
 //
 // J^-1/2 and J^1/2 come from the scaled Denman-Beavers iteration (product
-// form, see metric_inv_sqrt: one SPD inverse by the block sweep and two DMMA
-// GEMMs per step, 5-8 steps); it equals the eigendecomposition form of the
-// reference whenever no eigenvalue of J lies below thresh_df.  That is checked with lambda_min(J) >= 1 / trace(J^-1)
+// form, see metric_inv_sqrt: one SPD inverse by the block sweep refined by a
+// Newton-Schulz step, and four DMMA GEMMs per step, 5-8 steps); it equals the
+// eigendecomposition form of the reference whenever no eigenvalue of J lies
+// below thresh_df.  That is checked with lambda_min(J) >= 1 / trace(J^-1)
 // and, when this bound is inconclusive, by power iteration on J^-1/2 (the
 // reference's clamping of such eigenvalues is not reproduced: those metrics
 // are rejected with QX_ERR_NUMERICAL).
@@ -120,6 +121,19 @@ __global__ void k_db_m(double* __restrict__ M, const double* __restrict__ Mi, in
   }
   for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
   if ((threadIdx.x & 31) == 0) atomicMax(res, (unsigned long long)__double_as_longlong(m));
+}
+
+// One Newton-Schulz step of an approximate inverse Mi of M: Mi <- 2 Mi - X
+// with X = Mi M Mi, symmetrised (each thread owns the pair (r, c), (c, r)).
+__global__ void k_ns_step(double* __restrict__ Mi, const double* __restrict__ X, int n, int ld) {
+  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < (size_t)n * n;
+       e += (size_t)gridDim.x * blockDim.x) {
+    const size_t r = e / n, c = e % n;
+    if (c > r) continue;
+    const double v = 0.5 * ((2.0 * Mi[r * ld + c] - X[r * ld + c]) + (2.0 * Mi[c * ld + r] - X[c * ld + r]));
+    Mi[r * ld + c] = v;
+    Mi[c * ld + r] = v;
+  }
 }
 
 // sum of squares (one atomic per warp into a double via bits is not
@@ -250,13 +264,24 @@ double metric_inv_sqrt(qx_ctx* ctx, const double* J, int n, int ldj, double* Jm,
   // Scratch for the products: the work buffer after small.
   double* T = small + 520 + 2 * ((size_t)n + 8) + 64;
   bool done = false;
+  double fmi0 = 0.0;  // ||J^-1||_F, from the first step
   for (int it = 0; it < 100 && !done; ++it) {
     // Mi = M^-1 (the sweep leaves M^-1 - I in place; M is SPD).
     QX_CUDA(cudaMemcpyAsync(Mi, M, nn * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
     launch_invert_wc(ctx, Mi, n, ld, nn, 1, /*guard=*/0);
     k_axpi<<<blocks, 256, 0, ctx->stream>>>(Mi, n, ld, 1.0, 1.0, Mi, ld);
     check_launch(ctx);
-    const double mu = std::pow(frob(ctx, Mi, n, ld, small, blocks) / frob(ctx, M, n, ld, small, blocks), 0.25);
+    // The block sweep applies explicit inverses of its 128-wide diagonal
+    // blocks, which costs accuracy as kappa(M) grows (at kappa 1e6 the
+    // iteration's J^-1/2 moved ~1e-10 from LAPACK's); one Newton-Schulz step
+    // Mi <- 2 Mi - Mi M Mi brings the inverse back to ~kappa u.
+    gemm(ctx, n, n, n, Mi, ld, 0, M, ld, 0, T, ld, 0, 1);   // T = Mi M
+    gemm(ctx, n, n, n, Mi, ld, 0, T, ld, 0, X, ld, 0, 1);   // X = Mi (Mi M)^T = Mi M Mi
+    k_ns_step<<<blocks, 256, 0, ctx->stream>>>(Mi, X, n, ld);
+    check_launch(ctx);
+    const double fmi = frob(ctx, Mi, n, ld, small, blocks);
+    if (it == 0) fmi0 = fmi;
+    const double mu = std::pow(fmi / frob(ctx, M, n, ld, small, blocks), 0.25);
     QX_REQUIRE(std::isfinite(mu) && mu > 0.0, QX_ERR_NUMERICAL, "Denman-Beavers iteration of the metric diverged");
     // X = (I + Mi / mu^2) / 2;  Y <- mu Y X,  Z <- mu Z X (X symmetric: its rows are its columns).
     k_axpi<<<blocks, 256, 0, ctx->stream>>>(Mi, n, ld, 0.5 / (mu * mu), 0.5, X, ld);
@@ -278,7 +303,12 @@ double metric_inv_sqrt(qx_ctx* ctx, const double* J, int n, int ldj, double* Jm,
     QX_REQUIRE(std::isfinite(r), QX_ERR_NUMERICAL, "Denman-Beavers iteration of the metric diverged");
     if (r < 1e-14) done = true;
   }
-  QX_REQUIRE(done, QX_ERR_CONVERGENCE, "Denman-Beavers iteration of the metric did not converge");
+  // A metric this ill-conditioned has eigenvalues far below any useful
+  // thresh_df: report it as such, with 1 / ||J^-1||_F (<= lambda_min).
+  QX_REQUIRE(done, QX_ERR_NUMERICAL,
+             "Denman-Beavers iteration of the metric did not converge: lambda_min(J) ~ %.3e (1 / ||J^-1||_F; "
+             "thresh_df %.1e): remove the linear dependencies of the auxiliary basis first",
+             fmi0 > 0.0 ? 1.0 / fmi0 : 0.0, thresh);
   // Symmetrised results (the products keep them symmetric only to rounding).
   k_symmetrize<<<blocks, 256, 0, ctx->stream>>>(Z, n, ld, T);
   check_launch(ctx);
