@@ -22,11 +22,16 @@
 //      unpivoted elimination lost digits to element growth that the pivot
 //      and growth checks did not see;
 //   3. re-inverts every flagged matrix from its copy by Gauss-Jordan
-//      elimination with partial (row) pivoting, in panels of PIV_NB columns
-//      (k_piv_panel: the pivoted exchanges on the panel, one CTA per matrix;
-//      k_piv_update: the rank-PIV_NB update of the other columns on DMMA
-//      tiles; k_piv_permute: undo the pivot permutation into -eps^-1, the
-//      sweep's own output convention).
+//      elimination with partial (row) pivoting, in super-panels of PIV_SB
+//      columns, each worked as panels of PIV_NB (k_piv_panel: the pivoted
+//      exchanges on a panel, one CTA per matrix; k_piv_update on the rest of
+//      the super-panel); the columns outside the super-panel then take one
+//      rank-PIV_SB update on DMMA tiles (k_piv_update with the super-panel's
+//      pivot rows as they were before it, k_piv_gather), because consecutive
+//      exchange steps compose: with C = A[:, panel](new) R^T, R the panel's
+//      old pivot rows, a pivot row of the panel becomes -C and any other row
+//      A - C, for any panel width.  k_piv_permute finally undoes the pivot
+//      permutation into -eps^-1, the sweep's own output convention.
 // A zero or non-finite pivot in step 3 leaves the matrix flagged singular
 // (Wc = 0, the reference's identity fallback after a failed LU).
 #include <algorithm>
@@ -40,10 +45,14 @@ namespace qx {
 namespace {
 
 constexpr int PIV_NB = 16;
+// Super-panel width: one DMMA column tile, so the rank-PIV_SB update skips
+// exactly the super-panel's own tile.
+constexpr int PIV_SB = 64;
 // Rows of a panel held in shared memory ([n][PIV_NB] doubles plus n row states).
 constexpr int kPivSmemRows = 1700;
 constexpr size_t kPivSmemBytes = (size_t)kPivSmemRows * (PIV_NB * sizeof(double) + sizeof(int)) + 1024;
 using PivTile = F64Tile<64, 64, 2, 2, 3>;
+static_assert(PivTile::BN == PIV_SB && PIV_SB % PIV_NB == 0, "a super-panel is one column tile of whole panels");
 
 // Block-wide argmax of (v, r): largest v, ties to the smallest r (every
 // thread calls it; the result is returned to all threads).
@@ -257,27 +266,139 @@ __global__ void __launch_bounds__(512) k_piv_panel(const GuardMat* __restrict__ 
     }
     for (int r = threadIdx.x; r < n; r += blockDim.x) gstate[r] = state[r];
   }
-  // rbuf[j][b] = A[piv[k0 + b]][j] for columns outside the panel (A's columns
-  // outside the panel are untouched so far).
-  for (int b = warp; b < kb; b += nwarp) {
-    const double* src = g.bk + (size_t)piv[k0 + b] * g.ldn;
-    for (int jj = lane; jj < n; jj += 32)
-      g.rbuf[(size_t)jj * PIV_NB + b] = (jj >= k0 && jj < k0 + kb) ? 0.0 : src[jj];
+}
+
+// k_piv_panel with the panel in registers, for n <= 512 RPT: thread t holds
+// rows t + 512 i (i < RPT) across all PIV_NB columns, so a pivot step is one
+// block argmax, the pivot row published through shared memory and the
+// exchange applied in registers (three block barriers a step, no
+// shared-memory traffic per row).  The arithmetic is k_piv_panel's, operation
+// for operation.
+template <int RPT>
+__global__ void __launch_bounds__(512) k_piv_panel_reg(const GuardMat* __restrict__ tab, int k0) {
+  const GuardMat g = tab[blockIdx.x];
+  const int n = g.n;
+  if (k0 >= n || *g.status != 0) return;
+  const int kb = min(PIV_NB, n - k0);
+  int* gstate = g.ints;
+  int* piv = g.ints + n;
+  __shared__ double prow[PIV_NB];
+  __shared__ double sv[32];
+  __shared__ int sr[32];
+  double v[RPT][PIV_NB];
+  bool freer[RPT], mine[RPT];
+#pragma unroll
+  for (int i = 0; i < RPT; ++i) {
+    const int r = threadIdx.x + 512 * i;
+    const bool live = r < n;
+    freer[i] = live && gstate[r] < 0;
+    mine[i] = false;
+    const double* src = g.bk + (size_t)(live ? r : 0) * g.ldn + k0;
+#pragma unroll
+    for (int c = 0; c < PIV_NB; ++c) v[i][c] = (live && c < kb) ? src[c] : 0.0;
+  }
+  double best = -1.0;
+  int bi = INT_MAX;
+#pragma unroll
+  for (int i = 0; i < RPT; ++i) {
+    const int r = threadIdx.x + 512 * i;
+    const double a = fabs(v[i][0]);
+    if (freer[i] && (a > best || (a == best && r < bi))) {
+      best = a;
+      bi = r;
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < PIV_NB; ++j) {
+    if (j >= kb) break;  // uniform
+    block_argmax(best, bi, sv, sr);
+    const int p = bi;
+#pragma unroll
+    for (int i = 0; i < RPT; ++i)
+      if (threadIdx.x + 512 * i == p) {
+#pragma unroll
+        for (int c = 0; c < PIV_NB; ++c) prow[c] = v[i][c];
+      }
+    __syncthreads();
+    const double d = (p == INT_MAX) ? 0.0 : prow[j];
+    if (!(fabs(d) > 0.0) || !isfinite(d)) {  // uniform
+      if (threadIdx.x == 0) *g.status = 1;
+      return;
+    }
+    if (threadIdx.x == 0) piv[k0 + j] = p;
+    const double inv = 1.0 / d;
+    double pr[PIV_NB];
+#pragma unroll
+    for (int c = 0; c < PIV_NB; ++c) pr[c] = prow[c];
+    best = -1.0;
+    bi = INT_MAX;
+#pragma unroll
+    for (int i = 0; i < RPT; ++i) {
+      const int r = threadIdx.x + 512 * i;
+      if (r == p) {
+#pragma unroll
+        for (int c = 0; c < PIV_NB; ++c) v[i][c] = (c == j) ? inv : -pr[c] * inv;
+        freer[i] = false;
+        mine[i] = true;
+      } else {
+        const double t = v[i][j] * inv;
+#pragma unroll
+        for (int c = 0; c < PIV_NB; ++c) v[i][c] = (c == j) ? t : v[i][c] - t * pr[c];
+      }
+      if (j + 1 < PIV_NB) {
+        const double a = fabs(v[i][(j + 1) % PIV_NB]);
+        if (freer[i] && (a > best || (a == best && r < bi))) {
+          best = a;
+          bi = r;
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < RPT; ++i) {
+    const int r = threadIdx.x + 512 * i;
+    if (r >= n) continue;
+    double* dst = g.bk + (size_t)r * g.ldn + k0;
+#pragma unroll
+    for (int c = 0; c < PIV_NB; ++c)
+      if (c < kb) dst[c] = v[i][c];
+    if (mine[i]) gstate[r] = k0;
   }
 }
 
-// Columns outside the panel: with C = A[:, panel] (new) rbuf^T,
-//   A[r][j] = -C[r][j]         for the panel's pivot rows r,
-//   A[r][j] -= C[r][j]         otherwise.
-// grid (tiles, tiles, count).
-__global__ void __launch_bounds__(PivTile::THREADS) k_piv_update(const GuardMat* __restrict__ tab, int k0) {
+// rbuf[c][b] = A[piv[k0 + b]][c] (row stride PIV_SB) for the columns c in
+// [c_lo, min(c_hi, n)), zero inside [k0, k0 + kb): the old pivot rows of a
+// panel (kbmax = PIV_NB) or of a super-panel (kbmax = PIV_SB), read before
+// the update that consumes them.  One warp per pivot row.  grid (count, y).
+__global__ void k_piv_gather(const GuardMat* __restrict__ tab, int k0, int kbmax, int c_lo, int c_hi) {
+  const GuardMat g = tab[blockIdx.x];
+  const int n = g.n;
+  if (k0 >= n || *g.status != 0) return;
+  const int kb = min(kbmax, n - k0), lane = threadIdx.x & 31;
+  const int* piv = g.ints + n;
+  const int ch = min(c_hi, n);
+  for (int b = blockIdx.y * (blockDim.x >> 5) + (threadIdx.x >> 5); b < kb; b += gridDim.y * (blockDim.x >> 5)) {
+    const double* src = g.bk + (size_t)piv[k0 + b] * g.ldn;
+    for (int c = c_lo + lane; c < ch; c += 32)
+      g.rbuf[(size_t)c * PIV_SB + b] = (c >= k0 && c < k0 + kb) ? 0.0 : src[c];
+  }
+}
+
+// Columns c in [c_lo, min(c_hi, n)) outside the panel [k0, k0 + kb),
+// kb = min(kbmax, n - k0): with C = A[:, panel] (new) rbuf^T,
+//   A[r][c] = -C[r][c]         for the panel's pivot rows r (state in [pr_lo, pr_hi)),
+//   A[r][c] -= C[r][c]         otherwise.
+// grid (column tiles of [c_lo, c_hi), row tiles, count).
+__global__ void __launch_bounds__(PivTile::THREADS)
+    k_piv_update(const GuardMat* __restrict__ tab, int k0, int kbmax, int c_lo, int c_hi, int pr_lo, int pr_hi) {
   using T = PivTile;
   const GuardMat g = tab[blockIdx.z];
   const int n = g.n;
   if (k0 >= n || *g.status != 0) return;
-  const int kb = min(PIV_NB, n - k0);
-  const int m0 = blockIdx.y * T::BM, n0 = blockIdx.x * T::BN;
-  if (m0 >= n || n0 >= n) return;
+  const int kb = min(kbmax, n - k0);
+  const int ch = min(c_hi, n);
+  const int m0 = blockIdx.y * T::BM, n0 = c_lo + blockIdx.x * T::BN;
+  if (m0 >= n || n0 >= ch) return;
   if (n0 >= k0 && n0 + T::BN <= k0 + kb) return;
   extern __shared__ double smem[];
   double acc[T::MI][T::NJ][2];
@@ -286,20 +407,20 @@ __global__ void __launch_bounds__(PivTile::THREADS) k_piv_update(const GuardMat*
 #pragma unroll
     for (int j = 0; j < T::NJ; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
   const size_t ld = g.ldn;
-  f64_mainloop<T>(acc, smem, g.bk + (size_t)m0 * ld + k0, (int)ld, n - m0, g.rbuf + (size_t)n0 * PIV_NB, PIV_NB,
-                  n - n0, nullptr, kb);
+  f64_mainloop<T>(acc, smem, g.bk + (size_t)m0 * ld + k0, (int)ld, n - m0, g.rbuf + (size_t)n0 * PIV_SB, PIV_SB,
+                  ch - n0, nullptr, kb);
   const int* state = g.ints;
 #pragma unroll
   for (int i = 0; i < T::MI; ++i) {
     const int r = m0 + f64_row<T>(i);
     if (r >= n) continue;
-    const bool prow = state[r] == k0;
+    const bool prow = state[r] >= pr_lo && state[r] < pr_hi;
 #pragma unroll
     for (int j = 0; j < T::NJ; ++j)
 #pragma unroll
       for (int e = 0; e < 2; ++e) {
         const int c = n0 + f64_col<T>(j, e);
-        if (c >= n || (c >= k0 && c < k0 + kb)) continue;
+        if (c >= ch || (c >= k0 && c < k0 + kb)) continue;
         double* a = g.bk + (size_t)r * ld + c;
         *a = prow ? -acc[i][j][e] : *a - acc[i][j][e];
       }
@@ -332,7 +453,7 @@ inline size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
 
 size_t guard_bytes(int n, int ldn, int count) {
   const size_t per = align256((size_t)n * ldn * sizeof(double)) + align256((size_t)3 * n * sizeof(int)) +
-                     align256((size_t)n * PIV_NB * sizeof(double));
+                     align256((size_t)n * PIV_SB * sizeof(double));
   return per * count + align256(count * sizeof(GuardMat)) + 4 * align256(count * sizeof(unsigned long long)) + 256;
 }
 
@@ -340,7 +461,7 @@ void guard_layout(GuardSet& gs, void* mem, size_t bytes) {
   size_t need = align256(gs.mats.size() * sizeof(GuardMat)) + 4 * align256(gs.nall * sizeof(unsigned long long));
   for (const GuardMat& g : gs.mats)
     need += align256((size_t)g.n * g.ldn * sizeof(double)) + align256((size_t)3 * g.n * sizeof(int)) +
-            align256((size_t)g.n * PIV_NB * sizeof(double));
+            align256((size_t)g.n * PIV_SB * sizeof(double));
   QX_REQUIRE(need <= bytes, QX_ERR_INVALID_INPUT, "guarded inversion needs %zu bytes of workspace, have %zu", need,
              bytes);
   char* p = static_cast<char*>(mem);
@@ -360,7 +481,7 @@ void guard_layout(GuardSet& gs, void* mem, size_t bytes) {
     g.ints = reinterpret_cast<int*>(p);
     p += align256((size_t)3 * g.n * sizeof(int));
     g.rbuf = reinterpret_cast<double*>(p);
-    p += align256((size_t)g.n * PIV_NB * sizeof(double));
+    p += align256((size_t)g.n * PIV_SB * sizeof(double));
   }
 }
 
@@ -438,14 +559,32 @@ int guard_end(qx_ctx* ctx, GuardSet& gs) {
   const int tiles = ceil_div(nmax, PivTile::BM);
   const bool smem_panel = nmax <= kPivSmemRows;
   const size_t panel_smem = (size_t)nmax * (PIV_NB * sizeof(double) + sizeof(int));
-  for (int k0 = 0; k0 < nmax; k0 += PIV_NB) {
-    if (smem_panel)
-      k_piv_panel<true><<<F, 512, panel_smem, ctx->stream>>>(gs.d_tab, k0);
-    else
-      k_piv_panel<false><<<F, 512, 0, ctx->stream>>>(gs.d_tab, k0);
-    check_launch(ctx);
-    k_piv_update<<<dim3(tiles, tiles, F), PivTile::THREADS, PivTile::SMEM, ctx->stream>>>(gs.d_tab, k0);
-    check_launch(ctx);
+  for (int ks = 0; ks < nmax; ks += PIV_SB) {
+    for (int k0 = ks; k0 < std::min(ks + PIV_SB, nmax); k0 += PIV_NB) {
+      if (nmax <= 512)
+        k_piv_panel_reg<1><<<F, 512, 0, ctx->stream>>>(gs.d_tab, k0);
+      else if (nmax <= 1024)
+        k_piv_panel_reg<2><<<F, 512, 0, ctx->stream>>>(gs.d_tab, k0);
+      else if (smem_panel)
+        k_piv_panel<true><<<F, 512, panel_smem, ctx->stream>>>(gs.d_tab, k0);
+      else
+        k_piv_panel<false><<<F, 512, 0, ctx->stream>>>(gs.d_tab, k0);
+      check_launch(ctx);
+      // The rest of the super-panel (one column tile).
+      k_piv_gather<<<dim3(F, 2), 256, 0, ctx->stream>>>(gs.d_tab, k0, PIV_NB, ks, ks + PIV_SB);
+      check_launch(ctx);
+      k_piv_update<<<dim3(1, tiles, F), PivTile::THREADS, PivTile::SMEM, ctx->stream>>>(gs.d_tab, k0, PIV_NB, ks,
+                                                                                        ks + PIV_SB, k0, k0 + 1);
+      check_launch(ctx);
+    }
+    // Every column outside the super-panel: one rank-PIV_SB update.
+    if (ks + PIV_SB < nmax || ks > 0) {
+      k_piv_gather<<<dim3(F, 8), 256, 0, ctx->stream>>>(gs.d_tab, ks, PIV_SB, 0, nmax);
+      check_launch(ctx);
+      k_piv_update<<<dim3(tiles, tiles, F), PivTile::THREADS, PivTile::SMEM, ctx->stream>>>(
+          gs.d_tab, ks, PIV_SB, 0, nmax, ks, ks + PIV_SB);
+      check_launch(ctx);
+    }
   }
   k_piv_inverse_perm<<<F, 256, 0, ctx->stream>>>(gs.d_tab);
   check_launch(ctx);
