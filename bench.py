@@ -483,7 +483,7 @@ def bse_grad_fd_check(q, s, nocc, npoints):
             return float(q.bse_lowest_root(ev, lv, nocc, tol=1e-10))
 
     rng = np.random.default_rng(11)
-    an, fd = [], []
+    an, fd, where = [], [], []
     # Coordinates with gradients within 1e-2 of the largest (the others are
     # below the FD resolution of a 1e-10-converged root).
     gmag = ge.abs().cpu().numpy()
@@ -493,6 +493,7 @@ def bse_grad_fd_check(q, s, nocc, npoints):
         d[p] = 1e-5
         fd.append((f(e + d, lpq) - f(e - d, lpq)) / 2e-5)
         an.append(float(ge[p]))
+        where.append(f"e[{int(p)}]")
     mag = gl.abs()
     cand = torch.nonzero(mag > 1e-2 * mag.max()).cpu().numpy()
     for k in rng.choice(len(cand), npoints - npoints // 2, replace=False):
@@ -505,8 +506,10 @@ def bse_grad_fd_check(q, s, nocc, npoints):
         # The symmetric step moves both entries: its derivative is the sum of
         # the two gradient entries (the forward reads one triangle of some blocks).
         an.append(float(gl[P, a, b]) + (float(gl[P, b, a]) if a != b else 0.0))
+        where.append(f"lpq[{P},{a},{b}]")
     an, fd = np.array(an), np.array(fd)
     return {"points": npoints, "max_rel_err": float(np.abs(an - fd).max() / np.abs(fd).max()),
+            "coordinates": where, "analytic": an.tolist(), "central_difference": fd.tolist(),
             "s_forward_and_backward_fp64": t_fwd_bwd,
             "note": "bse_lowest_root (torch.autograd.Function) vs FP64 central differences of the same forward"}
 

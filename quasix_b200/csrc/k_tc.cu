@@ -196,13 +196,16 @@ template <int BN, int EPI, bool CONVB = false>
 struct TcSmem {
   static constexpr int A_BYTES = TC_BM * TcPipe<EPI>::BK * 2;
   static constexpr int B_BYTES = BN * TcPipe<EPI>::BK * 2;
-  // CONVB: the FP32 B tile as TMA lands it, two 32-column boxes with the
-  // 128-byte swizzle, read by the converter warps.
+  static constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;
+  // CONVB: a ring of F32_STAGES slots for the FP32 B tile as TMA lands it
+  // (two 32-column boxes with the 128-byte swizzle), read by the converter
+  // warps; it runs F32_STAGES k-blocks ahead of the converters.
+  static constexpr int F32_STAGES = 3;
   static constexpr int F32_BYTES = CONVB ? BN * TcPipe<EPI>::BK * 4 : 0;
-  static constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES + F32_BYTES;
-  static constexpr int BAR_OFF = TcPipe<EPI>::STAGES * STAGE_BYTES;
+  static constexpr int F32_OFF = TcPipe<EPI>::STAGES * STAGE_BYTES;
+  static constexpr int BAR_OFF = F32_OFF + (CONVB ? F32_STAGES * F32_BYTES : 0);
   static constexpr int RED_OFF = BAR_OFF + 256;  // ROWDOT: partial row sums [2][128] doubles + 2 flags
-  static constexpr int TOTAL = RED_OFF + 2048 + 64 + 1024;  // + alignment slack
+  static constexpr int TOTAL = RED_OFF + (EPI == EPI_ROWDOT ? 2048 + 64 : 0) + 1024;  // + alignment slack
 };
 
 struct TcArgs {
@@ -293,7 +296,9 @@ __global__ void __launch_bounds__(TcThreads<EPI, CONVB>::VALUE, 1)
   uint64_t* acc_empty = acc_full + 2;       // [2]
   uint64_t* drain = acc_empty + 2;          // all issued MMAs complete
   uint64_t* conv = drain + 1;               // CONVB: [TC_STAGES] converted B tile ready
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(conv + TC_STAGES);
+  uint64_t* f32_full = conv + TC_STAGES;    // CONVB: [F32_STAGES] FP32 tile landed
+  uint64_t* f32_empty = f32_full + L::F32_STAGES;  // CONVB: [F32_STAGES] FP32 slot read by every converter warp
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(f32_empty + L::F32_STAGES);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -368,6 +373,10 @@ __global__ void __launch_bounds__(TcThreads<EPI, CONVB>::VALUE, 1)
       // CONVB: one arrival per converter warp once the hi/lo B tile is written.
       if (CONVB) mbar_init(&conv[s], kConvWarps);
     }
+    for (int s = 0; s < (CONVB ? L::F32_STAGES : 0); ++s) {
+      mbar_init(&f32_full[s], 1);
+      mbar_init(&f32_empty[s], kConvWarps);
+    }
     for (int b = 0; b < 2; ++b) {
       mbar_init(&acc_full[b], 1);
       mbar_init(&acc_empty[b], TcWarps<EPI>::NEPI);  // one arrival per epilogue warp
@@ -401,7 +410,7 @@ __global__ void __launch_bounds__(TcThreads<EPI, CONVB>::VALUE, 1)
               if (!mbar_wait(&empty[s], ((g / TC_STAGES) - 1) & 1, abort_flag, args.err, 1)) goto producer_done;
             }
             uint8_t* st = smem + s * L::STAGE_BYTES;
-            mbar_expect_tx(&full[s], CONVB ? 2 * L::A_BYTES + L::F32_BYTES : L::STAGE_BYTES);
+            mbar_expect_tx(&full[s], CONVB ? 2 * L::A_BYTES : L::STAGE_BYTES);
             const int k0 = kb * TC_BK;
             if (args.a_batched) {
               tma_load_3d(st, &mapAh, &full[s], k0, m0, w);
@@ -410,11 +419,7 @@ __global__ void __launch_bounds__(TcThreads<EPI, CONVB>::VALUE, 1)
               tma_load_2d(st, &mapAh, &full[s], k0, row_off + m0);
               tma_load_2d(st + L::A_BYTES, &mapAl, &full[s], k0, row_off + m0);
             }
-            if (CONVB) {
-              uint8_t* f32 = st + 2 * L::A_BYTES + 2 * L::B_BYTES;
-              tma_load_2d(f32, &mapBh, &full[s], k0, n0);
-              tma_load_2d(f32 + L::F32_BYTES / 2, &mapBh, &full[s], k0 + TC_BK / 2, n0);
-            } else {
+            if (!CONVB) {
               tma_load_3d(st + 2 * L::A_BYTES, &mapBh, &full[s], k0, row_off + n0, w);
               tma_load_3d(st + 2 * L::A_BYTES + L::B_BYTES, &mapBl, &full[s], k0, row_off + n0, w);
             }
@@ -455,7 +460,8 @@ __global__ void __launch_bounds__(TcThreads<EPI, CONVB>::VALUE, 1)
               }
             }
             const int s = g % TC_STAGES;
-            if (!mbar_wait(CONVB ? &conv[s] : &full[s], (g / TC_STAGES) & 1, abort_flag, args.err, 3)) {
+            if (!mbar_wait(&full[s], (g / TC_STAGES) & 1, abort_flag, args.err, 3) ||
+                (CONVB && !mbar_wait(&conv[s], (g / TC_STAGES) & 1, abort_flag, args.err, 8))) {
               ok = false;
               break;
             }
@@ -508,8 +514,25 @@ __global__ void __launch_bounds__(TcThreads<EPI, CONVB>::VALUE, 1)
         cn1 = __ldg(reinterpret_cast<const float4*>(cw_scale + 4));
       }
       const int h = cc >> 2, q0 = 2 * (cc & 3);
-      int g = 0;
-      for (int kb = 0; kb < k_blocks; ++kb, ++g) {
+      const int n0 = nt_begin * BN;
+      constexpr int FS = L::F32_STAGES;
+      // Converter thread 0 keeps the FP32 ring FS blocks ahead.
+      auto issue_f32 = [&](int kb) {
+        const int f = kb % FS;
+        uint8_t* dst = smem + L::F32_OFF + f * L::F32_BYTES;
+        mbar_expect_tx(&f32_full[f], L::F32_BYTES);
+        tma_load_2d(dst, &mapBh, &f32_full[f], kb * TC_BK, n0);
+        tma_load_2d(dst + L::F32_BYTES / 2, &mapBh, &f32_full[f], kb * TC_BK + TC_BK / 2, n0);
+      };
+      // issued: FP32 blocks requested so far (kept identically by the lanes
+      // of converter warp 0; lane 0 issues).  Every exit from the loop below
+      // is warp-uniform.
+      const bool feeder = ct < 32;
+      int issued = 0;
+      for (; issued < FS && issued < k_blocks; ++issued)
+        if (ct == 0) issue_f32(issued);
+      int kb = 0;
+      for (; kb < k_blocks; ++kb) {
         const float4 c0 = cn0, c1 = cn1;
         const int kn = (kb + 1) * TC_BK + 8 * cc;
         if (kb + 1 < k_blocks && kn < args.K) {
@@ -518,11 +541,15 @@ __global__ void __launch_bounds__(TcThreads<EPI, CONVB>::VALUE, 1)
         } else {
           cn0 = cn1 = make_float4(0.f, 0.f, 0.f, 0.f);
         }
-        const int s = g % TC_STAGES;
-        if (!mbar_wait(&full[s], (g / TC_STAGES) & 1, abort_flag, args.err, 7)) break;
+        const int s = kb % TC_STAGES, f = kb % FS;
+        // The hi/lo stage must be released by the MMAs of its previous use,
+        // and the FP32 tile of this block must have landed.
+        bool ok = kb < TC_STAGES || mbar_wait(&empty[s], ((kb / TC_STAGES) - 1) & 1, abort_flag, args.err, 7);
+        ok = ok && mbar_wait(&f32_full[f], (kb / FS) & 1, abort_flag, args.err, 9);
+        if (__any_sync(0xffffffffu, !ok)) break;
         uint8_t* st = smem + s * L::STAGE_BYTES;
         const uint32_t bh = smem_u32(st + 2 * L::A_BYTES), bl = bh + L::B_BYTES;
-        const uint32_t f32 = bh + 2 * L::B_BYTES + h * (L::F32_BYTES / 2);
+        const uint32_t f32 = smem_u32(smem + L::F32_OFF + f * L::F32_BYTES) + h * (L::F32_BYTES / 2);
 #pragma unroll 4
         for (int i = 0; i < BN / ROWS_PER_PASS; ++i) {
           const int r = rg + ROWS_PER_PASS * i;
@@ -563,7 +590,27 @@ __global__ void __launch_bounds__(TcThreads<EPI, CONVB>::VALUE, 1)
         }
         asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
         __syncwarp();
-        if (lane == 0) mbar_arrive(&conv[s]);
+        if (lane == 0) {
+          mbar_arrive(&conv[s]);
+          mbar_arrive(&f32_empty[f]);
+        }
+        // Refill slot f once every converter warp has read it.
+        if (feeder && issued < k_blocks) {
+          bool rok = true;
+          if (ct == 0) {
+            rok = mbar_wait(&f32_empty[f], (kb / FS) & 1, abort_flag, args.err, 11);
+            if (rok) issue_f32(issued);
+          }
+          if (__any_sync(0xffffffffu, !rok)) break;
+          ++issued;
+        }
+      }
+      if (kb < k_blocks && ct == 0) {
+        // Aborted: let the FP32 copies still in flight land before the CTA exits.
+        for (int q = kb; q < issued; ++q) {
+          volatile int no_abort = 0;
+          mbar_wait(&f32_full[q % FS], (q / FS) & 1, &no_abort, args.err, 10);
+        }
       }
     } else if (EPI == EPI_ROWDOT) {
       // ---------------- epilogue (warps 2..9): row dot products ----------------

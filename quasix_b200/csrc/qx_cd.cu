@@ -80,6 +80,34 @@ __global__ void k_cd_solve_rows(const double* __restrict__ wc, int ldn, size_t s
   if (lane == 0) x[(size_t)r * ld + P] = br[P] + s;
 }
 
+// t[r][k] *= chi[r][k] over rc rows of n columns (row stride ld).
+__global__ void k_cd_scale_rows(double* __restrict__ t, const double* __restrict__ chi, int rc, int n, int ld) {
+  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < (size_t)rc * n;
+       e += (size_t)gridDim.x * blockDim.x) {
+    const size_t r = e / n, k = e % n;
+    t[r * ld + k] *= chi[r * ld + k];
+  }
+}
+
+// y <- b - x - y (the residual b - eps x with y = B (chi' B^T x)), rc rows of n.
+__global__ void k_cd_residual(const double* __restrict__ b, const double* __restrict__ x, double* __restrict__ y,
+                              int rc, int n, int ld) {
+  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < (size_t)rc * n;
+       e += (size_t)gridDim.x * blockDim.x) {
+    const size_t i = (e / n) * ld + e % n;
+    y[i] = b[i] - x[i] - y[i];
+  }
+}
+
+// x += d, rc rows of n.
+__global__ void k_cd_add_rows(double* __restrict__ x, const double* __restrict__ d, int rc, int n, int ld) {
+  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < (size_t)rc * n;
+       e += (size_t)gridDim.x * blockDim.x) {
+    const size_t i = (e / n) * ld + e % n;
+    x[i] += d[i];
+  }
+}
+
 // val[r] = b^T Wc b = sum_P b[P] (x[P] - b[P])   (one CTA per residue, fixed order)
 __global__ void k_cd_quad_reduce(const double* __restrict__ b, const double* __restrict__ x, int n, int ld,
                                  double* __restrict__ val) {
@@ -221,13 +249,15 @@ CdResidueChunk CdEngine::residue_buffers(int R) {
   const size_t per_res = (stride + S.ldov) * sizeof(double) + (tc ? (size_t)naux * S.ldov * 4 : 0);
   const int RC = (int)std::max<size_t>(1, std::min<size_t>((size_t)std::max(R, 1), ((size_t)2 << 30) / per_res));
   DevBuf& rb = ctx->ws[WS_CD2];
-  rb.reserve((size_t)RC * (stride + 2 * ldn + S.ldov + 4) * sizeof(double) + RC * sizeof(int2) + 1024);
+  rb.reserve((size_t)RC * (stride + 4 * ldn + S.ldov + 4) * sizeof(double) + RC * sizeof(int2) + 1024);
   CdResidueChunk c;
   c.cap = RC;
   c.eps = rb.as<double>();
   c.b = c.eps + (size_t)RC * stride;
   c.x = c.b + (size_t)RC * ldn;
-  c.tm = c.x + (size_t)RC * ldn;
+  c.y = c.x + (size_t)RC * ldn;
+  c.dx = c.y + (size_t)RC * ldn;
+  c.tm = c.dx + (size_t)RC * ldn;
   c.wr = c.tm + (size_t)RC * S.ldov;
   c.val = c.wr + RC;
   c.dv = c.val + RC;
@@ -272,6 +302,52 @@ void CdEngine::residue_post(CdResidueChunk& c, int rc) {
   launch_cd_gather(ctx, d_lpq, naux, nmo, c.nm, rc, c.b, ldn);
   k_cd_solve_rows<<<dim3(ceil_div(naux, 8), rc), 256, 0, ctx->stream>>>(c.eps, ldn, stride, c.b, naux, ldn, c.x);
   check_launch(ctx);
+  // One step of iterative refinement of x against the FP64 eps(w_r) = I + B_ov
+  // diag(chi') B_ov^T, applied without forming it: near an excitation eps is
+  // dominated by one huge rank-1 term, and the slope reads the small
+  // component B_ov^T x along it, which the explicit (pivoted) inverse alone
+  // gets only to ~kappa u (the reference's LU solve is componentwise accurate
+  // there; one refinement step restores that).
+  {
+    const int blk = std::min(ceil_div(rc * std::max(nov, naux), 256), 4 * ctx->sm_count);
+    GemmNT g{};
+    g.M = rc;
+    g.N = nov;
+    g.K = naux;
+    g.A = c.x;
+    g.lda = ldn;
+    g.B = bovT;
+    g.ldb = ldn;
+    g.C = c.tm;
+    g.ldc = S.ldov;
+    g.batch = 1;
+    g.alpha = 1.0;
+    g.splitk = 0;
+    gemm_nt_f64(ctx, g);
+    k_cd_scale_rows<<<blk, 256, 0, ctx->stream>>>(c.tm, c.chi, rc, nov, S.ldov);
+    check_launch(ctx);
+    GemmNT h{};
+    h.M = rc;
+    h.N = naux;
+    h.K = nov;
+    h.A = c.tm;
+    h.lda = S.ldov;
+    h.B = S.bov;
+    h.ldb = S.ldov;
+    h.C = c.y;
+    h.ldc = ldn;
+    h.batch = 1;
+    h.alpha = 1.0;
+    h.splitk = 0;
+    gemm_nt_f64(ctx, h);
+    k_cd_residual<<<blk, 256, 0, ctx->stream>>>(c.b, c.x, c.y, rc, naux, ldn);
+    check_launch(ctx);
+    k_cd_solve_rows<<<dim3(ceil_div(naux, 8), rc), 256, 0, ctx->stream>>>(c.eps, ldn, stride, c.y, naux, ldn,
+                                                                          c.dx);
+    check_launch(ctx);
+    k_cd_add_rows<<<blk, 256, 0, ctx->stream>>>(c.x, c.dx, rc, naux, ldn);
+    check_launch(ctx);
+  }
   k_cd_quad_reduce<<<rc, 256, 0, ctx->stream>>>(c.b, c.x, naux, ldn, c.val);
   check_launch(ctx);
   GemmNT g{};

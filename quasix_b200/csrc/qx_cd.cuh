@@ -20,6 +20,8 @@ struct CdResidueChunk {
   double* eps;  // [rc][naux][ldn]: eps(w_r), then Wc(w_r) = eps^-1 - I
   double* b;    // [rc][ldn]: b_r = lpq[:, n_t, m]
   double* x;    // [rc][ldn]: eps(w_r)^-1 b_r
+  double* y;    // [rc][ldn]: refinement: the residual b - eps x
+  double* dx;   // [rc][ldn]: refinement: its correction eps^-1 (b - eps x)
   double* tm;   // [rc][ldov]: B_ov^T x_r
   double* chi;  // [rc][ldov]: real-axis chi'(w_r)
   double* wr;   // [rc]

@@ -137,7 +137,11 @@ def test_cd_residue_shift_next_to_a_transition(q, delta):
     """Sigma_LUMO at w just above e_LUMO + gap: its residue eps(w_r) has a shift
     (1 + delta) x the smallest transition, where chi' of that pair is large and
     negative, so eps is indefinite and the inversion runs guarded.  The CD
-    Sigma and its slope match the oracle (numpy LU solve per residue)."""
+    Sigma and its slope match the oracle (numpy LU solve per residue).  The
+    slope reads B^T x along the resonant pair, a component ~delta of x times a
+    chi' derivative ~1/delta^2: at delta = 1e-9 the oracle's own LU value of
+    that residue is 1e-7 (relative) from its 50-digit value, so the slope is
+    compared at 1e-6 there and at 1e-8 otherwise."""
     from quasix_b200.synth import make_system
     s = make_system(3, 9, 30, seed=21, pi_norm=2.0)
     nocc = s.nocc
@@ -151,7 +155,8 @@ def test_cd_residue_shift_next_to_a_transition(q, delta):
     r = q.cd_sigma(s.mo_energy, s.lpq, nocc, [lumo], [om], nw=nw)
     got, dgot = r["sigma_c"][0], r["dsigma_c"][0]
     assert abs(got - ref) <= 1e-9 * max(1.0, abs(ref)), (got, ref)
-    assert abs(dgot - dref) <= 1e-8 * max(1.0, abs(dref)), (dgot, dref)
+    tol = 1e-6 if delta < 1e-7 else 1e-8
+    assert abs(dgot - dref) <= tol * max(1.0, abs(dref)), (dgot, dref)
 
 
 def test_eps_certificate_with_crossed_levels(q):
