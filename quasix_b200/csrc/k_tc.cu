@@ -205,7 +205,8 @@ struct TcSmem {
   static constexpr int F32_OFF = TcPipe<EPI>::STAGES * STAGE_BYTES;
   static constexpr int BAR_OFF = F32_OFF + (CONVB ? F32_STAGES * F32_BYTES : 0);
   static constexpr int RED_OFF = BAR_OFF + 256;  // ROWDOT: partial row sums [2][128] doubles + 2 flags
-  static constexpr int TOTAL = RED_OFF + (EPI == EPI_ROWDOT ? 2048 + 64 : 0) + 1024;  // + alignment slack
+  // ROWDOT: two buffers of [2][128] doubles + 2 flags (8 doubles), alternating per item.
+  static constexpr int TOTAL = RED_OFF + (EPI == EPI_ROWDOT ? 2 * (2 * TC_BM + 8) * 8 : 0) + 1024;  // + slack
 };
 
 struct TcArgs {
@@ -307,13 +308,25 @@ __global__ void __launch_bounds__(TcThreads<EPI, CONVB>::VALUE, 1)
   int mb, w, nt_begin, nt_end;
   GMat gmat{};
   const int n_tiles = (args.N + BN - 1) / BN;
-  if (EPI == EPI_ROWDOT) {
+  // ROWDOT is persistent: CTA b takes the items b, b + gridDim.x, ... of
+  // the (pair block, frequency) sequence, ordered so that the frequencies of
+  // a group of wgroup share each pair block while it is in L2; TMEM buffers,
+  // stages and barrier phases run on across items, so the epilogue of one
+  // item overlaps the MMAs of the next.  The other forms take one item.
+  const int n_items =
+      (EPI == EPI_ROWDOT) ? (args.nbatch + args.wgroup - 1) / args.wgroup * args.m_blocks * args.wgroup : 1;
+  const int item0 = (EPI == EPI_ROWDOT) ? (int)blockIdx.x : 0;
+  const int item_step = (EPI == EPI_ROWDOT) ? (int)gridDim.x : 1;
+  auto rowdot_item = [&](int b, int& mb_, int& w_) {
     const int g = args.wgroup;
     const int per_group = args.m_blocks * g;
-    const int b = blockIdx.x;
     const int grp = b / per_group, r = b % per_group;
-    mb = r / g;
-    w = grp * g + r % g;
+    mb_ = r / g;
+    w_ = grp * g + r % g;
+  };
+  if (EPI == EPI_ROWDOT) {
+    mb = 0;
+    w = 0;
     nt_begin = 0;
     nt_end = n_tiles;
   } else {
@@ -401,6 +414,13 @@ __global__ void __launch_bounds__(TcThreads<EPI, CONVB>::VALUE, 1)
       if (lane == 0) {
         int g = 0;
         int issued = 0;
+        for (int it = item0; it < n_items; it += item_step) {
+        int mi = mb, wi = w;
+        if (EPI == EPI_ROWDOT) {
+          rowdot_item(it, mi, wi);
+          if (wi >= args.nbatch) continue;
+        }
+        const int mi0 = mi * TC_BM;
         for (int nt = nt_begin; nt < nt_end; ++nt) {
           const int n0 = nt * BN;
           const int kbe = args.tri ? min(k_blocks, (n0 + BN + TC_BK - 1) / TC_BK) : k_blocks;
@@ -413,18 +433,19 @@ __global__ void __launch_bounds__(TcThreads<EPI, CONVB>::VALUE, 1)
             mbar_expect_tx(&full[s], CONVB ? 2 * L::A_BYTES : L::STAGE_BYTES);
             const int k0 = kb * TC_BK;
             if (args.a_batched) {
-              tma_load_3d(st, &mapAh, &full[s], k0, m0, w);
-              tma_load_3d(st + L::A_BYTES, &mapAl, &full[s], k0, m0, w);
+              tma_load_3d(st, &mapAh, &full[s], k0, mi0, wi);
+              tma_load_3d(st + L::A_BYTES, &mapAl, &full[s], k0, mi0, wi);
             } else {
-              tma_load_2d(st, &mapAh, &full[s], k0, row_off + m0);
-              tma_load_2d(st + L::A_BYTES, &mapAl, &full[s], k0, row_off + m0);
+              tma_load_2d(st, &mapAh, &full[s], k0, row_off + mi0);
+              tma_load_2d(st + L::A_BYTES, &mapAl, &full[s], k0, row_off + mi0);
             }
             if (!CONVB) {
-              tma_load_3d(st + 2 * L::A_BYTES, &mapBh, &full[s], k0, row_off + n0, w);
-              tma_load_3d(st + 2 * L::A_BYTES + L::B_BYTES, &mapBl, &full[s], k0, row_off + n0, w);
+              tma_load_3d(st + 2 * L::A_BYTES, &mapBh, &full[s], k0, row_off + n0, wi);
+              tma_load_3d(st + 2 * L::A_BYTES + L::B_BYTES, &mapBl, &full[s], k0, row_off + n0, wi);
             }
             issued = g + 1;
           }
+        }
         }
       producer_done:
         if (*abort_flag) {
@@ -446,6 +467,12 @@ __global__ void __launch_bounds__(TcThreads<EPI, CONVB>::VALUE, 1)
         const uint32_t idesc = umma_idesc_f16(TC_BM, BN, args.fp16);
         int g = 0, u = 0;
         bool ok = true;
+        for (int it = item0; it < n_items && ok; it += item_step) {
+        if (EPI == EPI_ROWDOT) {
+          int mi, wi;
+          rowdot_item(it, mi, wi);
+          if (wi >= args.nbatch) continue;
+        }
         for (int nt = nt_begin; nt < nt_end && ok; ++nt) {
           const int kbe = args.tri ? min(k_blocks, (nt * BN + BN + TC_BK - 1) / TC_BK) : k_blocks;
           for (int kb = 0; kb < kbe; ++kb, ++g) {
@@ -484,6 +511,7 @@ __global__ void __launch_bounds__(TcThreads<EPI, CONVB>::VALUE, 1)
               ++u;
             }
           }
+        }
         }
         // Wait until every MMA this thread issued has completed (TMEM and the
         // stages are released only after that).
@@ -618,47 +646,65 @@ __global__ void __launch_bounds__(TcThreads<EPI, CONVB>::VALUE, 1)
       const int quarter = warp & 3;  // TMEM lane quarter this warp may access
       const int half = (warp - 2) >> 2;
       const int row = quarter * 32 + lane;
-      const int m = m0 + row;
       constexpr int HB = BN / 2;
-      double rowsum = 0.0;
-      int t = 0;
-      for (int nt = nt_begin; nt < nt_end; ++nt, ++t) {
-        const int buf = t & 1;
-        if (!mbar_wait(&acc_full[buf], (t / 2) & 1, abort_flag, args.err, 4)) break;
-        tc_fence_after();
-        const int n0 = nt * BN + half * HB;
-        const uint32_t taddr = tmem_base + ((uint32_t)(quarter * 32) << 16) + buf * BN + half * HB;
-        // The pair-row values of the next 16 columns are loaded before the
-        // TMEM load of the current ones, so the two latencies overlap.
-        const float* xrow = args.X + (size_t)(m < args.M ? m : 0) * args.ldx + n0;
-        float xn[16];
-        load_x16(xrow, n0, args.N, m < args.M, xn);
+      int t = 0, done_items = 0;
+      bool ok = true;
+      for (int it = item0; it < n_items && ok; it += item_step) {
+        int mi, wi;
+        rowdot_item(it, mi, wi);
+        if (wi >= args.nbatch) continue;
+        const int m = mi * TC_BM + row;
+        double rowsum = 0.0;
+        int tiles_done = 0;
+        for (int nt = nt_begin; nt < nt_end; ++nt, ++t) {
+          const int buf = t & 1;
+          if (!mbar_wait(&acc_full[buf], (t / 2) & 1, abort_flag, args.err, 4)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const int n0 = nt * BN + half * HB;
+          const uint32_t taddr = tmem_base + ((uint32_t)(quarter * 32) << 16) + buf * BN + half * HB;
+          // The pair-row values of the next 16 columns are loaded before the
+          // TMEM load of the current ones, so the two latencies overlap.
+          const float* xrow = args.X + (size_t)(m < args.M ? m : 0) * args.ldx + n0;
+          float xn[16];
+          load_x16(xrow, n0, args.N, m < args.M, xn);
 #pragma unroll 1
-        for (int c = 0; c < HB; c += 16) {
-          float xc[16];
+          for (int c = 0; c < HB; c += 16) {
+            float xc[16];
 #pragma unroll
-          for (int q = 0; q < 16; ++q) xc[q] = xn[q];
-          if (c + 16 < HB) load_x16(xrow + c + 16, n0 + c + 16, args.N, m < args.M, xn);
-          float v[16];
-          tmem_ld16(taddr + c, v);
+            for (int q = 0; q < 16; ++q) xc[q] = xn[q];
+            if (c + 16 < HB) load_x16(xrow + c + 16, n0 + c + 16, args.N, m < args.M, xn);
+            float v[16];
+            tmem_ld16(taddr + c, v);
 #pragma unroll
-          for (int q = 0; q < 16; q += 4)
-            rowsum += (double)v[q] * xc[q] + (double)v[q + 1] * xc[q + 1] + (double)v[q + 2] * xc[q + 2] +
-                      (double)v[q + 3] * xc[q + 3];
+            for (int q = 0; q < 16; q += 4)
+              rowsum += (double)v[q] * xc[q] + (double)v[q + 1] * xc[q + 1] + (double)v[q + 2] * xc[q + 2] +
+                        (double)v[q + 3] * xc[q + 3];
+          }
+          tc_fence_before();
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&acc_empty[buf]);
+          ++tiles_done;
         }
-        tc_fence_before();
-        __syncwarp();
-        if (lane == 0) mbar_arrive(&acc_empty[buf]);
+        // Combine the two halves (named barrier of the 8 epilogue warps; every
+        // one of them reaches it, also after an abort).  The buffer alternates
+        // between items: item i + 2 rewrites it only after the barrier of item
+        // i + 1, which every reader of item i has passed.
+        double* red = reinterpret_cast<double*>(smem + L::RED_OFF) + (done_items & 1) * (2 * TC_BM + 8);
+        int* done = reinterpret_cast<int*>(red + 2 * TC_BM);  // two flags after the sums
+        const bool full_item = tiles_done == nt_end - nt_begin;
+        red[half * TC_BM + row] = full_item ? rowsum : 0.0;
+        if (lane == 0 && quarter == 0) done[half] = full_item ? 1 : 0;
+        asm volatile("bar.sync 1, 256;\n" ::: "memory");
+        if (half == 0 && m < args.M && done[0] && done[1])
+          args.out[(size_t)wi * args.ldo + m] =
+              (red[row] + red[TC_BM + row]) * unscale_rowdot(args, wi) * (args.tri ? 2.0 : 1.0);
+        ++done_items;
+        // Both halves leave the item loop together (the flags are shared).
+        ok = done[0] && done[1];
       }
-      // Combine the two halves (named barrier of the 8 epilogue warps; every
-      // one of them reaches it, also after an abort).
-      double* red = reinterpret_cast<double*>(smem + L::RED_OFF);
-      int* done = reinterpret_cast<int*>(red + 2 * TC_BM);  // two flags after the sums
-      red[half * TC_BM + row] = (t == nt_end - nt_begin) ? rowsum : 0.0;
-      if (lane == 0 && quarter == 0) done[half] = (t == nt_end - nt_begin) ? 1 : 0;
-      asm volatile("bar.sync 1, 256;\n" ::: "memory");
-      if (half == 0 && m < args.M && done[0] && done[1])
-        args.out[(size_t)w * args.ldo + m] = (red[row] + red[TC_BM + row]) * unscale_rowdot(args, w) * (args.tri ? 2.0 : 1.0);
     } else {
       // ---------------- epilogue (warps 2..9): FP64 sum of k-block partials ----------------
       constexpr int CPW = BN * 4 / TcWarps<EPI>::NEPI;  // columns per epilogue warp
@@ -1279,7 +1325,9 @@ void launch_pair_contract_tc(qx_ctx* ctx, const TcOperand& A, const float* bpt_f
   // per shape by timing the candidates on the call's own data.
   auto launch_with = [&](int g) {
     a.wgroup = g;
-    launch_tc<BN, EPI_ROWDOT>(ctx, ah, al, bh, bl, a, dim3(ceil_div(nw, g) * a.m_blocks * g));
+    // Persistent: one CTA per SM (192 KB of stages each) over all items.
+    const int items = ceil_div(nw, g) * a.m_blocks * g;
+    launch_tc<BN, EPI_ROWDOT>(ctx, ah, al, bh, bl, a, dim3(std::min(items, ctx->sm_count)));
   };
   a.wgroup = tuned_wgroup(ctx, npair, naux, nw, launch_with);
   launch_with(a.wgroup);
