@@ -474,13 +474,13 @@ def bse_grad_fd_check(q, s, nocc, npoints):
     e = torch.tensor(s.mo_energy, dtype=torch.float64, device="cuda", requires_grad=True)
     lpq = torch.tensor(s.lpq, dtype=torch.float64, device="cuda", requires_grad=True)
     t0 = time.perf_counter()
-    om = q.bse_lowest_root(e, lpq, nocc, tol=1e-10)
+    om = q.bse_lowest_root(e, lpq, nocc, tol=1e-10, max_iter=600)
     ge, gl = torch.autograd.grad(om, (e, lpq))
     t_fwd_bwd = time.perf_counter() - t0
 
     def f(ev, lv):
         with torch.no_grad():
-            return float(q.bse_lowest_root(ev, lv, nocc, tol=1e-10))
+            return float(q.bse_lowest_root(ev, lv, nocc, tol=1e-10, max_iter=600))
 
     rng = np.random.default_rng(11)
     an, fd, where = [], [], []

@@ -175,7 +175,15 @@ def _bse_function():
             delta = (e_h[None, nocc:] - e_h[:nocc, None]).reshape(-1)
             k = BSETDAKernel(nocc, nvir, l.shape[0], delta, dia, dij, dab, w0, precision=precision,
                              device=_dev_index(dev))
-            r = k.solve_davidson_with_config(DavidsonConfig(1, max_iter, None, tol))
+            # A block of four roots (and a subspace of 80) converges the lowest
+            # one far faster than a single-root Davidson restarting every 20
+            # vectors; a root short of tol would make the gradient inexact.
+            nroots = min(4, nvir * nocc)
+            r = k.solve_davidson_with_config(DavidsonConfig(nroots, max_iter, 20 * nroots, tol))
+            if not r["converged"][0]:
+                k.close()
+                raise RuntimeError(f"ConvergenceError: the lowest BSE root did not reach tol {tol:g} in {max_iter} "
+                                   f"iterations (residual {r['residual_norms'][0]:.2e})")
             ctx.kernel = k
             ctx.x = np.ascontiguousarray(r["eigenvectors"][:, 0])
             ctx.e = e_h
