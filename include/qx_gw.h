@@ -63,6 +63,14 @@ int64_t qx_ctx_last_launches(const qx_ctx* ctx);
  * and how many of those were re-inverted with pivoting (no reference
  * counterpart).  Either pointer may be NULL. */
 qx_status qx_ctx_last_guard_stats(const qx_ctx* ctx, int64_t* guarded, int64_t* reinverted);
+/* Form of the split-precision P0 (FP16X3 / BF16X3; no reference
+ * counterpart): QX_P0_MATERIALISED writes the hi/lo split of B_ov chi'(w) s_w
+ * for every frequency (4 nw naux nov bytes) and reads it back by TMA;
+ * QX_P0_CONVERTER applies chi'(w) while the B operand is staged in shared
+ * memory, so that nothing chi-scaled goes to memory; QX_P0_AUTO (default)
+ * materialises up to 6 GiB of such operands and converts beyond. */
+enum { QX_P0_AUTO = 0, QX_P0_MATERIALISED = 1, QX_P0_CONVERTER = 2 };
+qx_status qx_ctx_set_p0_form(qx_ctx* ctx, int form);
 /* Library version string. */
 const char* qx_version(void);
 

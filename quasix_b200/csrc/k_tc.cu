@@ -171,6 +171,9 @@ struct TcPipe {
 // direct term keeps unit 1, since with unit 2 the Davidson residuals of the
 // 26 400-dimensional problem stalled above 1e-8.  A third stage measured no
 // faster.
+// Largest chi-scaled P0 operand (hi + lo of B_ov chi'_w s_w for every
+// frequency) that is materialised; larger problems use the converter form.
+constexpr size_t kP0SplitBudget = (size_t)6 << 30;
 constexpr int kP0Unit = 128 / TcPipe<EPI_STORE>::BK;
 constexpr int kBseUnit = 64 / TcPipe<EPI_STORE>::BK;
 constexpr int kUpdateUnit = 2;
@@ -1369,8 +1372,64 @@ __global__ void k_chi_cols(const double* __restrict__ chi, int nov, int ldov, co
   for (int k = threadIdx.x; k < ldov; k += blockDim.x) cs[(size_t)w * ldov + k] = k < nov ? (float)(cw[k] * s) : 0.f;
 }
 
-void launch_eps_tc(qx_ctx* ctx, const double* bov, int ldov, int naux, int nov, const double* chi, int nw,
-                   double* eps, int ldn, size_t eps_stride, int fp16, int reuse_a) {
+// P0 with the chi-scaled B operand materialised: one pass splits B_ov chi'_w
+// s_w for every frequency (k_split8_bcast, 4 nw naux ldov bytes written),
+// then the STORE GEMM reads both operands by TMA.
+static void eps_tc_split(qx_ctx* ctx, const double* bov, int ldov, int naux, int nov, const double* chi, int nw,
+                         double* eps, int ldn, size_t eps_stride, int fp16, int reuse_a) {
+  constexpr int BN = 128;
+  const size_t a_elems = (size_t)naux * ldov;
+  DevBuf& buf = ctx->ws[WS_BOV_HI];
+  const size_t need = a_elems * 2 * 2 * (1 + (size_t)nw);
+  // The A split (and its scale in split slot 7) survive from the previous
+  // call on this context only if the buffer is not reallocated now.
+  reuse_a = reuse_a && buf.bytes >= need;
+  buf.reserve(need);
+  uint8_t* p = buf.as<uint8_t>();
+  void* a_hi = p;
+  void* a_lo = p + a_elems * 2;
+  void* b_hi = p + a_elems * 4;
+  void* b_lo = p + a_elems * 4 + a_elems * 2 * nw;
+  float *sa = nullptr, *sb = nullptr;
+  if (reuse_a)
+    sa = split_scratch(ctx, 7).scale;
+  else
+    split(ctx, bov, naux, nov, ldov, 0, a_hi, a_lo, ldov, 0, 1, nullptr, 0, fp16, 7, &sa);
+  split(ctx, bov, naux, nov, ldov, 0, b_hi, b_lo, ldov, a_elems, nw, chi, ldov, fp16, 1, &sb,
+        /*the bound of bov*/ split_scratch(ctx, 7).amax_src);
+  constexpr int BK = TcPipe<EPI_STORE>::BK;
+  CUtensorMap ah = make_map(a_hi, nov, naux, ldov, 1, TC_BM, 2, fp16, BK);
+  CUtensorMap al = make_map(a_lo, nov, naux, ldov, 1, TC_BM, 2, fp16, BK);
+  CUtensorMap bh = make_map(b_hi, nov, naux, ldov, nw, BN, 3, fp16, BK);
+  CUtensorMap bl = make_map(b_lo, nov, naux, ldov, nw, BN, 3, fp16, BK);
+  int* d_err = tc_err_slot(ctx);
+  QX_CUDA(cudaMemsetAsync(d_err, 0, sizeof(int), ctx->stream));
+  TcArgs a{};
+  a.M = naux;
+  a.N = naux;
+  a.K = nov;
+  a.nbatch = nw;
+  a.m_blocks = ceil_div(naux, TC_BM);
+  a.out = eps;
+  a.ldo = ldn;
+  a.out_stride = eps_stride;
+  a.lower_tiles = 1;
+  a.add_identity = 1;
+  a.unit = kP0Unit;
+  a.fp16 = fp16;
+  a.scaleA = sa;
+  a.scaleB = sb;
+  a.err = d_err;
+  const int tiles = ceil_div(naux, TC_BM);  // BM == BN for the symmetric product
+  static_assert(BN == TC_BM, "eps tiles are square");
+  launch_tc<BN, EPI_STORE>(ctx, ah, al, bh, bl, a, dim3(tiles * (tiles + 1) / 2, nw));
+  check_tc_err(ctx, d_err);
+}
+
+// P0 with chi applied while the B operand is staged (CONVB): no chi-scaled
+// operand in memory at all.
+static void eps_tc_conv(qx_ctx* ctx, const double* bov, int ldov, int naux, int nov, const double* chi, int nw,
+                        double* eps, int ldn, size_t eps_stride, int fp16, int reuse_a) {
   constexpr int BN = 128;
   const size_t a_elems = (size_t)naux * ldov;
   // A: the hi/lo split of B_ov (one scale, slot 7), reusable across calls.
@@ -1428,6 +1487,20 @@ void launch_eps_tc(qx_ctx* ctx, const double* bov, int ldov, int naux, int nov, 
   const CUtensorMap bm = make_map_f32(bf, nov, naux, ldov, BN);
   launch_tc<BN, EPI_STORE, true>(ctx, ah, al, bm, bm, a, dim3(tiles * (tiles + 1) / 2, nw));
   check_tc_err(ctx, d_err);
+}
+
+void launch_eps_tc(qx_ctx* ctx, const double* bov, int ldov, int naux, int nov, const double* chi, int nw,
+                   double* eps, int ldn, size_t eps_stride, int fp16, int reuse_a) {
+  // The materialised form is the faster one wherever its chi-scaled operand
+  // (4 nw naux ldov bytes) fits the budget; beyond it the converter form
+  // keeps P0's memory at the A split and one FP32 copy of B_ov.
+  const size_t chi_bytes = (size_t)4 * nw * naux * ldov;
+  const bool materialise =
+      ctx->p0_form == QX_P0_MATERIALISED || (ctx->p0_form == QX_P0_AUTO && chi_bytes <= kP0SplitBudget);
+  if (materialise)
+    eps_tc_split(ctx, bov, ldov, naux, nov, chi, nw, eps, ldn, eps_stride, fp16, reuse_a);
+  else
+    eps_tc_conv(ctx, bov, ldov, naux, nov, chi, nw, eps, ldn, eps_stride, fp16, reuse_a);
 }
 
 // out[w][m][n] = sum_k A[m][k] B[w][n][k] in FP64 from split operands:

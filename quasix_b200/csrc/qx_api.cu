@@ -525,6 +525,13 @@ qx_status qx_ctx_set_stream(qx_ctx* c, void* stream) {
   return QX_OK;
 }
 
+qx_status qx_ctx_set_p0_form(qx_ctx* c, int form) {
+  if (!c || form < QX_P0_AUTO || form > QX_P0_CONVERTER) return QX_ERR_INVALID_INPUT;
+  c->p0_form = form;
+  for (qx_ctx* w : c->workers) w->p0_form = form;
+  return QX_OK;
+}
+
 qx_status qx_ctx_last_timings(const qx_ctx* c, double* a, double* b, double* d, double* e, double* f) {
   if (!c) return QX_ERR_INVALID_INPUT;
   if (a) *a = c->stage_ms[QX_ST_P0];

@@ -129,6 +129,9 @@ struct qx_ctx {
   // Guarded inversions of the last call: matrices checked, and matrices
   // re-inverted with pivoting.
   int64_t guard_matrices = 0, guard_reinverted = 0;
+  // Form of the split-precision P0 (QX_P0_AUTO / _MATERIALISED / _CONVERTER);
+  // batch workers inherit it from their parent context.
+  int p0_form = 0;
 };
 
 namespace qx {

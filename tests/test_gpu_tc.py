@@ -27,13 +27,30 @@ TOL = {"bf16x3": 5e-6, "fp16x3": 3e-6}
 TOL_SIGMA = {"bf16x3": 2e-5, "fp16x3": 1e-5}
 
 
+@pytest.fixture
+def p0_form(q):
+    """Set the split P0 form of the default context for one test."""
+    from quasix_b200 import _native
+    ctx = _native.context(0)
+
+    def use(form):
+        ctx.set_p0_form(form)
+
+    yield use
+    ctx.set_p0_form("auto")
+
+
+@pytest.mark.parametrize("form", ["materialised", "converter"])
 @pytest.mark.parametrize("prec", ["bf16x3", "fp16x3"])
 @pytest.mark.parametrize("shape", [(5, 19, 84), (12, 61, 250), (20, 130, 520)])
-def test_rho_response_tc(q, shape, prec):
+def test_rho_response_tc(q, p0_form, shape, prec, form):
+    """Both forms of the split P0: the chi-scaled operand materialised, or
+    built in shared memory by the converter warps (chi applied while staged)."""
     nocc, nvir, naux = shape
     s = make_system(nocc, nvir, naux, seed=4, pi_norm=3.0)
     lov = np.ascontiguousarray(s.lpq[:, :nocc, nocc:])
     freqs = np.array([0.0, 0.3, 5.0])
+    p0_form(form)
     got = q.get_rho_response_batch(freqs, s.mo_energy, lov, precision=prec)
     for k, f in enumerate(freqs):
         ref = O.get_rho_response(f, s.mo_energy, lov)
@@ -54,10 +71,12 @@ def test_sigma_diag_tc(q, shape, nw, orbs, prec):
     assert np.abs(got - ref).max() < TOL_SIGMA[prec] * max(1.0, np.abs(ref).max())
 
 
+@pytest.mark.parametrize("form", ["materialised", "converter"])
 @pytest.mark.parametrize("prec", ["bf16x3", "fp16x3"])
-def test_evgw_tc_within_one_mev(q, prec):
+def test_evgw_tc_within_one_mev(q, p0_form, prec, form):
     s = make_system(12, 61, 250, seed=6, pi_norm=3.0)
     kw = dict(nfreq=32, fixed_iterations=3, max_iterations=3)
+    p0_form(form)
     a = q.run_evgw_blocks(s.mo_energy, s.lpq, np.zeros(s.nmo), s.nocc, precision=prec, **kw)
     b = q.run_evgw_blocks(s.mo_energy, s.lpq, np.zeros(s.nmo), s.nocc, precision="fp64", **kw)
     assert np.abs(a["qp_energies"] - b["qp_energies"]).max() * HA_MEV < 1.0
