@@ -53,6 +53,8 @@ def parse():
     p.add_argument("--no-bse", action="store_true")
     p.add_argument("--batch-workers", type=int, default=0)
     p.add_argument("--bse-fd-points", type=int, default=4)
+    p.add_argument("--p0-form", choices=["auto", "materialised", "converter"], default="auto",
+                   help="form of the split P0 (chi-scaled operand materialised, or built while staged)")
     return p.parse_args()
 
 
@@ -580,6 +582,7 @@ def main():
     # the second evGW iteration and the loop turns chaotic.)
     vxc = q.compute_exchange_diag(lpq_d, sysm.nocc, device=dev)
     ctx = N.context(dev)
+    ctx.set_p0_form(args.p0_form)
     have_tc = True
     prec_main = args.precision or "fp16x3"
 
@@ -713,7 +716,7 @@ def main():
             "data": "synthetic",
             "config": {"workload": WORKLOAD, "nocc": NOCC, "nvirt": NVIR, "naux": NAUX, "nw": NW, "seed": SEED,
                        "orbitals": "all", "qp": "linearized", "vxc": "diag(Sigma_x) (HF reference)",
-                       "precision": prec_main,
+                       "precision": prec_main, "p0_form": args.p0_form,
                        "parallelism": f"replicas{world}" if world > 1 else "single",
                        "l2": "inputs larger than L2 (lpq 720 MB, pair tensor 361 MB); no flush"},
             "fp64_gpu_iter_per_s": fp64_rate, "speedup_vs_fp64_gpu": value / fp64_rate,

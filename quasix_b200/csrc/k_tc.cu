@@ -585,13 +585,19 @@ __global__ void __launch_bounds__(TcThreads<EPI, CONVB>::VALUE, 1)
         for (int i = 0; i < BN / ROWS_PER_PASS; ++i) {
           const int r = rg + ROWS_PER_PASS * i;
           const uint32_t rb = f32 + r * 128;
-          float4 v0, v1;
+          // The eight threads of a 128-byte load phase (one row, cc = 0..7)
+          // must hit eight different 16-byte bank groups: the two box halves
+          // map to the same banks, so threads cc >= 4 load their second chunk
+          // first.
+          float4 u0, u1;
+          const int qa = q0 + h, qb = q0 + 1 - h;
           asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];\n"
-                       : "=f"(v0.x), "=f"(v0.y), "=f"(v0.z), "=f"(v0.w)
-                       : "r"(rb + ((q0 ^ (r & 7)) << 4)));
+                       : "=f"(u0.x), "=f"(u0.y), "=f"(u0.z), "=f"(u0.w)
+                       : "r"(rb + ((qa ^ (r & 7)) << 4)));
           asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];\n"
-                       : "=f"(v1.x), "=f"(v1.y), "=f"(v1.z), "=f"(v1.w)
-                       : "r"(rb + (((q0 + 1) ^ (r & 7)) << 4)));
+                       : "=f"(u1.x), "=f"(u1.y), "=f"(u1.z), "=f"(u1.w)
+                       : "r"(rb + ((qb ^ (r & 7)) << 4)));
+          const float4 v0 = h ? u1 : u0, v1 = h ? u0 : u1;
           const float x[8] = {v0.x * c0.x, v0.y * c0.y, v0.z * c0.z, v0.w * c0.w,
                               v1.x * c1.x, v1.y * c1.y, v1.z * c1.z, v1.w * c1.w};
           uint32_t hw[4], lw[4];
