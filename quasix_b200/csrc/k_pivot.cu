@@ -268,23 +268,33 @@ __global__ void __launch_bounds__(512) k_piv_panel(const GuardMat* __restrict__ 
   }
 }
 
-// k_piv_panel with the panel in registers, for n <= 512 RPT: thread t holds
-// rows t + 512 i (i < RPT) across all PIV_NB columns, so a pivot step is one
-// block argmax, the pivot row published through shared memory and the
-// exchange applied in registers (three block barriers a step, no
-// shared-memory traffic per row).  The arithmetic is k_piv_panel's, operation
-// for operation.
+// k_piv_panel with the panel in registers, for n <= 512 RPT, and the rest of
+// its super-panel updated in the same kernel.  Thread t holds rows t + 512 i
+// (i < RPT) across all PIV_NB columns.  A pivot step takes one block barrier:
+// every warp reduces its candidates by shuffles and the lane owning the
+// warp's best row publishes that row (value, index and its PIV_NB entries) in
+// the warp's slot; after the barrier every thread picks the best slot (ties
+// to the lowest row) and applies the exchange in registers.  The slots
+// alternate between steps, so a slot is rewritten only after a barrier that
+// follows every read of it.  The arithmetic is k_piv_panel's, operation for
+// operation.  Afterwards the super-panel's other columns take the panel's
+// rank-kb update (k_piv_gather + k_piv_update restricted to the super-panel,
+// in place): the old pivot rows of those columns go through shared memory.
 template <int RPT>
 __global__ void __launch_bounds__(512) k_piv_panel_reg(const GuardMat* __restrict__ tab, int k0) {
+  constexpr int NWARP = 16;
   const GuardMat g = tab[blockIdx.x];
   const int n = g.n;
   if (k0 >= n || *g.status != 0) return;
   const int kb = min(PIV_NB, n - k0);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   int* gstate = g.ints;
   int* piv = g.ints + n;
-  __shared__ double prow[PIV_NB];
-  __shared__ double sv[32];
-  __shared__ int sr[32];
+  __shared__ double slot_row[2][NWARP][PIV_NB];
+  __shared__ double slot_val[2][NWARP];
+  __shared__ int slot_idx[2][NWARP];
+  __shared__ double rb[PIV_NB][PIV_SB];
+  __shared__ int pivs[PIV_NB];
   double v[RPT][PIV_NB];
   bool freer[RPT], mine[RPT];
 #pragma unroll
@@ -297,6 +307,7 @@ __global__ void __launch_bounds__(512) k_piv_panel_reg(const GuardMat* __restric
 #pragma unroll
     for (int c = 0; c < PIV_NB; ++c) v[i][c] = (live && c < kb) ? src[c] : 0.0;
   }
+  // This thread's candidate for column 0.
   double best = -1.0;
   int bi = INT_MAX;
 #pragma unroll
@@ -311,25 +322,55 @@ __global__ void __launch_bounds__(512) k_piv_panel_reg(const GuardMat* __restric
 #pragma unroll
   for (int j = 0; j < PIV_NB; ++j) {
     if (j >= kb) break;  // uniform
-    block_argmax(best, bi, sv, sr);
-    const int p = bi;
+    const int sl = j & 1;
+    // Warp argmax, then the owner of the warp's best row publishes it.
+    double wv = best;
+    int wr = bi;
+    for (int o = 16; o > 0; o >>= 1) {
+      const double ov = __shfl_xor_sync(0xffffffffu, wv, o);
+      const int orr = __shfl_xor_sync(0xffffffffu, wr, o);
+      if (ov > wv || (ov == wv && orr < wr)) {
+        wv = ov;
+        wr = orr;
+      }
+    }
+    if (lane == 0) {
+      slot_val[sl][warp] = wv;
+      slot_idx[sl][warp] = wr;
+    }
 #pragma unroll
     for (int i = 0; i < RPT; ++i)
-      if (threadIdx.x + 512 * i == p) {
+      if (wr != INT_MAX && threadIdx.x + 512 * i == wr) {
 #pragma unroll
-        for (int c = 0; c < PIV_NB; ++c) prow[c] = v[i][c];
+        for (int c = 0; c < PIV_NB; ++c) slot_row[sl][warp][c] = v[i][c];
       }
     __syncthreads();
-    const double d = (p == INT_MAX) ? 0.0 : prow[j];
+    double gv = slot_val[sl][0];
+    int gr = slot_idx[sl][0], gw = 0;
+#pragma unroll
+    for (int k = 1; k < NWARP; ++k) {
+      const double ov = slot_val[sl][k];
+      const int orr = slot_idx[sl][k];
+      if (ov > gv || (ov == gv && orr < gr)) {
+        gv = ov;
+        gr = orr;
+        gw = k;
+      }
+    }
+    const int p = gr;
+    const double d = (p == INT_MAX) ? 0.0 : slot_row[sl][gw][j];
     if (!(fabs(d) > 0.0) || !isfinite(d)) {  // uniform
       if (threadIdx.x == 0) *g.status = 1;
       return;
     }
-    if (threadIdx.x == 0) piv[k0 + j] = p;
+    if (threadIdx.x == 0) {
+      piv[k0 + j] = p;
+      pivs[j] = p;
+    }
     const double inv = 1.0 / d;
     double pr[PIV_NB];
 #pragma unroll
-    for (int c = 0; c < PIV_NB; ++c) pr[c] = prow[c];
+    for (int c = 0; c < PIV_NB; ++c) pr[c] = slot_row[sl][gw][c];
     best = -1.0;
     bi = INT_MAX;
 #pragma unroll
@@ -354,14 +395,29 @@ __global__ void __launch_bounds__(512) k_piv_panel_reg(const GuardMat* __restric
       }
     }
   }
+  // Old pivot rows of the super-panel's other columns (zero inside the panel).
+  const int ks = (k0 / PIV_SB) * PIV_SB, ce = min(ks + PIV_SB, n);
+  __syncthreads();  // pivs complete
+  for (int e = threadIdx.x; e < PIV_NB * PIV_SB; e += blockDim.x) {
+    const int b = e / PIV_SB, cc = e % PIV_SB, c = ks + cc;
+    rb[b][cc] = (b < kb && c < ce && !(c >= k0 && c < k0 + kb)) ? g.bk[(size_t)pivs[b] * g.ldn + c] : 0.0;
+  }
+  __syncthreads();
 #pragma unroll
   for (int i = 0; i < RPT; ++i) {
     const int r = threadIdx.x + 512 * i;
     if (r >= n) continue;
-    double* dst = g.bk + (size_t)r * g.ldn + k0;
+    double* row = g.bk + (size_t)r * g.ldn;
+    for (int c = ks; c < ce; ++c) {
+      if (c >= k0 && c < k0 + kb) continue;
+      double acc = 0.0;
+#pragma unroll
+      for (int b = 0; b < PIV_NB; ++b) acc += v[i][b] * rb[b][c - ks];
+      row[c] = mine[i] ? -acc : row[c] - acc;
+    }
 #pragma unroll
     for (int c = 0; c < PIV_NB; ++c)
-      if (c < kb) dst[c] = v[i][c];
+      if (c < kb) row[k0 + c] = v[i][c];
     if (mine[i]) gstate[r] = k0;
   }
 }
@@ -561,11 +617,16 @@ int guard_end(qx_ctx* ctx, GuardSet& gs) {
   const size_t panel_smem = (size_t)nmax * (PIV_NB * sizeof(double) + sizeof(int));
   for (int ks = 0; ks < nmax; ks += PIV_SB) {
     for (int k0 = ks; k0 < std::min(ks + PIV_SB, nmax); k0 += PIV_NB) {
-      if (nmax <= 512)
-        k_piv_panel_reg<1><<<F, 512, 0, ctx->stream>>>(gs.d_tab, k0);
-      else if (nmax <= 1024)
-        k_piv_panel_reg<2><<<F, 512, 0, ctx->stream>>>(gs.d_tab, k0);
-      else if (smem_panel)
+      if (nmax <= 1024) {
+        // Panel and the rest of its super-panel in one kernel.
+        if (nmax <= 512)
+          k_piv_panel_reg<1><<<F, 512, 0, ctx->stream>>>(gs.d_tab, k0);
+        else
+          k_piv_panel_reg<2><<<F, 512, 0, ctx->stream>>>(gs.d_tab, k0);
+        check_launch(ctx);
+        continue;
+      }
+      if (smem_panel)
         k_piv_panel<true><<<F, 512, panel_smem, ctx->stream>>>(gs.d_tab, k0);
       else
         k_piv_panel<false><<<F, 512, 0, ctx->stream>>>(gs.d_tab, k0);
