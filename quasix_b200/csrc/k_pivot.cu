@@ -277,9 +277,9 @@ __global__ void __launch_bounds__(512) k_piv_panel(const GuardMat* __restrict__ 
 // to the lowest row) and applies the exchange in registers.  The slots
 // alternate between steps, so a slot is rewritten only after a barrier that
 // follows every read of it.  The arithmetic is k_piv_panel's, operation for
-// operation.  Afterwards the super-panel's other columns take the panel's
-// rank-kb update (k_piv_gather + k_piv_update restricted to the super-panel,
-// in place): the old pivot rows of those columns go through shared memory.
+// operation.  It also leaves in rbuf the old pivot rows of the super-panel's
+// other columns (k_piv_gather's job for the other panel kernels), read only
+// after the panel is written back: the panel's own columns are zero there.
 template <int RPT>
 __global__ void __launch_bounds__(512) k_piv_panel_reg(const GuardMat* __restrict__ tab, int k0) {
   constexpr int NWARP = 16;
@@ -293,7 +293,6 @@ __global__ void __launch_bounds__(512) k_piv_panel_reg(const GuardMat* __restric
   __shared__ double slot_row[2][NWARP][PIV_NB];
   __shared__ double slot_val[2][NWARP];
   __shared__ int slot_idx[2][NWARP];
-  __shared__ double rb[PIV_NB][PIV_SB];
   __shared__ int pivs[PIV_NB];
   double v[RPT][PIV_NB];
   bool freer[RPT], mine[RPT];
@@ -395,30 +394,24 @@ __global__ void __launch_bounds__(512) k_piv_panel_reg(const GuardMat* __restric
       }
     }
   }
-  // Old pivot rows of the super-panel's other columns (zero inside the panel).
-  const int ks = (k0 / PIV_SB) * PIV_SB, ce = min(ks + PIV_SB, n);
-  __syncthreads();  // pivs complete
-  for (int e = threadIdx.x; e < PIV_NB * PIV_SB; e += blockDim.x) {
-    const int b = e / PIV_SB, cc = e % PIV_SB, c = ks + cc;
-    rb[b][cc] = (b < kb && c < ce && !(c >= k0 && c < k0 + kb)) ? g.bk[(size_t)pivs[b] * g.ldn + c] : 0.0;
-  }
-  __syncthreads();
+  // Write the panel back, then the old pivot rows of the super-panel's other
+  // columns into rbuf (zero inside the panel) for k_piv_update.
 #pragma unroll
   for (int i = 0; i < RPT; ++i) {
     const int r = threadIdx.x + 512 * i;
     if (r >= n) continue;
-    double* row = g.bk + (size_t)r * g.ldn;
-    for (int c = ks; c < ce; ++c) {
-      if (c >= k0 && c < k0 + kb) continue;
-      double acc = 0.0;
-#pragma unroll
-      for (int b = 0; b < PIV_NB; ++b) acc += v[i][b] * rb[b][c - ks];
-      row[c] = mine[i] ? -acc : row[c] - acc;
-    }
+    double* row = g.bk + (size_t)r * g.ldn + k0;
 #pragma unroll
     for (int c = 0; c < PIV_NB; ++c)
-      if (c < kb) row[k0 + c] = v[i][c];
+      if (c < kb) row[c] = v[i][c];
     if (mine[i]) gstate[r] = k0;
+  }
+  const int ks = (k0 / PIV_SB) * PIV_SB, ce = min(ks + PIV_SB, n);
+  __syncthreads();  // pivs complete
+  for (int e = threadIdx.x; e < PIV_NB * PIV_SB; e += blockDim.x) {
+    const int b = e / PIV_SB, c = ks + e % PIV_SB;
+    if (b < kb && c < ce)
+      g.rbuf[(size_t)c * PIV_SB + b] = (c >= k0 && c < k0 + kb) ? 0.0 : g.bk[(size_t)pivs[b] * g.ldn + c];
   }
 }
 
@@ -618,22 +611,22 @@ int guard_end(qx_ctx* ctx, GuardSet& gs) {
   for (int ks = 0; ks < nmax; ks += PIV_SB) {
     for (int k0 = ks; k0 < std::min(ks + PIV_SB, nmax); k0 += PIV_NB) {
       if (nmax <= 1024) {
-        // Panel and the rest of its super-panel in one kernel.
+        // The panel kernel also gathers the pivot rows for the update.
         if (nmax <= 512)
           k_piv_panel_reg<1><<<F, 512, 0, ctx->stream>>>(gs.d_tab, k0);
         else
           k_piv_panel_reg<2><<<F, 512, 0, ctx->stream>>>(gs.d_tab, k0);
         check_launch(ctx);
-        continue;
+      } else {
+        if (smem_panel)
+          k_piv_panel<true><<<F, 512, panel_smem, ctx->stream>>>(gs.d_tab, k0);
+        else
+          k_piv_panel<false><<<F, 512, 0, ctx->stream>>>(gs.d_tab, k0);
+        check_launch(ctx);
+        k_piv_gather<<<dim3(F, 2), 256, 0, ctx->stream>>>(gs.d_tab, k0, PIV_NB, ks, ks + PIV_SB);
+        check_launch(ctx);
       }
-      if (smem_panel)
-        k_piv_panel<true><<<F, 512, panel_smem, ctx->stream>>>(gs.d_tab, k0);
-      else
-        k_piv_panel<false><<<F, 512, 0, ctx->stream>>>(gs.d_tab, k0);
-      check_launch(ctx);
       // The rest of the super-panel (one column tile).
-      k_piv_gather<<<dim3(F, 2), 256, 0, ctx->stream>>>(gs.d_tab, k0, PIV_NB, ks, ks + PIV_SB);
-      check_launch(ctx);
       k_piv_update<<<dim3(1, tiles, F), PivTile::THREADS, PivTile::SMEM, ctx->stream>>>(gs.d_tab, k0, PIV_NB, ks,
                                                                                         ks + PIV_SB, k0, k0 + 1);
       check_launch(ctx);

@@ -274,8 +274,9 @@ void CdEngine::residue_compute(CdResidueChunk& c, const CdResidue* list, int rc)
   // stays FP64 here, guarded unless every shift lies below the gap.
   double wmax = 0.0;
   for (int r = 0; r < rc; ++r) wmax = std::max(wmax, std::fabs(list[r].w));
-  launch_invert_wc(ctx, c.eps, naux, ldn, (size_t)naux * ldn, rc, !eps_at_least_identity(e.data(), nocc, nvir, wmax));
-  residue_post(c, rc);
+  const bool guard = !eps_at_least_identity(e.data(), nocc, nvir, wmax);
+  launch_invert_wc(ctx, c.eps, naux, ldn, (size_t)naux * ldn, rc, guard);
+  residue_post(c, rc, guard);
 }
 
 void CdEngine::residue_p0(CdResidueChunk& c, const CdResidue* list, int rc) {
@@ -297,7 +298,7 @@ void CdEngine::residue_p0(CdResidueChunk& c, const CdResidue* list, int rc) {
     launch_eps_fp64(ctx, S.bov, S.ldov, naux, nov, c.chi, rc, c.eps, ldn, stride);
 }
 
-void CdEngine::residue_post(CdResidueChunk& c, int rc) {
+void CdEngine::residue_post(CdResidueChunk& c, int rc, bool refine) {
   const size_t stride = (size_t)naux * ldn;
   launch_cd_gather(ctx, d_lpq, naux, nmo, c.nm, rc, c.b, ldn);
   k_cd_solve_rows<<<dim3(ceil_div(naux, 8), rc), 256, 0, ctx->stream>>>(c.eps, ldn, stride, c.b, naux, ldn, c.x);
@@ -307,8 +308,9 @@ void CdEngine::residue_post(CdResidueChunk& c, int rc) {
   // dominated by one huge rank-1 term, and the slope reads the small
   // component B_ov^T x along it, which the explicit (pivoted) inverse alone
   // gets only to ~kappa u (the reference's LU solve is componentwise accurate
-  // there; one refinement step restores that).
-  {
+  // there; one refinement step restores that).  A certified eps >= I (every
+  // shift below the gap) is well conditioned and needs none.
+  if (refine) {
     const int blk = std::min(ceil_div(rc * std::max(nov, naux), 256), 4 * ctx->sm_count);
     GemmNT g{};
     g.M = rc;
@@ -392,6 +394,7 @@ void CdEngine::evaluate_begin(const std::vector<int>& act, std::vector<GMat>* gr
   // The gap is min(virtual) - max(occupied): QP levels need not stay ordered.
   ev_spd = eps_at_least_identity(e.data(), nocc, nvir, wmax / 0.9);
   const int guard = !eps_at_least_identity(e.data(), nocc, nvir, wmax);
+  ev_guard = guard != 0;
   if (R == 0) return;
   ev_chunk = residue_buffers(R);
   CdResidueChunk& c = ev_chunk;
@@ -418,7 +421,7 @@ void CdEngine::evaluate_end() {
 void CdEngine::evaluate_post() {
   const int R = (int)ev_res.size();
   if (ev_grouped) {
-    residue_post(ev_chunk, R);
+    residue_post(ev_chunk, R, ev_guard);
     QX_CUDA(cudaMemcpyAsync(h_rv, ev_chunk.val, R * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     QX_CUDA(cudaMemcpyAsync(h_rd, ev_chunk.dv, R * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
   }

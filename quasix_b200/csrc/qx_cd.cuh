@@ -63,7 +63,9 @@ struct CdEngine {
   // residue_p0 (eps(w_r)), the FP64 inversion, residue_post (the rest).
   void residue_compute(CdResidueChunk& c, const CdResidue* list, int rc);
   void residue_p0(CdResidueChunk& c, const CdResidue* list, int rc);
-  void residue_post(CdResidueChunk& c, int rc);
+  // refine: one step of iterative refinement of the solves (eps not
+  // certified >= I: guarded, possibly pivoted, possibly ill-conditioned).
+  void residue_post(CdResidueChunk& c, int rc, bool refine);
   // sig/dsig of the targets in act at om (synchronises).
   void evaluate(const std::vector<int>& act);
   // evaluate in two halves.  With group given and the residues in one chunk,
@@ -85,6 +87,7 @@ struct CdEngine {
   CdResidueChunk ev_chunk{};
   bool ev_grouped = false;
   bool ev_spd = false;  // every residue eps of this evaluation is SPD (see evaluate_begin)
+  bool ev_guard = false;  // the residue eps of this evaluation are not certified >= I
   // Pinned staging in ctx->host_stage (reserved by setup_begin); sx is
   // filled from h_sx at the first evaluation's synchronisation.
   double *h_sx = nullptr, *h_hi = nullptr, *h_rv = nullptr, *h_rd = nullptr;
