@@ -597,8 +597,17 @@ static void sweep_update(qx_ctx* ctx, cudaStream_t st, double* eps, int n, int l
   check_launch(ctx);
 }
 
+// W' of the flagged matrices of a guard table (their re-inversion done):
+// grid (largest order, count).
+__global__ void k_finish_wc_tab(const GuardMat* __restrict__ tab, int half_lower) {
+  const GuardMat g = tab[blockIdx.y];
+  if ((int)blockIdx.x >= g.n) return;
+  finish_wc_row(g.M, g.n, g.ldn, *g.status != 0, half_lower, blockIdx.x);
+}
+
 void launch_invert_wc(qx_ctx* ctx, double* eps, int n, int ldn, size_t stride, int nw, int guard, int half_lower,
-                      int split_update) {
+                      int split_update, InvertDefer* defer) {
+  if (defer) defer->flagged.clear();
   QX_REQUIRE(nw >= 1 && nw <= 65535, QX_ERR_INVALID_INPUT, "%d matrices in one sweep (1 to 65535)", nw);
   // The split trailing update's error bound needs eps >= I: guarded matrices
   // are swept with FP64 updates.
@@ -694,11 +703,32 @@ void launch_invert_wc(qx_ctx* ctx, double* eps, int n, int ldn, size_t stride, i
     QX_CUDA(cudaEventRecord(ev_done, s0));
     QX_CUDA(cudaStreamWaitEvent(ctx->stream, ev_done, 0));
   }
-  // Guarded: the flagged matrices are inverted again with pivoting.
-  if (guard) guard_end(ctx, gs);
+  // Guarded: the flagged matrices are inverted again with pivoting, on the
+  // context stream, or (defer) on the side stream after the finish of the
+  // others, so that the caller's work on those overlaps the re-inversion.
+  int nflag = 0;
+  if (guard && defer) {
+    nflag = guard_flags(ctx, gs, &defer->flagged);
+  } else if (guard) {
+    guard_end(ctx, gs);
+  }
   dim3 fg(n, nw);
   k_finish_wc<<<fg, 256, 0, ctx->stream>>>(eps, n, ldn, stride, status, half_lower);
   check_launch(ctx);
+  if (nflag > 0) {
+    if (!ctx->fallback_stream) {
+      QX_CUDA(cudaStreamCreateWithFlags(&ctx->fallback_stream, cudaStreamNonBlocking));
+      QX_CUDA(cudaEventCreateWithFlags(&ctx->fallback_done, cudaEventDisableTiming));
+    }
+    // The side stream starts after the finish above (which also wrote the
+    // flagged matrices, from their unpivoted sweep).
+    QX_CUDA(cudaEventRecord(ctx->fallback_done, ctx->stream));
+    QX_CUDA(cudaStreamWaitEvent(ctx->fallback_stream, ctx->fallback_done, 0));
+    guard_fallback(ctx, gs, ctx->fallback_stream);
+    k_finish_wc_tab<<<dim3(gs.nmax_flagged, nflag), 256, 0, ctx->fallback_stream>>>(gs.d_tab, half_lower);
+    check_launch(ctx);
+    QX_CUDA(cudaEventRecord(ctx->fallback_done, ctx->fallback_stream));
+  }
   ctx->pending.push_back({status, nw, 1});
   if (tc) ctx->pending.push_back({tc_err, 2 * nsteps, 0});
 }
@@ -1015,20 +1045,30 @@ void launch_gather_ov(qx_ctx* ctx, const double* lpq, int naux, int nmo, int noc
   check_launch(ctx);
 }
 
-// sx[p] = -sum_{R,i} lpq[R][p][i]^2   (qp/evgw.rs:1167-1193)
-__global__ void k_exchange_diag(const double* __restrict__ lpq, int naux, int nmo, int nocc,
-                                const int* __restrict__ orbs, double* __restrict__ sx) {
+// sx[p] = -sum_{R,i} lpq[R][p][i]^2   (qp/evgw.rs:1167-1193).  One block of
+// 1024 threads per orbital; each thread keeps four loads in flight (the
+// elements are scattered over naux rows, so latency, not bandwidth, bounds a
+// block), and the sum has a fixed order.
+__global__ void __launch_bounds__(1024) k_exchange_diag(const double* __restrict__ lpq, int naux, int nmo, int nocc,
+                                                        const int* __restrict__ orbs, double* __restrict__ sx) {
   const int p = orbs ? orbs[blockIdx.x] : blockIdx.x;
-  double s = 0.0;
-  for (int idx = threadIdx.x; idx < naux * nocc; idx += blockDim.x) {
-    int R = idx / nocc, i = idx % nocc;
-    double v = lpq[(size_t)R * nmo * nmo + (size_t)p * nmo + i];
-    s += v * v;
+  const int total = naux * nocc;
+  double s[4] = {0.0, 0.0, 0.0, 0.0};
+  for (int idx = threadIdx.x; idx < total; idx += 4 * blockDim.x) {
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int k = idx + u * blockDim.x;
+      if (k < total) {
+        const int R = k / nocc, i = k % nocc;
+        const double v = __ldg(lpq + (size_t)R * nmo * nmo + (size_t)p * nmo + i);
+        s[u] += v * v;
+      }
+    }
   }
-  __shared__ double red[256];
-  red[threadIdx.x] = s;
+  __shared__ double red[1024];
+  red[threadIdx.x] = (s[0] + s[1]) + (s[2] + s[3]);
   __syncthreads();
-  for (int o = 128; o > 0; o >>= 1) {
+  for (int o = 512; o > 0; o >>= 1) {
     if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
     __syncthreads();
   }
@@ -1037,7 +1077,7 @@ __global__ void k_exchange_diag(const double* __restrict__ lpq, int naux, int nm
 
 void launch_exchange_diag(qx_ctx* ctx, const double* lpq, int naux, int nmo, int nocc, double* sx,
                           const int* orbs, int norbs) {
-  k_exchange_diag<<<orbs ? norbs : nmo, 256, 0, ctx->stream>>>(lpq, naux, nmo, nocc, orbs, sx);
+  k_exchange_diag<<<orbs ? norbs : nmo, 1024, 0, ctx->stream>>>(lpq, naux, nmo, nocc, orbs, sx);
   check_launch(ctx);
 }
 
