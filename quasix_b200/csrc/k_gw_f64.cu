@@ -597,17 +597,8 @@ static void sweep_update(qx_ctx* ctx, cudaStream_t st, double* eps, int n, int l
   check_launch(ctx);
 }
 
-// W' of the flagged matrices of a guard table (their re-inversion done):
-// grid (largest order, count).
-__global__ void k_finish_wc_tab(const GuardMat* __restrict__ tab, int half_lower) {
-  const GuardMat g = tab[blockIdx.y];
-  if ((int)blockIdx.x >= g.n) return;
-  finish_wc_row(g.M, g.n, g.ldn, *g.status != 0, half_lower, blockIdx.x);
-}
-
 void launch_invert_wc(qx_ctx* ctx, double* eps, int n, int ldn, size_t stride, int nw, int guard, int half_lower,
-                      int split_update, InvertDefer* defer) {
-  if (defer) defer->flagged.clear();
+                      int split_update) {
   QX_REQUIRE(nw >= 1 && nw <= 65535, QX_ERR_INVALID_INPUT, "%d matrices in one sweep (1 to 65535)", nw);
   // The split trailing update's error bound needs eps >= I: guarded matrices
   // are swept with FP64 updates.
@@ -703,32 +694,11 @@ void launch_invert_wc(qx_ctx* ctx, double* eps, int n, int ldn, size_t stride, i
     QX_CUDA(cudaEventRecord(ev_done, s0));
     QX_CUDA(cudaStreamWaitEvent(ctx->stream, ev_done, 0));
   }
-  // Guarded: the flagged matrices are inverted again with pivoting, on the
-  // context stream, or (defer) on the side stream after the finish of the
-  // others, so that the caller's work on those overlaps the re-inversion.
-  int nflag = 0;
-  if (guard && defer) {
-    nflag = guard_flags(ctx, gs, &defer->flagged);
-  } else if (guard) {
-    guard_end(ctx, gs);
-  }
+  // Guarded: the flagged matrices are inverted again with pivoting.
+  if (guard) guard_end(ctx, gs);
   dim3 fg(n, nw);
   k_finish_wc<<<fg, 256, 0, ctx->stream>>>(eps, n, ldn, stride, status, half_lower);
   check_launch(ctx);
-  if (nflag > 0) {
-    if (!ctx->fallback_stream) {
-      QX_CUDA(cudaStreamCreateWithFlags(&ctx->fallback_stream, cudaStreamNonBlocking));
-      QX_CUDA(cudaEventCreateWithFlags(&ctx->fallback_done, cudaEventDisableTiming));
-    }
-    // The side stream starts after the finish above (which also wrote the
-    // flagged matrices, from their unpivoted sweep).
-    QX_CUDA(cudaEventRecord(ctx->fallback_done, ctx->stream));
-    QX_CUDA(cudaStreamWaitEvent(ctx->fallback_stream, ctx->fallback_done, 0));
-    guard_fallback(ctx, gs, ctx->fallback_stream);
-    k_finish_wc_tab<<<dim3(gs.nmax_flagged, nflag), 256, 0, ctx->fallback_stream>>>(gs.d_tab, half_lower);
-    check_launch(ctx);
-    QX_CUDA(cudaEventRecord(ctx->fallback_done, ctx->fallback_stream));
-  }
   ctx->pending.push_back({status, nw, 1});
   if (tc) ctx->pending.push_back({tc_err, 2 * nsteps, 0});
 }

@@ -556,13 +556,6 @@ void guard_begin(qx_ctx* ctx, GuardSet& gs) {
 }
 
 int guard_end(qx_ctx* ctx, GuardSet& gs) {
-  const int F = guard_flags(ctx, gs, nullptr);
-  if (F > 0) guard_fallback(ctx, gs, ctx->stream);
-  return F;
-}
-
-int guard_flags(qx_ctx* ctx, GuardSet& gs, std::vector<int>* flagged_idx) {
-  if (flagged_idx) flagged_idx->clear();
   if (gs.mats.empty()) return 0;
   const int G = (int)gs.mats.size();
   // Probe residual of every result against its copy.
@@ -610,17 +603,7 @@ int guard_flags(qx_ctx* ctx, GuardSet& gs, std::vector<int>* flagged_idx) {
   const int F = (int)flagged.size();
   QX_REQUIRE(F <= 65535, QX_ERR_INVALID_INPUT, "%d matrices to re-invert in one call (at most 65535)", F);
   QX_CUDA(cudaMemcpyAsync(gs.d_tab, flagged.data(), F * sizeof(GuardMat), cudaMemcpyHostToDevice, ctx->stream));
-  gs.nmax_flagged = nmax;
-  if (flagged_idx)
-    for (const GuardMat& g : flagged) flagged_idx->push_back(g.idx);
-  return F;
-}
-
-void guard_fallback(qx_ctx* ctx, GuardSet& gs, cudaStream_t stream) {
-  const int F = gs.nflagged, nmax = gs.nmax_flagged;
-  if (F == 0) return;
-  cudaStream_t st = stream;
-  k_piv_init<<<F, 256, 0, st>>>(gs.d_tab);
+  k_piv_init<<<F, 256, 0, ctx->stream>>>(gs.d_tab);
   check_launch(ctx);
   const int tiles = ceil_div(nmax, PivTile::BM);
   const bool smem_panel = nmax <= kPivSmemRows;
@@ -630,37 +613,38 @@ void guard_fallback(qx_ctx* ctx, GuardSet& gs, cudaStream_t stream) {
       if (nmax <= 1024) {
         // The panel kernel also gathers the pivot rows for the update.
         if (nmax <= 512)
-          k_piv_panel_reg<1><<<F, 512, 0, st>>>(gs.d_tab, k0);
+          k_piv_panel_reg<1><<<F, 512, 0, ctx->stream>>>(gs.d_tab, k0);
         else
-          k_piv_panel_reg<2><<<F, 512, 0, st>>>(gs.d_tab, k0);
+          k_piv_panel_reg<2><<<F, 512, 0, ctx->stream>>>(gs.d_tab, k0);
         check_launch(ctx);
       } else {
         if (smem_panel)
-          k_piv_panel<true><<<F, 512, panel_smem, st>>>(gs.d_tab, k0);
+          k_piv_panel<true><<<F, 512, panel_smem, ctx->stream>>>(gs.d_tab, k0);
         else
-          k_piv_panel<false><<<F, 512, 0, st>>>(gs.d_tab, k0);
+          k_piv_panel<false><<<F, 512, 0, ctx->stream>>>(gs.d_tab, k0);
         check_launch(ctx);
-        k_piv_gather<<<dim3(F, 2), 256, 0, st>>>(gs.d_tab, k0, PIV_NB, ks, ks + PIV_SB);
+        k_piv_gather<<<dim3(F, 2), 256, 0, ctx->stream>>>(gs.d_tab, k0, PIV_NB, ks, ks + PIV_SB);
         check_launch(ctx);
       }
       // The rest of the super-panel (one column tile).
-      k_piv_update<<<dim3(1, tiles, F), PivTile::THREADS, PivTile::SMEM, st>>>(gs.d_tab, k0, PIV_NB, ks,
+      k_piv_update<<<dim3(1, tiles, F), PivTile::THREADS, PivTile::SMEM, ctx->stream>>>(gs.d_tab, k0, PIV_NB, ks,
                                                                                         ks + PIV_SB, k0, k0 + 1);
       check_launch(ctx);
     }
     // Every column outside the super-panel: one rank-PIV_SB update.
     if (ks + PIV_SB < nmax || ks > 0) {
-      k_piv_gather<<<dim3(F, 8), 256, 0, st>>>(gs.d_tab, ks, PIV_SB, 0, nmax);
+      k_piv_gather<<<dim3(F, 8), 256, 0, ctx->stream>>>(gs.d_tab, ks, PIV_SB, 0, nmax);
       check_launch(ctx);
-      k_piv_update<<<dim3(tiles, tiles, F), PivTile::THREADS, PivTile::SMEM, st>>>(
+      k_piv_update<<<dim3(tiles, tiles, F), PivTile::THREADS, PivTile::SMEM, ctx->stream>>>(
           gs.d_tab, ks, PIV_SB, 0, nmax, ks, ks + PIV_SB);
       check_launch(ctx);
     }
   }
-  k_piv_inverse_perm<<<F, 256, 0, st>>>(gs.d_tab);
+  k_piv_inverse_perm<<<F, 256, 0, ctx->stream>>>(gs.d_tab);
   check_launch(ctx);
-  k_piv_permute<<<dim3(nmax, F), 256, 0, st>>>(gs.d_tab);
+  k_piv_permute<<<dim3(nmax, F), 256, 0, ctx->stream>>>(gs.d_tab);
   check_launch(ctx);
+  return F;
 }
 
 }  // namespace qx

@@ -247,10 +247,6 @@ struct TcArgs {
   const int* gpre;
   int gcount;
   int unit;  // STORE: k-blocks per FP32 accumulation unit (0 counts as 1)
-  // ROWDOT: when wlist is given, the items cover only its nwl frequencies
-  // (wlist[i] in [0, nbatch)); v and the scales stay indexed by frequency.
-  const int* wlist;
-  int nwl;
   // CONVB: B[w][n][k] = convB[n][k] * convC[w][k] (FP32, zero past K): the
   // FP32 tile of convB arrives by TMA (map in the mapBh slot), and the
   // converter warps scale and split it into the hi/lo tile the MMA reads.
@@ -320,19 +316,16 @@ __global__ void __launch_bounds__(TcThreads<EPI, CONVB>::VALUE, 1)
   // a group of wgroup share each pair block while it is in L2; TMEM buffers,
   // stages and barrier phases run on across items, so the epilogue of one
   // item overlaps the MMAs of the next.  The other forms take one item.
-  const int n_freq = (EPI == EPI_ROWDOT && args.wlist) ? args.nwl : args.nbatch;
   const int n_items =
-      (EPI == EPI_ROWDOT) ? (n_freq + args.wgroup - 1) / args.wgroup * args.m_blocks * args.wgroup : 1;
+      (EPI == EPI_ROWDOT) ? (args.nbatch + args.wgroup - 1) / args.wgroup * args.m_blocks * args.wgroup : 1;
   const int item0 = (EPI == EPI_ROWDOT) ? (int)blockIdx.x : 0;
   const int item_step = (EPI == EPI_ROWDOT) ? (int)gridDim.x : 1;
-  // Item -> (pair block, frequency); w_ >= nbatch marks an item past the end.
   auto rowdot_item = [&](int b, int& mb_, int& w_) {
     const int g = args.wgroup;
     const int per_group = args.m_blocks * g;
     const int grp = b / per_group, r = b % per_group;
     mb_ = r / g;
-    const int k = grp * g + r % g;
-    w_ = !args.wlist ? k : (k < n_freq ? __ldg(args.wlist + k) : args.nbatch);
+    w_ = grp * g + r % g;
   };
   if (EPI == EPI_ROWDOT) {
     mb = 0;
@@ -1160,19 +1153,12 @@ static SplitScratch split_scratch(qx_ctx* ctx, int slot_offset) {
   return s;
 }
 
-// boff: the batch is entries [boff, boff + batch) of the slot's bound and
-// scale arrays (a sub-range of a larger batch split in pieces).
 static void split(qx_ctx* ctx, const double* src, int rows, int cols, int ld_src, size_t src_stride, void* hi,
                   void* lo, int ld_dst, size_t dst_stride, int batch, const double* colscale, int ld_cs, int fp16,
                   int slot, float** scale_out, const unsigned long long* given_amax = nullptr,
-                  cudaStream_t stream = nullptr, int boff = 0) {
-  QX_REQUIRE(batch >= 1 && boff >= 0 && boff + batch <= 1024, QX_ERR_INVALID_INPUT,
-             "at most 1024 frequencies per split");
+                  cudaStream_t stream = nullptr) {
+  QX_REQUIRE(batch <= 1024, QX_ERR_INVALID_INPUT, "at most 1024 frequencies per split");
   SplitScratch sc = split_scratch(ctx, slot);
-  float* const scale_base = sc.scale;
-  QX_REQUIRE(boff == 0 || (!colscale && !given_amax), QX_ERR_INVALID_INPUT, "split offsets need their own bounds");
-  sc.amax_src += boff;
-  sc.scale += boff;
   cudaStream_t st = stream ? stream : ctx->stream;
   if (fp16) {
     const int nsrc = src_stride ? batch : 1;
@@ -1182,8 +1168,7 @@ static void split(qx_ctx* ctx, const double* src, int rows, int cols, int ld_src
       sc.amax_src = const_cast<unsigned long long*>(given_amax);
       if (colscale) QX_CUDA(cudaMemsetAsync(sc.amax_col, 0, 1024 * sizeof(unsigned long long), st));
     } else {
-      QX_CUDA(cudaMemsetAsync(sc.amax_src, 0, nsrc * sizeof(unsigned long long), st));
-      if (colscale) QX_CUDA(cudaMemsetAsync(sc.amax_col, 0, 1024 * sizeof(unsigned long long), st));
+      QX_CUDA(cudaMemsetAsync(sc.amax_src, 0, 2048 * sizeof(unsigned long long), st));
       // About eight blocks per SM over all batches, each thread four
       // elements per step at least.
       const size_t tot = (size_t)rows * cols;
@@ -1241,14 +1226,14 @@ static void split(qx_ctx* ctx, const double* src, int rows, int cols, int ld_src
                                            dst_stride, fp16, sc.amax_src, acol, sc.scale);
   }
   check_launch(ctx);
-  if (scale_out) *scale_out = scale_base;
+  if (scale_out) *scale_out = sc.scale;
 }
 
 void launch_split(qx_ctx* ctx, const double* src, int rows, int cols, int ld_src, void* hi, void* lo, int ld_dst,
                   size_t src_stride, size_t dst_stride, int batch, int fp16, int slot, float** scale_out,
-                  const unsigned long long* given_amax, int boff) {
+                  const unsigned long long* given_amax) {
   split(ctx, src, rows, cols, ld_src, src_stride, hi, lo, ld_dst, dst_stride, batch, nullptr, 0, fp16, slot,
-        scale_out, given_amax, nullptr, boff);
+        scale_out, given_amax);
 }
 
 unsigned long long* split_amax_words(qx_ctx* ctx, int slot) { return split_scratch(ctx, slot).amax_src; }
@@ -1274,20 +1259,10 @@ static void launch_tc(qx_ctx* ctx, const CUtensorMap& ah, const CUtensorMap& al,
 // Autotuned frequency-group size of the pair contraction, per (npair, naux,
 // nw, device): candidates 4, 8, 16, 32 (<= nw) are timed with CUDA events on
 // the first call of a shape; later calls reuse the fastest.
-static std::mutex g_wgroup_mu;
-static std::map<std::array<int, 4>, int> g_wgroup_table;
-
-// The tuned grouping of a shape, or 0 when it has not been tuned yet.
-static int known_wgroup(qx_ctx* ctx, int npair, int naux, int nw) {
-  std::lock_guard<std::mutex> lock(g_wgroup_mu);
-  auto it = g_wgroup_table.find({npair, naux, nw, ctx->device});
-  return it == g_wgroup_table.end() ? 0 : it->second;
-}
-
 template <class F>
 static int tuned_wgroup(qx_ctx* ctx, int npair, int naux, int nw, F&& launch_with) {
-  auto& mu = g_wgroup_mu;
-  auto& table = g_wgroup_table;
+  static std::mutex mu;
+  static std::map<std::array<int, 4>, int> table;
   const std::array<int, 4> key{npair, naux, nw, ctx->device};
   {
     std::lock_guard<std::mutex> lock(mu);
@@ -1325,8 +1300,7 @@ static int tuned_wgroup(qx_ctx* ctx, int npair, int naux, int nw, F&& launch_wit
 // v[w][p] = 2 sum_Q X[p][Q] sum_{P <= Q} (Bh+Bl)[p][P] (W'h+W'l)[w][Q][P] / (sA sB[w]),
 // W' the half-lower form of Wc (three products per term)
 void launch_pair_contract_tc(qx_ctx* ctx, const TcOperand& A, const float* bpt_f32, int ldk, int npair, int naux,
-                             const TcOperand& W, int ldw, size_t wc_stride, int nw, double* v, int ldv, int fp16,
-                             const int* d_wlist, int nwl, int grid_cap) {
+                             const TcOperand& W, int ldw, size_t wc_stride, int nw, double* v, int ldv, int fp16) {
   constexpr int BN = 256;
   QX_REQUIRE(wc_stride == (size_t)naux * ldw, QX_ERR_INVALID_INPUT, "Wc stride must be naux*ldw");
   constexpr int BK = TcPipe<EPI_ROWDOT>::BK;
@@ -1358,25 +1332,14 @@ void launch_pair_contract_tc(qx_ctx* ctx, const TcOperand& A, const float* bpt_f
   // passes); every (frequency, pair block) is still one CTA with the same
   // arithmetic, so the choice does not change the result.  It is tuned once
   // per shape by timing the candidates on the call's own data.
-  const int cap = grid_cap > 0 ? std::min(grid_cap, ctx->sm_count) : ctx->sm_count;
   auto launch_with = [&](int g) {
     a.wgroup = g;
-    // Persistent: one CTA per SM (192 KB of stages each) over all items; a
-    // cap leaves SMs to work running beside it on another stream.
-    const int items = ceil_div(d_wlist ? nwl : nw, g) * a.m_blocks * g;
-    launch_tc<BN, EPI_ROWDOT>(ctx, ah, al, bh, bl, a, dim3(std::min(items, cap)));
+    // Persistent: one CTA per SM (192 KB of stages each) over all items.
+    const int items = ceil_div(nw, g) * a.m_blocks * g;
+    launch_tc<BN, EPI_ROWDOT>(ctx, ah, al, bh, bl, a, dim3(std::min(items, ctx->sm_count)));
   };
-  if (d_wlist) {
-    // A subset of the frequencies: the grouping tuned for the whole set when
-    // there is one (no timing here), else groups of up to 8.
-    a.wlist = d_wlist;
-    a.nwl = nwl;
-    const int g = known_wgroup(ctx, npair, naux, nw);
-    launch_with(std::max(1, std::min(g > 0 ? g : 8, nwl)));
-  } else {
-    a.wgroup = tuned_wgroup(ctx, npair, naux, nw, launch_with);
-    launch_with(a.wgroup);
-  }
+  a.wgroup = tuned_wgroup(ctx, npair, naux, nw, launch_with);
+  launch_with(a.wgroup);
   check_tc_err(ctx, d_err);
 }
 

@@ -263,61 +263,15 @@ void gw_wc_p0(qx_ctx* ctx, GWSystem& S, const double* e_host) {
 }
 
 // v[w][pair] = Wc_nm(iw) of every pair, from S.eps holding W' (half-lower Wc).
-// Split W' of the frequencies in ws (sorted) for the contraction, one
-// launch per run of consecutive frequencies.
-static void split_wc_runs(qx_ctx* ctx, GWSystem& S, const std::vector<int>& ws, int fp16) {
-  for (size_t a = 0; a < ws.size();) {
-    size_t b = a + 1;
-    while (b < ws.size() && ws[b] == ws[b - 1] + 1) ++b;
-    const int w0 = ws[a], len = (int)(b - a);
-    const size_t off = (size_t)w0 * S.eps_stride;
-    launch_split(ctx, S.eps + off, S.naux, S.naux, S.ldn, static_cast<uint16_t*>(S.wc_split.hi) + off,
-                 static_cast<uint16_t*>(S.wc_split.lo) + off, S.ldn, S.eps_stride, S.eps_stride, len, fp16, 0,
-                 &S.wc_split.scale, nullptr, w0);
-    a = b;
-  }
-}
-
-void gw_wc_contract(qx_ctx* ctx, GWSystem& S, const InvertDefer* defer) {
+void gw_wc_contract(qx_ctx* ctx, GWSystem& S) {
   record_stage(ctx, QX_ST_CONTRACT, true);
-  const bool deferred = defer && !defer->flagged.empty();
-  if (is_tc_precision(S.precision) && deferred) {
-    // The flagged frequencies are re-inverted on the side stream meanwhile:
-    // contract the others first on all SMs but as many as the re-inversion
-    // keeps busy (one CTA per flagged matrix), then the flagged ones.
-    const int fp16 = S.precision == QX_PREC_FP16X3;
-    std::vector<char> is_f(S.nw, 0);
-    for (int w : defer->flagged) is_f[w] = 1;
-    std::vector<int> lists;  // [others | flagged]
-    for (int w = 0; w < S.nw; ++w)
-      if (!is_f[w]) lists.push_back(w);
-    const int nkeep = (int)lists.size();
-    std::vector<int> flagged(defer->flagged);
-    std::sort(flagged.begin(), flagged.end());
-    lists.insert(lists.end(), flagged.begin(), flagged.end());
-    DevBuf& lb = ctx->ws[WS_WLIST];
-    lb.reserve(lists.size() * sizeof(int));
-    int* d_lists = lb.as<int>();
-    QX_CUDA(cudaMemcpyAsync(d_lists, lists.data(), lists.size() * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
-    if (nkeep > 0) {
-      split_wc_runs(ctx, S, std::vector<int>(lists.begin(), lists.begin() + nkeep), fp16);
-      const int cap = std::max(1, ctx->sm_count - std::min((int)flagged.size(), ctx->sm_count / 4));
-      launch_pair_contract_tc(ctx, S.bpt_split, S.bpt_f32, S.ldk, S.npair, S.naux, S.wc_split, S.ldn, S.eps_stride,
-                              S.nw, S.v, S.npair, fp16, d_lists, nkeep, cap);
-    }
-    QX_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->fallback_done, 0));
-    split_wc_runs(ctx, S, flagged, fp16);
-    launch_pair_contract_tc(ctx, S.bpt_split, S.bpt_f32, S.ldk, S.npair, S.naux, S.wc_split, S.ldn, S.eps_stride,
-                            S.nw, S.v, S.npair, fp16, d_lists + nkeep, (int)flagged.size());
-  } else if (is_tc_precision(S.precision)) {
-    if (deferred) QX_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->fallback_done, 0));
+  if (is_tc_precision(S.precision)) {
     const int fp16 = S.precision == QX_PREC_FP16X3;
     launch_split(ctx, S.eps, S.naux, S.naux, S.ldn, S.wc_split.hi, S.wc_split.lo, S.ldn, S.eps_stride, S.eps_stride,
                  S.nw, fp16, 0, &S.wc_split.scale);
     launch_pair_contract_tc(ctx, S.bpt_split, S.bpt_f32, S.ldk, S.npair, S.naux, S.wc_split, S.ldn, S.eps_stride, S.nw,
                             S.v, S.npair, fp16);
   } else {
-    if (deferred) QX_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->fallback_done, 0));
     launch_pair_contract_fp64(ctx, S.bpt, S.ldk, S.npair, S.naux, S.eps, S.ldn, S.eps_stride, S.nw, S.v, S.npair);
   }
   record_stage(ctx, QX_ST_CONTRACT, false);
@@ -331,15 +285,11 @@ void gw_wc_pairs(qx_ctx* ctx, GWSystem& S, const double* e_host) {
   // [1, 1 + ||Pi||], so the split trailing update of the sweep keeps Wc within
   // the split forms' error.  Once levels cross, eps may be indefinite and the
   // sweep runs guarded (with the pivoted fallback).
-  // The pivoted re-inversion of flagged frequencies (if any) runs beside the
-  // contraction of the others (split forms).
-  const bool guard = !eps_at_least_identity(e_host, S.nocc, S.nvir, 0.0);
-  InvertDefer defer;
-  launch_invert_wc(ctx, S.eps, S.naux, S.ldn, S.eps_stride, S.nw, guard, /*half_lower=*/1,
-                   /*split_update=*/is_tc_precision(S.precision),
-                   guard && is_tc_precision(S.precision) ? &defer : nullptr);
+  launch_invert_wc(ctx, S.eps, S.naux, S.ldn, S.eps_stride, S.nw,
+                   !eps_at_least_identity(e_host, S.nocc, S.nvir, 0.0), /*half_lower=*/1,
+                   /*split_update=*/is_tc_precision(S.precision));
   record_stage(ctx, QX_ST_INV, false);
-  gw_wc_contract(ctx, S, &defer);
+  gw_wc_contract(ctx, S);
 }
 
 // One imaginary-axis Sigma_c evaluation with energies e (host array [nmo]).
@@ -560,11 +510,6 @@ qx_status qx_ctx_destroy(qx_ctx* c) {
     if (e) cudaEventDestroy(e);
   if (c->sweep_hi) cudaStreamDestroy(c->sweep_hi);
   if (c->sweep_lo) cudaStreamDestroy(c->sweep_lo);
-  if (c->fallback_stream) {
-    cudaStreamSynchronize(c->fallback_stream);
-    cudaStreamDestroy(c->fallback_stream);
-  }
-  if (c->fallback_done) cudaEventDestroy(c->fallback_done);
   for (auto& e : c->ev)
     if (e) cudaEventDestroy(e);
   if (c->own_stream) cudaStreamDestroy(c->own_stream);

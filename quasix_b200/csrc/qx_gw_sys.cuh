@@ -37,9 +37,7 @@ void gw_wc_pairs(qx_ctx* ctx, GWSystem& S, const double* e_host);
 // The two halves of gw_wc_pairs around the inversion of S.eps (to W', the
 // half-lower Wc): P0 into S.eps, then the pair contraction.
 void gw_wc_p0(qx_ctx* ctx, GWSystem& S, const double* e_host);
-// defer (from launch_invert_wc): the frequencies still being re-inverted on
-// ctx->fallback_stream; their contraction runs after the others'.
-void gw_wc_contract(qx_ctx* ctx, GWSystem& S, const InvertDefer* defer = nullptr);
+void gw_wc_contract(qx_ctx* ctx, GWSystem& S);
 void gw_sigma(qx_ctx* ctx, GWSystem& S, const double* e_host);
 void record_stage(qx_ctx* ctx, int st, bool begin);
 void accumulate_stage_times(qx_ctx* ctx);

@@ -132,10 +132,6 @@ struct qx_ctx {
   // Form of the split-precision P0 (QX_P0_AUTO / _MATERIALISED / _CONVERTER);
   // batch workers inherit it from their parent context.
   int p0_form = 0;
-  // Side stream of the pivoted re-inversion when it runs beside the pair
-  // contraction of the frequencies that needed none, and its event.
-  cudaStream_t fallback_stream = nullptr;
-  cudaEvent_t fallback_done = nullptr;
 };
 
 namespace qx {
@@ -166,7 +162,6 @@ enum WsSlot {
   WS_GRAD0, WS_GRAD1, WS_GRAD2,  // CD adjoint: accumulators, per-frequency chunk, lpq gradient
   WS_SWEEP_SPLIT,  // split sweep panels (two steps in flight)
   WS_GUARD,        // guarded inversion: copies of eps and the pivoted fallback's work arrays
-  WS_WLIST,        // frequency lists of a contraction split around a deferred re-inversion
   WS_COUNT
 };
 static_assert(WS_COUNT <= 40, "workspace slots");
@@ -272,8 +267,7 @@ struct GuardSet {
   unsigned long long* growth = nullptr;  // [nall] max over the unswept entries met by the sweep
   unsigned long long* xmax = nullptr;    // [nall] max|eps^-1| of the sweep's result
   unsigned long long* rmax = nullptr;    // [nall] probe residual max|eps X v - v|
-  int nflagged = 0;                      // matrices flagged for re-inversion (first nflagged of d_tab)
-  int nmax_flagged = 0;                  // their largest order
+  int nflagged = 0;                      // matrices re-inverted by the last guard_end
 };
 // Workspace bytes of count guarded n x ldn matrices (an upper bound).
 size_t guard_bytes(int n, int ldn, int count);
@@ -285,17 +279,6 @@ void guard_begin(qx_ctx* ctx, GuardSet& gs);
 // re-inverts the flagged matrices with pivoting (queued on the context
 // stream).  Returns the number re-inverted.
 int guard_end(qx_ctx* ctx, GuardSet& gs);
-// guard_end in two halves: guard_flags probes, reads the flags and fills the
-// table of flagged matrices (their sweep indices in *flagged_idx), returning
-// their number; guard_fallback queues their pivoted re-inversion on stream.
-int guard_flags(qx_ctx* ctx, GuardSet& gs, std::vector<int>* flagged_idx);
-void guard_fallback(qx_ctx* ctx, GuardSet& gs, cudaStream_t stream);
-// Frequencies whose pivoted re-inversion runs on ctx->fallback_stream beside
-// later work on the context stream: flagged lists them (their W' final once
-// ctx->fallback_done, recorded after it, has fired).
-struct InvertDefer {
-  std::vector<int> flagged;
-};
 
 // eps >= I holds for eps = I + B diag(chi') B^T when every chi' >= 0: on the
 // imaginary axis when no occupied level lies above a virtual one, on the real
@@ -312,7 +295,7 @@ bool eps_at_least_identity(const double* energies, int nocc, int nvir, double wm
 // split_update: run the trailing updates on tcgen05 in the FP16X3 form
 // (launch_sweep_update_tc); the diagonal blocks and panels stay FP64.
 void launch_invert_wc(qx_ctx* ctx, double* eps, int n, int ldn, size_t stride, int nw, int guard,
-                      int half_lower = 0, int split_update = 0, InvertDefer* defer = nullptr);
+                      int half_lower = 0, int split_update = 0);
 
 // One matrix of a grouped block sweep: M [n][ldn], symmetric, inverted in
 // place.  prow (its first row in the concatenated panel arrays, a multiple of
@@ -407,7 +390,7 @@ inline bool is_tc_precision(int p) { return p == QX_PREC_BF16X3 || p == QX_PREC_
 // are already on the device; no amax pass.
 void launch_split(qx_ctx* ctx, const double* src, int rows, int cols, int ld_src, void* hi, void* lo, int ld_dst,
                   size_t src_stride, size_t dst_stride, int batch, int fp16, int slot, float** scale_out,
-                  const unsigned long long* given_amax = nullptr, int boff = 0);
+                  const unsigned long long* given_amax = nullptr);
 // The amax words of split slot `slot` (1024, for kernels that accumulate a
 // bound before the split).
 unsigned long long* split_amax_words(qx_ctx* ctx, int slot);
@@ -418,8 +401,7 @@ void launch_eps_tc(qx_ctx* ctx, const double* bov, int ldov, int naux, int nov, 
 void launch_gemm_tc(qx_ctx* ctx, const TcOperand& A, int M, int lda, const TcOperand& B, int N, int ldb, int K,
                     int nbatch, double* out, int ldo, size_t out_stride, int fp16);
 void launch_pair_contract_tc(qx_ctx* ctx, const TcOperand& A, const float* bpt_f32, int ldk, int npair, int naux,
-                             const TcOperand& W, int ldw, size_t wc_stride, int nw, double* v, int ldv, int fp16,
-                             const int* d_wlist = nullptr, int nwl = 0, int grid_cap = 0);
+                             const TcOperand& W, int ldw, size_t wc_stride, int nw, double* v, int ldv, int fp16);
 bool tc_supported(qx_ctx* ctx);
 
 // Block sweep in the FP16X3 form: split the step's panels (buffer half buf of
