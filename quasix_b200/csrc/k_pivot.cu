@@ -21,12 +21,7 @@
 //      whatever the conditioning, and it exceeds kGuardResidual when the
 //      unpivoted elimination lost digits to element growth that the pivot
 //      and growth checks did not see;
-//   2c. refines each flagged matrix without a zero pivot whose probe
-//      residual is below kRefineResidual by Newton-Schulz, X <- X + (I - X
-//      eps) X (two DMMA GEMMs a step, each squaring the residual), probing it
-//      again after each of up to kRefineSteps steps: those that then meet the
-//      backward-error bound leave the flagged set;
-//   3. re-inverts every still flagged matrix from its copy by Gauss-Jordan
+//   3. re-inverts every flagged matrix from its copy by Gauss-Jordan
 //      elimination with partial (row) pivoting, in super-panels of PIV_SB
 //      columns, each worked as panels of PIV_NB (k_piv_panel: the pivoted
 //      exchanges on a panel, one CTA per matrix; k_piv_update on the rest of
