@@ -38,7 +38,6 @@
 #include <climits>
 
 #include "gemm_f64.cuh"
-#include "qx_blas.cuh"
 #include "qx_internal.cuh"
 
 namespace qx {
@@ -497,74 +496,9 @@ __global__ void k_piv_permute(const GuardMat* __restrict__ tab) {
   for (int c = threadIdx.x; c < g.n; c += blockDim.x) dst[c] = -src[pinv[c]];
 }
 
-// T[i][i] += 1 over the n x n matrix (row stride ld).
-__global__ void k_ns_add_identity(double* __restrict__ T, int n, int ld) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) T[(size_t)i * ld + i] += 1.0;
-}
-
-// M <- M + (T + T^T) / 2 over n x n (each thread owns the pair (r, c), (c, r)).
-__global__ void k_ns_apply(double* __restrict__ M, const double* __restrict__ T, int n, int ld) {
-  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < (size_t)n * n;
-       e += (size_t)gridDim.x * blockDim.x) {
-    const size_t r = e / n, c = e % n;
-    if (c > r) continue;
-    const double d = 0.5 * (T[r * ld + c] + T[c * ld + r]);
-    M[r * ld + c] += d;
-    if (c != r) M[c * ld + r] += d;
-  }
-}
-
-// xmax and rmax of the table's matrices back to 0 (a new probe follows).
-__global__ void k_guard_reset(const GuardMat* __restrict__ tab, int count, unsigned long long* __restrict__ xmax,
-                              unsigned long long* __restrict__ rmax) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
-    xmax[tab[i].idx] = 0ull;
-    rmax[tab[i].idx] = 0ull;
-  }
-}
-
 inline size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
 
 }  // namespace
-
-// One Newton-Schulz step on each matrix of mats: with M = -X the sweep's
-// result (X ~ eps^-1) and eps its copy bk, X' = X + (I - X eps) X, i.e.
-//   M <- M + (I + M eps) M,
-// symmetrised; two DMMA GEMMs per matrix (X symmetric, eps symmetric).
-static void ns_refine(qx_ctx* ctx, const std::vector<GuardMat>& mats, int nmax) {
-  int ldmax = 0;
-  for (const GuardMat& g : mats) ldmax = std::max(ldmax, g.ldn);
-  DevBuf& wb = ctx->ws[WS_NS];
-  wb.reserve(2 * (size_t)nmax * ldmax * sizeof(double));
-  double* T1 = wb.as<double>();
-  double* T2 = T1 + (size_t)nmax * ldmax;
-  for (const GuardMat& g : mats) {
-    const int n = g.n, ld = g.ldn;
-    GemmNT a{};
-    a.M = n;
-    a.N = n;
-    a.K = n;
-    a.A = g.M;
-    a.lda = ld;
-    a.B = g.bk;
-    a.ldb = ld;
-    a.C = T1;
-    a.ldc = ld;
-    a.batch = 1;
-    a.alpha = 1.0;
-    gemm_nt_f64(ctx, a);  // T1 = M eps
-    k_ns_add_identity<<<ceil_div(n, 256), 256, 0, ctx->stream>>>(T1, n, ld);
-    check_launch(ctx);
-    GemmNT b = a;
-    b.A = T1;
-    b.B = g.M;
-    b.C = T2;
-    gemm_nt_f64(ctx, b);  // T2 = (I + M eps) M
-    const int blocks = std::min(ceil_div(n * n, 256), 4 * ctx->sm_count);
-    k_ns_apply<<<blocks, 256, 0, ctx->stream>>>(g.M, T2, n, ld);
-    check_launch(ctx);
-  }
-}
 
 size_t guard_bytes(int n, int ldn, int count) {
   const size_t per = align256((size_t)n * ldn * sizeof(double)) + align256((size_t)3 * n * sizeof(int)) +
@@ -651,58 +585,19 @@ int guard_end(qx_ctx* ctx, GuardSet& gs) {
     memcpy(&d, &u, sizeof d);
     return d;
   };
-  // Flagged matrices whose unpivoted result is close to the inverse (probe
-  // residual below kRefineResidual, no zero pivot) are refined by
-  // Newton-Schulz first; the others, and those the refinement does not bring
-  // under the backward-error bound, are re-inverted with pivoting.
-  std::vector<GuardMat> flagged, refine;
+  std::vector<GuardMat> flagged;
   nmax = 0;
-  int nmax_refine = 0;
   for (int i = 0; i < G; ++i) {
     const GuardMat& g = gs.mats[i];
     const double a = as_double(amax[g.idx]), gr = as_double(growth[g.idx]);
-    const double r = as_double(rmax[g.idx]);
-    const double eta = r / ((double)g.n * a * as_double(xmax[g.idx]));
+    const double eta = as_double(rmax[g.idx]) / ((double)g.n * a * as_double(xmax[g.idx]));
     if (st[i] != 0 || !(gr <= kGuardGrowth * a) || !(eta <= kGuardResidual)) {
-      if (st[i] == 0 && r < kRefineResidual) {
-        refine.push_back(g);
-        nmax_refine = std::max(nmax_refine, g.n);
-      } else {
-        flagged.push_back(g);
-        nmax = std::max(nmax, g.n);
-      }
+      flagged.push_back(g);
+      nmax = std::max(nmax, g.n);
     }
-  }
-  ctx->guard_matrices += G;
-  for (int step = 0; step < kRefineSteps && !refine.empty(); ++step) {
-    const int R = (int)refine.size();
-    ns_refine(ctx, refine, nmax_refine);
-    // Probe the refined matrices again.
-    QX_CUDA(cudaMemcpyAsync(gs.d_tab, refine.data(), R * sizeof(GuardMat), cudaMemcpyHostToDevice, ctx->stream));
-    k_guard_reset<<<1, 256, 0, ctx->stream>>>(gs.d_tab, R, gs.xmax, gs.rmax);
-    check_launch(ctx);
-    const dim3 rg((unsigned)R, std::max(1, std::min(ceil_div(nmax_refine, 8), 64)));
-    k_guard_probe_xv<<<rg, 256, 0, ctx->stream>>>(gs.d_tab, gs.xmax);
-    check_launch(ctx);
-    k_guard_probe_res<<<rg, 256, 0, ctx->stream>>>(gs.d_tab, gs.rmax);
-    check_launch(ctx);
-    QX_CUDA(cudaMemcpyAsync(xmax.data(), gs.xmax, gs.nall * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
-                            ctx->stream));
-    QX_CUDA(cudaMemcpyAsync(rmax.data(), gs.rmax, gs.nall * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
-                            ctx->stream));
-    QX_CUDA(cudaStreamSynchronize(ctx->stream));
-    std::vector<GuardMat> again;
-    for (const GuardMat& g : refine) {
-      const double eta = as_double(rmax[g.idx]) / ((double)g.n * as_double(amax[g.idx]) * as_double(xmax[g.idx]));
-      if (!(eta <= kGuardResidual)) again.push_back(g);
-    }
-    refine.swap(again);
-  }
-  for (const GuardMat& g : refine) {  // not converged: pivoting after all
-    flagged.push_back(g);
-    nmax = std::max(nmax, g.n);
   }
   gs.nflagged = (int)flagged.size();
+  ctx->guard_matrices += G;
   ctx->guard_reinverted += gs.nflagged;
   if (flagged.empty()) return 0;
   const int F = (int)flagged.size();

@@ -162,7 +162,6 @@ enum WsSlot {
   WS_GRAD0, WS_GRAD1, WS_GRAD2,  // CD adjoint: accumulators, per-frequency chunk, lpq gradient
   WS_SWEEP_SPLIT,  // split sweep panels (two steps in flight)
   WS_GUARD,        // guarded inversion: copies of eps and the pivoted fallback's work arrays
-  WS_NS,           // Newton-Schulz refinement of flagged matrices: two n x ldn products
   WS_COUNT
 };
 static_assert(WS_COUNT <= 40, "workspace slots");
@@ -247,11 +246,6 @@ constexpr double kGuardGrowth = 1e4;
 // Probe backward error max|eps X v - v| / (n max|eps| max|X|) above which the
 // sweep's inverse is redone with pivoting (a stable inverse gives ~1e-17).
 constexpr double kGuardResidual = 1e-15;
-// A flagged matrix whose probe residual max|eps X v - v| is below
-// kRefineResidual is refined by Newton-Schulz (up to kRefineSteps steps,
-// each squaring the residual) before any pivoted re-inversion.
-constexpr double kRefineResidual = 1e-3;
-constexpr int kRefineSteps = 2;
 
 // One guarded matrix.  The caller sets M, n, ldn, idx and status;
 // guard_layout places bk, ints and rbuf.
