@@ -303,8 +303,18 @@ __global__ void __launch_bounds__(512) k_piv_panel_reg(const GuardMat* __restric
     freer[i] = live && gstate[r] < 0;
     mine[i] = false;
     const double* src = g.bk + (size_t)(live ? r : 0) * g.ldn + k0;
+    if (live && kb == PIV_NB && (g.ldn & 1) == 0) {
+      // bk is 256-byte aligned, k0 a multiple of 16 and ldn even: 16-byte pairs.
 #pragma unroll
-    for (int c = 0; c < PIV_NB; ++c) v[i][c] = (live && c < kb) ? src[c] : 0.0;
+      for (int c = 0; c < PIV_NB; c += 2) {
+        const double2 x = __ldg(reinterpret_cast<const double2*>(src + c));
+        v[i][c] = x.x;
+        v[i][c + 1] = x.y;
+      }
+    } else {
+#pragma unroll
+      for (int c = 0; c < PIV_NB; ++c) v[i][c] = (live && c < kb) ? src[c] : 0.0;
+    }
   }
   // This thread's candidate for column 0.
   double best = -1.0;
@@ -318,80 +328,93 @@ __global__ void __launch_bounds__(512) k_piv_panel_reg(const GuardMat* __restric
       bi = r;
     }
   }
-#pragma unroll
+  // One pivot step per iteration, not unrolled (sixteen unrolled copies of
+  // the step missed the instruction cache: "no instruction" was the top
+  // stall).  The registers rotate by one column per step instead, so the
+  // step's column is always v[.][0] and every register index stays a
+  // compile-time constant; after PIV_NB steps the columns are back in order
+  // (steps past kb only rotate).
+#pragma unroll 1
   for (int j = 0; j < PIV_NB; ++j) {
-    if (j >= kb) break;  // uniform
-    const int sl = j & 1;
-    // Warp argmax, then the owner of the warp's best row publishes it.
-    double wv = best;
-    int wr = bi;
-    for (int o = 16; o > 0; o >>= 1) {
-      const double ov = __shfl_xor_sync(0xffffffffu, wv, o);
-      const int orr = __shfl_xor_sync(0xffffffffu, wr, o);
-      if (ov > wv || (ov == wv && orr < wr)) {
-        wv = ov;
-        wr = orr;
+    if (j < kb) {  // uniform
+      const int sl = j & 1;
+      // Warp argmax, then the owner of the warp's best row publishes it.
+      double wv = best;
+      int wr = bi;
+      for (int o = 16; o > 0; o >>= 1) {
+        const double ov = __shfl_xor_sync(0xffffffffu, wv, o);
+        const int orr = __shfl_xor_sync(0xffffffffu, wr, o);
+        if (ov > wv || (ov == wv && orr < wr)) {
+          wv = ov;
+          wr = orr;
+        }
       }
-    }
-    if (lane == 0) {
-      slot_val[sl][warp] = wv;
-      slot_idx[sl][warp] = wr;
-    }
-#pragma unroll
-    for (int i = 0; i < RPT; ++i)
-      if (wr != INT_MAX && threadIdx.x + 512 * i == wr) {
-#pragma unroll
-        for (int c = 0; c < PIV_NB; ++c) slot_row[sl][warp][c] = v[i][c];
+      if (lane == 0) {
+        slot_val[sl][warp] = wv;
+        slot_idx[sl][warp] = wr;
       }
-    __syncthreads();
-    double gv = slot_val[sl][0];
-    int gr = slot_idx[sl][0], gw = 0;
 #pragma unroll
-    for (int k = 1; k < NWARP; ++k) {
-      const double ov = slot_val[sl][k];
-      const int orr = slot_idx[sl][k];
-      if (ov > gv || (ov == gv && orr < gr)) {
-        gv = ov;
-        gr = orr;
-        gw = k;
+      for (int i = 0; i < RPT; ++i)
+        if (wr != INT_MAX && threadIdx.x + 512 * i == wr) {
+#pragma unroll
+          for (int c = 0; c < PIV_NB; ++c) slot_row[sl][warp][c] = v[i][c];
+        }
+      __syncthreads();
+      double gv = slot_val[sl][0];
+      int gr = slot_idx[sl][0], gw = 0;
+#pragma unroll
+      for (int k = 1; k < NWARP; ++k) {
+        const double ov = slot_val[sl][k];
+        const int orr = slot_idx[sl][k];
+        if (ov > gv || (ov == gv && orr < gr)) {
+          gv = ov;
+          gr = orr;
+          gw = k;
+        }
       }
-    }
-    const int p = gr;
-    const double d = (p == INT_MAX) ? 0.0 : slot_row[sl][gw][j];
-    if (!(fabs(d) > 0.0) || !isfinite(d)) {  // uniform
-      if (threadIdx.x == 0) *g.status = 1;
-      return;
-    }
-    if (threadIdx.x == 0) {
-      piv[k0 + j] = p;
-      pivs[j] = p;
-    }
-    const double inv = 1.0 / d;
-    double pr[PIV_NB];
-#pragma unroll
-    for (int c = 0; c < PIV_NB; ++c) pr[c] = slot_row[sl][gw][c];
-    best = -1.0;
-    bi = INT_MAX;
-#pragma unroll
-    for (int i = 0; i < RPT; ++i) {
-      const int r = threadIdx.x + 512 * i;
-      if (r == p) {
-#pragma unroll
-        for (int c = 0; c < PIV_NB; ++c) v[i][c] = (c == j) ? inv : -pr[c] * inv;
-        freer[i] = false;
-        mine[i] = true;
-      } else {
-        const double t = v[i][j] * inv;
-#pragma unroll
-        for (int c = 0; c < PIV_NB; ++c) v[i][c] = (c == j) ? t : v[i][c] - t * pr[c];
+      const int p = gr;
+      const double d = (p == INT_MAX) ? 0.0 : slot_row[sl][gw][0];
+      if (!(fabs(d) > 0.0) || !isfinite(d)) {  // uniform
+        if (threadIdx.x == 0) *g.status = 1;
+        return;
       }
-      if (j + 1 < PIV_NB) {
-        const double a = fabs(v[i][(j + 1) % PIV_NB]);
+      if (threadIdx.x == 0) {
+        piv[k0 + j] = p;
+        pivs[j] = p;
+      }
+      const double inv = 1.0 / d;
+      double pr[PIV_NB];
+#pragma unroll
+      for (int c = 0; c < PIV_NB; ++c) pr[c] = slot_row[sl][gw][c];
+      best = -1.0;
+      bi = INT_MAX;
+#pragma unroll
+      for (int i = 0; i < RPT; ++i) {
+        const int r = threadIdx.x + 512 * i;
+        if (r == p) {
+#pragma unroll
+          for (int c = 0; c < PIV_NB; ++c) v[i][c] = (c == 0) ? inv : -pr[c] * inv;
+          freer[i] = false;
+          mine[i] = true;
+        } else {
+          const double t = v[i][0] * inv;
+#pragma unroll
+          for (int c = 0; c < PIV_NB; ++c) v[i][c] = (c == 0) ? t : v[i][c] - t * pr[c];
+        }
+        // The next step's column is v[.][1] (before the rotation below).
+        const double a = fabs(v[i][1]);
         if (freer[i] && (a > best || (a == best && r < bi))) {
           best = a;
           bi = r;
         }
       }
+    }
+#pragma unroll
+    for (int i = 0; i < RPT; ++i) {
+      const double t0 = v[i][0];
+#pragma unroll
+      for (int c = 0; c + 1 < PIV_NB; ++c) v[i][c] = v[i][c + 1];
+      v[i][PIV_NB - 1] = t0;
     }
   }
   // Write the panel back, then the old pivot rows of the super-panel's other
@@ -401,9 +424,14 @@ __global__ void __launch_bounds__(512) k_piv_panel_reg(const GuardMat* __restric
     const int r = threadIdx.x + 512 * i;
     if (r >= n) continue;
     double* row = g.bk + (size_t)r * g.ldn + k0;
+    if (kb == PIV_NB && (g.ldn & 1) == 0) {
 #pragma unroll
-    for (int c = 0; c < PIV_NB; ++c)
-      if (c < kb) row[c] = v[i][c];
+      for (int c = 0; c < PIV_NB; c += 2) *reinterpret_cast<double2*>(row + c) = make_double2(v[i][c], v[i][c + 1]);
+    } else {
+#pragma unroll
+      for (int c = 0; c < PIV_NB; ++c)
+        if (c < kb) row[c] = v[i][c];
+    }
     if (mine[i]) gstate[r] = k0;
   }
   const int ks = (k0 / PIV_SB) * PIV_SB, ce = min(ks + PIV_SB, n);
