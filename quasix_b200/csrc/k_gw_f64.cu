@@ -126,39 +126,45 @@ constexpr int SWEEP_NB = 128;
 // swept after each pivot step (the element growth of the elimination).
 template <bool GUARD>
 __device__ __forceinline__ void sweep32_warp(double* S, int q0, int lane, bool& bad_any, double tol, double& gm) {
-  // r[i] holds S[q0 + i][q0 + lane]; both loops are unrolled, so every
-  // register index is a compile-time constant.  Per pivot p the lanes other
-  // than p take r[i] - S[i][p] S[p][lane] / d and lane p takes S[i][p] / d,
-  // both as one FMA: fma(ci, b, r[i] * a) with (a, b) = (1, -rj) or (0, inv).
-  double r[32];
+  // c[k] holds S[(p + k) % 32][lane] at pivot step p: the pivot row is always
+  // c[0] and the array rotates by one after each step, so every register index
+  // is a compile-time constant without unrolling the pivot loop (an unrolled
+  // loop of 32 steps measured slower: it misses the instruction cache).  The
+  // lanes other than p take c[i] - S[p+i][p] S[p][lane] / d and lane p takes
+  // S[p+i][p] / d, both as one FMA: fma(ci, b, c[i] * a) with (a, b) = (1, -rj)
+  // or (0, inv).
+  double c[32];
 #pragma unroll
-  for (int i = 0; i < 32; ++i) r[i] = S[(q0 + i) * SWEEP_NB + q0 + lane];
-#pragma unroll
+  for (int i = 0; i < 32; ++i) c[i] = S[(q0 + i) * SWEEP_NB + q0 + lane];
+#pragma unroll 1
   for (int p = 0; p < 32; ++p) {
-    const double d = __shfl_sync(0xffffffffu, r[p], p);
+    const double d = __shfl_sync(0xffffffffu, c[0], p);
     const bool bad = !(fabs(d) > tol) || !isfinite(d);
     bad_any |= bad;
     const double inv = bad ? 0.0 : 1.0 / d;
-    const double rj = r[p] * inv;  // S[p][lane] / d
+    const double rj = c[0] * inv;  // S[p][lane] / d
     const bool piv = (lane == p);
     const double a = piv ? 0.0 : 1.0, b = piv ? inv : -rj;
 #pragma unroll
-    for (int i = 0; i < 32; ++i) {
-      if (i == p) continue;
-      const double ci = __shfl_sync(0xffffffffu, r[i], p);  // S[i][p]
-      r[i] = fma(ci, b, r[i] * a);
+    for (int i = 1; i < 32; ++i) {
+      const double ci = __shfl_sync(0xffffffffu, c[i], p);  // S[p + i][p]
+      c[i] = fma(ci, b, c[i] * a);
     }
-    r[p] = piv ? -inv : rj;
+    c[0] = piv ? -inv : rj;
     // Growth of the columns not yet swept, sampled every eighth pivot (the
     // serial pivot chain is this kernel's bound; the probe backward error of
     // the guard catches any loss between samples).
     if (GUARD && (p & 7) == 7 && lane > p) {
 #pragma unroll
-      for (int i = 0; i < 32; ++i) gm = fmax(gm, isfinite(r[i]) ? fabs(r[i]) : INFINITY);
+      for (int i = 0; i < 32; ++i) gm = fmax(gm, isfinite(c[i]) ? fabs(c[i]) : INFINITY);
     }
+    const double t = c[0];
+#pragma unroll
+    for (int i = 0; i < 31; ++i) c[i] = c[i + 1];
+    c[31] = t;
   }
 #pragma unroll
-  for (int i = 0; i < 32; ++i) S[(q0 + i) * SWEEP_NB + q0 + lane] = r[i];
+  for (int i = 0; i < 32; ++i) S[(q0 + i) * SWEEP_NB + q0 + lane] = c[i];
 }
 
 // D = -(A_KK)^-1 for the kb x kb diagonal block whose first element is at
