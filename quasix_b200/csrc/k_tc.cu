@@ -209,7 +209,18 @@ struct TcSmem {
   static constexpr int BAR_OFF = F32_OFF + (CONVB ? F32_STAGES * F32_BYTES : 0);
   static constexpr int RED_OFF = BAR_OFF + 256;  // ROWDOT: partial row sums [2][128] doubles + 2 flags
   // ROWDOT: two buffers of [2][128] doubles + 2 flags (8 doubles), alternating per item.
-  static constexpr int TOTAL = RED_OFF + (EPI == EPI_ROWDOT ? 2 * (2 * TC_BM + 8) * 8 : 0) + 1024;  // + slack
+  static constexpr int CS_OFF = RED_OFF + (EPI == EPI_ROWDOT ? 2 * (2 * TC_BM + 8) * 8 : 0);
+  // UPDATE: the FP32 tile C, staged for the coalesced row passes of the
+  // read-modify-write (row stride CS_LD floats against bank conflicts).
+  static constexpr int CS_LD = BN + 1;
+  static constexpr int CS_BYTES = EPI == EPI_UPDATE ? TC_BM * CS_LD * 4 : 0;
+  // UPDATE, grouped: a shared-memory copy of the prefix table of CTA counts
+  // (up to GP_CAP matrices), so that finding a tile's matrix costs no
+  // dependent global loads.
+  static constexpr int GP_CAP = 2048;
+  static constexpr int GP_OFF = CS_OFF + CS_BYTES;
+  static constexpr int GP_BYTES = EPI == EPI_UPDATE ? GP_CAP * 4 : 0;
+  static constexpr int TOTAL = GP_OFF + GP_BYTES + 1024;  // + slack for the 1024-byte alignment
 };
 
 struct TcArgs {
@@ -246,6 +257,7 @@ struct TcArgs {
   const GMat* gmats;
   const int* gpre;
   int gcount;
+  int items;  // tiles of the grouped table (the item count with gmats)
   int unit;  // STORE: k-blocks per FP32 accumulation unit (0 counts as 1)
   // CONVB: B[w][n][k] = convB[n][k] * convC[w][k] (FP32, zero past K): the
   // FP32 tile of convB arrives by TMA (map in the mapBh slot), and the
@@ -284,6 +296,14 @@ __device__ __forceinline__ double unscale_rowdot(const TcArgs& a, int w) {
   return 1.0 / ((double)a.scaleA[0] * (double)a.scaleB[w]);
 }
 
+// A STORE / UPDATE output tile: 128-row block mb and BN-column tile nt of
+// the matrix out (leading dimension ld, outM x outN; out already points at
+// frequency w), whose operand rows start at row_off (grouped panels).
+struct StoreTile {
+  int mb, nt, w, row_off, outM, outN, ld;
+  double* out;
+};
+
 template <int BN, int EPI, bool CONVB = false>
 __global__ void __launch_bounds__(TcThreads<EPI, CONVB>::VALUE, 1)
     k_tc_gemm(const __grid_constant__ CUtensorMap mapAh, const __grid_constant__ CUtensorMap mapAl,
@@ -307,19 +327,21 @@ __global__ void __launch_bounds__(TcThreads<EPI, CONVB>::VALUE, 1)
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
-  // CTA -> (m block, batch, n tile range).
-  int mb, w, nt_begin, nt_end;
-  GMat gmat{};
   const int n_tiles = (args.N + BN - 1) / BN;
-  // ROWDOT is persistent: CTA b takes the items b, b + gridDim.x, ... of
-  // the (pair block, frequency) sequence, ordered so that the frequencies of
-  // a group of wgroup share each pair block while it is in L2; TMEM buffers,
-  // stages and barrier phases run on across items, so the epilogue of one
-  // item overlaps the MMAs of the next.  The other forms take one item.
-  const int n_items =
-      (EPI == EPI_ROWDOT) ? (args.nbatch + args.wgroup - 1) / args.wgroup * args.m_blocks * args.wgroup : 1;
-  const int item0 = (EPI == EPI_ROWDOT) ? (int)blockIdx.x : 0;
-  const int item_step = (EPI == EPI_ROWDOT) ? (int)gridDim.x : 1;
+  const int k_blocks = (args.K + TC_BK - 1) / TC_BK;
+  // Items.  ROWDOT: (pair block, frequency), ordered so that the frequencies
+  // of a group of wgroup share each pair block while it is in L2.  STORE and
+  // UPDATE: (frequency, output tile), or a tile of the grouped table.  CTA b
+  // of a grid of G CTAs takes the items b, b + G, ...: a persistent grid (one
+  // CTA per SM) runs many, a grid of one CTA per item runs one.  TMEM
+  // buffers, stages and barrier phases run on across items, so the epilogue
+  // of one item overlaps the loads and MMAs of the next.
+  const int tiles_pb = args.lower_tiles ? args.m_blocks * (args.m_blocks + 1) / 2 : args.m_blocks * n_tiles;
+  const int n_items = (EPI == EPI_ROWDOT)
+                          ? (args.nbatch + args.wgroup - 1) / args.wgroup * args.m_blocks * args.wgroup
+                          : (args.gmats ? args.items : tiles_pb * args.nbatch);
+  const int item0 = (int)(blockIdx.x + blockIdx.y * gridDim.x);
+  const int item_step = (int)(gridDim.x * gridDim.y);
   auto rowdot_item = [&](int b, int& mb_, int& w_) {
     const int g = args.wgroup;
     const int per_group = args.m_blocks * g;
@@ -327,60 +349,72 @@ __global__ void __launch_bounds__(TcThreads<EPI, CONVB>::VALUE, 1)
     mb_ = r / g;
     w_ = grp * g + r % g;
   };
-  if (EPI == EPI_ROWDOT) {
-    mb = 0;
-    w = 0;
-    nt_begin = 0;
-    nt_end = n_tiles;
-  } else {
-    w = blockIdx.y;
+  // STORE / UPDATE item -> output tile; false when the tile is left alone
+  // (the sweep update's pivot row and column, and the look-ahead filter).
+  const bool gp_shared = EPI == EPI_UPDATE && args.gmats && args.gcount <= L::GP_CAP;
+  const int* gpre = args.gpre;
+  if (gp_shared) {
+    int* gs = reinterpret_cast<int*>(smem + L::GP_OFF);
+    for (int i = threadIdx.x; i < args.gcount; i += blockDim.x) gs[i] = __ldg(args.gpre + i);
+    gpre = gs;
+    __syncthreads();
+  }
+  auto tile_item = [&](int it, StoreTile& t) -> bool {
+    int r = it, tm, tn;
+    t.w = 0;
     if (args.gmats) {
       int lo = 0, hi = args.gcount - 1;
       while (lo < hi) {
         const int mid = (lo + hi + 1) >> 1;
-        if (__ldg(args.gpre + mid) <= (int)blockIdx.x)
+        if (gpre[mid] <= it)
           lo = mid;
         else
           hi = mid - 1;
       }
-      gmat = args.gmats[lo];
-      const int t = blockIdx.x - args.gpre[lo];
-      int tm = (int)floor((sqrt(8.0 * t + 1.0) - 1.0) * 0.5);
-      while ((tm + 1) * (tm + 2) / 2 <= t) ++tm;
-      while (tm * (tm + 1) / 2 > t) --tm;
-      mb = tm;
-      nt_begin = t - tm * (tm + 1) / 2;
-    } else if (args.lower_tiles) {
-      const int t = blockIdx.x;
-      int tm = (int)floor((sqrt(8.0 * t + 1.0) - 1.0) * 0.5);
-      while ((tm + 1) * (tm + 2) / 2 <= t) ++tm;
-      while (tm * (tm + 1) / 2 > t) --tm;
-      mb = tm;
-      nt_begin = t - tm * (tm + 1) / 2;
+      const GMat gm = args.gmats[lo];
+      r = it - gpre[lo];
+      t.row_off = gm.prow;
+      t.outM = t.outN = gm.n;
+      t.ld = gm.ldn;
+      t.out = gm.M;
     } else {
-      mb = blockIdx.x / n_tiles;
-      nt_begin = blockIdx.x % n_tiles;
+      t.w = it / tiles_pb;
+      r = it - t.w * tiles_pb;
+      t.row_off = 0;
+      t.outM = args.M;
+      t.outN = args.N;
+      t.ld = args.ldo;
+      t.out = args.out + (size_t)t.w * args.out_stride;
     }
-    nt_end = nt_begin + 1;
-  }
-  if (EPI != EPI_ROWDOT && args.subtract) {
-    // Whole-CTA exit before any barrier or TMEM allocation.
-    if (mb == args.skip_tile || nt_begin == args.skip_tile) return;
-    if (args.filter_mode) {
-      const bool touches = (mb == args.filter_tile || nt_begin == args.filter_tile);
-      if (touches != (args.filter_mode == 1)) return;
+    if (args.gmats || args.lower_tiles) {
+      tm = (int)floor((sqrt(8.0 * r + 1.0) - 1.0) * 0.5);
+      while ((tm + 1) * (tm + 2) / 2 <= r) ++tm;
+      while (tm * (tm + 1) / 2 > r) --tm;
+      tn = r - tm * (tm + 1) / 2;
+    } else {
+      tm = r / n_tiles;
+      tn = r - tm * n_tiles;
     }
+    t.mb = tm;
+    t.nt = tn;
+    if (args.subtract) {
+      if (tm == args.skip_tile || tn == args.skip_tile) return false;
+      if (args.filter_mode) {
+        const bool touches = (tm == args.filter_tile || tn == args.filter_tile);
+        if (touches != (args.filter_mode == 1)) return false;
+      }
+    }
+    return true;
+  };
+  // The first item of this CTA with work (CONVB runs exactly one item per
+  // CTA and takes its frequency and tile from it); a CTA without any exits
+  // before any barrier or TMEM allocation.
+  StoreTile t0{};
+  if (EPI != EPI_ROWDOT) {
+    int it = item0;
+    while (it < n_items && !tile_item(it, t0)) it += item_step;
+    if (it >= n_items) return;
   }
-  const bool active = (w < args.nbatch);
-  const int m0 = mb * TC_BM;
-  // STORE output shape and the panel row offsets of a grouped matrix.
-  const bool grouped = (EPI != EPI_ROWDOT) && args.gmats != nullptr;
-  const int outM = grouped ? gmat.n : args.M, outN = grouped ? gmat.n : args.N;
-  const int out_ld = grouped ? gmat.ldn : args.ldo;
-  const size_t out_stride = grouped ? 0 : args.out_stride;
-  double* const out_base = grouped ? gmat.M : args.out;
-  const int row_off = grouped ? gmat.prow : 0;
-  const int k_blocks = (args.K + TC_BK - 1) / TC_BK;
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < TC_STAGES; ++s) {
@@ -411,20 +445,30 @@ __global__ void __launch_bounds__(TcThreads<EPI, CONVB>::VALUE, 1)
   tc_fence_after();
   const uint32_t tmem_base = *tmem_slot;
 
-  if (active) {
+  {
     if (warp == 0) {
       // ---------------- TMA producer ----------------
       if (lane == 0) {
         int g = 0;
         int issued = 0;
         for (int it = item0; it < n_items; it += item_step) {
-        int mi = mb, wi = w;
+        int mi, wi, ntb, nte, row_off = 0;
         if (EPI == EPI_ROWDOT) {
           rowdot_item(it, mi, wi);
           if (wi >= args.nbatch) continue;
+          ntb = 0;
+          nte = n_tiles;
+        } else {
+          StoreTile ti;
+          if (!tile_item(it, ti)) continue;
+          mi = ti.mb;
+          wi = ti.w;
+          ntb = ti.nt;
+          nte = ti.nt + 1;
+          row_off = ti.row_off;
         }
         const int mi0 = mi * TC_BM;
-        for (int nt = nt_begin; nt < nt_end; ++nt) {
+        for (int nt = ntb; nt < nte; ++nt) {
           const int n0 = nt * BN;
           const int kbe = args.tri ? min(k_blocks, (n0 + BN + TC_BK - 1) / TC_BK) : k_blocks;
           for (int kb = 0; kb < kbe; ++kb, ++g) {
@@ -471,12 +515,20 @@ __global__ void __launch_bounds__(TcThreads<EPI, CONVB>::VALUE, 1)
         int g = 0, u = 0;
         bool ok = true;
         for (int it = item0; it < n_items && ok; it += item_step) {
+        int ntb, nte;
         if (EPI == EPI_ROWDOT) {
           int mi, wi;
           rowdot_item(it, mi, wi);
           if (wi >= args.nbatch) continue;
+          ntb = 0;
+          nte = n_tiles;
+        } else {
+          StoreTile ti;
+          if (!tile_item(it, ti)) continue;
+          ntb = ti.nt;
+          nte = ti.nt + 1;
         }
-        for (int nt = nt_begin; nt < nt_end && ok; ++nt) {
+        for (int nt = ntb; nt < nte && ok; ++nt) {
           const int kbe = args.tri ? min(k_blocks, (nt * BN + BN + TC_BK - 1) / TC_BK) : k_blocks;
           for (int kb = 0; kb < kbe; ++kb, ++g) {
             const int unit = args.unit > 0 ? args.unit : 1;
@@ -537,7 +589,7 @@ __global__ void __launch_bounds__(TcThreads<EPI, CONVB>::VALUE, 1)
       const int ct = threadIdx.x - 32 * (2 + TcWarps<EPI>::NEPI);
       const int cc = ct & 7, rg = ct >> 3;
       constexpr int ROWS_PER_PASS = 4 * kConvWarps;  // row groups of 8 chunk threads
-      const float* cw_scale = args.convC + (size_t)w * args.ldcc + 8 * cc;
+      const float* cw_scale = args.convC + (size_t)t0.w * args.ldcc + 8 * cc;
       // Column scales of the next k block, loaded one block ahead.
       float4 cn0 = make_float4(0.f, 0.f, 0.f, 0.f), cn1 = cn0;
       if (8 * cc < args.K) {
@@ -545,7 +597,7 @@ __global__ void __launch_bounds__(TcThreads<EPI, CONVB>::VALUE, 1)
         cn1 = __ldg(reinterpret_cast<const float4*>(cw_scale + 4));
       }
       const int h = cc >> 2, q0 = 2 * (cc & 3);
-      const int n0 = nt_begin * BN;
+      const int n0 = t0.nt * BN;
       constexpr int FS = L::F32_STAGES;
       // Converter thread 0 keeps the FP32 ring FS blocks ahead.
       auto issue_f32 = [&](int kb) {
@@ -665,7 +717,7 @@ __global__ void __launch_bounds__(TcThreads<EPI, CONVB>::VALUE, 1)
         const int m = mi * TC_BM + row;
         double rowsum = 0.0;
         int tiles_done = 0;
-        for (int nt = nt_begin; nt < nt_end; ++nt, ++t) {
+        for (int nt = 0; nt < n_tiles; ++nt, ++t) {
           const int buf = t & 1;
           if (!mbar_wait(&acc_full[buf], (t / 2) & 1, abort_flag, args.err, 4)) {
             ok = false;
@@ -703,7 +755,7 @@ __global__ void __launch_bounds__(TcThreads<EPI, CONVB>::VALUE, 1)
         // i + 1, which every reader of item i has passed.
         double* red = reinterpret_cast<double*>(smem + L::RED_OFF) + (done_items & 1) * (2 * TC_BM + 8);
         int* done = reinterpret_cast<int*>(red + 2 * TC_BM);  // two flags after the sums
-        const bool full_item = tiles_done == nt_end - nt_begin;
+        const bool full_item = tiles_done == n_tiles;
         red[half * TC_BM + row] = full_item ? rowsum : 0.0;
         if (lane == 0 && quarter == 0) done[half] = full_item ? 1 : 0;
         asm volatile("bar.sync 1, 256;\n" ::: "memory");
@@ -719,124 +771,158 @@ __global__ void __launch_bounds__(TcThreads<EPI, CONVB>::VALUE, 1)
       constexpr int CPW = BN * 4 / TcWarps<EPI>::NEPI;  // columns per epilogue warp
       const int quarter = warp & 3;
       const int part = (warp - 2) >> 2;  // columns [CPW part, CPW part + CPW) of the tile
-      const int m = m0 + quarter * 32 + lane;
-      const double unscale = 1.0 / ((double)args.scaleA[args.a_batched ? w : 0] * (double)args.scaleB[w]);
-      double acc[CPW];
-#pragma unroll
-      for (int c = 0; c < CPW; ++c) acc[c] = 0.0;
-      bool ok = true;
       const int unit = args.unit > 0 ? args.unit : 1;
       const int n_units = (k_blocks + unit - 1) / unit;
-      for (int u = 0; u < n_units; ++u) {
-        const int buf = u & 1;
-        if (!mbar_wait(&acc_full[buf], (u / 2) & 1, abort_flag, args.err, 4)) {
-          ok = false;
-          break;
+      // After a failed wait a warp waits no more but still passes the named
+      // barriers of every later item, as the other epilogue warps do.
+      bool ok = true;
+      int u = 0;
+      int it = item0;
+      StoreTile ti;
+      while (it < n_items && !tile_item(it, ti)) it += item_step;
+      while (it < n_items) {
+        // UPDATE: the next item of this CTA is decoded now, so that its table
+        // loads are in flight during this item's work (STORE, with its FP64
+        // accumulators live, decodes it after the item).
+        int nit = it + item_step;
+        StoreTile tnext;
+        if (EPI == EPI_UPDATE)
+          while (nit < n_items && !tile_item(nit, tnext)) nit += item_step;
+        const int m0 = ti.mb * TC_BM;
+        const int m = m0 + quarter * 32 + lane;
+        const double unscale =
+            1.0 / ((double)args.scaleA[args.a_batched ? ti.w : 0] * (double)args.scaleB[ti.w]);
+        double acc[CPW];
+#pragma unroll
+        for (int c = 0; c < CPW; ++c) acc[c] = 0.0;
+        for (int uu = 0; uu < n_units; ++uu, ++u) {
+          const int buf = u & 1;
+          if (!ok || !mbar_wait(&acc_full[buf], (u / 2) & 1, abort_flag, args.err, 4)) {
+            ok = false;
+            continue;
+          }
+          tc_fence_after();
+          const uint32_t taddr = tmem_base + ((uint32_t)(quarter * 32) << 16) + buf * BN + CPW * part;
+#pragma unroll
+          for (int j = 0; j < CPW / 16; ++j) {
+            // Columns past N (a narrow GEMM, e.g. a few vectors) are not
+            // drained; the condition is warp-uniform.
+            if (ti.nt * BN + CPW * part + 16 * j >= ti.outN) continue;
+            float v[16];
+            tmem_ld16(taddr + 16 * j, v);
+#pragma unroll
+            for (int q = 0; q < 16; ++q) acc[16 * j + q] += (double)v[q];
+          }
+          tc_fence_before();
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&acc_empty[buf]);
         }
-        tc_fence_after();
-        const uint32_t taddr = tmem_base + ((uint32_t)(quarter * 32) << 16) + buf * BN + CPW * part;
+        if (EPI == EPI_UPDATE) {
+          // One FP32 accumulation unit covers K here (the launchers ask for
+          // it), so the tile C is exactly FP32.  It is staged in its own
+          // shared-memory area (the stages already hold the next item's
+          // operands), then the lower tile and its mirror are updated in
+          // row-wise passes that are coalesced along the rows of M; the mirror
+          // reads its old value from the upper element itself, M being stored
+          // exactly symmetric.  After an abort nothing more is written.
+          constexpr int CLD = L::CS_LD;
+          float* Cs = reinterpret_cast<float*>(smem + L::CS_OFF);
+          const int rl = quarter * 32 + lane;
+          if (ok) {
 #pragma unroll
-        for (int j = 0; j < CPW / 16; ++j) {
-          // Columns past N (a narrow GEMM, e.g. a few vectors) are not
-          // drained; the condition is warp-uniform.
-          if (nt_begin * BN + CPW * part + 16 * j >= outN) continue;
-          float v[16];
-          tmem_ld16(taddr + 16 * j, v);
-#pragma unroll
-          for (int q = 0; q < 16; ++q) acc[16 * j + q] += (double)v[q];
-        }
-        tc_fence_before();
-        __syncwarp();
-        if (lane == 0) mbar_arrive(&acc_empty[buf]);
-      }
-      if (EPI == EPI_UPDATE) {
-        // One FP32 accumulation unit covers K here (the launchers ask for
-        // it), so the tile C is exactly FP32.  It is staged in the drained
-        // stage buffers, then the lower tile and its mirror are updated in
-        // row-wise passes that are coalesced along the rows of M; the mirror
-        // reads its old value from the upper element itself, M being stored
-        // exactly symmetric.  Every epilogue thread reaches the barrier; after
-        // an abort nothing is written.
-        constexpr int CLD = BN + 1;
-        static_assert(TC_BM * CLD * 4 <= TC_STAGES * L::STAGE_BYTES, "staged tile fits the stage buffers");
-        float* Cs = reinterpret_cast<float*>(smem);
-        const int rl = quarter * 32 + lane;
-#pragma unroll
-        for (int c = 0; c < CPW; ++c) Cs[rl * CLD + CPW * part + c] = (float)acc[c];
-        asm volatile("bar.sync 1, 256;\n" ::: "memory");
-        if (!*abort_flag) {
-          // Warp e takes rows e, e + 8, ... of each pass, RB = 8 at a time, and
-          // issues all 32 loads of a lane before its stores, so that enough
-          // bytes are in flight per SM for HBM (4 and 16 rows measured slower).
-          constexpr int RB = 8;
-          const int e = warp - 2;
-          const int nb = nt_begin * BN;
-          double* outw = out_base + (size_t)w * out_stride;
-          static_assert(EPI != EPI_UPDATE || (TC_BM == 128 && BN == 128), "row passes assume 128 x 128 tiles");
-          // Lower tile: row mm = m0 + r, columns n = nb + lane + 32 q, n <= mm.
-#pragma unroll 1
-          for (int r0 = e; r0 < TC_BM; r0 += 8 * RB) {
-            double x[RB][4];
-#pragma unroll
-            for (int k = 0; k < RB; ++k) {
-              const int mm = m0 + r0 + 8 * k;
-#pragma unroll
-              for (int q = 0; q < 4; ++q) {
-                const int n = nb + lane + 32 * q;
-                x[k][q] = (mm < outM && n < outN && n <= mm) ? outw[(size_t)mm * out_ld + n] : 0.0;
+            for (int c = 0; c < CPW; ++c) Cs[rl * CLD + CPW * part + c] = (float)acc[c];
+          }
+          asm volatile("bar.sync 1, 256;\n" ::: "memory");
+          if (ok && !*abort_flag) {
+            // Warp e updates eight batches of RB = 4 rows: rows e + 32 b + 8 k
+            // of the lower tile (b < 4), then rows nb + e + 32 (b - 4) + 8 k of
+            // the mirror in the upper tile (b >= 4), each row 128 coalesced
+            // doubles.  The loads of batch b + 1 are issued before the stores
+            // of batch b: with all warps passing the tile's barriers together,
+            // loads followed by stores in lockstep kept only half of HBM busy
+            // (3.4 against 6.1 TB/s pipelined, measured on this access pattern
+            // alone; two batches of 4 rows fit the 168 registers of the
+            // 320-thread CTA).  The lower and mirror elements are disjoint, so
+            // no store of a batch aliases a later load.
+            constexpr int RB = 4, NBT = 8;
+            const int e = warp - 2;
+            const int nb = ti.nt * BN;
+            const int outM = ti.outM, outN = ti.outN, out_ld = ti.ld;
+            double* outw = ti.out;
+            static_assert(EPI != EPI_UPDATE || (TC_BM == 128 && BN == 128), "row passes assume 128 x 128 tiles");
+            auto elem = [&](int b, int k, int q, bool& v) -> double* {
+              if (b < NBT / 2) {
+                const int mm = m0 + e + 32 * b + 8 * k, n = nb + lane + 32 * q;
+                v = mm < outM && n < outN && n <= mm;
+                return outw + (size_t)mm * out_ld + n;
               }
-            }
+              const int n = nb + e + 32 * (b - NBT / 2) + 8 * k, mm = m0 + lane + 32 * q;
+              v = mm < outM && n < outN && n < mm;
+              return outw + (size_t)n * out_ld + mm;
+            };
+            auto cval = [&](int b, int k, int q) -> double {
+              return (double)(b < NBT / 2 ? Cs[(e + 32 * b + 8 * k) * CLD + lane + 32 * q]
+                                          : Cs[(lane + 32 * q) * CLD + e + 32 * (b - NBT / 2) + 8 * k]);
+            };
+            double x[RB][4], y[RB][4];
 #pragma unroll
-            for (int k = 0; k < RB; ++k) {
-              const int r = r0 + 8 * k, mm = m0 + r;
+            for (int k = 0; k < RB; ++k)
 #pragma unroll
               for (int q = 0; q < 4; ++q) {
-                const int cc = lane + 32 * q, n = nb + cc;
-                if (mm < outM && n < outN && n <= mm)
-                  outw[(size_t)mm * out_ld + n] = x[k][q] - (double)Cs[r * CLD + cc] * unscale;
+                bool v;
+                const double* ptr = elem(0, k, q, v);
+                x[k][q] = v ? *ptr : 0.0;
+              }
+#pragma unroll
+            for (int b = 0; b < NBT; ++b) {
+              if (b + 1 < NBT) {
+#pragma unroll
+                for (int k = 0; k < RB; ++k)
+#pragma unroll
+                  for (int q = 0; q < 4; ++q) {
+                    bool v;
+                    const double* ptr = elem(b + 1, k, q, v);
+                    y[k][q] = v ? *ptr : 0.0;
+                  }
+              }
+#pragma unroll
+              for (int k = 0; k < RB; ++k)
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                  bool v;
+                  double* ptr = elem(b, k, q, v);
+                  if (v) *ptr = x[k][q] - cval(b, k, q) * unscale;
+                }
+              if (b + 1 < NBT) {
+#pragma unroll
+                for (int k = 0; k < RB; ++k)
+#pragma unroll
+                  for (int q = 0; q < 4; ++q) x[k][q] = y[k][q];
               }
             }
           }
-          // Mirror: row n = nb + cc, columns mm = m0 + lane + 32 q, n < mm.
-#pragma unroll 1
-          for (int c0 = e; c0 < BN; c0 += 8 * RB) {
-            double x[RB][4];
+          // The next item rewrites Cs only after every warp has read this one.
+          asm volatile("bar.sync 1, 256;\n" ::: "memory");
+        } else if (ok && m < ti.outM) {
+          const int n0 = ti.nt * BN + CPW * part;
+          double* orow = ti.out + (size_t)m * ti.ld;
 #pragma unroll
-            for (int k = 0; k < RB; ++k) {
-              const int n = nb + c0 + 8 * k;
-#pragma unroll
-              for (int q = 0; q < 4; ++q) {
-                const int mm = m0 + lane + 32 * q;
-                x[k][q] = (mm < outM && n < outN && n < mm) ? outw[(size_t)n * out_ld + mm] : 0.0;
-              }
-            }
-#pragma unroll
-            for (int k = 0; k < RB; ++k) {
-              const int cc = c0 + 8 * k, n = nb + cc;
-#pragma unroll
-              for (int q = 0; q < 4; ++q) {
-                const int r = lane + 32 * q, mm = m0 + r;
-                if (mm < outM && n < outN && n < mm)
-                  outw[(size_t)n * out_ld + mm] = x[k][q] - (double)Cs[r * CLD + cc] * unscale;
-              }
+          for (int c = 0; c < CPW; ++c) {
+            const int n = n0 + c;
+            // Lower-triangular mode writes the lower triangle and mirrors it,
+            // so the stored matrix is exactly symmetric.
+            if (n < ti.outN && !(args.lower_tiles && n > m)) {
+              const double val = args.subtract ? orow[n] - acc[c] * unscale
+                                               : acc[c] * unscale + ((args.add_identity && m == n) ? 1.0 : 0.0);
+              orow[n] = val;
+              if (args.lower_tiles && n != m) ti.out[(size_t)n * ti.ld + m] = val;
             }
           }
         }
-      } else if (ok && m < outM) {
-        const int n0 = nt_begin * BN + CPW * part;
-        double* orow = out_base + (size_t)w * out_stride + (size_t)m * out_ld;
-#pragma unroll
-        for (int c = 0; c < CPW; ++c) {
-          const int n = n0 + c;
-          // Lower-triangular mode writes the lower triangle and mirrors it,
-          // so the stored matrix is exactly symmetric.
-          if (n < outN && !(args.lower_tiles && n > m)) {
-            const double val = args.subtract ? orow[n] - acc[c] * unscale
-                                             : acc[c] * unscale + ((args.add_identity && m == n) ? 1.0 : 0.0);
-            orow[n] = val;
-            if (args.lower_tiles && n != m) out_base[(size_t)w * out_stride + (size_t)n * out_ld + m] = val;
-          }
-        }
+        if (EPI != EPI_UPDATE)
+          while (nit < n_items && !tile_item(nit, tnext)) nit += item_step;
+        ti = tnext;
+        it = nit;
       }
     }
   }
@@ -1428,7 +1514,10 @@ static void eps_tc_split(qx_ctx* ctx, const double* bov, int ldov, int naux, int
   a.err = d_err;
   const int tiles = ceil_div(naux, TC_BM);  // BM == BN for the symmetric product
   static_assert(BN == TC_BM, "eps tiles are square");
-  launch_tc<BN, EPI_STORE>(ctx, ah, al, bh, bl, a, dim3(tiles * (tiles + 1) / 2, nw));
+  // Persistent: at most one CTA per SM over the (frequency, tile) items, in
+  // tile-fastest order so that neighbouring CTAs share a frequency's operand.
+  const int items = tiles * (tiles + 1) / 2 * nw;
+  launch_tc<BN, EPI_STORE>(ctx, ah, al, bh, bl, a, dim3(std::min(items, ctx->sm_count)));
   check_tc_err(ctx, d_err);
 }
 
@@ -1628,7 +1717,11 @@ void launch_gsweep_update_tc(qx_ctx* ctx, const GMat* d_mats, const int* d_pre, 
   a.gmats = d_mats;
   a.gpre = d_pre;
   a.gcount = count;
-  launch_tc<BN, EPI_UPDATE>(ctx, ah, al, bh, bl, a, dim3(ntiles, 1));
+  a.items = ntiles;
+  // Persistent: one CTA per SM walks the tiles of all matrices, so that the
+  // loads and MMAs of its next tile run under the read-modify-write of this
+  // one (the update is bound by that HBM traffic).
+  launch_tc<BN, EPI_UPDATE>(ctx, ah, al, bh, bl, a, dim3(std::min(ntiles, ctx->sm_count)));
 }
 
 }  // namespace qx
