@@ -387,7 +387,9 @@ __global__ void __launch_bounds__(TcThreads<EPI, CONVB>::VALUE, 1)
       t.out = args.out + (size_t)t.w * args.out_stride;
     }
     if (args.gmats || args.lower_tiles) {
-      tm = (int)floor((sqrt(8.0 * r + 1.0) - 1.0) * 0.5);
+      // Single precision is exact for 8 r + 1 < 2^24; the loops below fix
+      // any off-by-one of the rounded root.
+      tm = (int)((sqrtf(8.0f * (float)r + 1.0f) - 1.0f) * 0.5f);
       while ((tm + 1) * (tm + 2) / 2 <= r) ++tm;
       while (tm * (tm + 1) / 2 > r) --tm;
       tn = r - tm * (tm + 1) / 2;
@@ -778,6 +780,8 @@ __global__ void __launch_bounds__(TcThreads<EPI, CONVB>::VALUE, 1)
       bool ok = true;
       int u = 0;
       int it = item0;
+      int unscale_w = -1;
+      double unscale = 1.0;
       StoreTile ti;
       while (it < n_items && !tile_item(it, ti)) it += item_step;
       while (it < n_items) {
@@ -790,8 +794,15 @@ __global__ void __launch_bounds__(TcThreads<EPI, CONVB>::VALUE, 1)
           while (nit < n_items && !tile_item(nit, tnext)) nit += item_step;
         const int m0 = ti.mb * TC_BM;
         const int m = m0 + quarter * 32 + lane;
-        const double unscale =
-            1.0 / ((double)args.scaleA[args.a_batched ? ti.w : 0] * (double)args.scaleB[ti.w]);
+        // The scales change with the frequency only (once per launch in the
+        // grouped update).
+        if (ti.w != unscale_w) {
+          unscale = 1.0 / ((double)args.scaleA[args.a_batched ? ti.w : 0] * (double)args.scaleB[ti.w]);
+          unscale_w = ti.w;
+        }
+        constexpr int CLD = L::CS_LD;
+        float* Cs = reinterpret_cast<float*>(smem + L::CS_OFF);
+        const int rl = quarter * 32 + lane;
         double acc[CPW];
 #pragma unroll
         for (int c = 0; c < CPW; ++c) acc[c] = 0.0;
@@ -810,28 +821,29 @@ __global__ void __launch_bounds__(TcThreads<EPI, CONVB>::VALUE, 1)
             if (ti.nt * BN + CPW * part + 16 * j >= ti.outN) continue;
             float v[16];
             tmem_ld16(taddr + 16 * j, v);
+            if (EPI == EPI_UPDATE) {
+              // UPDATE stages the FP32 tile as it is drained (one
+              // accumulation unit covers K; further units would add).
+              float* cr = Cs + rl * CLD + CPW * part + 16 * j;
 #pragma unroll
-            for (int q = 0; q < 16; ++q) acc[16 * j + q] += (double)v[q];
+              for (int q = 0; q < 16; ++q) cr[q] = uu == 0 ? v[q] : cr[q] + v[q];
+            } else {
+#pragma unroll
+              for (int q = 0; q < 16; ++q) acc[16 * j + q] += (double)v[q];
+            }
           }
           tc_fence_before();
           __syncwarp();
           if (lane == 0) mbar_arrive(&acc_empty[buf]);
         }
         if (EPI == EPI_UPDATE) {
-          // One FP32 accumulation unit covers K here (the launchers ask for
-          // it), so the tile C is exactly FP32.  It is staged in its own
-          // shared-memory area (the stages already hold the next item's
-          // operands), then the lower tile and its mirror are updated in
-          // row-wise passes that are coalesced along the rows of M; the mirror
-          // reads its old value from the upper element itself, M being stored
-          // exactly symmetric.  After an abort nothing more is written.
-          constexpr int CLD = L::CS_LD;
-          float* Cs = reinterpret_cast<float*>(smem + L::CS_OFF);
-          const int rl = quarter * 32 + lane;
-          if (ok) {
-#pragma unroll
-            for (int c = 0; c < CPW; ++c) Cs[rl * CLD + CPW * part + c] = (float)acc[c];
-          }
+          // The tile C (exactly FP32: one accumulation unit covers K, the
+          // launchers ask for it) was staged in its own shared-memory area
+          // while drained (the stages already hold the next item's operands);
+          // the lower tile and its mirror are now updated in row-wise passes
+          // that are coalesced along the rows of M; the mirror reads its old
+          // value from the upper element itself, M being stored exactly
+          // symmetric.  After an abort nothing more is written.
           asm volatile("bar.sync 1, 256;\n" ::: "memory");
           if (ok && !*abort_flag) {
             // Warp e updates eight batches of RB = 4 rows: rows e + 32 b + 8 k
