@@ -53,7 +53,7 @@ def parse():
     p.add_argument("--no-bse", action="store_true")
     p.add_argument("--batch-workers", type=int, default=0)
     p.add_argument("--bse-fd-points", type=int, default=4)
-    p.add_argument("--p0-form", choices=["auto", "materialised", "converter"], default="auto",
+    p.add_argument("--p0-form", choices=["auto", "materialised", "pair", "converter"], default="auto",
                    help="form of the split P0 (chi-scaled operand materialised, or built while staged)")
     return p.parse_args()
 

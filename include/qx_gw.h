@@ -66,10 +66,12 @@ qx_status qx_ctx_last_guard_stats(const qx_ctx* ctx, int64_t* guarded, int64_t* 
 /* Form of the split-precision P0 (FP16X3 / BF16X3; no reference
  * counterpart): QX_P0_MATERIALISED writes the hi/lo split of B_ov chi'(w) s_w
  * for every frequency (4 nw naux nov bytes) and reads it back by TMA;
- * QX_P0_CONVERTER applies chi'(w) while the B operand is staged in shared
- * memory, so that nothing chi-scaled goes to memory; QX_P0_AUTO (default)
- * materialises up to 6 GiB of such operands and converts beyond. */
-enum { QX_P0_AUTO = 0, QX_P0_MATERIALISED = 1, QX_P0_CONVERTER = 2 };
+ * QX_P0_PAIR reads the same operands with tiles on CTA pairs (tcgen05
+ * cta_group::2, two 128-row tiles per MMA of M = 256); QX_P0_CONVERTER
+ * applies chi'(w) while the B operand is staged in shared memory, so that
+ * nothing chi-scaled goes to memory; QX_P0_AUTO (default) materialises up to
+ * 6 GiB of such operands and converts beyond. */
+enum { QX_P0_AUTO = 0, QX_P0_MATERIALISED = 1, QX_P0_CONVERTER = 2, QX_P0_PAIR = 3 };
 qx_status qx_ctx_set_p0_form(qx_ctx* ctx, int form);
 /* Library version string. */
 const char* qx_version(void);

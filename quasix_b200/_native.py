@@ -21,7 +21,7 @@ STATUS_NAMES = {
 }
 PREC = {"fp64": 0, "bf16x3": 1, "fp16x3": 2}
 QP_SOLVER = {"newton": 0, "linearized": 1}
-P0_FORM = {"auto": 0, "materialised": 1, "converter": 2}
+P0_FORM = {"auto": 0, "materialised": 1, "converter": 2, "pair": 3}
 
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int)
@@ -208,7 +208,7 @@ class Context:
         return int(self.lib.qx_ctx_last_launches(self.handle))
 
     def set_p0_form(self, form: str):
-        """'auto', 'materialised' or 'converter' (qx_ctx_set_p0_form)."""
+        """'auto', 'materialised', 'pair' or 'converter' (qx_ctx_set_p0_form)."""
         self.check(self.lib.qx_ctx_set_p0_form(self.handle, P0_FORM[form]))
 
     def guard_stats(self):

@@ -1476,11 +1476,418 @@ __global__ void k_chi_cols(const double* __restrict__ chi, int nov, int ldov, co
   for (int k = threadIdx.x; k < ldov; k += blockDim.x) cs[(size_t)w * ldov + k] = k < nov ? (float)(cw[k] * s) : 0.f;
 }
 
+// ---------------------------------------------------------------------------
+// P0 on CTA pairs (tcgen05 cta_group::2, M = 256).
+// ---------------------------------------------------------------------------
+// The two CTAs of a cluster compute two 128-row tiles (m_a, n) and (m_b, n)
+// of one column of lower tiles of eps[w] with MMAs of M = 256, N = 128: each
+// CTA stages its own 128 A rows and one half (64 rows) of the B tile, the MMA
+// issued by the even CTA reads all four operand tiles, and each CTA's
+// 128 x 128 accumulator lands in its own TMEM.  Per MMA an SM then reads 6 KB
+// of operands from shared memory instead of 8 KB, and loads 48 KB per k block
+// instead of 64 KB: the single-CTA 128 x 128 tile reads 128 bytes per tensor
+// cycle, all of shared memory's bandwidth before the TMA writes into it.  A
+// column with an odd count of lower tiles pairs its last tile with a copy of
+// itself whose result is not stored.  Barriers: the even CTA's full[s] counts
+// the bytes of both CTAs' loads (each CTA's TMA signals it); the MMA commits
+// arrive on empty[s] and acc_full[b] of both CTAs (multicast); the even CTA's
+// acc_empty[b] takes an arrival from each of its epilogue warps and one for
+// all of the odd CTA's.  The epilogue sums the accumulation units in
+// Kahan-compensated FP32 (below).
+// Measured at nmo 300 / naux 1000 / nw 32 (a P0 stage with its split): with
+// the FP64 sums of the single-CTA epilogue the pair took 2.35 ms, its MMAs
+// waiting on the drain of the accumulators; with the compensated FP32 sums
+// 1.74 ms, against 1.69 ms for single-CTA tiles (which drain in FP64: the
+// compensated sums measured no faster there).  The single-CTA form stays the
+// default; this one is QX_P0_PAIR.
+namespace pairp0 {
+constexpr int STAGES = 4;
+constexpr int BK = 64;
+constexpr int A_BYTES = TC_BM * BK * 2;            // 16 KB: this CTA's 128 A rows
+constexpr int B_BYTES = (TC_BM / 2) * BK * 2;      // 8 KB: half of the N = 128 B tile
+constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;  // 48 KB
+constexpr int BAR_OFF = STAGES * STAGE_BYTES;
+constexpr int TOTAL = BAR_OFF + 256 + 1024;  // + slack for the 1024-byte alignment
+constexpr int NEPI = 8;
+constexpr int THREADS = 64 + 32 * NEPI;
+constexpr int CPW = TC_BM * 4 / NEPI;  // accumulator columns per epilogue warp
+// TMEM accumulators (128 columns each, all 512 columns): the MMAs may run up
+// to NBUF - 1 accumulation units ahead of the slower of the two epilogues,
+// whose release of a buffer reaches the even CTA by a remote arrival.
+constexpr int NBUF = 4;
+}  // namespace pairp0
+
+// Pairs of lower tiles per frequency for T tile rows: column nt holds T - nt tiles.
+__host__ __device__ inline int p0_pair_count(int T) {
+  int s = 0;
+  for (int nt = 0; nt < T; ++nt) s += (T - nt + 1) / 2;
+  return s;
+}
+// Pair r of a frequency -> its column nt and first tile row ma (the second is
+// ma + 1, past the last tile row for the odd tile of a column).
+__device__ __forceinline__ void p0_pair_tile(int r, int T, int& nt, int& ma) {
+  int c = 0;
+  for (nt = 0; nt < T - 1; ++nt) {
+    const int cnt = (T - nt + 1) / 2;
+    if (r < c + cnt) break;
+    c += cnt;
+  }
+  ma = nt + 2 * (r - c);
+}
+
+__device__ __forceinline__ uint32_t cluster_ctarank() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;\n" : "=r"(r));
+  return r;
+}
+__device__ __forceinline__ uint32_t cluster_nctarank() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%cluster_nctarank;\n" : "=r"(r));
+  return r;
+}
+__device__ __forceinline__ uint32_t cluster_id_x() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%clusterid.x;\n" : "=r"(r));
+  return r;
+}
+__device__ __forceinline__ uint32_t cluster_count_x() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%nclusterid.x;\n" : "=r"(r));
+  return r;
+}
+// The shared::cluster address of the same shared-memory offset in CTA rank.
+__device__ __forceinline__ uint32_t mapa_rank(uint32_t saddr, uint32_t rank) {
+  uint32_t r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;\n" : "=r"(r) : "r"(saddr), "r"(rank));
+  return r;
+}
+__device__ __forceinline__ void cluster_sync_all() {
+  asm volatile("barrier.cluster.arrive.release.aligned;\n" ::: "memory");
+  asm volatile("barrier.cluster.wait.acquire.aligned;\n" ::: "memory");
+}
+// TMA loads into this CTA's shared memory whose completion is counted on an
+// mbarrier of either CTA of the pair (shared::cluster address).
+__device__ __forceinline__ void tma_load_2d_pair(uint32_t dst, const CUtensorMap* map, uint32_t bar, int c0, int c1) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, "
+      "%4}], [%2];\n" ::"r"(dst),
+      "l"(map), "r"(bar), "r"(c0), "r"(c1)
+      : "memory");
+}
+__device__ __forceinline__ void tma_load_3d_pair(uint32_t dst, const CUtensorMap* map, uint32_t bar, int c0, int c1,
+                                                 int c2) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, "
+      "%4, %5}], [%2];\n" ::"r"(dst),
+      "l"(map), "r"(bar), "r"(c0), "r"(c1), "r"(c2)
+      : "memory");
+}
+__device__ __forceinline__ void umma_f16_pair(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                              uint32_t accumulate) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(
+          tmem_d),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
+}
+// Arrive on the mbarrier at this offset in both CTAs once the MMAs issued so far complete.
+__device__ __forceinline__ void umma_commit_pair_both(uint64_t* bar) {
+  asm volatile(
+      "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], %1;\n" ::"r"(
+          smem_u32(bar)),
+      "h"((unsigned short)3)
+      : "memory");
+}
+__device__ __forceinline__ void umma_commit_pair_own(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(smem_u32(bar))
+               : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_rank(uint64_t* bar, uint32_t rank) {
+  asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];\n" ::"r"(mapa_rank(smem_u32(bar), rank))
+               : "memory");
+}
+// mbar_wait with cluster-scope acquire (arrivals from the other CTA).
+__device__ __forceinline__ bool mbar_wait_cluster(uint64_t* bar, uint32_t parity, volatile int* abort_flag, int* err,
+                                                  int code) {
+  const long long t0 = clock64();
+  while (true) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, "
+        "0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    if (ok) return true;
+    if (*abort_flag) return false;
+    if (clock64() - t0 > WAIT_CYCLES) {
+      *abort_flag = 1;
+      atomicCAS(err, 0, code);
+      return false;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(pairp0::THREADS, 1)
+    k_p0_pair(const __grid_constant__ CUtensorMap mapAh, const __grid_constant__ CUtensorMap mapAl,
+              const __grid_constant__ CUtensorMap mapBh, const __grid_constant__ CUtensorMap mapBl, TcArgs args) {
+  namespace P = pairp0;
+  // Launched only in clusters of two (the launcher sets the attribute); any
+  // other shape records an error before touching the tensor cores.
+  if (cluster_nctarank() != 2) {
+    if (threadIdx.x == 0) atomicCAS(args.err, 0, 20);
+    return;
+  }
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + P::BAR_OFF);
+  uint64_t* empty = full + P::STAGES;
+  uint64_t* acc_full = empty + P::STAGES;   // [NBUF]
+  uint64_t* acc_empty = acc_full + P::NBUF;  // [NBUF]
+  uint64_t* drain = acc_empty + P::NBUF;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain + 1);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t rank = cluster_ctarank();
+  const bool leader = rank == 0;
+  const int T = args.m_blocks;
+  const int pairs_pb = p0_pair_count(T);
+  const int n_items = pairs_pb * args.nbatch;
+  const int item0 = (int)cluster_id_x(), item_step = (int)cluster_count_x();
+  const int k_blocks = (args.K + P::BK - 1) / P::BK;
+  const int unit = args.unit > 0 ? args.unit : 1;
+  // Item -> frequency w, column nt, this CTA's tile row m, and whether its
+  // tile is stored (the odd tile's copy is not).
+  auto item_tile = [&](int it, int& w, int& nt, int& m, bool& store) {
+    w = it / pairs_pb;
+    int ma;
+    p0_pair_tile(it - w * pairs_pb, T, nt, ma);
+    store = leader || ma + 1 < T;
+    m = (leader || ma + 1 >= T) ? ma : ma + 1;
+  };
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < P::STAGES; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    for (int b = 0; b < P::NBUF; ++b) {
+      mbar_init(&acc_full[b], 1);
+      mbar_init(&acc_empty[b], P::NEPI + 1);  // the even CTA's epilogue warps, one arrival for the odd CTA's
+    }
+    mbar_init(drain, 1);
+    *abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  if (warp == 1) {
+    // Both CTAs' MMA warps allocate together; the columns are the same in both.
+    asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(tmem_slot)),
+                 "r"(P::NBUF * TC_BM));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;\n" ::);
+  }
+  tc_fence_before();
+  __syncthreads();
+  // The other CTA's barriers are initialised before any remote arrival.
+  cluster_sync_all();
+  tc_fence_after();
+  const uint32_t tmem_base = *tmem_slot;
+
+  if (warp == 0) {
+    // ---------------- TMA producer (both CTAs) ----------------
+    if (lane == 0) {
+      const uint32_t full_leader = mapa_rank(smem_u32(full), 0);
+      int g = 0;
+      bool ok = true;
+      for (int it = item0; it < n_items && ok; it += item_step) {
+        int w, nt, m;
+        bool st;
+        item_tile(it, w, nt, m, st);
+        for (int kb = 0; kb < k_blocks; ++kb, ++g) {
+          const int s = g % P::STAGES;
+          if (g >= P::STAGES && !mbar_wait(&empty[s], ((g / P::STAGES) - 1) & 1, abort_flag, args.err, 21)) {
+            ok = false;
+            break;
+          }
+          if (leader) mbar_expect_tx(&full[s], 2 * P::STAGE_BYTES);
+          const uint32_t dst = smem_u32(smem + s * P::STAGE_BYTES);
+          const uint32_t fb = full_leader + s * 8;
+          const int k0 = kb * P::BK;
+          tma_load_2d_pair(dst, &mapAh, fb, k0, m * TC_BM);
+          tma_load_2d_pair(dst + P::A_BYTES, &mapAl, fb, k0, m * TC_BM);
+          tma_load_3d_pair(dst + 2 * P::A_BYTES, &mapBh, fb, k0, nt * TC_BM + (TC_BM / 2) * (int)rank, w);
+          tma_load_3d_pair(dst + 2 * P::A_BYTES + P::B_BYTES, &mapBl, fb, k0, nt * TC_BM + (TC_BM / 2) * (int)rank,
+                           w);
+        }
+      }
+      // The MMA commits of the last stages arrive on this CTA's empty[] too:
+      // they have landed before the CTA leaves.
+      for (int q = (g > P::STAGES ? g - P::STAGES : 0); q < g; ++q) {
+        volatile int no_abort = 0;
+        mbar_wait(&empty[q % P::STAGES], (q / P::STAGES) & 1, &no_abort, args.err, 22);
+      }
+    }
+  } else if (warp == 1) {
+    // ---------------- MMA issuer (even CTA) ----------------
+    if (leader && lane == 0) {
+      const uint32_t idesc = umma_idesc_f16(2 * TC_BM, TC_BM, args.fp16);
+      int g = 0, u = 0;
+      bool ok = true;
+      for (int it = item0; it < n_items && ok; it += item_step) {
+        for (int kb = 0; kb < k_blocks; ++kb, ++g) {
+          const bool unit_start = kb % unit == 0;
+          const bool unit_end = kb % unit == unit - 1 || kb == k_blocks - 1;
+          const int buf = u % P::NBUF;
+          if (unit_start && u >= P::NBUF &&
+              !mbar_wait_cluster(&acc_empty[buf], ((u / P::NBUF) - 1) & 1, abort_flag, args.err, 23)) {
+            ok = false;
+            break;
+          }
+          const int s = g % P::STAGES;
+          if (!mbar_wait(&full[s], (g / P::STAGES) & 1, abort_flag, args.err, 24)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t dacc = tmem_base + buf * TC_BM;
+          const uint32_t ah = smem_u32(smem + s * P::STAGE_BYTES), al = ah + P::A_BYTES;
+          const uint32_t bh = ah + 2 * P::A_BYTES, bl = bh + P::B_BYTES;
+#pragma unroll
+          for (int kk = 0; kk < P::BK / 16; ++kk) {
+            const uint32_t off = kk * 32;
+            const uint32_t acc0 = (!unit_start || kk > 0) ? 1u : 0u;
+            umma_f16_pair(dacc, umma_desc<P::BK>(ah + off), umma_desc<P::BK>(bh + off), idesc, acc0);
+            umma_f16_pair(dacc, umma_desc<P::BK>(ah + off), umma_desc<P::BK>(bl + off), idesc, 1u);
+            umma_f16_pair(dacc, umma_desc<P::BK>(al + off), umma_desc<P::BK>(bh + off), idesc, 1u);
+          }
+          umma_commit_pair_both(&empty[s]);
+          if (unit_end) {
+            umma_commit_pair_both(&acc_full[buf]);
+            ++u;
+          }
+        }
+      }
+      umma_commit_pair_own(drain);
+      volatile int no_abort = 0;
+      mbar_wait(drain, 0, &no_abort, args.err, 25);
+    }
+  } else {
+    // ---------------- epilogue (warps 2..9, both CTAs) ----------------
+    const int quarter = warp & 3;
+    const int part = (warp - 2) >> 2;
+    const int n_units = (k_blocks + unit - 1) / unit;
+    bool ok = true;
+    int u = 0;
+    for (int it = item0; it < n_items; it += item_step) {
+      int w, nt, mt;
+      bool st;
+      item_tile(it, w, nt, mt, st);
+      const int m = mt * TC_BM + quarter * 32 + lane;
+      const double unscale = 1.0 / ((double)args.scaleA[0] * (double)args.scaleB[w]);
+      // Kahan-compensated FP32 sums of the FP32 accumulation units (sum
+      // hs, compensation hc): four FP32 additions per value instead of an
+      // FP32 -> FP64 conversion and an FP64 addition, whose throughput bounded
+      // the drain.  The compensated sum is rounded once to FP32 at the end
+      // (2^-24 relative), below the FP32 rounding inside one unit.
+      float hs[P::CPW], hc[P::CPW];
+#pragma unroll
+      for (int c = 0; c < P::CPW; ++c) hs[c] = hc[c] = 0.0f;
+      for (int uu = 0; uu < n_units; ++uu, ++u) {
+        const int buf = u % P::NBUF;
+        // After a failed wait a warp waits no more, but the odd CTA's warps
+        // still pass the unit's named barrier together.
+        const bool got = ok && mbar_wait(&acc_full[buf], (u / P::NBUF) & 1, abort_flag, args.err, 26);
+        ok = got;
+        if (got) {
+          tc_fence_after();
+          const uint32_t taddr = tmem_base + ((uint32_t)(quarter * 32) << 16) + buf * TC_BM + P::CPW * part;
+#pragma unroll
+          for (int j = 0; j < P::CPW / 16; ++j) {
+            if (nt * TC_BM + P::CPW * part + 16 * j >= args.N) continue;  // warp-uniform
+            float v[16];
+            tmem_ld16(taddr + 16 * j, v);
+#pragma unroll
+            for (int q = 0; q < 16; ++q) {
+              const int c = 16 * j + q;
+              const float y = v[q] - hc[c];
+              const float t = hs[c] + y;
+              hc[c] = (t - hs[c]) - y;
+              hs[c] = t;
+            }
+          }
+          tc_fence_before();
+        }
+        if (leader) {
+          __syncwarp();
+          if (got && lane == 0) mbar_arrive(&acc_empty[buf]);
+        } else {
+          // The odd CTA's eight warps meet first, and one remote arrival
+          // releases the buffer (a cluster-scope release per warp and unit
+          // doubled the odd CTA's drain time).
+          asm volatile("bar.sync 1, 256;\n" ::: "memory");
+          if (got && warp == 2 && lane == 0) mbar_arrive_rank(&acc_empty[buf], 0);
+        }
+      }
+      if (ok && st && m < args.M) {
+        const int n0 = nt * TC_BM + P::CPW * part;
+        double* out = args.out + (size_t)w * args.out_stride;
+        double* orow = out + (size_t)m * args.ldo;
+#pragma unroll
+        for (int c = 0; c < P::CPW; ++c) {
+          const int n = n0 + c;
+          // The lower triangle and its mirror: the stored matrix is exactly symmetric.
+          if (n < args.N && n <= m) {
+            const double val = (double)(hs[c] - hc[c]) * unscale + ((args.add_identity && m == n) ? 1.0 : 0.0);
+            orow[n] = val;
+            if (n != m) out[(size_t)n * args.ldo + m] = val;
+          }
+        }
+      }
+    }
+  }
+  // Teardown: every warp of both CTAs reaches this point (all waits are
+  // bounded); no remote arrival is still on its way to a CTA that leaves.
+  tc_fence_before();
+  __syncthreads();
+  cluster_sync_all();
+  tc_fence_after();
+  if (warp == 1) {
+    asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;\n" ::"r"(tmem_base), "r"(P::NBUF * TC_BM));
+  }
+}
+
 // P0 with the chi-scaled B operand materialised: one pass splits B_ov chi'_w
 // s_w for every frequency (k_split8_bcast, 4 nw naux ldov bytes written),
 // then the STORE GEMM reads both operands by TMA.
+static void launch_p0_pair(qx_ctx* ctx, const CUtensorMap& ah, const CUtensorMap& al, const CUtensorMap& bh,
+                           const CUtensorMap& bl, const TcArgs& a) {
+  static PerDeviceOnce attr_once;
+  static int max_clusters[PerDeviceOnce::kMaxDevices] = {};
+  cudaLaunchConfig_t cfg = {};
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = 2;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.blockDim = dim3(pairp0::THREADS);
+  cfg.dynamicSmemBytes = pairp0::TOTAL;
+  cfg.stream = ctx->stream;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  attr_once(ctx->device, [&] {
+    QX_CUDA(cudaFuncSetAttribute(k_p0_pair, cudaFuncAttributeMaxDynamicSharedMemorySize, pairp0::TOTAL));
+    cfg.gridDim = dim3(2 * ctx->sm_count);
+    int n = 0;
+    QX_CUDA(cudaOccupancyMaxActiveClusters(&n, k_p0_pair, &cfg));
+    max_clusters[ctx->device] = std::max(n, 1);
+  });
+  // Persistent: as many pairs as fit at once, each walking the pair items.
+  const int items = p0_pair_count(a.m_blocks) * a.nbatch;
+  cfg.gridDim = dim3(2 * std::min(items, max_clusters[ctx->device]));
+  QX_CUDA(cudaLaunchKernelEx(&cfg, k_p0_pair, ah, al, bh, bl, a));
+  check_launch(ctx);
+}
+
 static void eps_tc_split(qx_ctx* ctx, const double* bov, int ldov, int naux, int nov, const double* chi, int nw,
-                         double* eps, int ldn, size_t eps_stride, int fp16, int reuse_a) {
+                         double* eps, int ldn, size_t eps_stride, int fp16, int reuse_a, bool pair) {
   constexpr int BN = 128;
   const size_t a_elems = (size_t)naux * ldov;
   DevBuf& buf = ctx->ws[WS_BOV_HI];
@@ -1504,8 +1911,9 @@ static void eps_tc_split(qx_ctx* ctx, const double* bov, int ldov, int naux, int
   constexpr int BK = TcPipe<EPI_STORE>::BK;
   CUtensorMap ah = make_map(a_hi, nov, naux, ldov, 1, TC_BM, 2, fp16, BK);
   CUtensorMap al = make_map(a_lo, nov, naux, ldov, 1, TC_BM, 2, fp16, BK);
-  CUtensorMap bh = make_map(b_hi, nov, naux, ldov, nw, BN, 3, fp16, BK);
-  CUtensorMap bl = make_map(b_lo, nov, naux, ldov, nw, BN, 3, fp16, BK);
+  // CTA pairs stage half of the B tile each.
+  CUtensorMap bh = make_map(b_hi, nov, naux, ldov, nw, pair ? BN / 2 : BN, 3, fp16, BK);
+  CUtensorMap bl = make_map(b_lo, nov, naux, ldov, nw, pair ? BN / 2 : BN, 3, fp16, BK);
   int* d_err = tc_err_slot(ctx);
   QX_CUDA(cudaMemsetAsync(d_err, 0, sizeof(int), ctx->stream));
   TcArgs a{};
@@ -1526,10 +1934,14 @@ static void eps_tc_split(qx_ctx* ctx, const double* bov, int ldov, int naux, int
   a.err = d_err;
   const int tiles = ceil_div(naux, TC_BM);  // BM == BN for the symmetric product
   static_assert(BN == TC_BM, "eps tiles are square");
-  // Persistent: at most one CTA per SM over the (frequency, tile) items, in
-  // tile-fastest order so that neighbouring CTAs share a frequency's operand.
-  const int items = tiles * (tiles + 1) / 2 * nw;
-  launch_tc<BN, EPI_STORE>(ctx, ah, al, bh, bl, a, dim3(std::min(items, ctx->sm_count)));
+  if (pair) {
+    launch_p0_pair(ctx, ah, al, bh, bl, a);
+  } else {
+    // Persistent: at most one CTA per SM over the (frequency, tile) items, in
+    // tile-fastest order so that neighbouring CTAs share a frequency's operand.
+    const int items = tiles * (tiles + 1) / 2 * nw;
+    launch_tc<BN, EPI_STORE>(ctx, ah, al, bh, bl, a, dim3(std::min(items, ctx->sm_count)));
+  }
   check_tc_err(ctx, d_err);
 }
 
@@ -1602,10 +2014,11 @@ void launch_eps_tc(qx_ctx* ctx, const double* bov, int ldov, int naux, int nov, 
   // (4 nw naux ldov bytes) fits the budget; beyond it the converter form
   // keeps P0's memory at the A split and one FP32 copy of B_ov.
   const size_t chi_bytes = (size_t)4 * nw * naux * ldov;
-  const bool materialise =
-      ctx->p0_form == QX_P0_MATERIALISED || (ctx->p0_form == QX_P0_AUTO && chi_bytes <= kP0SplitBudget);
+  const bool materialise = ctx->p0_form == QX_P0_MATERIALISED || ctx->p0_form == QX_P0_PAIR ||
+                           (ctx->p0_form == QX_P0_AUTO && chi_bytes <= kP0SplitBudget);
   if (materialise)
-    eps_tc_split(ctx, bov, ldov, naux, nov, chi, nw, eps, ldn, eps_stride, fp16, reuse_a);
+    eps_tc_split(ctx, bov, ldov, naux, nov, chi, nw, eps, ldn, eps_stride, fp16, reuse_a,
+                 ctx->p0_form == QX_P0_PAIR);
   else
     eps_tc_conv(ctx, bov, ldov, naux, nov, chi, nw, eps, ldn, eps_stride, fp16, reuse_a);
 }

@@ -526,7 +526,7 @@ qx_status qx_ctx_set_stream(qx_ctx* c, void* stream) {
 }
 
 qx_status qx_ctx_set_p0_form(qx_ctx* c, int form) {
-  if (!c || form < QX_P0_AUTO || form > QX_P0_CONVERTER) return QX_ERR_INVALID_INPUT;
+  if (!c || form < QX_P0_AUTO || form > QX_P0_PAIR) return QX_ERR_INVALID_INPUT;
   c->p0_form = form;
   for (qx_ctx* w : c->workers) w->p0_form = form;
   return QX_OK;

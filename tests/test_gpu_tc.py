@@ -40,12 +40,14 @@ def p0_form(q):
     ctx.set_p0_form("auto")
 
 
-@pytest.mark.parametrize("form", ["materialised", "converter"])
+@pytest.mark.parametrize("form", ["materialised", "pair", "converter"])
 @pytest.mark.parametrize("prec", ["bf16x3", "fp16x3"])
 @pytest.mark.parametrize("shape", [(5, 19, 84), (12, 61, 250), (20, 130, 520)])
 def test_rho_response_tc(q, p0_form, shape, prec, form):
-    """Both forms of the split P0: the chi-scaled operand materialised, or
-    built in shared memory by the converter warps (chi applied while staged)."""
+    """The forms of the split P0: the chi-scaled operand materialised (tiles on
+    one CTA, or two tiles of a column on a CTA pair: with 1, 2 and 5 tile rows
+    every column count, even and odd, occurs), or built in shared memory by
+    the converter warps (chi applied while staged)."""
     nocc, nvir, naux = shape
     s = make_system(nocc, nvir, naux, seed=4, pi_norm=3.0)
     lov = np.ascontiguousarray(s.lpq[:, :nocc, nocc:])
@@ -71,7 +73,7 @@ def test_sigma_diag_tc(q, shape, nw, orbs, prec):
     assert np.abs(got - ref).max() < TOL_SIGMA[prec] * max(1.0, np.abs(ref).max())
 
 
-@pytest.mark.parametrize("form", ["materialised", "converter"])
+@pytest.mark.parametrize("form", ["materialised", "pair", "converter"])
 @pytest.mark.parametrize("prec", ["bf16x3", "fp16x3"])
 def test_evgw_tc_within_one_mev(q, p0_form, prec, form):
     s = make_system(12, 61, 250, seed=6, pi_norm=3.0)
