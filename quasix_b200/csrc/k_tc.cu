@@ -143,7 +143,12 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
 // ---------------------------------------------------------------------------
 // EPI_UPDATE is the STORE epilogue in its subtract form (the sweep's trailing
 // update), instantiated apart so that profiles tell it from P0.
-enum { EPI_ROWDOT = 0, EPI_STORE = 1, EPI_UPDATE = 2 };
+// EPI_GUPDATE is the grouped form of the update (one persistent CTA per SM
+// over the tiles of many matrices): two groups of four epilogue warps take
+// alternate tiles, each with its own TMEM buffer, staging area and named
+// barrier, so that one group's drain and barriers overlap the other's
+// read-modify-write.
+enum { EPI_ROWDOT = 0, EPI_STORE = 1, EPI_UPDATE = 2, EPI_GUPDATE = 3 };
 
 constexpr int TC_BM = 128;
 // Pipeline shape per epilogue: 64-wide K blocks in 2 stages.  32-wide blocks
@@ -155,7 +160,9 @@ constexpr int TC_BM = 128;
 template <int EPI>
 struct TcPipe {
   static constexpr int BK = 64;
-  static constexpr int STAGES = 2;
+  // The grouped update holds two staging tiles instead of a second stage
+  // (its K of 128 is two blocks, loaded and multiplied one after the other).
+  static constexpr int STAGES = EPI == EPI_GUPDATE ? 1 : 2;
 };
 
 // STORE (the FP64-output GEMMs: P0, the sweep update, the BSE direct term):
@@ -213,13 +220,13 @@ struct TcSmem {
   // UPDATE: the FP32 tile C, staged for the coalesced row passes of the
   // read-modify-write (row stride CS_LD floats against bank conflicts).
   static constexpr int CS_LD = BN + 1;
-  static constexpr int CS_BYTES = EPI == EPI_UPDATE ? TC_BM * CS_LD * 4 : 0;
+  static constexpr int CS_BYTES = EPI == EPI_UPDATE ? TC_BM * CS_LD * 4 : EPI == EPI_GUPDATE ? 2 * TC_BM * CS_LD * 4 : 0;
   // UPDATE, grouped: a shared-memory copy of the prefix table of CTA counts
   // (up to GP_CAP matrices), so that finding a tile's matrix costs no
   // dependent global loads.
   static constexpr int GP_CAP = 2048;
   static constexpr int GP_OFF = CS_OFF + CS_BYTES;
-  static constexpr int GP_BYTES = EPI == EPI_UPDATE ? GP_CAP * 4 : 0;
+  static constexpr int GP_BYTES = (EPI == EPI_UPDATE || EPI == EPI_GUPDATE) ? GP_CAP * 4 : 0;
   static constexpr int TOTAL = GP_OFF + GP_BYTES + 1024;  // + slack for the 1024-byte alignment
 };
 
@@ -351,7 +358,7 @@ __global__ void __launch_bounds__(TcThreads<EPI, CONVB>::VALUE, 1)
   };
   // STORE / UPDATE item -> output tile; false when the tile is left alone
   // (the sweep update's pivot row and column, and the look-ahead filter).
-  const bool gp_shared = EPI == EPI_UPDATE && args.gmats && args.gcount <= L::GP_CAP;
+  const bool gp_shared = (EPI == EPI_UPDATE || EPI == EPI_GUPDATE) && args.gmats && args.gcount <= L::GP_CAP;
   const int* gpre = args.gpre;
   if (gp_shared) {
     int* gs = reinterpret_cast<int*>(smem + L::GP_OFF);
@@ -431,7 +438,9 @@ __global__ void __launch_bounds__(TcThreads<EPI, CONVB>::VALUE, 1)
     }
     for (int b = 0; b < 2; ++b) {
       mbar_init(&acc_full[b], 1);
-      mbar_init(&acc_empty[b], TcWarps<EPI>::NEPI);  // one arrival per epilogue warp
+      // One arrival per epilogue warp (GUPDATE: per warp of the group that
+      // owns the buffer).
+      mbar_init(&acc_empty[b], EPI == EPI_GUPDATE ? TcWarps<EPI>::NEPI / 2 : TcWarps<EPI>::NEPI);
     }
     mbar_init(drain, 1);
     *abort_flag = 0;
@@ -767,6 +776,112 @@ __global__ void __launch_bounds__(TcThreads<EPI, CONVB>::VALUE, 1)
         ++done_items;
         // Both halves leave the item loop together (the flags are shared).
         ok = done[0] && done[1];
+      }
+    } else if (EPI == EPI_GUPDATE) {
+      // ---------------- epilogue (warps 2..9): grouped update, two groups ----------------
+      // Group gi (warps 2..5 or 6..9, one per TMEM lane quarter) takes the
+      // CTA's runnable tiles j = gi, gi + 2, ...; tile j is accumulation unit
+      // j (one unit covers K), so it sits in TMEM buffer gi, and the group
+      // stages it in its own FP32 area, passes its own named barrier and
+      // updates the lower tile and its mirror, 32 rows of each per warp in
+      // pipelined batches of RB = 4.
+      const int quarter = warp & 3;
+      const int gi = (warp - 2) >> 2;
+      const int e = (warp - 2) & 3;  // this warp's rank in its group
+      constexpr int CLD = L::CS_LD;
+      float* Cs = reinterpret_cast<float*>(smem + L::CS_OFF) + gi * (TC_BM * CLD);
+      const int rl = quarter * 32 + lane;
+      const uint32_t bar_id = 1 + gi;
+      bool ok = true;
+      int unscale_w = -1;
+      double unscale = 1.0;
+      int j = 0;  // runnable tiles of this CTA seen so far
+      for (int it = item0; it < n_items; it += item_step) {
+        StoreTile ti;
+        if (!tile_item(it, ti)) continue;
+        const int jj = j++;
+        if ((jj & 1) != gi) continue;
+        const int buf = gi;
+        if (ti.w != unscale_w) {
+          unscale = 1.0 / ((double)args.scaleA[args.a_batched ? ti.w : 0] * (double)args.scaleB[ti.w]);
+          unscale_w = ti.w;
+        }
+        const bool got = ok && mbar_wait(&acc_full[buf], (jj >> 1) & 1, abort_flag, args.err, 4);
+        ok = got;
+        if (got) {
+          tc_fence_after();
+          const uint32_t taddr = tmem_base + ((uint32_t)(quarter * 32) << 16) + buf * BN;
+#pragma unroll
+          for (int c = 0; c < BN; c += 16) {
+            float v[16];
+            tmem_ld16(taddr + c, v);
+            float* cr = Cs + rl * CLD + c;
+#pragma unroll
+            for (int q = 0; q < 16; ++q) cr[q] = v[q];
+          }
+          tc_fence_before();
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&acc_empty[buf]);
+        }
+        asm volatile("bar.sync %0, 128;\n" ::"r"(bar_id) : "memory");
+        if (ok && !*abort_flag) {
+          constexpr int RB = 4, NBT = 16;  // 8 batches of the lower tile, 8 of the mirror
+          const int m0 = ti.mb * TC_BM, nb = ti.nt * BN;
+          const int outM = ti.outM, outN = ti.outN, out_ld = ti.ld;
+          double* outw = ti.out;
+          static_assert(EPI != EPI_GUPDATE || (TC_BM == 128 && BN == 128), "row passes assume 128 x 128 tiles");
+          auto elem = [&](int b, int k, int q, bool& v) -> double* {
+            if (b < NBT / 2) {
+              const int mm = m0 + e + 16 * b + 4 * k, n = nb + lane + 32 * q;
+              v = mm < outM && n < outN && n <= mm;
+              return outw + (size_t)mm * out_ld + n;
+            }
+            const int n = nb + e + 16 * (b - NBT / 2) + 4 * k, mm = m0 + lane + 32 * q;
+            v = mm < outM && n < outN && n < mm;
+            return outw + (size_t)n * out_ld + mm;
+          };
+          auto cval = [&](int b, int k, int q) -> double {
+            return (double)(b < NBT / 2 ? Cs[(e + 16 * b + 4 * k) * CLD + lane + 32 * q]
+                                        : Cs[(lane + 32 * q) * CLD + e + 16 * (b - NBT / 2) + 4 * k]);
+          };
+          double x[RB][4], y[RB][4];
+#pragma unroll
+          for (int k = 0; k < RB; ++k)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+              bool v;
+              const double* ptr = elem(0, k, q, v);
+              x[k][q] = v ? *ptr : 0.0;
+            }
+#pragma unroll 2
+          for (int b = 0; b < NBT; ++b) {
+            if (b + 1 < NBT) {
+#pragma unroll
+              for (int k = 0; k < RB; ++k)
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                  bool v;
+                  const double* ptr = elem(b + 1, k, q, v);
+                  y[k][q] = v ? *ptr : 0.0;
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < RB; ++k)
+#pragma unroll
+              for (int q = 0; q < 4; ++q) {
+                bool v;
+                double* ptr = elem(b, k, q, v);
+                if (v) *ptr = x[k][q] - cval(b, k, q) * unscale;
+              }
+#pragma unroll
+            for (int k = 0; k < RB; ++k)
+#pragma unroll
+              for (int q = 0; q < 4; ++q) x[k][q] = y[k][q];
+          }
+        }
+        // The group's next tile rewrites its staging area only after every
+        // warp of the group has read this one.
+        asm volatile("bar.sync %0, 128;\n" ::"r"(bar_id) : "memory");
       }
     } else {
       // ---------------- epilogue (warps 2..9): FP64 sum of k-block partials ----------------
@@ -2122,7 +2237,7 @@ void launch_sweep_update_tc(qx_ctx* ctx, cudaStream_t st, double* eps, int n, in
 void launch_gsweep_update_tc(qx_ctx* ctx, const GMat* d_mats, const int* d_pre, int count, int ntiles, int step,
                              const TcOperand& T, const TcOperand& P, int rows, int* err) {
   constexpr int BN = 128;
-  constexpr int BK = TcPipe<EPI_UPDATE>::BK;
+  constexpr int BK = TcPipe<EPI_GUPDATE>::BK;
   const int K = kSweepPanelCols;
   CUtensorMap ah = make_map(T.hi, K, rows, K, 1, TC_BM, 2, 1, BK);
   CUtensorMap al = make_map(T.lo, K, rows, K, 1, TC_BM, 2, 1, BK);
@@ -2145,8 +2260,9 @@ void launch_gsweep_update_tc(qx_ctx* ctx, const GMat* d_mats, const int* d_pre, 
   a.items = ntiles;
   // Persistent: one CTA per SM walks the tiles of all matrices, so that the
   // loads and MMAs of its next tile run under the read-modify-write of this
-  // one (the update is bound by that HBM traffic).
-  launch_tc<BN, EPI_UPDATE>(ctx, ah, al, bh, bl, a, dim3(std::min(ntiles, ctx->sm_count)));
+  // one (the update is bound by that HBM traffic), with the two-group
+  // epilogue.
+  launch_tc<BN, EPI_GUPDATE>(ctx, ah, al, bh, bl, a, dim3(std::min(ntiles, ctx->sm_count)));
 }
 
 }  // namespace qx
