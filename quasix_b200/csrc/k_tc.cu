@@ -21,6 +21,7 @@
 
 #include <array>
 #include <map>
+#include <cstring>
 #include <mutex>
 #include <vector>
 
@@ -1450,6 +1451,20 @@ void launch_split(qx_ctx* ctx, const double* src, int rows, int cols, int ld_src
 }
 
 unsigned long long* split_amax_words(qx_ctx* ctx, int slot) { return split_scratch(ctx, slot).amax_src; }
+
+__global__ void k_fill_u64(unsigned long long* __restrict__ w, int n, unsigned long long v) {
+  for (int i = threadIdx.x; i < n; i += blockDim.x) w[i] = v;
+}
+
+unsigned long long* split_bound_words(qx_ctx* ctx, int slot, int n, double bound) {
+  QX_REQUIRE(n > 0 && n <= 1024, QX_ERR_INVALID_INPUT, "at most 1024 bounds per split");
+  unsigned long long* w = split_scratch(ctx, slot).amax_src;
+  unsigned long long bits;
+  std::memcpy(&bits, &bound, sizeof bits);
+  k_fill_u64<<<1, 256, 0, ctx->stream>>>(w, n, bits);
+  check_launch(ctx);
+  return w;
+}
 
 // One error word per launch, from the context's status arena.
 static int* tc_err_slot(qx_ctx* ctx) { return status_words(ctx, 1); }

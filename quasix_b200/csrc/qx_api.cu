@@ -267,8 +267,9 @@ void gw_wc_contract(qx_ctx* ctx, GWSystem& S) {
   record_stage(ctx, QX_ST_CONTRACT, true);
   if (is_tc_precision(S.precision)) {
     const int fp16 = S.precision == QX_PREC_FP16X3;
+    const unsigned long long* bound = S.wc_unit_bound && fp16 ? split_bound_words(ctx, 0, S.nw, 1.0) : nullptr;
     launch_split(ctx, S.eps, S.naux, S.naux, S.ldn, S.wc_split.hi, S.wc_split.lo, S.ldn, S.eps_stride, S.eps_stride,
-                 S.nw, fp16, 0, &S.wc_split.scale);
+                 S.nw, fp16, 0, &S.wc_split.scale, bound);
     launch_pair_contract_tc(ctx, S.bpt_split, S.bpt_f32, S.ldk, S.npair, S.naux, S.wc_split, S.ldn, S.eps_stride, S.nw,
                             S.v, S.npair, fp16);
   } else {
@@ -285,8 +286,8 @@ void gw_wc_pairs(qx_ctx* ctx, GWSystem& S, const double* e_host) {
   // [1, 1 + ||Pi||], so the split trailing update of the sweep keeps Wc within
   // the split forms' error.  Once levels cross, eps may be indefinite and the
   // sweep runs guarded (with the pivoted fallback).
-  launch_invert_wc(ctx, S.eps, S.naux, S.ldn, S.eps_stride, S.nw,
-                   !eps_at_least_identity(e_host, S.nocc, S.nvir, 0.0), /*half_lower=*/1,
+  S.wc_unit_bound = eps_at_least_identity(e_host, S.nocc, S.nvir, 0.0);
+  launch_invert_wc(ctx, S.eps, S.naux, S.ldn, S.eps_stride, S.nw, !S.wc_unit_bound, /*half_lower=*/1,
                    /*split_update=*/is_tc_precision(S.precision));
   record_stage(ctx, QX_ST_INV, false);
   gw_wc_contract(ctx, S);

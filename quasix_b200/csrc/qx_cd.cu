@@ -204,6 +204,8 @@ void CdEngine::eps_matrices(std::vector<GMat>& out) const {
 }
 
 void CdEngine::setup_end() {
+  // The imaginary-axis eps was inverted unguarded exactly when it is certified >= I.
+  S.wc_unit_bound = eps_at_least_identity(e.data(), nocc, nvir, 0.0);
   gw_wc_contract(ctx, S);
   DevBuf& cb = ctx->ws[WS_CD0];
   cb.reserve((size_t)(nmo + 4 * ntarget + 64) * sizeof(double));

@@ -27,6 +27,11 @@ struct GWSystem {
   SigmaGrid grid;
   TcOperand bpt_split{}, wc_split{};
   float* bpt_f32 = nullptr;
+  // eps(iw) >= I was certified for the last inversion: eps^-1 has its
+  // eigenvalues in (0, 1], so every entry of Wc = eps^-1 - I (and of W') is at
+  // most 1 in magnitude, and the split of W' takes 1 as its bound instead of a
+  // pass over the matrices.
+  bool wc_unit_bound = false;
 };
 
 SigmaGrid sigma_grid(int nw, double cutoff, double x0);

@@ -394,6 +394,9 @@ void launch_split(qx_ctx* ctx, const double* src, int rows, int cols, int ld_src
 // The amax words of split slot `slot` (1024, for kernels that accumulate a
 // bound before the split).
 unsigned long long* split_amax_words(qx_ctx* ctx, int slot);
+// The amax words of split slot `slot` set to a known bound for n sources (in
+// place of a pass over them), on the context stream.
+unsigned long long* split_bound_words(qx_ctx* ctx, int slot, int n, double bound);
 // reuse_a: B_ov is the one split by the previous call on this context; its
 // hi/lo split is reused (unless the operand buffer has to grow).
 void launch_eps_tc(qx_ctx* ctx, const double* bov, int ldov, int naux, int nov, const double* chi, int nw,
