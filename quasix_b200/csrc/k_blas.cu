@@ -285,24 +285,31 @@ __device__ __forceinline__ double cta_sum(double v, double* red) {
   return t;
 }
 
-__device__ int sturm_count(const double* d, const double* e, int n, double x, double pivmin) {
+// Sturm count of T - x I from the diagonal d and the squared off-diagonal e2
+// (e2[i] = e[i]^2): the number of eigenvalues of T below x.
+__device__ int sturm_count_sq(const double* d, const double* e2, int n, double x, double pivmin) {
   int c = 0;
   double q = d[0] - x;
   if (q < 0.0) ++c;
   for (int i = 1; i < n; ++i) {
     if (fabs(q) < pivmin) q = -pivmin;
-    q = d[i] - x - e[i - 1] * e[i - 1] / q;
+    q = d[i] - x - e2[i - 1] / q;
     if (q < 0.0) ++c;
   }
   return c;
 }
+
+constexpr int kEighMaxMulti = 64;  // eigenvalues found by multisection (more: bisection per thread)
 
 __global__ void __launch_bounds__(1024) k_eigh_lowest(const double* __restrict__ A, int n, int lda, int k,
                                                       double* __restrict__ W, double* __restrict__ work,
                                                       int* __restrict__ iwork, double* __restrict__ w_out,
                                                       double* __restrict__ Z, int ldz) {
   __shared__ double red[32];
-  extern __shared__ double sm[];  // u [n], q [n]
+  __shared__ int cnt[1024];
+  __shared__ double br_lo[kEighMaxMulti], br_hi[kEighMaxMulti];
+  __shared__ int br_done;
+  extern __shared__ double sm[];  // u [n], q [n]; then d [n], e^2 [n]
   double* u = sm;
   double* q = sm + n;
   double* tau = work;           // [n]
@@ -312,12 +319,14 @@ __global__ void __launch_bounds__(1024) k_eigh_lowest(const double* __restrict__
   double* Y = work + 4 * n;     // [k][n] eigenvectors of T, then of A
   double* LU = Y + (size_t)k * n;  // [5][k][n] per-vector factors
   const int tid = threadIdx.x, nt = blockDim.x;
-  for (int idx = tid; idx < n * n; idx += nt) {
-    const int r = idx / n, c = idx % n;
-    W[idx] = 0.5 * (A[(size_t)r * lda + c] + A[(size_t)c * lda + r]);
-  }
+  const int lane = tid & 31, warp = tid >> 5, nwarp = nt >> 5;
+  // Rows and columns by warps and lanes: no index division in the loops.
+  for (int r = warp; r < n; r += nwarp)
+    for (int c = lane; c < n; c += 32) W[(size_t)r * n + c] = 0.5 * (A[(size_t)r * lda + c] + A[(size_t)c * lda + r]);
   __syncthreads();
   // Tridiagonalisation: H_j = I - tau_j u_j u_j^T on rows/cols j+1..n-1.
+  // W stays exactly symmetric (the rank-2 update gives (r, c) and (c, r)
+  // the same value), so B u is taken along contiguous rows.
   for (int j = 0; j + 2 < n; ++j) {
     const int m = n - j - 1;
     double s = 0.0;
@@ -340,11 +349,13 @@ __global__ void __launch_bounds__(1024) k_eigh_lowest(const double* __restrict__
     const double t = 1.0 / (alpha * (alpha + fabs(x0)));  // 2 / (u^T u)
     for (int i = tid; i < m; i += nt) u[i] = W[(size_t)(j + 1 + i) * n + j] - (i == 0 ? as : 0.0);
     __syncthreads();
-    // p = B u (B symmetric: column access is coalesced)
-    for (int i = tid; i < m; i += nt) {
+    // p = B u: one warp per row of B, lanes along the row.
+    for (int i = warp; i < m; i += nwarp) {
+      const double* row = W + (size_t)(j + 1 + i) * n + j + 1;
       double acc = 0.0;
-      for (int l = 0; l < m; ++l) acc += W[(size_t)(j + 1 + l) * n + j + 1 + i] * u[l];
-      q[i] = acc;
+      for (int l = lane; l < m; l += 32) acc += row[l] * u[l];
+      for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+      if (lane == 0) q[i] = acc;
     }
     __syncthreads();
     double up = 0.0;
@@ -352,9 +363,10 @@ __global__ void __launch_bounds__(1024) k_eigh_lowest(const double* __restrict__
     const double K = cta_sum(up, red);
     for (int i = tid; i < m; i += nt) q[i] = t * q[i] - 0.5 * t * t * K * u[i];
     __syncthreads();
-    for (int idx = tid; idx < m * m; idx += nt) {
-      const int r = idx / m, c = idx % m;
-      W[(size_t)(j + 1 + r) * n + j + 1 + c] -= u[r] * q[c] + q[r] * u[c];
+    for (int r = warp; r < m; r += nwarp) {
+      const double ur = u[r], qr = q[r];
+      double* row = W + (size_t)(j + 1 + r) * n + j + 1;
+      for (int c = lane; c < m; c += 32) row[c] -= ur * q[c] + qr * u[c];
     }
     // keep u in the column below the diagonal for the back-transformation
     for (int i = tid; i < m; i += nt) W[(size_t)(j + 1 + i) * n + j] = u[i];
@@ -375,7 +387,14 @@ __global__ void __launch_bounds__(1024) k_eigh_lowest(const double* __restrict__
     tau[n - 1] = 0.0;
   }
   __syncthreads();
-  // Bisection for eigenvalues r = 0..k-1 (ascending).
+  // T in shared memory for the Sturm counts: d and e^2.
+  double* ds = u;
+  double* e2s = q;
+  for (int i = tid; i < n; i += nt) {
+    ds[i] = d[i];
+    e2s[i] = (i + 1 < n) ? e[i] * e[i] : 0.0;
+  }
+  __syncthreads();
   double lo = 1e300, hi = -1e300, emax = 0.0;
   for (int i = 0; i < n; ++i) {
     const double r0 = (i > 0) ? fabs(e[i - 1]) : 0.0, r1 = (i + 1 < n) ? fabs(e[i]) : 0.0;
@@ -385,17 +404,66 @@ __global__ void __launch_bounds__(1024) k_eigh_lowest(const double* __restrict__
   }
   const double tnorm = fmax(fabs(lo), fabs(hi));
   const double pivmin = fmax(1e-300, 1e-290 * fmax(1.0, emax * emax));
-  for (int r = tid; r < k; r += nt) {
-    double a = lo - 1e-14 * tnorm - 1e-300, b = hi + 1e-14 * tnorm + 1e-300;
-    for (int it = 0; it < 200; ++it) {
-      const double mid = 0.5 * (a + b);
-      if (b - a <= 2.0 * 2.2e-16 * fmax(fabs(a), fabs(b)) + 1e-300) break;
-      if (sturm_count(d, e, n, mid, pivmin) > r)
-        b = mid;
-      else
-        a = mid;
+  const double a0 = lo - 1e-14 * tnorm - 1e-300, b0 = hi + 1e-14 * tnorm + 1e-300;
+  auto converged = [](double a, double b) { return b - a <= 2.0 * 2.2e-16 * fmax(fabs(a), fabs(b)) + 1e-300; };
+  if (k <= kEighMaxMulti && nt / k >= 2) {
+    // Multisection for the eigenvalues r = 0..k-1 (ascending): each round
+    // cuts every bracket [a_r, b_r] at P interior points, one Sturm count per
+    // thread, and keeps the sub-interval holding eigenvalue r (count(a) <= r
+    // < count(b)); a bracket shrinks (P + 1)-fold per round.
+    const int P = nt / k;
+    // Point j (1..P) of a bracket, computed the same way for the count and the update.
+    auto point = [P](double a, double b, int j) { return a + (b - a) * ((double)j / (double)(P + 1)); };
+    for (int r = tid; r < k; r += nt) {
+      br_lo[r] = a0;
+      br_hi[r] = b0;
     }
-    lam[r] = 0.5 * (a + b);
+    __syncthreads();
+    for (int round = 0; round < 64; ++round) {
+      const int r = tid / P, pp = tid - r * P;
+      if (r < k) {
+        const double a = br_lo[r], b = br_hi[r];
+        cnt[tid] = converged(a, b) ? -1 : sturm_count_sq(ds, e2s, n, point(a, b, pp + 1), pivmin);
+      }
+      __syncthreads();
+      if (tid == 0) br_done = 1;
+      __syncthreads();
+      if (tid < k) {
+        const double a = br_lo[tid], b = br_hi[tid];
+        if (!converged(a, b)) {
+          // First point whose count exceeds r: the eigenvalue lies between it
+          // and the point before.
+          int pf = P;
+          for (int p2 = 0; p2 < P; ++p2)
+            if (cnt[tid * P + p2] > tid) {
+              pf = p2;
+              break;
+            }
+          const double na = (pf == 0) ? a : point(a, b, pf);
+          const double nb = (pf == P) ? b : point(a, b, pf + 1);
+          br_lo[tid] = na;
+          br_hi[tid] = nb;
+          if (!converged(na, nb)) br_done = 0;
+        }
+      }
+      __syncthreads();
+      if (br_done) break;
+    }
+    for (int r = tid; r < k; r += nt) lam[r] = 0.5 * (br_lo[r] + br_hi[r]);
+  } else {
+    // Bisection, one thread per eigenvalue.
+    for (int r = tid; r < k; r += nt) {
+      double a = a0, b = b0;
+      for (int it = 0; it < 200; ++it) {
+        const double mid = 0.5 * (a + b);
+        if (converged(a, b)) break;
+        if (sturm_count_sq(ds, e2s, n, mid, pivmin) > r)
+          b = mid;
+        else
+          a = mid;
+      }
+      lam[r] = 0.5 * (a + b);
+    }
   }
   __syncthreads();
   // Inverse iteration on T - lam I (partial pivoting), three solves.
@@ -479,7 +547,6 @@ __global__ void __launch_bounds__(1024) k_eigh_lowest(const double* __restrict__
     __syncthreads();
   }
   // z = H_0 H_1 ... H_{n-3} y: one warp per vector.
-  const int lane = tid & 31, warp = tid >> 5, nwarp = nt >> 5;
   for (int r = warp; r < k; r += nwarp) {
     double* y = Y + (size_t)r * n;
     for (int j = n - 3; j >= 0; --j) {
