@@ -52,6 +52,8 @@ def parse():
     p.add_argument("--no-grad", action="store_true")
     p.add_argument("--no-bse", action="store_true")
     p.add_argument("--batch-workers", type=int, default=0)
+    p.add_argument("--batch-largest", type=int, default=0,
+                   help="profiling aid: run the batch leg on its K largest systems only (0: all 64)")
     p.add_argument("--bse-fd-points", type=int, default=4)
     p.add_argument("--p0-form", choices=["auto", "materialised", "pair", "converter"], default="auto",
                    help="form of the split P0 (chi-scaled operand materialised, or built while staged)")
@@ -295,7 +297,7 @@ def batch64_flops(shapes, nw):
     return tot
 
 
-def bench_batch64(q, dev, precision, steps, warmup, nworkers):
+def bench_batch64(q, dev, precision, steps, warmup, nworkers, largest=0):
     """64 independent G0W0-CD systems (nmo ~ U[40, 400], nocc = round(nmo/6),
     naux = round(3.5 nmo), ||Pi(0)|| ~ U[1, 6], 24-point grid, HOMO-2..LUMO+2,
     HF reference Vxc = diag(Sigma_x), linearized QP step: batched G0W0 = one
@@ -306,6 +308,9 @@ def bench_batch64(q, dev, precision, steps, warmup, nworkers):
     import torch
     from quasix_b200.synth import batch64_shapes, systems_on_device
     shapes = batch64_shapes()
+    if largest:
+        # A small case of the same kernels (profiling): the largest systems only.
+        shapes = sorted(shapes, key=lambda sh: -(sh[1] + sh[2]))[:largest]
     systems = []
     t_draw = time.perf_counter()
     drawn = systems_on_device(shapes, device=dev, threads=min(16, host_cores()))
@@ -335,7 +340,9 @@ def bench_batch64(q, dev, precision, steps, warmup, nworkers):
     flops = batch64_flops(shapes, nw)
     del systems
     torch.cuda.empty_cache()
-    return {"workload": "g0w0_cd_batch64_nmo40-400_nw24", "systems": n, "nworkers": nworkers,
+    return {"workload": ("g0w0_cd_batch64_nmo40-400_nw24" if not largest
+                         else f"g0w0_cd_batch64_largest{largest}_nw24 (profiling subset)"),
+            "systems": n, "nworkers": nworkers,
             "mode": "grouped (every inversion one grouped block sweep)" if nworkers == 0
             else f"{nworkers} per-system worker streams", "qp": "linearized",
             "precision": precision, "steps": steps, "warmup": warmup,
@@ -742,7 +749,8 @@ def main():
     if not args.no_bse:
         line["bse_dim26400"] = bench_bse_dim26400(q, prec_main, fd_points=args.bse_fd_points)
     if not args.no_batch64:
-        line["batch64_g0w0_cd"] = bench_batch64(q, dev, prec_main, steps=3, warmup=1, nworkers=args.batch_workers)
+        line["batch64_g0w0_cd"] = bench_batch64(q, dev, prec_main, steps=3, warmup=1, nworkers=args.batch_workers,
+                                                    largest=args.batch_largest)
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(sysm, vxc.cpu().numpy() if hasattr(vxc, "cpu") else vxc)
     if rank == 0:
