@@ -57,6 +57,8 @@ def parse():
     p.add_argument("--bse-fd-points", type=int, default=4)
     p.add_argument("--p0-form", choices=["auto", "materialised", "pair", "converter"], default="auto",
                    help="form of the split P0 (chi-scaled operand materialised, or built while staged)")
+    p.add_argument("--contraction-form", choices=["auto", "single", "pair"], default="auto",
+                   help="tiles of the split pair contraction (one CTA, or CTA pairs)")
     return p.parse_args()
 
 
@@ -590,6 +592,7 @@ def main():
     vxc = q.compute_exchange_diag(lpq_d, sysm.nocc, device=dev)
     ctx = N.context(dev)
     ctx.set_p0_form(args.p0_form)
+    ctx.set_contraction_form(args.contraction_form)
     have_tc = True
     prec_main = args.precision or "fp16x3"
 
@@ -723,7 +726,7 @@ def main():
             "data": "synthetic",
             "config": {"workload": WORKLOAD, "nocc": NOCC, "nvirt": NVIR, "naux": NAUX, "nw": NW, "seed": SEED,
                        "orbitals": "all", "qp": "linearized", "vxc": "diag(Sigma_x) (HF reference)",
-                       "precision": prec_main, "p0_form": args.p0_form,
+                       "precision": prec_main, "p0_form": args.p0_form, "contraction_form": args.contraction_form,
                        "parallelism": f"replicas{world}" if world > 1 else "single",
                        "l2": "inputs larger than L2 (lpq 720 MB, pair tensor 361 MB); no flush"},
             "fp64_gpu_iter_per_s": fp64_rate, "speedup_vs_fp64_gpu": value / fp64_rate,

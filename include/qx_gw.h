@@ -73,6 +73,13 @@ qx_status qx_ctx_last_guard_stats(const qx_ctx* ctx, int64_t* guarded, int64_t* 
  * 6 GiB of such operands and converts beyond. */
 enum { QX_P0_AUTO = 0, QX_P0_MATERIALISED = 1, QX_P0_CONVERTER = 2, QX_P0_PAIR = 3 };
 qx_status qx_ctx_set_p0_form(qx_ctx* ctx, int form);
+/* Tiles of the split-precision pair contraction Sigma_c needs (v = B W' B^T
+ * row by row; no reference counterpart): QX_CONTRACT_SINGLE one 128-row pair
+ * block per CTA; QX_CONTRACT_PAIR two pair blocks per CTA pair (tcgen05
+ * cta_group::2, M = 256), each CTA staging half of the W' tile;
+ * QX_CONTRACT_AUTO (default) takes the pair form. */
+enum { QX_CONTRACT_AUTO = 0, QX_CONTRACT_SINGLE = 1, QX_CONTRACT_PAIR = 2 };
+qx_status qx_ctx_set_contraction_form(qx_ctx* ctx, int form);
 /* Library version string. */
 const char* qx_version(void);
 

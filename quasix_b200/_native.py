@@ -22,6 +22,7 @@ STATUS_NAMES = {
 PREC = {"fp64": 0, "bf16x3": 1, "fp16x3": 2}
 QP_SOLVER = {"newton": 0, "linearized": 1}
 P0_FORM = {"auto": 0, "materialised": 1, "converter": 2, "pair": 3}
+CONTRACTION_FORM = {"auto": 0, "single": 1, "pair": 2}
 
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int)
@@ -95,6 +96,7 @@ SIGNATURES = {
     "qx_ctx_last_launches": (C.c_int64, [_vp]),
     "qx_ctx_last_guard_stats": (C.c_int, [_vp, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
     "qx_ctx_set_p0_form": (C.c_int, [_vp, C.c_int]),
+    "qx_ctx_set_contraction_form": (C.c_int, [_vp, C.c_int]),
     "qx_version": (C.c_char_p, []),
     "qx_get_scaled_legendre_roots": (C.c_int, [C.c_int, C.c_double, _vp, _vp]),
     "qx_get_rho_response": (C.c_int, [_vp, C.c_int, _vp, _vp, _vp, C.c_int, C.c_int, C.c_int, C.c_int, _vp]),
@@ -210,6 +212,10 @@ class Context:
     def set_p0_form(self, form: str):
         """'auto', 'materialised', 'pair' or 'converter' (qx_ctx_set_p0_form)."""
         self.check(self.lib.qx_ctx_set_p0_form(self.handle, P0_FORM[form]))
+
+    def set_contraction_form(self, form: str):
+        """'auto', 'single' or 'pair' (qx_ctx_set_contraction_form)."""
+        self.check(self.lib.qx_ctx_set_contraction_form(self.handle, CONTRACTION_FORM[form]))
 
     def guard_stats(self):
         """(guarded, reinverted): eps inversions of the last call that ran

@@ -139,6 +139,99 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
   for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+// CTA-pair (cluster of two) helpers.
+__device__ __forceinline__ uint32_t cluster_ctarank() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;\n" : "=r"(r));
+  return r;
+}
+__device__ __forceinline__ uint32_t cluster_nctarank() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%cluster_nctarank;\n" : "=r"(r));
+  return r;
+}
+__device__ __forceinline__ uint32_t cluster_id_x() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%clusterid.x;\n" : "=r"(r));
+  return r;
+}
+__device__ __forceinline__ uint32_t cluster_count_x() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%nclusterid.x;\n" : "=r"(r));
+  return r;
+}
+// The shared::cluster address of the same shared-memory offset in CTA rank.
+__device__ __forceinline__ uint32_t mapa_rank(uint32_t saddr, uint32_t rank) {
+  uint32_t r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;\n" : "=r"(r) : "r"(saddr), "r"(rank));
+  return r;
+}
+__device__ __forceinline__ void cluster_sync_all() {
+  asm volatile("barrier.cluster.arrive.release.aligned;\n" ::: "memory");
+  asm volatile("barrier.cluster.wait.acquire.aligned;\n" ::: "memory");
+}
+// TMA loads into this CTA's shared memory whose completion is counted on an
+// mbarrier of either CTA of the pair (shared::cluster address).
+__device__ __forceinline__ void tma_load_2d_pair(uint32_t dst, const CUtensorMap* map, uint32_t bar, int c0, int c1) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, "
+      "%4}], [%2];\n" ::"r"(dst),
+      "l"(map), "r"(bar), "r"(c0), "r"(c1)
+      : "memory");
+}
+__device__ __forceinline__ void tma_load_3d_pair(uint32_t dst, const CUtensorMap* map, uint32_t bar, int c0, int c1,
+                                                 int c2) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, "
+      "%4, %5}], [%2];\n" ::"r"(dst),
+      "l"(map), "r"(bar), "r"(c0), "r"(c1), "r"(c2)
+      : "memory");
+}
+__device__ __forceinline__ void umma_f16_pair(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                              uint32_t accumulate) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(
+          tmem_d),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
+}
+// Arrive on the mbarrier at this offset in both CTAs once the MMAs issued so far complete.
+__device__ __forceinline__ void umma_commit_pair_both(uint64_t* bar) {
+  asm volatile(
+      "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], %1;\n" ::"r"(
+          smem_u32(bar)),
+      "h"((unsigned short)3)
+      : "memory");
+}
+__device__ __forceinline__ void umma_commit_pair_own(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(smem_u32(bar))
+               : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_rank(uint64_t* bar, uint32_t rank) {
+  asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];\n" ::"r"(mapa_rank(smem_u32(bar), rank))
+               : "memory");
+}
+// mbar_wait with cluster-scope acquire (arrivals from the other CTA).
+__device__ __forceinline__ bool mbar_wait_cluster(uint64_t* bar, uint32_t parity, volatile int* abort_flag, int* err,
+                                                  int code) {
+  const long long t0 = clock64();
+  while (true) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, "
+        "0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    if (ok) return true;
+    if (*abort_flag) return false;
+    if (clock64() - t0 > WAIT_CYCLES) {
+      *abort_flag = 1;
+      atomicCAS(err, 0, code);
+      return false;
+    }
+  }
+}
+
 // ---------------------------------------------------------------------------
 // The GEMM kernel.
 // ---------------------------------------------------------------------------
@@ -1527,6 +1620,280 @@ static int tuned_wgroup(qx_ctx* ctx, int npair, int naux, int nw, F&& launch_wit
 
 // v[w][p] = 2 sum_Q X[p][Q] sum_{P <= Q} (Bh+Bl)[p][P] (W'h+W'l)[w][Q][P] / (sA sB[w]),
 // W' the half-lower form of Wc (three products per term)
+// ---------------------------------------------------------------------------
+// The pair contraction on CTA pairs (tcgen05 cta_group::2, M = 256, N = 256).
+// ---------------------------------------------------------------------------
+// The two CTAs of a cluster take the items (pair-block pair, frequency) in the
+// order of the single-CTA form; CTA r of the pair holds pair block 2 i + r
+// (a copy of 2 i, not stored, past the last block) and, of each 256-wide N
+// tile of W', the rows [n0 + 128 r, n0 + 128 r + 128).  The even CTA's MMAs
+// read both CTAs' operands and leave each CTA's 128 x 256 accumulator in its
+// own TMEM, which its ROWDOT epilogue contracts with its own pair rows.  Per
+// k block an SM loads 64 KB (its A rows and half of the W' tile) instead of
+// 96 KB: in the single-CTA form the MMA thread waited ~40 % of each k block
+// for the TMA loads.  Barrier protocol as in k_p0_pair.
+namespace pairrd {
+constexpr int STAGES = 3;
+constexpr int BK = 64;
+constexpr int BN = 256;                              // N of the MMA (both CTAs)
+constexpr int A_BYTES = TC_BM * BK * 2;              // 16 KB: this CTA's 128 pair rows
+constexpr int B_BYTES = (BN / 2) * BK * 2;           // 16 KB: half of the W' tile
+constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;  // 64 KB
+constexpr int BAR_OFF = STAGES * STAGE_BYTES;
+constexpr int RED_OFF = BAR_OFF + 256;
+constexpr int TOTAL = RED_OFF + 2 * (2 * TC_BM + 8) * 8 + 1024;
+constexpr int NEPI = 8;
+constexpr int THREADS = 64 + 32 * NEPI;
+}  // namespace pairrd
+
+__global__ void __launch_bounds__(pairrd::THREADS, 1)
+    k_rowdot_pair(const __grid_constant__ CUtensorMap mapAh, const __grid_constant__ CUtensorMap mapAl,
+                  const __grid_constant__ CUtensorMap mapBh, const __grid_constant__ CUtensorMap mapBl, TcArgs args) {
+  namespace P = pairrd;
+  if (cluster_nctarank() != 2) {
+    if (threadIdx.x == 0) atomicCAS(args.err, 0, 30);
+    return;
+  }
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + P::BAR_OFF);
+  uint64_t* empty = full + P::STAGES;
+  uint64_t* acc_full = empty + P::STAGES;  // [2]
+  uint64_t* acc_empty = acc_full + 2;      // [2]
+  uint64_t* drain = acc_empty + 2;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain + 1);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t rank = cluster_ctarank();
+  const bool leader = rank == 0;
+  const int n_tiles = (args.N + P::BN - 1) / P::BN;
+  const int k_blocks = (args.K + P::BK - 1) / P::BK;
+  const int mpairs = (args.m_blocks + 1) / 2;
+  const int g = args.wgroup;
+  const int n_items = (args.nbatch + g - 1) / g * mpairs * g;
+  const int item0 = (int)cluster_id_x(), item_step = (int)cluster_count_x();
+  // Item -> frequency, this CTA's pair block and whether its rows are stored.
+  auto item_of = [&](int b, int& mb, int& w, bool& store) {
+    const int per_group = mpairs * g;
+    const int grp = b / per_group, r = b % per_group;
+    const int mp = r / g;
+    w = grp * g + r % g;
+    mb = 2 * mp + (int)rank;
+    store = mb < args.m_blocks;
+    if (!store) mb = 2 * mp;
+  };
+  // K range of N tile nt: W' is half-lower, zero past column n0 + BN.
+  auto kbe_of = [&](int nt) { return min(k_blocks, (nt * P::BN + P::BN + P::BK - 1) / P::BK); };
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < P::STAGES; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&acc_full[b], 1);
+      mbar_init(&acc_empty[b], 2 * P::NEPI);  // every epilogue warp of both CTAs
+    }
+    mbar_init(drain, 1);
+    *abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(tmem_slot)),
+                 "r"(2 * P::BN));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;\n" ::);
+  }
+  tc_fence_before();
+  __syncthreads();
+  cluster_sync_all();
+  tc_fence_after();
+  const uint32_t tmem_base = *tmem_slot;
+
+  if (warp == 0) {
+    // ---------------- TMA producer (both CTAs) ----------------
+    if (lane == 0) {
+      const uint32_t full_leader = mapa_rank(smem_u32(full), 0);
+      int gk = 0;
+      bool ok = true;
+      for (int it = item0; it < n_items && ok; it += item_step) {
+        int mb, w;
+        bool st;
+        item_of(it, mb, w, st);
+        if (w >= args.nbatch) continue;
+        for (int nt = 0; nt < n_tiles && ok; ++nt) {
+          const int kbe = kbe_of(nt);
+          for (int kb = 0; kb < kbe; ++kb, ++gk) {
+            const int s = gk % P::STAGES;
+            if (gk >= P::STAGES && !mbar_wait(&empty[s], ((gk / P::STAGES) - 1) & 1, abort_flag, args.err, 31)) {
+              ok = false;
+              break;
+            }
+            if (leader) mbar_expect_tx(&full[s], 2 * P::STAGE_BYTES);
+            const uint32_t dst = smem_u32(smem + s * P::STAGE_BYTES);
+            const uint32_t fb = full_leader + s * 8;
+            const int k0 = kb * P::BK;
+            const int brow = nt * P::BN + (P::BN / 2) * (int)rank;
+            tma_load_2d_pair(dst, &mapAh, fb, k0, mb * TC_BM);
+            tma_load_2d_pair(dst + P::A_BYTES, &mapAl, fb, k0, mb * TC_BM);
+            tma_load_3d_pair(dst + 2 * P::A_BYTES, &mapBh, fb, k0, brow, w);
+            tma_load_3d_pair(dst + 2 * P::A_BYTES + P::B_BYTES, &mapBl, fb, k0, brow, w);
+          }
+        }
+      }
+      for (int q = (gk > P::STAGES ? gk - P::STAGES : 0); q < gk; ++q) {
+        volatile int no_abort = 0;
+        mbar_wait(&empty[q % P::STAGES], (q / P::STAGES) & 1, &no_abort, args.err, 32);
+      }
+    }
+  } else if (warp == 1) {
+    // ---------------- MMA issuer (even CTA) ----------------
+    if (leader && lane == 0) {
+      const uint32_t idesc = umma_idesc_f16(2 * TC_BM, P::BN, args.fp16);
+      int gk = 0, t = 0;
+      bool ok = true;
+      for (int it = item0; it < n_items && ok; it += item_step) {
+        int mb, w;
+        bool st;
+        item_of(it, mb, w, st);
+        if (w >= args.nbatch) continue;
+        for (int nt = 0; nt < n_tiles && ok; ++nt, ++t) {
+          const int kbe = kbe_of(nt);
+          const int buf = t & 1;
+          if (t >= 2 && !mbar_wait_cluster(&acc_empty[buf], ((t / 2) - 1) & 1, abort_flag, args.err, 33)) {
+            ok = false;
+            break;
+          }
+          const uint32_t dacc = tmem_base + buf * P::BN;
+          for (int kb = 0; kb < kbe; ++kb, ++gk) {
+            const int s = gk % P::STAGES;
+            if (!mbar_wait(&full[s], (gk / P::STAGES) & 1, abort_flag, args.err, 34)) {
+              ok = false;
+              break;
+            }
+            tc_fence_after();
+            const uint32_t ah = smem_u32(smem + s * P::STAGE_BYTES), al = ah + P::A_BYTES;
+            const uint32_t bh = ah + 2 * P::A_BYTES, bl = bh + P::B_BYTES;
+#pragma unroll
+            for (int kk = 0; kk < P::BK / 16; ++kk) {
+              const uint32_t off = kk * 32;
+              const uint32_t acc0 = (kb > 0 || kk > 0) ? 1u : 0u;
+              umma_f16_pair(dacc, umma_desc<P::BK>(ah + off), umma_desc<P::BK>(bh + off), idesc, acc0);
+              umma_f16_pair(dacc, umma_desc<P::BK>(ah + off), umma_desc<P::BK>(bl + off), idesc, 1u);
+              umma_f16_pair(dacc, umma_desc<P::BK>(al + off), umma_desc<P::BK>(bh + off), idesc, 1u);
+            }
+            umma_commit_pair_both(&empty[s]);
+          }
+          if (!ok) break;
+          umma_commit_pair_both(&acc_full[buf]);
+        }
+      }
+      umma_commit_pair_own(drain);
+      volatile int no_abort = 0;
+      mbar_wait(drain, 0, &no_abort, args.err, 35);
+    }
+  } else {
+    // ---------------- epilogue (warps 2..9, both CTAs): row dot products ----------------
+    const int quarter = warp & 3;
+    const int half = (warp - 2) >> 2;
+    const int row = quarter * 32 + lane;
+    constexpr int HB = P::BN / 2;
+    int t = 0, done_items = 0;
+    bool ok = true;
+    for (int it = item0; it < n_items && ok; it += item_step) {
+      int mb, w;
+      bool st;
+      item_of(it, mb, w, st);
+      if (w >= args.nbatch) continue;
+      const int m = mb * TC_BM + row;
+      double rowsum = 0.0;
+      int tiles_done = 0;
+      for (int nt = 0; nt < n_tiles; ++nt, ++t) {
+        const int buf = t & 1;
+        if (!mbar_wait(&acc_full[buf], (t / 2) & 1, abort_flag, args.err, 36)) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const int n0 = nt * P::BN + half * HB;
+        const uint32_t taddr = tmem_base + ((uint32_t)(quarter * 32) << 16) + buf * P::BN + half * HB;
+        const float* xrow = args.X + (size_t)(m < args.M ? m : 0) * args.ldx + n0;
+        float xn[16];
+        load_x16(xrow, n0, args.N, m < args.M, xn);
+#pragma unroll 1
+        for (int c = 0; c < HB; c += 16) {
+          float xc[16];
+#pragma unroll
+          for (int q = 0; q < 16; ++q) xc[q] = xn[q];
+          if (c + 16 < HB) load_x16(xrow + c + 16, n0 + c + 16, args.N, m < args.M, xn);
+          float v[16];
+          tmem_ld16(taddr + c, v);
+#pragma unroll
+          for (int q = 0; q < 16; q += 4)
+            rowsum += (double)v[q] * xc[q] + (double)v[q + 1] * xc[q + 1] + (double)v[q + 2] * xc[q + 2] +
+                      (double)v[q + 3] * xc[q + 3];
+        }
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) {
+          if (leader)
+            mbar_arrive(&acc_empty[buf]);
+          else
+            mbar_arrive_rank(&acc_empty[buf], 0);
+        }
+        ++tiles_done;
+      }
+      // Combine the two halves (named barrier of the 8 epilogue warps, reached
+      // by every one of them, also after an abort); the buffer alternates
+      // between items.
+      double* red = reinterpret_cast<double*>(smem + P::RED_OFF) + (done_items & 1) * (2 * TC_BM + 8);
+      int* done = reinterpret_cast<int*>(red + 2 * TC_BM);
+      const bool full_item = tiles_done == n_tiles;
+      red[half * TC_BM + row] = full_item ? rowsum : 0.0;
+      if (lane == 0 && quarter == 0) done[half] = full_item ? 1 : 0;
+      asm volatile("bar.sync 1, 256;\n" ::: "memory");
+      if (half == 0 && st && m < args.M && done[0] && done[1])
+        args.out[(size_t)w * args.ldo + m] = (red[row] + red[TC_BM + row]) * unscale_rowdot(args, w) * 2.0;
+      ++done_items;
+      ok = done[0] && done[1];
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  cluster_sync_all();
+  tc_fence_after();
+  if (warp == 1) {
+    asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;\n" ::"r"(tmem_base), "r"(2 * P::BN));
+  }
+}
+
+static void launch_rowdot_pair(qx_ctx* ctx, const CUtensorMap& ah, const CUtensorMap& al, const CUtensorMap& bh,
+                               const CUtensorMap& bl, const TcArgs& a) {
+  static PerDeviceOnce attr_once;
+  static int max_clusters[PerDeviceOnce::kMaxDevices] = {};
+  cudaLaunchConfig_t cfg = {};
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = 2;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.blockDim = dim3(pairrd::THREADS);
+  cfg.dynamicSmemBytes = pairrd::TOTAL;
+  cfg.stream = ctx->stream;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  attr_once(ctx->device, [&] {
+    QX_CUDA(cudaFuncSetAttribute(k_rowdot_pair, cudaFuncAttributeMaxDynamicSharedMemorySize, pairrd::TOTAL));
+    cfg.gridDim = dim3(2 * ctx->sm_count);
+    int n = 0;
+    QX_CUDA(cudaOccupancyMaxActiveClusters(&n, k_rowdot_pair, &cfg));
+    max_clusters[ctx->device] = std::max(n, 1);
+  });
+  const int items = ceil_div(a.nbatch, a.wgroup) * ceil_div(a.m_blocks, 2) * a.wgroup;
+  cfg.gridDim = dim3(2 * std::min(items, max_clusters[ctx->device]));
+  QX_CUDA(cudaLaunchKernelEx(&cfg, k_rowdot_pair, ah, al, bh, bl, a));
+  check_launch(ctx);
+}
+
 void launch_pair_contract_tc(qx_ctx* ctx, const TcOperand& A, const float* bpt_f32, int ldk, int npair, int naux,
                              const TcOperand& W, int ldw, size_t wc_stride, int nw, double* v, int ldv, int fp16) {
   constexpr int BN = 256;
@@ -1534,8 +1901,10 @@ void launch_pair_contract_tc(qx_ctx* ctx, const TcOperand& A, const float* bpt_f
   constexpr int BK = TcPipe<EPI_ROWDOT>::BK;
   CUtensorMap ah = make_map(A.hi, naux, npair, ldk, 1, TC_BM, 2, fp16, BK);
   CUtensorMap al = make_map(A.lo, naux, npair, ldk, 1, TC_BM, 2, fp16, BK);
-  CUtensorMap bh = make_map(W.hi, naux, naux, ldw, nw, BN, 3, fp16, BK);
-  CUtensorMap bl = make_map(W.lo, naux, naux, ldw, nw, BN, 3, fp16, BK);
+  // CTA pairs stage half of each W' tile per CTA.
+  const bool pair = ctx->contraction_form != QX_CONTRACT_SINGLE;
+  CUtensorMap bh = make_map(W.hi, naux, naux, ldw, nw, pair ? BN / 2 : BN, 3, fp16, BK);
+  CUtensorMap bl = make_map(W.lo, naux, naux, ldw, nw, pair ? BN / 2 : BN, 3, fp16, BK);
   int* d_err = tc_err_slot(ctx);
   QX_CUDA(cudaMemsetAsync(d_err, 0, sizeof(int), ctx->stream));
   TcArgs a{};
@@ -1562,9 +1931,13 @@ void launch_pair_contract_tc(qx_ctx* ctx, const TcOperand& A, const float* bpt_f
   // per shape by timing the candidates on the call's own data.
   auto launch_with = [&](int g) {
     a.wgroup = g;
-    // Persistent: one CTA per SM (192 KB of stages each) over all items.
-    const int items = ceil_div(nw, g) * a.m_blocks * g;
-    launch_tc<BN, EPI_ROWDOT>(ctx, ah, al, bh, bl, a, dim3(std::min(items, ctx->sm_count)));
+    if (pair) {
+      launch_rowdot_pair(ctx, ah, al, bh, bl, a);
+    } else {
+      // Persistent: one CTA per SM (192 KB of stages each) over all items.
+      const int items = ceil_div(nw, g) * a.m_blocks * g;
+      launch_tc<BN, EPI_ROWDOT>(ctx, ah, al, bh, bl, a, dim3(std::min(items, ctx->sm_count)));
+    }
   };
   a.wgroup = tuned_wgroup(ctx, npair, naux, nw, launch_with);
   launch_with(a.wgroup);
@@ -1663,98 +2036,6 @@ __device__ __forceinline__ void p0_pair_tile(int r, int T, int& nt, int& ma) {
     c += cnt;
   }
   ma = nt + 2 * (r - c);
-}
-
-__device__ __forceinline__ uint32_t cluster_ctarank() {
-  uint32_t r;
-  asm volatile("mov.u32 %0, %%cluster_ctarank;\n" : "=r"(r));
-  return r;
-}
-__device__ __forceinline__ uint32_t cluster_nctarank() {
-  uint32_t r;
-  asm volatile("mov.u32 %0, %%cluster_nctarank;\n" : "=r"(r));
-  return r;
-}
-__device__ __forceinline__ uint32_t cluster_id_x() {
-  uint32_t r;
-  asm volatile("mov.u32 %0, %%clusterid.x;\n" : "=r"(r));
-  return r;
-}
-__device__ __forceinline__ uint32_t cluster_count_x() {
-  uint32_t r;
-  asm volatile("mov.u32 %0, %%nclusterid.x;\n" : "=r"(r));
-  return r;
-}
-// The shared::cluster address of the same shared-memory offset in CTA rank.
-__device__ __forceinline__ uint32_t mapa_rank(uint32_t saddr, uint32_t rank) {
-  uint32_t r;
-  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;\n" : "=r"(r) : "r"(saddr), "r"(rank));
-  return r;
-}
-__device__ __forceinline__ void cluster_sync_all() {
-  asm volatile("barrier.cluster.arrive.release.aligned;\n" ::: "memory");
-  asm volatile("barrier.cluster.wait.acquire.aligned;\n" ::: "memory");
-}
-// TMA loads into this CTA's shared memory whose completion is counted on an
-// mbarrier of either CTA of the pair (shared::cluster address).
-__device__ __forceinline__ void tma_load_2d_pair(uint32_t dst, const CUtensorMap* map, uint32_t bar, int c0, int c1) {
-  asm volatile(
-      "cp.async.bulk.tensor.2d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, "
-      "%4}], [%2];\n" ::"r"(dst),
-      "l"(map), "r"(bar), "r"(c0), "r"(c1)
-      : "memory");
-}
-__device__ __forceinline__ void tma_load_3d_pair(uint32_t dst, const CUtensorMap* map, uint32_t bar, int c0, int c1,
-                                                 int c2) {
-  asm volatile(
-      "cp.async.bulk.tensor.3d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, "
-      "%4, %5}], [%2];\n" ::"r"(dst),
-      "l"(map), "r"(bar), "r"(c0), "r"(c1), "r"(c2)
-      : "memory");
-}
-__device__ __forceinline__ void umma_f16_pair(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
-                                              uint32_t accumulate) {
-  asm volatile(
-      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(
-          tmem_d),
-      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
-}
-// Arrive on the mbarrier at this offset in both CTAs once the MMAs issued so far complete.
-__device__ __forceinline__ void umma_commit_pair_both(uint64_t* bar) {
-  asm volatile(
-      "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], %1;\n" ::"r"(
-          smem_u32(bar)),
-      "h"((unsigned short)3)
-      : "memory");
-}
-__device__ __forceinline__ void umma_commit_pair_own(uint64_t* bar) {
-  asm volatile("tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(smem_u32(bar))
-               : "memory");
-}
-__device__ __forceinline__ void mbar_arrive_rank(uint64_t* bar, uint32_t rank) {
-  asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];\n" ::"r"(mapa_rank(smem_u32(bar), rank))
-               : "memory");
-}
-// mbar_wait with cluster-scope acquire (arrivals from the other CTA).
-__device__ __forceinline__ bool mbar_wait_cluster(uint64_t* bar, uint32_t parity, volatile int* abort_flag, int* err,
-                                                  int code) {
-  const long long t0 = clock64();
-  while (true) {
-    uint32_t ok;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, "
-        "0, p;\n}\n"
-        : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity)
-        : "memory");
-    if (ok) return true;
-    if (*abort_flag) return false;
-    if (clock64() - t0 > WAIT_CYCLES) {
-      *abort_flag = 1;
-      atomicCAS(err, 0, code);
-      return false;
-    }
-  }
 }
 
 __global__ void __launch_bounds__(pairp0::THREADS, 1)

@@ -526,6 +526,13 @@ qx_status qx_ctx_set_stream(qx_ctx* c, void* stream) {
   return QX_OK;
 }
 
+qx_status qx_ctx_set_contraction_form(qx_ctx* c, int form) {
+  if (!c || form < QX_CONTRACT_AUTO || form > QX_CONTRACT_PAIR) return QX_ERR_INVALID_INPUT;
+  c->contraction_form = form;
+  for (qx_ctx* w : c->workers) w->contraction_form = form;
+  return QX_OK;
+}
+
 qx_status qx_ctx_set_p0_form(qx_ctx* c, int form) {
   if (!c || form < QX_P0_AUTO || form > QX_P0_PAIR) return QX_ERR_INVALID_INPUT;
   c->p0_form = form;

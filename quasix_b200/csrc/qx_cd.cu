@@ -633,7 +633,10 @@ static void cd_batch_grouped(qx_ctx* ctx, qx_cd_system* systems, int nsys, int n
     }
     const int W = (int)wave.size();
     while ((int)ctx->workers.size() < W) ctx->workers.push_back(make_worker(ctx->device));
-    for (qx_ctx* wk : ctx->workers) wk->p0_form = ctx->p0_form;
+    for (qx_ctx* wk : ctx->workers) {
+      wk->p0_form = ctx->p0_form;
+      wk->contraction_form = ctx->contraction_form;
+    }
     std::vector<CdProblem> probs(W);
     std::vector<CdRun> runs(W);
     std::vector<char> ok(W, 1);
@@ -821,7 +824,10 @@ extern "C" qx_status qx_g0w0_cd_batch(qx_ctx* ctx, qx_cd_system* systems, int ns
     if (nworkers < 0) nworkers = 4;
     nworkers = std::min(std::min(nworkers, 16), nsys);
     while ((int)ctx->workers.size() < nworkers) ctx->workers.push_back(make_worker(ctx->device));
-    for (qx_ctx* wk : ctx->workers) wk->p0_form = ctx->p0_form;
+    for (qx_ctx* wk : ctx->workers) {
+      wk->p0_form = ctx->p0_form;
+      wk->contraction_form = ctx->contraction_form;
+    }
     // Largest systems first (P0 cost nov * naux^2 dominates), so that the
     // small ones fill in behind them.
     std::vector<int> order(nsys);

@@ -132,6 +132,7 @@ struct qx_ctx {
   // Form of the split-precision P0 (QX_P0_AUTO / _MATERIALISED / _CONVERTER);
   // batch workers inherit it from their parent context.
   int p0_form = 0;
+  int contraction_form = 0;  // QX_CONTRACT_*: tiles of the split pair contraction
 };
 
 namespace qx {

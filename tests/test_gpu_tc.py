@@ -40,6 +40,19 @@ def p0_form(q):
     ctx.set_p0_form("auto")
 
 
+@pytest.fixture
+def contraction_form(q):
+    """Set the split pair-contraction form of the default context for one test."""
+    from quasix_b200 import _native
+    ctx = _native.context(0)
+
+    def use(form):
+        ctx.set_contraction_form(form)
+
+    yield use
+    ctx.set_contraction_form("auto")
+
+
 @pytest.mark.parametrize("form", ["materialised", "pair", "converter"])
 @pytest.mark.parametrize("prec", ["bf16x3", "fp16x3"])
 @pytest.mark.parametrize("shape", [(5, 19, 84), (12, 61, 250), (20, 130, 520)])
@@ -61,10 +74,14 @@ def test_rho_response_tc(q, p0_form, shape, prec, form):
         assert np.abs(got[k] - got[k].T).max() < 1e-12 * max(scale, 1.0)
 
 
+@pytest.mark.parametrize("cform", ["single", "pair"])
 @pytest.mark.parametrize("prec", ["bf16x3", "fp16x3"])
 @pytest.mark.parametrize("shape,nw,orbs", [((5, 19, 84), 16, None), ((12, 61, 250), 24, [0, 11, 12, 72]),
                                            ((20, 130, 520), 20, [19, 20])])
-def test_sigma_diag_tc(q, shape, nw, orbs, prec):
+def test_sigma_diag_tc(q, contraction_form, shape, nw, orbs, prec, cform):
+    """The pair contraction on one CTA per pair block, or on CTA pairs (the
+    pair counts give odd and even numbers of 128-row pair blocks)."""
+    contraction_form(cform)
     nocc, nvir, naux = shape
     s = make_system(nocc, nvir, naux, seed=5, pi_norm=3.0)
     orbs = list(range(s.nmo)) if orbs is None else orbs
