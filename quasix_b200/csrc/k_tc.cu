@@ -393,6 +393,21 @@ __device__ __forceinline__ void load_x16(const float* xr, int col0, int N, bool 
   }
 }
 
+// sum_q v[q] x[q] over a 16-value chunk: two FP32 FMA chains, one conversion
+// to FP64 per chunk.  Converting both factors of every product to FP64 (two
+// conversions and an FP64 FMA per value) bounded the ROWDOT epilogue; the
+// chunk sums err by ~1e-6 relative, below the FP32 accumulation of the
+// accumulator itself over K.
+__device__ __forceinline__ double chunk_dot16(const float (&v)[16], const float (&x)[16]) {
+  float s0 = 0.0f, s1 = 0.0f;
+#pragma unroll
+  for (int q = 0; q < 16; q += 2) {
+    s0 = fmaf(v[q], x[q], s0);
+    s1 = fmaf(v[q + 1], x[q + 1], s1);
+  }
+  return (double)s0 + (double)s1;
+}
+
 __device__ __forceinline__ double unscale_rowdot(const TcArgs& a, int w) {
   return 1.0 / ((double)a.scaleA[0] * (double)a.scaleB[w]);
 }
@@ -844,10 +859,7 @@ __global__ void __launch_bounds__(TcThreads<EPI, CONVB>::VALUE, 1)
             if (c + 16 < HB) load_x16(xrow + c + 16, n0 + c + 16, args.N, m < args.M, xn);
             float v[16];
             tmem_ld16(taddr + c, v);
-#pragma unroll
-            for (int q = 0; q < 16; q += 4)
-              rowsum += (double)v[q] * xc[q] + (double)v[q + 1] * xc[q + 1] + (double)v[q + 2] * xc[q + 2] +
-                        (double)v[q + 3] * xc[q + 3];
+            rowsum += chunk_dot16(v, xc);
           }
           tc_fence_before();
           __syncwarp();
@@ -1827,10 +1839,7 @@ __global__ void __launch_bounds__(pairrd::THREADS, 1)
           if (c + 16 < HB) load_x16(xrow + c + 16, n0 + c + 16, args.N, m < args.M, xn);
           float v[16];
           tmem_ld16(taddr + c, v);
-#pragma unroll
-          for (int q = 0; q < 16; q += 4)
-            rowsum += (double)v[q] * xc[q] + (double)v[q + 1] * xc[q + 1] + (double)v[q + 2] * xc[q + 2] +
-                      (double)v[q + 3] * xc[q + 3];
+          rowsum += chunk_dot16(v, xc);
         }
         tc_fence_before();
         __syncwarp();
