@@ -256,7 +256,15 @@ struct TcPipe {
   static constexpr int BK = 64;
   // The grouped update holds two staging tiles instead of a second stage
   // (its K of 128 is two blocks, loaded and multiplied one after the other).
-  static constexpr int STAGES = EPI == EPI_GUPDATE ? 1 : 2;
+  // (STORE with the converter's FP32 ring keeps two: TcStages.)
+  static constexpr int STAGES = EPI == EPI_GUPDATE ? 1 : EPI == EPI_STORE ? 3 : 2;
+  // TMEM accumulators of BN columns (STORE: four, so that P0 can drain its
+  // accumulation units in pairs while the MMAs fill the other two).
+  static constexpr int NBUF = EPI == EPI_STORE ? 4 : 2;
+};
+template <int EPI, bool CONVB>
+struct TcStages {
+  static constexpr int VALUE = CONVB ? 2 : TcPipe<EPI>::STAGES;
 };
 
 // STORE (the FP64-output GEMMs: P0, the sweep update, the BSE direct term):
@@ -306,7 +314,7 @@ struct TcSmem {
   // warps; it runs F32_STAGES k-blocks ahead of the converters.
   static constexpr int F32_STAGES = 3;
   static constexpr int F32_BYTES = CONVB ? BN * TcPipe<EPI>::BK * 4 : 0;
-  static constexpr int F32_OFF = TcPipe<EPI>::STAGES * STAGE_BYTES;
+  static constexpr int F32_OFF = TcStages<EPI, CONVB>::VALUE * STAGE_BYTES;
   static constexpr int BAR_OFF = F32_OFF + (CONVB ? F32_STAGES * F32_BYTES : 0);
   static constexpr int RED_OFF = BAR_OFF + 256;  // ROWDOT: partial row sums [2][128] doubles + 2 flags
   // ROWDOT: two buffers of [2][128] doubles + 2 flags (8 doubles), alternating per item.
@@ -360,6 +368,7 @@ struct TcArgs {
   int gcount;
   int items;  // tiles of the grouped table (the item count with gmats)
   int unit;  // STORE: k-blocks per FP32 accumulation unit (0 counts as 1)
+  int pair_units;  // STORE: drain the accumulation units two at a time (P0)
   // CONVB: B[w][n][k] = convB[n][k] * convC[w][k] (FP32, zero past K): the
   // FP32 tile of convB arrives by TMA (map in the mapBh slot), and the
   // converter warps scale and split it into the hi/lo tile the MMA reads.
@@ -427,14 +436,15 @@ __global__ void __launch_bounds__(TcThreads<EPI, CONVB>::VALUE, 1)
   static_assert(!CONVB || (EPI == EPI_STORE && BN == 128), "the converted B operand serves P0's STORE tiles");
   using L = TcSmem<BN, EPI, CONVB>;
   constexpr int TC_BK = TcPipe<EPI>::BK;
-  constexpr int TC_STAGES = TcPipe<EPI>::STAGES;
+  constexpr int TC_STAGES = TcStages<EPI, CONVB>::VALUE;
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + L::BAR_OFF);
   uint64_t* empty = full + TC_STAGES;
-  uint64_t* acc_full = empty + TC_STAGES;   // [2]
-  uint64_t* acc_empty = acc_full + 2;       // [2]
-  uint64_t* drain = acc_empty + 2;          // all issued MMAs complete
+  constexpr int NBUF = TcPipe<EPI>::NBUF;
+  uint64_t* acc_full = empty + TC_STAGES;   // [NBUF]
+  uint64_t* acc_empty = acc_full + NBUF;    // [NBUF]
+  uint64_t* drain = acc_empty + NBUF;       // all issued MMAs complete
   uint64_t* conv = drain + 1;               // CONVB: [TC_STAGES] converted B tile ready
   uint64_t* f32_full = conv + TC_STAGES;    // CONVB: [F32_STAGES] FP32 tile landed
   uint64_t* f32_empty = f32_full + L::F32_STAGES;  // CONVB: [F32_STAGES] FP32 slot read by every converter warp
@@ -545,7 +555,7 @@ __global__ void __launch_bounds__(TcThreads<EPI, CONVB>::VALUE, 1)
       mbar_init(&f32_full[s], 1);
       mbar_init(&f32_empty[s], kConvWarps);
     }
-    for (int b = 0; b < 2; ++b) {
+    for (int b = 0; b < NBUF; ++b) {
       mbar_init(&acc_full[b], 1);
       // One arrival per epilogue warp (GUPDATE: per warp of the group that
       // owns the buffer).
@@ -557,7 +567,7 @@ __global__ void __launch_bounds__(TcThreads<EPI, CONVB>::VALUE, 1)
   }
   if (warp == 1) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(tmem_slot)),
-                 "r"(2 * BN));
+                 "r"(NBUF * BN));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
   }
   tc_fence_before();
@@ -654,9 +664,9 @@ __global__ void __launch_bounds__(TcThreads<EPI, CONVB>::VALUE, 1)
             const int unit = args.unit > 0 ? args.unit : 1;
             const bool unit_start = (EPI != EPI_ROWDOT) ? (kb % unit == 0) : kb == 0;
             const bool unit_end = (EPI != EPI_ROWDOT) ? (kb % unit == unit - 1 || kb == kbe - 1) : kb == kbe - 1;
-            const int buf = u & 1;
-            if (unit_start && u >= 2) {
-              if (!mbar_wait(&acc_empty[buf], ((u / 2) - 1) & 1, abort_flag, args.err, 2)) {
+            const int buf = u % NBUF;
+            if (unit_start && u >= NBUF) {
+              if (!mbar_wait(&acc_empty[buf], ((u / NBUF) - 1) & 1, abort_flag, args.err, 2)) {
                 ok = false;
                 break;
               }
@@ -838,8 +848,8 @@ __global__ void __launch_bounds__(TcThreads<EPI, CONVB>::VALUE, 1)
         double rowsum = 0.0;
         int tiles_done = 0;
         for (int nt = 0; nt < n_tiles; ++nt, ++t) {
-          const int buf = t & 1;
-          if (!mbar_wait(&acc_full[buf], (t / 2) & 1, abort_flag, args.err, 4)) {
+          const int buf = t % NBUF;
+          if (!mbar_wait(&acc_full[buf], (t / NBUF) & 1, abort_flag, args.err, 4)) {
             ok = false;
             break;
           }
@@ -1027,14 +1037,24 @@ __global__ void __launch_bounds__(TcThreads<EPI, CONVB>::VALUE, 1)
         double acc[CPW];
 #pragma unroll
         for (int c = 0; c < CPW; ++c) acc[c] = 0.0;
-        for (int uu = 0; uu < n_units; ++uu, ++u) {
-          const int buf = u & 1;
-          if (!ok || !mbar_wait(&acc_full[buf], (u / 2) & 1, abort_flag, args.err, 4)) {
+        for (int uu = 0; uu < n_units;) {
+          // P0 (pair_units) drains two accumulation units at once: their FP32
+          // partials are added in FP32 (one rounding to nearest) before the
+          // conversion to FP64, so the drain converts half as many values.
+          const int nu = (EPI == EPI_STORE && args.pair_units && uu + 1 < n_units) ? 2 : 1;
+          const int buf = u % NBUF, buf2 = (u + 1) % NBUF;
+          const bool got = ok && mbar_wait(&acc_full[buf], (u / NBUF) & 1, abort_flag, args.err, 4) &&
+                           (nu == 1 || mbar_wait(&acc_full[buf2], ((u + 1) / NBUF) & 1, abort_flag, args.err, 4));
+          if (!got) {
             ok = false;
+            uu += nu;
+            u += nu;
             continue;
           }
           tc_fence_after();
-          const uint32_t taddr = tmem_base + ((uint32_t)(quarter * 32) << 16) + buf * BN + CPW * part;
+          const uint32_t lrow = (uint32_t)(quarter * 32) << 16;
+          const uint32_t taddr = tmem_base + lrow + buf * BN + CPW * part;
+          const uint32_t taddr2 = tmem_base + lrow + buf2 * BN + CPW * part;
 #pragma unroll
           for (int j = 0; j < CPW / 16; ++j) {
             // Columns past N (a narrow GEMM, e.g. a few vectors) are not
@@ -1049,13 +1069,24 @@ __global__ void __launch_bounds__(TcThreads<EPI, CONVB>::VALUE, 1)
 #pragma unroll
               for (int q = 0; q < 16; ++q) cr[q] = uu == 0 ? v[q] : cr[q] + v[q];
             } else {
+              if (nu == 2) {
+                float v2[16];
+                tmem_ld16(taddr2 + 16 * j, v2);
+#pragma unroll
+                for (int q = 0; q < 16; ++q) v[q] += v2[q];
+              }
 #pragma unroll
               for (int q = 0; q < 16; ++q) acc[16 * j + q] += (double)v[q];
             }
           }
           tc_fence_before();
           __syncwarp();
-          if (lane == 0) mbar_arrive(&acc_empty[buf]);
+          if (lane == 0) {
+            mbar_arrive(&acc_empty[buf]);
+            if (nu == 2) mbar_arrive(&acc_empty[buf2]);
+          }
+          uu += nu;
+          u += nu;
         }
         if (EPI == EPI_UPDATE) {
           // The tile C (exactly FP32: one accumulation unit covers K, the
@@ -1164,7 +1195,7 @@ __global__ void __launch_bounds__(TcThreads<EPI, CONVB>::VALUE, 1)
   __syncthreads();
   tc_fence_after();
   if (warp == 1) {
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem_base), "r"(2 * BN));
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem_base), "r"(NBUF * BN));
   }
 }
 
@@ -2348,6 +2379,7 @@ static void eps_tc_split(qx_ctx* ctx, const double* bov, int ldov, int naux, int
   a.lower_tiles = 1;
   a.add_identity = 1;
   a.unit = kP0Unit;
+  a.pair_units = 1;
   a.fp16 = fp16;
   a.scaleA = sa;
   a.scaleB = sb;
@@ -2414,6 +2446,7 @@ static void eps_tc_conv(qx_ctx* ctx, const double* bov, int ldov, int naux, int 
   a.lower_tiles = 1;
   a.add_identity = 1;
   a.unit = kP0Unit;
+  a.pair_units = 1;
   a.fp16 = fp16;
   a.scaleA = sa;
   a.scaleB = sb;
