@@ -201,7 +201,11 @@ def contraction_mma_flops(nmo, naux, nw):
 # DRAM bytes (read + write) of one pair-contraction launch at nmo 300 / naux 1000 /
 # nw 32, from one ncu capture of the bench's own command (dram__bytes_read.sum +
 # dram__bytes_write.sum of the launch the bench keeps).
-CONTRACTION_DRAM_BYTES = 1.563380e9 + 0.015538e9
+# DRAM bytes of one pair-contraction launch at nmo 300 / naux 1000 / nw 32 (ncu,
+# the frequency grouping the autotuner keeps): CTA-pair and single-CTA tiles.
+CONTRACTION_DRAM_BYTES = {"pair": 1.617387e9 + 0.015371e9, "single": 1.563380e9 + 0.015538e9}
+CONTRACTION_KERNEL = {"pair": "k_rowdot_pair (pair contraction on CTA pairs, cta_group::2)",
+                      "single": "k_tc_gemm<256,EPI_ROWDOT> (pair contraction, one CTA per pair block)"}
 
 
 def iteration_flops(nocc, nvir, naux, nw):
@@ -712,9 +716,12 @@ def main():
                 "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (FP64 has no entry in MEASURED_PEAKS.json)"}
     else:
         pk = peaks.get("bf16_tflops_sustained", peaks.get("bf16_tflops"))
+        cform = "single" if args.contraction_form == "single" else "pair"
+        burst = peaks.get("bf16_tflops")
         roof = {"bound": "tensor", "achieved": achieved, "peak": pk, "unit": "TFLOP/s", "frac": achieved / pk,
-                "traffic": CONTRACTION_DRAM_BYTES, "kernel": "k_tc_gemm<256,EPI_ROWDOT> (pair contraction)",
-                "peak_source": f"bf16_tflops_sustained, {peak_src}",
+                "traffic": CONTRACTION_DRAM_BYTES[cform], "kernel": CONTRACTION_KERNEL[cform],
+                "peak_source": f"bf16_tflops_sustained, {peak_src} (the kernel runs inside a seconds-long step)",
+                "frac_of_burst_peak": achieved / burst if burst else None,
                 "algorithmic_flops_per_launch": cflops,
                 "executed_mma_tflops": executed, "executed_mma_frac": executed / pk,
                 "note": "algorithmic = 2 naux^2 norbs nmo nw; executed = 3 split products over the "
