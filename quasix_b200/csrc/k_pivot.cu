@@ -328,93 +328,108 @@ __global__ void __launch_bounds__(512) k_piv_panel_reg(const GuardMat* __restric
       bi = r;
     }
   }
-  // One pivot step per iteration, not unrolled (sixteen unrolled copies of
-  // the step missed the instruction cache: "no instruction" was the top
-  // stall).  The registers rotate by one column per step instead, so the
-  // step's column is always v[.][0] and every register index stays a
-  // compile-time constant; after PIV_NB steps the columns are back in order
-  // (steps past kb only rotate).
+  // Four pivot steps per loop iteration, then the registers rotate by four
+  // columns, so that step s of an iteration works on column s and every
+  // register index stays a compile-time constant.  (Sixteen unrolled steps
+  // missed the instruction cache -- "no instruction" was the top stall --
+  // and one step per iteration spent 32 register moves per row and pivot on
+  // the rotation.)  Steps past kb only rotate.
+  constexpr int UNR = 4;
+  static_assert(PIV_NB % UNR == 0, "whole rotations");
 #pragma unroll 1
-  for (int j = 0; j < PIV_NB; ++j) {
-    if (j < kb) {  // uniform
-      const int sl = j & 1;
-      // Warp argmax, then the owner of the warp's best row publishes it.
-      double wv = best;
-      int wr = bi;
-      for (int o = 16; o > 0; o >>= 1) {
-        const double ov = __shfl_xor_sync(0xffffffffu, wv, o);
-        const int orr = __shfl_xor_sync(0xffffffffu, wr, o);
-        if (ov > wv || (ov == wv && orr < wr)) {
-          wv = ov;
-          wr = orr;
+  for (int j4 = 0; j4 < PIV_NB; j4 += UNR) {
+#pragma unroll
+    for (int s = 0; s < UNR; ++s) {
+      const int j = j4 + s;
+      if (j < kb) {  // uniform
+        const int sl = j & 1;
+        // Warp argmax, then the owner of the warp's best row publishes it.
+        double wv = best;
+        int wr = bi;
+        for (int o = 16; o > 0; o >>= 1) {
+          const double ov = __shfl_xor_sync(0xffffffffu, wv, o);
+          const int orr = __shfl_xor_sync(0xffffffffu, wr, o);
+          if (ov > wv || (ov == wv && orr < wr)) {
+            wv = ov;
+            wr = orr;
+          }
         }
-      }
-      if (lane == 0) {
-        slot_val[sl][warp] = wv;
-        slot_idx[sl][warp] = wr;
-      }
-#pragma unroll
-      for (int i = 0; i < RPT; ++i)
-        if (wr != INT_MAX && threadIdx.x + 512 * i == wr) {
-#pragma unroll
-          for (int c = 0; c < PIV_NB; ++c) slot_row[sl][warp][c] = v[i][c];
+        if (lane == 0) {
+          slot_val[sl][warp] = wv;
+          slot_idx[sl][warp] = wr;
         }
-      __syncthreads();
-      double gv = slot_val[sl][0];
-      int gr = slot_idx[sl][0], gw = 0;
 #pragma unroll
-      for (int k = 1; k < NWARP; ++k) {
-        const double ov = slot_val[sl][k];
-        const int orr = slot_idx[sl][k];
-        if (ov > gv || (ov == gv && orr < gr)) {
-          gv = ov;
-          gr = orr;
-          gw = k;
+        for (int i = 0; i < RPT; ++i)
+          if (wr != INT_MAX && threadIdx.x + 512 * i == wr) {
+#pragma unroll
+            for (int c = 0; c < PIV_NB; ++c) slot_row[sl][warp][c] = v[i][c];
+          }
+        __syncthreads();
+        // Block argmax over the warps' slots: lane k < NWARP holds slot k,
+        // a shuffle tree picks the largest value (ties to the lowest row),
+        // and lane 0's result goes to the whole warp.
+        double gv = lane < NWARP ? slot_val[sl][lane] : -2.0;
+        int gr = lane < NWARP ? slot_idx[sl][lane] : INT_MAX;
+        int gw = lane;
+        for (int o = NWARP / 2; o > 0; o >>= 1) {
+          const double ov = __shfl_xor_sync(0xffffffffu, gv, o);
+          const int orr = __shfl_xor_sync(0xffffffffu, gr, o);
+          const int ow = __shfl_xor_sync(0xffffffffu, gw, o);
+          if (ov > gv || (ov == gv && orr < gr)) {
+            gv = ov;
+            gr = orr;
+            gw = ow;
+          }
         }
-      }
-      const int p = gr;
-      const double d = (p == INT_MAX) ? 0.0 : slot_row[sl][gw][0];
-      if (!(fabs(d) > 0.0) || !isfinite(d)) {  // uniform
-        if (threadIdx.x == 0) *g.status = 1;
-        return;
-      }
-      if (threadIdx.x == 0) {
-        piv[k0 + j] = p;
-        pivs[j] = p;
-      }
-      const double inv = 1.0 / d;
-      double pr[PIV_NB];
-#pragma unroll
-      for (int c = 0; c < PIV_NB; ++c) pr[c] = slot_row[sl][gw][c];
-      best = -1.0;
-      bi = INT_MAX;
-#pragma unroll
-      for (int i = 0; i < RPT; ++i) {
-        const int r = threadIdx.x + 512 * i;
-        if (r == p) {
-#pragma unroll
-          for (int c = 0; c < PIV_NB; ++c) v[i][c] = (c == 0) ? inv : -pr[c] * inv;
-          freer[i] = false;
-          mine[i] = true;
-        } else {
-          const double t = v[i][0] * inv;
-#pragma unroll
-          for (int c = 0; c < PIV_NB; ++c) v[i][c] = (c == 0) ? t : v[i][c] - t * pr[c];
+        gr = __shfl_sync(0xffffffffu, gr, 0);
+        gw = __shfl_sync(0xffffffffu, gw, 0);
+        const int p = gr;
+        const double d = (p == INT_MAX) ? 0.0 : slot_row[sl][gw][s];
+        if (!(fabs(d) > 0.0) || !isfinite(d)) {  // uniform
+          if (threadIdx.x == 0) *g.status = 1;
+          return;
         }
-        // The next step's column is v[.][1] (before the rotation below).
-        const double a = fabs(v[i][1]);
-        if (freer[i] && (a > best || (a == best && r < bi))) {
-          best = a;
-          bi = r;
+        if (threadIdx.x == 0) {
+          piv[k0 + j] = p;
+          pivs[j] = p;
+        }
+        const double inv = 1.0 / d;
+        double pr[PIV_NB];
+#pragma unroll
+        for (int c = 0; c < PIV_NB; ++c) pr[c] = slot_row[sl][gw][c];
+        best = -1.0;
+        bi = INT_MAX;
+#pragma unroll
+        for (int i = 0; i < RPT; ++i) {
+          const int r = threadIdx.x + 512 * i;
+          if (r == p) {
+#pragma unroll
+            for (int c = 0; c < PIV_NB; ++c) v[i][c] = (c == s) ? inv : -pr[c] * inv;
+            freer[i] = false;
+            mine[i] = true;
+          } else {
+            const double t = v[i][s] * inv;
+#pragma unroll
+            for (int c = 0; c < PIV_NB; ++c) v[i][c] = (c == s) ? t : v[i][c] - t * pr[c];
+          }
+          // The next step's column is v[.][s + 1] (before the rotation below).
+          const double a = fabs(v[i][s + 1]);
+          if (freer[i] && (a > best || (a == best && r < bi))) {
+            best = a;
+            bi = r;
+          }
         }
       }
     }
 #pragma unroll
     for (int i = 0; i < RPT; ++i) {
-      const double t0 = v[i][0];
+      double t0[UNR];
 #pragma unroll
-      for (int c = 0; c + 1 < PIV_NB; ++c) v[i][c] = v[i][c + 1];
-      v[i][PIV_NB - 1] = t0;
+      for (int c = 0; c < UNR; ++c) t0[c] = v[i][c];
+#pragma unroll
+      for (int c = 0; c + UNR < PIV_NB; ++c) v[i][c] = v[i][c + UNR];
+#pragma unroll
+      for (int c = 0; c < UNR; ++c) v[i][PIV_NB - UNR + c] = t0[c];
     }
   }
   // Write the panel back, then the old pivot rows of the super-panel's other
