@@ -126,42 +126,52 @@ constexpr int SWEEP_NB = 128;
 // swept after each pivot step (the element growth of the elimination).
 template <bool GUARD>
 __device__ __forceinline__ void sweep32_warp(double* S, int q0, int lane, bool& bad_any, double tol, double& gm) {
-  // c[k] holds S[(p + k) % 32][lane] at pivot step p: the pivot row is always
-  // c[0] and the array rotates by one after each step, so every register index
-  // is a compile-time constant without unrolling the pivot loop (an unrolled
-  // loop of 32 steps measured slower: it misses the instruction cache).  The
-  // lanes other than p take c[i] - S[p+i][p] S[p][lane] / d and lane p takes
-  // S[p+i][p] / d, both as one FMA: fma(ci, b, c[i] * a) with (a, b) = (1, -rj)
-  // or (0, inv).
+  // Four pivot steps per loop iteration: at the start of group p4, c[k]
+  // holds S[(p4 + k) % 32][lane], so step s's pivot row is c[s] and every
+  // register index is a compile-time constant; the array then rotates by four
+  // (an unrolled loop of 32 steps measured slower, it misses the instruction
+  // cache; one step per iteration spent 64 register moves per pivot on the
+  // rotation).  The lanes other than p take c[k] - S[r][p] S[p][lane] / d and
+  // lane p takes S[r][p] / d, both as one FMA: fma(ck, b, c[k] * a) with
+  // (a, b) = (1, -rj) or (0, inv).
   double c[32];
 #pragma unroll
   for (int i = 0; i < 32; ++i) c[i] = S[(q0 + i) * SWEEP_NB + q0 + lane];
+  constexpr int UNR = 4;
 #pragma unroll 1
-  for (int p = 0; p < 32; ++p) {
-    const double d = __shfl_sync(0xffffffffu, c[0], p);
-    const bool bad = !(fabs(d) > tol) || !isfinite(d);
-    bad_any |= bad;
-    const double inv = bad ? 0.0 : 1.0 / d;
-    const double rj = c[0] * inv;  // S[p][lane] / d
-    const bool piv = (lane == p);
-    const double a = piv ? 0.0 : 1.0, b = piv ? inv : -rj;
+  for (int p4 = 0; p4 < 32; p4 += UNR) {
 #pragma unroll
-    for (int i = 1; i < 32; ++i) {
-      const double ci = __shfl_sync(0xffffffffu, c[i], p);  // S[p + i][p]
-      c[i] = fma(ci, b, c[i] * a);
+    for (int s = 0; s < UNR; ++s) {
+      const int p = p4 + s;
+      const double d = __shfl_sync(0xffffffffu, c[s], p);
+      const bool bad = !(fabs(d) > tol) || !isfinite(d);
+      bad_any |= bad;
+      const double inv = bad ? 0.0 : 1.0 / d;
+      const double rj = c[s] * inv;  // S[p][lane] / d
+      const bool piv = (lane == p);
+      const double a = piv ? 0.0 : 1.0, b = piv ? inv : -rj;
+#pragma unroll
+      for (int k = 0; k < 32; ++k) {
+        if (k == s) continue;
+        const double ck = __shfl_sync(0xffffffffu, c[k], p);  // S[row k][p]
+        c[k] = fma(ck, b, c[k] * a);
+      }
+      c[s] = piv ? -inv : rj;
+      // Growth of the columns not yet swept, sampled every eighth pivot (the
+      // serial pivot chain is this kernel's bound; the probe backward error of
+      // the guard catches any loss between samples).
+      if (GUARD && (p & 7) == 7 && lane > p) {
+#pragma unroll
+        for (int i = 0; i < 32; ++i) gm = fmax(gm, isfinite(c[i]) ? fabs(c[i]) : INFINITY);
+      }
     }
-    c[0] = piv ? -inv : rj;
-    // Growth of the columns not yet swept, sampled every eighth pivot (the
-    // serial pivot chain is this kernel's bound; the probe backward error of
-    // the guard catches any loss between samples).
-    if (GUARD && (p & 7) == 7 && lane > p) {
+    double t[UNR];
 #pragma unroll
-      for (int i = 0; i < 32; ++i) gm = fmax(gm, isfinite(c[i]) ? fabs(c[i]) : INFINITY);
-    }
-    const double t = c[0];
+    for (int i = 0; i < UNR; ++i) t[i] = c[i];
 #pragma unroll
-    for (int i = 0; i < 31; ++i) c[i] = c[i + 1];
-    c[31] = t;
+    for (int i = 0; i + UNR < 32; ++i) c[i] = c[i + UNR];
+#pragma unroll
+    for (int i = 0; i < UNR; ++i) c[32 - UNR + i] = t[i];
   }
 #pragma unroll
   for (int i = 0; i < 32; ++i) S[(q0 + i) * SWEEP_NB + q0 + lane] = c[i];
