@@ -516,20 +516,26 @@ __global__ void __launch_bounds__(256) k_sweep_write(double* __restrict__ M, int
 // half_lower the output is W' = strict lower triangle of Wc + diag(Wc) / 2 and
 // zeros above, so that b^T Wc b = 2 b^T W' b needs only the lower triangle.
 // Row r of the finish (one block per row).
-__device__ __forceinline__ void finish_wc_row(double* __restrict__ A, int n, int ldn, bool singular, int half_lower,
-                                              int r) {
+// Rows [8 b, 8 b + 8) of the finish, one warp per row with the lanes along it
+// (a block per row left each block ~1 KB of work and the launch bound by
+// block scheduling).
+constexpr int kFinishRows = 8;
+__device__ __forceinline__ void finish_wc_rows(double* __restrict__ A, int n, int ldn, bool singular, int half_lower,
+                                               int b) {
+  const int r = kFinishRows * b + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+  if (r >= n) return;
   double* row = A + (size_t)r * ldn;
-  for (int c = threadIdx.x; c < n; c += blockDim.x) {
+  for (int c = lane; c < n; c += 32) {
     double v = singular ? 0.0 : -row[c] - (r == c ? 1.0 : 0.0);
     if (half_lower) v = (c < r) ? v : (c == r ? 0.5 * v : 0.0);
     row[c] = v;
   }
 }
 
-__global__ void k_finish_wc(double* __restrict__ M, int n, int ldn, size_t stride, const int* __restrict__ status,
-                            int half_lower) {
+__global__ void __launch_bounds__(32 * kFinishRows) k_finish_wc(double* __restrict__ M, int n, int ldn, size_t stride,
+                                                               const int* __restrict__ status, int half_lower) {
   const int w = blockIdx.y;
-  finish_wc_row(M + (size_t)w * stride, n, ldn, status[w] != 0, half_lower, blockIdx.x);
+  finish_wc_rows(M + (size_t)w * stride, n, ldn, status[w] != 0, half_lower, blockIdx.x);
 }
 
 static_assert(kSweepPanelCols == SWEEP_NB, "panel width");
@@ -712,7 +718,7 @@ void launch_invert_wc(qx_ctx* ctx, double* eps, int n, int ldn, size_t stride, i
   }
   // Guarded: the flagged matrices are inverted again with pivoting.
   if (guard) guard_end(ctx, gs);
-  dim3 fg(n, nw);
+  dim3 fg(ceil_div(n, kFinishRows), nw);
   k_finish_wc<<<fg, 256, 0, ctx->stream>>>(eps, n, ldn, stride, status, half_lower);
   check_launch(ctx);
   ctx->pending.push_back({status, nw, 1});
@@ -735,7 +741,7 @@ void launch_invert_wc_panels(qx_ctx* ctx, double* eps, int n, int ldn, size_t st
     sweep_update(ctx, ctx->stream, eps, n, ldn, stride, nw, k0, kb, Tp, Pp, pstride, 0, 0, 0);
   }
   if (guard_mem) guard_end(ctx, gs);
-  dim3 fg(n, nw);
+  dim3 fg(ceil_div(n, kFinishRows), nw);
   k_finish_wc<<<fg, 256, 0, ctx->stream>>>(eps, n, ldn, stride, status, 0);
   check_launch(ctx);
 }
@@ -807,11 +813,12 @@ __global__ void __launch_bounds__(SweepTile::THREADS) k_gsweep_update(const GMat
                     Pcat + (size_t)m.prow * SWEEP_NB, tm, tn, 0, 0, 0);
 }
 
-__global__ void k_gfinish_wc(const GMat* __restrict__ mats, const int* __restrict__ pre, int count,
-                             const int* __restrict__ status, int half_lower) {
+__global__ void __launch_bounds__(32 * kFinishRows) k_gfinish_wc(const GMat* __restrict__ mats,
+                                                                 const int* __restrict__ pre, int count,
+                                                                 const int* __restrict__ status, int half_lower) {
   const int g = group_of(pre, count, blockIdx.x);
   const GMat m = mats[g];
-  finish_wc_row(m.M, m.n, m.ldn, status[g] != 0, half_lower, blockIdx.x - pre[g]);
+  finish_wc_rows(m.M, m.n, m.ldn, status[g] != 0, half_lower, blockIdx.x - pre[g]);
 }
 
 // Zero the padding rows [n, n rounded up to 128) of each matrix's panels
@@ -882,7 +889,7 @@ void launch_invert_wc_group(qx_ctx* ctx, const GMat* mats_in, int G, int half_lo
         return t * (t + 1) / 2;
       });
   }
-  const size_t off_fin = add_table(G, [](const GMat& x) { return (long long)x.n; });
+  const size_t off_fin = add_table(G, [](const GMat& x) { return (long long)ceil_div(x.n, kFinishRows); });
   // Workspace: T, P [R][128] FP64, D [G][128][128], the matrix and prefix tables.
   const size_t pan = (size_t)R * SWEEP_NB;
   const size_t dsz = (size_t)G * SWEEP_NB * SWEEP_NB;
