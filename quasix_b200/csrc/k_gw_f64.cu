@@ -1018,23 +1018,25 @@ void launch_gather_pairs(qx_ctx* ctx, const double* lpq, int naux, int nmo, cons
 }
 
 // bov[P][i*nvir + a] = lpq[P][i][nocc + a]
+// bov[P][i nvir + a] = lpq[P][i][nocc + a], zero in the padding columns
+// [nocc nvir, ldov): block (i, P) copies one contiguous run of nvir values
+// (block i = nocc writes the padding), so no index is divided.
 __global__ void k_gather_ov(const double* __restrict__ lpq, int naux, int nmo, int nocc, double* __restrict__ bov,
                             int ldov) {
-  const int P = blockIdx.y;
+  const int i = blockIdx.x, P = blockIdx.y;
   const int nvir = nmo - nocc;
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < ldov; k += gridDim.x * blockDim.x) {
-    double v = 0.0;
-    if (k < nocc * nvir) {
-      int i = k / nvir, a = k % nvir;
-      v = lpq[(size_t)P * nmo * nmo + (size_t)i * nmo + nocc + a];
-    }
-    bov[(size_t)P * ldov + k] = v;
+  double* dst = bov + (size_t)P * ldov;
+  if (i == nocc) {
+    for (int k = nocc * nvir + threadIdx.x; k < ldov; k += blockDim.x) dst[k] = 0.0;
+    return;
   }
+  const double* src = lpq + (size_t)P * nmo * nmo + (size_t)i * nmo + nocc;
+  for (int a = threadIdx.x; a < nvir; a += blockDim.x) dst[(size_t)i * nvir + a] = src[a];
 }
 
 void launch_gather_ov(qx_ctx* ctx, const double* lpq, int naux, int nmo, int nocc, double* bov, int ldov) {
-  dim3 grid(ceil_div(ldov, 256), naux);
-  k_gather_ov<<<grid, 256, 0, ctx->stream>>>(lpq, naux, nmo, nocc, bov, ldov);
+  dim3 grid(nocc + 1, naux);
+  k_gather_ov<<<grid, 128, 0, ctx->stream>>>(lpq, naux, nmo, nocc, bov, ldov);
   check_launch(ctx);
 }
 
