@@ -245,12 +245,12 @@ __device__ __forceinline__ bool mbar_wait_cluster(uint64_t* bar, uint32_t parity
 enum { EPI_ROWDOT = 0, EPI_STORE = 1, EPI_UPDATE = 2, EPI_GUPDATE = 3 };
 
 constexpr int TC_BM = 128;
-// Pipeline shape per epilogue: 64-wide K blocks in 2 stages.  32-wide blocks
-// in 4 stages (the same shared memory, more TMA requests in flight) measured
-// slower for the pair contraction (7.8 vs 6.1 ms at nmo 300 / naux 1000 /
-// nw 32); for P0, 3 stages of 64 gave 1.87 vs 1.91 ms and 6 stages of 32 were
-// slower: its limit is the operand traffic from shared memory of the
-// 128-wide tile, not the pipeline depth.
+// Pipeline shape per epilogue: 64-wide K blocks, in 2 stages except where
+// noted below.  32-wide blocks in 4 stages (the same shared memory, more TMA
+// requests in flight) measured slower for the pair contraction (7.8 vs 6.1 ms
+// at nmo 300 / naux 1000 / nw 32).  STORE runs 3 stages: with P0's drain made
+// cheaper (units drained in pairs), the MMA thread's waits for the loads
+// showed, and the third stage took P0 from 1.73 to 1.70 ms per iteration.
 template <int EPI>
 struct TcPipe {
   static constexpr int BK = 64;
@@ -278,8 +278,10 @@ struct TcStages {
 // unit 2 (1.86 vs 1.89 ms) and doubled the error, so P0 uses unit 2; the
 // sweep's update uses unit 2 too (one unit covers its K of 128); the BSE
 // direct term keeps unit 1, since with unit 2 the Davidson residuals of the
-// 26 400-dimensional problem stalled above 1e-8.  A third stage measured no
-// faster.
+// 26 400-dimensional problem stalled above 1e-8.  P0 (TcArgs::pair_units)
+// then drains its units two at a time, adding their FP32 partials in FP32
+// before the one conversion (1.73 -> 1.62 ms; the BSE term's Davidson took 177
+// instead of 167 iterations with the same pairing, so it drains one unit).
 // Largest chi-scaled P0 operand (hi + lo of B_ov chi'_w s_w for every
 // frequency) that is materialised; larger problems use the converter form.
 constexpr size_t kP0SplitBudget = (size_t)6 << 30;
