@@ -1040,6 +1040,85 @@ void launch_gather_ov(qx_ctx* ctx, const double* lpq, int naux, int nmo, int noc
   check_launch(ctx);
 }
 
+// bov[P][i nvir + a] = bpt[pair(i, nocc + a)][P], zero in the padding columns
+// [nocc nvir, ldov), when every orbital is a target (row i of the pair index
+// table pidx lists the pairs of orbital i).  The occupied-virtual block is
+// then transposed out of the gathered pair tensor instead of being read from
+// lpq a second time (lpq may be host memory read in place).  Tiled transpose
+// through shared memory: 32 columns x 32 aux rows per block.
+__global__ void k_ov_from_pairs(const double* __restrict__ bpt, int ldk, const int* __restrict__ pidx, int naux,
+                                int nmo, int nocc, double* __restrict__ bov, int ldov) {
+  __shared__ double tile[32][33];
+  __shared__ int row[32];
+  const int c0 = blockIdx.x * 32, P0 = blockIdx.y * 32;
+  const int nvir = nmo - nocc, nov = nocc * nvir;
+  if (threadIdx.y == 0) {
+    const int c = c0 + threadIdx.x;
+    int r = -1;
+    if (c < nov) {
+      const int i = c / nvir;
+      r = pidx[(size_t)i * nmo + nocc + (c - i * nvir)];
+    }
+    row[threadIdx.x] = r;
+  }
+  __syncthreads();
+  for (int cc = threadIdx.y; cc < 32; cc += blockDim.y) {
+    const int r = row[cc], P = P0 + threadIdx.x;
+    tile[cc][threadIdx.x] = (r >= 0 && P < naux) ? bpt[(size_t)r * ldk + P] : 0.0;
+  }
+  __syncthreads();
+  for (int pp = threadIdx.y; pp < 32; pp += blockDim.y) {
+    const int P = P0 + pp, c = c0 + threadIdx.x;
+    if (P < naux && c < ldov) bov[(size_t)P * ldov + c] = tile[threadIdx.x][pp];
+  }
+}
+
+void launch_ov_from_pairs(qx_ctx* ctx, const double* bpt, int ldk, const int* pidx, int naux, int nmo, int nocc,
+                          double* bov, int ldov) {
+  dim3 grid(ceil_div(ldov, 32), ceil_div(naux, 32));
+  k_ov_from_pairs<<<grid, dim3(32, 8), 0, ctx->stream>>>(bpt, ldk, pidx, naux, nmo, nocc, bov, ldov);
+  check_launch(ctx);
+}
+
+// sx[t] = -sum_{i < nocc} sum_R bpt[pair(t, i)][R]^2 for the targets t (row
+// t of pidx): the exchange diagonal of qp/evgw.rs:1167-1193 read from the
+// gathered pair tensor, whose rows are contiguous in R, instead of from
+// lpq's scattered lpq[R][t][i].  One block per target, a fixed summation
+// order (per thread over i and R, then a tree over the block).
+__global__ void __launch_bounds__(256) k_exchange_pairs(const double* __restrict__ bpt, int ldk,
+                                                        const int* __restrict__ pidx, int naux, int nmo, int nocc,
+                                                        double* __restrict__ sx) {
+  const int t = blockIdx.x;
+  double s0 = 0.0, s1 = 0.0;
+  for (int i = 0; i < nocc; ++i) {
+    const double* row = bpt + (size_t)__ldg(pidx + (size_t)t * nmo + i) * ldk;
+    int R = threadIdx.x;
+    for (; R + 256 < naux; R += 512) {
+      const double u = __ldg(row + R), v = __ldg(row + R + 256);
+      s0 += u * u;
+      s1 += v * v;
+    }
+    if (R < naux) {
+      const double u = __ldg(row + R);
+      s0 += u * u;
+    }
+  }
+  __shared__ double red[256];
+  red[threadIdx.x] = s0 + s1;
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) sx[t] = -red[0];
+}
+
+void launch_exchange_pairs(qx_ctx* ctx, const double* bpt, int ldk, const int* pidx, int naux, int nmo, int nocc,
+                           int norbs, double* sx) {
+  k_exchange_pairs<<<norbs, 256, 0, ctx->stream>>>(bpt, ldk, pidx, naux, nmo, nocc, sx);
+  check_launch(ctx);
+}
+
 // sx[p] = -sum_{R,i} lpq[R][p][i]^2   (qp/evgw.rs:1167-1193).  One block of
 // 1024 threads per orbital; each thread keeps four loads in flight (the
 // elements are scattered over naux rows, so latency, not bandwidth, bounds a

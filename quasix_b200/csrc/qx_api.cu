@@ -29,6 +29,19 @@ const void* device_view(qx_ctx* ctx, int slot, const void* p, size_t bytes) {
   return b.ptr;
 }
 
+const void* mapped_view(qx_ctx* ctx, int slot, const void* p, size_t bytes) {
+  if (p != nullptr) {
+    cudaPointerAttributes at;
+    if (cudaPointerGetAttributes(&at, p) == cudaSuccess) {
+      if (at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged) return p;
+      if (at.type == cudaMemoryTypeHost && at.devicePointer != nullptr) return at.devicePointer;
+    } else {
+      cudaGetLastError();
+    }
+  }
+  return device_view(ctx, slot, p, bytes);
+}
+
 // Gauss-Legendre rule by Newton iteration on P_n (the nodes and weights of the
 // Golub-Welsch eigen-solve, correlation_ac.rs:122-160, to rounding).
 void scaled_legendre_roots(int nw, double x0, double* freqs, double* wts) {
@@ -144,7 +157,6 @@ void gw_setup(qx_ctx* ctx, GWSystem& S, const double* d_lpq, int nmo, int nocc, 
   S.ldn = round_up(naux, 8);
   S.nw = nw;
   S.precision = precision;
-  S.lpq = d_lpq;
   S.orbs = orbs;
   S.norbs = (int)orbs.size();
   S.grid = sigma_grid(nw, cutoff, x0);
@@ -186,7 +198,14 @@ void gw_setup(qx_ctx* ctx, GWSystem& S, const double* d_lpq, int nmo, int nocc, 
                           ctx->stream));
   QX_CUDA(cudaMemcpyAsync(S.d_orbs, orbs.data(), orbs.size() * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
   launch_gather_pairs(ctx, d_lpq, naux, nmo, d_pairs, S.npair, S.bpt, S.ldk);
-  launch_gather_ov(ctx, d_lpq, naux, nmo, nocc, S.bov, S.ldov);
+  // With every orbital a target the pair tensor holds the occupied-virtual
+  // block: B_ov comes from it, and the setup reads only lpq's upper triangle.
+  bool all_orbitals = S.norbs == nmo;
+  for (int t = 0; all_orbitals && t < S.norbs; ++t) all_orbitals = orbs[t] == t;
+  if (all_orbitals)
+    launch_ov_from_pairs(ctx, S.bpt, S.ldk, S.d_pidx, naux, nmo, nocc, S.bov, S.ldov);
+  else
+    launch_gather_ov(ctx, d_lpq, naux, nmo, nocc, S.bov, S.ldov);
   if (is_tc_precision(precision)) {
     QX_REQUIRE(tc_supported(ctx), QX_ERR_NO_DEVICE, "tensor-core precision needs an sm_100 device");
     const int fp16 = precision == QX_PREC_FP16X3;
@@ -676,7 +695,9 @@ qx_status qx_get_sigma_diag(qx_ctx* ctx, const double* mo_energy, const double* 
     for (int v : o) QX_REQUIRE(v >= 0 && v < nmo, QX_ERR_INVALID_INPUT, "orbital index %d out of range", v);
     std::vector<double> e(nmo);
     QX_CUDA(cudaMemcpy(e.data(), mo_energy, nmo * sizeof(double), cudaMemcpyDefault));
-    const double* d_lpq = (const double*)device_view(ctx, WS_LPQ, lpq, (size_t)naux * nmo * nmo * sizeof(double));
+    // Page-locked host lpq is read in place by the setup gathers (only the
+    // pairs they need cross the host link).
+    const double* d_lpq = (const double*)mapped_view(ctx, WS_LPQ, lpq, (size_t)naux * nmo * nmo * sizeof(double));
     GWSystem S;
     gw_setup(ctx, S, d_lpq, nmo, nocc, naux, o, nw, iw_cutoff, x0, precision);
     QX_REQUIRE(nw_sigma_max >= S.nws, QX_ERR_INVALID_INPUT, "nw_sigma_max %d < %d", nw_sigma_max, S.nws);
@@ -724,7 +745,10 @@ qx_status qx_evgw(qx_ctx* ctx, const double* mo_energy, const double* lpq, const
     std::vector<double> e0(nmo), vx(nmo);
     QX_CUDA(cudaMemcpy(e0.data(), mo_energy, nmo * sizeof(double), cudaMemcpyDefault));
     QX_CUDA(cudaMemcpy(vx.data(), vxc, nmo * sizeof(double), cudaMemcpyDefault));
-    const double* d_lpq = (const double*)device_view(ctx, WS_LPQ, lpq, (size_t)naux * nmo * nmo * sizeof(double));
+    // Page-locked host lpq is read in place: the setup gathers its upper
+    // triangle (the pairs p <= q) straight into the pair tensor, and nothing
+    // reads it afterwards, so half of it crosses the host link.
+    const double* d_lpq = (const double*)mapped_view(ctx, WS_LPQ, lpq, (size_t)naux * nmo * nmo * sizeof(double));
     std::vector<int> orbs(nmo);
     for (int i = 0; i < nmo; ++i) orbs[i] = i;
     GWSystem S;
@@ -747,7 +771,7 @@ qx_status qx_evgw(qx_ctx* ctx, const double* mo_energy, const double* lpq, const
     QX_CUDA(cudaMemcpyAsync(d_mo, e0.data(), nmo * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
     QX_CUDA(cudaMemcpyAsync(d_vx, vx.data(), nmo * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
     QX_CUDA(cudaMemcpyAsync(d_fit, fit.data(), nfit * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
-    launch_exchange_diag(ctx, d_lpq, naux, nmo, nocc, d_sx);
+    launch_exchange_pairs(ctx, S.bpt, S.ldk, S.d_pidx, naux, nmo, nocc, nmo, d_sx);
     std::vector<double> sx(nmo);
     QX_CUDA(cudaMemcpyAsync(sx.data(), d_sx, nmo * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
 

@@ -18,7 +18,6 @@ struct PairSet {
 struct GWSystem {
   int nmo, nocc, nvir, naux, nov, ldk, ldov, ldn, npair, nw, nws, norbs;
   int precision;
-  const double* lpq;
   double *bpt, *bov, *chi, *eps, *v, *sigma;
   double *d_freqs, *d_wts, *d_iw, *d_en;
   int *d_pidx, *d_orbs;

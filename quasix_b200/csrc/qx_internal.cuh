@@ -186,6 +186,12 @@ bool is_device_ptr(const void* p);
 // device pointer to read.
 const void* device_view(qx_ctx* ctx, int slot, const void* p, size_t bytes);
 
+// As device_view, but page-locked host memory with a device mapping is not
+// copied: the kernels read it in place over the host link, so only the bytes
+// they touch cross it (the setup gathers read lpq's upper triangle, half of
+// it).  For arrays that are read once, by kernels that touch part of them.
+const void* mapped_view(qx_ctx* ctx, int slot, const void* p, size_t bytes);
+
 inline int ceil_div(int a, int b) { return (a + b - 1) / b; }
 inline int round_up(int a, int b) { return ceil_div(a, b) * b; }
 
@@ -336,6 +342,10 @@ void launch_pair_contract_fp64(qx_ctx* ctx, const double* bpt, int ldk, int npai
 void launch_gather_pairs(qx_ctx* ctx, const double* lpq, int naux, int nmo, const int2* pairs, int npair,
                          double* bpt, int ldk);
 void launch_gather_ov(qx_ctx* ctx, const double* lpq, int naux, int nmo, int nocc, double* bov, int ldov);
+void launch_ov_from_pairs(qx_ctx* ctx, const double* bpt, int ldk, const int* pidx, int naux, int nmo, int nocc,
+                          double* bov, int ldov);
+void launch_exchange_pairs(qx_ctx* ctx, const double* bpt, int ldk, const int* pidx, int naux, int nmo, int nocc,
+                           int norbs, double* sx);
 // sx[p] = -sum_{R,i} lpq[R][p][i]^2 for every orbital, or only for the norbs
 // orbitals orbs (device array) when given.
 void launch_exchange_diag(qx_ctx* ctx, const double* lpq, int naux, int nmo, int nocc, double* sx,
