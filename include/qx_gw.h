@@ -9,7 +9,10 @@
  *    interleaved (re, im) doubles.
  *  - Every array argument may be a host pointer or a device pointer of the
  *    context's device; the library checks with cudaPointerGetAttributes and
- *    copies host data in and results out inside the call.
+ *    copies host data in and results out inside the call.  The lpq of
+ *    qx_evgw and qx_get_sigma_diag is not copied when it is page-locked
+ *    host memory: the setup kernels read the pairs they need from it in
+ *    place (with every orbital a target, its upper triangle p <= q).
  *  - Every call returns a qx_status; on failure qx_last_error(ctx) holds a
  *    message.  No exceptions cross the ABI and no device code traps.
  *  - A context owns one CUDA stream and a cached device workspace; calls on
