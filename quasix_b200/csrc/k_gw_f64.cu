@@ -989,31 +989,42 @@ void launch_invert_wc_group(qx_ctx* ctx, const GMat* mats_in, int G, int half_lo
 // Gathers.
 // bpt[p][P] = lpq[P][pairs[p].x][pairs[p].y]   (tiled transpose through smem)
 // ---------------------------------------------------------------------------
+// Tiles of 32 pairs x 32 aux rows, pair block fastest; a block walks the tiles
+// blockIdx.x, blockIdx.x + gridDim.x, ... (one tile each on a full grid; a
+// grid of one block per SM when lpq is host memory read over the host link,
+// which leaves room on every SM for the kernels that run beside it).
 __global__ void k_gather_pairs(const double* __restrict__ lpq, int naux, int nmo, const int2* __restrict__ pairs,
                                int npair, double* __restrict__ bpt, int ldk) {
   __shared__ double tile[32][33];
   __shared__ int off[32];
-  const int p0 = blockIdx.x * 32, P0 = blockIdx.y * 32;
-  if (threadIdx.y == 0) {
-    int p = p0 + threadIdx.x;
-    off[threadIdx.x] = (p < npair) ? pairs[p].x * nmo + pairs[p].y : 0;
-  }
-  __syncthreads();
-  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
-    int P = P0 + r, p = p0 + threadIdx.x;
-    tile[r][threadIdx.x] = (P < naux && p < npair) ? lpq[(size_t)P * nmo * nmo + off[threadIdx.x]] : 0.0;
-  }
-  __syncthreads();
-  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
-    int p = p0 + r, P = P0 + threadIdx.x;
-    if (p < npair && P < ldk) bpt[(size_t)p * ldk + P] = (P < naux) ? tile[threadIdx.x][r] : 0.0;
+  const int npb = (npair + 31) / 32, ntiles = npb * ((ldk + 31) / 32);
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const int Pb = t / npb;
+    const int p0 = (t - Pb * npb) * 32, P0 = Pb * 32;
+    if (threadIdx.y == 0) {
+      int p = p0 + threadIdx.x;
+      off[threadIdx.x] = (p < npair) ? pairs[p].x * nmo + pairs[p].y : 0;
+    }
+    __syncthreads();
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+      int P = P0 + r, p = p0 + threadIdx.x;
+      tile[r][threadIdx.x] = (P < naux && p < npair) ? lpq[(size_t)P * nmo * nmo + off[threadIdx.x]] : 0.0;
+    }
+    __syncthreads();
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+      int p = p0 + r, P = P0 + threadIdx.x;
+      if (p < npair && P < ldk) bpt[(size_t)p * ldk + P] = (P < naux) ? tile[threadIdx.x][r] : 0.0;
+    }
+    __syncthreads();
   }
 }
 
-void launch_gather_pairs(qx_ctx* ctx, const double* lpq, int naux, int nmo, const int2* pairs, int npair,
-                         double* bpt, int ldk) {
-  dim3 grid(ceil_div(npair, 32), ceil_div(ldk, 32));
-  k_gather_pairs<<<grid, dim3(32, 8), 0, ctx->stream>>>(lpq, naux, nmo, pairs, npair, bpt, ldk);
+void launch_gather_pairs(qx_ctx* ctx, cudaStream_t st, const double* lpq, int naux, int nmo, const int2* pairs,
+                         int npair, double* bpt, int ldk, int max_blocks) {
+  if (npair <= 0) return;
+  const int ntiles = ceil_div(npair, 32) * ceil_div(ldk, 32);
+  const int grid = max_blocks > 0 ? std::min(ntiles, max_blocks) : ntiles;
+  k_gather_pairs<<<grid, dim3(32, 8), 0, st>>>(lpq, naux, nmo, pairs, npair, bpt, ldk);
   check_launch(ctx);
 }
 

@@ -29,12 +29,16 @@ const void* device_view(qx_ctx* ctx, int slot, const void* p, size_t bytes) {
   return b.ptr;
 }
 
-const void* mapped_view(qx_ctx* ctx, int slot, const void* p, size_t bytes) {
+const void* mapped_view(qx_ctx* ctx, int slot, const void* p, size_t bytes, bool* in_place) {
+  if (in_place) *in_place = false;
   if (p != nullptr) {
     cudaPointerAttributes at;
     if (cudaPointerGetAttributes(&at, p) == cudaSuccess) {
       if (at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged) return p;
-      if (at.type == cudaMemoryTypeHost && at.devicePointer != nullptr) return at.devicePointer;
+      if (at.type == cudaMemoryTypeHost && at.devicePointer != nullptr) {
+        if (in_place) *in_place = true;
+        return at.devicePointer;
+      }
     } else {
       cudaGetLastError();
     }
@@ -146,7 +150,7 @@ __global__ void k_to_f32(const double* __restrict__ s, float* __restrict__ d, si
 }
 
 void gw_setup(qx_ctx* ctx, GWSystem& S, const double* d_lpq, int nmo, int nocc, int naux, const std::vector<int>& orbs,
-              int nw, double cutoff, double x0, int precision) {
+              int nw, double cutoff, double x0, int precision, bool host_lpq) {
   S.nmo = nmo;
   S.nocc = nocc;
   S.nvir = nmo - nocc;
@@ -197,18 +201,38 @@ void gw_setup(qx_ctx* ctx, GWSystem& S, const double* d_lpq, int nmo, int nocc, 
   QX_CUDA(cudaMemcpyAsync(S.d_pidx, ps.index.data(), ps.index.size() * sizeof(int), cudaMemcpyHostToDevice,
                           ctx->stream));
   QX_CUDA(cudaMemcpyAsync(S.d_orbs, orbs.data(), orbs.size() * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
-  launch_gather_pairs(ctx, d_lpq, naux, nmo, d_pairs, S.npair, S.bpt, S.ldk);
   // With every orbital a target the pair tensor holds the occupied-virtual
   // block: B_ov comes from it, and the setup reads only lpq's upper triangle.
   bool all_orbitals = S.norbs == nmo;
   for (int t = 0; all_orbitals && t < S.norbs; ++t) all_orbitals = orbs[t] == t;
+  // Host lpq read in place with every orbital a target: the pairs of the
+  // occupied rows (a < nocc, the first pairs in row-major order) hold B_ov and
+  // everything the exchange diagonal reads, so they are gathered first; the
+  // rest crosses the host link on the side stream, one block per SM, while the
+  // first P0 and inversion run, and the first contraction waits for it.
+  const bool overlap = host_lpq && all_orbitals;
+  const int npre = overlap ? std::min(S.npair, nocc * nmo - nocc * (nocc - 1) / 2) : S.npair;
+  launch_gather_pairs(ctx, ctx->stream, d_lpq, naux, nmo, d_pairs, npre, S.bpt, S.ldk);
   if (all_orbitals)
     launch_ov_from_pairs(ctx, S.bpt, S.ldk, S.d_pidx, naux, nmo, nocc, S.bov, S.ldov);
   else
     launch_gather_ov(ctx, d_lpq, naux, nmo, nocc, S.bov, S.ldov);
+  S.pairs_wait = nullptr;
+  if (npre < S.npair) {
+    if (!ctx->side) {
+      QX_CUDA(cudaStreamCreateWithFlags(&ctx->side, cudaStreamNonBlocking));
+      for (auto& e : ctx->side_ev) QX_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    }
+    QX_CUDA(cudaEventRecord(ctx->side_ev[0], ctx->stream));
+    QX_CUDA(cudaStreamWaitEvent(ctx->side, ctx->side_ev[0], 0));
+    launch_gather_pairs(ctx, ctx->side, d_lpq, naux, nmo, d_pairs + npre, S.npair - npre,
+                        S.bpt + (size_t)npre * S.ldk, S.ldk, ctx->sm_count);
+    QX_CUDA(cudaEventRecord(ctx->side_ev[1], ctx->side));
+    S.pairs_wait = ctx->side_ev[1];
+  }
+  S.pairs_split_due = false;
   if (is_tc_precision(precision)) {
     QX_REQUIRE(tc_supported(ctx), QX_ERR_NO_DEVICE, "tensor-core precision needs an sm_100 device");
-    const int fp16 = precision == QX_PREC_FP16X3;
     const size_t nb = (size_t)S.npair * S.ldk;
     ctx->ws[WS_BPT_HI].reserve(nb * 2);
     ctx->ws[WS_BPT_LO].reserve(nb * 2);
@@ -216,15 +240,29 @@ void gw_setup(qx_ctx* ctx, GWSystem& S, const double* d_lpq, int nmo, int nocc, 
     S.bpt_split.hi = ctx->ws[WS_BPT_HI].ptr;
     S.bpt_split.lo = ctx->ws[WS_BPT_LO].ptr;
     S.bpt_f32 = ctx->ws[WS_BPT_F32].as<float>();
-    launch_split(ctx, S.bpt, S.npair, S.ldk, S.ldk, S.bpt_split.hi, S.bpt_split.lo, S.ldk, 0, 0, 1, fp16, 2,
-                 &S.bpt_split.scale);
-    k_to_f32<<<1184, 256, 0, ctx->stream>>>(S.bpt, S.bpt_f32, nb);
-    check_launch(ctx);
+    S.pairs_split_due = true;
     const size_t nwc = (size_t)nw * S.eps_stride;
     ctx->ws[WS_WC_HI].reserve(nwc * 2);
     ctx->ws[WS_WC_LO].reserve(nwc * 2);
     S.wc_split.hi = ctx->ws[WS_WC_HI].ptr;
     S.wc_split.lo = ctx->ws[WS_WC_LO].ptr;
+  }
+  if (!S.pairs_wait) gw_pairs_ready(ctx, S);
+}
+
+void gw_pairs_ready(qx_ctx* ctx, GWSystem& S) {
+  if (S.pairs_wait) {
+    QX_CUDA(cudaStreamWaitEvent(ctx->stream, S.pairs_wait, 0));
+    S.pairs_wait = nullptr;
+  }
+  if (S.pairs_split_due) {
+    const int fp16 = S.precision == QX_PREC_FP16X3;
+    const size_t nb = (size_t)S.npair * S.ldk;
+    launch_split(ctx, S.bpt, S.npair, S.ldk, S.ldk, S.bpt_split.hi, S.bpt_split.lo, S.ldk, 0, 0, 1, fp16, 2,
+                 &S.bpt_split.scale);
+    k_to_f32<<<1184, 256, 0, ctx->stream>>>(S.bpt, S.bpt_f32, nb);
+    check_launch(ctx);
+    S.pairs_split_due = false;
   }
 }
 
@@ -283,6 +321,7 @@ void gw_wc_p0(qx_ctx* ctx, GWSystem& S, const double* e_host) {
 
 // v[w][pair] = Wc_nm(iw) of every pair, from S.eps holding W' (half-lower Wc).
 void gw_wc_contract(qx_ctx* ctx, GWSystem& S) {
+  gw_pairs_ready(ctx, S);
   record_stage(ctx, QX_ST_CONTRACT, true);
   if (is_tc_precision(S.precision)) {
     const int fp16 = S.precision == QX_PREC_FP16X3;
@@ -460,6 +499,12 @@ void validate_common(int nmo, int nocc, int naux) {
 
 using namespace qx;
 
+// A call that fails may leave setup work on the side stream reading the
+// caller's host arrays: it ends before the call returns.
+static void settle_side(qx_ctx* ctx) {
+  if (ctx && ctx->side) cudaStreamSynchronize(ctx->side);
+}
+
 template <class F>
 static qx_status guarded(qx_ctx* ctx, F&& f) {
   try {
@@ -473,12 +518,15 @@ static qx_status guarded(qx_ctx* ctx, F&& f) {
     if (ctx) ctx->err.clear();
     return QX_OK;
   } catch (const Error& e) {
+    settle_side(ctx);
     if (ctx) ctx->err = e.what();
     return e.status;
   } catch (const std::bad_alloc&) {
+    settle_side(ctx);
     if (ctx) ctx->err = "host allocation failed";
     return QX_ERR_CUDA;
   } catch (const std::exception& e) {
+    settle_side(ctx);
     if (ctx) ctx->err = e.what();
     return QX_ERR_INVALID_INPUT;
   }
@@ -530,6 +578,10 @@ qx_status qx_ctx_destroy(qx_ctx* c) {
     if (e) cudaEventDestroy(e);
   if (c->sweep_hi) cudaStreamDestroy(c->sweep_hi);
   if (c->sweep_lo) cudaStreamDestroy(c->sweep_lo);
+  if (c->side) cudaStreamSynchronize(c->side);
+  for (auto& e : c->side_ev)
+    if (e) cudaEventDestroy(e);
+  if (c->side) cudaStreamDestroy(c->side);
   for (auto& e : c->ev)
     if (e) cudaEventDestroy(e);
   if (c->own_stream) cudaStreamDestroy(c->own_stream);
@@ -748,11 +800,14 @@ qx_status qx_evgw(qx_ctx* ctx, const double* mo_energy, const double* lpq, const
     // Page-locked host lpq is read in place: the setup gathers its upper
     // triangle (the pairs p <= q) straight into the pair tensor, and nothing
     // reads it afterwards, so half of it crosses the host link.
-    const double* d_lpq = (const double*)mapped_view(ctx, WS_LPQ, lpq, (size_t)naux * nmo * nmo * sizeof(double));
+    bool in_place = false;
+    const double* d_lpq =
+        (const double*)mapped_view(ctx, WS_LPQ, lpq, (size_t)naux * nmo * nmo * sizeof(double), &in_place);
     std::vector<int> orbs(nmo);
     for (int i = 0; i < nmo; ++i) orbs[i] = i;
     GWSystem S;
-    gw_setup(ctx, S, d_lpq, nmo, nocc, naux, orbs, cfg.nfreq, cfg.iw_cutoff, cfg.x0, cfg.precision);
+    gw_setup(ctx, S, d_lpq, nmo, nocc, naux, orbs, cfg.nfreq, cfg.iw_cutoff, cfg.x0, cfg.precision,
+             /*host_lpq=*/in_place);
     std::vector<int> fit = pade_indices(S.nws, cfg.npade);
     const int nfit = (int)fit.size();
     QX_REQUIRE(nfit > 0, QX_ERR_INVALID_INPUT, "not enough sigma points for a Pade fit (nw_sigma=%d)", S.nws);

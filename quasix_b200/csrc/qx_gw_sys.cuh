@@ -22,6 +22,11 @@ struct GWSystem {
   double *d_freqs, *d_wts, *d_iw, *d_en;
   int *d_pidx, *d_orbs;
   size_t eps_stride;
+  // The rest of the pair gather may still run on the context's side stream
+  // (pairs_wait: the event to wait on), and the pair tensor's split forms may
+  // still be due; gw_pairs_ready settles both before the first contraction.
+  cudaEvent_t pairs_wait = nullptr;
+  bool pairs_split_due = false;
   std::vector<int> orbs;
   SigmaGrid grid;
   TcOperand bpt_split{}, wc_split{};
@@ -35,8 +40,13 @@ struct GWSystem {
 
 SigmaGrid sigma_grid(int nw, double cutoff, double x0);
 PairSet build_pairs(const std::vector<int>& orbs, int nmo);
+// host_lpq: d_lpq is host memory read in place over the host link (the
+// setup then overlaps part of its gather with the first P0 and inversion).
 void gw_setup(qx_ctx* ctx, GWSystem& S, const double* d_lpq, int nmo, int nocc, int naux, const std::vector<int>& orbs,
-              int nw, double cutoff, double x0, int precision);
+              int nw, double cutoff, double x0, int precision, bool host_lpq = false);
+// Before the first contraction: wait for the rest of the pair gather and
+// make the pair tensor's split forms.
+void gw_pairs_ready(qx_ctx* ctx, GWSystem& S);
 void gw_wc_pairs(qx_ctx* ctx, GWSystem& S, const double* e_host);
 // The two halves of gw_wc_pairs around the inversion of S.eps (to W', the
 // half-lower Wc): P0 into S.eps, then the pair contraction.

@@ -119,6 +119,11 @@ struct qx_ctx {
   // Streams of the look-ahead inversion (critical chain at high priority,
   // trailing updates at low priority) and their events; created on first use.
   cudaStream_t sweep_hi = nullptr, sweep_lo = nullptr;
+  // Side stream of the setup (the rest of the pair gather from host lpq,
+  // beside the first P0 and inversion) and its two events: prefix gathered,
+  // all pairs gathered; created on first use.
+  cudaStream_t side = nullptr;
+  cudaEvent_t side_ev[2] = {};
   // Batch workers share the GPU with each other: their look-ahead streams keep
   // the default priority (a high-priority chain there stalls the other
   // workers' kernels while SMs drain for its large-shared-memory CTAs).
@@ -190,7 +195,8 @@ const void* device_view(qx_ctx* ctx, int slot, const void* p, size_t bytes);
 // copied: the kernels read it in place over the host link, so only the bytes
 // they touch cross it (the setup gathers read lpq's upper triangle, half of
 // it).  For arrays that are read once, by kernels that touch part of them.
-const void* mapped_view(qx_ctx* ctx, int slot, const void* p, size_t bytes);
+// *in_place (when given) tells whether the result is such host memory.
+const void* mapped_view(qx_ctx* ctx, int slot, const void* p, size_t bytes, bool* in_place = nullptr);
 
 inline int ceil_div(int a, int b) { return (a + b - 1) / b; }
 inline int round_up(int a, int b) { return ceil_div(a, b) * b; }
@@ -339,8 +345,10 @@ void launch_pair_contract_fp64(qx_ctx* ctx, const double* bpt, int ldk, int npai
                                int ldn, size_t wc_stride, int nw, double* v, int ldv);
 
 // Gathers.
-void launch_gather_pairs(qx_ctx* ctx, const double* lpq, int naux, int nmo, const int2* pairs, int npair,
-                         double* bpt, int ldk);
+// bpt[p][P] = lpq[P][pairs[p].x][pairs[p].y] on stream st; max_blocks > 0
+// caps the grid (the blocks then walk the tiles).
+void launch_gather_pairs(qx_ctx* ctx, cudaStream_t st, const double* lpq, int naux, int nmo, const int2* pairs,
+                         int npair, double* bpt, int ldk, int max_blocks = 0);
 void launch_gather_ov(qx_ctx* ctx, const double* lpq, int naux, int nmo, int nocc, double* bov, int ldov);
 void launch_ov_from_pairs(qx_ctx* ctx, const double* bpt, int ldk, const int* pidx, int naux, int nmo, int nocc,
                           double* bov, int ldov);
