@@ -58,3 +58,18 @@ def test_sigma_all_orbitals_pinned_matches_oracle():
     got, _ = q.get_sigma_diag(s.mo_energy, pinned_t.numpy(), orbs, s.nocc, nw=12, precision="fp64")
     ref, _ = O.get_sigma_diag(s.mo_energy, s.lpq, orbs, s.nocc, nw=12)
     assert np.abs(got - ref).max() < 1e-10 * max(1.0, np.abs(ref).max())
+
+
+def test_sigma_subset_pinned_matches_device():
+    """get_sigma_diag over a few targets (B_ov gathered from lpq itself, in
+    place over the host link) from page-locked host lpq: the same bits as from
+    device lpq."""
+    import torch
+    import quasix_b200 as q
+    s = make_system(7, 33, 140, seed=14, pi_norm=3.0)
+    orbs = [0, 5, 6, 7, 20]
+    pinned_t = torch.from_numpy(s.lpq).pin_memory()
+    for prec in ("fp64", "fp16x3"):
+        a, _ = q.get_sigma_diag(s.mo_energy, pinned_t.numpy(), orbs, s.nocc, nw=12, precision=prec)
+        b, _ = q.get_sigma_diag(s.mo_energy, torch.from_numpy(s.lpq).cuda(), orbs, s.nocc, nw=12, precision=prec)
+        assert np.array_equal(a, b), prec
